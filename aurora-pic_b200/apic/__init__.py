@@ -1,0 +1,335 @@
+"""Python bindings (ctypes) to libaurorapic_b200.so, the B200-native
+electrostatic PIC particle step.
+
+The library is the product; this module only marshals arguments across the
+C ABI declared in include/aurorapic_b200.h.  It loads the in-tree library
+and fails loudly when it is missing -- there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libaurorapic_b200.so")
+
+MAX_SPECIES = 4
+MAX_MODELS = 4
+MAX_CHANNELS = 8
+
+PERIODIC, DIRICHLET = 0, 1
+NORMALIZED, SI = 0, 1
+FP64, FP32 = 0, 1
+ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, CHARGE_EXCHANGE = range(5)
+ISOTROPIC, BACKWARD = 0, 1
+
+STATUS = {
+    0: "APIC_OK", 1: "APIC_ERR_INVALID", 2: "APIC_ERR_CUDA", 3: "APIC_ERR_CAPACITY",
+    4: "APIC_ERR_MAJORANT", 5: "APIC_ERR_CANDIDATES", 6: "APIC_ERR_NONFINITE",
+    7: "APIC_ERR_TIMEOUT", 8: "APIC_ERR_UNSUPPORTED", 9: "APIC_ERR_STATE", 10: "APIC_ERR_NO_DEVICE",
+}
+
+
+class ApicError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class McChannel(C.Structure):
+    _fields_ = [
+        ("process", C.c_int), ("angular", C.c_int), ("energy_frame", C.c_int),
+        ("threshold_energy", C.c_double), ("secondary_species", C.c_int), ("ion_species", C.c_int),
+        ("rows", C.c_size_t), ("energy", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)),
+    ]
+
+
+class MccModel(C.Structure):
+    _fields_ = [
+        ("species", C.c_int), ("neutral_density", C.c_double), ("max_frequency", C.c_double),
+        ("neutral_mass", C.c_double), ("neutral_temperature", C.c_double), ("gas_units_si", C.c_int),
+        ("max_candidates", C.c_size_t), ("nch", C.c_int), ("ch", McChannel * MAX_CHANNELS),
+    ]
+
+
+class VoltageDrive(C.Structure):
+    _fields_ = [("amplitude", C.c_double), ("frequency", C.c_double), ("phase", C.c_double)]
+
+
+class SpeciesCfg(C.Structure):
+    _fields_ = [("charge", C.c_double), ("mass", C.c_double), ("weight", C.c_double),
+                ("capacity", C.c_size_t)]
+
+
+class Config1D(C.Structure):
+    _fields_ = [
+        ("boundary", C.c_int), ("velocity_dimensions", C.c_int), ("units", C.c_int),
+        ("relative_permittivity", C.c_double), ("nx", C.c_size_t), ("length", C.c_double),
+        ("dt", C.c_double), ("phi_left", C.c_double), ("phi_right", C.c_double),
+        ("drive_left", VoltageDrive), ("drive_right", VoltageDrive), ("precision", C.c_int),
+        ("seed", C.c_uint64), ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
+        ("nmodels", C.c_int), ("models", MccModel * MAX_MODELS),
+    ]
+
+
+class Sample1D(C.Structure):
+    _fields_ = [
+        ("step", C.c_uint64), ("time", C.c_double), ("kinetic_energy", C.c_double),
+        ("field_energy", C.c_double), ("total_energy", C.c_double), ("charge_l1", C.c_double),
+        ("live_particles", C.c_uint64), ("phi_left", C.c_double), ("phi_right", C.c_double),
+        ("kinetic_by_species", C.c_double * MAX_SPECIES), ("live_by_species", C.c_uint64 * MAX_SPECIES),
+    ]
+
+
+class CollisionTotals(C.Structure):
+    _fields_ = [
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64),
+        ("channel_collisions", (C.c_uint64 * MAX_CHANNELS) * MAX_MODELS),
+        ("channel_energy_change", (C.c_double * MAX_CHANNELS) * MAX_MODELS),
+    ]
+
+
+class BoundaryLoss(C.Structure):
+    _fields_ = [("absorbed_left", C.c_uint64), ("absorbed_right", C.c_uint64),
+                ("kinetic_energy_left", C.c_double), ("kinetic_energy_right", C.c_double)]
+
+
+class CollideStats(C.Structure):
+    _fields_ = [
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64),
+        ("channel_collisions", C.c_uint32 * MAX_CHANNELS), ("energy_change", C.c_double * MAX_CHANNELS),
+        ("nsecondaries", C.c_int), ("secondary_channel", C.c_int * 4),
+        ("secondary_velocity", (C.c_double * 3) * 4), ("secondary_ion_velocity", (C.c_double * 3) * 4),
+        ("removed", C.c_int), ("draws", C.c_uint32),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+_U8P = C.POINTER(C.c_uint8)
+_U64P = C.POINTER(C.c_uint64)
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Loads the in-tree library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libaurorapic_b200.so is not built ({LIB_PATH}); run aurora-pic_b200/build.py")
+    L = C.CDLL(LIB_PATH)
+    L.apic_version.restype = C.c_char_p
+    L.apic_status_string.restype = C.c_char_p
+    L.apic_sim1d_create.argtypes = [C.POINTER(Config1D), C.POINTER(C.c_void_p)]
+    L.apic_sim1d_destroy.argtypes = [C.c_void_p]
+    L.apic_sim1d_last_error.restype = C.c_char_p
+    L.apic_sim1d_last_error.argtypes = [C.c_void_p]
+    L.apic_sim1d_load_particles.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _DP, _DP, _U8P]
+    L.apic_sim1d_initialize.argtypes = [C.c_void_p]
+    L.apic_sim1d_resume.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
+    L.apic_sim1d_step.argtypes = [C.c_void_p, C.c_size_t]
+    L.apic_sim1d_synchronize.argtypes = [C.c_void_p]
+    L.apic_sim1d_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
+    L.apic_sim1d_read_particles.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _DP, _DP,
+                                            C.POINTER(C.c_size_t)]
+    L.apic_sim1d_read_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+    L.apic_sim1d_sample.argtypes = [C.c_void_p, C.POINTER(Sample1D)]
+    L.apic_sim1d_collision_totals.argtypes = [C.c_void_p, C.POINTER(CollisionTotals)]
+    L.apic_sim1d_boundary_losses.argtypes = [C.c_void_p, C.c_int, C.POINTER(BoundaryLoss)]
+    L.apic_sim1d_time.restype = C.c_double
+    L.apic_sim1d_time.argtypes = [C.c_void_p]
+    L.apic_sim1d_step_count.restype = C.c_uint64
+    L.apic_sim1d_step_count.argtypes = [C.c_void_p]
+    L.apic_deposit_solve_gather_1d.argtypes = [
+        C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _DP, _DP,
+        C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
+    L.apic_collide3.argtypes = [C.POINTER(MccModel), C.c_double, C.c_size_t, _DP, C.c_double, _U64P, _U64P,
+                                C.c_uint64, C.c_uint64, C.c_uint32, C.POINTER(CollideStats)]
+    _lib = L
+    return L
+
+
+def dptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_DP)
+
+
+def _check(rc: int, handle=None) -> None:
+    if rc != 0:
+        msg = lib().apic_sim1d_last_error(handle).decode() if handle is not None else ""
+        if not msg:
+            msg = lib().apic_sim1d_last_error(None).decode()
+        raise ApicError(rc, msg)
+
+
+class Tables:
+    """Owns the numpy arrays behind the table pointers of a configuration."""
+
+    def __init__(self):
+        self.keep = []
+
+    def channel(self, process, energy, sigma, threshold=0.0, secondary=-1, ion=-1, angular=ISOTROPIC,
+                frame=0) -> McChannel:
+        e = np.ascontiguousarray(energy, dtype=np.float64)
+        s = np.ascontiguousarray(sigma, dtype=np.float64)
+        self.keep += [e, s]
+        return McChannel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+
+
+def mcc_model(species, channels, neutral_density, max_frequency, neutral_mass=0.0, neutral_temperature=0.0,
+              gas_units_si=1, max_candidates=64) -> MccModel:
+    m = MccModel()
+    m.species = species
+    m.neutral_density = neutral_density
+    m.max_frequency = max_frequency
+    m.neutral_mass = neutral_mass
+    m.neutral_temperature = neutral_temperature
+    m.gas_units_si = gas_units_si
+    m.max_candidates = max_candidates
+    m.nch = len(channels)
+    for i, ch in enumerate(channels):
+        m.ch[i] = ch
+    return m
+
+
+def config1d(*, boundary, velocity_dimensions, units, nx, length, dt, species, models=(), phi_left=0.0,
+             phi_right=0.0, drive_left=(0.0, 0.0, 0.0), drive_right=(0.0, 0.0, 0.0), precision=FP64, seed=1,
+             relative_permittivity=1.0) -> Config1D:
+    c = Config1D()
+    c.boundary, c.velocity_dimensions, c.units = boundary, velocity_dimensions, units
+    c.relative_permittivity = relative_permittivity
+    c.nx, c.length, c.dt = nx, length, dt
+    c.phi_left, c.phi_right = phi_left, phi_right
+    c.drive_left = VoltageDrive(*drive_left)
+    c.drive_right = VoltageDrive(*drive_right)
+    c.precision, c.seed = precision, seed
+    c.nspecies = len(species)
+    for i, (q, m, w, cap) in enumerate(species):
+        c.species[i] = SpeciesCfg(q, m, w, cap)
+    c.nmodels = len(models)
+    for i, mm in enumerate(models):
+        c.models[i] = mm
+    return c
+
+
+class Simulation1D:
+    """pic::Simulation (1D1V/1D3V) on the device, through the C ABI."""
+
+    def __init__(self, cfg: Config1D, tables: Tables | None = None):
+        self.cfg = cfg
+        self._tables = tables
+        h = C.c_void_p()
+        rc = lib().apic_sim1d_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise ApicError(rc, lib().apic_sim1d_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().apic_sim1d_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def load(self, species, x, v, v_half=None, vy=None, vz=None, alive=None):
+        n = len(x)
+        conv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        x, v, v_half, vy, vz = map(conv, (x, v, v_half, vy, vz))
+        al = None if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        _check(lib().apic_sim1d_load_particles(self.h, species, n, dptr(x), dptr(v), dptr(v_half), dptr(vy),
+                                               dptr(vz), None if al is None else al.ctypes.data_as(_U8P)), self.h)
+
+    def initialize(self):
+        _check(lib().apic_sim1d_initialize(self.h), self.h)
+
+    def resume(self, time, step):
+        _check(lib().apic_sim1d_resume(self.h, time, step), self.h)
+
+    def step(self, n=1):
+        _check(lib().apic_sim1d_step(self.h, n), self.h)
+
+    def synchronize(self):
+        _check(lib().apic_sim1d_synchronize(self.h), self.h)
+
+    def count(self, species) -> int:
+        n = C.c_size_t()
+        _check(lib().apic_sim1d_count(self.h, species, C.byref(n)), self.h)
+        return n.value
+
+    def particles(self, species) -> dict:
+        n = self.count(species)
+        out = {k: np.zeros(n) for k in ("x", "v", "vh", "vy", "vz")}
+        got = C.c_size_t()
+        _check(lib().apic_sim1d_read_particles(self.h, species, n, *[dptr(out[k]) for k in ("x", "v", "vh", "vy", "vz")],
+                                               C.byref(got)), self.h)
+        return out
+
+    def fields(self):
+        n = self.cfg.nx
+        rho, phi, E = np.zeros(n), np.zeros(n), np.zeros(n)
+        _check(lib().apic_sim1d_read_fields(self.h, dptr(rho), dptr(phi), dptr(E)), self.h)
+        return rho, phi, E
+
+    def sample(self) -> Sample1D:
+        s = Sample1D()
+        _check(lib().apic_sim1d_sample(self.h, C.byref(s)), self.h)
+        return s
+
+    def collision_totals(self) -> CollisionTotals:
+        t = CollisionTotals()
+        _check(lib().apic_sim1d_collision_totals(self.h, C.byref(t)), self.h)
+        return t
+
+    def boundary_losses(self, species) -> BoundaryLoss:
+        b = BoundaryLoss()
+        _check(lib().apic_sim1d_boundary_losses(self.h, species, C.byref(b)), self.h)
+        return b
+
+    @property
+    def time(self) -> float:
+        return lib().apic_sim1d_time(self.h)
+
+    @property
+    def step_count(self) -> int:
+        return lib().apic_sim1d_step_count(self.h)
+
+
+def deposit_solve_gather_1d(boundary, nx, length, permittivity, phi_left, phi_right, charges, weights, xs, xq=None):
+    ns = len(xs)
+    xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]
+    counts = (C.c_size_t * ns)(*[len(x) for x in xs])
+    ptrs = (_DP * ns)(*[dptr(x) for x in xs])
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    rho, phi, E = np.zeros(nx), np.zeros(nx), np.zeros(nx)
+    xq = np.zeros(0) if xq is None else np.ascontiguousarray(xq, dtype=np.float64)
+    eq = np.zeros(len(xq))
+    rc = lib().apic_deposit_solve_gather_1d(boundary, nx, length, permittivity, phi_left, phi_right, ns, dptr(q),
+                                            dptr(w), counts, ptrs, dptr(rho), dptr(phi), dptr(E), len(xq),
+                                            dptr(xq) if len(xq) else None, dptr(eq) if len(xq) else None)
+    _check(rc)
+    return rho, phi, E, eq
+
+
+def collide3(model: MccModel, particle_mass, v3, dt, draws=None, offsets=None, seed=0, step=0, stream=0):
+    v3 = np.ascontiguousarray(v3, dtype=np.float64).copy()
+    n = v3.shape[0]
+    stats = (CollideStats * n)()
+    if draws is not None:
+        draws = np.ascontiguousarray(draws, dtype=np.uint64)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        dp, op = draws.ctypes.data_as(_U64P), offsets.ctypes.data_as(_U64P)
+    else:
+        dp = op = None
+    _check(lib().apic_collide3(C.byref(model), particle_mass, n, dptr(v3), dt, dp, op, seed, step, stream, stats))
+    return v3, stats

@@ -1,0 +1,184 @@
+"""Synthetic inputs for the named workloads of the particle step.
+
+Every workload is seeded and fully determined by its arguments.  The same
+arrays feed the device library, the CPU oracle and the reference harness, so
+parity tests and benchmarks run on identical inputs.
+
+Cross sections are analytic forms tabulated once on a shared energy grid
+(the reference reads tables, src/Collision.cpp:158-219, and interpolates
+linearly, :221-237):
+
+* electron elastic momentum transfer  6e-20 / sqrt(1 + E/10 eV) m^2
+* electron excitation, threshold 19.8 eV: 1.5e-21 * t * exp(1 - t) m^2,
+  t = (E - 19.8 eV) / (60 eV - 19.8 eV)          (peak 1.5e-21 m^2 at 60 eV)
+* electron ionization, threshold 24.6 eV: 3.5e-21 * t * exp(1 - t) m^2,
+  t = (E - 24.6 eV) / (120 eV - 24.6 eV)         (peak 3.5e-21 m^2 at 120 eV)
+* ion isotropic elastic 2e-19 m^2 and resonant charge exchange 5e-19 m^2.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+E_CHARGE = 1.602176634e-19
+M_E = 9.1093837139e-31
+AMU = 1.66053906660e-27
+K_B = 1.380649e-23
+EPS0 = 8.8541878128e-12
+
+ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, CHARGE_EXCHANGE = range(5)
+
+
+def hump(E, threshold, peak_energy, peak):
+    t = np.clip((E - threshold) / (peak_energy - threshold), 0.0, None)
+    return peak * t * np.exp(1.0 - t)
+
+
+@dataclass
+class ChannelSpec:
+    process: int
+    energy: np.ndarray  # J
+    sigma: np.ndarray   # m^2
+    threshold: float = 0.0  # J
+    secondary: int = -1
+    ion: int = -1
+
+
+@dataclass
+class ModelSpec:
+    species: int
+    channels: list
+    neutral_density: float
+    max_frequency: float
+    neutral_mass: float
+    neutral_temperature: float
+    max_candidates: int = 64
+
+
+@dataclass
+class SpeciesSpec:
+    charge: float
+    mass: float
+    weight: float
+    capacity: int
+    x: np.ndarray
+    v: np.ndarray
+    vy: np.ndarray | None = None
+    vz: np.ndarray | None = None
+
+
+@dataclass
+class Workload1D:
+    name: str
+    dirichlet: bool
+    vdim: int
+    si: bool
+    nx: int
+    length: float
+    dt: float
+    species: list
+    models: list = field(default_factory=list)
+    phi_left: float = 0.0
+    phi_right: float = 0.0
+    drive_left: tuple = (0.0, 0.0, 0.0)
+    drive_right: tuple = (0.0, 0.0, 0.0)
+    steps: int = 100
+
+    @property
+    def particles(self) -> int:
+        return sum(len(s.x) for s in self.species)
+
+
+def two_stream(particles_per_beam=16384, nx=256, seed=1, steps=2000) -> Workload1D:
+    """1D1V electrostatic two-stream instability in normalized units
+    (omega_p = 1, lambda_D = 1): L = 2 pi / 0.5, beams at +/-1.0 with 0.01
+    Maxwellian spread, positions U[0, L) plus a 1e-3 cos(k x) displacement."""
+    L = 2 * math.pi / 0.5
+    k = 2 * math.pi / L
+    n = 2 * particles_per_beam
+    w = L / n  # unit mean density
+    rx = np.random.default_rng(seed)
+    rv = np.random.default_rng(seed + 1)
+    sp = []
+    for sign in (1.0, -1.0):
+        x = rx.uniform(0.0, L, particles_per_beam)
+        x = np.mod(x + 1e-3 * np.cos(k * x), L)
+        v = sign * 1.0 + 0.01 * rv.standard_normal(particles_per_beam)
+        sp.append(SpeciesSpec(-1.0, 1.0, w, particles_per_beam, x, v))
+    return Workload1D("two_stream_1d1v", False, 1, False, nx, L, 0.1, sp, steps=steps)
+
+
+def _rate_bound(mass, channels, e_max_ev, neutral_density, neutral_mass, temperature, grid=20001):
+    s_max = math.sqrt(2 * e_max_ev * E_CHARGE / mass)
+    v = np.linspace(0.0, s_max, grid)
+    spread = 8.0 * math.sqrt(K_B * temperature / neutral_mass) if temperature > 0 else 0.0
+    tot = np.zeros_like(v)
+    for ch in channels:
+        E = 0.5 * mass * v ** 2
+        tot += np.where(E >= ch.threshold, np.interp(E, ch.energy, ch.sigma), 0.0)
+    return float(np.max(neutral_density * tot * (v + spread)))
+
+
+def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096) -> Workload1D:
+    """1D3V capacitive RF discharge with null-collision MCC: Dirichlet gap
+    0.067 m, `cells` cells, grounded left electrode, right electrode driven at
+    450 V / 13.56 MHz, dt = 1 / (400 f); electrons and He+ (4 amu) at
+    particles_per_cell per cell each, Maxwellian Te = 1 eV, Ti = 0.026 eV;
+    neutral helium 9.64e20 m^-3 at 300 K (thermal neutrals).  max_frequency is
+    1.25 x the thermal-neutral rate bound over each table's energy range."""
+    f_rf = 13.56e6
+    L = 0.067
+    nx = cells + 1
+    n = particles_per_cell * cells
+    n0 = 2.56e14
+    w = n0 * L / n
+    m_he = 4 * AMU
+    ng = 9.64e20
+    T = 300.0
+    Ee = np.concatenate([[0.0], np.logspace(-3, 4, table_rows - 1)])
+    Ei = np.concatenate([[0.0], np.logspace(-3, math.log10(2000.0), table_rows // 2 - 1)])
+    e_ch = [
+        ChannelSpec(ELASTIC, Ee * E_CHARGE, 6e-20 / np.sqrt(1 + Ee / 10.0)),
+        ChannelSpec(EXCITATION, Ee * E_CHARGE, hump(Ee, 19.8, 60.0, 1.5e-21), 19.8 * E_CHARGE),
+        ChannelSpec(IONIZATION, Ee * E_CHARGE, hump(Ee, 24.6, 120.0, 3.5e-21), 24.6 * E_CHARGE, 0, 1),
+    ]
+    i_ch = [
+        ChannelSpec(ELASTIC, Ei * E_CHARGE, np.full_like(Ei, 2e-19)),
+        ChannelSpec(CHARGE_EXCHANGE, Ei * E_CHARGE, np.full_like(Ei, 5e-19)),
+    ]
+    nu_e = 1.25 * _rate_bound(M_E, e_ch, 1e4, ng, m_he, T)
+    nu_i = 1.25 * _rate_bound(m_he, i_ch, 2000.0, ng, m_he, T)
+    rng = np.random.default_rng(seed)
+    ve = math.sqrt(E_CHARGE * 1.0 / M_E)
+    vi = math.sqrt(E_CHARGE * 0.026 / m_he)
+    cap = int(n * 1.5) + 4096
+    sp = []
+    for q, m, vt in ((-E_CHARGE, M_E, ve), (E_CHARGE, m_he, vi)):
+        x = rng.uniform(0.0, L, n)
+        v3 = vt * rng.standard_normal((3, n))
+        sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), v3[1].copy(), v3[2].copy()))
+    models = [
+        ModelSpec(0, e_ch, ng, nu_e, m_he, T),
+        ModelSpec(1, i_ch, ng, nu_i, m_he, T),
+    ]
+    return Workload1D("ccp_helium_1d3v", True, 3, True, nx, L, 1.0 / (400 * f_rf), sp, models,
+                      drive_right=(450.0, f_rf, 0.0), steps=steps)
+
+
+def to_device_config(wl: Workload1D, precision=0, seed=1):
+    """Builds the device library's apic_config1d (and the table keeper)."""
+    from . import (DIRICHLET, PERIODIC, SI, NORMALIZED, Tables, config1d, mcc_model)
+    tabs = Tables()
+    models = []
+    for m in wl.models:
+        chans = [tabs.channel(c.process, c.energy, c.sigma, c.threshold, c.secondary, c.ion) for c in m.channels]
+        models.append(mcc_model(m.species, chans, m.neutral_density, m.max_frequency, m.neutral_mass,
+                                m.neutral_temperature, 1 if wl.si else 0, m.max_candidates))
+    cfg = config1d(boundary=DIRICHLET if wl.dirichlet else PERIODIC, velocity_dimensions=wl.vdim,
+                   units=SI if wl.si else NORMALIZED, nx=wl.nx, length=wl.length, dt=wl.dt,
+                   species=[(s.charge, s.mass, s.weight, s.capacity) for s in wl.species], models=models,
+                   phi_left=wl.phi_left, phi_right=wl.phi_right, drive_left=wl.drive_left,
+                   drive_right=wl.drive_right, precision=precision, seed=seed)
+    return cfg, tabs

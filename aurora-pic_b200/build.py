@@ -1,0 +1,74 @@
+"""Builds libaurorapic_b200.so in-tree for sm_100a with nvcc.
+
+Usage: python aurora-pic_b200/build.py [--force]
+
+Every .cu file under csrc/ is compiled separately with its own flags (the
+FP64 files that must keep the reference's rounding are built with
+--fmad=false), then linked into one shared library exporting the C ABI
+declared in include/aurorapic_b200.h.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "lib")
+LIB = os.path.join(OUT_DIR, "libaurorapic_b200.so")
+OBJ_DIR = os.path.join(HERE, "_build")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
+          "--expt-relaxed-constexpr", "--extended-lambda", "-I", os.path.join(ROOT, "include")]
+# Files whose FP64 arithmetic mirrors the reference operation by operation.
+NO_FMA = {"pic1d.cu", "pic2d3d.cu"}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def sources():
+    return sorted(f for f in os.listdir(CSRC) if f.endswith(".cu"))
+
+
+def headers():
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))] + [
+        os.path.join(ROOT, "include", "aurorapic_b200.h")]
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(OUT_DIR, exist_ok=True)
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    hdr_mtime = max(os.path.getmtime(h) for h in headers())
+    objs = []
+    for src in sources():
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(OBJ_DIR, src.replace(".cu", ".o"))
+        objs.append(obj)
+        if not force and os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(path), hdr_mtime):
+            continue
+        flags = list(COMMON) + ARCH
+        flags += ["--fmad=false"] if src in NO_FMA else ["--fmad=true"]
+        if os.environ.get("APIC_PTXAS_VERBOSE"):
+            flags += ["-Xptxas", "-v"]
+        cmd = [nvcc()] + flags + ["-c", path, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,239 @@
+// Null-collision Monte Carlo collisions on the device.
+//
+// collide3() follows NullCollisionModel::collide(Vec3&) (src/Collision.cpp:907-993)
+// decision for decision: exponential waiting times at the majorant, thermal
+// neutral sampling, channel selection against cumulative rates, channel
+// kinematics (src/Collision.cpp:762-829) and ionization secondaries.  The
+// per-candidate full-table frequency-bound scan of the reference
+// (validate_frequency_bound, src/Collision.cpp:627-685) becomes a precomputed
+// safe speed: below it the bound provably holds, above it the exact check runs
+// and a violation sets APIC_ERR_MAJORANT instead of throwing.
+#pragma once
+#include "apic_rng.cuh"
+
+namespace apic {
+
+constexpr int kMaxChannels = 8;
+constexpr double kThermalSigma = 8.0;  // include/pic/Collision.hpp:139
+constexpr double kDblEpsilon = 2.220446049250313080847e-16;
+
+enum : int { kElastic = 0, kExcitation = 1, kIonization = 2, kAttachment = 3, kChargeExchange = 4 };
+
+// Device errors (bit flags in the handle's error word).
+enum : unsigned {
+    kErrMajorant = 1u << 0,
+    kErrCandidates = 1u << 1,
+    kErrNonFinite = 1u << 2,
+    kErrCapacity = 1u << 3,
+    kErrTimeout = 1u << 4,
+    kErrReplay = 1u << 5,
+    kErrBirths = 1u << 6,
+};
+
+struct MccChannelDev {
+    int process, angular, frame;
+    double threshold;
+    int secondary, ion;
+    int rows;
+    const double* energy;
+    const double* sigma;
+};
+
+struct MccModelDev {
+    int nch;
+    int species;
+    double particle_mass, neutral_mass, neutral_density, max_frequency, neutral_stddev;
+    double com_mass;      // particle_mass * neutral_mass / (particle_mass + neutral_mass)
+    double v_safe;        // |v| <= v_safe passes the frequency-bound check without evaluation
+    unsigned max_candidates;
+    MccChannelDev ch[kMaxChannels];
+};
+
+// CrossSectionTable::evaluate, src/Collision.cpp:221-237
+__device__ inline double table_eval(const MccChannelDev& c, double energy) {
+    const double* e = c.energy;
+    const int n = c.rows;
+    if (energy <= __ldg(e)) return __ldg(c.sigma);
+    if (energy >= __ldg(e + n - 1)) return __ldg(c.sigma + n - 1);
+    int lo = 0, hi = n;  // first index with e[i] > energy (std::upper_bound)
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (__ldg(e + mid) > energy) hi = mid; else lo = mid + 1;
+    }
+    const int high = lo, low = high - 1;
+    const double el = __ldg(e + low), eh = __ldg(e + high);
+    const double sl = __ldg(c.sigma + low), sh = __ldg(c.sigma + high);
+    const double fraction = (energy - el) / (eh - el);
+    return sl + fraction * (sh - sl);
+}
+
+// collision_energy, src/Collision.cpp:579-594
+__device__ inline double collision_energy(const MccModelDev& m, const MccChannelDev& c, double rel) {
+    const double mass = c.frame == 1 ? m.com_mass : m.particle_mass;
+    return 0.5 * mass * rel * rel;
+}
+
+// rates_for_speed, src/Collision.cpp:596-625; returns false when the total
+// exceeds max_frequency (+64 eps tolerance).
+__device__ inline bool rates_for_speed(const MccModelDev& m, double speed, double* rates) {
+    double total = 0.0;
+    for (int i = 0; i < m.nch; ++i) {
+        const MccChannelDev& c = m.ch[i];
+        const double energy = collision_energy(m, c, speed);
+        double rate = 0.0;
+        if (energy >= c.threshold) rate = m.neutral_density * table_eval(c, energy) * speed;
+        rates[i] = rate;
+        total += rate;
+    }
+    const double mx = m.max_frequency > total ? m.max_frequency : total;
+    return !(total > m.max_frequency + 64.0 * kDblEpsilon * mx);
+}
+
+// validate_frequency_bound, src/Collision.cpp:627-685 (exact form, run only
+// above the precomputed safe speed).
+__device__ inline bool frequency_bound_ok(const MccModelDev& m, double speed) {
+    if (speed <= m.v_safe) return true;
+    double rates[kMaxChannels];
+    if (m.neutral_stddev == 0.0) return rates_for_speed(m, speed, rates);
+    const double limit = kThermalSigma * m.neutral_stddev;
+    const double max_rel = speed + limit;
+    double bound = 0.0;
+    for (int i = 0; i < m.nch; ++i) {
+        const MccChannelDev& c = m.ch[i];
+        const double max_e = collision_energy(m, c, max_rel);
+        if (max_e < c.threshold) continue;
+        const double min_rel = speed - limit > 0.0 ? speed - limit : 0.0;
+        double min_e = collision_energy(m, c, min_rel);
+        if (c.threshold > min_e) min_e = c.threshold;
+        double smax = table_eval(c, min_e);
+        const double s2 = table_eval(c, max_e);
+        if (s2 > smax) smax = s2;
+        for (int k = 0; k < c.rows; ++k) {
+            const double e = __ldg(c.energy + k);
+            const double s = __ldg(c.sigma + k);
+            if (e >= min_e && e <= max_e && s > smax) smax = s;
+        }
+        bound += m.neutral_density * smax * max_rel;
+    }
+    const double mx = m.max_frequency > bound ? m.max_frequency : bound;
+    return !(bound > m.max_frequency + 64.0 * kDblEpsilon * mx);
+}
+
+__device__ inline double norm3(double x, double y, double z) { return sqrt(x * x + y * y + z * z); }
+
+// isotropic_velocity, src/Collision.cpp:53-64
+template <class S>
+__device__ inline void isotropic(double speed, S& s, double out[3]) {
+    const double cosine = 2.0 * uniform01(s) - 1.0;
+    const double t = 1.0 - cosine * cosine;
+    const double sine = sqrt(0.0 > t ? 0.0 : t);
+    const double azimuth = 2.0 * 3.141592653589793 * uniform01(s);
+    double sn, cs;
+    sincos(azimuth, &sn, &cs);
+    out[0] = speed * sine * cs;
+    out[1] = speed * sine * sn;
+    out[2] = speed * cosine;
+}
+
+struct CollideResult {
+    unsigned candidates = 0, nulls = 0;
+    unsigned channel[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double energy_change[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool removed = false;
+    unsigned error = 0;
+};
+
+// NullCollisionModel::collide(Vec3&), src/Collision.cpp:907-993.  on_secondary
+// receives (channel, secondary velocity[3], ion velocity[3]) per ionization.
+template <class S, class OnSecondary>
+__device__ inline void collide3(const MccModelDev& m, double v[3], double dt, S& s, CollideResult& r,
+                                OnSecondary&& on_secondary) {
+    if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) { r.error |= kErrNonFinite; return; }
+    double elapsed = 0.0;
+    for (;;) {
+        if (!frequency_bound_ok(m, norm3(v[0], v[1], v[2]))) { r.error |= kErrMajorant; return; }
+        // open_unit_interval, src/Collision.cpp:46-51 (bounded for replay arrays)
+        double u = uniform01(s);
+        for (int guard = 0; !(u > 0.0) && guard < 64 && !s.overrun(); ++guard) u = uniform01(s);
+        if (s.overrun()) { r.error |= kErrReplay; return; }
+        const double waiting = -log(u) / m.max_frequency;
+        if (!isfinite(waiting) || waiting >= dt - elapsed) break;
+        elapsed += waiting;
+        ++r.candidates;
+        if (r.candidates > m.max_candidates) { r.error |= kErrCandidates; return; }
+        // sample_neutral_velocity_3v, src/Collision.cpp:702-715
+        double vn[3] = {0.0, 0.0, 0.0};
+        if (m.neutral_stddev != 0.0) {
+            NormalState ns;
+            const double limit = kThermalSigma * m.neutral_stddev;
+            int attempt = 0;
+            for (; attempt < 1024; ++attempt) {
+                vn[0] = normal(ns, s, 0.0, m.neutral_stddev);
+                vn[1] = normal(ns, s, 0.0, m.neutral_stddev);
+                vn[2] = normal(ns, s, 0.0, m.neutral_stddev);
+                if (norm3(vn[0], vn[1], vn[2]) <= limit) break;
+            }
+            if (attempt == 1024) { r.error |= kErrMajorant; return; }
+        }
+        double rates[kMaxChannels];
+        if (!rates_for_speed(m, norm3(v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]), rates)) {
+            r.error |= kErrMajorant;
+            return;
+        }
+        const double selection = canonical(s) * m.max_frequency;
+        double cumulative = 0.0;
+        bool accepted = false;
+        for (int ci = 0; ci < m.nch; ++ci) {
+            cumulative += rates[ci];
+            if (selection < cumulative) {
+                const MccChannelDev& c = m.ch[ci];
+                const double before = 0.5 * m.particle_mass * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                // apply_channel (3V), src/Collision.cpp:762-829
+                if (c.process == kAttachment) {
+                    v[0] = v[1] = v[2] = 0.0;
+                } else if (c.process == kChargeExchange) {
+                    v[0] = vn[0]; v[1] = vn[1]; v[2] = vn[2];
+                } else {
+                    const double rel[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+                    const double initial_speed = norm3(rel[0], rel[1], rel[2]);
+                    double energy = 0.5 * m.particle_mass * initial_speed * initial_speed;
+                    if (c.process == kExcitation || c.process == kIonization) {
+                        const double e2 = energy - c.threshold;
+                        energy = 0.0 > e2 ? 0.0 : e2;
+                    }
+                    if (c.process == kIonization) energy *= 0.5;
+                    const double speed = sqrt(2.0 * energy / m.particle_mass);
+                    double sc[3];
+                    if (c.angular == 1) { sc[0] = -rel[0]; sc[1] = -rel[1]; sc[2] = -rel[2]; }
+                    else isotropic(speed, s, sc);
+                    if (c.process == kElastic && m.neutral_mass > 0.0) {
+                        const double total = m.particle_mass + m.neutral_mass;
+                        const double rf = m.neutral_mass / total;
+                        for (int d = 0; d < 3; ++d)
+                            v[d] = (m.particle_mass * v[d] + m.neutral_mass * vn[d]) / total + rf * sc[d];
+                    } else {
+                        for (int d = 0; d < 3; ++d) v[d] = vn[d] + sc[d];
+                    }
+                }
+                r.energy_change[ci] +=
+                    0.5 * m.particle_mass * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - before;
+                if (c.process == kIonization) {
+                    const double sspeed = norm3(v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]);
+                    double iso[3];
+                    isotropic(sspeed, s, iso);
+                    const double vs[3] = {vn[0] + iso[0], vn[1] + iso[1], vn[2] + iso[2]};
+                    on_secondary(ci, vs, vn);
+                }
+                ++r.channel[ci];
+                if (c.process == kAttachment) r.removed = true;
+                accepted = true;
+                break;
+            }
+        }
+        if (!accepted) ++r.nulls;
+        if (r.removed) break;
+    }
+    if (s.overrun()) r.error |= kErrReplay;
+}
+
+}  // namespace apic

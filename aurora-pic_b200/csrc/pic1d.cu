@@ -1,0 +1,1584 @@
+// 1D1V / 1D3V electrostatic PIC particle step on one B200 (FP64 form).
+//
+// Replaces pic::Simulation's hot loop (src/Simulation.cpp:1008-1138) and the
+// routines it calls: interpolate_electric (src/FieldSolver.cpp:909-924), the
+// leapfrog kick/drift/synchronize/initialize (src/Pusher.cpp:66-80), the
+// periodic wrap / absorbing walls (src/Simulation.cpp:1039-1077),
+// Species::deposit_charge (src/Species.cpp:161-185), FieldSolver::solve(Grid&)
+// (src/FieldSolver.cpp:384-440, :733-759) and Simulation::apply_collisions
+// (src/Simulation.cpp:771-1006).
+//
+// Device layout: per species, structure-of-arrays x, v_half, v_y, v_z (and a
+// time-centred v written only when the state is read back), double-buffered;
+// live particles are kept compacted in [0, n).  One step is two launches:
+//
+//   pass kernel  (persistent grid, one 1024-particle tile per iteration):
+//       [synchronize -> MCC -> re-initialise half step]  (the collision part of
+//        the previous step, done while the particle is in registers anyway)
+//       kick -> drift -> wall/wrap -> CIC deposit into a shared-memory copy of
+//       the grid (64-bit fixed point) -> order-preserving compaction of the
+//       survivors (decoupled look-back across tiles) -> write.
+//   post kernel  (one CTA): sort and append this pass's ionization products
+//       (pushed and deposited like everyone else), convert the fixed-point
+//       density to FP64, Poisson solve (scan-form Thomas for Dirichlet walls,
+//       exact-twiddle DFT for periodic), E field, advance time and step.
+//
+// This file is compiled with --fmad=false: every FP64 expression is evaluated
+// with the reference's operation order and rounding, so a particle's state
+// differs from the reference only through the field it sees.
+#include <cub/block/block_radix_sort.cuh>
+#include <cub/block/block_scan.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "apic_common.cuh"
+#include "apic_mcc.cuh"
+#include "apic_rng.cuh"
+
+namespace apic {
+
+constexpr int kThreads = 256;
+constexpr int kItems = 4;
+constexpr int kTile = kThreads * kItems;
+constexpr int kMaxSpecies = APIC_MAX_SPECIES;
+constexpr int kMaxModels = APIC_MAX_MODELS;
+constexpr int kPostThreads = 1024;
+constexpr int kPostItems = 4;
+constexpr int kMaxBirths = kPostThreads * kPostItems;  // products per pass the post kernel sorts
+constexpr int kMaxNx1D = 4096;
+
+enum : unsigned {
+    kModeSyncMcc = 1u << 0,   // synchronize + collide + re-initialise (pending collision part)
+    kModeKickDrift = 1u << 1, // kick + drift + boundary
+    kModeDeposit = 1u << 2,   // CIC deposit of the resulting positions
+    kModeWriteV = 1u << 3,    // write time-centred v (state read back)
+    kModeInitHalf = 1u << 4,  // v_half = v - qm E dt / 2 (Simulation::initialize)
+};
+enum : unsigned {
+    kPostSolve = 1u << 0,
+    kPostAdvance = 1u << 1,
+    kPostPushBirths = 1u << 2,
+};
+
+struct DevState {
+    unsigned n[kMaxSpecies];
+    unsigned ticket;
+    unsigned epoch;
+    unsigned nbirths;
+    unsigned error;
+    unsigned long long step;
+    double time;
+    unsigned long long candidates, nulls;
+    unsigned long long chan[kMaxModels][kMaxChannels];
+    double chan_energy[kMaxModels][kMaxChannels];
+    unsigned long long lost[kMaxSpecies][2];
+    double lost_energy[kMaxSpecies][2];
+};
+
+struct BirthRec {
+    unsigned long long key;  // (parent species, parent slot, product index) ordering key
+    double x, v[3];
+    int species;
+    int pad;
+};
+
+struct SpeciesDev {
+    double qm, hqm, qw, qwdx, mass, weight;
+    int model;
+    unsigned capacity;
+    unsigned long long* lookback;
+    // [0] = input buffer of this pass, [1] = output buffer
+    double* x[2];
+    double* vh[2];
+    double* vy[2];
+    double* vz[2];
+    double* v;  // time-centred velocity (valid after a read-back pass)
+};
+
+struct Params1D {
+    int nspecies, vdim, dirichlet, nx;
+    double L, dx, dt, eps, rho_scale, inv_rho_scale;
+    unsigned mode;
+    uint64_t seed;
+    double phi_left, phi_right;
+    apic_voltage_drive drive_left, drive_right;
+    SpeciesDev sp[kMaxSpecies];
+    MccModelDev model[kMaxModels];
+    double* E;
+    double* rho;
+    double* phi;
+    unsigned long long* rho_acc;
+    const double* tw;       // periodic: twiddles (cos, sin)(2 pi m / n), m < n
+    double* scratch;        // periodic: 4 * nx per-mode spectra
+    const double* thomas_r; // Dirichlet: 1/denominator of the Thomas forward sweep
+    const double* thomas_a; // Dirichlet: -cp of the back substitution
+    BirthRec* births;
+    unsigned births_cap;
+    DevState* st;
+};
+
+// ---- field gather / deposit (reference arithmetic) ----------------------
+
+__device__ __forceinline__ double wrap_periodic(double x, double L) { return fmod(fmod(x, L) + L, L); }
+
+struct Cic {
+    int i0, i1;
+    double w0, w1;  // (1 - f), f
+};
+
+// interpolate_electric / deposit_charge index + fraction, src/FieldSolver.cpp:909-924,
+// src/Species.cpp:167-183
+__device__ __forceinline__ Cic cic_periodic(double x, double L, double dx, int nx) {
+    const double xp = wrap_periodic(x, L);
+    const double g = xp / dx;
+    const double fl = floor(g);
+    const unsigned long long i = (unsigned long long)fl;
+    const double f = g - (double)i;
+    Cic c;
+    c.i0 = (int)(i % (unsigned long long)nx);
+    c.i1 = (int)((i + 1) % (unsigned long long)nx);
+    c.w0 = 1.0 - f;
+    c.w1 = f;
+    return c;
+}
+
+__device__ __forceinline__ Cic cic_dirichlet(double x, double L, double dx, int nx) {
+    const double xp = x < 0.0 ? 0.0 : (L < x ? L : x);  // std::clamp
+    const double g = xp / dx;
+    double fl = floor(g);
+    const double lim = (double)(nx - 2);
+    if (lim < fl) fl = lim;  // std::min<double>(floor(g), nx - 2)
+    const unsigned long long i = (unsigned long long)fl;
+    const double f = g - (double)i;
+    Cic c;
+    c.i0 = (int)i;
+    c.i1 = (int)i + 1;
+    c.w0 = 1.0 - f;
+    c.w1 = f;
+    return c;
+}
+
+template <bool DIRICHLET>
+__device__ __forceinline__ Cic cic(double x, const Params1D& p) {
+    return DIRICHLET ? cic_dirichlet(x, p.L, p.dx, p.nx) : cic_periodic(x, p.L, p.dx, p.nx);
+}
+
+__device__ __forceinline__ double gather(const double* E, const Cic& c) {
+    return E[c.i0] * c.w0 + E[c.i1] * c.w1;
+}
+
+// One particle's two fixed-point contributions.
+template <bool DIRICHLET>
+__device__ __forceinline__ void deposit_contrib(const Cic& c, const SpeciesDev& s, const Params1D& p,
+                                                long long& a0, long long& a1) {
+    if (!DIRICHLET) {
+        a0 = to_fixed(s.qwdx * c.w0, p.rho_scale);
+        a1 = to_fixed(s.qwdx * c.w1, p.rho_scale);
+    } else {
+        const double v0 = (c.i0 == 0 || c.i0 + 1 == p.nx) ? 0.5 * p.dx : p.dx;
+        const double v1 = (c.i1 == 0 || c.i1 + 1 == p.nx) ? 0.5 * p.dx : p.dx;
+        a0 = to_fixed(s.qw * c.w0 / v0, p.rho_scale);
+        a1 = to_fixed(s.qw * c.w1 / v1, p.rho_scale);
+    }
+}
+
+// ---- decoupled look-back -------------------------------------------------
+
+constexpr unsigned long long kLbValueMask = (1ull << 38) - 1;
+constexpr unsigned long long kLbAggregate = 1ull << 38;
+constexpr unsigned long long kLbInclusive = 2ull << 38;
+
+__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned long long flag,
+                                                       unsigned long long value) {
+    return ((unsigned long long)(epoch & 0xFFFFFFu) << 40) | flag | value;
+}
+
+// Returns the exclusive prefix of `tile` in its species chain.  Spins on
+// predecessors with an iteration bound; gives up with kErrTimeout.
+__device__ unsigned long long lookback(unsigned long long* lb, unsigned tile, unsigned count,
+                                       unsigned epoch, unsigned* error) {
+    if (tile == 0) {
+        atomicExch(lb, lb_word(epoch, kLbInclusive, count));
+        return 0;
+    }
+    atomicExch(lb + tile, lb_word(epoch, kLbAggregate, count));
+    unsigned long long excl = 0;
+    long long p = (long long)tile - 1;
+    const unsigned ep = epoch & 0xFFFFFFu;
+    while (p >= 0) {
+        unsigned long long w = 0;
+        unsigned spins = 0;
+        for (;;) {
+            w = *((volatile unsigned long long*)(lb + p));
+            if ((unsigned)(w >> 40) == ep && (w & (3ull << 38)) != 0) break;
+            if (++spins > (1u << 24)) {
+                atomicOr(error, kErrTimeout);
+                return 0;
+            }
+            if (spins > 64) __nanosleep(64);
+        }
+        excl += w & kLbValueMask;
+        if ((w & (3ull << 38)) == kLbInclusive) break;
+        --p;
+    }
+    atomicExch(lb + tile, lb_word(epoch, kLbInclusive, excl + count));
+    return excl;
+}
+
+// ---- the fused particle pass -----------------------------------------------
+
+template <int VDIM, bool DIRICHLET>
+__global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* sE = reinterpret_cast<double*>(smem_raw);
+    unsigned long long* sRho = reinterpret_cast<unsigned long long*>(sE + p.nx);
+    __shared__ unsigned s_ticket;
+    __shared__ unsigned s_cnt[kItems * (kThreads / 32)];
+    __shared__ unsigned long long s_base;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned mode = p.mode;
+    for (int i = tid; i < p.nx; i += kThreads) {
+        sE[i] = p.E[i];
+        sRho[i] = 0ull;
+    }
+    DevState* st = p.st;
+    const unsigned epoch = st->epoch;
+    unsigned tiles_before[kMaxSpecies + 1];
+    tiles_before[0] = 0;
+    for (int s = 0; s < kMaxSpecies; ++s)
+        tiles_before[s + 1] = tiles_before[s] + (s < p.nspecies ? (st->n[s] + kTile - 1) / kTile : 0);
+    const unsigned total_tiles = tiles_before[kMaxSpecies];
+    __syncthreads();
+
+    for (;;) {
+        if (tid == 0) s_ticket = atomicAdd(&st->ticket, 1u);
+        __syncthreads();
+        const unsigned t = s_ticket;
+        if (t >= total_tiles) break;
+        int s = 0;
+        while (t >= tiles_before[s + 1]) ++s;
+        const unsigned tile = t - tiles_before[s];
+        const SpeciesDev& S = p.sp[s];
+        const unsigned n = st->n[s];
+        const unsigned base = tile * kTile;
+
+        double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems];
+        bool keep[kItems];
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const unsigned idx = base + k * kThreads + tid;
+            const bool live = idx < n;
+            keep[k] = live;
+            x[k] = live ? S.x[0][idx] : 0.0;
+            vh[k] = live ? S.vh[0][idx] : 0.0;
+            vy[k] = (VDIM == 3 && live) ? S.vy[0][idx] : 0.0;
+            vz[k] = (VDIM == 3 && live) ? S.vz[0][idx] : 0.0;
+            vc[k] = 0.0;
+            if ((mode & kModeInitHalf) && live) vc[k] = S.v[idx];
+        }
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            if (!keep[k]) continue;
+            const unsigned idx = base + k * kThreads + tid;
+            const Cic c = cic<DIRICHLET>(x[k], p);
+            const double E = gather(sE, c);
+            if (mode & kModeInitHalf) {
+                // initialize_leapfrog_half_step, src/Pusher.cpp:66-68
+                vh[k] = vc[k] - S.hqm * E * p.dt;
+            }
+            if (mode & kModeSyncMcc) {
+                // synchronize_leapfrog, src/Pusher.cpp:78-80
+                double v = vh[k] + S.hqm * E * p.dt;
+                if (S.model >= 0 && VDIM == 3) {
+                    const MccModelDev& M = p.model[S.model];
+                    double vel[3] = {v, vy[k], vz[k]};
+                    PhiloxStream rng(p.seed, idx, (uint32_t)(st->step - 1ull), (uint32_t)s);
+                    CollideResult r;
+                    unsigned nion = 0;
+                    const double xk = x[k];
+                    collide3(M, vel, p.dt, rng, r, [&](int ch, const double* vs, const double* vi) {
+                        const unsigned slot = atomicAdd(&st->nbirths, 2u);
+                        const MccChannelDev& C = M.ch[ch];
+                        if (slot + 2u <= p.births_cap) {
+                            const unsigned long long key =
+                                ((unsigned long long)s << 56) | ((unsigned long long)idx << 16) | (nion << 1);
+                            BirthRec a, b;
+                            a.key = key; a.x = xk; a.species = C.secondary; a.pad = 0;
+                            b.key = key | 1ull; b.x = xk; b.species = C.ion; b.pad = 0;
+                            for (int d = 0; d < 3; ++d) { a.v[d] = vs[d]; b.v[d] = vi[d]; }
+                            p.births[slot] = a;
+                            p.births[slot + 1] = b;
+                        } else {
+                            atomicOr(&st->error, kErrBirths);
+                        }
+                        const SpeciesDev& A = p.sp[C.secondary];
+                        const SpeciesDev& B = p.sp[C.ion];
+                        const double added =
+                            0.5 * A.mass * A.weight * (vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]) +
+                            0.5 * B.mass * B.weight * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
+                        atomicAdd(&st->chan_energy[S.model][ch], added);
+                        ++nion;
+                    });
+                    if (r.error) atomicOr(&st->error, r.error);
+                    if (r.candidates) {
+                        atomicAdd(&st->candidates, (unsigned long long)r.candidates);
+                        if (r.nulls) atomicAdd(&st->nulls, (unsigned long long)r.nulls);
+                        for (int ch = 0; ch < M.nch; ++ch) {
+                            if (r.channel[ch]) {
+                                atomicAdd(&st->chan[S.model][ch], (unsigned long long)r.channel[ch]);
+                                atomicAdd(&st->chan_energy[S.model][ch], r.energy_change[ch] * S.weight);
+                            }
+                        }
+                    }
+                    v = vel[0];
+                    vy[k] = vel[1];
+                    vz[k] = vel[2];
+                    // initialize_leapfrog_half_step after the collision, src/Simulation.cpp:924-926
+                    vh[k] = v - S.hqm * E * p.dt;
+                }
+                vc[k] = v;
+            }
+            if (mode & kModeKickDrift) {
+                // kick_leapfrog + drift_leapfrog, src/Pusher.cpp:70-76
+                vh[k] = vh[k] + S.qm * E * p.dt;
+                x[k] = x[k] + vh[k] * p.dt;
+                if (!DIRICHLET) {
+                    x[k] = wrap_periodic(x[k], p.L);
+                } else if (x[k] < 0.0 || x[k] > p.L) {
+                    // absorbing walls and loss ledger, src/Simulation.cpp:1047-1077
+                    const double sp2 = vh[k] * vh[k] + vy[k] * vy[k] + vz[k] * vz[k];
+                    const double e = 0.5 * S.mass * S.weight * sp2;
+                    const int side = x[k] < 0.0 ? 0 : 1;
+                    atomicAdd(&st->lost[s][side], 1ull);
+                    atomicAdd(&st->lost_energy[s][side], e);
+                    keep[k] = false;
+                }
+                if (!isfinite(x[k]) || !isfinite(vh[k])) atomicOr(&st->error, kErrNonFinite);
+            }
+            if ((mode & kModeDeposit) && keep[k]) {
+                const Cic d = cic<DIRICHLET>(x[k], p);
+                long long a0, a1;
+                deposit_contrib<DIRICHLET>(d, S, p, a0, a1);
+                atomicAdd(&sRho[d.i0], (unsigned long long)a0);
+                atomicAdd(&sRho[d.i1], (unsigned long long)a1);
+            }
+        }
+        // ---- order-preserving compaction of the survivors ----
+        unsigned ballots[kItems];
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            ballots[k] = __ballot_sync(0xffffffffu, keep[k]);
+            if (lane == 0) s_cnt[k * (kThreads / 32) + warp] = __popc(ballots[k]);
+        }
+        __syncthreads();
+        if (warp == 0) {
+            const unsigned c = s_cnt[lane];
+            unsigned incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            s_cnt[lane] = incl - c;
+            const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 0) {
+                s_base = lookback(S.lookback, tile, total, epoch, &st->error);
+            }
+        }
+        __syncthreads();
+        const unsigned long long out_base = s_base;
+        const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            if (!keep[k]) continue;
+            const unsigned long long o =
+                out_base + s_cnt[k * (kThreads / 32) + warp] + __popc(ballots[k] & lt);
+            if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
+            S.x[1][o] = x[k];
+            S.vh[1][o] = vh[k];
+            if (VDIM == 3) {
+                S.vy[1][o] = vy[k];
+                S.vz[1][o] = vz[k];
+            }
+            if (mode & (kModeWriteV | kModeInitHalf)) S.v[o] = vc[k];
+        }
+        __syncthreads();
+    }
+    if (mode & kModeDeposit) {
+        for (int i = tid; i < p.nx; i += kThreads) {
+            const unsigned long long a = sRho[i];
+            if (a) atomicAdd(&p.rho_acc[i], a);
+        }
+    }
+}
+
+// ---- post kernel: products, density, field solve -----------------------------
+
+struct Affine {
+    double a, b;
+};
+struct AffineCompose {
+    __device__ Affine operator()(const Affine& l, const Affine& r) const {
+        return Affine{r.a * l.a, r.a * l.b + r.b};
+    }
+};
+
+__device__ __forceinline__ double electrode(double offset, const apic_voltage_drive& d, double t) {
+    // electrode_potential, src/Simulation.cpp:678-685
+    return offset + d.amplitude * sin(2.0 * 3.141592653589793 * d.frequency * t + d.phase);
+}
+
+template <int VDIM, bool DIRICHLET>
+__global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned post) {
+    using Sort = cub::BlockRadixSort<unsigned long long, kPostThreads, kPostItems, int>;
+    using ScanU = cub::BlockScan<unsigned, kPostThreads>;
+    using ScanA = cub::BlockScan<Affine, kPostThreads>;
+    __shared__ union {
+        typename Sort::TempStorage sort;
+        typename ScanU::TempStorage scan;
+        typename ScanA::TempStorage scana;
+    } tmp;
+    __shared__ unsigned s_surv[kMaxSpecies], s_kept[kMaxSpecies];
+    __shared__ double s_red[kPostThreads / 32];
+    __shared__ double s_mean;
+    DevState* st = p.st;
+    const int tid = threadIdx.x;
+    const unsigned epoch = st->epoch;
+
+    if (tid < kMaxSpecies) {
+        unsigned surv = 0;
+        if (tid < p.nspecies) {
+            const unsigned n = st->n[tid];
+            const unsigned tiles = (n + kTile - 1) / kTile;
+            if (tiles) {
+                const unsigned long long w = *((volatile unsigned long long*)(p.sp[tid].lookback + tiles - 1));
+                if ((unsigned)(w >> 40) == (epoch & 0xFFFFFFu) && (w & (3ull << 38)) == kLbInclusive)
+                    surv = (unsigned)(w & kLbValueMask);
+                else
+                    atomicOr(&st->error, kErrTimeout);
+            }
+        }
+        s_surv[tid] = surv;
+        s_kept[tid] = 0;
+    }
+    __syncthreads();
+
+    // -- ionization products, in (parent species, parent slot, product) order --
+    unsigned nb = st->nbirths;
+    if (nb > p.births_cap) nb = p.births_cap;
+    if (nb > (unsigned)kMaxBirths) {
+        if (tid == 0) atomicOr(&st->error, kErrBirths);
+        nb = kMaxBirths;
+    }
+    if (nb > 0) {
+        unsigned long long keys[kPostItems];
+        int idx[kPostItems];
+#pragma unroll
+        for (int k = 0; k < kPostItems; ++k) {
+            const unsigned i = tid * kPostItems + k;
+            keys[k] = i < nb ? p.births[i].key : ~0ull;
+            idx[k] = (int)i;
+        }
+        Sort(tmp.sort).Sort(keys, idx);
+        __syncthreads();
+        // process births in sorted order: thread holds sorted ranks tid*kPostItems + k
+        double bx[kPostItems], bvh[kPostItems], bv[kPostItems][3];
+        int bs[kPostItems];
+        bool keep[kPostItems];
+#pragma unroll
+        for (int k = 0; k < kPostItems; ++k) {
+            keep[k] = false;
+            bs[k] = -1;
+            const unsigned rank = tid * kPostItems + k;
+            if (rank >= nb) continue;
+            const BirthRec r = p.births[idx[k]];
+            const SpeciesDev& S = p.sp[r.species];
+            bs[k] = r.species;
+            bx[k] = r.x;
+            bv[k][0] = r.v[0]; bv[k][1] = r.v[1]; bv[k][2] = r.v[2];
+            const Cic c = cic<DIRICHLET>(r.x, p);
+            const double E = gather(p.E, c);
+            // append_product: v_half = v, then initialize_leapfrog_half_step, src/Simulation.cpp:985-1004
+            bvh[k] = r.v[0] - S.hqm * E * p.dt;
+            keep[k] = true;
+            if (post & kPostPushBirths) {
+                bvh[k] = bvh[k] + S.qm * E * p.dt;
+                bx[k] = bx[k] + bvh[k] * p.dt;
+                if (!DIRICHLET) {
+                    bx[k] = wrap_periodic(bx[k], p.L);
+                } else if (bx[k] < 0.0 || bx[k] > p.L) {
+                    const double sp2 = bvh[k] * bvh[k] + bv[k][1] * bv[k][1] + bv[k][2] * bv[k][2];
+                    const int side = bx[k] < 0.0 ? 0 : 1;
+                    atomicAdd(&st->lost[r.species][side], 1ull);
+                    atomicAdd(&st->lost_energy[r.species][side], 0.5 * S.mass * S.weight * sp2);
+                    keep[k] = false;
+                }
+                if (keep[k]) {
+                    const Cic d = cic<DIRICHLET>(bx[k], p);
+                    long long a0, a1;
+                    deposit_contrib<DIRICHLET>(d, S, p, a0, a1);
+                    atomicAdd(&p.rho_acc[d.i0], (unsigned long long)a0);
+                    atomicAdd(&p.rho_acc[d.i1], (unsigned long long)a1);
+                }
+            }
+        }
+        for (int s = 0; s < p.nspecies; ++s) {
+            unsigned flags[kPostItems], ranks[kPostItems];
+#pragma unroll
+            for (int k = 0; k < kPostItems; ++k) flags[k] = (keep[k] && bs[k] == s) ? 1u : 0u;
+            unsigned total;
+            __syncthreads();
+            ScanU(tmp.scan).ExclusiveSum(flags, ranks, total);
+            const SpeciesDev& S = p.sp[s];
+#pragma unroll
+            for (int k = 0; k < kPostItems; ++k) {
+                if (!flags[k]) continue;
+                const unsigned long long o = (unsigned long long)s_surv[s] + ranks[k];
+                if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
+                S.x[1][o] = bx[k];
+                S.vh[1][o] = bvh[k];
+                if (VDIM == 3) {
+                    S.vy[1][o] = bv[k][1];
+                    S.vz[1][o] = bv[k][2];
+                }
+                S.v[o] = bv[k][0];
+            }
+            if (tid == 0) s_kept[s] = total;
+        }
+        __syncthreads();
+    }
+    if (tid < p.nspecies) {
+        unsigned long long n = (unsigned long long)s_surv[tid] + s_kept[tid];
+        if (n > p.sp[tid].capacity) { atomicOr(&st->error, kErrCapacity); n = p.sp[tid].capacity; }
+        st->n[tid] = (unsigned)n;
+    }
+    if (tid == 0) {
+        st->ticket = 0;
+        st->nbirths = 0;
+        st->epoch = epoch + 1;
+    }
+    if (!(post & kPostSolve)) return;
+
+    // -- density: fixed point -> FP64 ---------------------------------------
+    const int nx = p.nx;
+    double local = 0.0;
+    for (int i = tid; i < nx; i += kPostThreads) {
+        const long long a = (long long)p.rho_acc[i];
+        const double r = (double)a * p.inv_rho_scale;
+        p.rho[i] = r;
+        p.rho_acc[i] = 0ull;
+        local += r;
+    }
+    const double field_time = (post & kPostAdvance) ? st->time + p.dt : st->time;
+    if (!DIRICHLET) {
+        // solve_periodic_spectral(Grid&), src/FieldSolver.cpp:407-440
+        for (int o = 16; o > 0; o >>= 1) local += __shfl_down_sync(0xffffffffu, local, o);
+        if ((tid & 31) == 0) s_red[tid >> 5] = local;
+        __syncthreads();
+        if (tid == 0) {
+            double m = 0.0;
+            for (int w = 0; w < kPostThreads / 32; ++w) m += s_red[w];
+            s_mean = m / (double)nx;
+        }
+        __syncthreads();
+        const double mean = s_mean;
+        const double twopi = 2.0 * 3.141592653589793;
+        // forward transform: mode k per thread, summed over j in the reference's order;
+        // stored in phi (real part) and E (imaginary part) scratch
+        double* rk = p.phi;
+        double* ik = p.E;
+        for (int k = tid; k < nx; k += kPostThreads) {
+            double re = 0.0, im = 0.0;
+            if (k > 0) {
+                unsigned m = 0;
+                for (int j = 0; j < nx; ++j) {
+                    const double a = p.rho[j] - mean;
+                    re += a * p.tw[2 * m];
+                    im += a * (-p.tw[2 * m + 1]);
+                    m += (unsigned)k;
+                    if (m >= (unsigned)nx) m -= (unsigned)nx;
+                }
+                re /= (double)nx;
+                im /= (double)nx;
+            }
+            rk[k] = re;
+            ik[k] = im;
+        }
+        __syncthreads();
+        // per-mode potential and field, src/FieldSolver.cpp:426-428
+        double* sp_r = p.scratch;
+        double* sp_i = p.scratch + nx;
+        double* se_r = p.scratch + 2 * nx;
+        double* se_i = p.scratch + 3 * nx;
+        for (int k = tid; k < nx; k += kPostThreads) {
+            if (k == 0) { sp_r[0] = sp_i[0] = se_r[0] = se_i[0] = 0.0; continue; }
+            const double kk = (k <= nx / 2) ? (double)k : -(double)(nx - k);
+            const double wave = twopi * kk / p.L;
+            const double den = p.eps * wave * wave;
+            const double pr = rk[k] / den, pi = ik[k] / den;
+            sp_r[k] = pr;
+            sp_i[k] = pi;
+            se_r[k] = wave * pi;    // -(0,1) * wave * phik
+            se_i[k] = -(wave * pr);
+        }
+        __syncthreads();
+        // inverse: each node j sums its modes in order k = 1 .. n-1
+        for (int j = tid; j < nx; j += kPostThreads) {
+            double ph = 0.0, ef = 0.0;
+            unsigned m = (unsigned)j;
+            for (int k = 1; k < nx; ++k) {
+                const double cs = p.tw[2 * m], sn = p.tw[2 * m + 1];
+                ph += sp_r[k] * cs - sp_i[k] * sn;
+                ef += se_r[k] * cs - se_i[k] * sn;
+                m += (unsigned)j;
+                if (m >= (unsigned)nx) m -= (unsigned)nx;
+            }
+            p.phi[j] = ph;
+            p.E[j] = ef;
+        }
+    } else {
+        __syncthreads();
+        // solve_dirichlet_tridiagonal, src/FieldSolver.cpp:733-759, with the
+        // forward sweep and the back substitution evaluated as affine scans
+        const double phil = electrode(p.phi_left, p.drive_left, field_time);
+        const double phir = electrode(p.phi_right, p.drive_right, field_time);
+        const int m = nx - 2;
+        const double dx2 = p.dx * p.dx;
+        constexpr int IPT = kMaxNx1D / kPostThreads;
+        Affine f[IPT];
+        for (int k = 0; k < IPT; ++k) {
+            const int i = tid * IPT + k;
+            if (i < m) {
+                double d = p.rho[i + 1] * dx2 / p.eps;
+                if (i == 0) d += phil;
+                if (i == m - 1) d += phir;
+                const double r = p.thomas_r[i];
+                f[k] = Affine{r, r * d};
+            } else {
+                f[k] = Affine{1.0, 0.0};
+            }
+        }
+        ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
+        __syncthreads();
+        // dp[i] = f[i].b (the recurrence starts from 0); keep in phi[i+1] scratch
+        for (int k = 0; k < IPT; ++k) {
+            const int i = tid * IPT + k;
+            if (i < m) p.E[i] = f[k].b;  // dp
+        }
+        __syncthreads();
+        // back substitution in reverse: z_t = a[m-1-t] z_{t-1} + dp[m-1-t]
+        for (int k = 0; k < IPT; ++k) {
+            const int t = tid * IPT + k;
+            if (t < m) {
+                const int ii = m - 1 - t;
+                f[k] = Affine{p.thomas_a[ii], p.E[ii]};
+            } else {
+                f[k] = Affine{1.0, 0.0};
+            }
+        }
+        __syncthreads();
+        ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
+        __syncthreads();
+        for (int k = 0; k < IPT; ++k) {
+            const int t = tid * IPT + k;
+            if (t < m) p.phi[m - t] = f[k].b;
+        }
+        if (tid == 0) {
+            p.phi[0] = phil;
+            p.phi[nx - 1] = phir;
+        }
+        __syncthreads();
+        for (int i = tid; i < nx; i += kPostThreads) {
+            double e;
+            if (i == 0) e = -(p.phi[1] - p.phi[0]) / p.dx;
+            else if (i == nx - 1) e = -(p.phi[nx - 1] - p.phi[nx - 2]) / p.dx;
+            else e = -(p.phi[i + 1] - p.phi[i - 1]) / (2.0 * p.dx);
+            p.E[i] = e;
+        }
+    }
+    if (tid == 0 && (post & kPostAdvance)) {
+        st->time = field_time;
+        st->step = st->step + 1ull;
+    }
+}
+
+// interpolate_electric(Grid&, x) at query points, src/FieldSolver.cpp:909-924
+template <bool DIRICHLET>
+__global__ void k_gather_points1d(Params1D p, const double* xq, double* eq, int nq) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    eq[i] = gather(p.E, cic<DIRICHLET>(xq[i], p));
+}
+
+// ---- stateless collide (replay or Philox) -----------------------------------
+
+__global__ void k_collide3(MccModelDev m, int n, double* v3, double dt, const uint64_t* draws,
+                           const uint64_t* offsets, uint64_t seed, uint32_t step, uint32_t stream,
+                           apic_collide_stats* stats) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v[3] = {v3[3 * i], v3[3 * i + 1], v3[3 * i + 2]};
+    CollideResult r;
+    apic_collide_stats out;
+    memset(&out, 0, sizeof out);
+    auto on_sec = [&](int ch, const double* vs, const double* vi) {
+        const int k = out.nsecondaries++;
+        if (k < 4) {
+            out.secondary_channel[k] = ch;
+            for (int d = 0; d < 3; ++d) {
+                out.secondary_velocity[k][d] = vs[d];
+                out.secondary_ion_velocity[k][d] = vi[d];
+            }
+        }
+    };
+    unsigned used;
+    if (draws) {
+        ReplayStream s{draws + offsets[i], offsets[i + 1] - offsets[i]};
+        collide3(m, v, dt, s, r, on_sec);
+        used = s.index;
+    } else {
+        PhiloxStream s(seed, (uint32_t)i, step, stream);
+        collide3(m, v, dt, s, r, on_sec);
+        used = s.index;
+    }
+    v3[3 * i] = v[0]; v3[3 * i + 1] = v[1]; v3[3 * i + 2] = v[2];
+    out.candidates = r.candidates;
+    out.null_collisions = r.nulls;
+    for (int c = 0; c < kMaxChannels; ++c) {
+        out.channel_collisions[c] = r.channel[c];
+        out.energy_change[c] = r.energy_change[c];
+    }
+    out.removed = r.removed ? 1 : 0;
+    out.draws = used | (r.error ? 0x80000000u : 0u);
+    stats[i] = out;
+}
+
+// ---- host side ----------------------------------------------------------------
+
+cudaError_t bounded_wait(cudaStream_t stream, double seconds) {
+    cudaEvent_t ev;
+    cudaError_t e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(ev, stream);
+    if (e != cudaSuccess) { cudaEventDestroy(ev); return e; }
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        e = cudaEventQuery(ev);
+        if (e != cudaErrorNotReady) break;
+        const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > seconds) { e = cudaErrorNotReady; break; }
+        std::this_thread::sleep_for(std::chrono::microseconds(el < 0.01 ? 2 : 200));
+    }
+    cudaEventDestroy(ev);
+    return e;
+}
+
+int status_from_device(unsigned w) {
+    if (w & kErrMajorant) return APIC_ERR_MAJORANT;
+    if (w & kErrCandidates) return APIC_ERR_CANDIDATES;
+    if (w & kErrNonFinite) return APIC_ERR_NONFINITE;
+    if (w & (kErrCapacity | kErrBirths)) return APIC_ERR_CAPACITY;
+    if (w & kErrTimeout) return APIC_ERR_TIMEOUT;
+    if (w & kErrReplay) return APIC_ERR_INVALID;
+    return APIC_OK;
+}
+
+std::string describe_device_error(unsigned w) {
+    std::string s;
+    if (w & kErrMajorant) s += "MCC total collision frequency exceeds configured max_frequency; ";
+    if (w & kErrCandidates) s += "MCC candidate limit exceeded; reduce dt or increase max_candidates_per_particle; ";
+    if (w & kErrNonFinite) s += "particle state became non-finite; ";
+    if (w & kErrCapacity) s += "reactive collisions exceeded max_particles_per_species; ";
+    if (w & kErrBirths) s += "ionization products in one step exceeded the per-step product buffer; ";
+    if (w & kErrTimeout) s += "device look-back wait timed out; ";
+    if (w & kErrReplay) s += "recorded draw array exhausted; ";
+    return s;
+}
+
+// Largest speed below which the reference's frequency-bound check
+// (validate_frequency_bound, src/Collision.cpp:627-685) cannot fail.  Each
+// channel's cross section is piecewise linear in energy and energy is
+// quadratic in speed, so between breakpoints the total rate is
+// n v (A + B v^2); its maximum per interval is exact.  Thermal neutrals use
+// the monotone majorant n (v + 8 sigma) sum_c max_{E <= E(v + 8 sigma)} sigma_c.
+static double safe_speed(const apic_mcc_model& m, double particle_mass, double neutral_stddev) {
+    const double margin = 1.0 - 1e-9;
+    const double target = m.max_frequency * margin;
+    const double com = m.neutral_mass > 0 ? particle_mass * m.neutral_mass / (particle_mass + m.neutral_mass) : 0;
+    auto mass_of = [&](const apic_mcc_channel& c) { return c.energy_frame == APIC_FRAME_CENTER_OF_MASS ? com : particle_mass; };
+    auto sigma_at = [&](const apic_mcc_channel& c, double e) {
+        if (e <= c.energy[0]) return c.sigma[0];
+        if (e >= c.energy[c.rows - 1]) return c.sigma[c.rows - 1];
+        const double* up = std::upper_bound(c.energy, c.energy + c.rows, e);
+        const size_t hi = (size_t)(up - c.energy), lo = hi - 1;
+        const double f = (e - c.energy[lo]) / (c.energy[hi] - c.energy[lo]);
+        return c.sigma[lo] + f * (c.sigma[hi] - c.sigma[lo]);
+    };
+    if (neutral_stddev == 0.0) {
+        // speed breakpoints of every channel
+        std::vector<double> br{0.0};
+        for (int i = 0; i < m.nch; ++i) {
+            const auto& c = m.ch[i];
+            const double ms = mass_of(c);
+            for (size_t k = 0; k < c.rows; ++k) br.push_back(std::sqrt(2.0 * c.energy[k] / ms));
+            if (c.threshold_energy > 0) br.push_back(std::sqrt(2.0 * c.threshold_energy / ms));
+        }
+        std::sort(br.begin(), br.end());
+        auto total = [&](double v) {
+            double t = 0;
+            for (int i = 0; i < m.nch; ++i) {
+                const auto& c = m.ch[i];
+                const double e = 0.5 * mass_of(c) * v * v;
+                if (e >= c.threshold_energy) t += m.neutral_density * sigma_at(c, e) * v;
+            }
+            return t;
+        };
+        for (size_t k = 0; k + 1 < br.size(); ++k) {
+            const double v1 = br[k], v2 = br[k + 1];
+            if (!(v2 > v1)) continue;
+            // sample the cubic densely enough to bound it (endpoints + interior extremum)
+            double mx = std::max(total(v1 * (1 + 1e-12) + 1e-300), total(v2 * (1 - 1e-12)));
+            for (int q = 1; q < 16; ++q) mx = std::max(mx, total(v1 + (v2 - v1) * q / 16.0));
+            if (mx * (1 + 1e-6) > target) return v1;
+        }
+        // beyond the last breakpoint every sigma is constant: rate = n v sum sigma_last
+        double s_last = 0;
+        for (int i = 0; i < m.nch; ++i) s_last += m.ch[i].sigma[m.ch[i].rows - 1];
+        if (s_last <= 0) return 1e300;
+        return std::min(std::max(br.back(), 0.0) == br.back() ? 1e300 : 0.0,
+                        target / (m.neutral_density * s_last) * (1 - 1e-6));
+    }
+    const double limit = kThermalSigma * neutral_stddev;
+    auto majorant = [&](double v) {
+        double b = 0;
+        for (int i = 0; i < m.nch; ++i) {
+            const auto& c = m.ch[i];
+            const double emax = 0.5 * mass_of(c) * (v + limit) * (v + limit);
+            if (emax < c.threshold_energy) continue;
+            double smax = sigma_at(c, 0.0);
+            for (size_t k = 0; k < c.rows && c.energy[k] <= emax; ++k) smax = std::max(smax, c.sigma[k]);
+            smax = std::max(smax, sigma_at(c, emax));
+            b += m.neutral_density * smax * (v + limit);
+        }
+        return b;
+    };
+    if (majorant(0.0) * (1 + 1e-6) > target) return -1.0;  // always check exactly
+    double lo = 0.0, hi = 1.0;
+    while (majorant(hi) * (1 + 1e-6) <= target && hi < 1e12) hi *= 2;
+    if (hi >= 1e12) return 1e300;
+    for (int it = 0; it < 200; ++it) {
+        const double mid = 0.5 * (lo + hi);
+        if (majorant(mid) * (1 + 1e-6) <= target) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+struct Sim1D {
+    apic_config1d cfg{};
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    Params1D p{};
+    DevState* st = nullptr;
+    std::vector<void*> allocations;
+    std::vector<std::vector<double>> tables;  // host copies (kept for safe_speed)
+    bool pending = false;   // collision part of the last step not yet applied
+    bool initialized = false;
+    int parity = 0;         // which of the two buffers holds the current state
+    double time = 0.0;
+    uint64_t step = 0;
+    double neutral_stddev[kMaxModels] = {0, 0, 0, 0};
+
+    template <class T>
+    T* dalloc(size_t count) {
+        void* ptr = nullptr;
+        APIC_CUDA(cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T)));
+        allocations.push_back(ptr);
+        APIC_CUDA(cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), stream));
+        return static_cast<T*>(ptr);
+    }
+
+    ~Sim1D() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* a : allocations) cudaFree(a);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void create(const apic_config1d& c) {
+        cfg = c;
+        require(c.boundary == APIC_PERIODIC || c.boundary == APIC_DIRICHLET, "unknown boundary");
+        require(c.velocity_dimensions == 1 || c.velocity_dimensions == 3,
+                "simulation velocity_dimensions must be 1 or 3");
+        require(c.nx >= 3, "grid nx must be at least 3");
+        require(c.nx <= (size_t)kMaxNx1D, "grid nx above the 1D device limit (4096)", APIC_ERR_UNSUPPORTED);
+        require(std::isfinite(c.length) && c.length > 0, "domain length must be positive and finite");
+        require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
+        require(c.nspecies >= 1 && c.nspecies <= kMaxSpecies, "species count out of range");
+        require(c.nmodels >= 0 && c.nmodels <= kMaxModels, "model count out of range");
+        require(c.precision == APIC_FP64, "this entry point builds the FP64 form", APIC_ERR_UNSUPPORTED);
+        const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
+        require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
+        APIC_CUDA(cudaGetDevice(&device));
+        APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+
+        const bool dir = c.boundary == APIC_DIRICHLET;
+        p.nspecies = c.nspecies;
+        p.vdim = c.velocity_dimensions;
+        p.dirichlet = dir;
+        p.nx = (int)c.nx;
+        p.L = c.length;
+        p.dx = c.length / (double)(dir ? c.nx - 1 : c.nx);  // Grid::Grid, src/Grid.cpp:19-22
+        p.dt = c.dt;
+        p.eps = (c.units == APIC_SI ? 8.8541878128e-12 : 1.0) * rel;  // include/pic/Types.hpp:17-27
+        p.seed = c.seed;
+        p.phi_left = c.phi_left;
+        p.phi_right = c.phi_right;
+        p.drive_left = c.drive_left;
+        p.drive_right = c.drive_right;
+
+        // fixed-point scale: worst-case |rho| bound below 2^62
+        double bound = 0.0;
+        for (int s = 0; s < c.nspecies; ++s) {
+            const auto& sp = c.species[s];
+            require(std::isfinite(sp.mass) && sp.mass > 0, "species mass must be positive and finite");
+            require(std::isfinite(sp.charge) && std::isfinite(sp.weight), "species charge/weight must be finite");
+            require(sp.capacity > 0 && sp.capacity < (1ull << 31), "species capacity out of range");
+            bound += (double)sp.capacity * std::fabs(sp.charge * sp.weight) / (dir ? 0.5 * p.dx : p.dx);
+        }
+        int bits = bound > 0 ? (int)std::floor(61.0 - std::log2(bound)) : 0;
+        p.rho_scale = std::ldexp(1.0, bits);
+        p.inv_rho_scale = std::ldexp(1.0, -bits);
+
+        st = dalloc<DevState>(1);
+        p.st = st;
+        for (int s = 0; s < c.nspecies; ++s) {
+            const auto& sp = c.species[s];
+            SpeciesDev& S = p.sp[s];
+            S.qm = sp.charge / sp.mass;
+            S.hqm = 0.5 * S.qm;
+            S.qw = sp.charge * sp.weight;
+            S.qwdx = sp.charge * sp.weight / p.dx;
+            S.mass = sp.mass;
+            S.weight = sp.weight;
+            S.model = -1;
+            S.capacity = (unsigned)sp.capacity;
+            const size_t cap = sp.capacity;
+            S.lookback = dalloc<unsigned long long>((cap + kTile - 1) / kTile + 1);
+            for (int b = 0; b < 2; ++b) {
+                S.x[b] = dalloc<double>(cap);
+                S.vh[b] = dalloc<double>(cap);
+                S.vy[b] = c.velocity_dimensions == 3 ? dalloc<double>(cap) : nullptr;
+                S.vz[b] = c.velocity_dimensions == 3 ? dalloc<double>(cap) : nullptr;
+            }
+            S.v = dalloc<double>(cap);
+        }
+        for (int mi = 0; mi < c.nmodels; ++mi) {
+            const apic_mcc_model& m = c.models[mi];
+            require(m.species >= 0 && m.species < c.nspecies, "MCC species does not exist");
+            require(p.sp[m.species].model < 0, "one MCC model per species is supported", APIC_ERR_UNSUPPORTED);
+            require(c.velocity_dimensions == 3, "1D MCC on the device requires velocity_dimensions = 3",
+                    APIC_ERR_UNSUPPORTED);
+            require(std::isfinite(m.neutral_density) && m.neutral_density > 0, "MCC neutral_density must be positive and finite");
+            require(std::isfinite(m.max_frequency) && m.max_frequency > 0, "MCC max_frequency must be positive and finite");
+            require(m.max_candidates > 0, "MCC max_candidates_per_particle must be positive");
+            require(m.nch >= 1 && m.nch <= kMaxChannels, "MCC requires at least one collision channel");
+            const double mass = c.species[m.species].mass;
+            MccModelDev& D = p.model[mi];
+            D.nch = m.nch;
+            D.species = m.species;
+            D.particle_mass = mass;
+            D.neutral_mass = m.neutral_mass;
+            D.neutral_density = m.neutral_density;
+            D.max_frequency = m.max_frequency;
+            D.max_candidates = (unsigned)std::min<size_t>(m.max_candidates, 0xFFFFFFFFu);
+            D.com_mass = m.neutral_mass > 0 ? mass * m.neutral_mass / (mass + m.neutral_mass) : 0.0;
+            double sd = 0.0;
+            if (m.gas_units_si && m.neutral_temperature > 0) {
+                require(m.neutral_mass > 0, "thermal-neutral MCC requires positive neutral_mass");
+                sd = std::sqrt(1.380649e-23 * m.neutral_temperature / m.neutral_mass);
+            }
+            D.neutral_stddev = sd;
+            neutral_stddev[mi] = sd;
+            for (int ci = 0; ci < m.nch; ++ci) {
+                const apic_mcc_channel& ch = m.ch[ci];
+                require(ch.rows >= 2 && ch.energy && ch.sigma, "collision cross-section table requires at least two rows");
+                for (size_t k = 0; k < ch.rows; ++k) {
+                    require(std::isfinite(ch.energy[k]) && ch.energy[k] >= 0 && std::isfinite(ch.sigma[k]) && ch.sigma[k] >= 0,
+                            "collision table values must be finite and non-negative");
+                    require(k == 0 || ch.energy[k] > ch.energy[k - 1], "collision table energies must be strictly increasing");
+                }
+                require(ch.angular == APIC_ISOTROPIC || ch.angular == APIC_BACKWARD,
+                        "Henyey-Greenstein scattering is not supported", APIC_ERR_UNSUPPORTED);
+                require(ch.process != APIC_ATTACHMENT, "1D MCC does not support attachment");
+                if (ch.process == APIC_IONIZATION) {
+                    require(ch.secondary_species >= 0 && ch.secondary_species < c.nspecies &&
+                                ch.ion_species >= 0 && ch.ion_species < c.nspecies,
+                            "ionization MCC channel requires secondary and ion species");
+                    const auto& tgt = c.species[m.species];
+                    const auto& sec = c.species[ch.secondary_species];
+                    const auto& ion = c.species[ch.ion_species];
+                    require(tgt.charge != 0.0 && tgt.weight == sec.weight && tgt.weight == ion.weight &&
+                                tgt.mass == sec.mass && tgt.charge == sec.charge && ion.charge == -tgt.charge,
+                            "1D ionization products violate the equal-weight charge-conservation contract");
+                }
+                if (ch.process == APIC_CHARGE_EXCHANGE) {
+                    const double tol = 64.0 * 2.220446049250313e-16 * std::max(mass, m.neutral_mass);
+                    require(m.neutral_mass > 0 && std::fabs(mass - m.neutral_mass) <= tol,
+                            "resonant charge exchange requires projectile mass equal to neutral_mass");
+                }
+                MccChannelDev& C = D.ch[ci];
+                C.process = ch.process;
+                C.angular = ch.angular;
+                C.frame = ch.energy_frame;
+                C.threshold = ch.threshold_energy;
+                C.secondary = ch.secondary_species;
+                C.ion = ch.ion_species;
+                C.rows = (int)ch.rows;
+                double* e = dalloc<double>(ch.rows);
+                double* s = dalloc<double>(ch.rows);
+                APIC_CUDA(cudaMemcpyAsync(e, ch.energy, ch.rows * sizeof(double), cudaMemcpyHostToDevice, stream));
+                APIC_CUDA(cudaMemcpyAsync(s, ch.sigma, ch.rows * sizeof(double), cudaMemcpyHostToDevice, stream));
+                C.energy = e;
+                C.sigma = s;
+            }
+            D.v_safe = safe_speed(m, mass, sd);
+            p.sp[m.species].model = mi;
+            APIC_CUDA(cudaStreamSynchronize(stream));  // host tables may be freed after create
+        }
+        p.E = dalloc<double>(c.nx);
+        p.rho = dalloc<double>(c.nx);
+        p.phi = dalloc<double>(c.nx);
+        p.rho_acc = dalloc<unsigned long long>(c.nx);
+        if (!dir) {
+            std::vector<double> tw(2 * c.nx);
+            const double twopi = 2.0 * 3.141592653589793;
+            for (size_t m = 0; m < c.nx; ++m) {
+                const double a = twopi * (double)m / (double)c.nx;
+                tw[2 * m] = std::cos(a);
+                tw[2 * m + 1] = std::sin(a);
+            }
+            double* d = dalloc<double>(tw.size());
+            APIC_CUDA(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+            p.tw = d;
+            p.scratch = dalloc<double>(4 * c.nx);
+            APIC_CUDA(cudaStreamSynchronize(stream));
+        } else {
+            // Thomas coefficients of the constant [-1 2 -1] matrix, src/FieldSolver.cpp:745-752
+            const size_t m = c.nx - 2;
+            std::vector<double> cp(m), r(m), a(m);
+            cp[0] = -1.0 / 2.0;
+            r[0] = 0.5;
+            for (size_t i = 1; i < m; ++i) {
+                const double den = 2.0 + cp[i - 1];
+                cp[i] = (i == m - 1) ? 0.0 : -1.0 / den;
+                r[i] = 1.0 / den;
+            }
+            for (size_t i = 0; i < m; ++i) a[i] = -cp[i];
+            double* dr = dalloc<double>(m);
+            double* da = dalloc<double>(m);
+            APIC_CUDA(cudaMemcpyAsync(dr, r.data(), m * sizeof(double), cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(da, a.data(), m * sizeof(double), cudaMemcpyHostToDevice, stream));
+            p.thomas_r = dr;
+            p.thomas_a = da;
+            APIC_CUDA(cudaStreamSynchronize(stream));
+        }
+        size_t cap_total = 0;
+        for (int s = 0; s < c.nspecies; ++s) cap_total += c.species[s].capacity;
+        p.births_cap = (unsigned)std::min<size_t>(std::max<size_t>(kMaxBirths, cap_total / 64), kMaxBirths);
+        p.births = dalloc<BirthRec>(p.births_cap);
+        DevState init{};
+        init.epoch = 1;
+        APIC_CUDA(cudaMemcpyAsync(st, &init, sizeof init, cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        static bool attr_done = false;
+        if (!attr_done) {
+            const int smem = kMaxNx1D * 16;
+            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            attr_done = true;
+        }
+    }
+
+    // Buffers as seen by the next pass.
+    Params1D pass_params(unsigned mode) {
+        Params1D q = p;
+        q.mode = mode;
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            SpeciesDev& S = q.sp[s];
+            const SpeciesDev& B = p.sp[s];
+            const int in = parity, out = parity ^ 1;
+            S.x[0] = B.x[in]; S.x[1] = B.x[out];
+            S.vh[0] = B.vh[in]; S.vh[1] = B.vh[out];
+            S.vy[0] = B.vy[in]; S.vy[1] = B.vy[out];
+            S.vz[0] = B.vz[in]; S.vz[1] = B.vz[out];
+        }
+        return q;
+    }
+
+    int grid_blocks() const {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        size_t tiles = 0;
+        for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
+        return (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 4));
+    }
+
+    void launch_pass(unsigned mode, unsigned post) {
+        const Params1D q = pass_params(mode);
+        const int blocks = grid_blocks();
+        const size_t smem = (size_t)cfg.nx * 16;
+        const bool dir = cfg.boundary == APIC_DIRICHLET;
+        if (cfg.velocity_dimensions == 3) {
+            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); k_post1d<3, true><<<1, kPostThreads, 0, stream>>>(q, post); }
+            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); k_post1d<3, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+        } else {
+            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); k_post1d<1, true><<<1, kPostThreads, 0, stream>>>(q, post); }
+            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); k_post1d<1, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+        }
+        APIC_CUDA(cudaGetLastError());
+        parity ^= 1;
+    }
+
+    void load(int s, size_t n, const double* x, const double* v, const double* vh, const double* vy,
+              const double* vz, const uint8_t* alive) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        require(x && v, "x and v are required");
+        std::vector<double> hx, hv, hvh, hvy, hvz;
+        for (size_t i = 0; i < n; ++i) {
+            if (alive && !alive[i]) continue;
+            hx.push_back(x[i]);
+            hv.push_back(v[i]);
+            hvh.push_back(vh ? vh[i] : v[i]);
+            hvy.push_back(vy ? vy[i] : 0.0);
+            hvz.push_back(vz ? vz[i] : 0.0);
+        }
+        const size_t m = hx.size();
+        require(m <= cfg.species[s].capacity, "initial particle count exceeds max_particles_per_species",
+                APIC_ERR_CAPACITY);
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        SpeciesDev& B = p.sp[s];
+        const size_t bytes = m * sizeof(double);
+        APIC_CUDA(cudaMemcpyAsync(B.x[parity], hx.data(), bytes, cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(B.vh[parity], hvh.data(), bytes, cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(B.v, hv.data(), bytes, cudaMemcpyHostToDevice, stream));
+        if (cfg.velocity_dimensions == 3) {
+            APIC_CUDA(cudaMemcpyAsync(B.vy[parity], hvy.data(), bytes, cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(B.vz[parity], hvz.data(), bytes, cudaMemcpyHostToDevice, stream));
+        }
+        const unsigned n32 = (unsigned)m;
+        APIC_CUDA(cudaMemcpyAsync(&st->n[s], &n32, sizeof n32, cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        initialized = false;
+        pending = false;
+    }
+
+    void set_time(double t, uint64_t k) {
+        time = t;
+        step = k;
+        APIC_CUDA(cudaMemcpyAsync(&st->time, &time, sizeof time, cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(&st->step, &step, sizeof step, cudaMemcpyHostToDevice, stream));
+    }
+
+    // Simulation::initialize, src/Simulation.cpp:698-769
+    void initialize() {
+        set_time(0.0, 0);
+        launch_pass(kModeDeposit, kPostSolve);
+        launch_pass(kModeInitHalf, 0);
+        pending = false;
+        initialized = true;
+    }
+
+    void resume(double t, uint64_t k) {
+        set_time(t, k);
+        launch_pass(kModeDeposit, kPostSolve);
+        pending = false;
+        initialized = true;
+    }
+
+    void do_steps(size_t nsteps) {
+        require(initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
+        for (size_t i = 0; i < nsteps; ++i) {
+            const unsigned mode = (pending ? kModeSyncMcc : 0u) | kModeKickDrift | kModeDeposit;
+            launch_pass(mode, kPostSolve | kPostAdvance | kPostPushBirths);
+            pending = true;
+            time += cfg.dt;
+            ++step;
+        }
+    }
+
+    // Applies the pending collision part of the last step so the state equals
+    // the reference's state after step() returned.
+    void finish() {
+        if (!initialized) return;
+        if (pending) {
+            launch_pass(kModeSyncMcc | kModeWriteV, 0);
+            pending = false;
+        }
+    }
+
+    int sync_status() {
+        const cudaError_t e = bounded_wait(stream, 600.0);
+        if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
+        APIC_CUDA(e);
+        unsigned word = 0;
+        APIC_CUDA(cudaMemcpy(&word, &st->error, sizeof word, cudaMemcpyDeviceToHost));
+        if (word) {
+            const int s = status_from_device(word);
+            const unsigned zero = 0;
+            APIC_CUDA(cudaMemcpy(&st->error, &zero, sizeof zero, cudaMemcpyHostToDevice));
+            throw Error(s, describe_device_error(word));
+        }
+        return APIC_OK;
+    }
+
+    DevState read_state() {
+        sync_status();
+        DevState h;
+        APIC_CUDA(cudaMemcpy(&h, st, sizeof h, cudaMemcpyDeviceToHost));
+        return h;
+    }
+
+    size_t count(int s) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        finish();
+        return read_state().n[s];
+    }
+
+    size_t read_particles(int s, size_t cap, double* x, double* v, double* vh, double* vy, double* vz) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        finish();
+        const size_t n = read_state().n[s];
+        require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
+        const SpeciesDev& B = p.sp[s];
+        const size_t bytes = n * sizeof(double);
+        if (x) APIC_CUDA(cudaMemcpy(x, B.x[parity], bytes, cudaMemcpyDeviceToHost));
+        if (v) APIC_CUDA(cudaMemcpy(v, B.v, bytes, cudaMemcpyDeviceToHost));
+        if (vh) APIC_CUDA(cudaMemcpy(vh, B.vh[parity], bytes, cudaMemcpyDeviceToHost));
+        if (cfg.velocity_dimensions == 3) {
+            if (vy) APIC_CUDA(cudaMemcpy(vy, B.vy[parity], bytes, cudaMemcpyDeviceToHost));
+            if (vz) APIC_CUDA(cudaMemcpy(vz, B.vz[parity], bytes, cudaMemcpyDeviceToHost));
+        } else {
+            if (vy) std::memset(vy, 0, bytes);
+            if (vz) std::memset(vz, 0, bytes);
+        }
+        return n;
+    }
+
+    void read_fields(double* rho, double* phi, double* E) {
+        sync_status();
+        const size_t bytes = cfg.nx * sizeof(double);
+        if (rho) APIC_CUDA(cudaMemcpy(rho, p.rho, bytes, cudaMemcpyDeviceToHost));
+        if (phi) APIC_CUDA(cudaMemcpy(phi, p.phi, bytes, cudaMemcpyDeviceToHost));
+        if (E) APIC_CUDA(cudaMemcpy(E, p.E, bytes, cudaMemcpyDeviceToHost));
+    }
+};
+
+}  // namespace apic
+
+// ---- C ABI ----------------------------------------------------------------------
+
+using apic::Error;
+
+struct apic_sim1d {
+    apic::Sim1D impl;
+};
+
+namespace {
+thread_local std::string g_error;
+
+template <class F>
+int guarded(apic_sim1d* h, F&& f) {
+    try {
+        f();
+        return APIC_OK;
+    } catch (const Error& e) {
+        if (h) h->impl.last_error = e.what();
+        g_error = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        if (h) h->impl.last_error = e.what();
+        g_error = e.what();
+        return APIC_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+const char* apic_version(void) { return "aurora-pic-b200 0.1 (sm_100a)"; }
+
+const char* apic_status_string(int s) {
+    switch (s) {
+        case APIC_OK: return "ok";
+        case APIC_ERR_INVALID: return "invalid argument";
+        case APIC_ERR_CUDA: return "CUDA error";
+        case APIC_ERR_CAPACITY: return "particle capacity exceeded";
+        case APIC_ERR_MAJORANT: return "collision frequency above max_frequency";
+        case APIC_ERR_CANDIDATES: return "MCC candidate limit exceeded";
+        case APIC_ERR_NONFINITE: return "non-finite particle state";
+        case APIC_ERR_TIMEOUT: return "device wait timed out";
+        case APIC_ERR_UNSUPPORTED: return "unsupported configuration";
+        case APIC_ERR_STATE: return "call out of order";
+        case APIC_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+int apic_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int apic_sim1d_create(const apic_config1d* cfg, apic_sim1d** out) {
+    if (!cfg || !out) return APIC_ERR_INVALID;
+    *out = nullptr;
+    auto h = std::make_unique<apic_sim1d>();
+    const int rc = guarded(h.get(), [&] { h->impl.create(*cfg); });
+    if (rc == APIC_OK) *out = h.release();
+    return rc;
+}
+
+void apic_sim1d_destroy(apic_sim1d* sim) { delete sim; }
+
+const char* apic_sim1d_last_error(const apic_sim1d* sim) {
+    return sim ? sim->impl.last_error.c_str() : g_error.c_str();
+}
+
+int apic_sim1d_load_particles(apic_sim1d* sim, int species, size_t n, const double* x, const double* v,
+                              const double* v_half, const double* vy, const double* vz, const uint8_t* alive) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.load(species, n, x, v, v_half, vy, vz, alive); });
+}
+
+int apic_sim1d_initialize(apic_sim1d* sim) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.initialize(); });
+}
+
+int apic_sim1d_resume(apic_sim1d* sim, double time, uint64_t step) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.resume(time, step); });
+}
+
+int apic_sim1d_step(apic_sim1d* sim, size_t nsteps) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.do_steps(nsteps); });
+}
+
+int apic_sim1d_synchronize(apic_sim1d* sim) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.sync_status(); });
+}
+
+int apic_sim1d_count(apic_sim1d* sim, int species, size_t* n) {
+    if (!sim || !n) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { *n = sim->impl.count(species); });
+}
+
+int apic_sim1d_read_particles(apic_sim1d* sim, int species, size_t capacity, double* x, double* v,
+                              double* v_half, double* vy, double* vz, size_t* n) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        const size_t got = sim->impl.read_particles(species, capacity, x, v, v_half, vy, vz);
+        if (n) *n = got;
+    });
+}
+
+int apic_sim1d_read_fields(apic_sim1d* sim, double* rho, double* phi, double* electric) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.read_fields(rho, phi, electric); });
+}
+
+int apic_sim1d_collision_totals(apic_sim1d* sim, apic_collision_totals* out) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        sim->impl.finish();
+        const apic::DevState h = sim->impl.read_state();
+        std::memset(out, 0, sizeof *out);
+        out->candidates = h.candidates;
+        out->null_collisions = h.nulls;
+        for (int m = 0; m < APIC_MAX_MODELS; ++m)
+            for (int c = 0; c < APIC_MAX_CHANNELS; ++c) {
+                out->channel_collisions[m][c] = h.chan[m][c];
+                out->channel_energy_change[m][c] = h.chan_energy[m][c];
+            }
+    });
+}
+
+int apic_sim1d_boundary_losses(apic_sim1d* sim, int species, apic_boundary_loss* out) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        apic::require(species >= 0 && species < sim->impl.cfg.nspecies, "species index out of range");
+        const apic::DevState h = sim->impl.read_state();
+        out->absorbed_left = h.lost[species][0];
+        out->absorbed_right = h.lost[species][1];
+        out->kinetic_energy_left = h.lost_energy[species][0];
+        out->kinetic_energy_right = h.lost_energy[species][1];
+    });
+}
+
+int apic_sim1d_sample(apic_sim1d* sim, apic_sample1d* out) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        auto& S = sim->impl;
+        S.finish();
+        std::memset(out, 0, sizeof *out);
+        const apic::DevState h = S.read_state();
+        const size_t nx = S.cfg.nx;
+        std::vector<double> rho(nx), phi(nx), E(nx);
+        S.read_fields(rho.data(), phi.data(), E.data());
+        // Species::kinetic_energy and Simulation::sample, src/Species.cpp:338-351,
+        // src/Simulation.cpp:1140-1161 (reduced on the host from the read-back state)
+        for (int s = 0; s < S.cfg.nspecies; ++s) {
+            const size_t n = h.n[s];
+            std::vector<double> v(n), vy(n), vz(n);
+            S.read_particles(s, n, nullptr, v.data(), nullptr, vy.data(), vz.data());
+            double e = 0.0;
+            const auto& sp = S.cfg.species[s];
+            for (size_t i = 0; i < n; ++i) {
+                double sq = v[i] * v[i];
+                if (S.cfg.velocity_dimensions == 3) sq += vy[i] * vy[i] + vz[i] * vz[i];
+                e += 0.5 * sp.mass * sp.weight * sq;
+            }
+            out->kinetic_by_species[s] = e;
+            out->live_by_species[s] = n;
+            out->kinetic_energy += e;
+            out->live_particles += n;
+        }
+        const bool dir = S.cfg.boundary == APIC_DIRICHLET;
+        for (size_t i = 0; i < nx; ++i) {
+            const double vol = dir ? ((i == 0 || i + 1 == nx) ? 0.5 * S.p.dx : S.p.dx) : S.p.dx;
+            out->field_energy += 0.5 * S.p.eps * E[i] * E[i] * vol;
+            out->charge_l1 += std::fabs(rho[i]) * vol;
+        }
+        out->total_energy = out->kinetic_energy + out->field_energy;
+        if (dir) {
+            out->phi_left = phi.front();
+            out->phi_right = phi.back();
+        }
+        out->step = S.step;
+        out->time = S.time;
+    });
+}
+
+double apic_sim1d_time(const apic_sim1d* sim) { return sim ? sim->impl.time : 0.0; }
+uint64_t apic_sim1d_step_count(const apic_sim1d* sim) { return sim ? sim->impl.step : 0; }
+
+int apic_deposit_solve_gather_1d(int boundary, size_t nx, double length, double permittivity, double phi_left,
+                                 double phi_right, int nspecies, const double* charge, const double* weight,
+                                 const size_t* counts, const double* const* xs, double* rho, double* phi,
+                                 double* electric, size_t nq, const double* xq, double* eq) {
+    return guarded(nullptr, [&] {
+        apic::require(nspecies >= 1 && nspecies <= APIC_MAX_SPECIES, "species count out of range");
+        apic::require(std::isfinite(permittivity) && permittivity > 0,
+                      "field-solver permittivity must be positive and finite");
+        apic_config1d c{};
+        c.boundary = boundary;
+        c.velocity_dimensions = 1;
+        c.units = APIC_NORMALIZED;
+        c.relative_permittivity = permittivity;
+        c.nx = nx;
+        c.length = length;
+        c.dt = 1.0;
+        c.phi_left = phi_left;
+        c.phi_right = phi_right;
+        c.nspecies = nspecies;
+        for (int s = 0; s < nspecies; ++s) {
+            c.species[s].charge = charge[s];
+            c.species[s].weight = weight[s];
+            c.species[s].mass = 1.0;
+            c.species[s].capacity = std::max<size_t>(counts[s], 1);
+        }
+        apic::Sim1D S;
+        S.create(c);
+        for (int s = 0; s < nspecies; ++s) {
+            std::vector<double> zeros(counts[s], 0.0);
+            S.load(s, counts[s], xs[s], zeros.data(), zeros.data(), nullptr, nullptr, nullptr);
+        }
+        S.resume(0.0, 0);
+        S.read_fields(rho, phi, electric);
+        if (nq > 0) {
+            double* dq = S.dalloc<double>(nq);
+            double* de = S.dalloc<double>(nq);
+            APIC_CUDA(cudaMemcpyAsync(dq, xq, nq * sizeof(double), cudaMemcpyHostToDevice, S.stream));
+            const unsigned blocks = (unsigned)((nq + 255) / 256);
+            if (boundary == APIC_DIRICHLET)
+                apic::k_gather_points1d<true><<<blocks, 256, 0, S.stream>>>(S.p, dq, de, (int)nq);
+            else
+                apic::k_gather_points1d<false><<<blocks, 256, 0, S.stream>>>(S.p, dq, de, (int)nq);
+            APIC_CUDA(cudaGetLastError());
+            APIC_CUDA(cudaMemcpyAsync(eq, de, nq * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+            APIC_CUDA(cudaStreamSynchronize(S.stream));
+        }
+    });
+}
+
+int apic_collide3(const apic_mcc_model* model, double particle_mass, size_t n, double* v3, double dt,
+                  const uint64_t* draws, const uint64_t* offsets, uint64_t seed, uint64_t step, uint32_t stream,
+                  apic_collide_stats* stats) {
+    return guarded(nullptr, [&] {
+        apic::require(model && v3 && stats, "null argument");
+        apic::require(n > 0 && n < (1u << 30), "particle count out of range");
+        apic::require(std::isfinite(dt) && dt > 0, "MCC timestep must be positive and finite");
+        apic_config1d c{};
+        c.boundary = APIC_DIRICHLET;
+        c.velocity_dimensions = 3;
+        c.units = APIC_SI;
+        c.nx = 3;
+        c.length = 1.0;
+        c.dt = dt;
+        // a projectile species plus an opposite-charge product species satisfy
+        // the model validation; the stateless form reports products in stats
+        c.nspecies = 2;
+        c.species[0].charge = 1.0;
+        c.species[0].mass = particle_mass;
+        c.species[0].weight = 1.0;
+        c.species[0].capacity = 1;
+        c.species[1] = c.species[0];
+        c.species[1].charge = -1.0;
+        c.nmodels = 1;
+        c.models[0] = *model;
+        c.models[0].species = 0;
+        for (int i = 0; i < model->nch; ++i) {
+            c.models[0].ch[i].secondary_species = 0;
+            c.models[0].ch[i].ion_species = 1;
+        }
+        apic::Sim1D S;
+        S.create(c);
+        cudaStream_t s = S.stream;
+        double* dv = S.dalloc<double>(3 * n);
+        apic_collide_stats* ds = S.dalloc<apic_collide_stats>(n);
+        uint64_t* dd = nullptr;
+        uint64_t* doff = nullptr;
+        if (draws) {
+            apic::require(offsets != nullptr, "replay draws need per-particle offsets");
+            const uint64_t total = offsets[n];
+            dd = S.dalloc<uint64_t>(total);
+            doff = S.dalloc<uint64_t>(n + 1);
+            APIC_CUDA(cudaMemcpyAsync(dd, draws, total * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            APIC_CUDA(cudaMemcpyAsync(doff, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        }
+        APIC_CUDA(cudaMemcpyAsync(dv, v3, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+        apic::k_collide3<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(S.p.model[0], (int)n, dv, dt, dd, doff, seed,
+                                                                    (uint32_t)step, stream, ds);
+        APIC_CUDA(cudaGetLastError());
+        APIC_CUDA(cudaMemcpyAsync(v3, dv, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+        APIC_CUDA(cudaMemcpyAsync(stats, ds, n * sizeof(apic_collide_stats), cudaMemcpyDeviceToHost, s));
+        APIC_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+/*
+ * aurorapic_b200.h - C ABI of the B200-native electrostatic PIC particle step.
+ *
+ * Drop-in boundary for AuroraPIC's structured-grid particle step.  The
+ * reference is a C++ library (include/pic/*.hpp); each entry point below names
+ * the reference interface it replaces.  All entry points:
+ *   - take plain pointers and sizes (host memory unless stated otherwise),
+ *   - never throw and never retain caller memory after returning,
+ *   - return an apic_status; the handle's last-error string explains failures
+ *     (reference exceptions become status codes, see apic_status).
+ * Calls on one handle are serialised on that handle's CUDA stream; separate
+ * handles are independent.  Device memory is owned by the handle.
+ */
+#ifndef AURORAPIC_B200_H
+#define AURORAPIC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define APIC_EXPORT __attribute__((visibility("default")))
+#else
+#define APIC_EXPORT
+#endif
+
+#define APIC_MAX_SPECIES 4
+#define APIC_MAX_MODELS 4
+#define APIC_MAX_CHANNELS 8
+
+/* Reference exceptions map onto these codes:
+ *   std::invalid_argument          -> APIC_ERR_INVALID
+ *   MCC "exceeds max_frequency"    -> APIC_ERR_MAJORANT   (src/Collision.cpp:620-623, :680-684)
+ *   MCC candidate limit            -> APIC_ERR_CANDIDATES (src/Collision.cpp:938-943)
+ *   max_particles_per_species      -> APIC_ERR_CAPACITY   (src/Simulation.cpp:941-964)
+ *   non-finite particle state      -> APIC_ERR_NONFINITE  (src/Collision.cpp:910-916)
+ */
+typedef enum {
+    APIC_OK = 0,
+    APIC_ERR_INVALID = 1,
+    APIC_ERR_CUDA = 2,
+    APIC_ERR_CAPACITY = 3,
+    APIC_ERR_MAJORANT = 4,
+    APIC_ERR_CANDIDATES = 5,
+    APIC_ERR_NONFINITE = 6,
+    APIC_ERR_TIMEOUT = 7,
+    APIC_ERR_UNSUPPORTED = 8,
+    APIC_ERR_STATE = 9,
+    APIC_ERR_NO_DEVICE = 10
+} apic_status;
+
+typedef enum { APIC_PERIODIC = 0, APIC_DIRICHLET = 1 } apic_boundary;
+typedef enum { APIC_NORMALIZED = 0, APIC_SI = 1 } apic_units;
+/* Particle storage form.  FP64: x and velocities in double, bit-faithful to
+ * the reference arithmetic.  FP32: integer cell index + float in-cell offset
+ * and float velocities; charge accumulation, field solve and diagnostics
+ * stay FP64. */
+typedef enum { APIC_FP64 = 0, APIC_FP32 = 1 } apic_precision;
+
+/* CollisionProcessKind, include/pic/Config.hpp:42-48 */
+typedef enum {
+    APIC_ELASTIC = 0,
+    APIC_EXCITATION = 1,
+    APIC_IONIZATION = 2,
+    APIC_ATTACHMENT = 3,
+    APIC_CHARGE_EXCHANGE = 4
+} apic_process;
+/* AngularScatteringKind, include/pic/Config.hpp:33-37 (Henyey-Greenstein is
+ * not supported by this build and is rejected with APIC_ERR_UNSUPPORTED). */
+typedef enum { APIC_ISOTROPIC = 0, APIC_BACKWARD = 1 } apic_angular;
+/* CollisionEnergyFrame, include/pic/Config.hpp:38-41 */
+typedef enum { APIC_FRAME_PROJECTILE = 0, APIC_FRAME_CENTER_OF_MASS = 1 } apic_frame;
+
+/* CollisionChannelConfig + CrossSectionTable, include/pic/Config.hpp:82-98,
+ * include/pic/Collision.hpp:15-31.  Energies in joules (SI) or normalized
+ * energy units, already multiplied by any energy_scale; strictly increasing. */
+typedef struct {
+    int process;            /* apic_process */
+    int angular;            /* apic_angular */
+    int energy_frame;       /* apic_frame */
+    double threshold_energy;
+    int secondary_species;  /* ionization: species index receiving the secondary */
+    int ion_species;        /* ionization: species index receiving the ion */
+    size_t rows;
+    const double* energy;
+    const double* sigma;
+} apic_mcc_channel;
+
+/* CollisionConfig (null_collision), include/pic/Config.hpp:110-132 */
+typedef struct {
+    int species;                /* projectile species index */
+    double neutral_density;
+    double max_frequency;
+    double neutral_mass;
+    double neutral_temperature; /* thermal (8-sigma bounded Maxwellian) neutrals when > 0 and gas_units_si */
+    int gas_units_si;
+    size_t max_candidates;      /* max_candidates_per_particle */
+    int nch;
+    apic_mcc_channel ch[APIC_MAX_CHANNELS];
+} apic_mcc_model;
+
+/* SinusoidalVoltageConfig, include/pic/Config.hpp:139-143 */
+typedef struct { double amplitude, frequency, phase; } apic_voltage_drive;
+
+/* SpeciesConfig subset that the particle step reads, include/pic/Config.hpp:16-30 */
+typedef struct {
+    double charge, mass, weight;
+    size_t capacity;            /* max_particles_per_species */
+} apic_species;
+
+/* Config subset of the 1D particle step, include/pic/Config.hpp:170-209 */
+typedef struct {
+    int boundary;               /* apic_boundary */
+    int velocity_dimensions;    /* 1 or 3 */
+    int units;                  /* apic_units */
+    double relative_permittivity;
+    size_t nx;
+    double length, dt;
+    double phi_left, phi_right;
+    apic_voltage_drive drive_left, drive_right;
+    int precision;              /* apic_precision */
+    uint64_t seed;              /* Philox key of the collision streams */
+    int nspecies;
+    apic_species species[APIC_MAX_SPECIES];
+    int nmodels;
+    apic_mcc_model models[APIC_MAX_MODELS];
+} apic_config1d;
+
+/* DiagnosticSample, include/pic/Diagnostics.hpp (Simulation::sample,
+ * src/Simulation.cpp:1140-1161). */
+typedef struct {
+    uint64_t step;
+    double time;
+    double kinetic_energy;
+    double field_energy;
+    double total_energy;
+    double charge_l1;
+    uint64_t live_particles;
+    double phi_left, phi_right;
+    double kinetic_by_species[APIC_MAX_SPECIES];
+    uint64_t live_by_species[APIC_MAX_SPECIES];
+} apic_sample1d;
+
+/* CollisionDiagnostics totals, include/pic/Collision.hpp:64-70, laid out
+ * [model][channel]. */
+typedef struct {
+    uint64_t candidates;
+    uint64_t null_collisions;
+    uint64_t channel_collisions[APIC_MAX_MODELS][APIC_MAX_CHANNELS];
+    double channel_energy_change[APIC_MAX_MODELS][APIC_MAX_CHANNELS];
+} apic_collision_totals;
+
+/* BoundaryLoss1D, include/pic/Simulation.hpp:20-25 */
+typedef struct {
+    uint64_t absorbed_left, absorbed_right;
+    double kinetic_energy_left, kinetic_energy_right;
+} apic_boundary_loss;
+
+/* Per-call collision statistics of one particle (CollisionStepStatistics,
+ * include/pic/Collision.hpp:51-62).  Secondaries beyond 4 are counted only. */
+typedef struct {
+    uint64_t candidates, null_collisions;
+    uint32_t channel_collisions[APIC_MAX_CHANNELS];
+    double energy_change[APIC_MAX_CHANNELS];
+    int nsecondaries;
+    int secondary_channel[4];
+    double secondary_velocity[4][3];
+    double secondary_ion_velocity[4][3];
+    int removed;
+    uint32_t draws;             /* raw 64-bit draws consumed */
+} apic_collide_stats;
+
+typedef struct apic_sim1d apic_sim1d;
+
+/* ---- library ------------------------------------------------------------ */
+APIC_EXPORT const char* apic_version(void);
+APIC_EXPORT const char* apic_status_string(int status);
+/* Number of visible CUDA devices (0 when none). */
+APIC_EXPORT int apic_device_count(void);
+
+/* ---- 1D simulation (replaces pic::Simulation, include/pic/Simulation.hpp:56-64) */
+
+/* Simulation::Simulation(Config), src/Simulation.cpp:341-470.  Validates the
+ * configuration and allocates device storage for every species' capacity. */
+APIC_EXPORT int apic_sim1d_create(const apic_config1d* cfg, apic_sim1d** out);
+APIC_EXPORT void apic_sim1d_destroy(apic_sim1d* sim);
+APIC_EXPORT const char* apic_sim1d_last_error(const apic_sim1d* sim);
+
+/* Species::particles() mutation (include/pic/Species.hpp:18): replaces the
+ * species' particles.  vy/vz may be NULL for 1D1V; v_half may be NULL
+ * (then v_half = v, as the external-state loader does, src/Simulation.cpp:751-752);
+ * alive may be NULL (all alive).  Dead entries are dropped. */
+APIC_EXPORT int apic_sim1d_load_particles(apic_sim1d* sim, int species, size_t n,
+                              const double* x, const double* v, const double* v_half,
+                              const double* vy, const double* vz, const uint8_t* alive);
+
+/* Simulation::initialize() after loaded particles, src/Simulation.cpp:698-769:
+ * deposit_and_solve(0) then initialize_leapfrog_half_step for every particle. */
+APIC_EXPORT int apic_sim1d_initialize(apic_sim1d* sim);
+
+/* Restart from a state whose v_half is already set (the state after a
+ * reference step() or checkpoint, src/Simulation.cpp:2018-2899): sets
+ * time/step and runs deposit_and_solve(time). */
+APIC_EXPORT int apic_sim1d_resume(apic_sim1d* sim, double time, uint64_t step);
+
+/* Simulation::step() repeated nsteps times, src/Simulation.cpp:1008-1138.
+ * Asynchronous: returns after enqueueing; errors surface at the next
+ * synchronising call. */
+APIC_EXPORT int apic_sim1d_step(apic_sim1d* sim, size_t nsteps);
+
+/* Waits (bounded) for the handle's stream and returns the device error word. */
+APIC_EXPORT int apic_sim1d_synchronize(apic_sim1d* sim);
+
+/* Species::particles() read access.  Brings the state to the reference's
+ * post-step() form (time-centred v) before copying. */
+APIC_EXPORT int apic_sim1d_count(apic_sim1d* sim, int species, size_t* n);
+APIC_EXPORT int apic_sim1d_read_particles(apic_sim1d* sim, int species, size_t capacity,
+                              double* x, double* v, double* v_half,
+                              double* vy, double* vz, size_t* n);
+/* Grid::rho()/phi()/electric(), include/pic/Grid.hpp:15-20 */
+APIC_EXPORT int apic_sim1d_read_fields(apic_sim1d* sim, double* rho, double* phi, double* electric);
+/* Simulation::sample(), src/Simulation.cpp:1140-1161 */
+APIC_EXPORT int apic_sim1d_sample(apic_sim1d* sim, apic_sample1d* out);
+/* Simulation::collision_diagnostics(), include/pic/Simulation.hpp:70-72 */
+APIC_EXPORT int apic_sim1d_collision_totals(apic_sim1d* sim, apic_collision_totals* out);
+/* Simulation::species_boundary_losses(), include/pic/Simulation.hpp:73-76 */
+APIC_EXPORT int apic_sim1d_boundary_losses(apic_sim1d* sim, int species, apic_boundary_loss* out);
+APIC_EXPORT double apic_sim1d_time(const apic_sim1d* sim);
+APIC_EXPORT uint64_t apic_sim1d_step_count(const apic_sim1d* sim);
+
+/* ---- stateless kernels (host buffers in, host buffers out) --------------- */
+
+/* Species::deposit_charge(Grid&) summed over species + FieldSolver::solve(Grid&,
+ * phi_left, phi_right) + interpolate_electric(Grid&, x) at nq query points
+ * (src/Species.cpp:161-185, src/FieldSolver.cpp:384-387, :407-440, :733-759,
+ * :909-924).  xs[s] holds counts[s] positions of species s. */
+APIC_EXPORT int apic_deposit_solve_gather_1d(int boundary, size_t nx, double length, double permittivity,
+                                 double phi_left, double phi_right, int nspecies,
+                                 const double* charge, const double* weight,
+                                 const size_t* counts, const double* const* xs,
+                                 double* rho, double* phi, double* electric,
+                                 size_t nq, const double* xq, double* eq);
+
+/* NullCollisionModel::collide(Vec3&, dt, rng), src/Collision.cpp:907-993, on n
+ * particles in parallel.  Draw source: when draws != NULL, particle i consumes
+ * the recorded raw 64-bit values draws[offsets[i] .. offsets[i+1]) (replay of
+ * a std::mt19937_64 stream, including libstdc++'s distribution transforms);
+ * otherwise a Philox4x32-10 stream keyed on (seed, i, step, stream).
+ * v3 is updated in place (3 doubles per particle). */
+APIC_EXPORT int apic_collide3(const apic_mcc_model* model, double particle_mass, size_t n, double* v3,
+                  double dt, const uint64_t* draws, const uint64_t* offsets,
+                  uint64_t seed, uint64_t step, uint32_t stream, apic_collide_stats* stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AURORAPIC_B200_H */

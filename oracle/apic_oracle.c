@@ -1,0 +1,810 @@
+/* Test infrastructure only: the CPU oracle (a plain-C restatement of the
+ * reference's electrostatic PIC particle step).  Each function cites the
+ * reference file:line it restates.  Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg load this library, as the checker.
+ *
+ * Pinned against golden vectors produced by the reference library itself
+ * (tests/golden/make_golden.py drives oracle/_ref/libapic_ref.so). */
+#include "apic_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+static char g_err[256];
+const char* ora_last_error(void) { return g_err; }
+static int seterr(int code, const char* msg) {
+    snprintf(g_err, sizeof g_err, "%s", msg);
+    return code;
+}
+
+/* ======================================================================= */
+/* mt19937_64: Matsumoto & Nishimura's 64-bit Mersenne Twister as specified
+ * by ISO C++ [rand.predef] (the reference's engine, include/pic/Simulation.hpp:177). */
+void ora_mt64_seed(ora_mt64* g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (int i = 1; i < 312; ++i)
+        g->mt[i] = 6364136223846793005ULL * (g->mt[i - 1] ^ (g->mt[i - 1] >> 62)) + (uint64_t)i;
+    g->mti = 312;
+}
+
+uint64_t ora_mt64_next(ora_mt64* g) {
+    static const uint64_t mag[2] = {0ULL, 0xB5026F5AA96619E9ULL};
+    const uint64_t upper = 0xFFFFFFFF80000000ULL, lower = 0x7FFFFFFFULL;
+    if (g->mti >= 312) {
+        int i;
+        for (i = 0; i < 312 - 156; ++i) {
+            uint64_t x = (g->mt[i] & upper) | (g->mt[i + 1] & lower);
+            g->mt[i] = g->mt[i + 156] ^ (x >> 1) ^ mag[x & 1ULL];
+        }
+        for (; i < 311; ++i) {
+            uint64_t x = (g->mt[i] & upper) | (g->mt[i + 1] & lower);
+            g->mt[i] = g->mt[i + (156 - 312)] ^ (x >> 1) ^ mag[x & 1ULL];
+        }
+        uint64_t x = (g->mt[311] & upper) | (g->mt[0] & lower);
+        g->mt[311] = g->mt[155] ^ (x >> 1) ^ mag[x & 1ULL];
+        g->mti = 0;
+    }
+    uint64_t y = g->mt[g->mti++];
+    y ^= (y >> 29) & 0x5555555555555555ULL;
+    y ^= (y << 17) & 0x71D67FFFEDA60000ULL;
+    y ^= (y << 37) & 0xFFF7EEE000000000ULL;
+    y ^= y >> 43;
+    return y;
+}
+
+/* Philox4x32-10 (Salmon, Moraes, Dror & Shaw, SC'11): the device's
+ * counter-based stream.  The same function runs in the CUDA kernels. */
+void ora_philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4]) {
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int round = 0; round < 10; ++round) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+uint64_t ora_draw(ora_rng* r) {
+    const uint64_t k = r->index++;
+    switch (r->kind) {
+        case ORA_SRC_MT64: return ora_mt64_next(r->mt);
+        case ORA_SRC_PHILOX: {
+            const uint32_t ctr[4] = {(uint32_t)(k >> 1), r->ctr[0], r->ctr[1], r->ctr[2]};
+            uint32_t out[4];
+            ora_philox4x32_10(ctr, r->key, out);
+            return (k & 1) ? ((uint64_t)out[3] << 32 | out[2]) : ((uint64_t)out[1] << 32 | out[0]);
+        }
+        default:
+            if (k >= r->array_len) { r->overrun = 1; return 0; }
+            return r->array[k];
+    }
+}
+
+/* libstdc++ generate_canonical<double, b> on a 64-bit engine (<bits/random.tcc>):
+ * one draw, sum / 2^64, values that round to 1 become nextafter(1, 0).  Used for
+ * uniform_real_distribution (src/Collision.cpp:46-51) and the channel
+ * selection generate_canonical<double, 64> (src/Collision.cpp:948). */
+double ora_canonical(ora_rng* r) {
+    const double sum = (double)ora_draw(r);
+    double ret = sum / 18446744073709551616.0;
+    if (ret >= 1.0) ret = nextafter(1.0, 0.0);
+    return ret;
+}
+
+double ora_uniform01(ora_rng* r) { return ora_canonical(r) * (1.0 - 0.0) + 0.0; }
+
+/* uniform_int_distribution<int>(0, 1) on a 64-bit engine: Lemire's
+ * nearly-divisionless reduction (ACM TOMACS 29(1), 2019) with range 2, whose
+ * rejection threshold is 0, so it is the draw's top bit (src/Collision.cpp:745). */
+int ora_bit(ora_rng* r) { return (int)(ora_draw(r) >> 63); }
+
+/* normal_distribution: Marsaglia's polar method with one saved value, as in
+ * libstdc++ (<bits/random.tcc>, normal_distribution::operator()). */
+double ora_normal_draw(ora_normal* st, ora_rng* r, double mean, double stddev) {
+    double ret;
+    if (st->saved_available) {
+        st->saved_available = 0;
+        ret = st->saved;
+    } else {
+        double x, y, r2;
+        do {
+            x = 2.0 * ora_canonical(r) - 1.0;
+            y = 2.0 * ora_canonical(r) - 1.0;
+            r2 = x * x + y * y;
+        } while (r2 > 1.0 || r2 == 0.0);
+        const double mult = sqrt(-2 * log(r2) / r2);
+        st->saved = x * mult;
+        st->saved_available = 1;
+        ret = y * mult;
+    }
+    return ret * stddev + mean;
+}
+
+/* ======================================================================= */
+/* MCC: NullCollisionModel (src/Collision.cpp). */
+
+static const double kBoltzmann = 1.380649e-23; /* src/Collision.cpp:16 */
+static const double kThermalSigma = 8.0;       /* include/pic/Collision.hpp:139 */
+static const double kEpsilon = 2.220446049250313080847e-16;
+
+/* CrossSectionTable::evaluate, src/Collision.cpp:221-237 (clamped ends,
+ * upper_bound, linear interpolation). */
+static double table_eval(const ora_channel* ch, double energy) {
+    const double* e = ch->energy;
+    const size_t n = ch->rows;
+    if (energy <= e[0]) return ch->sigma[0];
+    if (energy >= e[n - 1]) return ch->sigma[n - 1];
+    size_t lo = 0, hi = n; /* first index with e[i] > energy */
+    while (lo < hi) {
+        size_t mid = lo + (hi - lo) / 2;
+        if (e[mid] > energy) hi = mid; else lo = mid + 1;
+    }
+    const size_t high = lo, low = high - 1;
+    const double fraction = (energy - e[low]) / (e[high] - e[low]);
+    return ch->sigma[low] + fraction * (ch->sigma[high] - ch->sigma[low]);
+}
+
+int ora_collider_init(ora_collider* c, const ora_mcc_model* m, double particle_mass) {
+    memset(c, 0, sizeof *c);
+    c->m = *m;
+    c->particle_mass = particle_mass;
+    /* src/Collision.cpp:348-362: thermal neutrals only with SI gas data */
+    if (m->si && m->neutral_temperature > 0.0) {
+        c->neutral_stddev = sqrt(kBoltzmann * m->neutral_temperature / m->neutral_mass);
+    }
+    if (!(m->max_frequency > 0.0) || m->max_candidates == 0 || m->nch <= 0)
+        return seterr(4, "invalid MCC model");
+    return 0;
+}
+
+/* collision_energy, src/Collision.cpp:579-594 */
+static double collision_energy(const ora_collider* c, const ora_channel* ch, double rel_speed) {
+    double energy_mass = c->particle_mass;
+    if (ch->energy_frame == ORA_FRAME_CENTER_OF_MASS)
+        energy_mass = c->particle_mass * c->m.neutral_mass / (c->particle_mass + c->m.neutral_mass);
+    return 0.5 * energy_mass * rel_speed * rel_speed;
+}
+
+/* rates_for_speed, src/Collision.cpp:596-625 */
+static int rates_for_speed(const ora_collider* c, double speed, double* rates) {
+    double total = 0.0;
+    for (int i = 0; i < c->m.nch; ++i) {
+        const ora_channel* ch = &c->m.ch[i];
+        const double energy = collision_energy(c, ch, speed);
+        double rate = 0.0;
+        if (energy >= ch->threshold_energy)
+            rate = c->m.neutral_density * table_eval(ch, energy) * speed;
+        rates[i] = rate;
+        total += rate;
+    }
+    const double mx = c->m.max_frequency > total ? c->m.max_frequency : total;
+    const double tolerance = 64.0 * kEpsilon * mx;
+    if (total > c->m.max_frequency + tolerance)
+        return seterr(1, "MCC total collision frequency exceeds configured max_frequency");
+    return 0;
+}
+
+/* validate_frequency_bound, src/Collision.cpp:627-685 */
+static int validate_bound(const ora_collider* c, double projectile_speed) {
+    double rates[ORA_MAX_CHANNELS];
+    if (c->neutral_stddev == 0.0) return rates_for_speed(c, projectile_speed, rates);
+    const double limit = kThermalSigma * c->neutral_stddev;
+    const double max_rel = projectile_speed + limit;
+    double bound = 0.0;
+    for (int i = 0; i < c->m.nch; ++i) {
+        const ora_channel* ch = &c->m.ch[i];
+        const double max_e = collision_energy(c, ch, max_rel);
+        if (max_e < ch->threshold_energy) continue;
+        const double min_rel = projectile_speed - limit > 0.0 ? projectile_speed - limit : 0.0;
+        double min_e = collision_energy(c, ch, min_rel);
+        if (ch->threshold_energy > min_e) min_e = ch->threshold_energy;
+        double smax = table_eval(ch, min_e);
+        const double s2 = table_eval(ch, max_e);
+        if (s2 > smax) smax = s2;
+        for (size_t k = 0; k < ch->rows; ++k) {
+            const double e = ch->energy[k];
+            if (e >= min_e && e <= max_e && ch->sigma[k] > smax) smax = ch->sigma[k];
+        }
+        bound += c->m.neutral_density * smax * max_rel;
+    }
+    const double mx = c->m.max_frequency > bound ? c->m.max_frequency : bound;
+    if (bound > c->m.max_frequency + 64.0 * kEpsilon * mx)
+        return seterr(3, "MCC thermal-neutral collision-frequency bound exceeds configured max_frequency");
+    return 0;
+}
+
+/* open_unit_interval, src/Collision.cpp:46-51 */
+static double open_unit(ora_rng* r) {
+    double value = ora_uniform01(r);
+    while (!(value > 0.0)) value = ora_uniform01(r);
+    return value;
+}
+
+/* isotropic_velocity, src/Collision.cpp:53-64 */
+static void isotropic(double speed, ora_rng* r, double out[3]) {
+    const double cosine = 2.0 * ora_uniform01(r) - 1.0;
+    const double t = 1.0 - cosine * cosine;
+    const double sine = sqrt(0.0 > t ? 0.0 : t);
+    const double azimuth = 2.0 * acos(-1.0) * ora_uniform01(r);
+    out[0] = speed * sine * cos(azimuth);
+    out[1] = speed * sine * sin(azimuth);
+    out[2] = speed * cosine;
+}
+
+static double norm3(const double v[3]) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+/* sample_neutral_velocity_3v, src/Collision.cpp:702-715 (a fresh normal
+ * distribution object per call, bounded at 8 sigma) */
+static int neutral_3v(const ora_collider* c, ora_rng* r, double out[3]) {
+    out[0] = out[1] = out[2] = 0.0;
+    if (c->neutral_stddev == 0.0) return 0;
+    ora_normal nd = {0, 0.0};
+    const double limit = kThermalSigma * c->neutral_stddev;
+    for (int attempt = 0; attempt < 1024; ++attempt) {
+        out[0] = ora_normal_draw(&nd, r, 0.0, c->neutral_stddev);
+        out[1] = ora_normal_draw(&nd, r, 0.0, c->neutral_stddev);
+        out[2] = ora_normal_draw(&nd, r, 0.0, c->neutral_stddev);
+        if (norm3(out) <= limit) return 0;
+    }
+    return seterr(6, "thermal-neutral 3V sampler exceeded its rejection limit");
+}
+
+/* apply_channel (3V), src/Collision.cpp:762-829; anisotropic tables are not
+ * part of this restatement (isotropic and backward only). */
+static void apply_channel3(const ora_collider* c, int idx, double v[3], const double vn[3], ora_rng* r) {
+    const ora_channel* ch = &c->m.ch[idx];
+    if (ch->process == ORA_ATTACHMENT) { v[0] = v[1] = v[2] = 0.0; return; }
+    if (ch->process == ORA_CHARGE_EXCHANGE) { v[0] = vn[0]; v[1] = vn[1]; v[2] = vn[2]; return; }
+    const double rel[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+    const double initial_speed = norm3(rel);
+    double energy = 0.5 * c->particle_mass * initial_speed * initial_speed;
+    if (ch->process == ORA_EXCITATION || ch->process == ORA_IONIZATION) {
+        const double e2 = energy - ch->threshold_energy;
+        energy = 0.0 > e2 ? 0.0 : e2;
+    }
+    if (ch->process == ORA_IONIZATION) energy *= 0.5;
+    const double speed = sqrt(2.0 * energy / c->particle_mass);
+    double sc[3];
+    if (ch->angular == ORA_BACKWARD) { sc[0] = -rel[0]; sc[1] = -rel[1]; sc[2] = -rel[2]; }
+    else isotropic(speed, r, sc);
+    if (ch->process == ORA_ELASTIC && c->m.neutral_mass > 0.0) {
+        const double total = c->particle_mass + c->m.neutral_mass;
+        const double rf = c->m.neutral_mass / total;
+        for (int d = 0; d < 3; ++d)
+            v[d] = (c->particle_mass * v[d] + c->m.neutral_mass * vn[d]) / total + rf * sc[d];
+    } else {
+        for (int d = 0; d < 3; ++d) v[d] = vn[d] + sc[d];
+    }
+}
+
+/* NullCollisionModel::collide(Vec3&), src/Collision.cpp:907-993 */
+int ora_collide3(const ora_collider* c, double v[3], double dt, ora_rng* r, ora_collide_stats* st) {
+    memset(st, 0, sizeof *st);
+    const uint64_t start = r->index;
+    if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2]))
+        return seterr(4, "MCC particle velocity must be finite");
+    double elapsed = 0.0;
+    int rc;
+    for (;;) {
+        if ((rc = validate_bound(c, norm3(v)))) return rc;
+        const double waiting = -log(open_unit(r)) / c->m.max_frequency;
+        if (!isfinite(waiting) || waiting >= dt - elapsed) break;
+        elapsed += waiting;
+        ++st->candidates;
+        if (st->candidates > c->m.max_candidates)
+            return seterr(2, "MCC candidate limit exceeded");
+        double vn[3];
+        if ((rc = neutral_3v(c, r, vn))) return rc;
+        const double rel[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+        double rates[ORA_MAX_CHANNELS];
+        if ((rc = rates_for_speed(c, norm3(rel), rates))) return rc;
+        const double selection = ora_canonical(r) * c->m.max_frequency;
+        double cumulative = 0.0;
+        int accepted = 0;
+        for (int ch = 0; ch < c->m.nch; ++ch) {
+            cumulative += rates[ch];
+            if (selection < cumulative) {
+                const double before = 0.5 * c->particle_mass * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                apply_channel3(c, ch, v, vn, r);
+                st->energy_change[ch] += 0.5 * c->particle_mass * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) - before;
+                if (c->m.ch[ch].process == ORA_IONIZATION) {
+                    const double rel2[3] = {v[0] - vn[0], v[1] - vn[1], v[2] - vn[2]};
+                    const double sspeed = norm3(rel2);
+                    double iso[3];
+                    isotropic(sspeed, r, iso);
+                    if (st->nsecondaries < 16) {
+                        const int k = st->nsecondaries;
+                        st->secondary_channel[k] = ch;
+                        for (int d = 0; d < 3; ++d) {
+                            st->secondary_velocity[k][d] = vn[d] + iso[d];
+                            st->secondary_ion_velocity[k][d] = vn[d];
+                        }
+                    }
+                    st->nsecondaries++;
+                }
+                ++st->channel_collisions[ch];
+                if (c->m.ch[ch].process == ORA_ATTACHMENT) st->removed = 1;
+                accepted = 1;
+                break;
+            }
+        }
+        if (!accepted) ++st->null_collisions;
+        if (st->removed) break;
+    }
+    st->draws = r->index - start;
+    if (r->overrun) return seterr(5, "recorded draw array overrun");
+    return 0;
+}
+
+/* ======================================================================= */
+/* 1D grid kernels. */
+
+/* wrap_periodic, src/FieldSolver.cpp:15-17 (also src/Simulation.cpp:1041-1046) */
+static double wrap(double x, double L) { return fmod(fmod(x, L) + L, L); }
+
+/* interpolate_electric(const Grid&), src/FieldSolver.cpp:909-924 */
+double ora_gather1d(const double* E, size_t nx, double length, double dx, int dirichlet, double x) {
+    if (!dirichlet) {
+        const double xp = wrap(x, length);
+        const double g = xp / dx;
+        const size_t i = (size_t)floor(g);
+        const double f = g - (double)i;
+        return E[i % nx] * (1.0 - f) + E[(i + 1) % nx] * f;
+    }
+    const double xp = x < 0.0 ? 0.0 : (x > length ? length : x);
+    const double g = xp / dx;
+    double fl = floor(g);
+    if ((double)(nx - 2) < fl) fl = (double)(nx - 2);
+    const size_t i = (size_t)fl;
+    const double f = g - (double)i;
+    return E[i] * (1.0 - f) + E[i + 1] * f;
+}
+
+/* Grid::node_volume, src/Grid.cpp:26-30 */
+static double node_volume(size_t i, size_t nx, double dx, int dirichlet) {
+    if (!dirichlet) return dx;
+    return (i == 0 || i + 1 == nx) ? 0.5 * dx : dx;
+}
+
+/* Species::deposit_charge, src/Species.cpp:161-185 */
+void ora_deposit1d(double* rho, size_t nx, double length, double dx, int dirichlet,
+                   double charge, double weight, size_t n, const double* x, const uint8_t* alive) {
+    const double qwdx = charge * weight / dx;
+    for (size_t p = 0; p < n; ++p) {
+        if (alive && !alive[p]) continue;
+        if (!dirichlet) {
+            const double xp = wrap(x[p], length);
+            const double g = xp / dx;
+            const size_t i = (size_t)floor(g);
+            const double f = g - (double)i;
+            rho[i % nx] += qwdx * (1.0 - f);
+            rho[(i + 1) % nx] += qwdx * f;
+        } else {
+            const double xp = x[p] < 0.0 ? 0.0 : (x[p] > length ? length : x[p]);
+            const double g = xp / dx;
+            double fl = floor(g);
+            if ((double)(nx - 2) < fl) fl = (double)(nx - 2);
+            const size_t i = (size_t)fl;
+            const double f = g - (double)i;
+            rho[i] += charge * weight * (1.0 - f) / node_volume(i, nx, dx, 1);
+            rho[i + 1] += charge * weight * f / node_volume(i + 1, nx, dx, 1);
+        }
+    }
+}
+
+/* FieldSolver::solve_periodic_spectral(Grid&), src/FieldSolver.cpp:407-440:
+ * mean removal, a direct DFT per mode, phi_k = rho_k/(eps k^2), E_k = -i k phi_k. */
+static void solve_periodic(const double* rho, double* phi, double* E, size_t n, double L, double eps) {
+    const double twopi = 2.0 * 3.14159265358979323846;
+    double mean = 0.0;
+    for (size_t j = 0; j < n; ++j) mean += rho[j];
+    mean /= (double)n;
+    for (size_t j = 0; j < n; ++j) { phi[j] = 0.0; E[j] = 0.0; }
+    for (size_t k = 1; k < n; ++k) {
+        const double kk = (k <= n / 2) ? (double)k : -(double)(n - k);
+        const double wave = twopi * kk / L;
+        double re = 0.0, im = 0.0;
+        for (size_t j = 0; j < n; ++j) {
+            const double angle = -twopi * (double)(k * j) / (double)n;
+            const double a = rho[j] - mean;
+            /* complex += real * (cos, sin): libstdc++ real*complex is component-wise */
+            re += a * cos(angle);
+            im += a * sin(angle);
+        }
+        re /= (double)n;
+        im /= (double)n;
+        const double den = eps * wave * wave;
+        const double pr = re / den, pi = im / den;
+        /* Ek = -(0,1) * wave * phik = (wave*pi, -wave*pr) */
+        const double ekr = wave * pi, eki = -(wave * pr);
+        for (size_t j = 0; j < n; ++j) {
+            const double angle = twopi * (double)(k * j) / (double)n;
+            const double c = cos(angle), s = sin(angle);
+            phi[j] += pr * c - pi * s;
+            E[j] += ekr * c - eki * s;
+        }
+    }
+}
+
+/* FieldSolver::solve_dirichlet_tridiagonal, src/FieldSolver.cpp:733-759 */
+static void solve_dirichlet(const double* rho, double* phi, double* E, size_t n, double dx,
+                            double eps, double phil, double phir) {
+    const double dx2 = dx * dx;
+    phi[0] = phil;
+    phi[n - 1] = phir;
+    const size_t m = n - 2;
+    double* cp = (double*)calloc(m, sizeof(double));
+    double* dp = (double*)calloc(m, sizeof(double));
+    double* d = (double*)calloc(m, sizeof(double));
+    for (size_t i = 0; i < m; ++i) d[i] = rho[i + 1] * dx2 / eps;
+    d[0] += phil;
+    d[m - 1] += phir;
+    cp[0] = -1.0 / 2.0;
+    dp[0] = d[0] / 2.0;
+    for (size_t i = 1; i < m; ++i) {
+        const double denom = 2.0 + cp[i - 1];
+        cp[i] = (i == m - 1) ? 0.0 : -1.0 / denom;
+        dp[i] = (d[i] + dp[i - 1]) / denom;
+    }
+    phi[n - 2] = dp[m - 1];
+    for (size_t ii = m - 1; ii-- > 0;) phi[ii + 1] = dp[ii] - cp[ii] * phi[ii + 2];
+    for (size_t i = 1; i + 1 < n; ++i) E[i] = -(phi[i + 1] - phi[i - 1]) / (2.0 * dx);
+    E[0] = -(phi[1] - phi[0]) / dx;
+    E[n - 1] = -(phi[n - 1] - phi[n - 2]) / dx;
+    free(cp); free(dp); free(d);
+}
+
+void ora_solve1d(double* rho, double* phi, double* E, size_t nx, double length, double dx,
+                 int dirichlet, double eps, double phi_left, double phi_right) {
+    if (dirichlet) solve_dirichlet(rho, phi, E, nx, dx, eps, phi_left, phi_right);
+    else solve_periodic(rho, phi, E, nx, length, eps);
+}
+
+/* ======================================================================= */
+/* 1D simulation driver: Simulation::step / deposit_and_solve /
+ * apply_collisions (src/Simulation.cpp:678-1138). */
+
+typedef struct {
+    size_t n, cap;
+    double *x, *v, *vh, *vy, *vz;
+    uint8_t* alive;
+    uint64_t lost_left, lost_right;
+    double e_left, e_right;
+} ora_store;
+
+typedef struct {
+    double x, v[3];
+    int species;
+} ora_product;
+
+struct ora_sim1d {
+    ora_config1d cfg;
+    int mode;
+    uint64_t philox_seed;
+    double dx, eps, time;
+    uint64_t step;
+    double *rho, *phi, *E;
+    ora_store sp[ORA_MAX_SPECIES];
+    ora_collider col[ORA_MAX_MODELS];
+    ora_mt64 mt;
+    uint64_t candidates, nulls, per_channel[ORA_MAX_MODELS][ORA_MAX_CHANNELS];
+    ora_product* staged;
+    size_t nstaged, staged_cap;
+};
+
+static void store_reserve(ora_store* s, size_t cap) {
+    if (cap <= s->cap) return;
+    s->x = realloc(s->x, cap * sizeof(double));
+    s->v = realloc(s->v, cap * sizeof(double));
+    s->vh = realloc(s->vh, cap * sizeof(double));
+    s->vy = realloc(s->vy, cap * sizeof(double));
+    s->vz = realloc(s->vz, cap * sizeof(double));
+    s->alive = realloc(s->alive, cap);
+    s->cap = cap;
+}
+
+ora_sim1d* ora_sim1d_create(const ora_config1d* cfg, int mode, uint64_t philox_seed) {
+    ora_sim1d* s = calloc(1, sizeof *s);
+    s->cfg = *cfg;
+    s->mode = mode;
+    s->philox_seed = philox_seed;
+    s->dx = cfg->length / (double)(cfg->dirichlet ? cfg->nx - 1 : cfg->nx);
+    s->eps = cfg->si ? 8.8541878128e-12 : 1.0; /* include/pic/Types.hpp:7-8 */
+    s->rho = calloc(cfg->nx, sizeof(double));
+    s->phi = calloc(cfg->nx, sizeof(double));
+    s->E = calloc(cfg->nx, sizeof(double));
+    ora_mt64_seed(&s->mt, cfg->seed);
+    for (int m = 0; m < cfg->nmodels; ++m) {
+        const ora_mcc_model* mm = &cfg->models[m];
+        if (ora_collider_init(&s->col[m], mm, cfg->species[mm->species].mass)) {
+            ora_sim1d_destroy(s);
+            return NULL;
+        }
+    }
+    return s;
+}
+
+void ora_sim1d_destroy(ora_sim1d* s) {
+    if (!s) return;
+    for (int i = 0; i < ORA_MAX_SPECIES; ++i) {
+        free(s->sp[i].x); free(s->sp[i].v); free(s->sp[i].vh);
+        free(s->sp[i].vy); free(s->sp[i].vz); free(s->sp[i].alive);
+    }
+    free(s->rho); free(s->phi); free(s->E); free(s->staged);
+    free(s);
+}
+
+int ora_sim1d_load(ora_sim1d* s, int species, size_t n, const double* x, const double* v,
+                   const double* vh, const double* vy, const double* vz, const uint8_t* alive) {
+    ora_store* st = &s->sp[species];
+    store_reserve(st, n + 16);
+    st->n = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (s->mode == 1 && alive && !alive[i]) continue; /* device layout holds live particles only */
+        const size_t k = st->n++;
+        st->x[k] = x[i]; st->v[k] = v[i]; st->vh[k] = vh[i];
+        st->vy[k] = vy ? vy[i] : 0.0; st->vz[k] = vz ? vz[i] : 0.0;
+        st->alive[k] = alive ? alive[i] : 1;
+    }
+    return 0;
+}
+
+/* electrode_potential, src/Simulation.cpp:678-685 */
+static double electrode(double offset, const double drive[3], double t) {
+    return offset + drive[0] * sin(2.0 * 3.14159265358979323846 * drive[1] * t + drive[2]);
+}
+
+/* deposit_and_solve, src/Simulation.cpp:687-696 */
+static void deposit_and_solve(ora_sim1d* s, double field_time) {
+    const ora_config1d* c = &s->cfg;
+    memset(s->rho, 0, c->nx * sizeof(double));
+    for (int k = 0; k < c->nspecies; ++k)
+        ora_deposit1d(s->rho, c->nx, c->length, s->dx, c->dirichlet, c->species[k].charge,
+                      c->species[k].weight, s->sp[k].n, s->sp[k].x, s->sp[k].alive);
+    ora_solve1d(s->rho, s->phi, s->E, c->nx, c->length, s->dx, c->dirichlet, s->eps,
+                electrode(c->phi_left, c->drive_left, field_time),
+                electrode(c->phi_right, c->drive_right, field_time));
+}
+
+/* Simulation::initialize after the particles are loaded, src/Simulation.cpp:760-767 */
+int ora_sim1d_initialize(ora_sim1d* s) {
+    s->time = 0.0;
+    s->step = 0;
+    deposit_and_solve(s, 0.0);
+    for (int sid = 0; sid < s->cfg.nspecies; ++sid) {
+        ora_store* st = &s->sp[sid];
+        const double qm = s->cfg.species[sid].charge / s->cfg.species[sid].mass;
+        for (size_t i = 0; i < st->n; ++i)
+            if (st->alive[i])
+                st->vh[i] = st->v[i] - 0.5 * qm * ora_gather1d(s->E, s->cfg.nx, s->cfg.length, s->dx,
+                                                              s->cfg.dirichlet, st->x[i]) * s->cfg.dt;
+    }
+    return 0;
+}
+
+int ora_sim1d_initialize_fields(ora_sim1d* s, double time, uint64_t step) {
+    s->time = time;
+    s->step = step;
+    deposit_and_solve(s, time);
+    return 0;
+}
+
+static double gather(const ora_sim1d* s, double x) {
+    return ora_gather1d(s->E, s->cfg.nx, s->cfg.length, s->dx, s->cfg.dirichlet, x);
+}
+
+static int stage_product(ora_sim1d* s, int species, double x, const double v[3]) {
+    if (s->nstaged == s->staged_cap) {
+        s->staged_cap = s->staged_cap ? 2 * s->staged_cap : 64;
+        s->staged = realloc(s->staged, s->staged_cap * sizeof(ora_product));
+    }
+    ora_product* p = &s->staged[s->nstaged++];
+    p->x = x; p->species = species;
+    p->v[0] = v[0]; p->v[1] = v[1]; p->v[2] = v[2];
+    return 0;
+}
+
+/* initialize_leapfrog_half_step, src/Pusher.cpp:66-68 */
+static double init_half(double v, double E, double qm, double dt) { return v - 0.5 * qm * E * dt; }
+
+/* apply_collisions (named null-collision models), src/Simulation.cpp:835-1006 */
+static int apply_collisions(ora_sim1d* s) {
+    const ora_config1d* c = &s->cfg;
+    s->nstaged = 0;
+    for (int m = 0; m < c->nmodels; ++m) {
+        const int sid = c->models[m].species;
+        ora_store* st = &s->sp[sid];
+        const double qm = c->species[sid].charge / c->species[sid].mass;
+        const size_t initial = st->n;
+        for (size_t i = 0; i < initial; ++i) {
+            if (!st->alive[i]) continue;
+            ora_rng r;
+            memset(&r, 0, sizeof r);
+            if (s->mode == 0) { r.kind = ORA_SRC_MT64; r.mt = &s->mt; }
+            else {
+                r.kind = ORA_SRC_PHILOX;
+                r.key[0] = (uint32_t)s->philox_seed; r.key[1] = (uint32_t)(s->philox_seed >> 32);
+                r.ctr[0] = (uint32_t)i; r.ctr[1] = (uint32_t)s->step; r.ctr[2] = (uint32_t)sid;
+            }
+            ora_collide_stats cs;
+            int rc;
+            if (c->vdim == 3) {
+                double v[3] = {st->v[i], st->vy[i], st->vz[i]};
+                rc = ora_collide3(&s->col[m], v, c->dt, &r, &cs);
+                st->v[i] = v[0]; st->vy[i] = v[1]; st->vz[i] = v[2];
+            } else {
+                return seterr(7, "1V MCC is not part of this restatement");
+            }
+            if (rc) return rc;
+            s->candidates += cs.candidates;
+            s->nulls += cs.null_collisions;
+            for (int ch = 0; ch < c->models[m].nch; ++ch) s->per_channel[m][ch] += cs.channel_collisions[ch];
+            for (int k = 0; k < cs.nsecondaries && k < 16; ++k) {
+                const ora_channel* ch = &c->models[m].ch[cs.secondary_channel[k]];
+                stage_product(s, ch->secondary_species, st->x[i], cs.secondary_velocity[k]);
+                stage_product(s, ch->ion_species, st->x[i], cs.secondary_ion_velocity[k]);
+            }
+            if (cs.removed) return seterr(8, "1D MCC produced an unsupported primary removal event");
+            st->vh[i] = init_half(st->v[i], gather(s, st->x[i]), qm, c->dt);
+        }
+    }
+    /* capacity preflight, src/Simulation.cpp:929-965 */
+    size_t need[ORA_MAX_SPECIES] = {0};
+    for (size_t k = 0; k < s->nstaged; ++k) need[s->staged[k].species]++;
+    for (int sid = 0; sid < c->nspecies; ++sid) {
+        ora_store* st = &s->sp[sid];
+        size_t dead = 0;
+        for (size_t i = 0; i < st->n; ++i) dead += !st->alive[i];
+        const size_t cap = c->max_particles ? c->max_particles : 10000000;
+        if (need[sid] > cap - st->n + dead)
+            return seterr(9, "reactive collisions exceeded max_particles_per_species");
+    }
+    /* append_product, src/Simulation.cpp:966-1005 */
+    for (size_t k = 0; k < s->nstaged; ++k) {
+        const ora_product* p = &s->staged[k];
+        ora_store* st = &s->sp[p->species];
+        size_t slot = st->n;
+        if (s->mode == 0) {
+            for (size_t i = 0; i < st->n; ++i)
+                if (!st->alive[i]) { slot = i; break; }
+        }
+        if (slot == st->n) { store_reserve(st, st->n * 2 + 16); st->n++; }
+        const double qm = c->species[p->species].charge / c->species[p->species].mass;
+        st->x[slot] = p->x;
+        st->v[slot] = p->v[0]; st->vy[slot] = p->v[1]; st->vz[slot] = p->v[2];
+        st->alive[slot] = 1;
+        st->vh[slot] = init_half(st->v[slot], gather(s, p->x), qm, c->dt);
+    }
+    return 0;
+}
+
+/* Simulation::step, src/Simulation.cpp:1008-1138 */
+static int step_once(ora_sim1d* s) {
+    const ora_config1d* c = &s->cfg;
+    for (int sid = 0; sid < c->nspecies; ++sid) {
+        ora_store* st = &s->sp[sid];
+        const double qm = c->species[sid].charge / c->species[sid].mass;
+        const double mw = c->species[sid].mass * c->species[sid].weight;
+        size_t out = 0;
+        for (size_t i = 0; i < st->n; ++i) {
+            if (!st->alive[i]) { if (s->mode == 0) continue; else continue; }
+            /* kick_leapfrog + drift_leapfrog, src/Pusher.cpp:70-76 */
+            st->vh[i] += qm * gather(s, st->x[i]) * c->dt;
+            st->x[i] += st->vh[i] * c->dt;
+            if (!c->dirichlet) {
+                st->x[i] = wrap(st->x[i], c->length);
+            } else if (st->x[i] < 0.0 || st->x[i] > c->length) {
+                const double sp2 = st->vh[i] * st->vh[i] + st->vy[i] * st->vy[i] + st->vz[i] * st->vz[i];
+                const double e = 0.5 * c->species[sid].mass * c->species[sid].weight * sp2;
+                if (st->x[i] < 0.0) { st->lost_left++; st->e_left += e; }
+                else { st->lost_right++; st->e_right += e; }
+                st->alive[i] = 0;
+            }
+            (void)mw;
+            if (s->mode == 1 && st->alive[i]) {
+                /* device layout: survivors compacted in order */
+                st->x[out] = st->x[i]; st->v[out] = st->v[i]; st->vh[out] = st->vh[i];
+                st->vy[out] = st->vy[i]; st->vz[out] = st->vz[i]; st->alive[out] = 1;
+                ++out;
+            }
+        }
+        if (s->mode == 1) st->n = out;
+    }
+    deposit_and_solve(s, s->time + c->dt);
+    for (int sid = 0; sid < c->nspecies; ++sid) {
+        ora_store* st = &s->sp[sid];
+        const double qm = c->species[sid].charge / c->species[sid].mass;
+        for (size_t i = 0; i < st->n; ++i) {
+            if (!st->alive[i]) continue;
+            /* synchronize_leapfrog, src/Pusher.cpp:78-80 */
+            st->v[i] = st->vh[i] + 0.5 * qm * gather(s, st->x[i]) * c->dt;
+        }
+    }
+    const int rc = apply_collisions(s);
+    if (rc) return rc;
+    ++s->step;
+    s->time += c->dt;
+    return 0;
+}
+
+int ora_sim1d_step(ora_sim1d* s, size_t steps) {
+    for (size_t i = 0; i < steps; ++i) {
+        const int rc = step_once(s);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+size_t ora_sim1d_count(const ora_sim1d* s, int species) { return s->sp[species].n; }
+
+int ora_sim1d_get(const ora_sim1d* s, int species, double* x, double* v, double* vh,
+                  double* vy, double* vz, uint8_t* alive) {
+    const ora_store* st = &s->sp[species];
+    for (size_t i = 0; i < st->n; ++i) {
+        if (x) x[i] = st->x[i];
+        if (v) v[i] = st->v[i];
+        if (vh) vh[i] = st->vh[i];
+        if (vy) vy[i] = st->vy[i];
+        if (vz) vz[i] = st->vz[i];
+        if (alive) alive[i] = st->alive[i];
+    }
+    return 0;
+}
+
+void ora_sim1d_fields(const ora_sim1d* s, double* rho, double* phi, double* E) {
+    const size_t n = s->cfg.nx * sizeof(double);
+    if (rho) memcpy(rho, s->rho, n);
+    if (phi) memcpy(phi, s->phi, n);
+    if (E) memcpy(E, s->E, n);
+}
+
+double ora_sim1d_time(const ora_sim1d* s) { return s->time; }
+
+void ora_sim1d_set_mt(ora_sim1d* s, const uint64_t* state313) {
+    for (int i = 0; i < 312; ++i) s->mt.mt[i] = state313[i];
+    s->mt.mti = (int)state313[312];
+}
+
+void ora_sim1d_collisions(const ora_sim1d* s, uint64_t* candidates, uint64_t* nulls, uint64_t* per_channel) {
+    *candidates = s->candidates;
+    *nulls = s->nulls;
+    if (per_channel) memcpy(per_channel, s->per_channel, sizeof s->per_channel);
+}
+
+void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t* right,
+                      double* eleft, double* eright) {
+    const ora_store* st = &s->sp[species];
+    *left = st->lost_left; *right = st->lost_right; *eleft = st->e_left; *eright = st->e_right;
+}
+
+/* Species::kinetic_energy, src/Species.cpp:338-351 */
+double ora_sim1d_kinetic(const ora_sim1d* s, int species) {
+    const ora_store* st = &s->sp[species];
+    const ora_species* sc = &s->cfg.species[species];
+    double e = 0.0;
+    for (size_t i = 0; i < st->n; ++i) {
+        if (!st->alive[i]) continue;
+        double sq = st->v[i] * st->v[i];
+        if (s->cfg.vdim == 3) sq += st->vy[i] * st->vy[i] + st->vz[i] * st->vz[i];
+        e += 0.5 * sc->mass * sc->weight * sq;
+    }
+    return e;
+}
+
+/* Simulation::sample field energy, src/Simulation.cpp:1149-1155 */
+double ora_sim1d_field_energy(const ora_sim1d* s) {
+    double fe = 0.0;
+    for (size_t i = 0; i < s->cfg.nx; ++i)
+        fe += 0.5 * s->eps * s->E[i] * s->E[i] * node_volume(i, s->cfg.nx, s->dx, s->cfg.dirichlet);
+    return fe;
+}

@@ -1,0 +1,93 @@
+/* Test infrastructure only: the CPU oracle for the electrostatic PIC particle
+ * step.  A plain-C restatement of the reference's algorithm, used by tests/,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.
+ * The product never links or calls it.
+ *
+ * Parity pinning: every function below is checked against golden vectors that
+ * the reference library itself produced (tests/golden/make_golden.py, which
+ * drives oracle/_ref/libapic_ref.so built from the reference sources). */
+#ifndef APIC_ORACLE_H
+#define APIC_ORACLE_H
+#include "oracle_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- random numbers ----------------------------------------------------- */
+typedef struct { uint64_t mt[312]; int mti; } ora_mt64;
+void ora_mt64_seed(ora_mt64* g, uint64_t seed);
+uint64_t ora_mt64_next(ora_mt64* g);
+
+/* A stream of raw 64-bit draws: an mt19937_64 engine (reference mode), a
+ * Philox4x32-10 counter stream (device mode), or a recorded array (replay). */
+enum { ORA_SRC_MT64 = 0, ORA_SRC_PHILOX = 1, ORA_SRC_ARRAY = 2 };
+typedef struct {
+    int kind;
+    ora_mt64* mt;
+    uint32_t key[2];
+    uint32_t ctr[3];       /* particle slot, step, stream word */
+    uint64_t index;        /* draws consumed so far */
+    const uint64_t* array;
+    uint64_t array_len;
+    int overrun;
+} ora_rng;
+uint64_t ora_draw(ora_rng* r);
+void ora_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+double ora_canonical(ora_rng* r);           /* generate_canonical<double, 53|64> */
+double ora_uniform01(ora_rng* r);           /* uniform_real_distribution(0,1) */
+int ora_bit(ora_rng* r);                    /* uniform_int_distribution<int>(0,1) */
+typedef struct { int saved_available; double saved; } ora_normal;
+double ora_normal_draw(ora_normal* st, ora_rng* r, double mean, double stddev);
+
+/* ---- MCC (NullCollisionModel) ------------------------------------------- */
+typedef struct {
+    ora_mcc_model m;
+    double particle_mass;
+    double neutral_stddev;
+} ora_collider;
+/* returns 0, or an error code: 1 rate above max_frequency, 2 candidate cap,
+ * 3 thermal bound above max_frequency, 4 invalid input, 5 draw array overrun */
+int ora_collider_init(ora_collider* c, const ora_mcc_model* m, double particle_mass);
+int ora_collide3(const ora_collider* c, double v[3], double dt, ora_rng* r, ora_collide_stats* st);
+
+/* ---- 1D grid kernels ---------------------------------------------------- */
+double ora_gather1d(const double* E, size_t nx, double length, double dx, int dirichlet, double x);
+void ora_deposit1d(double* rho, size_t nx, double length, double dx, int dirichlet,
+                   double charge, double weight, size_t n, const double* x, const uint8_t* alive);
+void ora_solve1d(double* rho, double* phi, double* E, size_t nx, double length, double dx,
+                 int dirichlet, double eps, double phi_left, double phi_right);
+
+/* ---- 1D simulation ------------------------------------------------------ */
+typedef struct ora_sim1d ora_sim1d;
+/* mode 0: reference layout and one shared mt19937_64 stream (bit-exact with
+ *         the reference's Simulation);
+ * mode 1: device layout (survivors compacted in order, products appended in
+ *         parent order) and per-(seed, species, slot, step) Philox streams. */
+ora_sim1d* ora_sim1d_create(const ora_config1d* cfg, int mode, uint64_t philox_seed);
+void ora_sim1d_destroy(ora_sim1d* s);
+int ora_sim1d_load(ora_sim1d* s, int species, size_t n, const double* x, const double* v,
+                   const double* vh, const double* vy, const double* vz, const uint8_t* alive);
+int ora_sim1d_initialize_fields(ora_sim1d* s, double time, uint64_t step);
+int ora_sim1d_initialize(ora_sim1d* s);
+int ora_sim1d_step(ora_sim1d* s, size_t steps);
+size_t ora_sim1d_count(const ora_sim1d* s, int species);
+int ora_sim1d_get(const ora_sim1d* s, int species, double* x, double* v, double* vh,
+                  double* vy, double* vz, uint8_t* alive);
+void ora_sim1d_fields(const ora_sim1d* s, double* rho, double* phi, double* E);
+double ora_sim1d_time(const ora_sim1d* s);
+/* engine state in std::mersenne_twister_engine's text order: 312 words, index */
+void ora_sim1d_set_mt(ora_sim1d* s, const uint64_t* state313);
+void ora_sim1d_collisions(const ora_sim1d* s, uint64_t* candidates, uint64_t* nulls,
+                          uint64_t* per_channel /* [nmodels][ORA_MAX_CHANNELS] */);
+void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t* right,
+                      double* eleft, double* eright);
+double ora_sim1d_kinetic(const ora_sim1d* s, int species);
+double ora_sim1d_field_energy(const ora_sim1d* s);
+const char* ora_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,403 @@
+"""Test infrastructure only: ctypes bindings to the CPU oracle.
+
+Two libraries sit behind this module:
+
+* ``build/libapic_oracle.so`` -- the plain-C restatement of the reference's
+  particle step (``apic_oracle.c``), always available once ``make oracle`` ran;
+* ``_ref/libapic_ref.so`` -- the reference's own library compiled from its
+  sources plus ``ref_harness.cpp``; present only where the reference tree was
+  available at build time (it then travels with the repository snapshot).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module.  The product (``aurora-pic_b200``) never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "build", "libapic_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libapic_ref.so")
+
+MAX_CHANNELS = 8
+MAX_SPECIES = 4
+MAX_MODELS = 4
+
+ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, CHARGE_EXCHANGE = range(5)
+
+
+class Channel(C.Structure):
+    _fields_ = [
+        ("process", C.c_int), ("angular", C.c_int), ("energy_frame", C.c_int),
+        ("threshold_energy", C.c_double),
+        ("secondary_species", C.c_int), ("ion_species", C.c_int),
+        ("rows", C.c_size_t),
+        ("energy", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)),
+    ]
+
+
+class MccModel(C.Structure):
+    _fields_ = [
+        ("species", C.c_int),
+        ("neutral_density", C.c_double), ("max_frequency", C.c_double),
+        ("neutral_mass", C.c_double), ("neutral_temperature", C.c_double),
+        ("si", C.c_int), ("max_candidates", C.c_size_t),
+        ("nch", C.c_int), ("ch", Channel * MAX_CHANNELS),
+    ]
+
+
+class SpeciesCfg(C.Structure):
+    _fields_ = [
+        ("charge", C.c_double), ("mass", C.c_double), ("weight", C.c_double),
+        ("particles", C.c_size_t), ("drift", C.c_double), ("thermal", C.c_double),
+        ("thermal_y", C.c_double), ("thermal_z", C.c_double),
+    ]
+
+
+class Config1D(C.Structure):
+    _fields_ = [
+        ("dirichlet", C.c_int), ("vdim", C.c_int), ("si", C.c_int),
+        ("nx", C.c_size_t), ("length", C.c_double), ("dt", C.c_double),
+        ("phi_left", C.c_double), ("phi_right", C.c_double),
+        ("drive_left", C.c_double * 3), ("drive_right", C.c_double * 3),
+        ("seed", C.c_uint), ("threads", C.c_int), ("max_particles", C.c_size_t),
+        ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
+        ("nmodels", C.c_int), ("models", MccModel * MAX_MODELS),
+    ]
+
+
+class CollideStats(C.Structure):
+    _fields_ = [
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64),
+        ("channel_collisions", C.c_uint64 * MAX_CHANNELS),
+        ("energy_change", C.c_double * MAX_CHANNELS),
+        ("nsecondaries", C.c_int),
+        ("secondary_channel", C.c_int * 16),
+        ("secondary_velocity", (C.c_double * 3) * 16),
+        ("secondary_ion_velocity", (C.c_double * 3) * 16),
+        ("removed", C.c_int),
+        ("draws", C.c_uint64),
+    ]
+
+
+class Rng(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int), ("mt", C.c_void_p), ("key", C.c_uint32 * 2),
+        ("ctr", C.c_uint32 * 3), ("index", C.c_uint64),
+        ("array", C.POINTER(C.c_uint64)), ("array_len", C.c_uint64), ("overrun", C.c_int),
+    ]
+
+
+def ensure_built() -> None:
+    """Build the C restatement (and the reference harness when the reference
+    tree is present) with oracle/Makefile."""
+    targets = ["oracle"]
+    if os.path.isdir(os.environ.get("APIC_REFERENCE", "/root/reference")):
+        targets.append("ref")
+    if not os.path.exists(ORACLE_SO) or ("ref" in targets and not os.path.exists(REF_SO)):
+        subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+_DP = C.POINTER(C.c_double)
+_U8P = C.POINTER(C.c_uint8)
+_U64P = C.POINTER(C.c_uint64)
+
+
+def dptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_DP)
+
+
+def u8ptr(a: np.ndarray):
+    assert a.dtype == np.uint8 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_U8P)
+
+
+def u64ptr(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_U64P)
+
+
+_oracle = None
+_ref = None
+
+
+def oracle() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        ensure_built()
+        L = C.CDLL(ORACLE_SO)
+        L.ora_mt64_next.restype = C.c_uint64
+        L.ora_draw.restype = C.c_uint64
+        L.ora_canonical.restype = C.c_double
+        L.ora_uniform01.restype = C.c_double
+        L.ora_normal_draw.restype = C.c_double
+        L.ora_gather1d.restype = C.c_double
+        L.ora_gather1d.argtypes = [_DP, C.c_size_t, C.c_double, C.c_double, C.c_int, C.c_double]
+        L.ora_deposit1d.argtypes = [_DP, C.c_size_t, C.c_double, C.c_double, C.c_int, C.c_double,
+                                    C.c_double, C.c_size_t, _DP, _U8P]
+        L.ora_solve1d.argtypes = [_DP, _DP, _DP, C.c_size_t, C.c_double, C.c_double, C.c_int,
+                                  C.c_double, C.c_double, C.c_double]
+        L.ora_sim1d_create.restype = C.c_void_p
+        L.ora_sim1d_create.argtypes = [C.POINTER(Config1D), C.c_int, C.c_uint64]
+        L.ora_sim1d_destroy.argtypes = [C.c_void_p]
+        L.ora_sim1d_load.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _DP, _DP, _U8P]
+        L.ora_sim1d_initialize_fields.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
+        L.ora_sim1d_step.argtypes = [C.c_void_p, C.c_size_t]
+        L.ora_sim1d_initialize.argtypes = [C.c_void_p]
+        L.ora_sim1d_count.restype = C.c_size_t
+        L.ora_sim1d_count.argtypes = [C.c_void_p, C.c_int]
+        L.ora_sim1d_get.argtypes = [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _DP, _U8P]
+        L.ora_sim1d_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+        L.ora_sim1d_time.restype = C.c_double
+        L.ora_sim1d_time.argtypes = [C.c_void_p]
+        L.ora_sim1d_set_mt.argtypes = [C.c_void_p, _U64P]
+        L.ora_sim1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P]
+        L.ora_sim1d_losses.argtypes = [C.c_void_p, C.c_int, _U64P, _U64P, _DP, _DP]
+        L.ora_sim1d_kinetic.restype = C.c_double
+        L.ora_sim1d_kinetic.argtypes = [C.c_void_p, C.c_int]
+        L.ora_sim1d_field_energy.restype = C.c_double
+        L.ora_sim1d_field_energy.argtypes = [C.c_void_p]
+        L.ora_last_error.restype = C.c_char_p
+        L.ora_collider_init.argtypes = [C.c_void_p, C.POINTER(MccModel), C.c_double]
+        L.ora_collide3.argtypes = [C.c_void_p, _DP, C.c_double, C.POINTER(Rng), C.POINTER(CollideStats)]
+        _oracle = L
+    return _oracle
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        ensure_built()
+        L = C.CDLL(REF_SO)
+        L.ref_last_error.restype = C.c_char_p
+        L.ref1d_create.argtypes = [C.POINTER(Config1D), C.c_char_p, C.POINTER(C.c_void_p)]
+        L.ref1d_destroy.argtypes = [C.c_void_p]
+        L.ref1d_initialize.argtypes = [C.c_void_p]
+        L.ref1d_step.argtypes = [C.c_void_p, C.c_size_t]
+        L.ref1d_count.restype = C.c_size_t
+        L.ref1d_count.argtypes = [C.c_void_p, C.c_int]
+        L.ref1d_time.restype = C.c_double
+        L.ref1d_time.argtypes = [C.c_void_p]
+        L.ref1d_get_particles.argtypes = [C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _DP, _U8P]
+        L.ref1d_get_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+        L.ref1d_sample.argtypes = [C.c_void_p, _DP, _DP, C.POINTER(C.c_size_t)]
+        L.ref1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, C.c_size_t]
+        L.ref1d_losses.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _DP, _DP]
+        L.ref1d_rng_state.argtypes = [C.c_void_p, C.c_char_p, _U64P]
+        L.ref_deposit_solve_gather_1d.argtypes = [
+            C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
+            _DP, _DP, C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
+        L.ref_collide3.argtypes = [C.POINTER(MccModel), C.c_double, C.c_char_p, C.c_size_t, _DP, _U64P,
+                                   C.c_double, C.POINTER(CollideStats), _U64P, C.c_size_t]
+        L.ref_mt64.argtypes = [C.c_uint64, C.c_size_t, _U64P]
+        L.ref_dist.argtypes = [C.c_int, C.c_uint64, C.c_size_t, _DP]
+        _ref = L
+    return _ref
+
+
+# ---------------------------------------------------------------------------
+# Configuration builders shared by tests, smoke() and bench.py.
+
+class TableSet:
+    """Keeps the numpy arrays behind ctypes table pointers alive."""
+
+    def __init__(self):
+        self.keep = []
+
+    def channel(self, process, energy, sigma, threshold=0.0, secondary=-1, ion=-1,
+                angular=0, frame=0) -> Channel:
+        e = np.ascontiguousarray(energy, dtype=np.float64)
+        s = np.ascontiguousarray(sigma, dtype=np.float64)
+        self.keep += [e, s]
+        return Channel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+
+
+def make_model(species, channels, neutral_density, max_frequency, neutral_mass=0.0,
+               neutral_temperature=0.0, si=1, max_candidates=64) -> MccModel:
+    m = MccModel()
+    m.species = species
+    m.neutral_density = neutral_density
+    m.max_frequency = max_frequency
+    m.neutral_mass = neutral_mass
+    m.neutral_temperature = neutral_temperature
+    m.si = si
+    m.max_candidates = max_candidates
+    m.nch = len(channels)
+    for i, ch in enumerate(channels):
+        m.ch[i] = ch
+    return m
+
+
+def config1d(*, dirichlet, vdim, si, nx, length, dt, species, models=(), phi_left=0.0,
+             phi_right=0.0, drive_left=(0, 0, 0), drive_right=(0, 0, 0), seed=12345, threads=0,
+             max_particles=0) -> Config1D:
+    c = Config1D()
+    c.dirichlet, c.vdim, c.si, c.nx, c.length, c.dt = dirichlet, vdim, si, nx, length, dt
+    c.phi_left, c.phi_right = phi_left, phi_right
+    c.drive_left[:] = list(drive_left)
+    c.drive_right[:] = list(drive_right)
+    c.seed, c.threads, c.max_particles = seed, threads, max_particles
+    c.nspecies = len(species)
+    for i, sp in enumerate(species):
+        c.species[i] = SpeciesCfg(*sp)
+    c.nmodels = len(models)
+    for i, m in enumerate(models):
+        c.models[i] = m
+    return c
+
+
+class Sim1D:
+    """Oracle 1D simulation (mode 0 = reference layout and stream, mode 1 =
+    device layout with Philox streams)."""
+
+    def __init__(self, cfg: Config1D, mode: int, philox_seed: int = 0):
+        L = oracle()
+        self.cfg = cfg
+        self.h = L.ora_sim1d_create(C.byref(cfg), mode, philox_seed)
+        if not self.h:
+            raise RuntimeError(L.ora_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            oracle().ora_sim1d_destroy(self.h)
+            self.h = None
+
+    def load(self, s, x, v, vh, vy=None, vz=None, alive=None):
+        n = len(x)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else np.zeros(n)
+                for a in (x, v, vh, vy, vz)]
+        al = np.ones(n, np.uint8) if alive is None else np.ascontiguousarray(alive, dtype=np.uint8)
+        oracle().ora_sim1d_load(self.h, s, n, *[dptr(a) for a in arrs], u8ptr(al))
+
+    def initialize_fields(self, time=0.0, step=0):
+        oracle().ora_sim1d_initialize_fields(self.h, time, step)
+
+    def initialize(self):
+        oracle().ora_sim1d_initialize(self.h)
+
+    def set_mt(self, state):
+        st = np.ascontiguousarray(state, dtype=np.uint64)
+        oracle().ora_sim1d_set_mt(self.h, u64ptr(st))
+
+    def step(self, n=1):
+        rc = oracle().ora_sim1d_step(self.h, n)
+        if rc:
+            raise RuntimeError(oracle().ora_last_error().decode())
+
+    def particles(self, s):
+        L = oracle()
+        n = L.ora_sim1d_count(self.h, s)
+        out = {k: np.zeros(n) for k in ("x", "v", "vh", "vy", "vz")}
+        al = np.zeros(n, np.uint8)
+        L.ora_sim1d_get(self.h, s, *[dptr(out[k]) for k in ("x", "v", "vh", "vy", "vz")], u8ptr(al))
+        out["alive"] = al
+        return out
+
+    def fields(self):
+        n = self.cfg.nx
+        rho, phi, E = np.zeros(n), np.zeros(n), np.zeros(n)
+        oracle().ora_sim1d_fields(self.h, dptr(rho), dptr(phi), dptr(E))
+        return rho, phi, E
+
+    def collisions(self):
+        c, nl = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        per = np.zeros(MAX_MODELS * MAX_CHANNELS, np.uint64)
+        oracle().ora_sim1d_collisions(self.h, u64ptr(c), u64ptr(nl), u64ptr(per))
+        return int(c[0]), int(nl[0]), per.reshape(MAX_MODELS, MAX_CHANNELS)
+
+    def losses(self, s):
+        a, b = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        ea, eb = np.zeros(1), np.zeros(1)
+        oracle().ora_sim1d_losses(self.h, s, u64ptr(a), u64ptr(b), dptr(ea), dptr(eb))
+        return int(a[0]), int(b[0]), float(ea[0]), float(eb[0])
+
+    def kinetic(self, s):
+        return oracle().ora_sim1d_kinetic(self.h, s)
+
+    def field_energy(self):
+        return oracle().ora_sim1d_field_energy(self.h)
+
+    def time(self):
+        return oracle().ora_sim1d_time(self.h)
+
+
+class Ref1D:
+    """The reference's own Simulation, driven through the harness."""
+
+    def __init__(self, cfg: Config1D, workdir: str):
+        L = ref()
+        self.cfg = cfg
+        self.workdir = workdir
+        h = C.c_void_p()
+        if L.ref1d_create(C.byref(cfg), workdir.encode(), C.byref(h)):
+            raise RuntimeError(L.ref_last_error().decode())
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().ref1d_destroy(self.h)
+            self.h = None
+
+    def _chk(self, rc):
+        if rc:
+            raise RuntimeError(ref().ref_last_error().decode())
+
+    def initialize(self):
+        self._chk(ref().ref1d_initialize(self.h))
+
+    def step(self, n=1):
+        self._chk(ref().ref1d_step(self.h, n))
+
+    def particles(self, s):
+        L = ref()
+        n = L.ref1d_count(self.h, s)
+        out = {k: np.zeros(n) for k in ("x", "v", "vh", "vy", "vz")}
+        al = np.zeros(n, np.uint8)
+        self._chk(L.ref1d_get_particles(self.h, s, *[dptr(out[k]) for k in ("x", "v", "vh", "vy", "vz")],
+                                        u8ptr(al)))
+        out["alive"] = al
+        return out
+
+    def fields(self):
+        n = self.cfg.nx
+        rho, phi, E = np.zeros(n), np.zeros(n), np.zeros(n)
+        ref().ref1d_get_fields(self.h, dptr(rho), dptr(phi), dptr(E))
+        return rho, phi, E
+
+    def rng_state(self):
+        st = np.zeros(313, np.uint64)
+        path = os.path.join(self.workdir, "rng_probe.apc")
+        self._chk(ref().ref1d_rng_state(self.h, path.encode(), u64ptr(st)))
+        return st
+
+    def collisions(self):
+        c, nl = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        per = np.zeros(64, np.uint64)
+        k = ref().ref1d_collisions(self.h, u64ptr(c), u64ptr(nl), u64ptr(per), 64)
+        return int(c[0]), int(nl[0]), per[:k]
+
+    def losses(self, s):
+        a, b = C.c_size_t(), C.c_size_t()
+        ea, eb = np.zeros(1), np.zeros(1)
+        ref().ref1d_losses(self.h, s, C.byref(a), C.byref(b), dptr(ea), dptr(eb))
+        return a.value, b.value, float(ea[0]), float(eb[0])
+
+    def sample(self):
+        ns = self.cfg.nspecies
+        ke = np.zeros(ns)
+        fe = np.zeros(1)
+        live = (C.c_size_t * ns)()
+        self._chk(ref().ref1d_sample(self.h, dptr(ke), dptr(fe), live))
+        return ke, float(fe[0]), list(live)
+
+    def time(self):
+        return ref().ref1d_time(self.h)

@@ -1,0 +1,358 @@
+// Test infrastructure only: a C-ABI shim that drives the reference's own
+// classes (compiled from the reference sources by oracle/Makefile) so that the
+// tests can generate golden vectors from the real reference and bench.py can
+// time the reference's CPU step.  It restates no algorithm: every number it
+// returns is computed by the reference library.
+#include "oracle_types.h"
+
+#include "pic/Collision.hpp"
+#include "pic/Config.hpp"
+#include "pic/FieldSolver.hpp"
+#include "pic/Grid.hpp"
+#include "pic/Mesh2D.hpp"
+#include "pic/Mesh3D.hpp"
+#include "pic/Pusher.hpp"
+#include "pic/Simulation.hpp"
+#include "pic/Simulation2D.hpp"
+#include "pic/Simulation3D.hpp"
+#include "pic/Species.hpp"
+#include "pic/Swarm.hpp"
+
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <iomanip>
+#include <memory>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace {
+thread_local std::string g_error;
+
+int fail(const std::exception& e) {
+    g_error = e.what();
+    return 1;
+}
+
+std::string write_table(const std::string& dir, const std::string& stem,
+                        size_t rows, const double* e, const double* s) {
+    std::filesystem::create_directories(dir);
+    const std::string path = dir + "/" + stem + ".dat";
+    std::ofstream out(path);
+    out << std::setprecision(17);
+    for (size_t i = 0; i < rows; ++i) out << e[i] << ' ' << s[i] << '\n';
+    if (!out) throw std::runtime_error("cannot write table " + path);
+    return path;
+}
+
+pic::CollisionProcessKind process_of(int p) {
+    switch (p) {
+        case ORA_ELASTIC: return pic::CollisionProcessKind::Elastic;
+        case ORA_EXCITATION: return pic::CollisionProcessKind::Excitation;
+        case ORA_IONIZATION: return pic::CollisionProcessKind::Ionization;
+        case ORA_ATTACHMENT: return pic::CollisionProcessKind::Attachment;
+        case ORA_CHARGE_EXCHANGE: return pic::CollisionProcessKind::ChargeExchange;
+    }
+    throw std::invalid_argument("unknown process");
+}
+
+std::string species_name(int index) { return "s" + std::to_string(index); }
+
+pic::CollisionConfig collision_config(const ora_mcc_model& m, const std::string& dir,
+                                      const std::string& tag) {
+    pic::CollisionConfig c;
+    c.enabled = true;
+    c.model = pic::CollisionModelKind::NullCollision;
+    c.neutral_density = m.neutral_density;
+    c.max_frequency = m.max_frequency;
+    c.neutral_mass = m.neutral_mass;
+    c.neutral_temperature = m.neutral_temperature;
+    c.species = species_name(m.species);
+    c.max_candidates_per_particle = m.max_candidates;
+    c.gas_data_units = m.si ? pic::UnitSystem::SI : pic::UnitSystem::Normalized;
+    if (m.neutral_temperature > 0.0) c.gas_name = "synthetic";
+    for (int i = 0; i < m.nch; ++i) {
+        const ora_channel& ch = m.ch[i];
+        pic::CollisionChannelConfig cc;
+        cc.name = tag + "_ch" + std::to_string(i);
+        cc.process = process_of(ch.process);
+        cc.threshold_energy = ch.threshold_energy;
+        cc.angular_scattering = ch.angular == ORA_BACKWARD
+                                    ? pic::AngularScatteringKind::Backward
+                                    : pic::AngularScatteringKind::Isotropic;
+        cc.energy_frame = ch.energy_frame == ORA_FRAME_CENTER_OF_MASS
+                              ? pic::CollisionEnergyFrame::CenterOfMass
+                              : pic::CollisionEnergyFrame::Projectile;
+        cc.cross_section_file = write_table(dir, cc.name, ch.rows, ch.energy, ch.sigma);
+        if (ch.process == ORA_IONIZATION) {
+            cc.secondary_species = species_name(ch.secondary_species);
+            cc.ion_species = species_name(ch.ion_species);
+        } else if (ch.process == ORA_ATTACHMENT) {
+            cc.attachment_species = "attached";
+        }
+        c.channels.push_back(cc);
+    }
+    return c;
+}
+
+struct Ref1D {
+    std::unique_ptr<pic::Simulation> sim;
+};
+
+pic::Config make_config_1d(const ora_config1d& in, const std::string& dir) {
+    pic::Config c;
+    c.units.system = in.si ? pic::UnitSystem::SI : pic::UnitSystem::Normalized;
+    c.velocity_dimensions = static_cast<size_t>(in.vdim);
+    c.nx = in.nx;
+    c.length = in.length;
+    c.dt = in.dt;
+    c.boundary = in.dirichlet ? pic::Boundary::Dirichlet : pic::Boundary::Periodic;
+    c.phi_left = in.phi_left;
+    c.phi_right = in.phi_right;
+    c.phi_left_drive = {in.drive_left[0], in.drive_left[1], in.drive_left[2]};
+    c.phi_right_drive = {in.drive_right[0], in.drive_right[1], in.drive_right[2]};
+    c.seed = in.seed;
+    c.output_dir = dir + "/out";
+    if (in.max_particles) c.max_particles_per_species = in.max_particles;
+    if (in.threads > 0) {
+        c.runtime.backend = pic::RuntimeBackend::OpenMP;
+        c.runtime.threads = static_cast<size_t>(in.threads);
+    }
+    for (int s = 0; s < in.nspecies; ++s) {
+        const ora_species& sp = in.species[s];
+        pic::SpeciesConfig sc;
+        sc.name = species_name(s);
+        sc.charge = sp.charge;
+        sc.mass = sp.mass;
+        sc.weight = sp.weight;
+        sc.particles = sp.particles;
+        sc.drift_velocity = sp.drift;
+        sc.thermal_velocity = sp.thermal;
+        if (in.vdim == 3) {
+            sc.initialization.thermal_velocity_y = sp.thermal_y;
+            sc.initialization.thermal_velocity_z = sp.thermal_z;
+        }
+        c.species.push_back(sc);
+    }
+    for (int m = 0; m < in.nmodels; ++m) {
+        pic::NamedCollisionConfig named;
+        named.name = "model" + std::to_string(m);
+        named.config = collision_config(in.models[m], dir, named.name);
+        c.collision_models.push_back(named);
+    }
+    return c;
+}
+} // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_error.c_str(); }
+
+int ref1d_create(const ora_config1d* cfg, const char* workdir, void** out) {
+    try {
+        auto r = std::make_unique<Ref1D>();
+        r->sim = std::make_unique<pic::Simulation>(make_config_1d(*cfg, workdir));
+        *out = r.release();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+void ref1d_destroy(void* h) { delete static_cast<Ref1D*>(h); }
+
+int ref1d_initialize(void* h) {
+    try { static_cast<Ref1D*>(h)->sim->initialize(); return 0; }
+    catch (const std::exception& e) { return fail(e); }
+}
+
+int ref1d_step(void* h, size_t steps) {
+    try {
+        auto& sim = *static_cast<Ref1D*>(h)->sim;
+        for (size_t i = 0; i < steps; ++i) sim.step();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+size_t ref1d_count(void* h, int species) {
+    return static_cast<Ref1D*>(h)->sim->species().at(species).particles().size();
+}
+
+double ref1d_time(void* h) { return static_cast<Ref1D*>(h)->sim->time(); }
+
+int ref1d_get_particles(void* h, int species, double* x, double* v, double* vh,
+                        double* vy, double* vz, uint8_t* alive) {
+    try {
+        const auto& ps = static_cast<Ref1D*>(h)->sim->species().at(species).particles();
+        for (size_t i = 0; i < ps.size(); ++i) {
+            x[i] = ps[i].x; v[i] = ps[i].v; vh[i] = ps[i].v_half;
+            vy[i] = ps[i].velocity_y; vz[i] = ps[i].velocity_z;
+            alive[i] = ps[i].alive ? 1 : 0;
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+int ref1d_get_fields(void* h, double* rho, double* phi, double* e) {
+    const auto& g = static_cast<Ref1D*>(h)->sim->grid();
+    std::memcpy(rho, g.rho().data(), g.nx() * sizeof(double));
+    std::memcpy(phi, g.phi().data(), g.nx() * sizeof(double));
+    std::memcpy(e, g.electric().data(), g.nx() * sizeof(double));
+    return 0;
+}
+
+// kinetic energy per species, field energy, live counts
+int ref1d_sample(void* h, double* kinetic, double* field_energy, size_t* live) {
+    try {
+        auto& sim = *static_cast<Ref1D*>(h)->sim;
+        const auto& sp = sim.species();
+        for (size_t s = 0; s < sp.size(); ++s) {
+            kinetic[s] = sp[s].kinetic_energy();
+            live[s] = sp[s].live_count();
+        }
+        *field_energy = sim.sample().field_energy;
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+int ref1d_collisions(void* h, uint64_t* candidates, uint64_t* nulls, uint64_t* per_channel,
+                     size_t cap) {
+    const auto& d = static_cast<Ref1D*>(h)->sim->collision_diagnostics();
+    *candidates = d.candidates;
+    *nulls = d.null_collisions;
+    for (size_t i = 0; i < d.channel_collisions.size() && i < cap; ++i)
+        per_channel[i] = d.channel_collisions[i];
+    return static_cast<int>(d.channel_collisions.size());
+}
+
+int ref1d_losses(void* h, int species, size_t* left, size_t* right, double* eleft,
+                 double* eright) {
+    const auto& l = static_cast<Ref1D*>(h)->sim->species_boundary_losses().at(species);
+    *left = l.absorbed_left; *right = l.absorbed_right;
+    *eleft = l.kinetic_energy_left; *eright = l.kinetic_energy_right;
+    return 0;
+}
+
+// The engine state of Simulation's private rng_, read back through the
+// reference's own checkpoint writer (the "rng" line, src/Simulation.cpp:2004).
+int ref1d_rng_state(void* h, const char* path, uint64_t* out313) {
+    try {
+        static_cast<Ref1D*>(h)->sim->save_checkpoint(path);
+        std::ifstream in(path);
+        std::string line;
+        while (std::getline(in, line)) {
+            if (line.rfind("rng ", 0) == 0) {
+                std::istringstream row(line.substr(4));
+                for (int i = 0; i < 313; ++i) row >> out313[i];
+                return row ? 0 : 2;
+            }
+        }
+        return 3;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// --- kernel-level entry points --------------------------------------------
+
+// Species::deposit_charge + FieldSolver::solve + interpolate_electric on one grid.
+int ref_deposit_solve_gather_1d(int dirichlet, size_t nx, double length, double eps,
+                                double phi_left, double phi_right,
+                                int nspecies, const double* charge, const double* weight,
+                                const size_t* counts, const double* const* xs,
+                                double* rho, double* phi, double* e,
+                                size_t nq, const double* xq, double* eq) {
+    try {
+        pic::Grid grid(nx, length, dirichlet ? pic::Boundary::Dirichlet : pic::Boundary::Periodic);
+        grid.clear_charge();
+        for (int s = 0; s < nspecies; ++s) {
+            pic::SpeciesConfig sc;
+            sc.charge = charge[s];
+            sc.weight = weight[s];
+            sc.particles = counts[s];
+            pic::Species sp(sc, 1);
+            sp.particles().resize(counts[s]);
+            for (size_t i = 0; i < counts[s]; ++i) {
+                sp.particles()[i].x = xs[s][i];
+                sp.particles()[i].alive = true;
+            }
+            sp.deposit_charge(grid);
+        }
+        std::memcpy(rho, grid.rho().data(), nx * sizeof(double));
+        pic::FieldSolver solver(eps);
+        solver.solve(grid, phi_left, phi_right);
+        std::memcpy(phi, grid.phi().data(), nx * sizeof(double));
+        std::memcpy(e, grid.electric().data(), nx * sizeof(double));
+        for (size_t i = 0; i < nq; ++i) eq[i] = pic::interpolate_electric(grid, xq[i]);
+        return 0;
+    } catch (const std::exception& e2) { return fail(e2); }
+}
+
+// NullCollisionModel::collide(Vec3&) with one fresh std::mt19937_64(seed[i])
+// per particle.  Records the raw 64-bit draws each call consumed.
+int ref_collide3(const ora_mcc_model* model, double particle_mass, const char* workdir,
+                 size_t n, double* v, const uint64_t* seeds, double dt,
+                 ora_collide_stats* stats, uint64_t* draws, size_t draws_cap) {
+    try {
+        const pic::NullCollisionModel m(collision_config(*model, workdir, "collide"), particle_mass);
+        for (size_t i = 0; i < n; ++i) {
+            std::mt19937_64 rng(seeds[i]);
+            std::mt19937_64 shadow(seeds[i]);
+            pic::Vec3 vel{v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+            const auto st = m.collide(vel, dt, rng);
+            v[3 * i] = vel.x; v[3 * i + 1] = vel.y; v[3 * i + 2] = vel.z;
+            ora_collide_stats& o = stats[i];
+            std::memset(&o, 0, sizeof(o));
+            o.candidates = st.candidates;
+            o.null_collisions = st.null_collisions;
+            for (size_t c = 0; c < st.channel_collisions.size() && c < ORA_MAX_CHANNELS; ++c) {
+                o.channel_collisions[c] = st.channel_collisions[c];
+                o.energy_change[c] = st.channel_projectile_energy_change[c];
+            }
+            o.nsecondaries = static_cast<int>(st.secondaries.size());
+            for (size_t k = 0; k < st.secondaries.size() && k < 16; ++k) {
+                o.secondary_channel[k] = static_cast<int>(st.secondaries[k].channel);
+                o.secondary_velocity[k][0] = st.secondaries[k].velocity.x;
+                o.secondary_velocity[k][1] = st.secondaries[k].velocity.y;
+                o.secondary_velocity[k][2] = st.secondaries[k].velocity.z;
+                o.secondary_ion_velocity[k][0] = st.secondaries[k].ion_velocity.x;
+                o.secondary_ion_velocity[k][1] = st.secondaries[k].ion_velocity.y;
+                o.secondary_ion_velocity[k][2] = st.secondaries[k].ion_velocity.z;
+            }
+            o.removed = st.primary_removal_channel.has_value() ? 1 : 0;
+            uint64_t used = 0;
+            while (!(shadow == rng)) {
+                const uint64_t d = shadow();
+                if (draws && used < draws_cap) draws[i * draws_cap + used] = d;
+                ++used;
+                if (used > 1000000) throw std::runtime_error("draw count runaway");
+            }
+            o.draws = used;
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// Raw output of std::mt19937_64(seed): pins the oracle's engine.
+void ref_mt64(uint64_t seed, size_t n, uint64_t* out) {
+    std::mt19937_64 g(seed);
+    for (size_t i = 0; i < n; ++i) out[i] = g();
+}
+
+// libstdc++ transforms on a std::mt19937_64(seed) stream, for pinning the
+// oracle's restatement: kind 0 uniform_real(0,1), 1 normal(0,1) sequence on one
+// object, 2 uniform_int<int>(0,1), 3 generate_canonical<double,64>.
+void ref_dist(int kind, uint64_t seed, size_t n, double* out) {
+    std::mt19937_64 g(seed);
+    std::uniform_real_distribution<double> u(0.0, 1.0);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    std::uniform_int_distribution<int> b(0, 1);
+    for (size_t i = 0; i < n; ++i) {
+        switch (kind) {
+            case 0: out[i] = u(g); break;
+            case 1: out[i] = nd(g); break;
+            case 2: out[i] = b(g); break;
+            default: out[i] = std::generate_canonical<double, 64>(g); break;
+        }
+    }
+}
+
+} // extern "C"
