@@ -147,6 +147,9 @@ def lib() -> C.CDLL:
     L.apic_sim1d_time.argtypes = [C.c_void_p]
     L.apic_sim1d_step_count.restype = C.c_uint64
     L.apic_sim1d_step_count.argtypes = [C.c_void_p]
+    L.apic_sim1d_cuda_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.apic_sim1d_set_kernel_timing.argtypes = [C.c_void_p, C.c_int]
+    L.apic_sim1d_kernel_times.argtypes = [C.c_void_p, _DP, _DP, _U64P]
     L.apic_deposit_solve_gather_1d.argtypes = [
         C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _DP, _DP,
         C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
@@ -294,6 +297,20 @@ class Simulation1D:
         b = BoundaryLoss()
         _check(lib().apic_sim1d_boundary_losses(self.h, species, C.byref(b)), self.h)
         return b
+
+    def cuda_stream(self) -> int:
+        ptr = C.c_void_p()
+        _check(lib().apic_sim1d_cuda_stream(self.h, C.byref(ptr)), self.h)
+        return ptr.value or 0
+
+    def set_kernel_timing(self, enable: bool):
+        _check(lib().apic_sim1d_set_kernel_timing(self.h, int(enable)), self.h)
+
+    def kernel_times(self):
+        a, b = C.c_double(), C.c_double()
+        n = C.c_uint64()
+        _check(lib().apic_sim1d_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(n)), self.h)
+        return a.value, b.value, n.value
 
     @property
     def time(self) -> float:

@@ -67,6 +67,8 @@ class SpeciesSpec:
     v: np.ndarray
     vy: np.ndarray | None = None
     vz: np.ndarray | None = None
+    drift: float = 0.0     # Maxwellian parameters of the loading (for codes that load their own)
+    thermal: float = 0.0
 
 
 @dataclass
@@ -106,7 +108,7 @@ def two_stream(particles_per_beam=16384, nx=256, seed=1, steps=2000) -> Workload
         x = rx.uniform(0.0, L, particles_per_beam)
         x = np.mod(x + 1e-3 * np.cos(k * x), L)
         v = sign * 1.0 + 0.01 * rv.standard_normal(particles_per_beam)
-        sp.append(SpeciesSpec(-1.0, 1.0, w, particles_per_beam, x, v))
+        sp.append(SpeciesSpec(-1.0, 1.0, w, particles_per_beam, x, v, drift=sign * 1.0, thermal=0.01))
     return Workload1D("two_stream_1d1v", False, 1, False, nx, L, 0.1, sp, steps=steps)
 
 
@@ -158,7 +160,7 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
     for q, m, vt in ((-E_CHARGE, M_E, ve), (E_CHARGE, m_he, vi)):
         x = rng.uniform(0.0, L, n)
         v3 = vt * rng.standard_normal((3, n))
-        sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), v3[1].copy(), v3[2].copy()))
+        sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), v3[1].copy(), v3[2].copy(), thermal=vt))
     models = [
         ModelSpec(0, e_ch, ng, nu_e, m_he, T),
         ModelSpec(1, i_ch, ng, nu_i, m_he, T),

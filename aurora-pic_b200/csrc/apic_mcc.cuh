@@ -30,6 +30,15 @@ enum : unsigned {
     kErrBirths = 1u << 6,
 };
 
+// Bracket index of a table: bin b of a uniform grid in log2(energy) stores the
+// first row whose energy exceeds the bin's lower edge, so an upper_bound search
+// only has to look between the entries of the neighbouring bins.
+struct TableIndex {
+    const unsigned* first_gt;  // nbins + 1 entries
+    int nbins;
+    double lmin, inv_width;    // bin = floor((log2(E) - lmin) * inv_width)
+};
+
 struct MccChannelDev {
     int process, angular, frame;
     double threshold;
@@ -37,6 +46,7 @@ struct MccChannelDev {
     int rows;
     const double* energy;
     const double* sigma;
+    TableIndex index;
 };
 
 struct MccModelDev {
@@ -46,8 +56,36 @@ struct MccModelDev {
     double com_mass;      // particle_mass * neutral_mass / (particle_mass + neutral_mass)
     double v_safe;        // |v| <= v_safe passes the frequency-bound check without evaluation
     unsigned max_candidates;
+    int shared_grid;      // every channel uses the same energy rows and the projectile frame
     MccChannelDev ch[kMaxChannels];
 };
+
+// std::upper_bound(e, e + n, energy) for energy strictly inside the table.
+__device__ inline int upper_bound_indexed(const MccChannelDev& c, double energy) {
+    const TableIndex& ix = c.index;
+    int lo = 0, hi = c.rows;
+    if (ix.nbins > 0) {
+        const double t = (log2(energy) - ix.lmin) * ix.inv_width;
+        const int b = t < -1.0 ? -1 : (t > (double)ix.nbins ? ix.nbins : (int)floor(t));
+        lo = b >= 1 ? (int)__ldg(ix.first_gt + (b - 1)) : 0;
+        hi = b + 2 <= ix.nbins ? (int)__ldg(ix.first_gt + (b + 2)) : c.rows;
+    }
+    const double* e = c.energy;
+    while (lo < hi) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (__ldg(e + mid) > energy) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+// Interpolation of table c at energy with a known bracket (high = upper_bound).
+__device__ inline double table_at(const MccChannelDev& c, double energy, int high) {
+    const int low = high - 1;
+    const double el = __ldg(c.energy + low), eh = __ldg(c.energy + high);
+    const double sl = __ldg(c.sigma + low), sh = __ldg(c.sigma + high);
+    const double fraction = (energy - el) / (eh - el);
+    return sl + fraction * (sh - sl);
+}
 
 // CrossSectionTable::evaluate, src/Collision.cpp:221-237
 __device__ inline double table_eval(const MccChannelDev& c, double energy) {
@@ -55,16 +93,7 @@ __device__ inline double table_eval(const MccChannelDev& c, double energy) {
     const int n = c.rows;
     if (energy <= __ldg(e)) return __ldg(c.sigma);
     if (energy >= __ldg(e + n - 1)) return __ldg(c.sigma + n - 1);
-    int lo = 0, hi = n;  // first index with e[i] > energy (std::upper_bound)
-    while (lo < hi) {
-        const int mid = lo + ((hi - lo) >> 1);
-        if (__ldg(e + mid) > energy) hi = mid; else lo = mid + 1;
-    }
-    const int high = lo, low = high - 1;
-    const double el = __ldg(e + low), eh = __ldg(e + high);
-    const double sl = __ldg(c.sigma + low), sh = __ldg(c.sigma + high);
-    const double fraction = (energy - el) / (eh - el);
-    return sl + fraction * (sh - sl);
+    return table_at(c, energy, upper_bound_indexed(c, energy));
 }
 
 // collision_energy, src/Collision.cpp:579-594
@@ -77,6 +106,26 @@ __device__ inline double collision_energy(const MccModelDev& m, const MccChannel
 // exceeds max_frequency (+64 eps tolerance).
 __device__ inline bool rates_for_speed(const MccModelDev& m, double speed, double* rates) {
     double total = 0.0;
+    if (m.shared_grid) {
+        // one bracket search serves every channel (same rows, same energy)
+        const MccChannelDev& c0 = m.ch[0];
+        const double energy = 0.5 * m.particle_mass * speed * speed;
+        const int n = c0.rows;
+        const bool below = energy <= __ldg(c0.energy), above = energy >= __ldg(c0.energy + n - 1);
+        const int high = (below || above) ? 0 : upper_bound_indexed(c0, energy);
+        for (int i = 0; i < m.nch; ++i) {
+            const MccChannelDev& c = m.ch[i];
+            double rate = 0.0;
+            if (energy >= c.threshold) {
+                const double sg = below ? __ldg(c.sigma) : above ? __ldg(c.sigma + n - 1) : table_at(c, energy, high);
+                rate = m.neutral_density * sg * speed;
+            }
+            rates[i] = rate;
+            total += rate;
+        }
+        const double mx = m.max_frequency > total ? m.max_frequency : total;
+        return !(total > m.max_frequency + 64.0 * kDblEpsilon * mx);
+    }
     for (int i = 0; i < m.nch; ++i) {
         const MccChannelDev& c = m.ch[i];
         const double energy = collision_energy(m, c, speed);
@@ -108,10 +157,21 @@ __device__ inline bool frequency_bound_ok(const MccModelDev& m, double speed) {
         double smax = table_eval(c, min_e);
         const double s2 = table_eval(c, max_e);
         if (s2 > smax) smax = s2;
-        for (int k = 0; k < c.rows; ++k) {
-            const double e = __ldg(c.energy + k);
+        // rows with min_e <= energy <= max_e: [lower_bound(min_e), upper_bound(max_e))
+        const int n = c.rows;
+        int k0, k1;
+        if (min_e <= __ldg(c.energy)) k0 = 0;
+        else if (min_e > __ldg(c.energy + n - 1)) k0 = n;
+        else {
+            k0 = upper_bound_indexed(c, min_e);
+            if (__ldg(c.energy + k0 - 1) == min_e) --k0;  // lower_bound
+        }
+        if (max_e >= __ldg(c.energy + n - 1)) k1 = n;
+        else if (max_e < __ldg(c.energy)) k1 = 0;
+        else k1 = upper_bound_indexed(c, max_e);
+        for (int k = k0; k < k1; ++k) {
             const double s = __ldg(c.sigma + k);
-            if (e >= min_e && e <= max_e && s > smax) smax = s;
+            if (s > smax) smax = s;
         }
         bound += m.neutral_density * smax * max_rel;
     }

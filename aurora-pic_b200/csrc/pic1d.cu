@@ -67,9 +67,8 @@ enum : unsigned {
 };
 
 struct DevState {
-    unsigned n[kMaxSpecies];
-    unsigned ticket;
-    unsigned epoch;
+    unsigned n[kMaxSpecies];        // live particles (logical count)
+    unsigned nranges[kMaxSpecies];  // ranges of the current input layout
     unsigned nbirths;
     unsigned error;
     unsigned long long step;
@@ -92,7 +91,13 @@ struct SpeciesDev {
     double qm, hqm, qw, qwdx, mass, weight;
     int model;
     unsigned capacity;
-    unsigned long long* lookback;
+    // Layout: the live particles, in logical order, are the concatenation of
+    // ranges r = 0..nranges-1 of physical slots [start[r], start[r] + count[r]);
+    // lstart[r] is the logical index of a range's first particle.
+    unsigned* rstart[2];
+    unsigned* rcount[2];
+    unsigned* rlstart[2];
+    unsigned* chunk_surv;  // survivors of each 1024-particle chunk of a pass
     // [0] = input buffer of this pass, [1] = output buffer
     double* x[2];
     double* vh[2];
@@ -188,47 +193,18 @@ __device__ __forceinline__ void deposit_contrib(const Cic& c, const SpeciesDev& 
     }
 }
 
-// ---- decoupled look-back -------------------------------------------------
+// ---- range-table layout -----------------------------------------------------
 
-constexpr unsigned long long kLbValueMask = (1ull << 38) - 1;
-constexpr unsigned long long kLbAggregate = 1ull << 38;
-constexpr unsigned long long kLbInclusive = 2ull << 38;
-
-__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned long long flag,
-                                                       unsigned long long value) {
-    return ((unsigned long long)(epoch & 0xFFFFFFu) << 40) | flag | value;
-}
-
-// Returns the exclusive prefix of `tile` in its species chain.  Spins on
-// predecessors with an iteration bound; gives up with kErrTimeout.
-__device__ unsigned long long lookback(unsigned long long* lb, unsigned tile, unsigned count,
-                                       unsigned epoch, unsigned* error) {
-    if (tile == 0) {
-        atomicExch(lb, lb_word(epoch, kLbInclusive, count));
-        return 0;
+// Physical slot of logical particle `idx`: the range containing it is found by
+// binary search over the ranges' logical starts.
+__device__ __forceinline__ unsigned physical_slot(const unsigned* lstart, const unsigned* start, unsigned nr,
+                                                  unsigned idx) {
+    unsigned lo = 0, hi = nr;  // last range with lstart <= idx
+    while (hi - lo > 1) {
+        const unsigned mid = (lo + hi) >> 1;
+        if (__ldg(lstart + mid) <= idx) lo = mid; else hi = mid;
     }
-    atomicExch(lb + tile, lb_word(epoch, kLbAggregate, count));
-    unsigned long long excl = 0;
-    long long p = (long long)tile - 1;
-    const unsigned ep = epoch & 0xFFFFFFu;
-    while (p >= 0) {
-        unsigned long long w = 0;
-        unsigned spins = 0;
-        for (;;) {
-            w = *((volatile unsigned long long*)(lb + p));
-            if ((unsigned)(w >> 40) == ep && (w & (3ull << 38)) != 0) break;
-            if (++spins > (1u << 24)) {
-                atomicOr(error, kErrTimeout);
-                return 0;
-            }
-            if (spins > 64) __nanosleep(64);
-        }
-        excl += w & kLbValueMask;
-        if ((w & (3ull << 38)) == kLbInclusive) break;
-        --p;
-    }
-    atomicExch(lb + tile, lb_word(epoch, kLbInclusive, excl + count));
-    return excl;
+    return __ldg(start + lo) + (idx - __ldg(lstart + lo));
 }
 
 // ---- the fused particle pass -----------------------------------------------
@@ -238,9 +214,7 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
     unsigned long long* sRho = reinterpret_cast<unsigned long long*>(sE + p.nx);
-    __shared__ unsigned s_ticket;
     __shared__ unsigned s_cnt[kItems * (kThreads / 32)];
-    __shared__ unsigned long long s_base;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned mode = p.mode;
@@ -249,7 +223,6 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
         sRho[i] = 0ull;
     }
     DevState* st = p.st;
-    const unsigned epoch = st->epoch;
     unsigned tiles_before[kMaxSpecies + 1];
     tiles_before[0] = 0;
     for (int s = 0; s < kMaxSpecies; ++s)
@@ -257,16 +230,14 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
     const unsigned total_tiles = tiles_before[kMaxSpecies];
     __syncthreads();
 
-    for (;;) {
-        if (tid == 0) s_ticket = atomicAdd(&st->ticket, 1u);
-        __syncthreads();
-        const unsigned t = s_ticket;
-        if (t >= total_tiles) break;
+    // chunks of kTile logical particles, statically strided over the grid
+    for (unsigned t = blockIdx.x; t < total_tiles; t += gridDim.x) {
         int s = 0;
         while (t >= tiles_before[s + 1]) ++s;
         const unsigned tile = t - tiles_before[s];
         const SpeciesDev& S = p.sp[s];
         const unsigned n = st->n[s];
+        const unsigned nr = st->nranges[s];
         const unsigned base = tile * kTile;
 
         double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems];
@@ -276,12 +247,13 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
             const unsigned idx = base + k * kThreads + tid;
             const bool live = idx < n;
             keep[k] = live;
-            x[k] = live ? S.x[0][idx] : 0.0;
-            vh[k] = live ? S.vh[0][idx] : 0.0;
-            vy[k] = (VDIM == 3 && live) ? S.vy[0][idx] : 0.0;
-            vz[k] = (VDIM == 3 && live) ? S.vz[0][idx] : 0.0;
+            const unsigned ph = live ? physical_slot(S.rlstart[0], S.rstart[0], nr, idx) : 0u;
+            x[k] = live ? S.x[0][ph] : 0.0;
+            vh[k] = live ? S.vh[0][ph] : 0.0;
+            vy[k] = (VDIM == 3 && live) ? S.vy[0][ph] : 0.0;
+            vz[k] = (VDIM == 3 && live) ? S.vz[0][ph] : 0.0;
             vc[k] = 0.0;
-            if ((mode & kModeInitHalf) && live) vc[k] = S.v[idx];
+            if ((mode & kModeInitHalf) && live) vc[k] = S.v[ph];
         }
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
@@ -388,12 +360,11 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
             }
             s_cnt[lane] = incl - c;
             const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-            if (lane == 0) {
-                s_base = lookback(S.lookback, tile, total, epoch, &st->error);
-            }
+            if (lane == 0) S.chunk_surv[tile] = total;
         }
         __syncthreads();
-        const unsigned long long out_base = s_base;
+        // survivors of this chunk keep their order at the chunk's own slots
+        const unsigned long long out_base = base;
         const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
@@ -445,30 +416,51 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         typename ScanU::TempStorage scan;
         typename ScanA::TempStorage scana;
     } tmp;
-    __shared__ unsigned s_surv[kMaxSpecies], s_kept[kMaxSpecies];
+    __shared__ unsigned s_surv[kMaxSpecies], s_kept[kMaxSpecies], s_bstart[kMaxSpecies], s_nch[kMaxSpecies];
     __shared__ double s_red[kPostThreads / 32];
     __shared__ double s_mean;
+    __shared__ unsigned s_carry;
     DevState* st = p.st;
     const int tid = threadIdx.x;
-    const unsigned epoch = st->epoch;
 
-    if (tid < kMaxSpecies) {
-        unsigned surv = 0;
-        if (tid < p.nspecies) {
-            const unsigned n = st->n[tid];
-            const unsigned tiles = (n + kTile - 1) / kTile;
-            if (tiles) {
-                const unsigned long long w = *((volatile unsigned long long*)(p.sp[tid].lookback + tiles - 1));
-                if ((unsigned)(w >> 40) == (epoch & 0xFFFFFFu) && (w & (3ull << 38)) == kLbInclusive)
-                    surv = (unsigned)(w & kLbValueMask);
-                else
-                    atomicOr(&st->error, kErrTimeout);
+    // -- output range table: chunk c of the pass kept its survivors at slots
+    //    [c * kTile, c * kTile + surv_c); logical starts are their prefix sums --
+    for (int s = 0; s < p.nspecies; ++s) {
+        const SpeciesDev& S = p.sp[s];
+        const unsigned nch = (st->n[s] + kTile - 1) / kTile;
+        if (tid == 0) s_carry = 0;
+        __syncthreads();
+        for (unsigned b0 = 0; b0 < nch; b0 += kPostThreads * kPostItems) {
+            unsigned cnt[kPostItems], pre[kPostItems];
+#pragma unroll
+            for (int k = 0; k < kPostItems; ++k) {
+                const unsigned c = b0 + tid * kPostItems + k;
+                cnt[k] = c < nch ? S.chunk_surv[c] : 0u;
             }
+            unsigned total;
+            ScanU(tmp.scan).ExclusiveSum(cnt, pre, total);
+            const unsigned carry = s_carry;
+#pragma unroll
+            for (int k = 0; k < kPostItems; ++k) {
+                const unsigned c = b0 + tid * kPostItems + k;
+                if (c < nch) {
+                    S.rstart[1][c] = c * kTile;
+                    S.rcount[1][c] = cnt[k];
+                    S.rlstart[1][c] = carry + pre[k];
+                }
+            }
+            __syncthreads();
+            if (tid == 0) s_carry = carry + total;
+            __syncthreads();
         }
-        s_surv[tid] = surv;
-        s_kept[tid] = 0;
+        if (tid == 0) {
+            s_surv[s] = s_carry;
+            s_nch[s] = nch;
+            s_bstart[s] = nch ? (nch - 1) * kTile + S.chunk_surv[nch - 1] : 0u;
+            s_kept[s] = 0;
+        }
+        __syncthreads();
     }
-    __syncthreads();
 
     // -- ionization products, in (parent species, parent slot, product) order --
     unsigned nb = st->nbirths;
@@ -540,7 +532,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
 #pragma unroll
             for (int k = 0; k < kPostItems; ++k) {
                 if (!flags[k]) continue;
-                const unsigned long long o = (unsigned long long)s_surv[s] + ranks[k];
+                const unsigned long long o = (unsigned long long)s_bstart[s] + ranks[k];
                 if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
                 S.x[1][o] = bx[k];
                 S.vh[1][o] = bvh[k];
@@ -555,15 +547,23 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         __syncthreads();
     }
     if (tid < p.nspecies) {
-        unsigned long long n = (unsigned long long)s_surv[tid] + s_kept[tid];
-        if (n > p.sp[tid].capacity) { atomicOr(&st->error, kErrCapacity); n = p.sp[tid].capacity; }
-        st->n[tid] = (unsigned)n;
+        const SpeciesDev& S = p.sp[tid];
+        unsigned kept = s_kept[tid];
+        if ((unsigned long long)s_bstart[tid] + kept > S.capacity) {
+            atomicOr(&st->error, kErrCapacity);
+            kept = S.capacity > s_bstart[tid] ? S.capacity - s_bstart[tid] : 0u;
+        }
+        unsigned nr = s_nch[tid];
+        if (kept) {  // this pass's products form one more range after the last chunk
+            S.rstart[1][nr] = s_bstart[tid];
+            S.rcount[1][nr] = kept;
+            S.rlstart[1][nr] = s_surv[tid];
+            ++nr;
+        }
+        st->nranges[tid] = nr;
+        st->n[tid] = s_surv[tid] + kept;
     }
-    if (tid == 0) {
-        st->ticket = 0;
-        st->nbirths = 0;
-        st->epoch = epoch + 1;
-    }
+    if (tid == 0) st->nbirths = 0;
     if (!(post & kPostSolve)) return;
 
     // -- density: fixed point -> FP64 ---------------------------------------
@@ -707,6 +707,58 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         st->time = field_time;
         st->step = st->step + 1ull;
     }
+}
+
+// Simulation::sample reductions (src/Simulation.cpp:1140-1161,
+// src/Species.cpp:338-351): per-block partial sums, then the last block adds
+// the partials in block order, so the result does not depend on scheduling.
+constexpr int kSampleBlocks = 148;
+__global__ void __launch_bounds__(256) k_sample1d(Params1D p, double* partial, unsigned* done, double* out) {
+    __shared__ double red[8];
+    __shared__ bool last;
+    const int tid = threadIdx.x;
+    for (int s = 0; s < p.nspecies; ++s) {
+        const SpeciesDev& S = p.sp[s];
+        const unsigned n = p.st->n[s];
+        const double hmw = 0.5 * S.mass * S.weight;
+        double acc = 0.0;
+        for (unsigned i = blockIdx.x * 256 + tid; i < n; i += gridDim.x * 256) {
+            const double v = S.v[i];
+            double sq = v * v;
+            if (p.vdim == 3) sq += S.vy[0][i] * S.vy[0][i] + S.vz[0][i] * S.vz[0][i];
+            acc += hmw * sq;
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if ((tid & 31) == 0) red[tid >> 5] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double b = 0.0;
+            for (int w = 0; w < 8; ++w) b += red[w];
+            partial[s * gridDim.x + blockIdx.x] = b;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || tid != 0) return;
+    __threadfence();
+    for (int s = 0; s < p.nspecies; ++s) {
+        double e = 0.0;
+        for (unsigned b = 0; b < gridDim.x; ++b) e += ((volatile double*)partial)[s * gridDim.x + b];
+        out[s] = e;
+    }
+    double fe = 0.0, l1 = 0.0;
+    for (int i = 0; i < p.nx; ++i) {
+        const double vol = p.dirichlet ? ((i == 0 || i + 1 == p.nx) ? 0.5 * p.dx : p.dx) : p.dx;
+        fe += 0.5 * p.eps * p.E[i] * p.E[i] * vol;
+        l1 += fabs(p.rho[i]) * vol;
+    }
+    out[kMaxSpecies] = fe;
+    out[kMaxSpecies + 1] = l1;
+    *done = 0;
 }
 
 // interpolate_electric(Grid&, x) at query points, src/FieldSolver.cpp:909-924
@@ -911,6 +963,32 @@ struct Sim1D {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    // Bracket index over log2(energy) for a strictly increasing table.
+    TableIndex build_index(const double* e, size_t rows) {
+        TableIndex ix{};
+        size_t first_pos = 0;
+        while (first_pos < rows && !(e[first_pos] > 0.0)) ++first_pos;
+        if (first_pos + 1 >= rows) return ix;  // no usable positive range: plain binary search
+        const double lmin = std::log2(e[first_pos]);
+        const double lmax = std::log2(e[rows - 1]);
+        if (!(lmax > lmin)) return ix;
+        const int nbins = (int)std::min<size_t>(std::max<size_t>(rows, 256), 8192);
+        std::vector<unsigned> first(nbins + 1);
+        for (int b = 0; b <= nbins; ++b) {
+            const double edge = std::exp2(lmin + (lmax - lmin) * (double)b / (double)nbins);
+            first[b] = (unsigned)(std::upper_bound(e, e + rows, edge) - e);
+        }
+        first[nbins] = (unsigned)rows;
+        unsigned* d = dalloc<unsigned>(first.size());
+        APIC_CUDA(cudaMemcpyAsync(d, first.data(), first.size() * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        ix.first_gt = d;
+        ix.nbins = nbins;
+        ix.lmin = lmin;
+        ix.inv_width = (double)nbins / (lmax - lmin);
+        return ix;
+    }
+
     void create(const apic_config1d& c) {
         cfg = c;
         require(c.boundary == APIC_PERIODIC || c.boundary == APIC_DIRICHLET, "unknown boundary");
@@ -973,7 +1051,13 @@ struct Sim1D {
             S.model = -1;
             S.capacity = (unsigned)sp.capacity;
             const size_t cap = sp.capacity;
-            S.lookback = dalloc<unsigned long long>((cap + kTile - 1) / kTile + 1);
+            const size_t maxr = (cap + kTile - 1) / kTile + 2;
+            for (int b = 0; b < 2; ++b) {
+                S.rstart[b] = dalloc<unsigned>(maxr);
+                S.rcount[b] = dalloc<unsigned>(maxr);
+                S.rlstart[b] = dalloc<unsigned>(maxr);
+            }
+            S.chunk_surv = dalloc<unsigned>(maxr);
             for (int b = 0; b < 2; ++b) {
                 S.x[b] = dalloc<double>(cap);
                 S.vh[b] = dalloc<double>(cap);
@@ -1050,6 +1134,15 @@ struct Sim1D {
                 APIC_CUDA(cudaMemcpyAsync(s, ch.sigma, ch.rows * sizeof(double), cudaMemcpyHostToDevice, stream));
                 C.energy = e;
                 C.sigma = s;
+                C.index = build_index(ch.energy, ch.rows);
+            }
+            D.shared_grid = 1;
+            for (int ci = 0; ci < m.nch; ++ci) {
+                const apic_mcc_channel& a = m.ch[0];
+                const apic_mcc_channel& b = m.ch[ci];
+                if (b.energy_frame != APIC_FRAME_PROJECTILE || b.rows != a.rows ||
+                    std::memcmp(a.energy, b.energy, a.rows * sizeof(double)) != 0)
+                    D.shared_grid = 0;
             }
             D.v_safe = safe_speed(m, mass, sd);
             p.sp[m.species].model = mi;
@@ -1097,7 +1190,6 @@ struct Sim1D {
         p.births_cap = (unsigned)std::min<size_t>(std::max<size_t>(kMaxBirths, cap_total / 64), kMaxBirths);
         p.births = dalloc<BirthRec>(p.births_cap);
         DevState init{};
-        init.epoch = 1;
         APIC_CUDA(cudaMemcpyAsync(st, &init, sizeof init, cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaStreamSynchronize(stream));
         static bool attr_done = false;
@@ -1123,6 +1215,9 @@ struct Sim1D {
             S.vh[0] = B.vh[in]; S.vh[1] = B.vh[out];
             S.vy[0] = B.vy[in]; S.vy[1] = B.vy[out];
             S.vz[0] = B.vz[in]; S.vz[1] = B.vz[out];
+            S.rstart[0] = B.rstart[in]; S.rstart[1] = B.rstart[out];
+            S.rcount[0] = B.rcount[in]; S.rcount[1] = B.rcount[out];
+            S.rlstart[0] = B.rlstart[in]; S.rlstart[1] = B.rlstart[out];
         }
         return q;
     }
@@ -1135,17 +1230,48 @@ struct Sim1D {
         return (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 4));
     }
 
+    // Optional per-kernel timing (CUDA events on the handle's stream).
+    bool timing = false;
+    struct EvPair { cudaEvent_t a, b, c; };
+    std::vector<EvPair> events;
+    double pass_ms = 0.0, post_ms = 0.0;
+    uint64_t timed_passes = 0;
+
+    void collect_timing() {
+        for (auto& e : events) {
+            float t1 = 0.f, t2 = 0.f;
+            APIC_CUDA(cudaEventElapsedTime(&t1, e.a, e.b));
+            APIC_CUDA(cudaEventElapsedTime(&t2, e.b, e.c));
+            pass_ms += t1;
+            post_ms += t2;
+            ++timed_passes;
+            cudaEventDestroy(e.a); cudaEventDestroy(e.b); cudaEventDestroy(e.c);
+        }
+        events.clear();
+    }
+
     void launch_pass(unsigned mode, unsigned post) {
         const Params1D q = pass_params(mode);
         const int blocks = grid_blocks();
         const size_t smem = (size_t)cfg.nx * 16;
         const bool dir = cfg.boundary == APIC_DIRICHLET;
+        EvPair ev{};
+        if (timing) {
+            APIC_CUDA(cudaEventCreate(&ev.a));
+            APIC_CUDA(cudaEventCreate(&ev.b));
+            APIC_CUDA(cudaEventCreate(&ev.c));
+            APIC_CUDA(cudaEventRecord(ev.a, stream));
+        }
         if (cfg.velocity_dimensions == 3) {
-            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); k_post1d<3, true><<<1, kPostThreads, 0, stream>>>(q, post); }
-            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); k_post1d<3, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, true><<<1, kPostThreads, 0, stream>>>(q, post); }
+            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, false><<<1, kPostThreads, 0, stream>>>(q, post); }
         } else {
-            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); k_post1d<1, true><<<1, kPostThreads, 0, stream>>>(q, post); }
-            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); k_post1d<1, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, true><<<1, kPostThreads, 0, stream>>>(q, post); }
+            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+        }
+        if (timing) {
+            APIC_CUDA(cudaEventRecord(ev.c, stream));
+            events.push_back(ev);
         }
         APIC_CUDA(cudaGetLastError());
         parity ^= 1;
@@ -1155,6 +1281,25 @@ struct Sim1D {
               const double* vz, const uint8_t* alive) {
         require(s >= 0 && s < cfg.nspecies, "species index out of range");
         require(x && v, "x and v are required");
+        if (!alive && vh && (cfg.velocity_dimensions == 1 || (vy && vz))) {
+            // every particle alive: copy straight from the caller's buffers
+            require(n <= cfg.species[s].capacity, "initial particle count exceeds max_particles_per_species",
+                    APIC_ERR_CAPACITY);
+            SpeciesDev& B = p.sp[s];
+            const size_t bytes = n * sizeof(double);
+            APIC_CUDA(cudaMemcpyAsync(B.x[parity], x, bytes, cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(B.vh[parity], vh, bytes, cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(B.v, v, bytes, cudaMemcpyHostToDevice, stream));
+            if (cfg.velocity_dimensions == 3) {
+                APIC_CUDA(cudaMemcpyAsync(B.vy[parity], vy, bytes, cudaMemcpyHostToDevice, stream));
+                APIC_CUDA(cudaMemcpyAsync(B.vz[parity], vz, bytes, cudaMemcpyHostToDevice, stream));
+            }
+            set_single_range(s, (unsigned)n);
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            initialized = false;
+            pending = false;
+            return;
+        }
         std::vector<double> hx, hv, hvh, hvy, hvz;
         for (size_t i = 0; i < n; ++i) {
             if (alive && !alive[i]) continue;
@@ -1177,11 +1322,23 @@ struct Sim1D {
             APIC_CUDA(cudaMemcpyAsync(B.vy[parity], hvy.data(), bytes, cudaMemcpyHostToDevice, stream));
             APIC_CUDA(cudaMemcpyAsync(B.vz[parity], hvz.data(), bytes, cudaMemcpyHostToDevice, stream));
         }
-        const unsigned n32 = (unsigned)m;
-        APIC_CUDA(cudaMemcpyAsync(&st->n[s], &n32, sizeof n32, cudaMemcpyHostToDevice, stream));
+        set_single_range(s, (unsigned)m);
         APIC_CUDA(cudaStreamSynchronize(stream));
         initialized = false;
         pending = false;
+    }
+
+    // The loaded particles are one contiguous range at slot 0.
+    unsigned range_host[kMaxSpecies][4];
+    void set_single_range(int s, unsigned n) {
+        SpeciesDev& B = p.sp[s];
+        unsigned* h = range_host[s];
+        h[0] = 0; h[1] = n; h[2] = 0; h[3] = n ? 1u : 0u;
+        APIC_CUDA(cudaMemcpyAsync(B.rstart[parity], &h[0], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(B.rcount[parity], &h[1], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(B.rlstart[parity], &h[2], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(&st->n[s], &h[1], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemcpyAsync(&st->nranges[s], &h[3], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
     }
 
     void set_time(double t, uint64_t k) {
@@ -1233,11 +1390,12 @@ struct Sim1D {
         if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
         APIC_CUDA(e);
         unsigned word = 0;
-        APIC_CUDA(cudaMemcpy(&word, &st->error, sizeof word, cudaMemcpyDeviceToHost));
+        APIC_CUDA(cudaMemcpyAsync(&word, &st->error, sizeof word, cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
         if (word) {
             const int s = status_from_device(word);
-            const unsigned zero = 0;
-            APIC_CUDA(cudaMemcpy(&st->error, &zero, sizeof zero, cudaMemcpyHostToDevice));
+            APIC_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(unsigned), stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
             throw Error(s, describe_device_error(word));
         }
         return APIC_OK;
@@ -1246,7 +1404,8 @@ struct Sim1D {
     DevState read_state() {
         sync_status();
         DevState h;
-        APIC_CUDA(cudaMemcpy(&h, st, sizeof h, cudaMemcpyDeviceToHost));
+        APIC_CUDA(cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
         return h;
     }
 
@@ -1263,25 +1422,54 @@ struct Sim1D {
         require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
         const SpeciesDev& B = p.sp[s];
         const size_t bytes = n * sizeof(double);
-        if (x) APIC_CUDA(cudaMemcpy(x, B.x[parity], bytes, cudaMemcpyDeviceToHost));
-        if (v) APIC_CUDA(cudaMemcpy(v, B.v, bytes, cudaMemcpyDeviceToHost));
-        if (vh) APIC_CUDA(cudaMemcpy(vh, B.vh[parity], bytes, cudaMemcpyDeviceToHost));
+        if (x) APIC_CUDA(cudaMemcpyAsync(x, B.x[parity], bytes, cudaMemcpyDeviceToHost, stream));
+        if (v) APIC_CUDA(cudaMemcpyAsync(v, B.v, bytes, cudaMemcpyDeviceToHost, stream));
+        if (vh) APIC_CUDA(cudaMemcpyAsync(vh, B.vh[parity], bytes, cudaMemcpyDeviceToHost, stream));
         if (cfg.velocity_dimensions == 3) {
-            if (vy) APIC_CUDA(cudaMemcpy(vy, B.vy[parity], bytes, cudaMemcpyDeviceToHost));
-            if (vz) APIC_CUDA(cudaMemcpy(vz, B.vz[parity], bytes, cudaMemcpyDeviceToHost));
+            if (vy) APIC_CUDA(cudaMemcpyAsync(vy, B.vy[parity], bytes, cudaMemcpyDeviceToHost, stream));
+            if (vz) APIC_CUDA(cudaMemcpyAsync(vz, B.vz[parity], bytes, cudaMemcpyDeviceToHost, stream));
         } else {
             if (vy) std::memset(vy, 0, bytes);
             if (vz) std::memset(vz, 0, bytes);
         }
+        APIC_CUDA(cudaStreamSynchronize(stream));
         return n;
+    }
+
+    double* sample_partial = nullptr;
+    unsigned* sample_done = nullptr;
+    double* sample_out = nullptr;
+
+    DevState sample_device(apic_sample1d* out) {
+        if (!sample_partial) {
+            sample_partial = dalloc<double>(kSampleBlocks * kMaxSpecies);
+            sample_done = dalloc<unsigned>(1);
+            sample_out = dalloc<double>(kMaxSpecies + 2);
+        }
+        Params1D q = pass_params(0);
+        k_sample1d<<<kSampleBlocks, 256, 0, stream>>>(q, sample_partial, sample_done, sample_out);
+        APIC_CUDA(cudaGetLastError());
+        double h[kMaxSpecies + 2];
+        APIC_CUDA(cudaMemcpyAsync(h, sample_out, sizeof h, cudaMemcpyDeviceToHost, stream));
+        const DevState st_h = read_state();
+        for (int s = 0; s < cfg.nspecies; ++s) out->kinetic_by_species[s] = h[s];
+        out->field_energy = h[kMaxSpecies];
+        out->charge_l1 = h[kMaxSpecies + 1];
+        if (cfg.boundary == APIC_DIRICHLET) {
+            APIC_CUDA(cudaMemcpyAsync(&out->phi_left, p.phi, sizeof(double), cudaMemcpyDeviceToHost, stream));
+            APIC_CUDA(cudaMemcpyAsync(&out->phi_right, p.phi + cfg.nx - 1, sizeof(double), cudaMemcpyDeviceToHost, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+        }
+        return st_h;
     }
 
     void read_fields(double* rho, double* phi, double* E) {
         sync_status();
         const size_t bytes = cfg.nx * sizeof(double);
-        if (rho) APIC_CUDA(cudaMemcpy(rho, p.rho, bytes, cudaMemcpyDeviceToHost));
-        if (phi) APIC_CUDA(cudaMemcpy(phi, p.phi, bytes, cudaMemcpyDeviceToHost));
-        if (E) APIC_CUDA(cudaMemcpy(E, p.E, bytes, cudaMemcpyDeviceToHost));
+        if (rho) APIC_CUDA(cudaMemcpyAsync(rho, p.rho, bytes, cudaMemcpyDeviceToHost, stream));
+        if (phi) APIC_CUDA(cudaMemcpyAsync(phi, p.phi, bytes, cudaMemcpyDeviceToHost, stream));
+        if (E) APIC_CUDA(cudaMemcpyAsync(E, p.E, bytes, cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
     }
 };
 
@@ -1436,41 +1624,49 @@ int apic_sim1d_sample(apic_sim1d* sim, apic_sample1d* out) {
         auto& S = sim->impl;
         S.finish();
         std::memset(out, 0, sizeof *out);
-        const apic::DevState h = S.read_state();
-        const size_t nx = S.cfg.nx;
-        std::vector<double> rho(nx), phi(nx), E(nx);
-        S.read_fields(rho.data(), phi.data(), E.data());
-        // Species::kinetic_energy and Simulation::sample, src/Species.cpp:338-351,
-        // src/Simulation.cpp:1140-1161 (reduced on the host from the read-back state)
+        const apic::DevState h = S.sample_device(out);
         for (int s = 0; s < S.cfg.nspecies; ++s) {
-            const size_t n = h.n[s];
-            std::vector<double> v(n), vy(n), vz(n);
-            S.read_particles(s, n, nullptr, v.data(), nullptr, vy.data(), vz.data());
-            double e = 0.0;
-            const auto& sp = S.cfg.species[s];
-            for (size_t i = 0; i < n; ++i) {
-                double sq = v[i] * v[i];
-                if (S.cfg.velocity_dimensions == 3) sq += vy[i] * vy[i] + vz[i] * vz[i];
-                e += 0.5 * sp.mass * sp.weight * sq;
-            }
-            out->kinetic_by_species[s] = e;
-            out->live_by_species[s] = n;
-            out->kinetic_energy += e;
-            out->live_particles += n;
-        }
-        const bool dir = S.cfg.boundary == APIC_DIRICHLET;
-        for (size_t i = 0; i < nx; ++i) {
-            const double vol = dir ? ((i == 0 || i + 1 == nx) ? 0.5 * S.p.dx : S.p.dx) : S.p.dx;
-            out->field_energy += 0.5 * S.p.eps * E[i] * E[i] * vol;
-            out->charge_l1 += std::fabs(rho[i]) * vol;
+            out->live_by_species[s] = h.n[s];
+            out->kinetic_energy += out->kinetic_by_species[s];
+            out->live_particles += h.n[s];
         }
         out->total_energy = out->kinetic_energy + out->field_energy;
-        if (dir) {
-            out->phi_left = phi.front();
-            out->phi_right = phi.back();
-        }
         out->step = S.step;
         out->time = S.time;
+    });
+}
+
+int apic_sim1d_model_safe_speed(const apic_sim1d* sim, int model, double* speed) {
+    if (!sim || !speed || model < 0 || model >= sim->impl.cfg.nmodels) return APIC_ERR_INVALID;
+    *speed = sim->impl.p.model[model].v_safe;
+    return APIC_OK;
+}
+
+int apic_sim1d_cuda_stream(apic_sim1d* sim, void** stream) {
+    if (!sim || !stream) return APIC_ERR_INVALID;
+    *stream = (void*)sim->impl.stream;
+    return APIC_OK;
+}
+
+int apic_sim1d_set_kernel_timing(apic_sim1d* sim, int enable) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        sim->impl.sync_status();
+        sim->impl.collect_timing();
+        sim->impl.timing = enable != 0;
+        sim->impl.pass_ms = sim->impl.post_ms = 0.0;
+        sim->impl.timed_passes = 0;
+    });
+}
+
+int apic_sim1d_kernel_times(apic_sim1d* sim, double* pass_ms, double* post_ms, uint64_t* passes) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        sim->impl.sync_status();
+        sim->impl.collect_timing();
+        if (pass_ms) *pass_ms = sim->impl.pass_ms;
+        if (post_ms) *post_ms = sim->impl.post_ms;
+        if (passes) *passes = sim->impl.timed_passes;
     });
 }
 

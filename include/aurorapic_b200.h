@@ -229,6 +229,17 @@ APIC_EXPORT int apic_sim1d_collision_totals(apic_sim1d* sim, apic_collision_tota
 /* Simulation::species_boundary_losses(), include/pic/Simulation.hpp:73-76 */
 APIC_EXPORT int apic_sim1d_boundary_losses(apic_sim1d* sim, int species, apic_boundary_loss* out);
 APIC_EXPORT double apic_sim1d_time(const apic_sim1d* sim);
+/* The handle's CUDA stream (cudaStream_t), for callers that order their own
+ * work or timing events with the simulation. */
+APIC_EXPORT int apic_sim1d_cuda_stream(apic_sim1d* sim, void** stream);
+/* Per-kernel timing with CUDA events on the handle's stream: enable resets the
+ * totals; kernel_times returns the summed particle-pass and post (field solve)
+ * kernel milliseconds and the number of passes timed. */
+APIC_EXPORT int apic_sim1d_set_kernel_timing(apic_sim1d* sim, int enable);
+/* Speed at or below which model `model` skips the frequency-bound evaluation
+ * (the bound provably holds there); above it the exact check runs. */
+APIC_EXPORT int apic_sim1d_model_safe_speed(const apic_sim1d* sim, int model, double* speed);
+APIC_EXPORT int apic_sim1d_kernel_times(apic_sim1d* sim, double* pass_ms, double* post_ms, uint64_t* passes);
 APIC_EXPORT uint64_t apic_sim1d_step_count(const apic_sim1d* sim);
 
 /* ---- stateless kernels (host buffers in, host buffers out) --------------- */

@@ -401,3 +401,25 @@ class Ref1D:
 
     def time(self):
         return ref().ref1d_time(self.h)
+
+
+def config_from_workload(wl, tables: TableSet, seed=12345, threads=0, particles=None, own_loading=False):
+    """The oracle / reference configuration of a workload (apic.workloads.Workload1D).
+    own_loading=True gives each species its Maxwellian parameters so that the
+    reference loads its own particles (bench.py's CPU timing)."""
+    models = []
+    for m in wl.models:
+        chans = [tables.channel(c.process, c.energy, c.sigma, c.threshold, c.secondary, c.ion) for c in m.channels]
+        models.append(make_model(m.species, chans, m.neutral_density, m.max_frequency, m.neutral_mass,
+                                 m.neutral_temperature, 1 if wl.si else 0, m.max_candidates))
+    species = []
+    for s in wl.species:
+        n = len(s.x) if particles is None else particles
+        if own_loading:
+            species.append((s.charge, s.mass, s.weight, n, s.drift, s.thermal, s.thermal, s.thermal))
+        else:
+            species.append((s.charge, s.mass, s.weight, n, 0.0, 0.0, 0.0, 0.0))
+    return config1d(dirichlet=int(wl.dirichlet), vdim=wl.vdim, si=int(wl.si), nx=wl.nx, length=wl.length,
+                    dt=wl.dt, species=species, models=models, phi_left=wl.phi_left, phi_right=wl.phi_right,
+                    drive_left=wl.drive_left, drive_right=wl.drive_right, seed=seed, threads=threads,
+                    max_particles=max(s.capacity for s in wl.species))

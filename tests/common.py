@@ -9,19 +9,7 @@ from apic import workloads as W
 
 
 def oracle_config(wl: W.Workload1D, tables: po.TableSet, seed=12345, threads=0, particles=None):
-    models = []
-    for m in wl.models:
-        chans = [tables.channel(c.process, c.energy, c.sigma, c.threshold, c.secondary, c.ion) for c in m.channels]
-        models.append(po.make_model(m.species, chans, m.neutral_density, m.max_frequency, m.neutral_mass,
-                                    m.neutral_temperature, 1 if wl.si else 0, m.max_candidates))
-    species = []
-    for s in wl.species:
-        n = len(s.x) if particles is None else particles
-        species.append((s.charge, s.mass, s.weight, n, 0.0, 0.0, 0.0, 0.0))
-    return po.config1d(dirichlet=int(wl.dirichlet), vdim=wl.vdim, si=int(wl.si), nx=wl.nx, length=wl.length,
-                       dt=wl.dt, species=species, models=models, phi_left=wl.phi_left, phi_right=wl.phi_right,
-                       drive_left=wl.drive_left, drive_right=wl.drive_right, seed=seed, threads=threads,
-                       max_particles=max(s.capacity for s in wl.species))
+    return po.config_from_workload(wl, tables, seed=seed, threads=threads, particles=particles)
 
 
 def load_oracle(sim: po.Sim1D, wl: W.Workload1D):
