@@ -123,7 +123,7 @@ def _rate_bound(mass, channels, e_max_ev, neutral_density, neutral_mass, tempera
     return float(np.max(neutral_density * tot * (v + spread)))
 
 
-def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096) -> Workload1D:
+def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096, te_ev=1.0) -> Workload1D:
     """1D3V capacitive RF discharge with null-collision MCC: Dirichlet gap
     0.067 m, `cells` cells, grounded left electrode, right electrode driven at
     450 V / 13.56 MHz, dt = 1 / (400 f); electrons and He+ (4 amu) at
@@ -153,7 +153,7 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
     nu_e = 1.25 * _rate_bound(M_E, e_ch, 1e4, ng, m_he, T)
     nu_i = 1.25 * _rate_bound(m_he, i_ch, 2000.0, ng, m_he, T)
     rng = np.random.default_rng(seed)
-    ve = math.sqrt(E_CHARGE * 1.0 / M_E)
+    ve = math.sqrt(E_CHARGE * te_ev / M_E)
     vi = math.sqrt(E_CHARGE * 0.026 / m_he)
     cap = int(n * 1.5) + 4096
     sp = []

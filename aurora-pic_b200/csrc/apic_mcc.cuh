@@ -205,18 +205,27 @@ struct CollideResult {
 
 // NullCollisionModel::collide(Vec3&), src/Collision.cpp:907-993.  on_secondary
 // receives (channel, secondary velocity[3], ion velocity[3]) per ionization.
+// When have_first is set, the caller already ran the first loop iteration's
+// bound check and waiting-time draw (the stream continues after them) and
+// passes that waiting time.
 template <class S, class OnSecondary>
 __device__ inline void collide3(const MccModelDev& m, double v[3], double dt, S& s, CollideResult& r,
-                                OnSecondary&& on_secondary) {
+                                OnSecondary&& on_secondary, bool have_first = false, double first_wait = 0.0) {
     if (!isfinite(v[0]) || !isfinite(v[1]) || !isfinite(v[2])) { r.error |= kErrNonFinite; return; }
     double elapsed = 0.0;
     for (;;) {
-        if (!frequency_bound_ok(m, norm3(v[0], v[1], v[2]))) { r.error |= kErrMajorant; return; }
-        // open_unit_interval, src/Collision.cpp:46-51 (bounded for replay arrays)
-        double u = uniform01(s);
-        for (int guard = 0; !(u > 0.0) && guard < 64 && !s.overrun(); ++guard) u = uniform01(s);
-        if (s.overrun()) { r.error |= kErrReplay; return; }
-        const double waiting = -log(u) / m.max_frequency;
+        double waiting;
+        if (have_first) {
+            waiting = first_wait;
+            have_first = false;
+        } else {
+            if (!frequency_bound_ok(m, norm3(v[0], v[1], v[2]))) { r.error |= kErrMajorant; return; }
+            // open_unit_interval, src/Collision.cpp:46-51 (bounded for replay arrays)
+            double u = uniform01(s);
+            for (int guard = 0; !(u > 0.0) && guard < 64 && !s.overrun(); ++guard) u = uniform01(s);
+            if (s.overrun()) { r.error |= kErrReplay; return; }
+            waiting = -log(u) / m.max_frequency;
+        }
         if (!isfinite(waiting) || waiting >= dt - elapsed) break;
         elapsed += waiting;
         ++r.candidates;

@@ -46,6 +46,11 @@ struct PhiloxStream {
         return (k & 1u) ? ((uint64_t)buf[3] << 32 | buf[2]) : ((uint64_t)buf[1] << 32 | buf[0]);
     }
     __device__ bool overrun() const { return false; }
+    // continue a stream that already produced k draws
+    __device__ void seek(uint32_t k) {
+        index = k;
+        if (k & 1u) philox4x32_10(k >> 1, slot, step, stream, k0, k1, buf);
+    }
 };
 
 struct ReplayStream {

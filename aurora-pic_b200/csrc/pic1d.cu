@@ -48,10 +48,11 @@ constexpr int kItems = 4;
 constexpr int kTile = kThreads * kItems;
 constexpr int kMaxSpecies = APIC_MAX_SPECIES;
 constexpr int kMaxModels = APIC_MAX_MODELS;
-constexpr int kPostThreads = 1024;
-constexpr int kPostItems = 4;
+constexpr int kPostThreads = 512;
+constexpr int kPostItems = 8;
 constexpr int kMaxBirths = kPostThreads * kPostItems;  // products per pass the post kernel sorts
-constexpr int kMaxNx1D = 4096;
+constexpr int kMaxNx1D = 4096;          // Dirichlet grids
+constexpr int kMaxNx1DPeriodic = 2048;  // periodic grids (direct DFT with shared-memory spectra)
 
 enum : unsigned {
     kModeSyncMcc = 1u << 0,   // synchronize + collide + re-initialise (pending collision part)
@@ -108,7 +109,7 @@ struct SpeciesDev {
 
 struct Params1D {
     int nspecies, vdim, dirichlet, nx;
-    double L, dx, dt, eps, rho_scale, inv_rho_scale;
+    double L, dx, inv_dx, dt, eps, rho_scale, inv_rho_scale;
     unsigned mode;
     uint64_t seed;
     double phi_left, phi_right;
@@ -120,7 +121,6 @@ struct Params1D {
     double* phi;
     unsigned long long* rho_acc;
     const double* tw;       // periodic: twiddles (cos, sin)(2 pi m / n), m < n
-    double* scratch;        // periodic: 4 * nx per-mode spectra
     const double* thomas_r; // Dirichlet: 1/denominator of the Thomas forward sweep
     const double* thomas_a; // Dirichlet: -cp of the back substitution
     BirthRec* births;
@@ -130,7 +130,15 @@ struct Params1D {
 
 // ---- field gather / deposit (reference arithmetic) ----------------------
 
-__device__ __forceinline__ double wrap_periodic(double x, double L) { return fmod(fmod(x, L) + L, L); }
+// wrap_periodic, src/FieldSolver.cpp:15-17: fmod(fmod(x, L) + L, L).  For
+// |x| < 2L every fmod is a single exact subtraction (Sterbenz), so the fast
+// branch returns the same bits as the two library fmod calls.
+__device__ __forceinline__ double wrap_periodic(double x, double L) {
+    if (!(fabs(x) < 2.0 * L)) return fmod(fmod(x, L) + L, L);
+    const double r = x >= L ? x - L : (x <= -L ? x + L : x);  // fmod(x, L)
+    const double y = r + L;
+    return y >= 2.0 * L ? 0.0 : (y >= L ? y - L : y);          // fmod(y, L), 0 < y <= 2L
+}
 
 struct Cic {
     int i0, i1;
@@ -186,10 +194,13 @@ __device__ __forceinline__ void deposit_contrib(const Cic& c, const SpeciesDev& 
         a0 = to_fixed(s.qwdx * c.w0, p.rho_scale);
         a1 = to_fixed(s.qwdx * c.w1, p.rho_scale);
     } else {
-        const double v0 = (c.i0 == 0 || c.i0 + 1 == p.nx) ? 0.5 * p.dx : p.dx;
-        const double v1 = (c.i1 == 0 || c.i1 + 1 == p.nx) ? 0.5 * p.dx : p.dx;
-        a0 = to_fixed(s.qw * c.w0 / v0, p.rho_scale);
-        a1 = to_fixed(s.qw * c.w1 / v1, p.rho_scale);
+        // q w (1 - f) / node_volume(i), src/Species.cpp:180-181: the reciprocal
+        // volume differs from the division by at most one rounding, far below
+        // the fixed-point resolution of the accumulated density
+        const double r0 = (c.i0 == 0 || c.i0 + 1 == p.nx) ? 2.0 * p.inv_dx : p.inv_dx;
+        const double r1 = (c.i1 == 0 || c.i1 + 1 == p.nx) ? 2.0 * p.inv_dx : p.inv_dx;
+        a0 = to_fixed(s.qw * c.w0 * r0, p.rho_scale);
+        a1 = to_fixed(s.qw * c.w1 * r1, p.rho_scale);
     }
 }
 
@@ -209,12 +220,28 @@ __device__ __forceinline__ unsigned physical_slot(const unsigned* lstart, const 
 
 // ---- the fused particle pass -----------------------------------------------
 
+// A particle whose first exponential waiting time falls inside the step is a
+// collision candidate (a few percent of particles).  Its full collision loop
+// runs in a second phase of the tile from a shared-memory queue, so that the
+// long, branchy loops are packed into few warps instead of diverging inside
+// every warp.
+struct CandidateEntry {
+    double v[3];
+    double x;
+    double first_wait;
+    unsigned slot;
+    unsigned draws;
+};
+constexpr int kQueue = 384;
+
 template <int VDIM, bool DIRICHLET>
-__global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
+__global__ void __launch_bounds__(kThreads, 3) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
     unsigned long long* sRho = reinterpret_cast<unsigned long long*>(sE + p.nx);
     __shared__ unsigned s_cnt[kItems * (kThreads / 32)];
+    __shared__ unsigned s_qlen;
+    __shared__ CandidateEntry s_queue[kQueue];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned mode = p.mode;
@@ -222,12 +249,14 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
         sE[i] = p.E[i];
         sRho[i] = 0ull;
     }
+    if (tid == 0) s_qlen = 0;
     DevState* st = p.st;
     unsigned tiles_before[kMaxSpecies + 1];
     tiles_before[0] = 0;
     for (int s = 0; s < kMaxSpecies; ++s)
         tiles_before[s + 1] = tiles_before[s] + (s < p.nspecies ? (st->n[s] + kTile - 1) / kTile : 0);
     const unsigned total_tiles = tiles_before[kMaxSpecies];
+    const uint32_t mcc_step = (uint32_t)(st->step - 1ull);
     __syncthreads();
 
     // chunks of kTile logical particles, statically strided over the grid
@@ -239,14 +268,17 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
         const unsigned n = st->n[s];
         const unsigned nr = st->nranges[s];
         const unsigned base = tile * kTile;
+        const bool mcc = (mode & kModeSyncMcc) && S.model >= 0 && VDIM == 3;
 
-        double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems];
+        double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems], Ek[kItems];
         bool keep[kItems];
+        int queued[kItems];
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const unsigned idx = base + k * kThreads + tid;
             const bool live = idx < n;
             keep[k] = live;
+            queued[k] = -1;
             const unsigned ph = live ? physical_slot(S.rlstart[0], S.rstart[0], nr, idx) : 0u;
             x[k] = live ? S.x[0][ph] : 0.0;
             vh[k] = live ? S.vh[0][ph] : 0.0;
@@ -255,67 +287,111 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
             vc[k] = 0.0;
             if ((mode & kModeInitHalf) && live) vc[k] = S.v[ph];
         }
+        // -- phase A: gather, synchronize, first collision draw --
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
+            Ek[k] = 0.0;
             if (!keep[k]) continue;
             const unsigned idx = base + k * kThreads + tid;
-            const Cic c = cic<DIRICHLET>(x[k], p);
-            const double E = gather(sE, c);
+            const double E = gather(sE, cic<DIRICHLET>(x[k], p));
+            Ek[k] = E;
             if (mode & kModeInitHalf) {
                 // initialize_leapfrog_half_step, src/Pusher.cpp:66-68
                 vh[k] = vc[k] - S.hqm * E * p.dt;
             }
             if (mode & kModeSyncMcc) {
                 // synchronize_leapfrog, src/Pusher.cpp:78-80
-                double v = vh[k] + S.hqm * E * p.dt;
-                if (S.model >= 0 && VDIM == 3) {
+                vc[k] = vh[k] + S.hqm * E * p.dt;
+                if (mcc) {
                     const MccModelDev& M = p.model[S.model];
-                    double vel[3] = {v, vy[k], vz[k]};
-                    PhiloxStream rng(p.seed, idx, (uint32_t)(st->step - 1ull), (uint32_t)s);
-                    CollideResult r;
-                    unsigned nion = 0;
-                    const double xk = x[k];
-                    collide3(M, vel, p.dt, rng, r, [&](int ch, const double* vs, const double* vi) {
-                        const unsigned slot = atomicAdd(&st->nbirths, 2u);
-                        const MccChannelDev& C = M.ch[ch];
-                        if (slot + 2u <= p.births_cap) {
-                            const unsigned long long key =
-                                ((unsigned long long)s << 56) | ((unsigned long long)idx << 16) | (nion << 1);
-                            BirthRec a, b;
-                            a.key = key; a.x = xk; a.species = C.secondary; a.pad = 0;
-                            b.key = key | 1ull; b.x = xk; b.species = C.ion; b.pad = 0;
-                            for (int d = 0; d < 3; ++d) { a.v[d] = vs[d]; b.v[d] = vi[d]; }
-                            p.births[slot] = a;
-                            p.births[slot + 1] = b;
+                    // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
+                    if (!frequency_bound_ok(M, norm3(vc[k], vy[k], vz[k]))) atomicOr(&st->error, kErrMajorant);
+                    PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
+                    double u = uniform01(rng);
+                    for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
+                    const double wait = -log(u) / M.max_frequency;
+                    if (isfinite(wait) && wait < p.dt) {
+                        const unsigned q = atomicAdd(&s_qlen, 1u);
+                        if (q < (unsigned)kQueue) {
+                            CandidateEntry& ce = s_queue[q];
+                            ce.v[0] = vc[k]; ce.v[1] = vy[k]; ce.v[2] = vz[k];
+                            ce.first_wait = wait;
+                            ce.x = x[k];
+                            ce.slot = idx;
+                            ce.draws = rng.index;
+                            queued[k] = (int)q;
                         } else {
-                            atomicOr(&st->error, kErrBirths);
-                        }
-                        const SpeciesDev& A = p.sp[C.secondary];
-                        const SpeciesDev& B = p.sp[C.ion];
-                        const double added =
-                            0.5 * A.mass * A.weight * (vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]) +
-                            0.5 * B.mass * B.weight * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
-                        atomicAdd(&st->chan_energy[S.model][ch], added);
-                        ++nion;
-                    });
-                    if (r.error) atomicOr(&st->error, r.error);
-                    if (r.candidates) {
-                        atomicAdd(&st->candidates, (unsigned long long)r.candidates);
-                        if (r.nulls) atomicAdd(&st->nulls, (unsigned long long)r.nulls);
-                        for (int ch = 0; ch < M.nch; ++ch) {
-                            if (r.channel[ch]) {
-                                atomicAdd(&st->chan[S.model][ch], (unsigned long long)r.channel[ch]);
-                                atomicAdd(&st->chan_energy[S.model][ch], r.energy_change[ch] * S.weight);
-                            }
+                            atomicOr(&st->error, kErrBirths);  // queue sized for > 30% candidates per tile
                         }
                     }
-                    v = vel[0];
-                    vy[k] = vel[1];
-                    vz[k] = vel[2];
-                    // initialize_leapfrog_half_step after the collision, src/Simulation.cpp:924-926
-                    vh[k] = v - S.hqm * E * p.dt;
                 }
-                vc[k] = v;
+            }
+        }
+        __syncthreads();
+        // -- phase B: full collision loops of the queued candidates --
+        if (mcc) {
+            const unsigned qlen = min(s_qlen, (unsigned)kQueue);
+            const MccModelDev& M = p.model[S.model];
+            for (unsigned q = tid; q < qlen; q += kThreads) {
+                CandidateEntry& ce = s_queue[q];
+                PhiloxStream rng(p.seed, ce.slot, mcc_step, (uint32_t)s);
+                rng.seek(ce.draws);
+                CollideResult r;
+                unsigned nion = 0;
+                const unsigned slot = ce.slot;
+                const double px = ce.x;
+                double vel[3] = {ce.v[0], ce.v[1], ce.v[2]};
+                collide3(M, vel, p.dt, rng, r,
+                         [&](int ch, const double* vs, const double* vi) {
+                             const unsigned bslot = atomicAdd(&st->nbirths, 2u);
+                             const MccChannelDev& C = M.ch[ch];
+                             if (bslot + 2u <= p.births_cap) {
+                                 const unsigned long long key =
+                                     ((unsigned long long)s << 56) | ((unsigned long long)slot << 16) | (nion << 1);
+                                 BirthRec a, b;
+                                 a.key = key; a.species = C.secondary; a.pad = 0;
+                                 b.key = key | 1ull; b.species = C.ion; b.pad = 0;
+                                 a.x = b.x = px;
+                                 for (int d = 0; d < 3; ++d) { a.v[d] = vs[d]; b.v[d] = vi[d]; }
+                                 p.births[bslot] = a;
+                                 p.births[bslot + 1] = b;
+                             } else {
+                                 atomicOr(&st->error, kErrBirths);
+                             }
+                             const SpeciesDev& A = p.sp[C.secondary];
+                             const SpeciesDev& B = p.sp[C.ion];
+                             const double added =
+                                 0.5 * A.mass * A.weight * (vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]) +
+                                 0.5 * B.mass * B.weight * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
+                             atomicAdd(&st->chan_energy[S.model][ch], added);
+                             ++nion;
+                         },
+                         true, ce.first_wait);
+                if (r.error) atomicOr(&st->error, r.error);
+                atomicAdd(&st->candidates, (unsigned long long)r.candidates);
+                if (r.nulls) atomicAdd(&st->nulls, (unsigned long long)r.nulls);
+                for (int ch = 0; ch < M.nch; ++ch) {
+                    if (r.channel[ch]) {
+                        atomicAdd(&st->chan[S.model][ch], (unsigned long long)r.channel[ch]);
+                        atomicAdd(&st->chan_energy[S.model][ch], r.energy_change[ch] * S.weight);
+                    }
+                }
+                ce.v[0] = vel[0]; ce.v[1] = vel[1]; ce.v[2] = vel[2];
+            }
+            __syncthreads();
+        }
+        // -- phase C: re-initialise, kick, drift, walls, deposit --
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            if (!keep[k]) continue;
+            const double E = Ek[k];
+            if (mcc) {
+                if (queued[k] >= 0) {
+                    const CandidateEntry& ce = s_queue[queued[k]];
+                    vc[k] = ce.v[0]; vy[k] = ce.v[1]; vz[k] = ce.v[2];
+                }
+                // initialize_leapfrog_half_step after the collision, src/Simulation.cpp:924-926
+                vh[k] = vc[k] - S.hqm * E * p.dt;
             }
             if (mode & kModeKickDrift) {
                 // kick_leapfrog + drift_leapfrog, src/Pusher.cpp:70-76
@@ -360,7 +436,10 @@ __global__ void __launch_bounds__(kThreads) k_pass1d(Params1D p) {
             }
             s_cnt[lane] = incl - c;
             const unsigned total = __shfl_sync(0xffffffffu, incl, 31);
-            if (lane == 0) S.chunk_surv[tile] = total;
+            if (lane == 0) {
+                S.chunk_surv[tile] = total;
+                s_qlen = 0;
+            }
         }
         __syncthreads();
         // survivors of this chunk keep their order at the chunk's own slots
@@ -406,6 +485,14 @@ __device__ __forceinline__ double electrode(double offset, const apic_voltage_dr
     return offset + d.amplitude * sin(2.0 * 3.141592653589793 * d.frequency * t + d.phase);
 }
 
+// Shared-memory layout of the post kernel (dynamic): the fixed-point density,
+// the solver's constant coefficients and, for the periodic solve, the per-mode
+// spectra.  Everything the solve needs is loaded in one round trip at entry.
+__host__ __device__ inline size_t post_smem_bytes(int nx, bool dirichlet) {
+    return (size_t)nx * 8 /* rho_i */ + (size_t)nx * 8 /* rho */ +
+           (dirichlet ? (size_t)2 * nx * 8 : (size_t)2 * nx * 8 /* twiddles */ + (size_t)4 * nx * 8 /* spectra */);
+}
+
 template <int VDIM, bool DIRICHLET>
 __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned post) {
     using Sort = cub::BlockRadixSort<unsigned long long, kPostThreads, kPostItems, int>;
@@ -420,8 +507,30 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
     __shared__ double s_red[kPostThreads / 32];
     __shared__ double s_mean;
     __shared__ unsigned s_carry;
+    extern __shared__ __align__(16) unsigned char post_raw[];
+    const int nx = p.nx;
+    unsigned long long* s_rhoi = reinterpret_cast<unsigned long long*>(post_raw);
+    double* s_rho = reinterpret_cast<double*>(s_rhoi + nx);
+    double* s_c0 = s_rho + nx;                       // Dirichlet: 1/denominators; periodic: twiddles (2 nx)
+    double* s_c1 = s_c0 + nx;                        // Dirichlet: -cp
+    double* s_spec = s_c0 + 2 * nx;                  // periodic: 4 nx spectra
     DevState* st = p.st;
     const int tid = threadIdx.x;
+    const bool solve = (post & kPostSolve) != 0;
+
+    // -- one round trip: density accumulators and solver coefficients --
+    if (solve) {
+        for (int i = tid; i < nx; i += kPostThreads) {
+            s_rhoi[i] = p.rho_acc[i];
+            p.rho_acc[i] = 0ull;
+            if (DIRICHLET) {
+                if (i < nx - 2) { s_c0[i] = p.thomas_r[i]; s_c1[i] = p.thomas_a[i]; }
+            } else {
+                s_c0[2 * i] = p.tw[2 * i];
+                s_c0[2 * i + 1] = p.tw[2 * i + 1];
+            }
+        }
+    }
 
     // -- output range table: chunk c of the pass kept its survivors at slots
     //    [c * kTile, c * kTile + surv_c); logical starts are their prefix sums --
@@ -480,7 +589,6 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         }
         Sort(tmp.sort).Sort(keys, idx);
         __syncthreads();
-        // process births in sorted order: thread holds sorted ranks tid*kPostItems + k
         double bx[kPostItems], bvh[kPostItems], bv[kPostItems][3];
         int bs[kPostItems];
         bool keep[kPostItems];
@@ -495,8 +603,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
             bs[k] = r.species;
             bx[k] = r.x;
             bv[k][0] = r.v[0]; bv[k][1] = r.v[1]; bv[k][2] = r.v[2];
-            const Cic c = cic<DIRICHLET>(r.x, p);
-            const double E = gather(p.E, c);
+            const double E = gather(p.E, cic<DIRICHLET>(r.x, p));
             // append_product: v_half = v, then initialize_leapfrog_half_step, src/Simulation.cpp:985-1004
             bvh[k] = r.v[0] - S.hqm * E * p.dt;
             keep[k] = true;
@@ -512,12 +619,12 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                     atomicAdd(&st->lost_energy[r.species][side], 0.5 * S.mass * S.weight * sp2);
                     keep[k] = false;
                 }
-                if (keep[k]) {
+                if (keep[k] && solve) {
                     const Cic d = cic<DIRICHLET>(bx[k], p);
                     long long a0, a1;
                     deposit_contrib<DIRICHLET>(d, S, p, a0, a1);
-                    atomicAdd(&p.rho_acc[d.i0], (unsigned long long)a0);
-                    atomicAdd(&p.rho_acc[d.i1], (unsigned long long)a1);
+                    atomicAdd(&s_rhoi[d.i0], (unsigned long long)a0);
+                    atomicAdd(&s_rhoi[d.i1], (unsigned long long)a1);
                 }
             }
         }
@@ -564,16 +671,15 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         st->n[tid] = s_surv[tid] + kept;
     }
     if (tid == 0) st->nbirths = 0;
-    if (!(post & kPostSolve)) return;
+    if (!solve) return;
+    __syncthreads();
 
     // -- density: fixed point -> FP64 ---------------------------------------
-    const int nx = p.nx;
     double local = 0.0;
     for (int i = tid; i < nx; i += kPostThreads) {
-        const long long a = (long long)p.rho_acc[i];
-        const double r = (double)a * p.inv_rho_scale;
+        const double r = (double)(long long)s_rhoi[i] * p.inv_rho_scale;
+        s_rho[i] = r;
         p.rho[i] = r;
-        p.rho_acc[i] = 0ull;
         local += r;
     }
     const double field_time = (post & kPostAdvance) ? st->time + p.dt : st->time;
@@ -590,39 +696,29 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         __syncthreads();
         const double mean = s_mean;
         const double twopi = 2.0 * 3.141592653589793;
-        // forward transform: mode k per thread, summed over j in the reference's order;
-        // stored in phi (real part) and E (imaginary part) scratch
-        double* rk = p.phi;
-        double* ik = p.E;
-        for (int k = tid; k < nx; k += kPostThreads) {
-            double re = 0.0, im = 0.0;
-            if (k > 0) {
-                unsigned m = 0;
-                for (int j = 0; j < nx; ++j) {
-                    const double a = p.rho[j] - mean;
-                    re += a * p.tw[2 * m];
-                    im += a * (-p.tw[2 * m + 1]);
-                    m += (unsigned)k;
-                    if (m >= (unsigned)nx) m -= (unsigned)nx;
-                }
-                re /= (double)nx;
-                im /= (double)nx;
-            }
-            rk[k] = re;
-            ik[k] = im;
-        }
-        __syncthreads();
-        // per-mode potential and field, src/FieldSolver.cpp:426-428
-        double* sp_r = p.scratch;
-        double* sp_i = p.scratch + nx;
-        double* se_r = p.scratch + 2 * nx;
-        double* se_i = p.scratch + 3 * nx;
+        double* sp_r = s_spec;
+        double* sp_i = s_spec + nx;
+        double* se_r = s_spec + 2 * nx;
+        double* se_i = s_spec + 3 * nx;
+        // forward transform: mode k per thread, summed over j in the reference's order,
+        // then the per-mode potential and field, src/FieldSolver.cpp:418-428
         for (int k = tid; k < nx; k += kPostThreads) {
             if (k == 0) { sp_r[0] = sp_i[0] = se_r[0] = se_i[0] = 0.0; continue; }
+            double re = 0.0, im = 0.0;
+            unsigned m = 0;
+            for (int j = 0; j < nx; ++j) {
+                const double a = s_rho[j] - mean;
+                re += a * s_c0[2 * m];
+                im += a * (-s_c0[2 * m + 1]);
+                m += (unsigned)k;
+                if (m >= (unsigned)nx) m -= (unsigned)nx;
+            }
+            re /= (double)nx;
+            im /= (double)nx;
             const double kk = (k <= nx / 2) ? (double)k : -(double)(nx - k);
             const double wave = twopi * kk / p.L;
             const double den = p.eps * wave * wave;
-            const double pr = rk[k] / den, pi = ik[k] / den;
+            const double pr = re / den, pi = im / den;
             sp_r[k] = pr;
             sp_i[k] = pi;
             se_r[k] = wave * pi;    // -(0,1) * wave * phik
@@ -634,7 +730,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
             double ph = 0.0, ef = 0.0;
             unsigned m = (unsigned)j;
             for (int k = 1; k < nx; ++k) {
-                const double cs = p.tw[2 * m], sn = p.tw[2 * m + 1];
+                const double cs = s_c0[2 * m], sn = s_c0[2 * m + 1];
                 ph += sp_r[k] * cs - sp_i[k] * sn;
                 ef += se_r[k] * cs - se_i[k] * sn;
                 m += (unsigned)j;
@@ -653,13 +749,14 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         const double dx2 = p.dx * p.dx;
         constexpr int IPT = kMaxNx1D / kPostThreads;
         Affine f[IPT];
+#pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int i = tid * IPT + k;
             if (i < m) {
-                double d = p.rho[i + 1] * dx2 / p.eps;
+                double d = s_rho[i + 1] * dx2 / p.eps;
                 if (i == 0) d += phil;
                 if (i == m - 1) d += phir;
-                const double r = p.thomas_r[i];
+                const double r = s_c0[i];
                 f[k] = Affine{r, r * d};
             } else {
                 f[k] = Affine{1.0, 0.0};
@@ -667,40 +764,44 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         }
         ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
         __syncthreads();
-        // dp[i] = f[i].b (the recurrence starts from 0); keep in phi[i+1] scratch
+        double* s_dp = s_rho;  // dp replaces rho (rho already written out)
+#pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int i = tid * IPT + k;
-            if (i < m) p.E[i] = f[k].b;  // dp
+            if (i < m) s_dp[i] = f[k].b;
         }
         __syncthreads();
         // back substitution in reverse: z_t = a[m-1-t] z_{t-1} + dp[m-1-t]
+#pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int t = tid * IPT + k;
             if (t < m) {
                 const int ii = m - 1 - t;
-                f[k] = Affine{p.thomas_a[ii], p.E[ii]};
+                f[k] = Affine{s_c1[ii], s_dp[ii]};
             } else {
                 f[k] = Affine{1.0, 0.0};
             }
         }
-        __syncthreads();
         ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
         __syncthreads();
+        double* s_phi = s_c0;  // coefficients no longer needed
+#pragma unroll
         for (int k = 0; k < IPT; ++k) {
             const int t = tid * IPT + k;
-            if (t < m) p.phi[m - t] = f[k].b;
+            if (t < m) s_phi[m - t] = f[k].b;
         }
         if (tid == 0) {
-            p.phi[0] = phil;
-            p.phi[nx - 1] = phir;
+            s_phi[0] = phil;
+            s_phi[nx - 1] = phir;
         }
         __syncthreads();
         for (int i = tid; i < nx; i += kPostThreads) {
             double e;
-            if (i == 0) e = -(p.phi[1] - p.phi[0]) / p.dx;
-            else if (i == nx - 1) e = -(p.phi[nx - 1] - p.phi[nx - 2]) / p.dx;
-            else e = -(p.phi[i + 1] - p.phi[i - 1]) / (2.0 * p.dx);
+            if (i == 0) e = -(s_phi[1] - s_phi[0]) / p.dx;
+            else if (i == nx - 1) e = -(s_phi[nx - 1] - s_phi[nx - 2]) / p.dx;
+            else e = -(s_phi[i + 1] - s_phi[i - 1]) / (2.0 * p.dx);
             p.E[i] = e;
+            p.phi[i] = s_phi[i];
         }
     }
     if (tid == 0 && (post & kPostAdvance)) {
@@ -995,7 +1096,8 @@ struct Sim1D {
         require(c.velocity_dimensions == 1 || c.velocity_dimensions == 3,
                 "simulation velocity_dimensions must be 1 or 3");
         require(c.nx >= 3, "grid nx must be at least 3");
-        require(c.nx <= (size_t)kMaxNx1D, "grid nx above the 1D device limit (4096)", APIC_ERR_UNSUPPORTED);
+        require(c.nx <= (size_t)(c.boundary == APIC_DIRICHLET ? kMaxNx1D : kMaxNx1DPeriodic),
+                "grid nx above the 1D device limit (4096 Dirichlet, 2048 periodic)", APIC_ERR_UNSUPPORTED);
         require(std::isfinite(c.length) && c.length > 0, "domain length must be positive and finite");
         require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
         require(c.nspecies >= 1 && c.nspecies <= kMaxSpecies, "species count out of range");
@@ -1016,6 +1118,7 @@ struct Sim1D {
         p.nx = (int)c.nx;
         p.L = c.length;
         p.dx = c.length / (double)(dir ? c.nx - 1 : c.nx);  // Grid::Grid, src/Grid.cpp:19-22
+        p.inv_dx = 1.0 / p.dx;
         p.dt = c.dt;
         p.eps = (c.units == APIC_SI ? 8.8541878128e-12 : 1.0) * rel;  // include/pic/Types.hpp:17-27
         p.seed = c.seed;
@@ -1163,7 +1266,6 @@ struct Sim1D {
             double* d = dalloc<double>(tw.size());
             APIC_CUDA(cudaMemcpyAsync(d, tw.data(), tw.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
             p.tw = d;
-            p.scratch = dalloc<double>(4 * c.nx);
             APIC_CUDA(cudaStreamSynchronize(stream));
         } else {
             // Thomas coefficients of the constant [-1 2 -1] matrix, src/FieldSolver.cpp:745-752
@@ -1199,6 +1301,12 @@ struct Sim1D {
             APIC_CUDA(cudaFuncSetAttribute(k_pass1d<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            const int psm = (int)post_smem_bytes(kMaxNx1D, true);
+            const int psm_p = (int)post_smem_bytes(kMaxNx1DPeriodic, false);
+            APIC_CUDA(cudaFuncSetAttribute(k_post1d<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
+            APIC_CUDA(cudaFuncSetAttribute(k_post1d<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
+            APIC_CUDA(cudaFuncSetAttribute(k_post1d<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm_p));
+            APIC_CUDA(cudaFuncSetAttribute(k_post1d<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm_p));
             attr_done = true;
         }
     }
@@ -1255,6 +1363,7 @@ struct Sim1D {
         const int blocks = grid_blocks();
         const size_t smem = (size_t)cfg.nx * 16;
         const bool dir = cfg.boundary == APIC_DIRICHLET;
+        const size_t post_smem = post_smem_bytes((int)cfg.nx, dir);
         EvPair ev{};
         if (timing) {
             APIC_CUDA(cudaEventCreate(&ev.a));
@@ -1263,11 +1372,11 @@ struct Sim1D {
             APIC_CUDA(cudaEventRecord(ev.a, stream));
         }
         if (cfg.velocity_dimensions == 3) {
-            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, true><<<1, kPostThreads, 0, stream>>>(q, post); }
-            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, true><<<1, kPostThreads, post_smem, stream>>>(q, post); }
+            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, false><<<1, kPostThreads, post_smem, stream>>>(q, post); }
         } else {
-            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, true><<<1, kPostThreads, 0, stream>>>(q, post); }
-            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, false><<<1, kPostThreads, 0, stream>>>(q, post); }
+            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, true><<<1, kPostThreads, post_smem, stream>>>(q, post); }
+            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, false><<<1, kPostThreads, post_smem, stream>>>(q, post); }
         }
         if (timing) {
             APIC_CUDA(cudaEventRecord(ev.c, stream));

@@ -220,6 +220,7 @@ def main():
 
     ext = torch.cuda.ExternalStream(sim.cuda_stream())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+    flush_sink = torch.empty((), dtype=torch.float32, device="cuda")
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     n_before = sum(sim.count(s) for s in range(len(wl.species)))
@@ -230,7 +231,10 @@ def main():
     with Clocks(local) as clk:
         with torch.cuda.stream(ext):
             for i in range(args.steps):
+                # write a buffer larger than L2, then read it back so the dirty
+                # lines are written out before the timed step starts
                 flush.zero_()
+                flush_sink.copy_(flush.sum())
                 starts[i].record(ext)
                 sim.step(1)
                 ends[i].record(ext)

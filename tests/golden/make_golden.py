@@ -1,0 +1,139 @@
+"""Generates the golden vectors under tests/golden/ by running the reference
+itself (its library compiled from the reference sources by oracle/Makefile,
+driven through oracle/ref_harness.cpp).  Run from the repository root:
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+The fixtures pin the CPU oracle (oracle/apic_oracle.c) in
+tests/test_oracle_golden.py; the GPU parity tests then compare the device
+library with the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "aurora-pic_b200"))
+
+import pyoracle as po  # noqa: E402
+from apic import workloads as W  # noqa: E402
+
+
+def rng_fixture():
+    R = po.ref()
+    raw = np.zeros(1000, np.uint64)
+    R.ref_mt64(42, 1000, po.u64ptr(raw))
+    dists = np.zeros((4, 500))
+    for k in range(4):
+        d = np.zeros(500)
+        R.ref_dist(k, 7, 500, po.dptr(d))
+        dists[k] = d
+    np.savez_compressed(os.path.join(HERE, "rng.npz"), mt64_seed42=raw, dist_seed7=dists)
+
+
+def grid_fixture():
+    R = po.ref()
+    rng = np.random.default_rng(21)
+    for name, dirichlet in (("periodic", 0), ("dirichlet", 1)):
+        nx, L, eps = 67, 2.3, 1.7
+        xs = [rng.uniform(0, L, 700), rng.uniform(0, L, 500)]
+        xs[0][:2] = [0.0, L]
+        q = np.array([-1.0, 1.0])
+        w = np.array([0.011, 0.017])
+        xq = rng.uniform(-0.3, L + 0.3, 300)
+        counts = (C.c_size_t * 2)(len(xs[0]), len(xs[1]))
+        ptrs = (C.POINTER(C.c_double) * 2)(po.dptr(xs[0]), po.dptr(xs[1]))
+        rho, phi, E, eq = np.zeros(nx), np.zeros(nx), np.zeros(nx), np.zeros(len(xq))
+        rc = R.ref_deposit_solve_gather_1d(dirichlet, nx, L, eps, 0.3, -1.1, 2, po.dptr(q), po.dptr(w), counts, ptrs,
+                                           po.dptr(rho), po.dptr(phi), po.dptr(E), len(xq), po.dptr(xq), po.dptr(eq))
+        assert rc == 0, R.ref_last_error()
+        np.savez_compressed(os.path.join(HERE, f"grid1d_{name}.npz"), nx=nx, length=L, eps=eps, phi_left=0.3,
+                            phi_right=-1.1, q=q, w=w, x0=xs[0], x1=xs[1], xq=xq, rho=rho, phi=phi, E=E, eq=eq)
+
+
+def small_ccp(ppc=8, cells=32, rows=96):
+    return W.ccp_helium(particles_per_cell=ppc, cells=cells, seed=5, steps=10, table_rows=rows)
+
+
+def collide_fixture():
+    R = po.ref()
+    wl = small_ccp()
+    out = {}
+    for mi, scale in ((0, 5e6), (1, 6e4)):
+        T = po.TableSet()
+        cfg = po.config_from_workload(wl, T)
+        m = cfg.models[mi]
+        rng = np.random.default_rng(100 + mi)
+        n = 300
+        v = rng.standard_normal((n, 3)) * scale
+        seeds = rng.integers(1, 2 ** 62, n, dtype=np.uint64)
+        stats = (po.CollideStats * n)()
+        vv = np.ascontiguousarray(v.copy())
+        dt = wl.dt * 40
+        work = tempfile.mkdtemp()
+        rc = R.ref_collide3(C.byref(m), wl.species[m.species].mass, work.encode(), n, po.dptr(vv.reshape(-1)),
+                            po.u64ptr(seeds), dt, stats, None, 0)
+        assert rc == 0, R.ref_last_error()
+        ch = [m.ch[i] for i in range(m.nch)]
+        out[f"m{mi}_v_in"] = v
+        out[f"m{mi}_v_out"] = vv
+        out[f"m{mi}_seeds"] = seeds
+        out[f"m{mi}_dt"] = dt
+        out[f"m{mi}_candidates"] = np.array([s.candidates for s in stats], np.uint64)
+        out[f"m{mi}_nulls"] = np.array([s.null_collisions for s in stats], np.uint64)
+        out[f"m{mi}_channels"] = np.array([list(s.channel_collisions) for s in stats], np.uint64)
+        out[f"m{mi}_nsec"] = np.array([s.nsecondaries for s in stats], np.int32)
+        out[f"m{mi}_draws"] = np.array([s.draws for s in stats], np.uint64)
+        out[f"m{mi}_sec_v"] = np.array([[list(s.secondary_velocity[k]) for k in range(4)] for s in stats])
+    np.savez_compressed(os.path.join(HERE, "collide3.npz"), **out)
+
+
+def sim_fixture(name, wl, steps, with_rng=False):
+    T = po.TableSet()
+    cfg = po.config_from_workload(wl, T, seed=2024, own_loading=True)
+    work = tempfile.mkdtemp()
+    R = po.Ref1D(cfg, work)
+    R.initialize()
+    out = {"steps": steps}
+    for s in range(cfg.nspecies):
+        p = R.particles(s)
+        for k, v in p.items():
+            out[f"init_s{s}_{k}"] = v
+    if with_rng:
+        out["rng_state"] = R.rng_state()
+    R.step(steps)
+    for s in range(cfg.nspecies):
+        p = R.particles(s)
+        for k, v in p.items():
+            out[f"final_s{s}_{k}"] = v
+        out[f"losses_s{s}"] = np.array(R.losses(s)[:2], np.uint64)
+    rho, phi, E = R.fields()
+    out.update(rho=rho, phi=phi, E=E, time=R.time())
+    c, nl, per = R.collisions()
+    out.update(candidates=c, nulls=nl, per_channel=per)
+    np.savez_compressed(os.path.join(HERE, f"sim1d_{name}.npz"), **out)
+
+
+def main():
+    rng_fixture()
+    grid_fixture()
+    collide_fixture()
+    ts = W.two_stream(particles_per_beam=256, nx=32, seed=4, steps=30)
+    sim_fixture("two_stream", ts, 30)
+    rf = small_ccp()
+    rf.models = []
+    sim_fixture("rf", rf, 30)
+    hot = W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0)
+    sim_fixture("mcc", hot, 30, with_rng=True)
+    print("golden vectors written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

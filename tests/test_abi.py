@@ -1,0 +1,60 @@
+"""The C ABI library loads and exports every entry point include/*.h declares;
+host-side behaviour that needs no GPU."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import apic
+from apic import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for fn in os.listdir(inc):
+        if fn.endswith(".h"):
+            text = open(os.path.join(inc, fn)).read()
+            names |= set(re.findall(r"APIC_EXPORT\s+[\w\s\*]+?\b(apic_\w+)\s*\(", text))
+    return sorted(names)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = apic.lib()
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings_and_version():
+    lib = apic.lib()
+    assert b"sm_100a" in lib.apic_version()
+    for code in range(11):
+        assert lib.apic_status_string(code)
+
+
+@pytest.mark.skipif(apic.lib().apic_device_count() > 0, reason="checks the no-device path")
+def test_create_without_device_fails_loudly():
+    wl = W.two_stream(particles_per_beam=64, nx=16)
+    cfg, tabs = W.to_device_config(wl)
+    with pytest.raises(apic.ApicError) as e:
+        apic.Simulation1D(cfg, tabs)
+    assert e.value.status == 10  # APIC_ERR_NO_DEVICE, never a CPU fallback
+
+
+def test_workload_shapes():
+    wl = W.ccp_helium()
+    assert wl.nx == 513 and len(wl.species) == 2
+    assert all(len(s.x) == 262144 for s in wl.species)
+    assert abs(wl.dt - 1.0 / (400 * 13.56e6)) < 1e-24
+    # max_frequency * dt stays well below 1 (the reference requires <= 0.1 for swarms)
+    for m in wl.models:
+        assert m.max_frequency * wl.dt < 0.1
+    ts = W.two_stream()
+    assert ts.nx == 256 and sum(len(s.x) for s in ts.species) == 32768
+    assert np.all((ts.species[0].x >= 0) & (ts.species[0].x < ts.length))

@@ -1,0 +1,144 @@
+"""The CPU oracle against golden vectors produced by the reference itself
+(tests/golden/make_golden.py).  Bit-exact where the oracle restates the
+reference operation by operation (random numbers, particle state, fields)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from apic import workloads as W
+
+G = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(G, name))
+
+
+def test_mt19937_64_and_libstdcxx_distributions():
+    f = load("rng.npz")
+    L = po.oracle()
+    g = (C.c_uint64 * 313)()
+    L.ora_mt64_seed(C.byref(g), C.c_uint64(42))
+    raw = np.array([L.ora_mt64_next(C.byref(g)) for _ in range(1000)], np.uint64)
+    assert np.array_equal(raw, f["mt64_seed42"])
+    for kind in range(4):
+        mt = (C.c_uint64 * 313)()
+        L.ora_mt64_seed(C.byref(mt), C.c_uint64(7))
+        r = po.Rng()
+        r.kind = 0
+        r.mt = C.cast(C.byref(mt), C.c_void_p)
+        nst = (C.c_double * 2)()
+        out = []
+        for _ in range(500):
+            if kind == 0:
+                out.append(L.ora_uniform01(C.byref(r)))
+            elif kind == 1:
+                out.append(L.ora_normal_draw(C.byref(nst), C.byref(r), C.c_double(0.0), C.c_double(1.0)))
+            elif kind == 2:
+                out.append(float(L.ora_bit(C.byref(r))))
+            else:
+                out.append(L.ora_canonical(C.byref(r)))
+        assert np.array_equal(np.array(out), f["dist_seed7"][kind]), kind
+
+
+@pytest.mark.parametrize("name,dirichlet", [("periodic", 0), ("dirichlet", 1)])
+def test_deposit_solve_gather(name, dirichlet):
+    f = load(f"grid1d_{name}.npz")
+    nx, L, eps = int(f["nx"]), float(f["length"]), float(f["eps"])
+    dx = L / (nx - 1 if dirichlet else nx)
+    O = po.oracle()
+    rho = np.zeros(nx)
+    for s, key in enumerate(("x0", "x1")):
+        x = np.ascontiguousarray(f[key])
+        O.ora_deposit1d(po.dptr(rho), nx, L, dx, dirichlet, float(f["q"][s]), float(f["w"][s]), len(x), po.dptr(x),
+                        None)
+    assert np.array_equal(rho, f["rho"])
+    phi, E = np.zeros(nx), np.zeros(nx)
+    O.ora_solve1d(po.dptr(rho), po.dptr(phi), po.dptr(E), nx, L, dx, dirichlet, eps, float(f["phi_left"]),
+                  float(f["phi_right"]))
+    assert np.array_equal(phi, f["phi"])
+    assert np.array_equal(E, f["E"])
+    eq = np.array([O.ora_gather1d(po.dptr(E), nx, L, dx, dirichlet, x) for x in f["xq"]])
+    assert np.array_equal(eq, f["eq"])
+
+
+def small_ccp():
+    return W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96)
+
+
+@pytest.mark.parametrize("mi", [0, 1])
+def test_collide3(mi):
+    f = load("collide3.npz")
+    wl = small_ccp()
+    T = po.TableSet()
+    cfg = po.config_from_workload(wl, T)
+    m = cfg.models[mi]
+    O = po.oracle()
+    col = (C.c_byte * 8192)()
+    assert O.ora_collider_init(col, C.byref(m), wl.species[m.species].mass) == 0
+    v_in, seeds = f[f"m{mi}_v_in"], f[f"m{mi}_seeds"]
+    dt = float(f[f"m{mi}_dt"])
+    for i in range(len(seeds)):
+        mt = (C.c_uint64 * 313)()
+        O.ora_mt64_seed(C.byref(mt), C.c_uint64(int(seeds[i])))
+        r = po.Rng()
+        r.kind = 0
+        r.mt = C.cast(C.byref(mt), C.c_void_p)
+        st = po.CollideStats()
+        v = np.ascontiguousarray(v_in[i].copy())
+        assert O.ora_collide3(col, po.dptr(v), dt, C.byref(r), C.byref(st)) == 0
+        assert np.array_equal(v, f[f"m{mi}_v_out"][i]), i
+        assert st.candidates == f[f"m{mi}_candidates"][i]
+        assert st.null_collisions == f[f"m{mi}_nulls"][i]
+        assert list(st.channel_collisions) == list(f[f"m{mi}_channels"][i])
+        assert st.nsecondaries == f[f"m{mi}_nsec"][i]
+        assert st.draws == f[f"m{mi}_draws"][i]
+        for k in range(min(st.nsecondaries, 4)):
+            assert np.array_equal(np.array(st.secondary_velocity[k]), f[f"m{mi}_sec_v"][i][k])
+    assert f[f"m{mi}_candidates"].sum() > 100
+
+
+def _run_sim(name, wl):
+    f = load(f"sim1d_{name}.npz")
+    T = po.TableSet()
+    cfg = po.config_from_workload(wl, T, seed=2024)
+    sim = po.Sim1D(cfg, 0)
+    for s in range(cfg.nspecies):
+        sim.load(s, *[f[f"init_s{s}_{k}"] for k in ("x", "v", "vh", "vy", "vz", "alive")])
+    sim.initialize_fields(0.0, 0)
+    if "rng_state" in f.files:
+        sim.set_mt(f["rng_state"])
+    sim.step(int(f["steps"]))
+    for s in range(cfg.nspecies):
+        p = sim.particles(s)
+        for k in ("x", "v", "vh", "vy", "vz", "alive"):
+            assert np.array_equal(p[k], f[f"final_s{s}_{k}"]), (name, s, k)
+        assert sim.losses(s)[:2] == tuple(int(v) for v in f[f"losses_s{s}"])
+    rho, phi, E = sim.fields()
+    assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
+    assert sim.time() == float(f["time"])
+    return sim, f
+
+
+def test_two_stream_run_bit_exact():
+    _run_sim("two_stream", W.two_stream(particles_per_beam=256, nx=32, seed=4, steps=30))
+
+
+def test_dirichlet_rf_run_bit_exact():
+    wl = small_ccp()
+    wl.models = []
+    _run_sim("rf", wl)
+
+
+def test_mcc_run_bit_exact():
+    """Shared mt19937_64 stream, ionization products in the first dead slot."""
+    hot = W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0)
+    sim, f = _run_sim("mcc", hot)
+    c, nl, per = sim.collisions()
+    assert c == int(f["candidates"]) and nl == int(f["nulls"])
+    ref_per = f["per_channel"]
+    assert list(per[0][:3]) + list(per[1][:2]) == [int(v) for v in ref_per]
+    assert ref_per[2] > 0  # ionization happened
