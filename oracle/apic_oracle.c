@@ -808,3 +808,346 @@ double ora_sim1d_field_energy(const ora_sim1d* s) {
         fe += 0.5 * s->eps * s->E[i] * s->E[i] * node_volume(i, s->cfg.nx, s->dx, s->cfg.dirichlet);
     return fe;
 }
+
+/* ======================================================================= */
+/* Structured 2D3V / 3D3V periodic step: Mesh2D/Mesh3D deposit and gather,
+ * Boris/leapfrog pushers, FFT spectral Poisson (Simulation2D::step,
+ * src/Simulation2D.cpp:1337-1364; Simulation3D::step, src/Simulation3D.cpp:342-365). */
+
+typedef struct { double re, im; } ora_cplx;
+
+/* fft_radix2, src/FieldSolver.cpp:171-201: bit reversal, butterflies with the
+ * twiddle recurrence w *= wlen, 1/n scaling of the inverse. */
+static void fft_radix2(ora_cplx* a, size_t n, int inverse) {
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) { ora_cplx t = a[i]; a[i] = a[j]; a[j] = t; }
+    }
+    const double twopi = 2.0 * 3.14159265358979323846;
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const double angle = (inverse ? 1.0 : -1.0) * twopi / (double)len;
+        const double wr = cos(angle), wi = sin(angle);
+        for (size_t i = 0; i < n; i += len) {
+            double cr = 1.0, ci = 0.0;
+            for (size_t j = 0; j < len / 2; ++j) {
+                const ora_cplx u = a[i + j];
+                const ora_cplx x = a[i + j + len / 2];
+                /* complex<double> multiply: (x.re*cr - x.im*ci, x.re*ci + x.im*cr) */
+                const ora_cplx v = {x.re * cr - x.im * ci, x.re * ci + x.im * cr};
+                a[i + j].re = u.re + v.re; a[i + j].im = u.im + v.im;
+                a[i + j + len / 2].re = u.re - v.re; a[i + j + len / 2].im = u.im - v.im;
+                const double nr = cr * wr - ci * wi, ni = cr * wi + ci * wr;
+                cr = nr; ci = ni;
+            }
+        }
+    }
+    if (inverse) {
+        const double scale = 1.0 / (double)n;
+        for (size_t i = 0; i < n; ++i) { a[i].re *= scale; a[i].im *= scale; }
+    }
+}
+
+/* transform_2d / transform_3d, src/FieldSolver.cpp:216-265: lines along x, then y, then z */
+static void transform_nd(ora_cplx* v, const size_t* n, int dims, int inverse) {
+    const size_t nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
+    size_t mx = nx > ny ? nx : ny; if (nz > mx) mx = nz;
+    ora_cplx* line = malloc(mx * sizeof(ora_cplx));
+    for (size_t k = 0; k < nz; ++k)
+        for (size_t j = 0; j < ny; ++j) {
+            for (size_t i = 0; i < nx; ++i) line[i] = v[(k * ny + j) * nx + i];
+            fft_radix2(line, nx, inverse);
+            for (size_t i = 0; i < nx; ++i) v[(k * ny + j) * nx + i] = line[i];
+        }
+    for (size_t k = 0; k < nz; ++k)
+        for (size_t i = 0; i < nx; ++i) {
+            for (size_t j = 0; j < ny; ++j) line[j] = v[(k * ny + j) * nx + i];
+            fft_radix2(line, ny, inverse);
+            for (size_t j = 0; j < ny; ++j) v[(k * ny + j) * nx + i] = line[j];
+        }
+    if (dims == 3)
+        for (size_t j = 0; j < ny; ++j)
+            for (size_t i = 0; i < nx; ++i) {
+                for (size_t k = 0; k < nz; ++k) line[k] = v[(k * ny + j) * nx + i];
+                fft_radix2(line, nz, inverse);
+                for (size_t k = 0; k < nz; ++k) v[(k * ny + j) * nx + i] = line[k];
+            }
+    free(line);
+}
+
+/* solve_periodic_spectral(Mesh2D&/Mesh3D&), src/FieldSolver.cpp:442-499, :659-731.
+ * E holds dims components, each of N = prod(n) values. */
+void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                  double eps) {
+    const size_t nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
+    const size_t N = nx * ny * nz;
+    const double twopi = 2.0 * 3.14159265358979323846;
+    double mean = 0.0;
+    for (size_t i = 0; i < N; ++i) mean += rho[i];
+    mean /= (double)N;
+    ora_cplx* rh = malloc(N * sizeof(ora_cplx));
+    ora_cplx* out[4];
+    for (int c = 0; c <= dims; ++c) out[c] = calloc(N, sizeof(ora_cplx));
+    for (size_t i = 0; i < N; ++i) { rh[i].re = rho[i] - mean; rh[i].im = 0.0; }
+    transform_nd(rh, n, dims, 0);
+    for (size_t kz = 0; kz < nz; ++kz) {
+        const double kzm = (kz <= nz / 2) ? (double)kz : -(double)(nz - kz);
+        const double kzw = dims == 3 ? twopi * kzm / L[2] : 0.0;
+        for (size_t ky = 0; ky < ny; ++ky) {
+            const double kym = (ky <= ny / 2) ? (double)ky : -(double)(ny - ky);
+            const double kyw = twopi * kym / L[1];
+            for (size_t kx = 0; kx < nx; ++kx) {
+                if (kx == 0 && ky == 0 && kz == 0) continue;
+                const double kxm = (kx <= nx / 2) ? (double)kx : -(double)(nx - kx);
+                const double kxw = twopi * kxm / L[0];
+                const double k2 = dims == 3 ? kxw * kxw + kyw * kyw + kzw * kzw : kxw * kxw + kyw * kyw;
+                const size_t idx = (kz * ny + ky) * nx + kx;
+                const double den = eps * k2;
+                const double pr = rh[idx].re / den, pi = rh[idx].im / den;
+                out[0][idx].re = pr; out[0][idx].im = pi;
+                /* -(0,1) * k * phik = (k * pi, -(k * pr)) */
+                const double kw[3] = {kxw, kyw, kzw};
+                for (int c = 0; c < dims; ++c) {
+                    out[1 + c][idx].re = kw[c] * pi;
+                    out[1 + c][idx].im = -(kw[c] * pr);
+                }
+            }
+        }
+    }
+    for (int c = 0; c <= dims; ++c) transform_nd(out[c], n, dims, 1);
+    for (size_t i = 0; i < N; ++i) {
+        phi[i] = out[0][i].re;
+        for (int c = 0; c < dims; ++c) E[c * N + i] = out[1 + c][i].re;
+    }
+    for (int c = 0; c <= dims; ++c) free(out[c]);
+    free(rh);
+}
+
+/* Periodic CIC stencil of one axis, src/Mesh2D.cpp:96-129, src/FieldSolver.cpp:936-960 */
+static void cic_axis(double x, double L, double d, size_t n, size_t* i0, size_t* i1, double* f) {
+    const double xp = wrap(x, L);
+    const double g = xp / d;
+    const size_t i = (size_t)floor(g);
+    *f = g - (double)i;
+    *i0 = i % n;
+    *i1 = (i + 1) % n;
+}
+
+/* interpolate_electric(Mesh2D&) / (Mesh3D&), src/FieldSolver.cpp:926-1038 (periodic) */
+void ora_gather_nd(const double* E, int dims, const size_t* n, const double* L, const double* pos,
+                   double* out) {
+    const size_t nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
+    const size_t N = nx * ny * nz;
+    size_t ii[3][2];
+    double f[3];
+    for (int a = 0; a < dims; ++a)
+        cic_axis(pos[a], L[a], L[a] / (double)n[a], n[a], &ii[a][0], &ii[a][1], &f[a]);
+    if (dims == 2) {
+        const double fx = f[0], fy = f[1];
+        const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
+        const size_t i00 = ii[1][0] * nx + ii[0][0], i10 = ii[1][0] * nx + ii[0][1];
+        const size_t i01 = ii[1][1] * nx + ii[0][0], i11 = ii[1][1] * nx + ii[0][1];
+        for (int c = 0; c < 2; ++c) {
+            const double* e = E + c * N;
+            out[c] = e[i00] * w00 + e[i10] * w10 + e[i01] * w01 + e[i11] * w11;
+        }
+        return;
+    }
+    const double wx[2] = {1.0 - f[0], f[0]}, wy[2] = {1.0 - f[1], f[1]}, wz[2] = {1.0 - f[2], f[2]};
+    out[0] = out[1] = out[2] = 0.0;
+    for (int c3 = 0; c3 < 2; ++c3)
+        for (int b = 0; b < 2; ++b)
+            for (int a = 0; a < 2; ++a) {
+                const double shape = wx[a] * wy[b] * wz[c3];
+                const size_t idx = (ii[2][c3] * ny + ii[1][b]) * nx + ii[0][a];
+                for (int c = 0; c < 3; ++c) out[c] += E[c * N + idx] * shape;
+            }
+}
+
+/* deposit_charge_cic(Mesh2D&) with q = charge * weight / depth, src/Mesh2D.cpp:90-144,
+ * src/Species2D.cpp:160-170; deposit_charge_cic(Mesh3D&), src/Mesh3D.cpp:62-126 (periodic) */
+void ora_deposit_nd(double* rho, int dims, const size_t* n, const double* L, double q, size_t np,
+                    const double* pos /* dims x np */) {
+    const size_t nx = n[0], ny = n[1];
+    double d[3];
+    for (int a = 0; a < dims; ++a) d[a] = L[a] / (double)n[a];
+    const double area = d[0] * d[1];
+    const double qv = dims == 3 ? q / (d[0] * d[1] * d[2]) : 0.0;
+    for (size_t p = 0; p < np; ++p) {
+        size_t ii[3][2];
+        double f[3];
+        for (int a = 0; a < dims; ++a) cic_axis(pos[a * np + p], L[a], d[a], n[a], &ii[a][0], &ii[a][1], &f[a]);
+        if (dims == 2) {
+            const double fx = f[0], fy = f[1];
+            rho[ii[1][0] * nx + ii[0][0]] += q * (1.0 - fx) * (1.0 - fy) / area;
+            rho[ii[1][0] * nx + ii[0][1]] += q * fx * (1.0 - fy) / area;
+            rho[ii[1][1] * nx + ii[0][0]] += q * (1.0 - fx) * fy / area;
+            rho[ii[1][1] * nx + ii[0][1]] += q * fx * fy / area;
+        } else {
+            const double wx[2] = {1.0 - f[0], f[0]}, wy[2] = {1.0 - f[1], f[1]}, wz[2] = {1.0 - f[2], f[2]};
+            for (int c3 = 0; c3 < 2; ++c3)
+                for (int b = 0; b < 2; ++b)
+                    for (int a = 0; a < 2; ++a) {
+                        const double shape = wx[a] * wy[b] * wz[c3];
+                        rho[(ii[2][c3] * ny + ii[1][b]) * nx + ii[0][a]] += qv * shape;
+                    }
+        }
+    }
+}
+
+/* boris_advance, src/Pusher.cpp:20-29 */
+void ora_boris(double v[3], const double E[3], const double B[3], double qm, double dt) {
+    const double h = 0.5 * qm * dt;
+    const double vm[3] = {v[0] + h * E[0], v[1] + h * E[1], v[2] + h * E[2]};
+    const double t[3] = {h * B[0], h * B[1], h * B[2]};
+    const double t2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
+    const double sf = 2.0 / (1.0 + t2);
+    const double s[3] = {sf * t[0], sf * t[1], sf * t[2]};
+    const double vp[3] = {vm[0] + (vm[1] * t[2] - vm[2] * t[1]), vm[1] + (vm[2] * t[0] - vm[0] * t[2]),
+                          vm[2] + (vm[0] * t[1] - vm[1] * t[0])};
+    const double vq[3] = {vm[0] + (vp[1] * s[2] - vp[2] * s[1]), vm[1] + (vp[2] * s[0] - vp[0] * s[2]),
+                          vm[2] + (vp[0] * s[1] - vp[1] * s[0])};
+    v[0] = vq[0] + h * E[0];
+    v[1] = vq[1] + h * E[1];
+    v[2] = vq[2] + h * E[2];
+}
+
+struct ora_simnd {
+    int dims, nspecies, boris;
+    size_t n[3];
+    double L[3], d[3], dt, eps, B[3], q[ORA_MAX_SPECIES], m[ORA_MAX_SPECIES], w[ORA_MAX_SPECIES];
+    size_t np[ORA_MAX_SPECIES];
+    double *pos[ORA_MAX_SPECIES], *v[ORA_MAX_SPECIES], *vh[ORA_MAX_SPECIES]; /* [3][np] each */
+    double *rho, *phi, *E;
+    double time;
+};
+
+ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double dt, double eps, const double* B,
+                            int nspecies, const double* q, const double* m, const double* w_eff) {
+    ora_simnd* s = calloc(1, sizeof *s);
+    s->dims = dims;
+    s->nspecies = nspecies;
+    size_t N = 1;
+    for (int a = 0; a < 3; ++a) {
+        s->n[a] = a < dims ? n[a] : 1;
+        s->L[a] = a < dims ? L[a] : 1.0;
+        s->d[a] = s->L[a] / (double)s->n[a];
+        s->B[a] = B[a];
+        N *= s->n[a];
+    }
+    s->boris = B[0] != 0.0 || B[1] != 0.0 || B[2] != 0.0;
+    s->dt = dt;
+    s->eps = eps;
+    for (int k = 0; k < nspecies; ++k) { s->q[k] = q[k]; s->m[k] = m[k]; s->w[k] = w_eff[k]; }
+    s->rho = calloc(N, sizeof(double));
+    s->phi = calloc(N, sizeof(double));
+    s->E = calloc(3 * N, sizeof(double));
+    return s;
+}
+
+void ora_simnd_destroy(ora_simnd* s) {
+    if (!s) return;
+    for (int k = 0; k < ORA_MAX_SPECIES; ++k) { free(s->pos[k]); free(s->v[k]); free(s->vh[k]); }
+    free(s->rho); free(s->phi); free(s->E); free(s);
+}
+
+/* arrays are [3][np] (component-major); for 2D the third position row is ignored */
+void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const double* v, const double* vh) {
+    s->np[k] = np;
+    free(s->pos[k]); free(s->v[k]); free(s->vh[k]);
+    s->pos[k] = malloc(3 * np * sizeof(double));
+    s->v[k] = malloc(3 * np * sizeof(double));
+    s->vh[k] = malloc(3 * np * sizeof(double));
+    memcpy(s->pos[k], pos, 3 * np * sizeof(double));
+    memcpy(s->v[k], v, 3 * np * sizeof(double));
+    memcpy(s->vh[k], vh, 3 * np * sizeof(double));
+}
+
+static void simnd_deposit_solve(ora_simnd* s) {
+    const size_t N = s->n[0] * s->n[1] * s->n[2];
+    memset(s->rho, 0, N * sizeof(double));
+    for (int k = 0; k < s->nspecies; ++k)
+        ora_deposit_nd(s->rho, s->dims, s->n, s->L, s->q[k] * s->w[k], s->np[k], s->pos[k]);
+    ora_solve_nd(s->rho, s->phi, s->E, s->dims, s->n, s->L, s->eps);
+}
+
+static void simnd_gather(const ora_simnd* s, const double* pos, size_t np, size_t i, double e[3]) {
+    double p[3] = {pos[i], pos[np + i], s->dims == 3 ? pos[2 * np + i] : 0.0};
+    e[2] = 0.0;
+    ora_gather_nd(s->E, s->dims, s->n, s->L, p, e);
+}
+
+void ora_simnd_initialize_fields(ora_simnd* s) { simnd_deposit_solve(s); }
+
+/* initialize(): deposit_and_solve + initialize_{boris,leapfrog}_half_step */
+void ora_simnd_initialize(ora_simnd* s) {
+    simnd_deposit_solve(s);
+    for (int k = 0; k < s->nspecies; ++k) {
+        const double qm = s->q[k] / s->m[k];
+        const size_t np = s->np[k];
+        for (size_t i = 0; i < np; ++i) {
+            double e[3];
+            simnd_gather(s, s->pos[k], np, i, e);
+            double v[3] = {s->v[k][i], s->v[k][np + i], s->v[k][2 * np + i]};
+            if (s->boris) {
+                ora_boris(v, e, s->B, qm, -0.5 * s->dt);
+            } else {
+                for (int a = 0; a < s->dims; ++a) v[a] = v[a] - 0.5 * qm * e[a] * s->dt;
+            }
+            for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
+        }
+    }
+}
+
+/* apply_lower/upper_boundary with periodic particle boundaries, src/Simulation2D.cpp:57-97 */
+static double wrap_if_outside(double c, double L) { return (c >= 0.0 && c <= L) ? c : wrap(c, L); }
+
+void ora_simnd_step(ora_simnd* s, size_t steps) {
+    for (size_t it = 0; it < steps; ++it) {
+        for (int k = 0; k < s->nspecies; ++k) {
+            const double qm = s->q[k] / s->m[k];
+            const size_t np = s->np[k];
+            for (size_t i = 0; i < np; ++i) {
+                double e[3];
+                simnd_gather(s, s->pos[k], np, i, e);
+                double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};
+                if (s->boris) ora_boris(v, e, s->B, qm, s->dt);
+                else for (int a = 0; a < s->dims; ++a) v[a] += qm * e[a] * s->dt;
+                for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
+                for (int a = 0; a < s->dims; ++a) {
+                    double c = s->pos[k][a * np + i] + v[a] * s->dt;
+                    s->pos[k][a * np + i] = wrap_if_outside(c, s->L[a]);
+                }
+            }
+        }
+        simnd_deposit_solve(s);
+        for (int k = 0; k < s->nspecies; ++k) {
+            const double qm = s->q[k] / s->m[k];
+            const size_t np = s->np[k];
+            for (size_t i = 0; i < np; ++i) {
+                double e[3];
+                simnd_gather(s, s->pos[k], np, i, e);
+                double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};
+                if (s->boris) ora_boris(v, e, s->B, qm, 0.5 * s->dt);
+                else for (int a = 0; a < s->dims; ++a) v[a] = v[a] + 0.5 * qm * e[a] * s->dt;
+                for (int a = 0; a < 3; ++a) s->v[k][a * np + i] = v[a];
+            }
+        }
+        s->time += s->dt;
+    }
+}
+
+void ora_simnd_get(const ora_simnd* s, int k, double* pos, double* v, double* vh) {
+    const size_t np = s->np[k];
+    if (pos) memcpy(pos, s->pos[k], 3 * np * sizeof(double));
+    if (v) memcpy(v, s->v[k], 3 * np * sizeof(double));
+    if (vh) memcpy(vh, s->vh[k], 3 * np * sizeof(double));
+}
+
+void ora_simnd_fields(const ora_simnd* s, double* rho, double* phi, double* E) {
+    const size_t N = s->n[0] * s->n[1] * s->n[2];
+    if (rho) memcpy(rho, s->rho, N * sizeof(double));
+    if (phi) memcpy(phi, s->phi, N * sizeof(double));
+    if (E) memcpy(E, s->E, 3 * N * sizeof(double));
+}

@@ -87,6 +87,25 @@ double ora_sim1d_kinetic(const ora_sim1d* s, int species);
 double ora_sim1d_field_energy(const ora_sim1d* s);
 const char* ora_last_error(void);
 
+/* ---- structured 2D3V / 3D3V periodic -------------------------------------- */
+void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                  double eps);
+void ora_gather_nd(const double* E, int dims, const size_t* n, const double* L, const double* pos, double* out);
+void ora_deposit_nd(double* rho, int dims, const size_t* n, const double* L, double q, size_t np,
+                    const double* pos);
+void ora_boris(double v[3], const double E[3], const double B[3], double qm, double dt);
+typedef struct ora_simnd ora_simnd;
+/* w_eff: the weight that multiplies the charge in the deposit (2D: weight / depth) */
+ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double dt, double eps, const double* B,
+                            int nspecies, const double* q, const double* m, const double* w_eff);
+void ora_simnd_destroy(ora_simnd* s);
+void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const double* v, const double* vh);
+void ora_simnd_initialize_fields(ora_simnd* s);
+void ora_simnd_initialize(ora_simnd* s);
+void ora_simnd_step(ora_simnd* s, size_t steps);
+void ora_simnd_get(const ora_simnd* s, int k, double* pos, double* v, double* vh);
+void ora_simnd_fields(const ora_simnd* s, double* rho, double* phi, double* E);
+
 #ifdef __cplusplus
 }
 #endif

@@ -423,3 +423,157 @@ def config_from_workload(wl, tables: TableSet, seed=12345, threads=0, particles=
                     dt=wl.dt, species=species, models=models, phi_left=wl.phi_left, phi_right=wl.phi_right,
                     drive_left=wl.drive_left, drive_right=wl.drive_right, seed=seed, threads=threads,
                     max_particles=max(s.capacity for s in wl.species))
+
+
+# ---------------------------------------------------------------------------
+# Structured 2D3V / 3D3V periodic
+
+_SZP = C.POINTER(C.c_size_t)
+
+
+def _nd_bind():
+    L = oracle()
+    if getattr(L, "_nd_bound", False):
+        return L
+    L.ora_solve_nd.argtypes = [_DP, _DP, _DP, C.c_int, _SZP, _DP, C.c_double]
+    L.ora_gather_nd.argtypes = [_DP, C.c_int, _SZP, _DP, _DP, _DP]
+    L.ora_deposit_nd.argtypes = [_DP, C.c_int, _SZP, _DP, C.c_double, C.c_size_t, _DP]
+    L.ora_boris.argtypes = [_DP, _DP, _DP, C.c_double, C.c_double]
+    L.ora_simnd_create.restype = C.c_void_p
+    L.ora_simnd_create.argtypes = [C.c_int, _SZP, _DP, C.c_double, C.c_double, _DP, C.c_int, _DP, _DP, _DP]
+    L.ora_simnd_destroy.argtypes = [C.c_void_p]
+    L.ora_simnd_load.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP]
+    L.ora_simnd_initialize_fields.argtypes = [C.c_void_p]
+    L.ora_simnd_initialize.argtypes = [C.c_void_p]
+    L.ora_simnd_step.argtypes = [C.c_void_p, C.c_size_t]
+    L.ora_simnd_get.argtypes = [C.c_void_p, C.c_int, _DP, _DP, _DP]
+    L.ora_simnd_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+    L._nd_bound = True
+    return L
+
+
+def sizes3(n):
+    n = list(n) + [1] * (3 - len(n))
+    return (C.c_size_t * 3)(*n)
+
+
+def arr3(v):
+    v = list(v) + [1.0] * (3 - len(v))
+    return np.ascontiguousarray(v, dtype=np.float64)
+
+
+class SimND:
+    """Oracle structured periodic simulation (2D3V or 3D3V)."""
+
+    def __init__(self, dims, n, L, dt, eps, B, species):
+        """species: list of (q, m, w_eff)."""
+        Lb = _nd_bind()
+        self.dims, self.n = dims, list(n)
+        self.N = int(np.prod(n))
+        self._L = arr3(L)
+        self._B = np.ascontiguousarray(B, dtype=np.float64)
+        q = np.array([s[0] for s in species]); m = np.array([s[1] for s in species]); w = np.array([s[2] for s in species])
+        self.ns = len(species)
+        self.h = Lb.ora_simnd_create(dims, sizes3(n), dptr(self._L), dt, eps, dptr(self._B), self.ns, dptr(q),
+                                     dptr(m), dptr(w))
+        self.np = [0] * self.ns
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _nd_bind().ora_simnd_destroy(self.h)
+            self.h = None
+
+    def load(self, k, pos, v, vh):
+        pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64).reshape(3, -1))
+        v = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(3, -1))
+        vh = np.ascontiguousarray(np.asarray(vh, dtype=np.float64).reshape(3, -1))
+        self.np[k] = pos.shape[1]
+        _nd_bind().ora_simnd_load(self.h, k, pos.shape[1], dptr(pos), dptr(v), dptr(vh))
+
+    def initialize(self):
+        _nd_bind().ora_simnd_initialize(self.h)
+
+    def initialize_fields(self):
+        _nd_bind().ora_simnd_initialize_fields(self.h)
+
+    def step(self, k=1):
+        _nd_bind().ora_simnd_step(self.h, k)
+
+    def particles(self, k):
+        n = self.np[k]
+        pos, v, vh = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+        _nd_bind().ora_simnd_get(self.h, k, dptr(pos), dptr(v), dptr(vh))
+        return pos, v, vh
+
+    def fields(self):
+        rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(3 * self.N)
+        _nd_bind().ora_simnd_fields(self.h, dptr(rho), dptr(phi), dptr(E))
+        return rho, phi, E[: self.dims * self.N].reshape(self.dims, self.N)
+
+
+def _refnd_bind():
+    L = ref()
+    if getattr(L, "_nd_bound", False):
+        return L
+    L.refnd_create.argtypes = [C.c_int, _SZP, _DP, C.c_double, C.c_int, _DP, C.c_int, _DP, _DP, _DP, _SZP, _DP, _DP,
+                               C.c_uint, C.c_int, C.POINTER(C.c_void_p)]
+    L.refnd_destroy.argtypes = [C.c_void_p]
+    L.refnd_initialize.argtypes = [C.c_void_p]
+    L.refnd_step.argtypes = [C.c_void_p, C.c_size_t]
+    L.refnd_count.restype = C.c_size_t
+    L.refnd_count.argtypes = [C.c_void_p, C.c_int]
+    L.refnd_get.argtypes = [C.c_void_p, C.c_int, _DP, _DP, _DP]
+    L.refnd_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+    L.refnd_time.restype = C.c_double
+    L.refnd_time.argtypes = [C.c_void_p]
+    L.ref_solve_nd.argtypes = [C.c_int, _SZP, _DP, C.c_double, _DP, _DP, _DP]
+    L._nd_bound = True
+    return L
+
+
+class RefND:
+    """The reference's Simulation2D / Simulation3D (periodic) through the harness."""
+
+    def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0):
+        """species: list of (q, m, w, count, drift_x, thermal)."""
+        Lb = _refnd_bind()
+        self.dims, self.n, self.N = dims, list(n), int(np.prod(n))
+        cols = [np.array([s[i] for s in species], dtype=np.float64) for i in (0, 1, 2, 4, 5)]
+        counts = (C.c_size_t * len(species))(*[s[3] for s in species])
+        self._keep = cols
+        Bv = np.ascontiguousarray(B, dtype=np.float64)
+        Lv = arr3(L)
+        h = C.c_void_p()
+        rc = Lb.refnd_create(dims, sizes3(n), dptr(Lv), dt, si, dptr(Bv), len(species), dptr(cols[0]), dptr(cols[1]),
+                             dptr(cols[2]), counts, dptr(cols[3]), dptr(cols[4]), seed, threads, C.byref(h))
+        if rc:
+            raise RuntimeError(Lb.ref_last_error().decode())
+        self.h = h
+        self.ns = len(species)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _refnd_bind().refnd_destroy(self.h)
+            self.h = None
+
+    def initialize(self):
+        if _refnd_bind().refnd_initialize(self.h):
+            raise RuntimeError(ref().ref_last_error().decode())
+
+    def step(self, k=1):
+        if _refnd_bind().refnd_step(self.h, k):
+            raise RuntimeError(ref().ref_last_error().decode())
+
+    def particles(self, k):
+        n = _refnd_bind().refnd_count(self.h, k)
+        pos, v, vh = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+        _refnd_bind().refnd_get(self.h, k, dptr(pos), dptr(v), dptr(vh))
+        return pos, v, vh
+
+    def fields(self):
+        rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(self.dims * self.N)
+        _refnd_bind().refnd_fields(self.h, dptr(rho), dptr(phi), dptr(E))
+        return rho, phi, E.reshape(self.dims, self.N)
+
+    def time(self):
+        return _refnd_bind().refnd_time(self.h)

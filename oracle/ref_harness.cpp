@@ -356,3 +356,160 @@ void ref_dist(int kind, uint64_t seed, size_t n, double* out) {
 }
 
 } // extern "C"
+
+// --- structured 2D3V / 3D3V periodic ------------------------------------------
+
+namespace {
+struct RefND {
+    int dims = 2;
+    std::unique_ptr<pic::Simulation2D> s2;
+    std::unique_ptr<pic::Simulation3D> s3;
+};
+}  // namespace
+
+extern "C" {
+
+// species: q, m, w, count, drift_x, thermal (isotropic) per species
+int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, const double* B, int nspecies,
+                 const double* q, const double* m, const double* w, const size_t* count, const double* drift,
+                 const double* thermal, unsigned seed, int threads, void** out) {
+    try {
+        auto r = std::make_unique<RefND>();
+        r->dims = dims;
+        pic::RuntimePolicy rt;
+        if (threads > 0) { rt.backend = pic::RuntimeBackend::OpenMP; rt.threads = (size_t)threads; }
+        if (dims == 2) {
+            pic::Simulation2DConfig c;
+            c.units.system = si ? pic::UnitSystem::SI : pic::UnitSystem::Normalized;
+            c.nx = n[0]; c.ny = n[1]; c.length_x = L[0]; c.length_y = L[1];
+            c.dt = dt; c.boundary = pic::Boundary::Periodic;
+            c.magnetic_field_x = B[0]; c.magnetic_field_y = B[1]; c.magnetic_field_z = B[2];
+            c.seed = seed; c.runtime = rt;
+            c.output_dir = std::filesystem::temp_directory_path() / "apic_ref2d";
+            size_t mx = 0;
+            for (int s = 0; s < nspecies; ++s) {
+                pic::Species2DConfig sc;
+                sc.name = "s" + std::to_string(s);
+                sc.charge = q[s]; sc.mass = m[s]; sc.weight = w[s]; sc.particles = count[s];
+                sc.drift_velocity_x = drift[s]; sc.thermal_velocity = thermal[s];
+                c.species.push_back(sc);
+                mx = std::max(mx, count[s]);
+            }
+            c.max_particles_per_species = std::max<size_t>(mx, 10);
+            r->s2 = std::make_unique<pic::Simulation2D>(c);
+        } else {
+            pic::Simulation3DConfig c;
+            c.units.system = si ? pic::UnitSystem::SI : pic::UnitSystem::Normalized;
+            c.nx = n[0]; c.ny = n[1]; c.nz = n[2];
+            c.length_x = L[0]; c.length_y = L[1]; c.length_z = L[2];
+            c.dt = dt; c.boundary = pic::Boundary::Periodic;
+            c.magnetic_field = {B[0], B[1], B[2]};
+            c.seed = seed; c.runtime = rt;
+            c.output_dir = std::filesystem::temp_directory_path() / "apic_ref3d";
+            for (int s = 0; s < nspecies; ++s) {
+                pic::Species3DConfig sc;
+                sc.name = "s" + std::to_string(s);
+                sc.charge = q[s]; sc.mass = m[s]; sc.weight = w[s]; sc.particles = count[s];
+                sc.drift_velocity_x = drift[s]; sc.thermal_velocity = thermal[s];
+                c.species.push_back(sc);
+            }
+            r->s3 = std::make_unique<pic::Simulation3D>(c);
+        }
+        *out = r.release();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+void refnd_destroy(void* h) { delete static_cast<RefND*>(h); }
+
+int refnd_initialize(void* h) {
+    try {
+        auto* r = static_cast<RefND*>(h);
+        if (r->dims == 2) r->s2->initialize(); else r->s3->initialize();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+int refnd_step(void* h, size_t steps) {
+    try {
+        auto* r = static_cast<RefND*>(h);
+        for (size_t i = 0; i < steps; ++i) { if (r->dims == 2) r->s2->step(); else r->s3->step(); }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+size_t refnd_count(void* h, int s) {
+    auto* r = static_cast<RefND*>(h);
+    return r->dims == 2 ? r->s2->species().at(s).particles().size() : r->s3->species().at(s).particles().size();
+}
+
+// pos, v, vh: [3][count] component-major
+int refnd_get(void* h, int s, double* pos, double* v, double* vh) {
+    auto* r = static_cast<RefND*>(h);
+    const size_t n = refnd_count(h, s);
+    if (r->dims == 2) {
+        const auto& ps = r->s2->species().at(s).particles();
+        for (size_t i = 0; i < n; ++i) {
+            pos[i] = ps[i].position.x; pos[n + i] = ps[i].position.y; pos[2 * n + i] = 0.0;
+            v[i] = ps[i].velocity.x; v[n + i] = ps[i].velocity.y; v[2 * n + i] = ps[i].velocity_z;
+            vh[i] = ps[i].velocity_half.x; vh[n + i] = ps[i].velocity_half.y; vh[2 * n + i] = ps[i].velocity_half_z;
+        }
+    } else {
+        const auto& ps = r->s3->species().at(s).particles();
+        for (size_t i = 0; i < n; ++i) {
+            pos[i] = ps[i].position.x; pos[n + i] = ps[i].position.y; pos[2 * n + i] = ps[i].position.z;
+            v[i] = ps[i].velocity.x; v[n + i] = ps[i].velocity.y; v[2 * n + i] = ps[i].velocity.z;
+            vh[i] = ps[i].velocity_half.x; vh[n + i] = ps[i].velocity_half.y; vh[2 * n + i] = ps[i].velocity_half.z;
+        }
+    }
+    return 0;
+}
+
+// rho, phi: N; E: [dims][N]
+int refnd_fields(void* h, double* rho, double* phi, double* E) {
+    auto* r = static_cast<RefND*>(h);
+    if (r->dims == 2) {
+        const auto& m = r->s2->mesh();
+        const size_t N = m.rho().size();
+        std::memcpy(rho, m.rho().data(), N * 8); std::memcpy(phi, m.phi().data(), N * 8);
+        std::memcpy(E, m.electric_x().data(), N * 8); std::memcpy(E + N, m.electric_y().data(), N * 8);
+    } else {
+        const auto& m = r->s3->mesh();
+        const size_t N = m.rho().size();
+        std::memcpy(rho, m.rho().data(), N * 8); std::memcpy(phi, m.phi().data(), N * 8);
+        std::memcpy(E, m.electric_x().data(), N * 8); std::memcpy(E + N, m.electric_y().data(), N * 8);
+        std::memcpy(E + 2 * N, m.electric_z().data(), N * 8);
+    }
+    return 0;
+}
+
+double refnd_time(void* h) {
+    auto* r = static_cast<RefND*>(h);
+    return r->dims == 2 ? r->s2->time() : r->s3->time();
+}
+
+// FieldSolver::solve(Mesh2D&/Mesh3D&) on a given charge density (periodic).
+int ref_solve_nd(int dims, const size_t* n, const double* L, double eps, const double* rho, double* phi, double* E) {
+    try {
+        pic::FieldSolver solver(eps);
+        if (dims == 2) {
+            pic::Mesh2D mesh(n[0], n[1], L[0], L[1], pic::Boundary::Periodic);
+            std::memcpy(mesh.rho().data(), rho, n[0] * n[1] * 8);
+            solver.solve(mesh);
+            const size_t N = n[0] * n[1];
+            std::memcpy(phi, mesh.phi().data(), N * 8);
+            std::memcpy(E, mesh.electric_x().data(), N * 8); std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+        } else {
+            pic::Mesh3D mesh(n[0], n[1], n[2], L[0], L[1], L[2], pic::Boundary::Periodic);
+            const size_t N = n[0] * n[1] * n[2];
+            std::memcpy(mesh.rho().data(), rho, N * 8);
+            solver.solve(mesh);
+            std::memcpy(phi, mesh.phi().data(), N * 8);
+            std::memcpy(E, mesh.electric_x().data(), N * 8); std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+            std::memcpy(E + 2 * N, mesh.electric_z().data(), N * 8);
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+}  // extern "C"

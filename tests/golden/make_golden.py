@@ -121,7 +121,36 @@ def sim_fixture(name, wl, steps, with_rng=False):
     np.savez_compressed(os.path.join(HERE, f"sim1d_{name}.npz"), **out)
 
 
+ND_CASES = {
+    # name: dims, cells, B, steps
+    "sim2d_boris": (2, (16, 8), (0.0, 0.0, 0.7), 25),
+    "sim2d_leapfrog": (2, (8, 8), (0.0, 0.0, 0.0), 25),
+    "sim3d_boris": (3, (8, 4, 8), (0.3, 0.0, 0.0), 25),
+}
+ND_SPECIES = [(-1.0, 1.0, 0.05, 400, 0.3, 0.4), (1.0, 50.0, 0.05, 400, 0.0, 0.05)]
+
+
+def nd_fixture(name):
+    dims, n, B, steps = ND_CASES[name]
+    L = [1.3 * ni for ni in n]
+    R = po.RefND(dims, n, L, 0.1, 0, B, ND_SPECIES, seed=9)
+    R.initialize()
+    out = {"steps": steps}
+    for k in range(len(ND_SPECIES)):
+        for key, arr in zip(("pos", "v", "vh"), R.particles(k)):
+            out[f"init_s{k}_{key}"] = arr
+    R.step(steps)
+    for k in range(len(ND_SPECIES)):
+        for key, arr in zip(("pos", "v", "vh"), R.particles(k)):
+            out[f"final_s{k}_{key}"] = arr
+    rho, phi, E = R.fields()
+    out.update(rho=rho, phi=phi, E=E, time=R.time())
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
 def main():
+    for name in ND_CASES:
+        nd_fixture(name)
     rng_fixture()
     grid_fixture()
     collide_fixture()

@@ -142,3 +142,30 @@ def test_mcc_run_bit_exact():
     ref_per = f["per_channel"]
     assert list(per[0][:3]) + list(per[1][:2]) == [int(v) for v in ref_per]
     assert ref_per[2] > 0  # ionization happened
+
+
+ND_CASES = {
+    "sim2d_boris": (2, (16, 8), (0.0, 0.0, 0.7)),
+    "sim2d_leapfrog": (2, (8, 8), (0.0, 0.0, 0.0)),
+    "sim3d_boris": (3, (8, 4, 8), (0.3, 0.0, 0.0)),
+}
+ND_SPECIES = [(-1.0, 1.0, 0.05), (1.0, 50.0, 0.05)]
+
+
+@pytest.mark.parametrize("name", sorted(ND_CASES))
+def test_structured_periodic_run_bit_exact(name):
+    """Simulation2D / Simulation3D with Boris or leapfrog pushers, CIC deposit,
+    FFT spectral Poisson: 25 steps, bit-exact."""
+    dims, n, B = ND_CASES[name]
+    f = load(f"{name}.npz")
+    L = [1.3 * ni for ni in n]
+    sim = po.SimND(dims, n, L, 0.1, 1.0, B, ND_SPECIES)
+    for k in range(2):
+        sim.load(k, f[f"init_s{k}_pos"], f[f"init_s{k}_v"], f[f"init_s{k}_vh"])
+    sim.initialize_fields()
+    sim.step(int(f["steps"]))
+    for k in range(2):
+        for key, arr in zip(("pos", "v", "vh"), sim.particles(k)):
+            assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
+    rho, phi, E = sim.fields()
+    assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
