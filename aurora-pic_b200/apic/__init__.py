@@ -350,3 +350,177 @@ def collide3(model: MccModel, particle_mass, v3, dt, draws=None, offsets=None, s
         dp = op = None
     _check(lib().apic_collide3(C.byref(model), particle_mass, n, dptr(v3), dt, dp, op, seed, step, stream, stats))
     return v3, stats
+
+
+# ---------------------------------------------------------------------------
+# Structured 2D3V / 3D3V periodic simulation
+
+
+class ConfigND(C.Structure):
+    _fields_ = [
+        ("dims", C.c_int), ("n", C.c_size_t * 3), ("length", C.c_double * 3), ("dt", C.c_double),
+        ("units", C.c_int), ("relative_permittivity", C.c_double), ("magnetic_field", C.c_double * 3),
+        ("out_of_plane_depth", C.c_double), ("precision", C.c_int), ("sort_interval", C.c_size_t),
+        ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
+    ]
+
+
+class SampleND(C.Structure):
+    _fields_ = [
+        ("step", C.c_uint64), ("time", C.c_double), ("kinetic_energy", C.c_double), ("field_energy", C.c_double),
+        ("total_energy", C.c_double), ("charge_l1", C.c_double), ("live_particles", C.c_uint64),
+        ("kinetic_by_species", C.c_double * MAX_SPECIES),
+    ]
+
+
+_SZP = C.POINTER(C.c_size_t)
+
+
+def _bind_nd():
+    L = lib()
+    if getattr(L, "_nd_bound", False):
+        return L
+    L.apic_simnd_create.argtypes = [C.POINTER(ConfigND), C.POINTER(C.c_void_p)]
+    L.apic_simnd_destroy.argtypes = [C.c_void_p]
+    L.apic_simnd_last_error.restype = C.c_char_p
+    L.apic_simnd_last_error.argtypes = [C.c_void_p]
+    L.apic_simnd_load_particles.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP]
+    L.apic_simnd_initialize.argtypes = [C.c_void_p]
+    L.apic_simnd_resume.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
+    L.apic_simnd_step.argtypes = [C.c_void_p, C.c_size_t]
+    L.apic_simnd_synchronize.argtypes = [C.c_void_p]
+    L.apic_simnd_count.argtypes = [C.c_void_p, C.c_int, _SZP]
+    L.apic_simnd_read_particles.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _SZP]
+    L.apic_simnd_read_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
+    L.apic_simnd_sample.argtypes = [C.c_void_p, C.POINTER(SampleND)]
+    L.apic_simnd_cuda_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+    L.apic_simnd_set_kernel_timing.argtypes = [C.c_void_p, C.c_int]
+    L.apic_simnd_kernel_times.argtypes = [C.c_void_p, _DP, _DP, _DP, _U64P]
+    L.apic_field_solve_periodic_nd.argtypes = [C.c_int, _SZP, _DP, C.c_double, _DP, _DP, _DP]
+    L._nd_bound = True
+    return L
+
+
+def _check_nd(rc, handle=None):
+    if rc != 0:
+        msg = _bind_nd().apic_simnd_last_error(handle).decode() if handle is not None else ""
+        if not msg:
+            msg = _bind_nd().apic_simnd_last_error(None).decode()
+        raise ApicError(rc, msg)
+
+
+def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), units=NORMALIZED,
+              relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16) -> ConfigND:
+    c = ConfigND()
+    c.dims = dims
+    c.n[:] = list(n) + [1] * (3 - len(n))
+    c.length[:] = list(length) + [1.0] * (3 - len(length))
+    c.dt, c.units, c.relative_permittivity = dt, units, relative_permittivity
+    c.magnetic_field[:] = list(magnetic_field)
+    c.out_of_plane_depth, c.precision, c.sort_interval = out_of_plane_depth, precision, sort_interval
+    c.nspecies = len(species)
+    for i, (q, m, w, cap) in enumerate(species):
+        c.species[i] = SpeciesCfg(q, m, w, cap)
+    return c
+
+
+class SimulationND:
+    """pic::Simulation2D / Simulation3D (fully periodic) on the device."""
+
+    def __init__(self, cfg: ConfigND):
+        self.cfg = cfg
+        self.dims = cfg.dims
+        self.N = int(np.prod([cfg.n[a] for a in range(cfg.dims)]))
+        h = C.c_void_p()
+        rc = _bind_nd().apic_simnd_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise ApicError(rc, _bind_nd().apic_simnd_last_error(None).decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _bind_nd().apic_simnd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load(self, species, pos, v, v_half=None):
+        pos = np.ascontiguousarray(np.asarray(pos, dtype=np.float64)[: self.dims])
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        vh = None if v_half is None else np.ascontiguousarray(v_half, dtype=np.float64)
+        n = pos.shape[1]
+        _check_nd(_bind_nd().apic_simnd_load_particles(self.h, species, n, dptr(pos), dptr(v), dptr(vh)), self.h)
+
+    def initialize(self):
+        _check_nd(_bind_nd().apic_simnd_initialize(self.h), self.h)
+
+    def resume(self, time, step):
+        _check_nd(_bind_nd().apic_simnd_resume(self.h, time, step), self.h)
+
+    def step(self, n=1):
+        _check_nd(_bind_nd().apic_simnd_step(self.h, n), self.h)
+
+    def synchronize(self):
+        _check_nd(_bind_nd().apic_simnd_synchronize(self.h), self.h)
+
+    def count(self, species):
+        n = C.c_size_t()
+        _check_nd(_bind_nd().apic_simnd_count(self.h, species, C.byref(n)), self.h)
+        return n.value
+
+    def particles(self, species):
+        n = self.count(species)
+        pos, v, vh = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
+        got = C.c_size_t()
+        _check_nd(_bind_nd().apic_simnd_read_particles(self.h, species, n, dptr(pos), dptr(v), dptr(vh), C.byref(got)),
+                  self.h)
+        return pos, v, vh
+
+    def fields(self):
+        rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(self.dims * self.N)
+        _check_nd(_bind_nd().apic_simnd_read_fields(self.h, dptr(rho), dptr(phi), dptr(E)), self.h)
+        return rho, phi, E.reshape(self.dims, self.N)
+
+    def sample(self) -> SampleND:
+        s = SampleND()
+        _check_nd(_bind_nd().apic_simnd_sample(self.h, C.byref(s)), self.h)
+        return s
+
+    def cuda_stream(self) -> int:
+        ptr = C.c_void_p()
+        _check_nd(_bind_nd().apic_simnd_cuda_stream(self.h, C.byref(ptr)), self.h)
+        return ptr.value or 0
+
+    def set_kernel_timing(self, enable: bool):
+        _check_nd(_bind_nd().apic_simnd_set_kernel_timing(self.h, int(enable)), self.h)
+
+    def kernel_times(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        n = C.c_uint64()
+        _check_nd(_bind_nd().apic_simnd_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(n)), self.h)
+        return a.value, b.value, c.value, n.value
+
+
+def field_solve_periodic_nd(dims, n, length, permittivity, rho):
+    N = int(np.prod(n[:dims]))
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    phi, E = np.zeros(N), np.zeros(dims * N)
+    ns = (C.c_size_t * 3)(*(list(n) + [1] * (3 - len(n))))
+    Lv = np.ascontiguousarray(list(length) + [1.0] * (3 - len(length)), dtype=np.float64)
+    _check_nd(_bind_nd().apic_field_solve_periodic_nd(dims, ns, dptr(Lv), permittivity, dptr(rho), dptr(phi), dptr(E)))
+    return phi, E.reshape(dims, N)
+
+
+def _simnd_load_maxwellian(self, species, n, seed, thermal_speed, drift_x=0.0, perturb_axis=0, perturb_amplitude=0.0):
+    L = _bind_nd()
+    L.apic_simnd_load_maxwellian.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_double, C.c_double,
+                                             C.c_int, C.c_double]
+    _check_nd(L.apic_simnd_load_maxwellian(self.h, species, n, seed, thermal_speed, drift_x, perturb_axis,
+                                           perturb_amplitude), self.h)
+
+
+SimulationND.load_maxwellian = _simnd_load_maxwellian

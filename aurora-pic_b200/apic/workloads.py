@@ -184,3 +184,72 @@ def to_device_config(wl: Workload1D, precision=0, seed=1):
                    phi_left=wl.phi_left, phi_right=wl.phi_right, drive_left=wl.drive_left,
                    drive_right=wl.drive_right, precision=precision, seed=seed)
     return cfg, tabs
+
+
+# ---------------------------------------------------------------------------
+# Structured periodic plasmas (2D3V with Bz, 3D3V with Bx)
+
+@dataclass
+class WorkloadND:
+    name: str
+    dims: int
+    n: tuple
+    length: tuple
+    dt: float
+    B: tuple
+    species: list  # (charge, mass, weight, pos[3][np], v[3][np])
+    si: bool = True
+    steps: int = 100
+
+    @property
+    def particles(self) -> int:
+        return sum(s[3].shape[1] for s in self.species)
+
+
+def _plasma_nd(dims, cells, ppc, te_ev, ti_ev, mass_ratio, B, modes, n0, seed, steps, name, dt_wpe=0.1):
+    """Maxwellian electrons and ions, cell size = Debye length at (n0, Te),
+    density perturbed by 1e-3 cos(k . x) on the given modes (position
+    displacement, like the two-stream loading)."""
+    rng = np.random.default_rng(seed)
+    lam = math.sqrt(EPS0 * te_ev * E_CHARGE / (n0 * E_CHARGE ** 2))
+    wpe = math.sqrt(n0 * E_CHARGE ** 2 / (EPS0 * M_E))
+    L = tuple(c * lam for c in cells)
+    ncell = int(np.prod(cells))
+    npart = ppc * ncell
+    volume = float(np.prod(L))
+    w = n0 * volume / npart
+    species = []
+    for q, m, t_ev in ((-E_CHARGE, M_E, te_ev), (E_CHARGE, M_E * mass_ratio, ti_ev)):
+        pos = np.zeros((3, npart))
+        for a in range(dims):
+            pos[a] = rng.uniform(0.0, L[a], npart)
+        for mode in modes:
+            a = mode
+            k = 2 * math.pi / L[a]
+            pos[a] = np.mod(pos[a] + 1e-3 / k * np.sin(k * pos[a]), L[a])
+        vt = math.sqrt(t_ev * E_CHARGE / m)
+        v = vt * rng.standard_normal((3, npart))
+        species.append((q, m, w, pos, v))
+    return WorkloadND(name, dims, tuple(cells), L, dt_wpe / wpe, B, species, steps=steps)
+
+
+def plasma_2d(cells=(512, 512), ppc=64, seed=11, steps=500):
+    """2D3V periodic plasma, uniform Bz = 0.01 T: cell = lambda_D at
+    n0 = 1e16 m^-3 and Te = 2 eV, Ti = 0.03 eV, m_i/m_e = 1836,
+    1e-3 perturbation on the lowest kx and ky modes, dt = 0.1 / omega_pe."""
+    return _plasma_nd(2, cells, ppc, 2.0, 0.03, 1836.0, (0.0, 0.0, 0.01), (0, 1), 1e16, seed, steps,
+                      "plasma_2d3v_bz")
+
+
+def plasma_3d(cells=(256, 256, 256), ppc=8, seed=13, steps=200):
+    """3D3V periodic Langmuir oscillation, uniform Bx = 0.005 T: Te = 1 eV,
+    m_i/m_e = 1836, 1e-3 perturbation on mode (1,0,0), dt = 0.1 / omega_pe."""
+    return _plasma_nd(3, cells, ppc, 1.0, 0.025, 1836.0, (0.005, 0.0, 0.0), (0,), 1e16, seed, steps,
+                      "plasma_3d3v_bx")
+
+
+def to_device_config_nd(wl: WorkloadND, precision=0, capacity_factor=1.0, sort_interval=16):
+    from . import SI, NORMALIZED, config_nd
+    sp = [(q, m, w, int(pos.shape[1] * capacity_factor) + 1) for (q, m, w, pos, v) in wl.species]
+    return config_nd(dims=wl.dims, n=wl.n, length=wl.length, dt=wl.dt, species=sp, magnetic_field=wl.B,
+                     units=SI if wl.si else NORMALIZED, precision=precision, sort_interval=sort_interval)

@@ -1,0 +1,1302 @@
+// Structured 2D3V / 3D3V periodic electrostatic PIC step on one B200 (FP64 form).
+//
+// Replaces Simulation2D::step / Simulation3D::step for fully periodic meshes
+// (src/Simulation2D.cpp:1337-1364, src/Simulation3D.cpp:342-365) and what they
+// call: interpolate_electric(Mesh2D&/Mesh3D&) (src/FieldSolver.cpp:926-1038),
+// kick_boris / kick_leapfrog / drift_leapfrog (src/Pusher.cpp:82-186), the
+// periodic particle boundaries (src/Simulation2D.cpp:57-97),
+// deposit_charge_cic (src/Mesh2D.cpp:90-144, src/Mesh3D.cpp:62-126) and
+// solve_periodic_spectral (src/FieldSolver.cpp:442-499, :659-731).
+//
+// One step: a push kernel per species (gather from an interleaved E grid,
+// Boris or leapfrog kick, drift, periodic wrap, CIC deposit into a 64-bit
+// fixed-point density with global atomics), then the spectral solve as line
+// FFTs in shared memory: forward along x (reading and clearing the fixed-point
+// density), [forward along y,] forward along the last axis fused with the
+// k-space multiply and the first inverse transform, [inverse along y,] and an
+// inverse along x that writes phi and the interleaved E field.  Particles are
+// re-sorted by cell every `sort_interval` steps so gathers and atomics stay
+// local.  Compiled with --fmad=false: particle arithmetic follows the
+// reference operation by operation.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "apic_common.cuh"
+#include "apic_rng.cuh"
+
+namespace apic {
+namespace nd {
+
+constexpr int kThreads = 256;
+constexpr int kMaxLine = 1024;
+
+struct Cplx {
+    double re, im;
+};
+
+struct SpeciesND {
+    double qm;
+    double dep;   // charge * weight (/ depth in 2D) times the inverse cell area/volume
+    double hmw;   // 0.5 * mass * weight
+    unsigned n;
+    double* pos[2][3];
+    double* vh[2][3];
+    unsigned* id[2];
+    double* v[3];
+};
+
+struct ParamsND {
+    int dims;
+    int n[3];
+    double L[3], d[3];
+    double dt, eps;
+    double B[3];
+    double rho_scale, inv_rho_scale;
+    const double* E;  // interleaved: 2 doubles per node (2D) or 4 (3D)
+    unsigned long long* rho_acc;
+};
+
+// wrap_periodic, src/FieldSolver.cpp:15-17, with the exact fast branch for |x| < 2L
+__device__ __forceinline__ double wrap_periodic(double x, double L) {
+    if (!(fabs(x) < 2.0 * L)) return fmod(fmod(x, L) + L, L);
+    const double r = x >= L ? x - L : (x <= -L ? x + L : x);
+    const double y = r + L;
+    return y >= 2.0 * L ? 0.0 : (y >= L ? y - L : y);
+}
+
+struct Axis {
+    int i0, i1;
+    double f;
+};
+
+// One axis of the periodic CIC stencil, src/Mesh2D.cpp:96-114, src/FieldSolver.cpp:936-960
+__device__ __forceinline__ Axis axis(double x, double L, double d, int n) {
+    const double xp = wrap_periodic(x, L);
+    const double g = xp / d;
+    const unsigned long long i = (unsigned long long)floor(g);
+    Axis a;
+    a.f = g - (double)i;
+    a.i0 = (int)(i % (unsigned long long)n);
+    a.i1 = (int)((i + 1) % (unsigned long long)n);
+    return a;
+}
+
+template <int DIM>
+__device__ __forceinline__ void gather(const ParamsND& p, const double pos[3], double e[3]) {
+    const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
+    const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+    const int nx = p.n[0];
+    if (DIM == 2) {
+        const double fx = ax.f, fy = ay.f;
+        const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy);
+        const double w01 = (1.0 - fx) * fy, w11 = fx * fy;
+        const double2* E2 = reinterpret_cast<const double2*>(p.E);
+        const double2 e00 = __ldg(E2 + ay.i0 * nx + ax.i0), e10 = __ldg(E2 + ay.i0 * nx + ax.i1);
+        const double2 e01 = __ldg(E2 + ay.i1 * nx + ax.i0), e11 = __ldg(E2 + ay.i1 * nx + ax.i1);
+        e[0] = e00.x * w00 + e10.x * w10 + e01.x * w01 + e11.x * w11;
+        e[1] = e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11;
+        e[2] = 0.0;
+    } else {
+        const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+        const double wx[2] = {1.0 - ax.f, ax.f}, wy[2] = {1.0 - ay.f, ay.f}, wz[2] = {1.0 - az.f, az.f};
+        const int ii[2] = {ax.i0, ax.i1}, jj[2] = {ay.i0, ay.i1}, kk[2] = {az.i0, az.i1};
+        const double4* E4 = reinterpret_cast<const double4*>(p.E);
+        e[0] = e[1] = e[2] = 0.0;
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const double shape = wx[a] * wy[b] * wz[c];
+                    const double4 ev = E4[((size_t)kk[c] * p.n[1] + jj[b]) * nx + ii[a]];
+                    e[0] += ev.x * shape;
+                    e[1] += ev.y * shape;
+                    e[2] += ev.z * shape;
+                }
+    }
+}
+
+// boris_advance, src/Pusher.cpp:20-29
+__device__ __forceinline__ void boris(double v[3], const double E[3], const double B[3], double qm, double dt) {
+    const double h = 0.5 * qm * dt;
+    const double vm0 = v[0] + h * E[0], vm1 = v[1] + h * E[1], vm2 = v[2] + h * E[2];
+    const double t0 = h * B[0], t1 = h * B[1], t2v = h * B[2];
+    const double t2 = t0 * t0 + t1 * t1 + t2v * t2v;
+    const double sf = 2.0 / (1.0 + t2);
+    const double s0 = sf * t0, s1 = sf * t1, s2 = sf * t2v;
+    const double vp0 = vm0 + (vm1 * t2v - vm2 * t1);
+    const double vp1 = vm1 + (vm2 * t0 - vm0 * t2v);
+    const double vp2 = vm2 + (vm0 * t1 - vm1 * t0);
+    const double vq0 = vm0 + (vp1 * s2 - vp2 * s1);
+    const double vq1 = vm1 + (vp2 * s0 - vp0 * s2);
+    const double vq2 = vm2 + (vp0 * s1 - vp1 * s0);
+    v[0] = vq0 + h * E[0];
+    v[1] = vq1 + h * E[1];
+    v[2] = vq2 + h * E[2];
+}
+
+template <int DIM>
+__device__ __forceinline__ void deposit(const ParamsND& p, const SpeciesND& S, const double pos[3]) {
+    const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
+    const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+    const int nx = p.n[0];
+    if (DIM == 2) {
+        // q (1 - fx)(1 - fy) / node_area, src/Mesh2D.cpp:131-142 (reciprocal area inside the fixed-point rounding)
+        const double fx = ax.f, fy = ay.f;
+        const double c00 = S.dep * (1.0 - fx) * (1.0 - fy), c10 = S.dep * fx * (1.0 - fy);
+        const double c01 = S.dep * (1.0 - fx) * fy, c11 = S.dep * fx * fy;
+        atomicAdd(p.rho_acc + ay.i0 * nx + ax.i0, (unsigned long long)to_fixed(c00, p.rho_scale));
+        atomicAdd(p.rho_acc + ay.i0 * nx + ax.i1, (unsigned long long)to_fixed(c10, p.rho_scale));
+        atomicAdd(p.rho_acc + ay.i1 * nx + ax.i0, (unsigned long long)to_fixed(c01, p.rho_scale));
+        atomicAdd(p.rho_acc + ay.i1 * nx + ax.i1, (unsigned long long)to_fixed(c11, p.rho_scale));
+    } else {
+        // q_over_volume * shape, src/Mesh3D.cpp:110-122
+        const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+        const double wx[2] = {1.0 - ax.f, ax.f}, wy[2] = {1.0 - ay.f, ay.f}, wz[2] = {1.0 - az.f, az.f};
+        const int ii[2] = {ax.i0, ax.i1}, jj[2] = {ay.i0, ay.i1}, kk[2] = {az.i0, az.i1};
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int b = 0; b < 2; ++b)
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const double shape = wx[a] * wy[b] * wz[c];
+                    atomicAdd(p.rho_acc + ((size_t)kk[c] * p.n[1] + jj[b]) * nx + ii[a],
+                              (unsigned long long)to_fixed(S.dep * shape, p.rho_scale));
+                }
+    }
+}
+
+// CIC deposit of a warp's particles with one atomic per node per run of lanes
+// that share a cell: particles are sorted by cell, so neighbouring lanes mostly
+// hit the same 2^DIM nodes.  Each lane's fixed-point contributions are summed
+// over its run with a segmented shuffle scan (integer, so the total does not
+// depend on the order), and the run's last lane commits them.  All 32 lanes
+// must call this; `valid` marks lanes that carry a particle.
+template <int DIM>
+__device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND& S, const double pos[3], bool valid) {
+    constexpr int K = DIM == 2 ? 4 : 8;
+    const int lane = threadIdx.x & 31;
+    long long a[K];
+    size_t node[K];
+    unsigned cell = 0xFFFFFFFFu;
+    if (valid) {
+        const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
+        const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+        const int nx = p.n[0];
+        if (DIM == 2) {
+            const double fx = ax.f, fy = ay.f;
+            a[0] = to_fixed(S.dep * (1.0 - fx) * (1.0 - fy), p.rho_scale);
+            a[1] = to_fixed(S.dep * fx * (1.0 - fy), p.rho_scale);
+            a[2] = to_fixed(S.dep * (1.0 - fx) * fy, p.rho_scale);
+            a[3] = to_fixed(S.dep * fx * fy, p.rho_scale);
+            node[0] = (size_t)ay.i0 * nx + ax.i0;
+            node[1] = (size_t)ay.i0 * nx + ax.i1;
+            node[2] = (size_t)ay.i1 * nx + ax.i0;
+            node[3] = (size_t)ay.i1 * nx + ax.i1;
+            cell = (unsigned)node[0];
+        } else {
+            const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+            const double wx[2] = {1.0 - ax.f, ax.f}, wy[2] = {1.0 - ay.f, ay.f}, wz[2] = {1.0 - az.f, az.f};
+            const int ii[2] = {ax.i0, ax.i1}, jj[2] = {ay.i0, ay.i1}, kk[2] = {az.i0, az.i1};
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int k = (c * 2 + b) * 2 + q;
+                        a[k] = to_fixed(S.dep * (wx[q] * wy[b] * wz[c]), p.rho_scale);
+                        node[k] = ((size_t)kk[c] * p.n[1] + jj[b]) * nx + ii[q];
+                    }
+            cell = (unsigned)node[0];
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < K; ++k) { a[k] = 0; node[k] = 0; }
+    }
+    const unsigned up = __shfl_up_sync(0xffffffffu, cell, 1);
+    const bool head = lane == 0 || up != cell;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const unsigned upto = lane == 31 ? heads : (heads & ((2u << lane) - 1u));
+    const int start = 31 - __clz(upto);
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        long long v = a[k];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const long long t = __shfl_up_sync(0xffffffffu, v, d);
+            if (lane - d >= start) v += t;
+        }
+        if (tail && valid) atomicAdd(p.rho_acc + node[k], (unsigned long long)v);
+    }
+}
+
+enum : int { kPushStep = 0, kPushDepositOnly = 1, kPushInitHalf = 2, kPushSync = 3 };
+
+// One particle per thread.  Modes: a full step (kick, drift, wrap, deposit),
+// deposit only (initialize/resume), half-step initialisation from v
+// (initialize_{boris,leapfrog}_half_step) and synchronisation into v.
+template <int DIM, bool BORIS, int MODE>
+__global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int buf) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = i < S.n;
+    if (MODE == kPushInitHalf || MODE == kPushSync) {
+        if (!valid) return;
+    } else if (blockIdx.x * kThreads + (threadIdx.x & ~31u) >= S.n) {
+        return;  // whole warp past the end
+    }
+    const unsigned j = valid ? i : 0u;
+    double pos[3] = {S.pos[buf][0][j], S.pos[buf][1][j], DIM == 3 ? S.pos[buf][2][j] : 0.0};
+    if (MODE == kPushDepositOnly) {
+        deposit_warp<DIM>(p, S, pos, valid);
+        return;
+    }
+    double e[3];
+    gather<DIM>(p, pos, e);
+    if (MODE == kPushInitHalf) {
+        double v[3] = {S.v[0][i], S.v[1][i], S.v[2][i]};
+        if (BORIS) {
+            boris(v, e, p.B, S.qm, -0.5 * p.dt);
+        } else {
+            // initialize_leapfrog_half_step, src/Pusher.cpp:88-92, :152-156
+            for (int a = 0; a < DIM; ++a) v[a] = v[a] - 0.5 * S.qm * e[a] * p.dt;
+        }
+        for (int a = 0; a < 3; ++a) S.vh[buf][a][i] = v[a];
+        return;
+    }
+    double vh[3] = {S.vh[buf][0][j], S.vh[buf][1][j], S.vh[buf][2][j]};
+    if (MODE == kPushSync) {
+        if (BORIS) {
+            boris(vh, e, p.B, S.qm, 0.5 * p.dt);
+        } else {
+            // synchronize_leapfrog, src/Pusher.cpp:131-135, :176-180
+            for (int a = 0; a < DIM; ++a) vh[a] = vh[a] + 0.5 * S.qm * e[a] * p.dt;
+        }
+        for (int a = 0; a < 3; ++a) S.v[a][i] = vh[a];
+        return;
+    }
+    // kick_boris / kick_leapfrog + drift_leapfrog, src/Pusher.cpp:109-128, :162-174
+    if (BORIS) {
+        boris(vh, e, p.B, S.qm, p.dt);
+    } else {
+        for (int a = 0; a < DIM; ++a) vh[a] += S.qm * e[a] * p.dt;
+    }
+    for (int a = 0; a < DIM; ++a) {
+        const double c = pos[a] + vh[a] * p.dt;
+        // periodic particle boundary: wrap only outside [0, L], src/Simulation2D.cpp:57-97
+        pos[a] = (c >= 0.0 && c <= p.L[a]) ? c : wrap_periodic(c, p.L[a]);
+    }
+    if (valid) {
+        for (int a = 0; a < DIM; ++a) S.pos[buf][a][i] = pos[a];
+        for (int a = 0; a < 3; ++a) S.vh[buf][a][i] = vh[a];
+    }
+    deposit_warp<DIM>(p, S, pos, valid);
+}
+
+// ---- particle sort by cell -------------------------------------------------------
+
+template <int DIM>
+__device__ __forceinline__ unsigned cell_of(const ParamsND& p, const double pos[3]) {
+    const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
+    const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+    unsigned c = (unsigned)ay.i0 * p.n[0] + ax.i0;
+    if (DIM == 3) {
+        const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+        c += (unsigned)az.i0 * p.n[0] * p.n[1];
+    }
+    return c;
+}
+
+template <int DIM>
+__global__ void k_cell_hist(ParamsND p, SpeciesND S, int buf, unsigned* count) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= S.n) return;
+    const double pos[3] = {S.pos[buf][0][i], S.pos[buf][1][i], DIM == 3 ? S.pos[buf][2][i] : 0.0};
+    atomicAdd(count + cell_of<DIM>(p, pos), 1u);
+}
+
+// exclusive scan of `count` (n entries) into `offset`, three launches
+constexpr int kScanItems = 8;
+constexpr int kScanBlock = kThreads * kScanItems;
+__global__ void k_scan_local(const unsigned* count, unsigned* offset, unsigned* block_sums, unsigned n) {
+    __shared__ unsigned s[kThreads];
+    const unsigned base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    unsigned v[kScanItems], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? count[base + k] : 0u;
+        sum += v[k];
+    }
+    s[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < kThreads; o <<= 1) {
+        const unsigned y = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
+        __syncthreads();
+        s[threadIdx.x] += y;
+        __syncthreads();
+    }
+    unsigned run = s[threadIdx.x] - sum;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) offset[base + k] = run;
+        run += v[k];
+    }
+    if (threadIdx.x == kThreads - 1) block_sums[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void k_scan_blocks(unsigned* block_sums, unsigned nblocks) {
+    // one CTA: exclusive scan in place (nblocks <= kThreads * kScanItems * kThreads handled by a loop)
+    __shared__ unsigned s[kThreads];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (unsigned b0 = 0; b0 < nblocks; b0 += kThreads) {
+        const unsigned i = b0 + threadIdx.x;
+        const unsigned v = i < nblocks ? block_sums[i] : 0u;
+        s[threadIdx.x] = v;
+        __syncthreads();
+        for (int o = 1; o < kThreads; o <<= 1) {
+            const unsigned y = threadIdx.x >= (unsigned)o ? s[threadIdx.x - o] : 0u;
+            __syncthreads();
+            s[threadIdx.x] += y;
+            __syncthreads();
+        }
+        const unsigned c = carry;
+        if (i < nblocks) block_sums[i] = c + s[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == kThreads - 1) carry = c + s[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_add(unsigned* offset, const unsigned* block_sums, unsigned n) {
+    const unsigned base = blockIdx.x * kScanBlock;
+    const unsigned add = block_sums[blockIdx.x];
+    for (unsigned k = threadIdx.x; k < (unsigned)kScanBlock; k += kThreads)
+        if (base + k < n) offset[base + k] += add;
+}
+
+template <int DIM>
+__global__ void k_cell_scatter(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= S.n) return;
+    const int to = from ^ 1;
+    const double pos[3] = {S.pos[from][0][i], S.pos[from][1][i], DIM == 3 ? S.pos[from][2][i] : 0.0};
+    const unsigned o = atomicAdd(cursor + cell_of<DIM>(p, pos), 1u);
+    for (int a = 0; a < DIM; ++a) S.pos[to][a][o] = pos[a];
+    for (int a = 0; a < 3; ++a) S.vh[to][a][o] = S.vh[from][a][i];
+    S.id[to][o] = S.id[from][i];
+}
+
+// Device-side loading for large runs: uniform positions displaced by
+// amp/k sin(k x) along `mode_axis` (amp = 0: none) and Maxwellian velocities
+// with thermal speed vt and x drift, from a Philox stream per particle
+// (Box-Muller on 53-bit uniforms).
+__global__ void k_load_maxwellian(SpeciesND S, int buf, int dims, unsigned n, uint64_t seed, double L0, double L1,
+                                  double L2, double vt, double drift, int mode_axis, double amp) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    uint32_t r[4], r2[4];
+    philox4x32_10(i, 0x5eedu, 0u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), r);
+    philox4x32_10(i, 0x5eedu, 1u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), r2);
+    auto u53 = [](uint32_t a, uint32_t b) {
+        return ((double)(((uint64_t)a << 21) ^ (uint64_t)b & 0x1FFFFFull) + 0.5) * 0x1.0p-53;
+    };
+    const double L[3] = {L0, L1, L2};
+    const double u[3] = {u53(r[0], r[1]), u53(r[2], r[3]), u53(r2[0], r2[1])};
+    for (int a = 0; a < dims; ++a) {
+        double x = u[a] * L[a];
+        if (amp != 0.0 && a == mode_axis) {
+            const double k = 2.0 * 3.141592653589793 / L[a];
+            x = x + amp / k * sin(k * x);
+            x = fmod(fmod(x, L[a]) + L[a], L[a]);
+        }
+        S.pos[buf][a][i] = x;
+    }
+    uint32_t g1[4], g2[4];
+    philox4x32_10(i, 0x5eedu, 2u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), g1);
+    philox4x32_10(i, 0x5eedu, 3u, 0u, (uint32_t)seed, (uint32_t)(seed >> 32), g2);
+    const double a1 = u53(g1[0], g1[1]), b1 = u53(g1[2], g1[3]), a2 = u53(g2[0], g2[1]), b2 = u53(g2[2], g2[3]);
+    const double r1 = sqrt(-2.0 * log(a1)), r2v = sqrt(-2.0 * log(a2));
+    const double twopi = 2.0 * 3.141592653589793;
+    const double nv[3] = {r1 * cos(twopi * b1), r1 * sin(twopi * b1), r2v * cos(twopi * b2)};
+    for (int a = 0; a < 3; ++a) {
+        const double v = vt * nv[a] + (a == 0 ? drift : 0.0);
+        S.v[a][i] = v;
+        S.vh[buf][a][i] = v;
+    }
+    S.id[buf][i] = i;
+}
+
+// Read-back in load order: dst[id[i]] = src[i].
+__global__ void k_unpermute(const unsigned* id, const double* src, double* dst, unsigned n) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < n) dst[id[i]] = src[i];
+}
+
+// ---- spectral Poisson solve: line FFTs in shared memory -----------------------------
+
+enum : int { kFwdFromRho = 0, kFwdInPlace = 1, kFwdMulInv = 2, kInvInPlace = 3, kInvToFields = 4 };
+
+struct FftPass {
+    int n, log2n;
+    long long es, ls;       // element stride, stride between the tile's lines
+    int T;                  // lines per tile
+    long long tiles_inner;  // tiles per outer slab
+    long long outer_stride;
+    const Cplx* tw;         // exp(-2 pi i k / n), k < n/2
+    int axis;               // axis of the lines (0, 1, 2)
+};
+
+struct FieldsND {
+    int dims, nx, ny, nz;
+    double L[3], eps, inv_scale, pack;  // pack: power of two that balances phi and E in one complex array
+    unsigned long long* rho_acc;
+    const double* rho_in;  // when set, the forward pass reads FP64 rho instead of the accumulator
+    double* rho;
+    Cplx* W;
+    Cplx* A;
+    Cplx* B;
+    double* phi;
+    double* E;
+};
+
+__device__ __forceinline__ unsigned bitrev(unsigned x, int bits) { return __brev(x) >> (32 - bits); }
+
+// In-place radix-2 DIT transform of `T` lines stored bit-reversed in smem
+// (line stride `ld`); forward uses exp(-2 pi i k/n), inverse the conjugate and
+// a 1/n scale, as fft_radix2 does (src/FieldSolver.cpp:171-201).
+__device__ void fft_lines(Cplx* buf, int T, int ld, int n, int log2n, const Cplx* tw, bool inverse) {
+    const int half_total = T * (n >> 1);
+    for (int s = 1; s <= log2n; ++s) {
+        const int len = 1 << s, half = len >> 1;
+        const int tstride = n >> s;  // twiddle index step
+        for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
+            const int l = b / (n >> 1);
+            const int j = b % (n >> 1);
+            const int grp = j / half, pos = j % half;
+            const int ia = l * ld + grp * len + pos;
+            const int ib = ia + half;
+            Cplx w = tw[pos * tstride];
+            if (inverse) w.im = -w.im;
+            const Cplx u = buf[ia], x = buf[ib];
+            const Cplx v = {x.re * w.re - x.im * w.im, x.re * w.im + x.im * w.re};
+            buf[ia] = {u.re + v.re, u.im + v.im};
+            buf[ib] = {u.re - v.re, u.im - v.im};
+        }
+        __syncthreads();
+    }
+    if (inverse) {
+        const double sc = 1.0 / (double)n;
+        for (int b = threadIdx.x; b < T * n; b += blockDim.x) {
+            const int l = b / n, e = b % n;
+            Cplx& c = buf[l * ld + e];
+            c.re *= sc;
+            c.im *= sc;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ long long tile_base(const FftPass& f, long long tile) {
+    return (tile % f.tiles_inner) * f.T * f.ls + (tile / f.tiles_inner) * f.outer_stride;
+}
+
+// element b of the tile: (line l, element e) so that consecutive b are consecutive in memory
+__device__ __forceinline__ void tile_elem(const FftPass& f, int b, int& l, int& e) {
+    if (f.es == 1) { l = b / f.n; e = b % f.n; }
+    else { e = b / f.T; l = b % f.T; }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
+    extern __shared__ __align__(16) unsigned char fsm[];
+    const int ld = f.n;
+    Cplx* X = reinterpret_cast<Cplx*>(fsm);
+    Cplx* Y = X + f.T * ld;  // second array (A/B pair passes)
+    Cplx* tws = Y + ((MODE == kFwdMulInv || MODE == kInvInPlace || MODE == kInvToFields) ? 2 : 0) * f.T * ld;
+    for (int k = threadIdx.x; k < (f.n >> 1); k += blockDim.x) tws[k] = f.tw[k];
+    const long long base = tile_base(f, blockIdx.x);
+    const int total = f.T * f.n;
+    // ---- load (bit-reversed within each line) ----
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        int l, e;
+        tile_elem(f, b, l, e);
+        const long long g = base + l * f.ls + e * f.es;
+        const int s = l * ld + bitrev(e, f.log2n);
+        if (MODE == kFwdFromRho) {
+            double r;
+            if (F.rho_in) {
+                r = F.rho_in[g];
+            } else {
+                r = (double)(long long)F.rho_acc[g] * F.inv_scale;
+                F.rho_acc[g] = 0ull;
+            }
+            F.rho[g] = r;
+            X[s] = {r, 0.0};
+        } else if (MODE == kFwdInPlace || MODE == kFwdMulInv) {
+            X[s] = F.W[g];
+        } else {
+            X[s] = F.A[g];
+            Y[s] = F.B[g];
+        }
+    }
+    __syncthreads();
+    const bool inverse_first = (MODE == kInvInPlace || MODE == kInvToFields);
+    fft_lines(X, f.T, ld, f.n, f.log2n, tws, inverse_first);
+    if (inverse_first) fft_lines(Y, f.T, ld, f.n, f.log2n, tws, true);
+    if (MODE == kFwdMulInv) {
+        // k-space multiply (src/FieldSolver.cpp:470-488, :687-712) into two packed
+        // spectra A = phi_k + i Ex_k / pack, B = Ey_k / pack + i Ez_k / pack,
+        // each E component restricted to its Hermitian part (zero on its own
+        // Nyquist plane) so that both inverse transforms are real pairs
+        const double twopi = 2.0 * 3.141592653589793;
+        const double ip = 1.0 / F.pack;
+        for (int b = threadIdx.x; b < total; b += blockDim.x) {
+            int l, e;
+            tile_elem(f, b, l, e);
+            const long long g = base + l * f.ls + e * f.es;
+            const int ix = (int)(g % F.nx);
+            const int iy = (int)((g / F.nx) % F.ny);
+            const int iz = F.dims == 3 ? (int)(g / ((long long)F.nx * F.ny)) : 0;
+            const Cplx r = X[l * ld + e];  // natural order after the forward transform
+            Cplx a = {0.0, 0.0}, bb = {0.0, 0.0};
+            if (ix != 0 || iy != 0 || iz != 0) {
+                const double mx = ix <= F.nx / 2 ? (double)ix : -(double)(F.nx - ix);
+                const double my = iy <= F.ny / 2 ? (double)iy : -(double)(F.ny - iy);
+                const double kx = twopi * mx / F.L[0];
+                const double ky = twopi * my / F.L[1];
+                double kz = 0.0, k2;
+                if (F.dims == 3) {
+                    const double mz = iz <= F.nz / 2 ? (double)iz : -(double)(F.nz - iz);
+                    kz = twopi * mz / F.L[2];
+                    k2 = kx * kx + ky * ky + kz * kz;
+                } else {
+                    k2 = kx * kx + ky * ky;
+                }
+                const double den = F.eps * k2;
+                const double pr = r.re / den, pi = r.im / den;
+                // -(0,1) k phik = (k pi, -(k pr))
+                const bool nyx = (F.nx % 2 == 0) && ix == F.nx / 2;
+                const bool nyy = (F.ny % 2 == 0) && iy == F.ny / 2;
+                const bool nyz = F.dims == 3 && (F.nz % 2 == 0) && iz == F.nz / 2;
+                const double exr = nyx ? 0.0 : kx * pi, exi = nyx ? 0.0 : -(kx * pr);
+                const double eyr = nyy ? 0.0 : ky * pi, eyi = nyy ? 0.0 : -(ky * pr);
+                const double ezr = nyz ? 0.0 : kz * pi, ezi = nyz ? 0.0 : -(kz * pr);
+                a = {pr - exi * ip, pi + exr * ip};
+                bb = {eyr * ip - ezi * ip, eyi * ip + ezr * ip};
+            }
+            const int s = l * ld + bitrev(e, f.log2n);
+            Y[s] = a;
+            Y[f.T * ld + s] = bb;
+        }
+        __syncthreads();
+        fft_lines(Y, 2 * f.T, ld, f.n, f.log2n, tws, true);
+    }
+    // ---- store ----
+    for (int b = threadIdx.x; b < total; b += blockDim.x) {
+        int l, e;
+        tile_elem(f, b, l, e);
+        const long long g = base + l * f.ls + e * f.es;
+        const int s = l * ld + e;
+        if (MODE == kFwdFromRho || MODE == kFwdInPlace) {
+            F.W[g] = X[s];
+        } else if (MODE == kFwdMulInv) {
+            F.A[g] = Y[s];
+            F.B[g] = Y[f.T * ld + s];
+        } else if (MODE == kInvInPlace) {
+            F.A[g] = X[s];
+            F.B[g] = Y[s];
+        } else {
+            const Cplx a = X[s], bb = Y[s];
+            F.phi[g] = a.re;
+            if (F.dims == 2) {
+                reinterpret_cast<double2*>(F.E)[g] = make_double2(a.im * F.pack, bb.re * F.pack);
+            } else {
+                reinterpret_cast<double4*>(F.E)[g] = make_double4(a.im * F.pack, bb.re * F.pack, bb.im * F.pack, 0.0);
+            }
+        }
+    }
+}
+
+// Simulation2D/3D sample reductions (src/Diagnostics.cpp:111-137, :205-232):
+// kinetic energy of v per species and field energy / charge_l1 of the grid;
+// per-block partials, the last block adds them in block order.
+constexpr int kSampleBlocks = 148;
+__global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double* partial, unsigned* done,
+                                                   double* out, const double* E, const double* rho,
+                                                   long long N, double half_eps_vol, double vol, int species,
+                                                   int last_species) {
+    __shared__ double red[8], red2[8], red3[8];
+    __shared__ bool last;
+    const int tid = threadIdx.x;
+    double ke = 0.0, fe = 0.0, l1 = 0.0;
+    for (unsigned i = blockIdx.x * 256 + tid; i < S.n; i += gridDim.x * 256)
+        ke += S.hmw * (S.v[0][i] * S.v[0][i] + S.v[1][i] * S.v[1][i] + S.v[2][i] * S.v[2][i]);
+    if (last_species) {
+        for (long long g = blockIdx.x * 256 + tid; g < N; g += gridDim.x * 256) {
+            double e2;
+            if (dims == 2) {
+                const double2 e = reinterpret_cast<const double2*>(E)[g];
+                e2 = e.x * e.x + e.y * e.y;
+            } else {
+                const double4 e = reinterpret_cast<const double4*>(E)[g];
+                e2 = e.x * e.x + e.y * e.y + e.z * e.z;
+            }
+            fe += half_eps_vol * e2;
+            l1 += fabs(rho[g]) * vol;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        ke += __shfl_down_sync(0xffffffffu, ke, o);
+        fe += __shfl_down_sync(0xffffffffu, fe, o);
+        l1 += __shfl_down_sync(0xffffffffu, l1, o);
+    }
+    if ((tid & 31) == 0) { red[tid >> 5] = ke; red2[tid >> 5] = fe; red3[tid >> 5] = l1; }
+    __syncthreads();
+    if (tid == 0) {
+        double a = 0, b = 0, c = 0;
+        for (int w = 0; w < 8; ++w) { a += red[w]; b += red2[w]; c += red3[w]; }
+        partial[3 * blockIdx.x] = a;
+        partial[3 * blockIdx.x + 1] = b;
+        partial[3 * blockIdx.x + 2] = c;
+        __threadfence();
+        last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || tid != 0) return;
+    __threadfence();
+    double a = 0, b = 0, c = 0;
+    for (unsigned k = 0; k < gridDim.x; ++k) {
+        a += ((volatile double*)partial)[3 * k];
+        b += ((volatile double*)partial)[3 * k + 1];
+        c += ((volatile double*)partial)[3 * k + 2];
+    }
+    out[species] = a;
+    if (last_species) { out[4] = b; out[5] = c; }
+    *done = 0;
+}
+
+// ---- host ----------------------------------------------------------------------------
+
+static bool pow2(size_t v) { return v >= 2 && (v & (v - 1)) == 0; }
+static int ilog2(size_t v) { int k = 0; while ((size_t(1) << k) < v) ++k; return k; }
+
+struct Solver {
+    FieldsND F{};
+    FftPass px{}, py{}, pz{};
+    size_t smem_fwd = 0, smem_pair = 0;
+    std::vector<void*>* allocs = nullptr;
+    cudaStream_t stream = nullptr;
+
+    template <class T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        APIC_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        allocs->push_back(p);
+        APIC_CUDA(cudaMemsetAsync(p, 0, std::max<size_t>(count, 1) * sizeof(T), stream));
+        return static_cast<T*>(p);
+    }
+
+    Cplx* twiddles(int n) {
+        std::vector<Cplx> h(n / 2);
+        const double twopi = 2.0 * 3.141592653589793;
+        for (int k = 0; k < n / 2; ++k) h[k] = {std::cos(twopi * k / n), -std::sin(twopi * k / n)};
+        Cplx* d = alloc<Cplx>(h.size());
+        APIC_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        return d;
+    }
+
+    FftPass pass(int ax, int T) const {
+        FftPass f{};
+        const long long nx = F.nx, ny = F.ny, nz = F.dims == 3 ? F.nz : 1;
+        f.axis = ax;
+        f.T = T;
+        if (ax == 0) {
+            f.n = F.nx; f.es = 1; f.ls = nx;
+            f.tiles_inner = ny * nz / T; f.outer_stride = 0;
+        } else if (ax == 1) {
+            f.n = F.ny; f.es = nx; f.ls = 1;
+            f.tiles_inner = nx / T; f.outer_stride = nx * ny;
+        } else {
+            f.n = F.nz; f.es = nx * ny; f.ls = 1;
+            f.tiles_inner = nx / T; f.outer_stride = nx;
+        }
+        f.log2n = ilog2(f.n);
+        return f;
+    }
+
+    long long tiles(const FftPass& f) const {
+        const long long N = (long long)F.nx * F.ny * (F.dims == 3 ? F.nz : 1);
+        return N / ((long long)f.T * f.n);
+    }
+
+    void setup(int dims, const size_t* n, const double* L, double eps, double inv_scale) {
+        F.dims = dims;
+        F.nx = (int)n[0]; F.ny = (int)n[1]; F.nz = dims == 3 ? (int)n[2] : 1;
+        for (int a = 0; a < 3; ++a) F.L[a] = a < dims ? L[a] : 1.0;
+        F.eps = eps;
+        F.inv_scale = inv_scale;
+        double kmax = 0;
+        for (int a = 0; a < dims; ++a) kmax = std::max(kmax, 3.141592653589793 * (double)n[a] / L[a]);
+        F.pack = std::ldexp(1.0, (int)std::lround(std::log2(kmax)));
+        const size_t N = (size_t)F.nx * F.ny * F.nz;
+        F.rho_acc = alloc<unsigned long long>(N);
+        F.rho = alloc<double>(N);
+        F.W = alloc<Cplx>(N);
+        F.A = alloc<Cplx>(N);
+        F.B = alloc<Cplx>(N);
+        F.phi = alloc<double>(N);
+        F.E = alloc<double>(N * (dims == 2 ? 2 : 4));
+        // lines per tile: up to 8 (128 B rows in the strided passes), bounded
+        // so that the paired passes (three line buffers) fit in shared memory
+        auto lines = [](int n, long long available) {
+            int T = 8;
+            while (T > 1 && (size_t)3 * T * n * sizeof(Cplx) + (n / 2) * sizeof(Cplx) > 200 * 1024) T >>= 1;
+            while (T > 1 && available % T) T >>= 1;
+            return T;
+        };
+        px = pass(0, lines(F.nx, (long long)F.ny * F.nz));
+        py = pass(1, lines(F.ny, F.nx));
+        if (dims == 3) pz = pass(2, lines(F.nz, F.nx));
+        px.tw = twiddles(F.nx);
+        py.tw = F.ny == F.nx ? px.tw : twiddles(F.ny);
+        if (dims == 3) pz.tw = F.nz == F.nx ? px.tw : (F.nz == F.ny ? py.tw : twiddles(F.nz));
+        smem_pair = std::max(smem_of(px, kFwdMulInv), smem_of(py, kFwdMulInv));
+        if (dims == 3) smem_pair = std::max(smem_pair, smem_of(pz, kFwdMulInv));
+        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdFromRho>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+        APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+        APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+    }
+
+    size_t smem_of(const FftPass& f, int mode) const {
+        const size_t line = (size_t)f.T * f.n * sizeof(Cplx);
+        const size_t tw = (size_t)(f.n / 2) * sizeof(Cplx);
+        return (mode == kFwdFromRho || mode == kFwdInPlace) ? line + tw : 3 * line + tw;
+    }
+
+    // rho_acc -> rho, phi, E (the fixed-point accumulator is cleared)
+    void solve() {
+        if (F.dims == 2) {
+            k_fft<kFwdFromRho><<<(unsigned)tiles(px), kThreads, smem_of(px, kFwdFromRho), stream>>>(F, px);
+            k_fft<kFwdMulInv><<<(unsigned)tiles(py), kThreads, smem_of(py, kFwdMulInv), stream>>>(F, py);
+            k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+        } else {
+            k_fft<kFwdFromRho><<<(unsigned)tiles(px), kThreads, smem_of(px, kFwdFromRho), stream>>>(F, px);
+            k_fft<kFwdInPlace><<<(unsigned)tiles(py), kThreads, smem_of(py, kFwdInPlace), stream>>>(F, py);
+            k_fft<kFwdMulInv><<<(unsigned)tiles(pz), kThreads, smem_of(pz, kFwdMulInv), stream>>>(F, pz);
+            k_fft<kInvInPlace><<<(unsigned)tiles(py), kThreads, smem_of(py, kInvInPlace), stream>>>(F, py);
+            k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+        }
+        APIC_CUDA(cudaGetLastError());
+    }
+};
+
+struct SimND {
+    apic_config_nd cfg{};
+    std::string last_error;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocations;
+    ParamsND p{};
+    SpeciesND sp[APIC_MAX_SPECIES]{};
+    int buf[APIC_MAX_SPECIES] = {0, 0, 0, 0};
+    Solver solver;
+    bool boris = false;
+    bool initialized = false;
+    double time = 0.0;
+    uint64_t step_count = 0;
+    size_t sort_interval = 16;
+    size_t steps_since_sort = 0;
+    unsigned* cell_count = nullptr;
+    unsigned* cell_offset = nullptr;
+    unsigned* block_sums = nullptr;
+    size_t ncells = 0;
+    double* sample_partial = nullptr;
+    unsigned* sample_done = nullptr;
+    double* sample_out = nullptr;
+    bool timing = false;
+    double push_ms = 0, solve_ms = 0, sort_ms = 0;
+    uint64_t timed_steps = 0;
+    struct Ev { cudaEvent_t a, b, c, d; bool sorted; };
+    std::vector<Ev> events;
+
+    template <class T>
+    T* dalloc(size_t count) {
+        void* ptr = nullptr;
+        APIC_CUDA(cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T)));
+        allocations.push_back(ptr);
+        APIC_CUDA(cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), stream));
+        return static_cast<T*>(ptr);
+    }
+
+    ~SimND() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& e : events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); cudaEventDestroy(e.c); cudaEventDestroy(e.d); }
+        for (void* a : allocations) cudaFree(a);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void create(const apic_config_nd& c) {
+        cfg = c;
+        require(c.dims == 2 || c.dims == 3, "dims must be 2 or 3");
+        require(c.precision == APIC_FP64, "this entry point builds the FP64 form", APIC_ERR_UNSUPPORTED);
+        for (int a = 0; a < c.dims; ++a) {
+            require(c.n[a] >= 3, "mesh extents must be at least 3");
+            require(pow2(c.n[a]) && c.n[a] <= (size_t)kMaxLine,
+                    "periodic device meshes need power-of-two extents up to 1024", APIC_ERR_UNSUPPORTED);
+            require(std::isfinite(c.length[a]) && c.length[a] > 0, "domain lengths must be positive and finite");
+        }
+        require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
+        require(c.nspecies >= 1 && c.nspecies <= APIC_MAX_SPECIES, "species count out of range");
+        const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
+        require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
+        const double depth = c.out_of_plane_depth == 0.0 ? 1.0 : c.out_of_plane_depth;
+        require(std::isfinite(depth) && depth > 0, "2D deposition depth must be positive and finite");
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
+        APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        sort_interval = c.sort_interval ? c.sort_interval : 16;
+
+        p.dims = c.dims;
+        size_t N = 1;
+        double cellvol = 1.0;
+        for (int a = 0; a < 3; ++a) {
+            p.n[a] = a < c.dims ? (int)c.n[a] : 1;
+            p.L[a] = a < c.dims ? c.length[a] : 1.0;
+            p.d[a] = p.L[a] / (double)p.n[a];  // Mesh2D/Mesh3D periodic dx, src/Mesh2D.cpp:59-62
+            p.B[a] = c.magnetic_field[a];
+            N *= (size_t)p.n[a];
+            if (a < c.dims) cellvol *= p.d[a];
+        }
+        ncells = N;
+        boris = c.magnetic_field[0] != 0.0 || c.magnetic_field[1] != 0.0 || c.magnetic_field[2] != 0.0;
+        p.dt = c.dt;
+        p.eps = (c.units == APIC_SI ? 8.8541878128e-12 : 1.0) * rel;
+        double bound = 0.0;
+        for (int s = 0; s < c.nspecies; ++s) {
+            const auto& S = c.species[s];
+            require(std::isfinite(S.mass) && S.mass > 0, "species mass must be positive and finite");
+            require(S.capacity > 0 && S.capacity < (1ull << 31), "species capacity out of range");
+            const double w = c.dims == 2 ? S.weight / depth : S.weight;  // Species2D::deposit_charge
+            bound += (double)S.capacity * std::fabs(S.charge * w) / cellvol;
+        }
+        const int bits = bound > 0 ? (int)std::floor(61.0 - std::log2(bound)) : 0;
+        p.rho_scale = std::ldexp(1.0, bits);
+        p.inv_rho_scale = std::ldexp(1.0, -bits);
+        for (int s = 0; s < c.nspecies; ++s) {
+            const auto& S = c.species[s];
+            SpeciesND& D = sp[s];
+            D.qm = S.charge / S.mass;
+            const double w = c.dims == 2 ? S.weight / depth : S.weight;
+            D.dep = S.charge * w / cellvol;
+            D.hmw = 0.5 * S.mass * S.weight;
+            D.n = 0;
+            for (int b = 0; b < 2; ++b) {
+                for (int a = 0; a < c.dims; ++a) D.pos[b][a] = dalloc<double>(S.capacity);
+                for (int a = 0; a < 3; ++a) D.vh[b][a] = dalloc<double>(S.capacity);
+                D.id[b] = dalloc<unsigned>(S.capacity);
+            }
+            for (int a = 0; a < 3; ++a) D.v[a] = dalloc<double>(S.capacity);
+        }
+        solver.allocs = &allocations;
+        solver.stream = stream;
+        solver.setup(c.dims, c.n, c.length, p.eps, p.inv_rho_scale);
+        p.E = solver.F.E;
+        p.rho_acc = solver.F.rho_acc;
+        cell_count = dalloc<unsigned>(N);
+        cell_offset = dalloc<unsigned>(N);
+        block_sums = dalloc<unsigned>((N + kScanBlock - 1) / kScanBlock + 1);
+        sample_partial = dalloc<double>(3 * kSampleBlocks);
+        sample_done = dalloc<unsigned>(1);
+        sample_out = dalloc<double>(8);
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    SpeciesND view(int s) const { return sp[s]; }
+
+    template <int MODE>
+    void launch_push(int s) {
+        const SpeciesND& S = sp[s];
+        if (S.n == 0) return;
+        const unsigned blocks = (S.n + kThreads - 1) / kThreads;
+        const int b = buf[s];
+        if (cfg.dims == 2) {
+            if (boris) k_push<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
+            else k_push<2, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
+        } else {
+            if (boris) k_push<3, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
+            else k_push<3, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
+        }
+        APIC_CUDA(cudaGetLastError());
+    }
+
+    void sort_species(int s) {
+        SpeciesND& S = sp[s];
+        if (S.n == 0) return;
+        const unsigned blocks = (S.n + kThreads - 1) / kThreads;
+        const unsigned nb = (unsigned)((ncells + kScanBlock - 1) / kScanBlock);
+        APIC_CUDA(cudaMemsetAsync(cell_count, 0, ncells * sizeof(unsigned), stream));
+        if (cfg.dims == 2) k_cell_hist<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
+        else k_cell_hist<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
+        k_scan_local<<<nb, kThreads, 0, stream>>>(cell_count, cell_offset, block_sums, (unsigned)ncells);
+        k_scan_blocks<<<1, kThreads, 0, stream>>>(block_sums, nb);
+        k_scan_add<<<nb, kThreads, 0, stream>>>(cell_offset, block_sums, (unsigned)ncells);
+        if (cfg.dims == 2) k_cell_scatter<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        else k_cell_scatter<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        APIC_CUDA(cudaGetLastError());
+        buf[s] ^= 1;
+    }
+
+    void load(int s, size_t n, const double* pos, const double* v, const double* vh) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        require(pos && v, "positions and velocities are required");
+        require(n <= cfg.species[s].capacity, "initial particle count exceeds max_particles_per_species",
+                APIC_ERR_CAPACITY);
+        SpeciesND& S = sp[s];
+        const int b = buf[s];
+        const size_t bytes = n * sizeof(double);
+        for (int a = 0; a < cfg.dims; ++a)
+            APIC_CUDA(cudaMemcpyAsync(S.pos[b][a], pos + a * n, bytes, cudaMemcpyHostToDevice, stream));
+        for (int a = 0; a < 3; ++a) {
+            APIC_CUDA(cudaMemcpyAsync(S.v[a], v + a * n, bytes, cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(S.vh[b][a], (vh ? vh : v) + a * n, bytes, cudaMemcpyHostToDevice, stream));
+        }
+        std::vector<unsigned> ids(n);
+        for (size_t i = 0; i < n; ++i) ids[i] = (unsigned)i;
+        APIC_CUDA(cudaMemcpyAsync(S.id[b], ids.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        S.n = (unsigned)n;
+        initialized = false;
+    }
+
+    void load_maxwellian(int s, size_t n, uint64_t seed, double vt, double drift, int axis, double amp) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        require(n <= cfg.species[s].capacity, "initial particle count exceeds max_particles_per_species",
+                APIC_ERR_CAPACITY);
+        require(std::isfinite(vt) && vt >= 0 && std::isfinite(drift) && std::isfinite(amp), "invalid loading parameters");
+        SpeciesND& S = sp[s];
+        const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
+        if (n) k_load_maxwellian<<<blocks, kThreads, 0, stream>>>(S, buf[s], cfg.dims, (unsigned)n, seed, p.L[0],
+                                                                   p.L[1], p.L[2], vt, drift, axis, amp);
+        APIC_CUDA(cudaGetLastError());
+        S.n = (unsigned)n;
+        initialized = false;
+    }
+
+    void deposit_and_solve() {
+        for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushDepositOnly>(s);
+        solver.solve();
+    }
+
+    void initialize() {
+        time = 0.0;
+        step_count = 0;
+        deposit_and_solve();
+        for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushInitHalf>(s);
+        initialized = true;
+        steps_since_sort = sort_interval;  // sort before the first step
+    }
+
+    void resume(double t, uint64_t k) {
+        time = t;
+        step_count = k;
+        deposit_and_solve();
+        initialized = true;
+        steps_since_sort = sort_interval;
+    }
+
+    void do_steps(size_t nsteps) {
+        require(initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
+        for (size_t it = 0; it < nsteps; ++it) {
+            Ev ev{};
+            const bool sort_now = steps_since_sort >= sort_interval;
+            if (timing) {
+                APIC_CUDA(cudaEventCreate(&ev.a)); APIC_CUDA(cudaEventCreate(&ev.b));
+                APIC_CUDA(cudaEventCreate(&ev.c)); APIC_CUDA(cudaEventCreate(&ev.d));
+                APIC_CUDA(cudaEventRecord(ev.a, stream));
+            }
+            if (sort_now) {
+                for (int s = 0; s < cfg.nspecies; ++s) sort_species(s);
+                steps_since_sort = 0;
+            }
+            if (timing) APIC_CUDA(cudaEventRecord(ev.b, stream));
+            for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
+            if (timing) APIC_CUDA(cudaEventRecord(ev.c, stream));
+            solver.solve();
+            if (timing) {
+                APIC_CUDA(cudaEventRecord(ev.d, stream));
+                ev.sorted = sort_now;
+                events.push_back(ev);
+            }
+            ++steps_since_sort;
+            time += cfg.dt;
+            ++step_count;
+        }
+    }
+
+    void collect_timing() {
+        for (auto& e : events) {
+            float t_sort = 0, t_push = 0, t_solve = 0;
+            APIC_CUDA(cudaEventElapsedTime(&t_sort, e.a, e.b));
+            APIC_CUDA(cudaEventElapsedTime(&t_push, e.b, e.c));
+            APIC_CUDA(cudaEventElapsedTime(&t_solve, e.c, e.d));
+            sort_ms += t_sort;
+            push_ms += t_push;
+            solve_ms += t_solve;
+            ++timed_steps;
+            cudaEventDestroy(e.a); cudaEventDestroy(e.b); cudaEventDestroy(e.c); cudaEventDestroy(e.d);
+        }
+        events.clear();
+    }
+
+    void sync() {
+        const cudaError_t e = bounded_wait(stream, 600.0);
+        if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
+        APIC_CUDA(e);
+    }
+
+    size_t read_particles(int s, size_t cap, double* pos, double* v, double* vh) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        const SpeciesND& S = sp[s];
+        const size_t n = S.n;
+        require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
+        if (initialized) launch_push<kPushSync>(s);  // time-centred v of the current state
+        const int b = buf[s];
+        const int o = b ^ 1;
+        // un-permute into the other buffer's arrays (free outside a sort)
+        double* scratch[7];
+        int k = 0;
+        for (int a = 0; a < cfg.dims; ++a) scratch[k++] = S.pos[o][a];
+        for (int a = 0; a < 3; ++a) scratch[k++] = S.vh[o][a];
+        const unsigned blocks = (unsigned)((n + kThreads - 1) / kThreads);
+        auto fetch = [&](const double* src, double* host, double* tmp) {
+            if (!host || n == 0) return;
+            k_unpermute<<<blocks, kThreads, 0, stream>>>(S.id[b], src, tmp, (unsigned)n);
+            APIC_CUDA(cudaGetLastError());
+            APIC_CUDA(cudaMemcpyAsync(host, tmp, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+        };
+        for (int a = 0; a < cfg.dims; ++a) fetch(S.pos[b][a], pos ? pos + a * n : nullptr, scratch[0]);
+        if (pos && cfg.dims == 2) std::memset(pos + 2 * n, 0, n * sizeof(double));
+        for (int a = 0; a < 3; ++a) fetch(S.vh[b][a], vh ? vh + a * n : nullptr, scratch[0]);
+        for (int a = 0; a < 3; ++a) fetch(S.v[a], v ? v + a * n : nullptr, scratch[0]);
+        sync();
+        return n;
+    }
+
+    void read_fields(double* rho, double* phi, double* E) {
+        sync();
+        const size_t N = ncells;
+        if (rho) APIC_CUDA(cudaMemcpyAsync(rho, solver.F.rho, N * 8, cudaMemcpyDeviceToHost, stream));
+        if (phi) APIC_CUDA(cudaMemcpyAsync(phi, solver.F.phi, N * 8, cudaMemcpyDeviceToHost, stream));
+        if (E) {
+            const int st = cfg.dims == 2 ? 2 : 4;
+            std::vector<double> h(N * st);
+            APIC_CUDA(cudaMemcpyAsync(h.data(), solver.F.E, N * st * 8, cudaMemcpyDeviceToHost, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            for (int c = 0; c < cfg.dims; ++c)
+                for (size_t g = 0; g < N; ++g) E[c * N + g] = h[g * st + c];
+        }
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void sample(apic_sample_nd* out) {
+        std::memset(out, 0, sizeof *out);
+        double vol = 1.0;
+        for (int a = 0; a < cfg.dims; ++a) vol *= p.d[a];
+        if (cfg.dims == 2) vol *= (cfg.out_of_plane_depth == 0.0 ? 1.0 : cfg.out_of_plane_depth);
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            if (initialized) launch_push<kPushSync>(s);
+            k_sample_nd<<<kSampleBlocks, 256, 0, stream>>>(sp[s], cfg.dims, sample_partial, sample_done, sample_out,
+                                                           solver.F.E, solver.F.rho, (long long)ncells,
+                                                           0.5 * p.eps * vol, vol, s, s == cfg.nspecies - 1);
+            APIC_CUDA(cudaGetLastError());
+        }
+        double h[8];
+        APIC_CUDA(cudaMemcpyAsync(h, sample_out, sizeof h, cudaMemcpyDeviceToHost, stream));
+        sync();
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            out->kinetic_by_species[s] = h[s];
+            out->kinetic_energy += h[s];
+            out->live_particles += sp[s].n;
+        }
+        out->field_energy = h[4];
+        out->charge_l1 = h[5];
+        out->total_energy = out->kinetic_energy + out->field_energy;
+        out->step = step_count;
+        out->time = time;
+    }
+};
+
+}  // namespace nd
+}  // namespace apic
+
+// ---- C ABI ---------------------------------------------------------------------------
+
+struct apic_sim_nd {
+    apic::nd::SimND impl;
+};
+
+namespace {
+thread_local std::string g_nd_error;
+
+template <class F>
+int guarded_nd(apic_sim_nd* h, F&& f) {
+    try {
+        f();
+        return APIC_OK;
+    } catch (const apic::Error& e) {
+        if (h) h->impl.last_error = e.what();
+        g_nd_error = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        if (h) h->impl.last_error = e.what();
+        g_nd_error = e.what();
+        return APIC_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int apic_simnd_create(const apic_config_nd* cfg, apic_sim_nd** out) {
+    if (!cfg || !out) return APIC_ERR_INVALID;
+    *out = nullptr;
+    auto h = std::make_unique<apic_sim_nd>();
+    const int rc = guarded_nd(h.get(), [&] { h->impl.create(*cfg); });
+    if (rc == APIC_OK) *out = h.release();
+    return rc;
+}
+
+void apic_simnd_destroy(apic_sim_nd* sim) { delete sim; }
+
+const char* apic_simnd_last_error(const apic_sim_nd* sim) {
+    return sim ? sim->impl.last_error.c_str() : g_nd_error.c_str();
+}
+
+int apic_simnd_load_particles(apic_sim_nd* sim, int species, size_t n, const double* pos, const double* v,
+                              const double* v_half) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.load(species, n, pos, v, v_half); });
+}
+
+int apic_simnd_load_maxwellian(apic_sim_nd* sim, int species, size_t n, uint64_t seed, double thermal_speed,
+                               double drift_x, int perturb_axis, double perturb_amplitude) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] {
+        sim->impl.load_maxwellian(species, n, seed, thermal_speed, drift_x, perturb_axis, perturb_amplitude);
+    });
+}
+
+int apic_simnd_initialize(apic_sim_nd* sim) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.initialize(); });
+}
+
+int apic_simnd_resume(apic_sim_nd* sim, double time, uint64_t step) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.resume(time, step); });
+}
+
+int apic_simnd_step(apic_sim_nd* sim, size_t nsteps) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.do_steps(nsteps); });
+}
+
+int apic_simnd_synchronize(apic_sim_nd* sim) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.sync(); });
+}
+
+int apic_simnd_count(apic_sim_nd* sim, int species, size_t* n) {
+    if (!sim || !n || species < 0 || species >= sim->impl.cfg.nspecies) return APIC_ERR_INVALID;
+    *n = sim->impl.sp[species].n;
+    return APIC_OK;
+}
+
+int apic_simnd_read_particles(apic_sim_nd* sim, int species, size_t capacity, double* pos, double* v, double* v_half,
+                              size_t* n) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] {
+        const size_t got = sim->impl.read_particles(species, capacity, pos, v, v_half);
+        if (n) *n = got;
+    });
+}
+
+int apic_simnd_read_fields(apic_sim_nd* sim, double* rho, double* phi, double* electric) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.read_fields(rho, phi, electric); });
+}
+
+int apic_simnd_sample(apic_sim_nd* sim, apic_sample_nd* out) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.sample(out); });
+}
+
+int apic_simnd_cuda_stream(apic_sim_nd* sim, void** stream) {
+    if (!sim || !stream) return APIC_ERR_INVALID;
+    *stream = (void*)sim->impl.stream;
+    return APIC_OK;
+}
+
+int apic_simnd_set_kernel_timing(apic_sim_nd* sim, int enable) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] {
+        sim->impl.sync();
+        sim->impl.collect_timing();
+        sim->impl.timing = enable != 0;
+        sim->impl.push_ms = sim->impl.solve_ms = sim->impl.sort_ms = 0;
+        sim->impl.timed_steps = 0;
+    });
+}
+
+int apic_simnd_kernel_times(apic_sim_nd* sim, double* push_ms, double* solve_ms, double* sort_ms, uint64_t* steps) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] {
+        sim->impl.sync();
+        sim->impl.collect_timing();
+        if (push_ms) *push_ms = sim->impl.push_ms;
+        if (solve_ms) *solve_ms = sim->impl.solve_ms;
+        if (sort_ms) *sort_ms = sim->impl.sort_ms;
+        if (steps) *steps = sim->impl.timed_steps;
+    });
+}
+
+int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,
+                                 const double* rho, double* phi, double* electric) {
+    return guarded_nd(nullptr, [&] {
+        apic::require(dims == 2 || dims == 3, "dims must be 2 or 3");
+        apic::require(std::isfinite(permittivity) && permittivity > 0,
+                      "field-solver permittivity must be positive and finite");
+        apic_config_nd c{};
+        c.dims = dims;
+        for (int a = 0; a < dims; ++a) { c.n[a] = n[a]; c.length[a] = length[a]; }
+        c.dt = 1.0;
+        c.units = APIC_NORMALIZED;
+        c.relative_permittivity = permittivity;
+        c.nspecies = 1;
+        c.species[0] = {1.0, 1.0, 1.0, 1};
+        apic::nd::SimND S;
+        S.create(c);
+        size_t N = 1;
+        for (int a = 0; a < dims; ++a) N *= n[a];
+        double* d_rho = S.dalloc<double>(N);
+        APIC_CUDA(cudaMemcpyAsync(d_rho, rho, N * 8, cudaMemcpyHostToDevice, S.stream));
+        S.solver.F.rho_in = d_rho;
+        S.solver.solve();
+        S.read_fields(nullptr, phi, electric);
+    });
+}
+
+}  // extern "C"

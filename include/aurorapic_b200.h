@@ -265,6 +265,89 @@ APIC_EXPORT int apic_collide3(const apic_mcc_model* model, double particle_mass,
                   double dt, const uint64_t* draws, const uint64_t* offsets,
                   uint64_t seed, uint64_t step, uint32_t stream, apic_collide_stats* stats);
 
+/* ---- structured 2D3V / 3D3V periodic simulation -------------------------- */
+
+/* Simulation2DConfig / Simulation3DConfig subset of the periodic particle
+ * step (include/pic/Simulation2D.hpp:118-165, include/pic/Simulation3D.hpp:30-66):
+ * fully periodic fields and particle boundaries, uniform magnetic field.
+ * Grid sizes must be powers of two (2..1024 per axis). */
+typedef struct {
+    int dims;                   /* 2 (2D3V) or 3 (3D3V) */
+    size_t n[3];                /* cells (= nodes, periodic) per axis */
+    double length[3];
+    double dt;
+    int units;                  /* apic_units */
+    double relative_permittivity;
+    double magnetic_field[3];   /* uniform B; all zero selects the leapfrog pusher */
+    double out_of_plane_depth;  /* 2D only: weight / depth enters the deposit (0 = 1) */
+    int precision;              /* apic_precision */
+    size_t sort_interval;       /* steps between particle sorts by cell (0 = default 16) */
+    int nspecies;
+    apic_species species[APIC_MAX_SPECIES];
+} apic_config_nd;
+
+/* DiagnosticSample2D / DiagnosticSample3D, src/Diagnostics.cpp:111-137, :205-232 */
+typedef struct {
+    uint64_t step;
+    double time;
+    double kinetic_energy;
+    double field_energy;
+    double total_energy;
+    double charge_l1;
+    uint64_t live_particles;
+    double kinetic_by_species[APIC_MAX_SPECIES];
+} apic_sample_nd;
+
+typedef struct apic_sim_nd apic_sim_nd;
+
+/* Simulation2D::Simulation2D / Simulation3D::Simulation3D (periodic). */
+APIC_EXPORT int apic_simnd_create(const apic_config_nd* cfg, apic_sim_nd** out);
+APIC_EXPORT void apic_simnd_destroy(apic_sim_nd* sim);
+APIC_EXPORT const char* apic_simnd_last_error(const apic_sim_nd* sim);
+/* Species2D/3D::particles() mutation.  pos is [dims][n] (component-major), v and
+ * v_half are [3][n]; v_half may be NULL (then v_half = v). */
+APIC_EXPORT int apic_simnd_load_particles(apic_sim_nd* sim, int species, size_t n, const double* pos,
+                                          const double* v, const double* v_half);
+/* Loads n particles generated on the device (for runs too large to stage on
+ * the host): uniform positions displaced by amplitude/k sin(k x) along
+ * perturb_axis (amplitude 0: none), Maxwellian velocities of the given thermal
+ * speed plus an x drift, v_half = v.  Seeded Philox streams; no reference
+ * counterpart (the reference's loaders, src/Species2D.cpp / Species3D.cpp, use
+ * its shared engine). */
+APIC_EXPORT int apic_simnd_load_maxwellian(apic_sim_nd* sim, int species, size_t n, uint64_t seed,
+                                           double thermal_speed, double drift_x, int perturb_axis,
+                                           double perturb_amplitude);
+/* Simulation2D/3D::initialize after the particles are loaded
+ * (src/Simulation2D.cpp:770-781): deposit_and_solve then the Boris or leapfrog
+ * half-step initialisation. */
+APIC_EXPORT int apic_simnd_initialize(apic_sim_nd* sim);
+/* Restart from a state whose v_half is set: deposit_and_solve only. */
+APIC_EXPORT int apic_simnd_resume(apic_sim_nd* sim, double time, uint64_t step);
+/* Simulation2D::step / Simulation3D::step (src/Simulation2D.cpp:1337-1364,
+ * src/Simulation3D.cpp:342-365) nsteps times; asynchronous. */
+APIC_EXPORT int apic_simnd_step(apic_sim_nd* sim, size_t nsteps);
+APIC_EXPORT int apic_simnd_synchronize(apic_sim_nd* sim);
+APIC_EXPORT int apic_simnd_count(apic_sim_nd* sim, int species, size_t* n);
+/* Particles in the order they were loaded, with the time-centred v of the
+ * reference's synchronize step (src/Pusher.cpp:131-186). */
+APIC_EXPORT int apic_simnd_read_particles(apic_sim_nd* sim, int species, size_t capacity, double* pos,
+                                          double* v, double* v_half, size_t* n);
+/* Mesh2D/Mesh3D rho(), phi(), electric_{x,y,z}() (E is [dims][N]). */
+APIC_EXPORT int apic_simnd_read_fields(apic_sim_nd* sim, double* rho, double* phi, double* electric);
+APIC_EXPORT int apic_simnd_sample(apic_sim_nd* sim, apic_sample_nd* out);
+APIC_EXPORT int apic_simnd_cuda_stream(apic_sim_nd* sim, void** stream);
+APIC_EXPORT int apic_simnd_set_kernel_timing(apic_sim_nd* sim, int enable);
+/* Summed milliseconds of the particle push, the field solve and the sorts,
+ * and the number of steps timed. */
+APIC_EXPORT int apic_simnd_kernel_times(apic_sim_nd* sim, double* push_ms, double* solve_ms, double* sort_ms,
+                                        uint64_t* steps);
+
+/* FieldSolver::solve(Mesh2D&/Mesh3D&) for a fully periodic mesh
+ * (src/FieldSolver.cpp:442-499, :659-731): rho (N values) -> phi (N) and
+ * E ([dims][N]). */
+APIC_EXPORT int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,
+                                             const double* rho, double* phi, double* electric);
+
 #ifdef __cplusplus
 }
 #endif
