@@ -47,6 +47,16 @@ struct SpeciesND {
     double* vh[2][3];
     unsigned* id[2];
     double* v[3];
+    // FP32 form: packed cell (10 bits per axis), in-cell offsets in [0, 1) and
+    // float velocities; the FP64 arrays above then only stage loads/read-backs
+    unsigned* cell[2];
+    float* off[2][3];
+    float* vel[2][3];
+    float hqmdt;       // 0.5 * qm * dt
+    float qmdt;        // qm * dt
+    float tb[3], sb[3];  // Boris t = hqmdt B and s = 2 t / (1 + t^2)
+    float drift[3];    // dt / d_a: cell units per unit velocity
+    float dep_fixed;   // dep * rho_scale
 };
 
 struct ParamsND {
@@ -57,8 +67,14 @@ struct ParamsND {
     double B[3];
     double rho_scale, inv_rho_scale;
     const double* E;  // interleaved: 2 doubles per node (2D) or 4 (3D)
+    const float* E32; // FP32 form: float copy of E
     unsigned long long* rho_acc;
 };
+
+// FP32 form: each CIC weight is rounded to a multiple of 2^-25 and summed per
+// species in 64-bit integers (runs of lanes in one cell first add theirs with a
+// single warp reduction), so the density does not depend on particle order.
+constexpr float kWeightScale = 33554432.0f;  // 2^25
 
 // wrap_periodic, src/FieldSolver.cpp:15-17, with the exact fast branch for |x| < 2L
 __device__ __forceinline__ double wrap_periodic(double x, double L) {
@@ -221,16 +237,15 @@ __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND&
         for (int k = 0; k < K; ++k) { a[k] = 0; node[k] = 0; }
     }
     const unsigned up = __shfl_up_sync(0xffffffffu, cell, 1);
-    const bool head = lane == 0 || up != cell;
+    const bool head = (lane & 7) == 0 || up != cell;  // runs capped at 8 lanes: three scan steps
     const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const unsigned upto = lane == 31 ? heads : (heads & ((2u << lane) - 1u));
-    const int start = 31 - __clz(upto);
+    const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
     const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         long long v = a[k];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
+        for (int d = 1; d < 8; d <<= 1) {
             const long long t = __shfl_up_sync(0xffffffffu, v, d);
             if (lane - d >= start) v += t;
         }
@@ -298,6 +313,226 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
         for (int a = 0; a < 3; ++a) S.vh[buf][a][i] = vh[a];
     }
     deposit_warp<DIM>(p, S, pos, valid);
+}
+
+// ---- FP32 particle form ---------------------------------------------------------
+//
+// A particle is a packed cell index (10 bits per axis), float offsets in
+// [0, 1) inside that cell and float velocities: 24 B (2D3V) or 28 B (3D3V) of
+// state instead of 40/48 B.  Positions never leave cell units, so the gather and
+// the deposit need no division and no wrap; the field solve, the fixed-point
+// density and the diagnostics stay FP64.
+
+__device__ __forceinline__ void unpack_cell(unsigned c, int& ix, int& iy, int& iz) {
+    ix = (int)(c & 1023u);
+    iy = (int)((c >> 10) & 1023u);
+    iz = (int)(c >> 20);
+}
+__device__ __forceinline__ unsigned pack_cell(int ix, int iy, int iz) {
+    return (unsigned)ix | ((unsigned)iy << 10) | ((unsigned)iz << 20);
+}
+
+template <int DIM>
+__device__ __forceinline__ void gather32(const ParamsND& p, int ix, int iy, int iz, const float f[3], float e[3]) {
+    const int nx = p.n[0], ny = p.n[1];
+    const int ix1 = (ix + 1) & (nx - 1), iy1 = (iy + 1) & (ny - 1);
+    const float wx[2] = {1.0f - f[0], f[0]}, wy[2] = {1.0f - f[1], f[1]};
+    if (DIM == 2) {
+        const float2* E = reinterpret_cast<const float2*>(p.E32);
+        const float2 a = E[iy * nx + ix], b = E[iy * nx + ix1], c = E[iy1 * nx + ix], d = E[iy1 * nx + ix1];
+        const float w00 = wx[0] * wy[0], w10 = wx[1] * wy[0], w01 = wx[0] * wy[1], w11 = wx[1] * wy[1];
+        e[0] = fmaf(a.x, w00, fmaf(b.x, w10, fmaf(c.x, w01, d.x * w11)));
+        e[1] = fmaf(a.y, w00, fmaf(b.y, w10, fmaf(c.y, w01, d.y * w11)));
+        e[2] = 0.0f;
+    } else {
+        const int iz1 = (iz + 1) & (p.n[2] - 1);
+        const float wz[2] = {1.0f - f[2], f[2]};
+        const int xx[2] = {ix, ix1}, yy[2] = {iy, iy1}, zz[2] = {iz, iz1};
+        const float4* E = reinterpret_cast<const float4*>(p.E32);
+        e[0] = e[1] = e[2] = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) {
+                const float wyz = wy[b] * wz[c];
+                const size_t row = ((size_t)zz[c] * ny + yy[b]) * nx;
+#pragma unroll
+                for (int a = 0; a < 2; ++a) {
+                    const float w = wx[a] * wyz;
+                    const float4 v = E[row + xx[a]];
+                    e[0] = fmaf(v.x, w, e[0]);
+                    e[1] = fmaf(v.y, w, e[1]);
+                    e[2] = fmaf(v.z, w, e[2]);
+                }
+            }
+    }
+}
+
+// Boris rotation in float (same algebra as boris_advance, src/Pusher.cpp:20-29)
+__device__ __forceinline__ void boris32(float v[3], const float e[3], float h, const float t[3], const float s[3]) {
+    const float vm0 = fmaf(h, e[0], v[0]), vm1 = fmaf(h, e[1], v[1]), vm2 = fmaf(h, e[2], v[2]);
+    const float vp0 = vm0 + fmaf(vm1, t[2], -vm2 * t[1]);
+    const float vp1 = vm1 + fmaf(vm2, t[0], -vm0 * t[2]);
+    const float vp2 = vm2 + fmaf(vm0, t[1], -vm1 * t[0]);
+    v[0] = fmaf(h, e[0], vm0 + fmaf(vp1, s[2], -vp2 * s[1]));
+    v[1] = fmaf(h, e[1], vm1 + fmaf(vp2, s[0], -vp0 * s[2]));
+    v[2] = fmaf(h, e[2], vm2 + fmaf(vp0, s[1], -vp1 * s[0]));
+}
+
+// Moves one axis by `disp` cells: integer carry into the periodic cell index.
+__device__ __forceinline__ void advance(float& f, int& i, float disp, int n) {
+    float g = f + disp;
+    const float k = floorf(g);
+    g -= k;
+    int ki = (int)k;
+    if (g >= 1.0f) { g -= 1.0f; ki += 1; }
+    f = g;
+    i = (i + ki) & (n - 1);
+}
+
+// Runs of lanes that share a cell (particles are sorted by cell) add their
+// 2^-25-quantised weights with a converged segmented shuffle scan; runs are
+// capped at 8 lanes so three shuffle steps suffice.  The last lane of each run
+// commits its sums with one 64-bit atomic per node.
+template <int DIM>
+__device__ __forceinline__ void deposit32_warp(const ParamsND& p, unsigned long long* acc, bool valid, int ix, int iy,
+                                               int iz, const float f[3]) {
+    const int lane = threadIdx.x & 31;
+    const int nx = p.n[0], ny = p.n[1];
+    const unsigned key = valid ? (((unsigned)iz * ny + iy) * nx + ix) : 0xFFFFFFFFu;
+    const unsigned prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = (lane & 7) == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    const int ix1 = (ix + 1) & (nx - 1), iy1 = (iy + 1) & (ny - 1);
+    const int iz1 = DIM == 3 ? (iz + 1) & (p.n[2] - 1) : 0;
+    const int xx[2] = {ix, ix1}, yy[2] = {iy, iy1}, zz[2] = {iz, iz1};
+    const float wx[2] = {1.0f - f[0], f[0]}, wy[2] = {1.0f - f[1], f[1]};
+    const float wz[2] = {DIM == 3 ? 1.0f - f[2] : 1.0f, DIM == 3 ? f[2] : 0.0f};
+#pragma unroll
+    for (int c = 0; c < (DIM == 3 ? 2 : 1); ++c)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                unsigned q = valid ? (unsigned)__float2int_rn(wx[a] * wy[b] * wz[c] * kWeightScale) : 0u;
+#pragma unroll
+                for (int d = 1; d < 8; d <<= 1) {
+                    const unsigned t = __shfl_up_sync(0xffffffffu, q, d);
+                    if (lane - d >= start) q += t;
+                }
+                if (tail && valid && q)
+                    atomicAdd(acc + ((size_t)zz[c] * ny + yy[b]) * nx + xx[a], (unsigned long long)q);
+            }
+}
+
+template <int DIM, bool BORIS, int MODE>
+__global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = i < S.n;
+    if ((MODE == kPushStep || MODE == kPushDepositOnly) && blockIdx.x * kThreads + (threadIdx.x & ~31u) >= S.n)
+        return;  // whole warp past the end
+    int ix = 0, iy = 0, iz = 0;
+    float f[3] = {0.0f, 0.0f, 0.0f}, v[3] = {0.0f, 0.0f, 0.0f};
+    if (valid) {
+        unpack_cell(S.cell[buf][i], ix, iy, iz);
+        for (int a = 0; a < DIM; ++a) f[a] = S.off[buf][a][i];
+        for (int a = 0; a < 3; ++a) v[a] = S.vel[buf][a][i];
+    }
+    if (MODE == kPushStep || MODE == kPushInitHalf || MODE == kPushSync) {
+        float e[3] = {0.0f, 0.0f, 0.0f};
+        if (valid) gather32<DIM>(p, ix, iy, iz, f, e);
+        if (MODE == kPushInitHalf || MODE == kPushSync) {
+            if (!valid) return;
+            float w[3] = {(float)S.v[0][i], (float)S.v[1][i], (float)S.v[2][i]};
+            float* vv = MODE == kPushInitHalf ? w : v;
+            const float h = MODE == kPushInitHalf ? -0.5f * S.hqmdt : 0.5f * S.hqmdt;
+            if (BORIS) {
+                float t[3], sb[3];
+                float t2 = 0.0f;
+                for (int a = 0; a < 3; ++a) { t[a] = S.tb[a] * (MODE == kPushInitHalf ? -0.5f : 0.5f); t2 = fmaf(t[a], t[a], t2); }
+                for (int a = 0; a < 3; ++a) sb[a] = 2.0f * t[a] / (1.0f + t2);
+                boris32(vv, e, h, t, sb);
+            } else {
+                for (int a = 0; a < DIM; ++a) vv[a] = fmaf(2.0f * h, e[a], vv[a]);
+            }
+            if (MODE == kPushInitHalf) {
+                for (int a = 0; a < 3; ++a) S.vel[buf][a][i] = vv[a];
+            } else {
+                for (int a = 0; a < 3; ++a) S.v[a][i] = (double)vv[a];
+            }
+            return;
+        }
+        // kick + drift
+        if (BORIS) {
+            boris32(v, e, S.hqmdt, S.tb, S.sb);
+        } else {
+            for (int a = 0; a < DIM; ++a) v[a] = fmaf(S.qmdt, e[a], v[a]);
+        }
+        int* idx[3] = {&ix, &iy, &iz};
+        for (int a = 0; a < DIM; ++a) advance(f[a], *idx[a], v[a] * S.drift[a], p.n[a]);
+        if (valid) {
+            S.cell[buf][i] = pack_cell(ix, iy, iz);
+            for (int a = 0; a < DIM; ++a) S.off[buf][a][i] = f[a];
+            for (int a = 0; a < 3; ++a) S.vel[buf][a][i] = v[a];
+        }
+    }
+    // ---- deposit ----
+    deposit32_warp<DIM>(p, acc, valid, ix, iy, iz, f);
+}
+
+// FP64 staging <-> FP32 state.  The cell/offset split follows the periodic CIC
+// index of the reference (wrap, divide by the cell size, floor).
+template <int DIM>
+__global__ void k_to_fp32(ParamsND p, SpeciesND S, int buf) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= S.n) return;
+    int ii[3] = {0, 0, 0};
+    for (int a = 0; a < DIM; ++a) {
+        const Axis ax = axis(S.pos[buf][a][i], p.L[a], p.d[a], p.n[a]);
+        float f = (float)ax.f;
+        int k = ax.i0;
+        if (f >= 1.0f) { f = 0.0f; k = ax.i1; }
+        ii[a] = k;
+        S.off[buf][a][i] = f;
+    }
+    S.cell[buf][i] = pack_cell(ii[0], ii[1], ii[2]);
+    for (int a = 0; a < 3; ++a) S.vel[buf][a][i] = (float)S.vh[buf][a][i];
+}
+
+template <int DIM>
+__global__ void k_to_fp64(ParamsND p, SpeciesND S, int buf) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= S.n) return;
+    int ii[3];
+    unpack_cell(S.cell[buf][i], ii[0], ii[1], ii[2]);
+    for (int a = 0; a < DIM; ++a) S.pos[buf][a][i] = ((double)ii[a] + (double)S.off[buf][a][i]) * p.d[a];
+    for (int a = 0; a < 3; ++a) S.vh[buf][a][i] = (double)S.vel[buf][a][i];
+}
+
+__device__ __forceinline__ unsigned linear_cell(const ParamsND& p, unsigned c) {
+    int x, y, z;
+    unpack_cell(c, x, y, z);
+    return ((unsigned)z * p.n[1] + y) * p.n[0] + x;
+}
+
+__global__ void k_cell_hist32(ParamsND p, SpeciesND S, int buf, unsigned* count) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i < S.n) atomicAdd(count + linear_cell(p, S.cell[buf][i]), 1u);
+}
+
+template <int DIM>
+__global__ void k_cell_scatter32(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= S.n) return;
+    const int to = from ^ 1;
+    const unsigned c = S.cell[from][i];
+    const unsigned o = atomicAdd(cursor + linear_cell(p, c), 1u);
+    S.cell[to][o] = c;
+    for (int a = 0; a < DIM; ++a) S.off[to][a][o] = S.off[from][a][i];
+    for (int a = 0; a < 3; ++a) S.vel[to][a][o] = S.vel[from][a][i];
+    S.id[to][o] = S.id[from][i];
 }
 
 // ---- particle sort by cell -------------------------------------------------------
@@ -466,43 +701,145 @@ struct FieldsND {
     Cplx* B;
     double* phi;
     double* E;
+    float* E32;  // FP32 form: interleaved float copy of E (2 or 4 floats per node)
+    int nacc;    // FP32 form: per-species weight accumulators
+    unsigned long long* acc[APIC_MAX_SPECIES];
+    double acc_scale[APIC_MAX_SPECIES];  // charge density per accumulator unit
 };
 
 __device__ __forceinline__ unsigned bitrev(unsigned x, int bits) { return __brev(x) >> (32 - bits); }
 
-// In-place radix-2 DIT transform of `T` lines stored bit-reversed in smem
-// (line stride `ld`); forward uses exp(-2 pi i k/n), inverse the conjugate and
-// a 1/n scale, as fft_radix2 does (src/FieldSolver.cpp:171-201).
-__device__ void fft_lines(Cplx* buf, int T, int ld, int n, int log2n, const Cplx* tw, bool inverse) {
-    const int half_total = T * (n >> 1);
-    for (int s = 1; s <= log2n; ++s) {
-        const int len = 1 << s, half = len >> 1;
-        const int tstride = n >> s;  // twiddle index step
-        for (int b = threadIdx.x; b < half_total; b += blockDim.x) {
-            const int l = b / (n >> 1);
-            const int j = b % (n >> 1);
-            const int grp = j / half, pos = j % half;
-            const int ia = l * ld + grp * len + pos;
-            const int ib = ia + half;
-            Cplx w = tw[pos * tstride];
-            if (inverse) w.im = -w.im;
-            const Cplx u = buf[ia], x = buf[ib];
-            const Cplx v = {x.re * w.re - x.im * w.im, x.re * w.im + x.im * w.re};
-            buf[ia] = {u.re + v.re, u.im + v.im};
-            buf[ib] = {u.re - v.re, u.im - v.im};
-        }
-        __syncthreads();
+// W16^k = exp(-2 pi i k / 16): cos and sin of 2 pi k / 16, k < 16.
+__device__ __forceinline__ double c16(int k) {
+    constexpr double a = 0.92387953251128675613, b = 0.70710678118654752440, c = 0.38268343236508977173;
+    switch (k & 15) {
+        case 0: return 1.0;  case 1: return a;   case 2: return b;   case 3: return c;
+        case 4: return 0.0;  case 5: return -c;  case 6: return -b;  case 7: return -a;
+        case 8: return -1.0; case 9: return -a;  case 10: return -b; case 11: return -c;
+        case 12: return 0.0; case 13: return c;  case 14: return b;  default: return a;
     }
-    if (inverse) {
+}
+__device__ __forceinline__ double s16(int k) { return c16(k + 12); }  // sin x = cos(x - pi/2)
+
+__device__ __forceinline__ Cplx cadd(Cplx x, Cplx y) { return {x.re + y.re, x.im + y.im}; }
+__device__ __forceinline__ Cplx csub(Cplx x, Cplx y) { return {x.re - y.re, x.im - y.im}; }
+// x * W16^k (forward) or x * conj(W16^k) (inverse)
+__device__ __forceinline__ Cplx cw16(Cplx x, int k, bool inv) {
+    const double wr = c16(k), wi = inv ? s16(k) : -s16(k);
+    return {x.re * wr - x.im * wi, x.re * wi + x.im * wr};
+}
+
+template <int R>
+__device__ __forceinline__ void dft_small(Cplx* a, bool inv);
+
+template <>
+__device__ __forceinline__ void dft_small<2>(Cplx* a, bool) {
+    const Cplx t = a[0];
+    a[0] = cadd(t, a[1]);
+    a[1] = csub(t, a[1]);
+}
+
+template <>
+__device__ __forceinline__ void dft_small<4>(Cplx* a, bool inv) {
+    const Cplx t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]), t2 = cadd(a[1], a[3]);
+    const Cplx d = csub(a[1], a[3]);
+    const Cplx t3 = inv ? Cplx{-d.im, d.re} : Cplx{d.im, -d.re};  // (+i) d or (-i) d
+    a[0] = cadd(t0, t2);
+    a[2] = csub(t0, t2);
+    a[1] = cadd(t1, t3);
+    a[3] = csub(t1, t3);
+}
+
+// R = R1 R2 point DFT from two smaller ones (index m = R2 m1 + m2 in, p = p1 + R1 p2 out).
+template <int R1, int R2>
+__device__ __forceinline__ void dft_split(Cplx* a, bool inv) {
+    constexpr int R = R1 * R2;
+    Cplx b[R2][R1];
+#pragma unroll
+    for (int m2 = 0; m2 < R2; ++m2) {
+        Cplx t[R1];
+#pragma unroll
+        for (int m1 = 0; m1 < R1; ++m1) t[m1] = a[R2 * m1 + m2];
+        dft_small<R1>(t, inv);
+#pragma unroll
+        for (int p1 = 0; p1 < R1; ++p1) b[m2][p1] = (p1 * m2 == 0) ? t[p1] : cw16(t[p1], p1 * m2 * (16 / R), inv);
+    }
+#pragma unroll
+    for (int p1 = 0; p1 < R1; ++p1) {
+        Cplx t[R2];
+#pragma unroll
+        for (int m2 = 0; m2 < R2; ++m2) t[m2] = b[m2][p1];
+        dft_small<R2>(t, inv);
+#pragma unroll
+        for (int p2 = 0; p2 < R2; ++p2) a[p1 + R1 * p2] = t[p2];
+    }
+}
+
+template <>
+__device__ __forceinline__ void dft_small<8>(Cplx* a, bool inv) { dft_split<4, 2>(a, inv); }
+template <>
+__device__ __forceinline__ void dft_small<16>(Cplx* a, bool inv) { dft_split<4, 4>(a, inv); }
+
+template <int R>
+__device__ __forceinline__ void dft_reg(Cplx (&a)[R], bool inv) { dft_small<R>(a, inv); }
+
+// One Stockham radix-R stage over `lines` lines of n points (src -> dst):
+// butterfly j reads src[j + m n/R], twiddles by w^(k m) with k = j mod L and
+// w = exp(-2 pi i / (L R)), and writes dst[(j - k) R + k + p L].
+template <int R>
+__device__ void stockham_stage(const Cplx* __restrict__ src, Cplx* __restrict__ dst, int lines, int n, int L,
+                               const Cplx* tw, bool inv) {
+    const int nb = n / R;
+    const int tstep = n / (L * R);
+    for (int b = threadIdx.x; b < lines * nb; b += blockDim.x) {
+        const int l = b / nb, j = b - l * nb;
+        const int k = j & (L - 1);
+        const Cplx* s = src + l * n;
+        Cplx a[R];
+#pragma unroll
+        for (int m = 0; m < R; ++m) a[m] = s[j + m * nb];
+        if (L > 1) {
+#pragma unroll
+            for (int m = 1; m < R; ++m) {
+                Cplx w = tw[k * m * tstep];
+                if (inv) w.im = -w.im;
+                const Cplx x = a[m];
+                a[m] = {x.re * w.re - x.im * w.im, x.re * w.im + x.im * w.re};
+            }
+        }
+        dft_reg<R>(a, inv);
+        Cplx* d = dst + l * n;
+        const int o = (j - k) * R + k;
+#pragma unroll
+        for (int p = 0; p < R; ++p) d[o + p * L] = a[p];
+    }
+    __syncthreads();
+}
+
+// Transforms `lines` lines held in buf0 (buf1 is scratch of the same size);
+// returns the buffer that holds the result.  Forward uses exp(-2 pi i k/n),
+// inverse the conjugate and a 1/n scale per line, as fft_radix2 does
+// (src/FieldSolver.cpp:171-201); the twiddles are exact table values.
+__device__ Cplx* fft_lines(Cplx* buf0, Cplx* buf1, int lines, int n, const Cplx* tw, bool inv) {
+    Cplx* src = buf0;
+    Cplx* dst = buf1;
+    int L = 1, rem = n;
+    while (rem > 1) {
+        if (rem % 16 == 0) { stockham_stage<16>(src, dst, lines, n, L, tw, inv); L *= 16; rem /= 16; }
+        else if (rem % 8 == 0) { stockham_stage<8>(src, dst, lines, n, L, tw, inv); L *= 8; rem /= 8; }
+        else if (rem % 4 == 0) { stockham_stage<4>(src, dst, lines, n, L, tw, inv); L *= 4; rem /= 4; }
+        else { stockham_stage<2>(src, dst, lines, n, L, tw, inv); L *= 2; rem /= 2; }
+        Cplx* t = src; src = dst; dst = t;
+    }
+    if (inv) {
         const double sc = 1.0 / (double)n;
-        for (int b = threadIdx.x; b < T * n; b += blockDim.x) {
-            const int l = b / n, e = b % n;
-            Cplx& c = buf[l * ld + e];
-            c.re *= sc;
-            c.im *= sc;
+        for (int b = threadIdx.x; b < lines * n; b += blockDim.x) {
+            src[b].re *= sc;
+            src[b].im *= sc;
         }
         __syncthreads();
     }
+    return src;
 }
 
 __device__ __forceinline__ long long tile_base(const FftPass& f, long long tile) {
@@ -518,11 +855,16 @@ __device__ __forceinline__ void tile_elem(const FftPass& f, int b, int& l, int& 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
     extern __shared__ __align__(16) unsigned char fsm[];
+    // shared memory: region0 (2 T lines) and region1 (2 T lines), then the
+    // n twiddles; a single array ping-pongs inside region0, an (A, B) pair
+    // occupies 2 T lines and ping-pongs between the two regions
     const int ld = f.n;
-    Cplx* X = reinterpret_cast<Cplx*>(fsm);
-    Cplx* Y = X + f.T * ld;  // second array (A/B pair passes)
-    Cplx* tws = Y + ((MODE == kFwdMulInv || MODE == kInvInPlace || MODE == kInvToFields) ? 2 : 0) * f.T * ld;
-    for (int k = threadIdx.x; k < (f.n >> 1); k += blockDim.x) tws[k] = f.tw[k];
+    Cplx* R0 = reinterpret_cast<Cplx*>(fsm);
+    Cplx* R1 = R0 + 2 * f.T * ld;
+    Cplx* tws = R1 + ((MODE == kFwdFromRho || MODE == kFwdInPlace) ? 0 : 2 * f.T * ld);
+    for (int k = threadIdx.x; k < f.n; k += blockDim.x) tws[k] = f.tw[k];
+    Cplx* X = R0;
+    Cplx* Y = R0 + f.T * ld;  // B lines of a pair, right after the A lines
     const long long base = tile_base(f, blockIdx.x);
     const int total = f.T * f.n;
     // ---- load (bit-reversed within each line) ----
@@ -530,11 +872,23 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
         int l, e;
         tile_elem(f, b, l, e);
         const long long g = base + l * f.ls + e * f.es;
-        const int s = l * ld + bitrev(e, f.log2n);
+        const int s = l * ld + e;
         if (MODE == kFwdFromRho) {
             double r;
             if (F.rho_in) {
                 r = F.rho_in[g];
+            } else if (F.nacc) {
+                unsigned long long q[APIC_MAX_SPECIES] = {0, 0, 0, 0};
+#pragma unroll
+                for (int k = 0; k < APIC_MAX_SPECIES; ++k)
+                    if (k < F.nacc) q[k] = F.acc[k][g];
+                r = 0.0;
+#pragma unroll
+                for (int k = 0; k < APIC_MAX_SPECIES; ++k)
+                    if (k < F.nacc) {
+                        r += (double)(long long)q[k] * F.acc_scale[k];
+                        F.acc[k][g] = 0ull;
+                    }
             } else {
                 r = (double)(long long)F.rho_acc[g] * F.inv_scale;
                 F.rho_acc[g] = 0ull;
@@ -550,8 +904,11 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
     }
     __syncthreads();
     const bool inverse_first = (MODE == kInvInPlace || MODE == kInvToFields);
-    fft_lines(X, f.T, ld, f.n, f.log2n, tws, inverse_first);
-    if (inverse_first) fft_lines(Y, f.T, ld, f.n, f.log2n, tws, true);
+    Cplx* res;
+    if (inverse_first) res = fft_lines(R0, R1, 2 * f.T, f.n, tws, true);           // A and B together
+    else res = fft_lines(X, X + f.T * ld, f.T, f.n, tws, false);                    // ping-pong inside region0
+    X = res;
+    Y = res + f.T * ld;
     if (MODE == kFwdMulInv) {
         // k-space multiply (src/FieldSolver.cpp:470-488, :687-712) into two packed
         // spectra A = phi_k + i Ex_k / pack, B = Ey_k / pack + i Ez_k / pack,
@@ -566,7 +923,7 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
             const int ix = (int)(g % F.nx);
             const int iy = (int)((g / F.nx) % F.ny);
             const int iz = F.dims == 3 ? (int)(g / ((long long)F.nx * F.ny)) : 0;
-            const Cplx r = X[l * ld + e];  // natural order after the forward transform
+            const Cplx r = X[l * ld + e];
             Cplx a = {0.0, 0.0}, bb = {0.0, 0.0};
             if (ix != 0 || iy != 0 || iz != 0) {
                 const double mx = ix <= F.nx / 2 ? (double)ix : -(double)(F.nx - ix);
@@ -593,12 +950,14 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
                 a = {pr - exi * ip, pi + exr * ip};
                 bb = {eyr * ip - ezi * ip, eyi * ip + ezr * ip};
             }
-            const int s = l * ld + bitrev(e, f.log2n);
-            Y[s] = a;
-            Y[f.T * ld + s] = bb;
+            const int s = l * ld + e;
+            R1[s] = a;
+            R1[f.T * ld + s] = bb;
         }
         __syncthreads();
-        fft_lines(Y, 2 * f.T, ld, f.n, f.log2n, tws, true);
+        Cplx* pair = fft_lines(R1, R0, 2 * f.T, f.n, tws, true);
+        X = pair;
+        Y = pair + f.T * ld;
     }
     // ---- store ----
     for (int b = threadIdx.x; b < total; b += blockDim.x) {
@@ -609,8 +968,8 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
         if (MODE == kFwdFromRho || MODE == kFwdInPlace) {
             F.W[g] = X[s];
         } else if (MODE == kFwdMulInv) {
-            F.A[g] = Y[s];
-            F.B[g] = Y[f.T * ld + s];
+            F.A[g] = X[s];
+            F.B[g] = Y[s];
         } else if (MODE == kInvInPlace) {
             F.A[g] = X[s];
             F.B[g] = Y[s];
@@ -619,8 +978,12 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
             F.phi[g] = a.re;
             if (F.dims == 2) {
                 reinterpret_cast<double2*>(F.E)[g] = make_double2(a.im * F.pack, bb.re * F.pack);
+                if (F.E32) reinterpret_cast<float2*>(F.E32)[g] = make_float2((float)(a.im * F.pack), (float)(bb.re * F.pack));
             } else {
                 reinterpret_cast<double4*>(F.E)[g] = make_double4(a.im * F.pack, bb.re * F.pack, bb.im * F.pack, 0.0);
+                if (F.E32)
+                    reinterpret_cast<float4*>(F.E32)[g] =
+                        make_float4((float)(a.im * F.pack), (float)(bb.re * F.pack), (float)(bb.im * F.pack), 0.0f);
             }
         }
     }
@@ -691,7 +1054,8 @@ static int ilog2(size_t v) { int k = 0; while ((size_t(1) << k) < v) ++k; return
 
 struct Solver {
     FieldsND F{};
-    FftPass px{}, py{}, pz{};
+    FftPass px{}, py{}, pz{};    // paired passes (four line buffers)
+    FftPass pxs{}, pys{};        // single-array forward passes (two line buffers)
     size_t smem_fwd = 0, smem_pair = 0;
     std::vector<void*>* allocs = nullptr;
     cudaStream_t stream = nullptr;
@@ -706,9 +1070,9 @@ struct Solver {
     }
 
     Cplx* twiddles(int n) {
-        std::vector<Cplx> h(n / 2);
+        std::vector<Cplx> h(n);
         const double twopi = 2.0 * 3.141592653589793;
-        for (int k = 0; k < n / 2; ++k) h[k] = {std::cos(twopi * k / n), -std::sin(twopi * k / n)};
+        for (int k = 0; k < n; ++k) h[k] = {std::cos(twopi * k / n), -std::sin(twopi * k / n)};
         Cplx* d = alloc<Cplx>(h.size());
         APIC_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaStreamSynchronize(stream));
@@ -758,17 +1122,21 @@ struct Solver {
         F.E = alloc<double>(N * (dims == 2 ? 2 : 4));
         // lines per tile: up to 8 (128 B rows in the strided passes), bounded
         // so that the paired passes (three line buffers) fit in shared memory
-        auto lines = [](int n, long long available) {
+        // lines per tile: up to 8 (128 B rows in the strided passes), bounded
+        // so that two CTAs fit on an SM (about 100 KB of shared memory each)
+        auto lines = [](int n, long long available, int buffers) {
             int T = 8;
-            while (T > 1 && (size_t)3 * T * n * sizeof(Cplx) + (n / 2) * sizeof(Cplx) > 200 * 1024) T >>= 1;
+            while (T > 1 && (size_t)buffers * T * n * sizeof(Cplx) + n * sizeof(Cplx) > 100 * 1024) T >>= 1;
             while (T > 1 && available % T) T >>= 1;
             return T;
         };
-        px = pass(0, lines(F.nx, (long long)F.ny * F.nz));
-        py = pass(1, lines(F.ny, F.nx));
-        if (dims == 3) pz = pass(2, lines(F.nz, F.nx));
-        px.tw = twiddles(F.nx);
-        py.tw = F.ny == F.nx ? px.tw : twiddles(F.ny);
+        px = pass(0, lines(F.nx, (long long)F.ny * F.nz, 4));
+        pxs = pass(0, lines(F.nx, (long long)F.ny * F.nz, 2));
+        py = pass(1, lines(F.ny, F.nx, 4));
+        pys = pass(1, lines(F.ny, F.nx, 2));
+        if (dims == 3) pz = pass(2, lines(F.nz, F.nx, 4));
+        px.tw = pxs.tw = twiddles(F.nx);
+        py.tw = pys.tw = F.ny == F.nx ? px.tw : twiddles(F.ny);
         if (dims == 3) pz.tw = F.nz == F.nx ? px.tw : (F.nz == F.ny ? py.tw : twiddles(F.nz));
         smem_pair = std::max(smem_of(px, kFwdMulInv), smem_of(py, kFwdMulInv));
         if (dims == 3) smem_pair = std::max(smem_pair, smem_of(pz, kFwdMulInv));
@@ -781,19 +1149,19 @@ struct Solver {
 
     size_t smem_of(const FftPass& f, int mode) const {
         const size_t line = (size_t)f.T * f.n * sizeof(Cplx);
-        const size_t tw = (size_t)(f.n / 2) * sizeof(Cplx);
-        return (mode == kFwdFromRho || mode == kFwdInPlace) ? line + tw : 3 * line + tw;
+        const size_t tw = (size_t)f.n * sizeof(Cplx);
+        return (mode == kFwdFromRho || mode == kFwdInPlace) ? 2 * line + tw : 4 * line + tw;
     }
 
     // rho_acc -> rho, phi, E (the fixed-point accumulator is cleared)
     void solve() {
         if (F.dims == 2) {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(px), kThreads, smem_of(px, kFwdFromRho), stream>>>(F, px);
+            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
             k_fft<kFwdMulInv><<<(unsigned)tiles(py), kThreads, smem_of(py, kFwdMulInv), stream>>>(F, py);
             k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
         } else {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(px), kThreads, smem_of(px, kFwdFromRho), stream>>>(F, px);
-            k_fft<kFwdInPlace><<<(unsigned)tiles(py), kThreads, smem_of(py, kFwdInPlace), stream>>>(F, py);
+            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
+            k_fft<kFwdInPlace><<<(unsigned)tiles(pys), kThreads, smem_of(pys, kFwdInPlace), stream>>>(F, pys);
             k_fft<kFwdMulInv><<<(unsigned)tiles(pz), kThreads, smem_of(pz, kFwdMulInv), stream>>>(F, pz);
             k_fft<kInvInPlace><<<(unsigned)tiles(py), kThreads, smem_of(py, kInvInPlace), stream>>>(F, py);
             k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
@@ -812,6 +1180,7 @@ struct SimND {
     int buf[APIC_MAX_SPECIES] = {0, 0, 0, 0};
     Solver solver;
     bool boris = false;
+    bool fp32 = false;
     bool initialized = false;
     double time = 0.0;
     uint64_t step_count = 0;
@@ -849,7 +1218,8 @@ struct SimND {
     void create(const apic_config_nd& c) {
         cfg = c;
         require(c.dims == 2 || c.dims == 3, "dims must be 2 or 3");
-        require(c.precision == APIC_FP64, "this entry point builds the FP64 form", APIC_ERR_UNSUPPORTED);
+        require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
+        fp32 = c.precision == APIC_FP32;
         for (int a = 0; a < c.dims; ++a) {
             require(c.n[a] >= 3, "mesh extents must be at least 3");
             require(pow2(c.n[a]) && c.n[a] <= (size_t)kMaxLine,
@@ -908,12 +1278,36 @@ struct SimND {
                 D.id[b] = dalloc<unsigned>(S.capacity);
             }
             for (int a = 0; a < 3; ++a) D.v[a] = dalloc<double>(S.capacity);
+            if (fp32) {
+                for (int b = 0; b < 2; ++b) {
+                    D.cell[b] = dalloc<unsigned>(S.capacity);
+                    for (int a = 0; a < c.dims; ++a) D.off[b][a] = dalloc<float>(S.capacity);
+                    for (int a = 0; a < 3; ++a) D.vel[b][a] = dalloc<float>(S.capacity);
+                }
+            }
+            const double hq = 0.5 * D.qm * c.dt;
+            D.hqmdt = (float)hq;
+            D.qmdt = (float)(D.qm * c.dt);
+            double t2 = 0.0;
+            for (int a = 0; a < 3; ++a) { D.tb[a] = (float)(hq * c.magnetic_field[a]); t2 += (hq * c.magnetic_field[a]) * (hq * c.magnetic_field[a]); }
+            for (int a = 0; a < 3; ++a) D.sb[a] = (float)(2.0 * hq * c.magnetic_field[a] / (1.0 + t2));
+            for (int a = 0; a < 3; ++a) D.drift[a] = a < c.dims ? (float)(c.dt / p.d[a]) : 0.0f;
+            D.dep_fixed = (float)(D.dep * p.rho_scale);
         }
         solver.allocs = &allocations;
         solver.stream = stream;
         solver.setup(c.dims, c.n, c.length, p.eps, p.inv_rho_scale);
         p.E = solver.F.E;
         p.rho_acc = solver.F.rho_acc;
+        if (fp32) {
+            solver.F.E32 = dalloc<float>(N * (c.dims == 2 ? 2 : 4));
+            p.E32 = solver.F.E32;
+            solver.F.nacc = c.nspecies;
+            for (int s = 0; s < c.nspecies; ++s) {
+                solver.F.acc[s] = dalloc<unsigned long long>(N);
+                solver.F.acc_scale[s] = sp[s].dep / (double)kWeightScale;
+            }
+        }
         cell_count = dalloc<unsigned>(N);
         cell_offset = dalloc<unsigned>(N);
         block_sums = dalloc<unsigned>((N + kScanBlock - 1) / kScanBlock + 1);
@@ -931,6 +1325,17 @@ struct SimND {
         if (S.n == 0) return;
         const unsigned blocks = (S.n + kThreads - 1) / kThreads;
         const int b = buf[s];
+        if (fp32) {
+            if (cfg.dims == 2) {
+                if (boris) k_push32<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                else k_push32<2, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+            } else {
+                if (boris) k_push32<3, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                else k_push32<3, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+            }
+            APIC_CUDA(cudaGetLastError());
+            return;
+        }
         if (cfg.dims == 2) {
             if (boris) k_push<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
             else k_push<2, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
@@ -947,15 +1352,40 @@ struct SimND {
         const unsigned blocks = (S.n + kThreads - 1) / kThreads;
         const unsigned nb = (unsigned)((ncells + kScanBlock - 1) / kScanBlock);
         APIC_CUDA(cudaMemsetAsync(cell_count, 0, ncells * sizeof(unsigned), stream));
-        if (cfg.dims == 2) k_cell_hist<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
+        if (fp32) k_cell_hist32<<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
+        else if (cfg.dims == 2) k_cell_hist<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
         else k_cell_hist<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_count);
         k_scan_local<<<nb, kThreads, 0, stream>>>(cell_count, cell_offset, block_sums, (unsigned)ncells);
         k_scan_blocks<<<1, kThreads, 0, stream>>>(block_sums, nb);
         k_scan_add<<<nb, kThreads, 0, stream>>>(cell_offset, block_sums, (unsigned)ncells);
-        if (cfg.dims == 2) k_cell_scatter<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
-        else k_cell_scatter<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        if (fp32) {
+            if (cfg.dims == 2) k_cell_scatter32<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+            else k_cell_scatter32<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        } else if (cfg.dims == 2) {
+            k_cell_scatter<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        } else {
+            k_cell_scatter<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+        }
         APIC_CUDA(cudaGetLastError());
         buf[s] ^= 1;
+    }
+
+    void to_fp32(int s) {
+        const SpeciesND& S = sp[s];
+        if (!fp32 || S.n == 0) return;
+        const unsigned blocks = (S.n + kThreads - 1) / kThreads;
+        if (cfg.dims == 2) k_to_fp32<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s]);
+        else k_to_fp32<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s]);
+        APIC_CUDA(cudaGetLastError());
+    }
+
+    void to_fp64(int s) {
+        const SpeciesND& S = sp[s];
+        if (!fp32 || S.n == 0) return;
+        const unsigned blocks = (S.n + kThreads - 1) / kThreads;
+        if (cfg.dims == 2) k_to_fp64<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s]);
+        else k_to_fp64<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s]);
+        APIC_CUDA(cudaGetLastError());
     }
 
     void load(int s, size_t n, const double* pos, const double* v, const double* vh) {
@@ -977,6 +1407,7 @@ struct SimND {
         APIC_CUDA(cudaMemcpyAsync(S.id[b], ids.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaStreamSynchronize(stream));
         S.n = (unsigned)n;
+        to_fp32(s);
         initialized = false;
     }
 
@@ -991,6 +1422,7 @@ struct SimND {
                                                                    p.L[1], p.L[2], vt, drift, axis, amp);
         APIC_CUDA(cudaGetLastError());
         S.n = (unsigned)n;
+        to_fp32(s);
         initialized = false;
     }
 
@@ -1071,6 +1503,7 @@ struct SimND {
         const SpeciesND& S = sp[s];
         const size_t n = S.n;
         require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
+        if (fp32) to_fp64(s);
         if (initialized) launch_push<kPushSync>(s);  // time-centred v of the current state
         const int b = buf[s];
         const int o = b ^ 1;

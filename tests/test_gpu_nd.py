@@ -78,3 +78,53 @@ def test_sort_keeps_identity_and_fields():
             assert np.array_equal(x, y)
     for x, y in zip(dev_a.fields(), dev_b.fields()):
         assert np.array_equal(x, y)  # fixed-point deposit: independent of particle order
+
+
+@pytest.mark.parametrize("case", ["2d_boris", "3d_boris"])
+def test_fp32_form_against_fp64_oracle(case):
+    """FP32 particles (packed cell + float offsets + float velocities) against the
+    FP64 oracle on the same inputs: positions within 1e-5 of a cell, velocities
+    within 1e-5 of the thermal scale, fields within 1e-4 (max-norm relative)."""
+    wl = W.plasma_2d(cells=(32, 16), ppc=8, seed=3) if case == "2d_boris" else W.plasma_3d(cells=(16, 8, 8), ppc=4, seed=5)
+    steps = 10
+    cfg = W.to_device_config_nd(wl, precision=apic.FP32, sort_interval=4)
+    dev = apic.SimulationND(cfg)
+    eps = 8.8541878128e-12
+    ora = po.SimND(wl.dims, wl.n, wl.length, wl.dt, eps, wl.B, [(q, m, w) for (q, m, w, pos, v) in wl.species])
+    for k, (q, m, w, pos, v) in enumerate(wl.species):
+        dev.load(k, pos, v)
+        ora.load(k, pos, v, v)
+    dev.initialize()
+    ora.initialize()
+    dev.step(steps)
+    ora.step(steps)
+    for k in range(2):
+        a, b = dev.particles(k), ora.particles(k)
+        cell = wl.length[0] / wl.n[0]
+        dpos = np.abs(a[0][: wl.dims] - b[0][: wl.dims])
+        dpos = np.minimum(dpos, np.array(wl.length)[: wl.dims, None] - dpos)  # periodic distance
+        assert dpos.max() < 1e-5 * cell, (k, dpos.max() / cell)
+        vs = np.max(np.abs(b[2]))
+        assert np.max(np.abs(a[2] - b[2])) < 1e-5 * vs
+    fa, fb = dev.fields(), ora.fields()
+    for name, x, y in zip(("rho", "phi", "E"), fa, fb):
+        assert rel_max(x, y) < 1e-4, (name, rel_max(x, y))
+
+
+def test_fp32_energy_conservation_2d():
+    """A larger FP32 2D run conserves total energy like the FP64 form does."""
+    wl = W.plasma_2d(cells=(64, 64), ppc=16, seed=21)
+    res = {}
+    for prec in (apic.FP64, apic.FP32):
+        dev = apic.SimulationND(W.to_device_config_nd(wl, precision=prec))
+        for k, (q, m, w, pos, v) in enumerate(wl.species):
+            dev.load(k, pos, v)
+        dev.initialize()
+        e0 = dev.sample().total_energy
+        dev.step(50)
+        e1 = dev.sample().total_energy
+        res[prec] = (e0, e1)
+    drift64 = abs(res[apic.FP64][1] - res[apic.FP64][0]) / res[apic.FP64][0]
+    drift32 = abs(res[apic.FP32][1] - res[apic.FP32][0]) / res[apic.FP32][0]
+    assert abs(res[apic.FP32][0] - res[apic.FP64][0]) < 1e-5 * res[apic.FP64][0]
+    assert drift32 < max(2 * drift64, 1e-4), (drift32, drift64)
