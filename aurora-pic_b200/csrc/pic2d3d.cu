@@ -22,6 +22,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1733,3 +1734,146 @@ int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length
 }
 
 }  // extern "C"
+
+// ---- allocation-free periodic field solve --------------------------------------
+//
+// Some callers cannot call cudaMalloc: hosts that own every byte of device
+// memory through their own pool or arena, and time-stepping loops that must not
+// hit cudaMalloc's implicit device synchronisation (or run where allocation is
+// not allowed).  apic_field_solve_periodic_nd_noalloc serves them: the caller
+// passes device buffers for rho, phi and E, and the FFT work arrays live in the
+// file-scope device array below, which every GPU that loads this library keeps
+// until the process exits.
+
+namespace apic {
+namespace nd {
+
+constexpr size_t kNoAllocMaxPoints = 65536;  // largest mesh (nx * ny * nz) the array serves
+constexpr size_t kNoAllocMaxLine = 1024;     // largest extent per axis
+// W, A, B (complex), interleaved E (4 doubles), rho copy, and three twiddle tables
+constexpr size_t kNoAllocScratchBytes =
+    3 * kNoAllocMaxPoints * sizeof(Cplx) + 4 * kNoAllocMaxPoints * sizeof(double) +
+    kNoAllocMaxPoints * sizeof(double) + 3 * kNoAllocMaxLine * sizeof(Cplx);
+
+static __device__ __align__(256) unsigned char g_solve_scratch[kNoAllocScratchBytes];
+
+// exp(-2 pi i k / n), k < n
+__global__ void k_noalloc_twiddles(Cplx* tw, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    double s, c;
+    sincospi(2.0 * (double)k / (double)n, &s, &c);
+    tw[k] = {c, -s};
+}
+
+// interleaved E (2 or 4 doubles per node) -> [dims][N]
+__global__ void k_noalloc_deinterleave(const double* E, int dims, long long N, double* out) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= N) return;
+    const int st = dims == 2 ? 2 : 4;
+    for (int c = 0; c < dims; ++c) out[c * N + g] = E[g * st + c];
+}
+
+}  // namespace nd
+}  // namespace apic
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[64] = {};
+}  // namespace
+
+extern "C" int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, const double* length,
+                                                     double permittivity, const double* d_rho, double* d_phi,
+                                                     double* d_electric, void* stream) {
+    using namespace apic::nd;
+    return guarded_nd(nullptr, [&] {
+        apic::require(dims == 2 || dims == 3, "dims must be 2 or 3");
+        apic::require(n && length && d_rho && d_phi && d_electric, "null argument");
+        apic::require(std::isfinite(permittivity) && permittivity > 0,
+                      "field-solver permittivity must be positive and finite");
+        size_t N = 1;
+        for (int a = 0; a < dims; ++a) {
+            apic::require(pow2(n[a]) && n[a] <= kNoAllocMaxLine,
+                          "allocation-free solve: extents must be powers of two up to 1024", APIC_ERR_UNSUPPORTED);
+            apic::require(std::isfinite(length[a]) && length[a] > 0, "domain lengths must be positive and finite");
+            N *= n[a];
+        }
+        apic::require(N <= kNoAllocMaxPoints,
+                      "allocation-free solve: mesh has " + std::to_string(N) + " points, the scratch array holds " +
+                          std::to_string(kNoAllocMaxPoints),
+                      APIC_ERR_CAPACITY);
+        int dev = 0;
+        APIC_CUDA(cudaGetDevice(&dev));
+        apic::require(dev >= 0 && dev < 64, "device index out of range");
+        void* base = nullptr;
+        {
+            // once per device, with that device current: the scratch array's
+            // device address, and the shared-memory limit of the FFT kernels
+            std::lock_guard<std::mutex> lock(g_noalloc_mu);
+            if (!g_noalloc_ptr[dev]) {
+                void* p = nullptr;
+                APIC_CUDA(cudaGetSymbolAddress(&p, g_solve_scratch));
+                g_noalloc_ptr[dev] = p;
+            }
+            base = g_noalloc_ptr[dev];
+            // the FFT tiles below stay under 118 KB of shared memory
+            const int smem = 118 * 1024;
+            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdFromRho>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        }
+        unsigned char* bytes = static_cast<unsigned char*>(base);
+        Cplx* W = reinterpret_cast<Cplx*>(bytes);
+        Cplx* A = W + kNoAllocMaxPoints;
+        Cplx* B = A + kNoAllocMaxPoints;
+        double* E = reinterpret_cast<double*>(B + kNoAllocMaxPoints);
+        double* rho = E + 4 * kNoAllocMaxPoints;
+        Cplx* tw = reinterpret_cast<Cplx*>(rho + kNoAllocMaxPoints);
+        cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+        Solver S;
+        S.stream = s;
+        FieldsND& F = S.F;
+        F.dims = dims;
+        F.nx = (int)n[0];
+        F.ny = (int)n[1];
+        F.nz = dims == 3 ? (int)n[2] : 1;
+        for (int a = 0; a < 3; ++a) F.L[a] = a < dims ? length[a] : 1.0;
+        F.eps = permittivity;
+        F.inv_scale = 1.0;
+        double kmax = 0;
+        for (int a = 0; a < dims; ++a) kmax = std::max(kmax, 3.141592653589793 * (double)n[a] / length[a]);
+        F.pack = std::ldexp(1.0, (int)std::lround(std::log2(kmax)));
+        F.rho_in = d_rho;  // every scratch element below is written before it is read
+        F.rho = rho;
+        F.W = W;
+        F.A = A;
+        F.B = B;
+        F.phi = d_phi;
+        F.E = E;
+        auto lines = [](int len, long long available, int buffers) {
+            int T = 8;
+            while (T > 1 && (size_t)buffers * T * len * sizeof(Cplx) + len * sizeof(Cplx) > 100 * 1024) T >>= 1;
+            while (T > 1 && available % T) T >>= 1;
+            return T;
+        };
+        S.px = S.pass(0, lines(F.nx, (long long)F.ny * F.nz, 4));
+        S.pxs = S.pass(0, lines(F.nx, (long long)F.ny * F.nz, 2));
+        S.py = S.pass(1, lines(F.ny, F.nx, 4));
+        S.pys = S.pass(1, lines(F.ny, F.nx, 2));
+        if (dims == 3) S.pz = S.pass(2, lines(F.nz, F.nx, 4));
+        const int len[3] = {F.nx, F.ny, F.nz};
+        for (int a = 0; a < dims; ++a) {
+            k_noalloc_twiddles<<<(len[a] + 255) / 256, 256, 0, s>>>(tw + a * kNoAllocMaxLine, len[a]);
+        }
+        S.px.tw = S.pxs.tw = tw;
+        S.py.tw = S.pys.tw = tw + kNoAllocMaxLine;
+        if (dims == 3) S.pz.tw = tw + 2 * kNoAllocMaxLine;
+        APIC_CUDA(cudaGetLastError());
+        S.solve();
+        k_noalloc_deinterleave<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(E, dims, (long long)N, d_electric);
+        APIC_CUDA(cudaGetLastError());
+    });
+}

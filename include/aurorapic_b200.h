@@ -348,6 +348,24 @@ APIC_EXPORT int apic_simnd_kernel_times(apic_sim_nd* sim, double* push_ms, doubl
 APIC_EXPORT int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,
                                              const double* rho, double* phi, double* electric);
 
+/* Allocation-free variant of apic_field_solve_periodic_nd.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc - hosts that
+ * manage all device memory through their own pool, and stepping loops that must
+ * not trigger cudaMalloc's implicit synchronisation.  d_rho (N values), d_phi
+ * (N) and d_electric ([dims][N]) are DEVICE pointers owned by the caller; the
+ * FFT work arrays live in a static device array inside the library (about
+ * 5.8 MB, kept by every GPU that loads the library until the process exits),
+ * so N = nx*ny*nz may not exceed 65536 (APIC_ERR_CAPACITY beyond) and each
+ * extent must be a power of two up to 1024.  The first call on a device looks
+ * up that array's device address; make it before any stream capture.  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the
+ * call returns without waiting.  Every call shares the one array, so calls
+ * whose work overlaps on the GPU (different streams, or different host
+ * threads on one device) race; serialise them on one stream. */
+APIC_EXPORT int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, const double* length,
+                                                     double permittivity, const double* d_rho, double* d_phi,
+                                                     double* d_electric, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
