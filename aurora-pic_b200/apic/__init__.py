@@ -505,6 +505,17 @@ class SimulationND:
         return a.value, b.value, c.value, n.value
 
 
+def _simnd_launch_count(self):
+    n = C.c_uint64()
+    L = _bind_nd()
+    L.apic_simnd_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+    _check_nd(L.apic_simnd_launch_count(self.h, C.byref(n)), self.h)
+    return n.value
+
+
+SimulationND.launch_count = _simnd_launch_count
+
+
 def field_solve_periodic_nd(dims, n, length, permittivity, rho):
     N = int(np.prod(n[:dims]))
     rho = np.ascontiguousarray(rho, dtype=np.float64)

@@ -44,6 +44,9 @@ class ChannelSpec:
     threshold: float = 0.0  # J
     secondary: int = -1
     ion: int = -1
+    angular: int = 0        # 0 isotropic, 1 backward, 2 Henyey-Greenstein
+    mu_energy: np.ndarray | None = None  # J, Henyey-Greenstein mean-cosine table
+    mu: np.ndarray | None = None
 
 
 @dataclass
@@ -253,3 +256,150 @@ def to_device_config_nd(wl: WorkloadND, precision=0, capacity_factor=1.0, sort_i
     sp = [(q, m, w, int(pos.shape[1] * capacity_factor) + 1) for (q, m, w, pos, v) in wl.species]
     return config_nd(dims=wl.dims, n=wl.n, length=wl.length, dt=wl.dt, species=sp, magnetic_field=wl.B,
                      units=SI if wl.si else NORMALIZED, precision=precision, sort_interval=sort_interval)
+
+
+@dataclass
+class PlasmaPlan:
+    """A 2D3V / 3D3V periodic deck whose particles are generated on the device
+    (sizes too large to stage through host arrays)."""
+    name: str
+    dims: int
+    n: tuple
+    length: tuple
+    dt: float
+    B: tuple
+    perturb_axis: int
+    amplitude: float
+    species: list  # (charge, mass, weight, count, thermal speed, seed)
+
+    @property
+    def particles(self) -> int:
+        return sum(s[3] for s in self.species)
+
+    def config(self, precision=0, sort_interval=16, capacity_factor=1.0):
+        from . import SI, config_nd
+        sp = [(q, m, w, int(n * capacity_factor) + 1) for (q, m, w, n, vt, seed) in self.species]
+        return config_nd(dims=self.dims, n=self.n, length=self.length, dt=self.dt, species=sp,
+                         magnetic_field=self.B, units=SI, precision=precision, sort_interval=sort_interval)
+
+    def load(self, sim):
+        for k, (q, m, w, n, vt, seed) in enumerate(self.species):
+            amp = self.amplitude if k == 0 else 0.0
+            sim.load_maxwellian(k, n, seed, vt, 0.0, self.perturb_axis, amp)
+
+
+def plasma_plan(dims, cells=None, ppc=None, seed=11):
+    """The 512^2 x 64 ppc 2D3V deck (Bz = 0.01 T, Te 2 eV, Ti 0.03 eV,
+    perturbation on the lowest kx and ky modes) or the 256^3 x 8 ppc 3D3V deck
+    (Bx = 0.005 T, Te 1 eV, Ti 0.025 eV, mode (1,0,0)); m_i/m_e = 1836,
+    cell = lambda_D at n0 = 1e16 m^-3, dt = 0.1 / omega_pe, electrons
+    perturbed by 1e-3."""
+    if dims == 2:
+        cells = tuple(cells or (512, 512))
+        ppc = ppc or 64
+        te, ti, B, axis, name = 2.0, 0.03, (0.0, 0.0, 0.01), -1, "plasma_2d3v_bz"
+    else:
+        cells = tuple(cells or (256, 256, 256))
+        ppc = ppc or 8
+        te, ti, B, axis, name = 1.0, 0.025, (0.005, 0.0, 0.0), 0, "plasma_3d3v_bx"
+    n0 = 1e16
+    lam = math.sqrt(EPS0 * te * E_CHARGE / (n0 * E_CHARGE ** 2))
+    wpe = math.sqrt(n0 * E_CHARGE ** 2 / (EPS0 * M_E))
+    L = tuple(c * lam for c in cells)
+    npart = ppc * int(np.prod(cells))
+    w = n0 * float(np.prod(L)) / npart
+    mi = M_E * 1836.0
+    species = [(-E_CHARGE, M_E, w, npart, math.sqrt(te * E_CHARGE / M_E), seed),
+               (E_CHARGE, mi, w, npart, math.sqrt(ti * E_CHARGE / mi), seed + 1)]
+    return PlasmaPlan(name, dims, cells, L, 0.1 / wpe, B, axis, 1e-3, species)
+
+
+# ---------------------------------------------------------------------------
+# Homogeneous electron swarms (run_swarm_benchmark)
+
+TOWNSEND = 1.0e-21
+
+
+def bethe(E, threshold, sigma0):
+    """sigma0 ln(u) / u, u = E / threshold (zero below threshold, peak sigma0 / e at u = e)."""
+    u = np.maximum(E / threshold, 1.0)
+    return sigma0 * np.log(u) / u
+
+
+@dataclass
+class SwarmSpec:
+    """One run_swarm_benchmark deck: a gas, the run controls and the reduced
+    fields (each field f runs with seed + f, like the reference)."""
+    name: str
+    channels: list          # ChannelSpec, projectile-frame energies in J
+    neutral_mass: float
+    neutral_density: float
+    neutral_temperature: float
+    max_frequency: float
+    timestep: float
+    steps: int
+    burn_in_steps: int
+    particles: int
+    fields_td: list
+    branching: bool = False
+    population_limit: int = 0
+    uncertainty_blocks: int = 10
+    initial_mean_energy_ev: float = 1.0
+    max_energy_ev: float = 1000.0
+    seed: int = 12345
+    max_candidates: int = 64
+
+
+def swarm_gas_4process(table_rows=2048, e_max_ev=2000.0):
+    """Synthetic 4-process electron gas: elastic momentum transfer
+    1e-20 (1.5 + 10 x^1.2 / (1 + x^2)) m^2 with x = E / 10 eV; excitations
+    at 11.5 eV and 13.0 eV and ionization at 15.8 eV with Bethe-like shapes
+    sigma0 ln(u)/u peaking at 3e-21, 5e-21 and 3e-20 m^2.  Argon-like
+    neutral mass (39.948 amu)."""
+    E = np.concatenate([[0.0], np.logspace(-3, math.log10(e_max_ev), table_rows - 1)])
+    x = E / 10.0
+    el = 1e-20 * (1.5 + 10.0 * x ** 1.2 / (1.0 + x ** 2))
+    ch = [
+        ChannelSpec(ELASTIC, E * E_CHARGE, el),
+        ChannelSpec(EXCITATION, E * E_CHARGE, bethe(E, 11.5, 3e-21 * math.e), 11.5 * E_CHARGE),
+        ChannelSpec(EXCITATION, E * E_CHARGE, bethe(E, 13.0, 5e-21 * math.e), 13.0 * E_CHARGE),
+        ChannelSpec(IONIZATION, E * E_CHARGE, bethe(E, 15.8, 3e-20 * math.e), 15.8 * E_CHARGE, 0, 1),
+    ]
+    return ch, 39.948 * AMU
+
+
+def swarm_gas_anisotropic(table_rows=512, e_max_ev=200.0, attachment=False):
+    """A small synthetic gas that exercises Henyey-Greenstein elastic
+    scattering (mean cosine rising from 0 to 0.6 over 0-100 eV), one
+    excitation at 4 eV, ionization at 9 eV and optionally a dissociative
+    attachment band near 2 eV."""
+    E = np.concatenate([[0.0], np.logspace(-3, math.log10(e_max_ev), table_rows - 1)])
+    mu_e = np.array([0.0, 1.0, 10.0, 100.0, E[-1]])
+    mu = np.array([0.0, 0.05, 0.3, 0.6, 0.6])
+    ch = [
+        ChannelSpec(ELASTIC, E * E_CHARGE, 8e-20 / np.sqrt(1.0 + E / 5.0), angular=2, mu_energy=mu_e * E_CHARGE, mu=mu),
+        ChannelSpec(EXCITATION, E * E_CHARGE, bethe(E, 4.0, 4e-21 * math.e), 4.0 * E_CHARGE),
+        ChannelSpec(IONIZATION, E * E_CHARGE, bethe(E, 9.0, 2e-20 * math.e), 9.0 * E_CHARGE, 0, 1),
+    ]
+    if attachment:
+        ch.append(ChannelSpec(ATTACHMENT, E * E_CHARGE, 6e-21 * np.exp(-((E - 2.0) / 0.8) ** 2)))
+    return ch, 28.0 * AMU
+
+
+def swarm_max_frequency(channels, neutral_density, neutral_mass, temperature, e_max_ev, margin=1.05):
+    """A max_frequency that bounds the total rate of every electron up to
+    e_max_ev (thermal neutrals add 8 sigma of relative speed)."""
+    return margin * _rate_bound(M_E, channels, e_max_ev, neutral_density, neutral_mass, temperature)
+
+
+def swarm_c5(fields_td=(10.0, 100.0, 1000.0), particles=100_000, steps=2000, burn_in_steps=1000, seed=12345,
+             max_energy_ev=1000.0, branching=False) -> SwarmSpec:
+    """The batched-serving swarm deck: the 4-process gas at 2.45e25 m^-3 and
+    300 K, dt = 0.1 / max_frequency (the reference's bound,
+    src/Swarm.cpp:300-303, at equality)."""
+    ch, mn = swarm_gas_4process(e_max_ev=2.0 * max_energy_ev)
+    ng, T = 2.45e25, 300.0
+    nu = swarm_max_frequency(ch, ng, mn, T, max_energy_ev)
+    return SwarmSpec("swarm_4process", ch, mn, ng, T, nu, 0.1 / nu, steps, burn_in_steps, particles,
+                     list(fields_td), branching=branching, initial_mean_energy_ev=1.0,
+                     max_energy_ev=max_energy_ev, seed=seed)

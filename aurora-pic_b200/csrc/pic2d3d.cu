@@ -649,7 +649,7 @@ __global__ void k_load_maxwellian(SpeciesND S, int buf, int dims, unsigned n, ui
     const double u[3] = {u53(r[0], r[1]), u53(r[2], r[3]), u53(r2[0], r2[1])};
     for (int a = 0; a < dims; ++a) {
         double x = u[a] * L[a];
-        if (amp != 0.0 && a == mode_axis) {
+        if (amp != 0.0 && (mode_axis < 0 || a == mode_axis)) {
             const double k = 2.0 * 3.141592653589793 / L[a];
             x = x + amp / k * sin(k * x);
             x = fmod(fmod(x, L[a]) + L[a], L[a]);
@@ -1186,6 +1186,7 @@ struct SimND {
     double time = 0.0;
     uint64_t step_count = 0;
     size_t sort_interval = 16;
+    uint64_t launches = 0;  // kernels launched by step()
     size_t steps_since_sort = 0;
     unsigned* cell_count = nullptr;
     unsigned* cell_offset = nullptr;
@@ -1462,11 +1463,13 @@ struct SimND {
             if (sort_now) {
                 for (int s = 0; s < cfg.nspecies; ++s) sort_species(s);
                 steps_since_sort = 0;
+                launches += 5 * (uint64_t)cfg.nspecies;  // histogram, three scan passes, scatter
             }
             if (timing) APIC_CUDA(cudaEventRecord(ev.b, stream));
             for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
             if (timing) APIC_CUDA(cudaEventRecord(ev.c, stream));
             solver.solve();
+            launches += (uint64_t)cfg.nspecies + (cfg.dims == 2 ? 3 : 5);  // pushes, FFT passes
             if (timing) {
                 APIC_CUDA(cudaEventRecord(ev.d, stream));
                 ev.sorted = sort_now;
@@ -1705,6 +1708,11 @@ int apic_simnd_kernel_times(apic_sim_nd* sim, double* push_ms, double* solve_ms,
         if (sort_ms) *sort_ms = sim->impl.sort_ms;
         if (steps) *steps = sim->impl.timed_steps;
     });
+}
+
+int apic_simnd_launch_count(apic_sim_nd* sim, uint64_t* launches) {
+    if (!sim || !launches) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { *launches = sim->impl.launches; });
 }
 
 int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,

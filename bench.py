@@ -1,13 +1,17 @@
 #!/usr/bin/env python
-"""Benchmark of the B200 particle step on the 1D3V capacitive RF discharge
-with null-collision MCC (512 cells, 512 electrons + 512 He+ per cell).
+"""Benchmark of the B200 particle step.
 
-One JSON line on rank 0.  A step is one PIC step of that discharge: push
-(gather, kick, drift, walls), CIC deposit, Poisson solve and MCC.
+Default workload: the 1D3V capacitive RF discharge with null-collision MCC
+(512 cells, 512 electrons + 512 He+ per cell).  `--workload plasma2d` /
+`plasma3d` run the 512^2 x 64 ppc 2D3V and 256^3 x 8 ppc 3D3V periodic decks
+(FP32 particles by default, `--precision fp64` for the plain form).
 
-  value  device-resident throughput (particle-steps/s), L2 flushed between
-         timed steps, max over ranks, summed over ranks (weak scaling: each
-         rank runs its own discharge, no collective on the data path)
+One JSON line on rank 0.  A step is one PIC step: push (gather, kick, drift,
+walls or wrap), CIC deposit, Poisson solve, and for the discharge MCC.
+
+  value  device-resident throughput (particle-steps/s), max over ranks for
+         time, summed over ranks for work (weak scaling: each rank runs its own
+         deck, no collective on the data path)
   e2e    the same metric through the C ABI with host buffers: every step loads
          the particles from pinned host memory, resumes, steps and reads the
          particles back
@@ -21,7 +25,6 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -34,22 +37,42 @@ sys.path.insert(0, os.path.join(ROOT, "aurora-pic_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "particle-steps/s (push+deposit+MCC)"
-WORKLOAD = "ccp_helium_1d3v: Dirichlet 0.067 m, 512 cells, 450 V 13.56 MHz, dt=1/(400 f), " \
-           "2x262144 particles (e-, He+ 4 amu), He 9.64e20 m^-3 300 K, 5-channel MCC"
+WORKLOAD_CCP = "ccp_helium_1d3v: Dirichlet 0.067 m, 512 cells, 450 V 13.56 MHz, dt=1/(400 f), " \
+               "2x262144 particles (e-, He+ 4 amu), He 9.64e20 m^-3 300 K, 5-channel MCC"
+WORKLOAD_2D = "plasma_2d3v_bz: periodic 512x512 cells (cell = lambda_D at 1e16 m^-3, 2 eV), 64 ppc e- + 64 ppc " \
+              "ions (33,554,432 particles), Bz 0.01 T, Te 2 eV, Ti 0.03 eV, m_i/m_e 1836, dt 0.1/omega_pe"
+WORKLOAD_3D = "plasma_3d3v_bx: periodic 256^3 cells, 8 ppc e- + 8 ppc ions (268,435,456 particles), " \
+              "Bx 0.005 T, Te 1 eV, Ti 0.025 eV, m_i/m_e 1836, dt 0.1/omega_pe"
+# algorithmic bytes per particle-step: read + write of the persistent state once
+BYTES_PER_PSTEP = {("plasma2d", "fp64"): 80, ("plasma3d", "fp64"): 96,
+                   ("plasma2d", "fp32"): 48, ("plasma3d", "fp32"): 56}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ppc", type=int, default=512)
-    ap.add_argument("--cells", type=int, default=512)
-    ap.add_argument("--e2e-steps", type=int, default=30)
+    ap.add_argument("--workload", default="ccp1d", choices=["ccp1d", "plasma2d", "plasma3d"])
+    ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
+    ap.add_argument("--ppc", type=int, default=None)
+    ap.add_argument("--cells", type=int, default=None, help="cells per axis")
+    ap.add_argument("--sort-interval", type=int, default=16)
+    ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    a = ap.parse_args()
+    big = a.workload != "ccp1d"
+    if a.steps is None:
+        a.steps = {"ccp1d": 200, "plasma2d": 100, "plasma3d": 20}[a.workload]
+    if a.warmup is None:
+        a.warmup = 5 if big else 20
+    if a.e2e_steps is None:
+        a.e2e_steps = 2 if big else 30
+    if a.precision is None:
+        a.precision = "fp32" if big else "fp64"
+    return a
 
 
 def peaks():
@@ -112,25 +135,61 @@ class Clocks:
                 "samples": len(rows)}
 
 
-def cpu_reference_sample(wl, seconds, threads):
-    """The reference's own Simulation::step on this host (oracle/_ref), or the C
-    restatement when the reference library is absent: a bounded sample."""
+# ---------------------------------------------------------------- CPU side
+
+def _ccp_cpu_sim(wl, threads):
+    """The reference's Simulation (oracle/_ref) on this host, or the C
+    restatement when the reference library is absent."""
     import pyoracle as po
     tabs = po.TableSet()
     work = tempfile.mkdtemp(prefix="apic_ref_")
-    n_per = len(wl.species[0].x)
     if po.reference_available():
         cfg = po.config_from_workload(wl, tabs, seed=12345, threads=threads, own_loading=True)
         sim = po.Ref1D(cfg, work)
         sim.initialize()
-        kind, cores = "reference", threads
+        return sim, "reference", threads, tabs
+    cfg = po.config_from_workload(wl, tabs, seed=12345)
+    sim = po.Sim1D(cfg, 0)
+    for i, s in enumerate(wl.species):
+        sim.load(i, s.x, s.v, s.v, s.vy, s.vz)
+    sim.initialize()
+    return sim, "port", 1, tabs
+
+
+def _plasma_cpu_sim(plan, threads):
+    """The reference's Simulation2D / Simulation3D on a scaled mesh with the
+    same particles per cell (the full decks take minutes per CPU step)."""
+    import pyoracle as po
+    from apic import workloads as W
+    cells = (128, 128) if plan.dims == 2 else (64, 64, 64)
+    small = W.plasma_plan(plan.dims, cells=cells, ppc=plan.species[0][3] // int(_prod(plan.n)))
+    sp = [(q, m, w, n, 0.0, vt) for (q, m, w, n, vt, seed) in small.species]
+    if po.reference_available():
+        sim = po.RefND(small.dims, small.n, small.length, small.dt, True, small.B, sp, seed=12345, threads=threads)
+        kind = "reference"
     else:
-        cfg = po.config_from_workload(wl, tabs, seed=12345)
-        sim = po.Sim1D(cfg, 0)
-        for i, s in enumerate(wl.species):
-            sim.load(i, s.x, s.v, s.v, s.vy, s.vz)
-        sim.initialize()
-        kind, cores = "port", 1
+        raise RuntimeError("the reference library was not built on this host")
+    sim.initialize()
+    return sim, kind, threads, small
+
+
+def _prod(t):
+    r = 1
+    for x in t:
+        r *= x
+    return r
+
+
+def cpu_reference_sample(args, wl, seconds, threads):
+    """A bounded sample of the reference's CPU step on this host's cores."""
+    if args.workload == "ccp1d":
+        sim, kind, cores, _ = _ccp_cpu_sim(wl, threads)
+        n = sum(len(s.x) for s in wl.species)
+        what = f"full steps of the same discharge ({n} particles)"
+    else:
+        sim, kind, cores, small = _plasma_cpu_sim(wl, threads)
+        n = small.particles
+        what = f"steps of the same deck on a {'x'.join(map(str, small.n))} mesh ({n} particles, same ppc)"
     sim.step(1)  # warm
     steps = 0
     t0 = time.perf_counter()
@@ -138,78 +197,78 @@ def cpu_reference_sample(wl, seconds, threads):
         sim.step(1)
         steps += 1
     dt = time.perf_counter() - t0
-    psteps = steps * n_per * len(wl.species)
-    return {"value": psteps / dt, "unit": "particle-steps/s", "cores": cores, "kind": kind,
-            "sample": f"{steps} full steps of the same discharge ({n_per * len(wl.species)} particles) "
-                      f"in {dt:.1f} s"}
+    return {"value": steps * n / dt, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{steps} {what} in {dt:.1f} s"}
 
 
 def run_reference(args):
-    from apic import workloads as W
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    wl = W.ccp_helium(particles_per_cell=args.ppc, cells=args.cells, seed=7)
+    from apic import workloads as W
     threads = os.cpu_count() or 1
-    import pyoracle as po
-    tabs = po.TableSet()
-    work = tempfile.mkdtemp(prefix="apic_ref_")
-    n = sum(len(s.x) for s in wl.species)
-    if po.reference_available():
-        cfg = po.config_from_workload(wl, tabs, seed=12345, threads=threads, own_loading=True)
-        sim = po.Ref1D(cfg, work)
-        sim.initialize()
-        kind = "reference"
+    if args.workload == "ccp1d":
+        wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7)
+        sim, kind, threads, _ = _ccp_cpu_sim(wl, threads)
+        n = sum(len(s.x) for s in wl.species)
+        workload, sample = WORKLOAD_CCP, "full discharge"
+        # the reference's thermal-neutral frequency bound scans every table row
+        # per candidate (src/Collision.cpp:627-685): 2-3 s per step here, so
+        # one CPU step per bench step and at most 10 of them
+        kmax = 10
     else:
-        cfg = po.config_from_workload(wl, tabs, seed=12345)
-        sim = po.Sim1D(cfg, 0)
-        for i, s in enumerate(wl.species):
-            sim.load(i, s.x, s.v, s.v, s.vy, s.vz)
-        sim.initialize()
-        kind, threads = "port", 1
-    # each bench step is a bounded sample of CPU steps so the run ends in minutes
-    # the reference's thermal-neutral frequency bound scans every table row per
-    # candidate (src/Collision.cpp:627-685): about 2-3 s per step here, so one
-    # CPU step per bench step and at most 10 of them
-    per_step = 1
-    sim.step(per_step * max(1, min(args.warmup, 2)))
+        plan = W.plasma_plan(2 if args.workload == "plasma2d" else 3)
+        sim, kind, threads, small = _plasma_cpu_sim(plan, threads)
+        n = small.particles
+        workload = WORKLOAD_2D if plan.dims == 2 else WORKLOAD_3D
+        sample = f"{'x'.join(map(str, small.n))} mesh, same ppc ({n} particles)"
+        kmax = 10
+    sim.step(max(1, min(args.warmup, 2)))
+    k = max(1, min(args.steps, kmax))
     t0 = time.perf_counter()
-    k = max(1, min(args.steps, 10))
-    sim.step(per_step * k)
+    sim.step(k)
     dt = time.perf_counter() - t0
-    value = n * per_step * k / dt
+    value = n * k / dt
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": k,
-            "warmup": args.warmup, "ms_per_step": 1e3 * dt / (per_step * k), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": WORKLOAD, "particles": n, "parallelism": "cpu threads"},
+            "config": {"workload": workload, "particles": n, "parallelism": "cpu threads"},
             "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": kind,
-                             "sample": f"{per_step * k} steps of the full discharge"},
+                             "sample": f"{k} steps of the {sample}"},
             "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def main():
-    args = parse()
-    if args.impl == "reference":
-        run_reference(args)
-        return
-    import numpy as np
+# ---------------------------------------------------------------- GPU side
+
+def _profiled_traffic(name):
+    """DRAM bytes (read + write) per launch of the dominant kernel, from the
+    committed ncu summary of the same workload (None when absent)."""
+    import re
+    try:
+        m = re.search(r"traffic_bytes_per_launch: (\d+)", open(os.path.join(ROOT, "profiles", name)).read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def _reduce(dist, t_ms, work):
+    import torch
+    t = torch.tensor([t_ms, work], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1])
+
+
+def bench_ccp1d(args, rank, dist):
+    """Returns the workload-specific part of the JSON line."""
     import torch
     import apic
     from apic import workloads as W
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    wl = W.ccp_helium(particles_per_cell=args.ppc, cells=args.cells, seed=7 + rank)
+    wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7 + rank)
     cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=1000 + rank)
     sim = apic.Simulation1D(cfg, tabs)
     for i, s in enumerate(wl.species):
@@ -228,7 +287,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    with Clocks(local) as clk:
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         with torch.cuda.stream(ext):
             for i in range(args.steps):
                 # write a buffer larger than L2, then read it back so the dirty
@@ -246,16 +305,9 @@ def main():
     pass_ms, post_ms, passes = sim.kernel_times()
     sim.set_kernel_timing(False)
     n_after = sum(sim.count(s) for s in range(len(wl.species)))
-    psteps = args.steps * 0.5 * (n_before + n_after)
-    t = torch.tensor([ms, psteps], dtype=torch.float64, device="cuda")
-    if dist:
-        mx = t.clone()
-        dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(mx[1:2], op=dist.ReduceOp.SUM)
-        ms_max, total_psteps = float(mx[0]), float(mx[1])
-    else:
-        ms_max, total_psteps = ms, psteps
-    value = total_psteps / (ms_max * 1e-3)
+    mean_n = 0.5 * (n_before + n_after)
+    ms_max, total = _reduce(dist, ms, args.steps * mean_n)
+    value = total / (ms_max * 1e-3)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     ns = len(wl.species)
@@ -298,52 +350,172 @@ def main():
         e_end.synchronize()
         e2e_ms += e_start.elapsed_time(e_end)
         t_sim, k_sim = sim.time, sim.step_count
-    e2e_psteps = args.e2e_steps * 0.5 * (n_before + n_after)
-    te = torch.tensor([e2e_ms, e2e_psteps], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(te[1:2], op=dist.ReduceOp.SUM)
-    e2e_value = float(te[1]) / (float(te[0]) * 1e-3)
+    e_ms, e_total = _reduce(dist, e2e_ms, args.e2e_steps * mean_n)
 
-    # ---- roofline of the fused particle pass ----
     hbm, peak_kind = peaks()
     bytes_per_pstep = 64  # FP64 1D3V: read + write x, v_half, v_y, v_z
     per_pass_ms = pass_ms / max(passes, 1)
-    achieved = bytes_per_pstep * 0.5 * (n_before + n_after) / (per_pass_ms * 1e-3) / 1e9
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pass1d_fp64_ccp_traffic.json")
-    if os.path.exists(prof):
-        try:
-            traffic = json.load(open(prof)).get("bytes_per_launch_full_size")
-        except Exception:
-            traffic = None
+    achieved = bytes_per_pstep * mean_n / (per_pass_ms * 1e-3) / 1e9
+    traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md")
+    sim.close()
+    return {
+        "value": value, "ms_per_step": ms_max / args.steps, "dtype": "f64",
+        "config": {"workload": WORKLOAD_CCP, "particles": int(mean_n),
+                   "form": "FP64 particles (bit-faithful arithmetic)", "l2": "flushed between timed steps"},
+        "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_pass1d<3,true>", "bytes_per_particle_step": bytes_per_pstep,
+                     "pass_ms": per_pass_ms, "post_ms": post_ms / max(passes, 1)},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+    }
+
+
+def bench_plasma(args, rank, dist):
+    """The 2D3V / 3D3V periodic decks, particles generated on the device."""
+    import numpy as np
+    import torch
+    import apic
+    from apic import workloads as W
+
+    dims = 2 if args.workload == "plasma2d" else 3
+    cells = None if args.cells is None else (args.cells,) * dims
+    plan = W.plasma_plan(dims, cells=cells, ppc=args.ppc, seed=11 + 2 * rank)
+    prec = apic.FP32 if args.precision == "fp32" else apic.FP64
+    sim = apic.SimulationND(plan.config(precision=prec, sort_interval=args.sort_interval))
+    plan.load(sim)
+    sim.initialize()
+    sim.step(args.warmup)
+    sim.synchronize()
+    P = plan.particles
+    ext = torch.cuda.ExternalStream(sim.cuda_stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sim.set_kernel_timing(True)
+    launches0 = sim.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(ext)
+        sim.step(args.steps)
+        e1.record(ext)
+        sim.synchronize()
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = sim.launch_count() - launches0
+    push_ms, solve_ms, sort_ms, nsteps = sim.kernel_times()
+    sim.set_kernel_timing(False)
+    ms_max, total = _reduce(dist, ms, args.steps * P)
+    value = total / (ms_max * 1e-3)
+
+    # ---- end to end: pinned host state in, one step, state out ----
+    ns = len(plan.species)
+    host = []
+    for k in range(ns):
+        n = plan.species[k][3]
+        host.append([torch.empty((3, n), dtype=torch.float64, pin_memory=True).numpy() for _ in range(3)])
+    L = apic._bind_nd()
+    got = apic.C.c_size_t()
+    for k in range(ns):
+        pos, v, vh = host[k]
+        apic._check_nd(L.apic_simnd_read_particles(sim.h, k, pos.shape[1], apic.dptr(pos), apic.dptr(v),
+                                                   apic.dptr(vh), apic.C.byref(got)), sim.h)
+    s0 = sim.sample()
+    t_sim, k_sim = s0.time, s0.step
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e2e_ms, h2d, d2h = 0.0, 0, 0
+    for it in range(args.e2e_steps):
+        e_start.record(ext)
+        for k in range(ns):
+            pos, v, vh = host[k]  # rows 0..dims-1 of pos are the [dims][n] block load reads
+            n = pos.shape[1]
+            apic._check_nd(L.apic_simnd_load_particles(sim.h, k, n, apic.dptr(pos),
+                                                       apic.dptr(v), apic.dptr(vh)), sim.h)
+            if it == 0:
+                h2d += (dims + 6) * 8 * n
+        sim.resume(t_sim, k_sim)
+        sim.step(1)
+        for k in range(ns):
+            pos, v, vh = host[k]
+            apic._check_nd(L.apic_simnd_read_particles(sim.h, k, pos.shape[1], apic.dptr(pos), apic.dptr(v),
+                                                       apic.dptr(vh), apic.C.byref(got)), sim.h)
+            if it == 0:
+                d2h += (dims + 6) * 8 * got.value
+        e_end.record(ext)
+        e_end.synchronize()
+        e2e_ms += e_start.elapsed_time(e_end)
+        t_sim, k_sim = t_sim + plan.dt, k_sim + 1
+    e_ms, e_total = _reduce(dist, e2e_ms, args.e2e_steps * P)
+
+    hbm, peak_kind = peaks()
+    bpp = BYTES_PER_PSTEP[(args.workload, args.precision)]
+    per_step_push = push_ms / max(nsteps, 1)
+    achieved = bpp * P / (per_step_push * 1e-3) / 1e9
+    form = ("FP32 particles: packed int32 cell + FP32 offsets + FP32 velocities; FP64 fixed-point deposit, "
+            "FP64 spectral solve") if prec == apic.FP32 else "FP64 particles (bit-faithful arithmetic)"
+    sim.close()
+    return {
+        "value": value, "ms_per_step": ms_max / args.steps, "dtype": "f32" if prec == apic.FP32 else "f64",
+        "config": {"workload": WORKLOAD_2D if dims == 2 else WORKLOAD_3D, "particles": P, "form": form,
+                   "sort_interval": args.sort_interval,
+                   "l2": f"inputs larger than L2 ({bpp // 2 * P / 1e9:.1f} GB of particle state)"},
+        "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": ("k_push32" if prec == apic.FP32 else "k_push") + f"<{dims}, boris>",
+                     "bytes_per_particle_step": bpp, "push_ms": per_step_push,
+                     "solve_ms": solve_ms / max(nsteps, 1), "sort_ms_per_step": sort_ms / max(nsteps, 1)},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    part = bench_ccp1d(args, rank, dist) if args.workload == "ccp1d" else bench_plasma(args, rank, dist)
 
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                cpu = cpu_reference_sample(wl, args.cpu_seconds, os.cpu_count() or 1)
+                from apic import workloads as W
+                wl = (W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7)
+                      if args.workload == "ccp1d" else W.plasma_plan(2 if args.workload == "plasma2d" else 3))
+                cpu = cpu_reference_sample(args, wl, args.cpu_seconds, os.cpu_count() or 1)
             except Exception as e:  # reported, never fatal
                 cpu = {"value": None, "error": str(e)}
+        cfg = dict(part["config"])
+        cfg["parallelism"] = f"replicas x{world}"
         line = {
-            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": int(0.5 * (n_before + n_after)),
-                       "form": "FP64 particles (bit-faithful arithmetic)", "l2": "flushed between timed steps",
-                       "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_pass1d<3,true>", "bytes_per_particle_step": bytes_per_pstep,
-                         "pass_ms": per_pass_ms, "post_ms": post_ms / max(passes, 1)},
-            "gpu_launches": 2 * args.steps,
-            "clocks": clk.summary(),
-            "cpu_baseline": cpu,
+            "metric": METRIC, "value": part["value"], "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": part["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": part["dtype"],
+            "data": "synthetic", "config": cfg, "e2e": part["e2e"], "roofline": part["roofline"],
+            "gpu_launches": part["gpu_launches"], "clocks": part["clocks"], "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    sim.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

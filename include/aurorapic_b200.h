@@ -310,7 +310,8 @@ APIC_EXPORT int apic_simnd_load_particles(apic_sim_nd* sim, int species, size_t 
                                           const double* v, const double* v_half);
 /* Loads n particles generated on the device (for runs too large to stage on
  * the host): uniform positions displaced by amplitude/k sin(k x) along
- * perturb_axis (amplitude 0: none), Maxwellian velocities of the given thermal
+ * perturb_axis, or along every axis of the mesh when perturb_axis < 0
+ * (amplitude 0: none), Maxwellian velocities of the given thermal
  * speed plus an x drift, v_half = v.  Seeded Philox streams; no reference
  * counterpart (the reference's loaders, src/Species2D.cpp / Species3D.cpp, use
  * its shared engine). */
@@ -341,6 +342,9 @@ APIC_EXPORT int apic_simnd_set_kernel_timing(apic_sim_nd* sim, int enable);
  * and the number of steps timed. */
 APIC_EXPORT int apic_simnd_kernel_times(apic_sim_nd* sim, double* push_ms, double* solve_ms, double* sort_ms,
                                         uint64_t* steps);
+/* Number of kernels step() has launched on this handle (pushes, FFT passes,
+ * sort passes); no reference counterpart. */
+APIC_EXPORT int apic_simnd_launch_count(apic_sim_nd* sim, uint64_t* launches);
 
 /* FieldSolver::solve(Mesh2D&/Mesh3D&) for a fully periodic mesh
  * (src/FieldSolver.cpp:442-499, :659-731): rho (N values) -> phi (N) and

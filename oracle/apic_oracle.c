@@ -243,6 +243,50 @@ static void isotropic(double speed, ora_rng* r, double out[3]) {
 
 static double norm3(const double v[3]) { return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
 
+/* MeanCosineTable::evaluate, src/Collision.cpp:296-313 */
+static double mean_cosine_eval(const ora_channel* ch, double energy) {
+    const double* e = ch->mu_energy;
+    const size_t n = ch->mu_rows;
+    if (energy <= e[0]) return ch->mu[0];
+    if (energy >= e[n - 1]) return ch->mu[n - 1];
+    size_t lo = 0, hi = n; /* upper_bound */
+    while (lo < hi) {
+        const size_t mid = lo + (hi - lo) / 2;
+        if (energy < e[mid]) hi = mid; else lo = mid + 1;
+    }
+    const size_t high = lo, low = high - 1;
+    const double fraction = (energy - e[low]) / (e[high] - e[low]);
+    return ch->mu[low] + fraction * (ch->mu[high] - ch->mu[low]);
+}
+
+/* angular_velocity (Henyey-Greenstein about the incoming direction),
+ * src/Collision.cpp:66-129 */
+static void angular_velocity(const double in[3], double speed, double g, ora_rng* r, double out[3]) {
+    const double in_speed = norm3(in);
+    if (!(in_speed > 0.0)) { isotropic(speed, r, out); return; }
+    const double sample = ora_uniform01(r);
+    double cosine = 2.0 * sample - 1.0;
+    if (g != 0.0) {
+        const double numerator = 1.0 - g * g;
+        const double denominator = 1.0 - g + 2.0 * g * sample;
+        const double ratio = numerator / denominator;
+        cosine = (1.0 + g * g - ratio * ratio) / (2.0 * g);
+        cosine = cosine < -1.0 ? -1.0 : (cosine > 1.0 ? 1.0 : cosine);
+    }
+    const double t = 1.0 - cosine * cosine;
+    const double sine = sqrt(0.0 > t ? 0.0 : t);
+    const double azimuth = 2.0 * acos(-1.0) * ora_uniform01(r);
+    const double dir[3] = {in[0] / in_speed, in[1] / in_speed, in[2] / in_speed};
+    const double h[3] = {0.0, fabs(dir[2]) < 0.9 ? 0.0 : 1.0, fabs(dir[2]) < 0.9 ? 1.0 : 0.0};
+    double tg[3] = {h[1] * dir[2] - h[2] * dir[1], h[2] * dir[0] - h[0] * dir[2], h[0] * dir[1] - h[1] * dir[0]};
+    const double tn = norm3(tg);
+    tg[0] /= tn; tg[1] /= tn; tg[2] /= tn;
+    const double bt[3] = {dir[1] * tg[2] - dir[2] * tg[1], dir[2] * tg[0] - dir[0] * tg[2],
+                          dir[0] * tg[1] - dir[1] * tg[0]};
+    const double tf = sine * cos(azimuth), bf = sine * sin(azimuth);
+    for (int d = 0; d < 3; ++d) out[d] = speed * (cosine * dir[d] + tf * tg[d] + bf * bt[d]);
+}
+
 /* sample_neutral_velocity_3v, src/Collision.cpp:702-715 (a fresh normal
  * distribution object per call, bounded at 8 sigma) */
 static int neutral_3v(const ora_collider* c, ora_rng* r, double out[3]) {
@@ -259,8 +303,7 @@ static int neutral_3v(const ora_collider* c, ora_rng* r, double out[3]) {
     return seterr(6, "thermal-neutral 3V sampler exceeded its rejection limit");
 }
 
-/* apply_channel (3V), src/Collision.cpp:762-829; anisotropic tables are not
- * part of this restatement (isotropic and backward only). */
+/* apply_channel (3V), src/Collision.cpp:762-829 */
 static void apply_channel3(const ora_collider* c, int idx, double v[3], const double vn[3], ora_rng* r) {
     const ora_channel* ch = &c->m.ch[idx];
     if (ch->process == ORA_ATTACHMENT) { v[0] = v[1] = v[2] = 0.0; return; }
@@ -276,6 +319,8 @@ static void apply_channel3(const ora_collider* c, int idx, double v[3], const do
     const double speed = sqrt(2.0 * energy / c->particle_mass);
     double sc[3];
     if (ch->angular == ORA_BACKWARD) { sc[0] = -rel[0]; sc[1] = -rel[1]; sc[2] = -rel[2]; }
+    else if (ch->angular == ORA_HENYEY_GREENSTEIN && ch->mu_rows)
+        angular_velocity(rel, speed, mean_cosine_eval(ch, collision_energy(c, ch, initial_speed)), r, sc);
     else isotropic(speed, r, sc);
     if (ch->process == ORA_ELASTIC && c->m.neutral_mass > 0.0) {
         const double total = c->particle_mass + c->m.neutral_mass;
@@ -1150,4 +1195,409 @@ void ora_simnd_fields(const ora_simnd* s, double* rho, double* phi, double* E) {
     if (rho) memcpy(rho, s->rho, N * sizeof(double));
     if (phi) memcpy(phi, s->phi, N * sizeof(double));
     if (E) memcpy(E, s->E, 3 * N * sizeof(double));
+}
+
+/* ======================================================================== */
+/* Homogeneous electron swarm (src/Swarm.cpp)                               */
+/* ======================================================================== */
+
+static const double kSwarmElectronMass = 9.1093837139e-31; /* src/Swarm.cpp:23 */
+static const double kSwarmEvToJ = 1.602176634e-19;         /* src/Swarm.cpp:24-25 */
+static const double kSwarmTownsend = 1.0e-21;              /* src/Swarm.cpp:26 */
+static const size_t kSwarmAllocationLimit = 10000000;      /* src/Swarm.cpp:27 */
+
+/* kinetic_energy_ev, src/Swarm.cpp:95-101 */
+static double swarm_ke_ev(const double v[3]) {
+    const double s2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    return 0.5 * kSwarmElectronMass * s2 / kSwarmEvToJ;
+}
+
+int ora_block_mean_and_error(const double* x, size_t n, size_t blocks, double* mean, double* se) {
+    if (n == 0 || blocks == 0 || blocks > n)
+        return seterr(4, "swarm block statistics require at least one sample per block");
+    double* means = (double*)malloc(blocks * sizeof(double));
+    for (size_t b = 0; b < blocks; ++b) {
+        const size_t begin = b * n / blocks, end = (b + 1) * n / blocks;
+        double total = 0.0;
+        for (size_t i = begin; i < end; ++i) total += x[i];
+        means[b] = total / (double)(end - begin);
+    }
+    double m = 0.0;
+    for (size_t b = 0; b < blocks; ++b) m += means[b];
+    m /= (double)blocks;
+    double e = 0.0;
+    if (blocks > 1) {
+        double sq = 0.0;
+        for (size_t b = 0; b < blocks; ++b) {
+            const double d = means[b] - m;
+            sq += d * d;
+        }
+        e = sqrt(sq / ((double)blocks * (double)(blocks - 1)));
+    }
+    free(means);
+    *mean = m;
+    *se = e;
+    return 0;
+}
+
+/* linear_slope, src/Swarm.cpp:136-163 */
+static double swarm_linear_slope(const double* v, size_t begin, size_t end, double timestep) {
+    const size_t count = end - begin;
+    const double mean_index = 0.5 * (double)(count - 1);
+    double covariance = 0.0, index_variance = 0.0, mean_value = 0.0;
+    for (size_t i = begin; i < end; ++i) mean_value += v[i];
+    mean_value /= (double)count;
+    for (size_t l = 0; l < count; ++l) {
+        const double ci = (double)l - mean_index;
+        covariance += ci * (v[begin + l] - mean_value);
+        index_variance += ci * ci;
+    }
+    return covariance / (index_variance * timestep);
+}
+
+int ora_block_slope_and_error(const double* x, size_t n, double timestep, size_t blocks, double* slope,
+                              double* se) {
+    if (blocks == 0 || n % blocks != 0 || n / blocks < 2)
+        return seterr(4, "swarm growth statistics require at least two samples per equal block");
+    const size_t bs = n / blocks;
+    double* slopes = (double*)malloc(blocks * sizeof(double));
+    for (size_t b = 0; b < blocks; ++b) slopes[b] = swarm_linear_slope(x, b * bs, (b + 1) * bs, timestep);
+    double m = 0.0;
+    for (size_t b = 0; b < blocks; ++b) m += slopes[b];
+    m /= (double)blocks;
+    double e = 0.0;
+    if (blocks > 1) {
+        double sq = 0.0;
+        for (size_t b = 0; b < blocks; ++b) {
+            const double d = slopes[b] - m;
+            sq += d * d;
+        }
+        e = sqrt(sq / ((double)blocks * (double)(blocks - 1)));
+    }
+    free(slopes);
+    *slope = m;
+    *se = e;
+    return 0;
+}
+
+size_t ora_swarm_population_limit(const ora_swarm_config* cfg) {
+    if (cfg->population_limit != 0) return cfg->population_limit;
+    if (cfg->particles >= kSwarmAllocationLimit) return cfg->particles;
+    const size_t source = kSwarmAllocationLimit - cfg->particles;
+    const size_t doubled = cfg->particles > source / 2 ? source : 2 * cfg->particles;
+    const size_t buffer = source < 1024 ? source : 1024;
+    const size_t buffered = cfg->particles > source - buffer ? source : cfg->particles + 1024;
+    const size_t mx = doubled > buffered ? doubled : buffered;
+    return source < mx ? source : mx;
+}
+
+/* One electron of the ensemble.  Mode 0 keeps the reference's SwarmParticle
+ * (src/Swarm.cpp:559-565: absolute position and sampling start); modes 1-2
+ * keep the displacement since the sampling start in pos[] and no start. */
+typedef struct {
+    double v[3], pos[3], start[3], w;
+    int alive;
+} swarm_particle;
+
+static void swarm_round_float(swarm_particle* p) {
+    for (int d = 0; d < 3; ++d) {
+        p->v[d] = (double)(float)p->v[d];
+        p->pos[d] = (double)(float)p->pos[d];
+    }
+}
+
+static void swarm_philox(ora_rng* r, uint64_t seed, uint32_t slot, uint32_t step, uint32_t stream) {
+    memset(r, 0, sizeof *r);
+    r->kind = ORA_SRC_PHILOX;
+    r->key[0] = (uint32_t)seed;
+    r->key[1] = (uint32_t)(seed >> 32);
+    r->ctr[0] = slot;
+    r->ctr[1] = step;
+    r->ctr[2] = stream;
+}
+
+int ora_swarm_run_field(const ora_swarm_config* cfg, const ora_mcc_model* gas, double td, uint64_t seed, int mode,
+                        ora_swarm_result* out, double* samples) {
+    memset(out, 0, sizeof *out);
+    /* collision_config, src/Swarm.cpp:520-557 */
+    ora_mcc_model model = *gas;
+    model.neutral_density = cfg->neutral_density;
+    model.max_frequency = cfg->max_frequency;
+    model.neutral_temperature = cfg->neutral_temperature;
+    model.si = 1;
+    if (model.max_candidates == 0) model.max_candidates = 64;
+    ora_collider col;
+    if (ora_collider_init(&col, &model, kSwarmElectronMass)) return 4;
+    if (cfg->steps == 0 || cfg->burn_in_steps >= cfg->steps || cfg->particles == 0)
+        return seterr(4, "invalid swarm steps or particles");
+
+    const size_t N = cfg->particles;
+    const size_t limit = ora_swarm_population_limit(cfg);
+    const size_t cap = cfg->branching ? limit : N;
+    swarm_particle* P = (swarm_particle*)calloc(cap, sizeof *P);
+    swarm_particle* R = cfg->branching ? (swarm_particle*)calloc(N, sizeof *R) : NULL;
+    const size_t ns = cfg->steps - cfg->burn_in_steps;
+    double* vs = (double*)malloc(ns * sizeof(double));
+    double* es = (double*)malloc(ns * sizeof(double));
+    double* ls = (double*)malloc(ns * sizeof(double));
+    int rc = 0;
+
+    ora_mt64 mt;
+    ora_mt64_seed(&mt, seed);
+    ora_rng shared;
+    memset(&shared, 0, sizeof shared);
+    shared.kind = ORA_SRC_MT64;
+    shared.mt = &mt;
+
+    const double sd = sqrt(2.0 * cfg->initial_mean_energy_ev * kSwarmEvToJ / (3.0 * kSwarmElectronMass));
+    ora_normal nst = {0, 0.0};
+    for (size_t i = 0; i < N; ++i) {
+        P[i].w = 1.0;
+        P[i].alive = 1;
+        if (mode == 0) {
+            for (int d = 0; d < 3; ++d) P[i].v[d] = ora_normal_draw(&nst, &shared, 0.0, sd);
+        } else {
+            ora_rng r;
+            swarm_philox(&r, seed, (uint32_t)i, 0xFFFFFFFFu, 2u);
+            ora_normal pn = {0, 0.0};
+            for (int d = 0; d < 3; ++d) P[i].v[d] = ora_normal_draw(&pn, &r, 0.0, sd);
+            if (mode == 2) swarm_round_float(&P[i]);
+        }
+    }
+    size_t M = N;
+    double w = 1.0; /* modes 1-2: the one weight of every electron */
+
+    const double E = td * kSwarmTownsend * cfg->neutral_density;
+    const double acceleration = -kSwarmEvToJ * E / kSwarmElectronMass;
+    const double half_kick = 0.5 * acceleration * cfg->timestep;
+    out->reduced_field_td = td;
+    out->electric_field_v_m = E;
+    out->initial_weight = (double)N;
+    out->diffusion_available = !cfg->branching;
+    out->nch = model.nch;
+    double wcoll[ORA_MAX_CHANNELS] = {0}, wcoll2[ORA_MAX_CHANNELS] = {0};
+    double exposure = 0.0;
+    size_t si = 0;
+
+    for (size_t step = 0; step < cfg->steps && !rc; ++step) {
+        if (mode == 0 && step == cfg->burn_in_steps)
+            for (size_t i = 0; i < M; ++i) memcpy(P[i].start, P[i].pos, sizeof P[i].pos);
+        const size_t active = M;
+        double start_weight;
+        if (mode == 0) {
+            start_weight = 0.0;
+            for (size_t i = 0; i < M; ++i) if (P[i].alive) start_weight += P[i].w;
+        } else {
+            start_weight = (double)M * w;
+        }
+        if (step >= cfg->burn_in_steps) exposure += start_weight * cfg->timestep;
+        uint64_t step_counts[ORA_MAX_CHANNELS] = {0};
+        for (size_t i = 0; i < active && !rc; ++i) {
+            swarm_particle* p = &P[i];
+            p->v[0] += half_kick;
+            const double pre = swarm_ke_ev(p->v);
+            if (pre > out->max_observed_energy_ev) out->max_observed_energy_ev = pre;
+            if (pre > cfg->max_energy_ev) {
+                rc = seterr(7, "swarm particle energy exceeded max_energy_ev before collision lookup");
+                break;
+            }
+            if (mode == 0 || step >= cfg->burn_in_steps)
+                for (int d = 0; d < 3; ++d) p->pos[d] += p->v[d] * cfg->timestep;
+            ora_rng r;
+            if (mode == 0) r = shared;
+            else swarm_philox(&r, seed, (uint32_t)i, (uint32_t)step, 0u);
+            ora_collide_stats st;
+            const int crc = ora_collide3(&col, p->v, cfg->timestep, &r, &st);
+            if (mode == 0) shared.index = r.index;
+            if (crc) { rc = crc; break; }
+            p->v[0] += half_kick;
+            const double e = swarm_ke_ev(p->v);
+            if (e > out->max_observed_energy_ev) out->max_observed_energy_ev = e;
+            if (e > cfg->max_energy_ev) {
+                rc = seterr(7, "swarm particle energy exceeded max_energy_ev");
+                break;
+            }
+            if (step >= cfg->burn_in_steps) {
+                out->candidates += st.candidates;
+                out->null_collisions += st.null_collisions;
+                for (int c = 0; c < model.nch; ++c) {
+                    out->channel_collisions[c] += st.channel_collisions[c];
+                    if (mode == 0) {
+                        wcoll[c] += p->w * (double)st.channel_collisions[c];
+                        wcoll2[c] += p->w * p->w * (double)st.channel_collisions[c];
+                    } else {
+                        step_counts[c] += st.channel_collisions[c];
+                    }
+                }
+            }
+            if (mode == 2) swarm_round_float(p);
+            if (cfg->branching) {
+                if (st.nsecondaries > 16) { rc = seterr(8, "more than 16 secondaries in one step"); break; }
+                for (int k = 0; k < st.nsecondaries; ++k) {
+                    if (M >= limit) {
+                        rc = seterr(9, "branching swarm exceeded population_limit before resampling");
+                        break;
+                    }
+                    swarm_particle* q = &P[M++];
+                    *q = P[i];
+                    q->alive = 1;
+                    memcpy(q->v, st.secondary_velocity[k], sizeof q->v);
+                    if (mode == 2) swarm_round_float(q);
+                }
+                if (st.removed) P[i].alive = 0;
+            }
+        }
+        if (rc) break;
+        if (mode != 0 && step >= cfg->burn_in_steps)
+            for (int c = 0; c < model.nch; ++c) {
+                wcoll[c] += w * (double)step_counts[c];
+                wcoll2[c] += w * w * (double)step_counts[c];
+            }
+        if (cfg->branching) {
+            size_t k = 0; /* erase_if, stable */
+            for (size_t i = 0; i < M; ++i) if (P[i].alive) P[k++] = P[i];
+            M = k;
+            if (M == 0) { rc = seterr(10, "branching swarm electron ensemble became extinct"); break; }
+            if (M != N) {
+                /* systematic_resample, src/Swarm.cpp:616-643 */
+                if (mode == 0) {
+                    double ws = 0.0;
+                    for (size_t i = 0; i < M; ++i) ws += P[i].w;
+                    const double ow = ws / (double)N;
+                    const double offset = ora_uniform01(&shared) * ow;
+                    size_t src = 0;
+                    double cumulative = P[0].w;
+                    for (size_t s = 0; s < N; ++s) {
+                        const double threshold = offset + (double)s * ow;
+                        while (src + 1 < M && cumulative < threshold) {
+                            ++src;
+                            cumulative += P[src].w;
+                        }
+                        R[s] = P[src];
+                        R[s].w = ow;
+                    }
+                } else {
+                    /* every electron carries the weight w: the cumulative weight
+                     * of the first j+1 is (j+1) w, so sample s takes source
+                     * ceil((u + s) M / N) - 1 */
+                    ora_rng r;
+                    swarm_philox(&r, seed, 0xFFFFFFFFu, (uint32_t)step, 1u);
+                    const double u = ora_uniform01(&r);
+                    for (size_t s = 0; s < N; ++s) {
+                        const double t = (u + (double)s) * (double)M / (double)N;
+                        double c = ceil(t) - 1.0;
+                        size_t j = c < 0.0 ? 0 : (size_t)c;
+                        if (j > M - 1) j = M - 1;
+                        R[s] = P[j];
+                    }
+                    w = (double)M * w / (double)N;
+                }
+                memcpy(P, R, N * sizeof *P);
+                M = N;
+            }
+        }
+        if (step < cfg->burn_in_steps) continue;
+        double vsum = 0.0, esum = 0.0, wsum = 0.0;
+        if (mode == 0) {
+            for (size_t i = 0; i < M; ++i) wsum += P[i].w;
+            for (size_t i = 0; i < M; ++i) {
+                vsum += P[i].w * P[i].v[0];
+                esum += P[i].w * swarm_ke_ev(P[i].v);
+            }
+            vs[si] = vsum / wsum;
+            es[si] = esum / wsum;
+            ls[si] = log(wsum);
+        } else {
+            for (size_t i = 0; i < M; ++i) {
+                vsum += P[i].v[0];
+                esum += swarm_ke_ev(P[i].v);
+            }
+            vs[si] = vsum / (double)M;
+            es[si] = esum / (double)M;
+            ls[si] = log((double)M * w);
+        }
+        ++si;
+    }
+
+    if (!rc) {
+        double m, e;
+        rc = ora_block_mean_and_error(vs, ns, cfg->uncertainty_blocks, &m, &e);
+        out->mean_velocity_x = m;
+        out->mean_velocity_x_se = e;
+        out->drift_velocity = -m;
+        out->reduced_mobility = E == 0.0 ? 0.0 : out->drift_velocity * cfg->neutral_density / E;
+        if (!rc) rc = ora_block_mean_and_error(es, ns, cfg->uncertainty_blocks, &m, &e);
+        out->mean_energy_ev = m;
+        out->mean_energy_se_ev = e;
+    }
+    if (!rc) {
+        const double sampling_time = (double)ns * cfg->timestep;
+        if (out->diffusion_available) {
+            double mx = 0.0, my = 0.0, mz = 0.0;
+            const double count = (double)M;
+            for (size_t i = 0; i < M; ++i) {
+                const double* a = P[i].pos;
+                const double* b = P[i].start; /* zero in modes 1-2 */
+                mx += a[0] - b[0];
+                my += a[1] - b[1];
+                mz += a[2] - b[2];
+            }
+            mx /= count; my /= count; mz /= count;
+            double vx = 0.0, vyz = 0.0;
+            for (size_t i = 0; i < M; ++i) {
+                const double* a = P[i].pos;
+                const double* b = P[i].start;
+                const double dx = a[0] - b[0] - mx, dy = a[1] - b[1] - my, dz = a[2] - b[2] - mz;
+                vx += dx * dx;
+                vyz += dy * dy + dz * dz;
+            }
+            vx /= count;
+            vyz /= count;
+            out->diffusion_longitudinal = vx / (2.0 * sampling_time);
+            out->diffusion_transverse = vyz / (4.0 * sampling_time);
+        }
+        for (int c = 0; c < model.nch; ++c) {
+            out->channel_rate[c] = wcoll[c] / exposure;
+            out->channel_rate_se[c] = sqrt(wcoll2[c]) / exposure;
+            if (model.ch[c].process == ORA_IONIZATION) {
+                out->ionization_rate += out->channel_rate[c];
+                out->ionization_rate_se = hypot(out->ionization_rate_se, out->channel_rate_se[c]);
+            } else if (model.ch[c].process == ORA_ATTACHMENT) {
+                out->attachment_rate += out->channel_rate[c];
+                out->attachment_rate_se = hypot(out->attachment_rate_se, out->channel_rate_se[c]);
+            }
+        }
+        out->net_rate = out->ionization_rate - out->attachment_rate;
+        out->net_rate_se = hypot(out->ionization_rate_se, out->attachment_rate_se);
+        if (mode == 0) {
+            double ws = 0.0;
+            for (size_t i = 0; i < M; ++i) ws += P[i].w;
+            out->final_weight = ws;
+        } else {
+            out->final_weight = (double)M * w;
+        }
+        out->final_particles = M;
+        if (cfg->branching) {
+            double g, ge;
+            rc = ora_block_slope_and_error(ls, ns, cfg->timestep, cfg->uncertainty_blocks, &g, &ge);
+            out->growth_rate = g;
+            out->growth_rate_se = ge;
+            if (!rc && out->drift_velocity > 0.0) {
+                const double drift = out->drift_velocity, de = out->mean_velocity_x_se;
+                out->townsend_available = 1;
+                out->townsend_growth = g / drift;
+                out->townsend_growth_se = hypot(ge / drift, g * de / (drift * drift));
+                out->townsend_rate = out->net_rate / drift;
+                out->townsend_rate_se = hypot(out->net_rate_se / drift, out->net_rate * de / (drift * drift));
+            }
+        }
+        if (samples)
+            for (size_t i = 0; i < ns; ++i) {
+                samples[i] = vs[i];
+                samples[ns + i] = es[i];
+                samples[2 * ns + i] = ls[i];
+            }
+    }
+    free(P); free(R); free(vs); free(es); free(ls);
+    return rc;
 }

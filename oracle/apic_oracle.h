@@ -106,6 +106,27 @@ void ora_simnd_step(ora_simnd* s, size_t steps);
 void ora_simnd_get(const ora_simnd* s, int k, double* pos, double* v, double* vh);
 void ora_simnd_fields(const ora_simnd* s, double* rho, double* phi, double* E);
 
+/* ---- homogeneous electron swarm (src/Swarm.cpp) ---------------------------- */
+/* block_mean_and_error, src/Swarm.cpp:103-134; returns 0 or 4 (invalid blocks) */
+int ora_block_mean_and_error(const double* x, size_t n, size_t blocks, double* mean, double* se);
+/* block_slope_and_error, src/Swarm.cpp:165-197 */
+int ora_block_slope_and_error(const double* x, size_t n, double timestep, size_t blocks, double* slope,
+                              double* se);
+/* effective_population_limit, src/Swarm.cpp:237-260 */
+size_t ora_swarm_population_limit(const ora_swarm_config* cfg);
+/* run_field, src/Swarm.cpp:940-1250, for one reduced field (Td) on the gas
+ * `gas` (channels and neutral_mass; density, temperature and max_frequency come
+ * from cfg).
+ * mode 0: the reference's particle layout and one shared mt19937_64 stream
+ *         seeded with `seed` (bit-exact with run_swarm_benchmark);
+ * mode 1: the device form in FP64: per-particle Philox streams keyed on
+ *         (seed, slot, step), displacements accumulated from the sampling
+ *         start, one weight per run, systematic resampling by index;
+ * mode 2: mode 1 with velocities and displacements stored in FP32 between steps.
+ * samples (optional): 3 x (steps - burn_in) doubles: velocity, energy, log weight. */
+int ora_swarm_run_field(const ora_swarm_config* cfg, const ora_mcc_model* gas, double td, uint64_t seed, int mode,
+                        ora_swarm_result* out, double* samples);
+
 #ifdef __cplusplus
 }
 #endif

@@ -11,7 +11,7 @@ extern "C" {
 #endif
 
 enum { ORA_ELASTIC = 0, ORA_EXCITATION = 1, ORA_IONIZATION = 2, ORA_ATTACHMENT = 3, ORA_CHARGE_EXCHANGE = 4 };
-enum { ORA_ISOTROPIC = 0, ORA_BACKWARD = 1 };
+enum { ORA_ISOTROPIC = 0, ORA_BACKWARD = 1, ORA_HENYEY_GREENSTEIN = 2 };
 enum { ORA_FRAME_PROJECTILE = 0, ORA_FRAME_CENTER_OF_MASS = 1 };
 
 #define ORA_MAX_CHANNELS 8
@@ -28,6 +28,9 @@ typedef struct {
     size_t rows;
     const double* energy;  /* strictly increasing */
     const double* sigma;
+    size_t mu_rows;        /* Henyey-Greenstein only: MeanCosineTable rows */
+    const double* mu_energy;
+    const double* mu;
 } ora_channel;
 
 typedef struct {
@@ -79,6 +82,38 @@ typedef struct {
     int removed;                 /* attachment removed the projectile */
     uint64_t draws;              /* raw 64-bit draws consumed */
 } ora_collide_stats;
+
+/* SwarmBenchmarkConfig subset of one run_field call, include/pic/Swarm.hpp:29-59 */
+typedef struct {
+    double neutral_density, neutral_temperature, max_frequency, timestep;
+    size_t steps, burn_in_steps, particles;
+    int branching;               /* 0 fixed_population_no_avalanche, 1 branching_resampled */
+    size_t population_limit;     /* 0: the reference's default */
+    size_t uncertainty_blocks;
+    double initial_mean_energy_ev, max_energy_ev;
+    uint64_t seed;
+} ora_swarm_config;
+
+/* SwarmBenchmarkResult subset, include/pic/Swarm.hpp:73-115 */
+typedef struct {
+    double reduced_field_td, electric_field_v_m;
+    double mean_velocity_x, mean_velocity_x_se, drift_velocity, reduced_mobility;
+    double mean_energy_ev, mean_energy_se_ev;
+    int diffusion_available;
+    double diffusion_longitudinal, diffusion_transverse;
+    double max_observed_energy_ev;
+    double initial_weight, final_weight;
+    uint64_t final_particles;
+    double growth_rate, growth_rate_se;
+    double ionization_rate, ionization_rate_se, attachment_rate, attachment_rate_se;
+    double net_rate, net_rate_se;
+    int townsend_available;
+    double townsend_growth, townsend_growth_se, townsend_rate, townsend_rate_se;
+    uint64_t candidates, null_collisions;
+    int nch;
+    uint64_t channel_collisions[ORA_MAX_CHANNELS];
+    double channel_rate[ORA_MAX_CHANNELS], channel_rate_se[ORA_MAX_CHANNELS];
+} ora_swarm_result;
 
 #ifdef __cplusplus
 }

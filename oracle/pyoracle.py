@@ -37,6 +37,8 @@ class Channel(C.Structure):
         ("secondary_species", C.c_int), ("ion_species", C.c_int),
         ("rows", C.c_size_t),
         ("energy", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)),
+        ("mu_rows", C.c_size_t),
+        ("mu_energy", C.POINTER(C.c_double)), ("mu", C.POINTER(C.c_double)),
     ]
 
 
@@ -214,11 +216,18 @@ class TableSet:
         self.keep = []
 
     def channel(self, process, energy, sigma, threshold=0.0, secondary=-1, ion=-1,
-                angular=0, frame=0) -> Channel:
+                angular=0, frame=0, mu_energy=None, mu=None) -> Channel:
+        """angular 2 (Henyey-Greenstein) takes a mean-cosine table mu(mu_energy)."""
         e = np.ascontiguousarray(energy, dtype=np.float64)
         s = np.ascontiguousarray(sigma, dtype=np.float64)
         self.keep += [e, s]
-        return Channel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+        ch = Channel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+        if mu is not None:
+            me = np.ascontiguousarray(mu_energy, dtype=np.float64)
+            mv = np.ascontiguousarray(mu, dtype=np.float64)
+            self.keep += [me, mv]
+            ch.mu_rows, ch.mu_energy, ch.mu = len(me), dptr(me), dptr(mv)
+        return ch
 
 
 def make_model(species, channels, neutral_density, max_frequency, neutral_mass=0.0,
@@ -577,3 +586,118 @@ class RefND:
 
     def time(self):
         return _refnd_bind().refnd_time(self.h)
+
+
+# ---------------------------------------------------------------------------
+# Homogeneous electron swarm (run_field / run_swarm_benchmark)
+
+class SwarmConfig(C.Structure):
+    _fields_ = [
+        ("neutral_density", C.c_double), ("neutral_temperature", C.c_double),
+        ("max_frequency", C.c_double), ("timestep", C.c_double),
+        ("steps", C.c_size_t), ("burn_in_steps", C.c_size_t), ("particles", C.c_size_t),
+        ("branching", C.c_int), ("population_limit", C.c_size_t), ("uncertainty_blocks", C.c_size_t),
+        ("initial_mean_energy_ev", C.c_double), ("max_energy_ev", C.c_double), ("seed", C.c_uint64),
+    ]
+
+
+class SwarmResult(C.Structure):
+    _fields_ = [
+        ("reduced_field_td", C.c_double), ("electric_field_v_m", C.c_double),
+        ("mean_velocity_x", C.c_double), ("mean_velocity_x_se", C.c_double),
+        ("drift_velocity", C.c_double), ("reduced_mobility", C.c_double),
+        ("mean_energy_ev", C.c_double), ("mean_energy_se_ev", C.c_double),
+        ("diffusion_available", C.c_int),
+        ("diffusion_longitudinal", C.c_double), ("diffusion_transverse", C.c_double),
+        ("max_observed_energy_ev", C.c_double),
+        ("initial_weight", C.c_double), ("final_weight", C.c_double),
+        ("final_particles", C.c_uint64),
+        ("growth_rate", C.c_double), ("growth_rate_se", C.c_double),
+        ("ionization_rate", C.c_double), ("ionization_rate_se", C.c_double),
+        ("attachment_rate", C.c_double), ("attachment_rate_se", C.c_double),
+        ("net_rate", C.c_double), ("net_rate_se", C.c_double),
+        ("townsend_available", C.c_int),
+        ("townsend_growth", C.c_double), ("townsend_growth_se", C.c_double),
+        ("townsend_rate", C.c_double), ("townsend_rate_se", C.c_double),
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64),
+        ("nch", C.c_int),
+        ("channel_collisions", C.c_uint64 * MAX_CHANNELS),
+        ("channel_rate", C.c_double * MAX_CHANNELS), ("channel_rate_se", C.c_double * MAX_CHANNELS),
+    ]
+
+    def as_dict(self):
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v)[: self.nch] if name.startswith("channel_") else v
+        return d
+
+
+def swarm_config(*, neutral_density, max_frequency, timestep, steps, burn_in_steps, particles,
+                 neutral_temperature=0.0, branching=False, population_limit=0, uncertainty_blocks=10,
+                 initial_mean_energy_ev=0.1, max_energy_ev=100.0, seed=12345) -> SwarmConfig:
+    return SwarmConfig(neutral_density, neutral_temperature, max_frequency, timestep, steps, burn_in_steps,
+                       particles, int(branching), population_limit, uncertainty_blocks, initial_mean_energy_ev,
+                       max_energy_ev, seed)
+
+
+def _swarm_bind(L):
+    L.ora_swarm_run_field.argtypes = [C.POINTER(SwarmConfig), C.POINTER(MccModel), C.c_double, C.c_uint64, C.c_int,
+                                      C.POINTER(SwarmResult), _DP]
+    L.ora_block_mean_and_error.argtypes = [_DP, C.c_size_t, C.c_size_t, _DP, _DP]
+    L.ora_block_slope_and_error.argtypes = [_DP, C.c_size_t, C.c_double, C.c_size_t, _DP, _DP]
+    L.ora_swarm_population_limit.restype = C.c_size_t
+    L.ora_swarm_population_limit.argtypes = [C.POINTER(SwarmConfig)]
+    return L
+
+
+def swarm_run_field(cfg: SwarmConfig, gas: MccModel, td: float, seed: int, mode: int, samples=False):
+    """run_field on the oracle; mode 0 reference form, 1 device FP64 form,
+    2 device FP32-storage form.  Returns (SwarmResult, samples or None)."""
+    L = _swarm_bind(oracle())
+    out = SwarmResult()
+    ns = cfg.steps - cfg.burn_in_steps
+    buf = np.zeros(3 * ns) if samples else None
+    rc = L.ora_swarm_run_field(C.byref(cfg), C.byref(gas), td, seed, mode, C.byref(out),
+                               dptr(buf) if samples else None)
+    if rc:
+        raise RuntimeError(L.ora_last_error().decode())
+    return out, (buf.reshape(3, ns) if samples else None)
+
+
+def block_mean_and_error(x, blocks):
+    L = _swarm_bind(oracle())
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    m, e = C.c_double(), C.c_double()
+    if L.ora_block_mean_and_error(dptr(x), len(x), blocks, C.byref(m), C.byref(e)):
+        raise ValueError(L.ora_last_error().decode())
+    return m.value, e.value
+
+
+def ref_swarm_run(cfg: SwarmConfig, gas: MccModel, fields, workdir):
+    """pic::run_swarm_benchmark through the harness: one SwarmResult per field
+    (field f runs with seed cfg.seed + f)."""
+    L = ref()
+    L.ref_swarm_run.argtypes = [C.POINTER(SwarmConfig), C.POINTER(MccModel), _DP, C.c_size_t, C.c_char_p,
+                                C.POINTER(SwarmResult)]
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    out = (SwarmResult * len(f))()
+    if L.ref_swarm_run(C.byref(cfg), C.byref(gas), dptr(f), len(f), workdir.encode(), out):
+        raise RuntimeError(L.ref_last_error().decode())
+    return list(out)
+
+
+def swarm_from_spec(spec, tables: TableSet):
+    """(SwarmConfig, MccModel) of an apic.workloads.SwarmSpec."""
+    chans = [tables.channel(c.process, c.energy, c.sigma, c.threshold, c.secondary, c.ion, angular=c.angular,
+                            mu_energy=c.mu_energy, mu=c.mu) for c in spec.channels]
+    gas = make_model(0, chans, spec.neutral_density, spec.max_frequency, spec.neutral_mass,
+                     spec.neutral_temperature, 1, spec.max_candidates)
+    cfg = swarm_config(neutral_density=spec.neutral_density, max_frequency=spec.max_frequency,
+                       timestep=spec.timestep, steps=spec.steps, burn_in_steps=spec.burn_in_steps,
+                       particles=spec.particles, neutral_temperature=spec.neutral_temperature,
+                       branching=spec.branching, population_limit=spec.population_limit,
+                       uncertainty_blocks=spec.uncertainty_blocks,
+                       initial_mean_energy_ev=spec.initial_mean_energy_ev, max_energy_ev=spec.max_energy_ev,
+                       seed=spec.seed)
+    return cfg, gas

@@ -81,7 +81,11 @@ pic::CollisionConfig collision_config(const ora_mcc_model& m, const std::string&
         cc.threshold_energy = ch.threshold_energy;
         cc.angular_scattering = ch.angular == ORA_BACKWARD
                                     ? pic::AngularScatteringKind::Backward
+                                    : ch.angular == ORA_HENYEY_GREENSTEIN
+                                    ? pic::AngularScatteringKind::HenyeyGreenstein
                                     : pic::AngularScatteringKind::Isotropic;
+        if (ch.angular == ORA_HENYEY_GREENSTEIN)
+            cc.mean_cosine_file = write_table(dir, cc.name + "_mu", ch.mu_rows, ch.mu_energy, ch.mu);
         cc.energy_frame = ch.energy_frame == ORA_FRAME_CENTER_OF_MASS
                               ? pic::CollisionEnergyFrame::CenterOfMass
                               : pic::CollisionEnergyFrame::Projectile;
@@ -510,6 +514,120 @@ int ref_solve_nd(int dims, const size_t* n, const double* L, double eps, const d
         }
         return 0;
     } catch (const std::exception& e) { return fail(e); }
+}
+
+}  // extern "C"
+
+/* ---- pic::run_swarm_benchmark (src/Swarm.cpp:1503-1524) ------------------ */
+namespace {
+const char* process_name(int p) {
+    switch (p) {
+        case ORA_ELASTIC: return "elastic";
+        case ORA_EXCITATION: return "excitation";
+        case ORA_IONIZATION: return "ionization";
+        case ORA_ATTACHMENT: return "attachment";
+        default: return "charge_exchange";
+    }
+}
+
+// A version-2 SI gas dataset (src/GasDataset.cpp:151-460) holding the
+// channels of `gas`, with tables in joules and square metres.
+std::string write_gas_dataset(const ora_mcc_model& gas, const std::string& dir) {
+    std::filesystem::create_directories(dir);
+    const std::string path = dir + "/gas.gas";
+    std::ofstream out(path);
+    out << std::setprecision(17);
+    out << "gas_data_version = 2\nunits = si\ngas = synthetic\nneutral_mass = " << gas.neutral_mass
+        << "\ndataset_id = oracle.synthetic\ndataset_version = 1\ndata_provenance = oracle harness\n"
+        << "citation = none\nretrieved = 2026-01-01\nlicense = synthetic test data\n";
+    for (int i = 0; i < gas.nch; ++i) {
+        const ora_channel& ch = gas.ch[i];
+        const std::string name = "ch" + std::to_string(i);
+        out << "\n[collision." << name << "]\ntype = " << process_name(ch.process) << "\n";
+        out << "cross_section_file = " << write_table(dir, name, ch.rows, ch.energy, ch.sigma) << "\n";
+        if (ch.threshold_energy != 0.0) out << "threshold_energy = " << ch.threshold_energy << "\n";
+        if (ch.energy_frame == ORA_FRAME_CENTER_OF_MASS) out << "energy_frame = center_of_mass\n";
+        if (ch.angular == ORA_BACKWARD) out << "angular_model = backward\n";
+        if (ch.angular == ORA_HENYEY_GREENSTEIN) {
+            out << "angular_model = henyey_greenstein\n";
+            out << "mean_cosine_file = " << write_table(dir, name + "_mu", ch.mu_rows, ch.mu_energy, ch.mu) << "\n";
+        }
+    }
+    if (!out) throw std::runtime_error("cannot write gas dataset " + path);
+    return path;
+}
+}  // namespace
+
+extern "C" {
+
+int ref_swarm_run(const ora_swarm_config* cfg, const ora_mcc_model* gas, const double* fields, size_t nfields,
+                  const char* workdir, ora_swarm_result* out) {
+    try {
+        pic::SwarmBenchmarkConfig c;
+        c.gas_data_file = write_gas_dataset(*gas, workdir);
+        c.neutral_density = cfg->neutral_density;
+        c.neutral_temperature = cfg->neutral_temperature;
+        c.reduced_fields_td.assign(fields, fields + nfields);
+        c.max_frequency = cfg->max_frequency;
+        c.timestep = cfg->timestep;
+        c.steps = cfg->steps;
+        c.burn_in_steps = cfg->burn_in_steps;
+        c.particles = cfg->particles;
+        c.population_model = cfg->branching ? pic::SwarmPopulationModel::BranchingResampled
+                                            : pic::SwarmPopulationModel::FixedPopulationNoAvalanche;
+        c.population_limit = cfg->population_limit;
+        c.uncertainty_blocks = cfg->uncertainty_blocks;
+        c.work_item_limit = 1000000000000000000ull;
+        c.initial_mean_energy_ev = cfg->initial_mean_energy_ev;
+        c.max_energy_ev = cfg->max_energy_ev;
+        c.seed = cfg->seed;
+        c.output_file = std::string(workdir) + "/swarm.csv";
+        const auto results = pic::run_swarm_benchmark(c);
+        for (size_t f = 0; f < results.size(); ++f) {
+            const auto& r = results[f];
+            ora_swarm_result& o = out[f];
+            std::memset(&o, 0, sizeof o);
+            o.reduced_field_td = r.reduced_field_td;
+            o.electric_field_v_m = r.electric_field_v_m;
+            o.mean_velocity_x = r.mean_velocity_x_m_s;
+            o.mean_velocity_x_se = r.mean_velocity_x_standard_error_m_s;
+            o.drift_velocity = r.electron_drift_velocity_m_s;
+            o.reduced_mobility = r.reduced_mobility_1_v_m_s;
+            o.mean_energy_ev = r.mean_energy_ev;
+            o.mean_energy_se_ev = r.mean_energy_standard_error_ev;
+            o.diffusion_available = r.diffusion_available;
+            o.diffusion_longitudinal = r.longitudinal_diffusion_m2_s;
+            o.diffusion_transverse = r.transverse_diffusion_m2_s;
+            o.max_observed_energy_ev = r.maximum_observed_energy_ev;
+            o.initial_weight = r.initial_total_electron_weight;
+            o.final_weight = r.final_total_electron_weight;
+            o.final_particles = r.final_computational_particles;
+            o.growth_rate = r.temporal_growth_rate_s;
+            o.growth_rate_se = r.temporal_growth_rate_standard_error_s;
+            o.ionization_rate = r.ionization_rate_s;
+            o.ionization_rate_se = r.ionization_rate_standard_error_s;
+            o.attachment_rate = r.attachment_rate_s;
+            o.attachment_rate_se = r.attachment_rate_standard_error_s;
+            o.net_rate = r.net_creation_rate_s;
+            o.net_rate_se = r.net_creation_rate_standard_error_s;
+            o.townsend_available = r.townsend_available;
+            o.townsend_growth = r.growth_over_flux_drift_townsend_1_m;
+            o.townsend_growth_se = r.growth_over_flux_drift_townsend_standard_error_1_m;
+            o.townsend_rate = r.rate_balance_effective_townsend_1_m;
+            o.townsend_rate_se = r.rate_balance_effective_townsend_standard_error_1_m;
+            o.candidates = r.collision_candidates;
+            o.null_collisions = r.null_collisions;
+            o.nch = static_cast<int>(r.channels.size());
+            for (size_t k = 0; k < r.channels.size() && k < ORA_MAX_CHANNELS; ++k) {
+                o.channel_collisions[k] = r.channels[k].collisions;
+                o.channel_rate[k] = r.channels[k].rate_per_electron_s;
+                o.channel_rate_se[k] = r.channels[k].poisson_standard_error_s;
+            }
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e);
+    }
 }
 
 }  // extern "C"

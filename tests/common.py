@@ -32,3 +32,23 @@ def rel_max(a, b):
     if scale == 0.0:
         return float(np.max(np.abs(a))) if a.size else 0.0
     return float(np.max(np.abs(a - b)) / scale)
+
+
+def swarm_cases():
+    """The small swarm decks pinned by golden vectors from the reference's
+    run_swarm_benchmark (tests/golden/swarm_*.npz)."""
+    fixed = W.swarm_c5(fields_td=(10.0, 300.0), particles=200, steps=300, burn_in_steps=100)
+    ch, mn = W.swarm_gas_anisotropic(attachment=True)
+    ng, T = 1e24, 300.0
+    nu = W.swarm_max_frequency(ch, ng, mn, T, 150.0)
+    branching = W.SwarmSpec("aniso_attach", ch, mn, ng, T, nu, 0.08 / nu, 400, 200, 300, [50.0, 400.0],
+                            branching=True, uncertainty_blocks=10, initial_mean_energy_ev=2.0, max_energy_ev=150.0,
+                            seed=99)
+    return {"swarm_fixed": fixed, "swarm_branching": branching}
+
+
+SWARM_KEYS = ("mean_velocity_x", "mean_velocity_x_se", "drift_velocity", "reduced_mobility", "mean_energy_ev",
+              "mean_energy_se_ev", "diffusion_longitudinal", "diffusion_transverse", "max_observed_energy_ev",
+              "final_weight", "final_particles", "growth_rate", "growth_rate_se", "ionization_rate",
+              "ionization_rate_se", "attachment_rate", "attachment_rate_se", "net_rate", "townsend_growth",
+              "townsend_rate", "candidates", "null_collisions")

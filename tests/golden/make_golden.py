@@ -148,7 +148,54 @@ def nd_fixture(name):
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
+def collide_hg_fixture():
+    """NullCollisionModel::collide with Henyey-Greenstein elastic scattering,
+    ionization and attachment (electron projectile, thermal neutrals)."""
+    R = po.ref()
+    ch, mn = W.swarm_gas_anisotropic(attachment=True)
+    T = po.TableSet()
+    chans = [T.channel(c.process, c.energy, c.sigma, c.threshold, 0 if c.process == W.IONIZATION else -1,
+                       1 if c.process == W.IONIZATION else -1, angular=c.angular, mu_energy=c.mu_energy, mu=c.mu)
+             for c in ch]
+    nu = W.swarm_max_frequency(ch, 1e24, mn, 300.0, 200.0)
+    m = po.make_model(0, chans, 1e24, nu, mn, 300.0, 1, 64)
+    rng = np.random.default_rng(300)
+    n = 400
+    v = rng.standard_normal((n, 3)) * 1.2e6
+    seeds = rng.integers(1, 2 ** 62, n, dtype=np.uint64)
+    stats = (po.CollideStats * n)()
+    vv = np.ascontiguousarray(v.copy())
+    dt = 2.0 / nu
+    rc = R.ref_collide3(C.byref(m), W.M_E, tempfile.mkdtemp().encode(), n, po.dptr(vv.reshape(-1)),
+                        po.u64ptr(seeds), dt, stats, None, 0)
+    assert rc == 0, R.ref_last_error()
+    np.savez_compressed(os.path.join(HERE, "collide3_hg.npz"), v_in=v, v_out=vv, seeds=seeds, dt=dt, nu=nu,
+                        candidates=np.array([s.candidates for s in stats], np.uint64),
+                        channels=np.array([list(s.channel_collisions) for s in stats], np.uint64),
+                        nsec=np.array([s.nsecondaries for s in stats], np.int32),
+                        removed=np.array([s.removed for s in stats], np.int32),
+                        draws=np.array([s.draws for s in stats], np.uint64),
+                        sec_v=np.array([[list(s.secondary_velocity[k]) for k in range(4)] for s in stats]))
+
+
+def swarm_fixture():
+    """pic::run_swarm_benchmark on the small decks of tests/common.py."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from common import swarm_cases, SWARM_KEYS
+    for name, spec in swarm_cases().items():
+        T = po.TableSet()
+        cfg, gas = po.swarm_from_spec(spec, T)
+        res = po.ref_swarm_run(cfg, gas, spec.fields_td, tempfile.mkdtemp())
+        out = {k: np.array([getattr(r, k) for r in res]) for k in SWARM_KEYS}
+        out["channel_collisions"] = np.array([list(r.channel_collisions)[: r.nch] for r in res], np.uint64)
+        out["channel_rate"] = np.array([list(r.channel_rate)[: r.nch] for r in res])
+        out["fields_td"] = np.array(spec.fields_td)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
 def main():
+    swarm_fixture()
+    collide_hg_fixture()
     for name in ND_CASES:
         nd_fixture(name)
     rng_fixture()
