@@ -24,7 +24,7 @@ PERIODIC, DIRICHLET = 0, 1
 NORMALIZED, SI = 0, 1
 FP64, FP32 = 0, 1
 ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, CHARGE_EXCHANGE = range(5)
-ISOTROPIC, BACKWARD = 0, 1
+ISOTROPIC, BACKWARD, HENYEY_GREENSTEIN = 0, 1, 2
 
 STATUS = {
     0: "APIC_OK", 1: "APIC_ERR_INVALID", 2: "APIC_ERR_CUDA", 3: "APIC_ERR_CAPACITY",
@@ -44,6 +44,8 @@ class McChannel(C.Structure):
         ("process", C.c_int), ("angular", C.c_int), ("energy_frame", C.c_int),
         ("threshold_energy", C.c_double), ("secondary_species", C.c_int), ("ion_species", C.c_int),
         ("rows", C.c_size_t), ("energy", C.POINTER(C.c_double)), ("sigma", C.POINTER(C.c_double)),
+        ("mean_cosine_rows", C.c_size_t), ("mean_cosine_energy", C.POINTER(C.c_double)),
+        ("mean_cosine", C.POINTER(C.c_double)),
     ]
 
 
@@ -181,11 +183,18 @@ class Tables:
         self.keep = []
 
     def channel(self, process, energy, sigma, threshold=0.0, secondary=-1, ion=-1, angular=ISOTROPIC,
-                frame=0) -> McChannel:
+                frame=0, mu_energy=None, mu=None) -> McChannel:
+        """angular HENYEY_GREENSTEIN takes the mean-cosine table mu(mu_energy)."""
         e = np.ascontiguousarray(energy, dtype=np.float64)
         s = np.ascontiguousarray(sigma, dtype=np.float64)
         self.keep += [e, s]
-        return McChannel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+        ch = McChannel(process, angular, frame, threshold, secondary, ion, len(e), dptr(e), dptr(s))
+        if mu is not None:
+            me = np.ascontiguousarray(mu_energy, dtype=np.float64)
+            mv = np.ascontiguousarray(mu, dtype=np.float64)
+            self.keep += [me, mv]
+            ch.mean_cosine_rows, ch.mean_cosine_energy, ch.mean_cosine = len(me), dptr(me), dptr(mv)
+        return ch
 
 
 def mcc_model(species, channels, neutral_density, max_frequency, neutral_mass=0.0, neutral_temperature=0.0,
@@ -535,3 +544,144 @@ def _simnd_load_maxwellian(self, species, n, seed, thermal_speed, drift_x=0.0, p
 
 
 SimulationND.load_maxwellian = _simnd_load_maxwellian
+
+
+# ---------------------------------------------------------------------------
+# Homogeneous electron swarms (run_swarm_benchmark) and the serving loop
+
+SWARM_FIXED, SWARM_BRANCHING = 0, 1
+
+
+class SwarmConfig(C.Structure):
+    _fields_ = [
+        ("neutral_density", C.c_double), ("neutral_temperature", C.c_double),
+        ("max_frequency", C.c_double), ("timestep", C.c_double),
+        ("steps", C.c_size_t), ("burn_in_steps", C.c_size_t), ("particles", C.c_size_t),
+        ("population_model", C.c_int), ("population_limit", C.c_size_t), ("uncertainty_blocks", C.c_size_t),
+        ("work_item_limit", C.c_uint64),
+        ("initial_mean_energy_ev", C.c_double), ("max_energy_ev", C.c_double), ("seed", C.c_uint64),
+        ("precision", C.c_int),
+    ]
+
+
+class SwarmResult(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64), ("status", C.c_int), ("message", C.c_char * 256),
+        ("steps_done", C.c_uint64), ("converged", C.c_int), ("latency_s", C.c_double), ("queue_s", C.c_double),
+        ("reduced_field_td", C.c_double), ("electric_field_v_m", C.c_double),
+        ("mean_velocity_x", C.c_double), ("mean_velocity_x_se", C.c_double),
+        ("drift_velocity", C.c_double), ("reduced_mobility", C.c_double),
+        ("mean_energy_ev", C.c_double), ("mean_energy_se_ev", C.c_double),
+        ("diffusion_available", C.c_int),
+        ("diffusion_longitudinal", C.c_double), ("diffusion_transverse", C.c_double),
+        ("max_observed_energy_ev", C.c_double),
+        ("initial_weight", C.c_double), ("final_weight", C.c_double),
+        ("final_particles", C.c_uint64),
+        ("growth_rate", C.c_double), ("growth_rate_se", C.c_double),
+        ("ionization_rate", C.c_double), ("ionization_rate_se", C.c_double),
+        ("attachment_rate", C.c_double), ("attachment_rate_se", C.c_double),
+        ("net_rate", C.c_double), ("net_rate_se", C.c_double),
+        ("townsend_available", C.c_int),
+        ("townsend_growth", C.c_double), ("townsend_growth_se", C.c_double),
+        ("townsend_rate", C.c_double), ("townsend_rate_se", C.c_double),
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64),
+        ("nch", C.c_int),
+        ("channel_collisions", C.c_uint64 * MAX_CHANNELS),
+        ("channel_rate", C.c_double * MAX_CHANNELS), ("channel_rate_se", C.c_double * MAX_CHANNELS),
+    ]
+
+
+class SwarmServerConfig(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_runs", C.c_int), ("precision", C.c_int),
+                ("steps_per_launch", C.c_size_t)]
+
+
+class SwarmRequest(C.Structure):
+    _fields_ = [
+        ("reduced_field_td", C.c_double), ("particles", C.c_size_t), ("seed", C.c_uint64),
+        ("steps", C.c_size_t), ("burn_in_steps", C.c_size_t), ("uncertainty_blocks", C.c_size_t),
+        ("tolerance", C.c_double), ("population_model", C.c_int), ("population_limit", C.c_size_t),
+        ("initial_mean_energy_ev", C.c_double), ("max_energy_ev", C.c_double), ("timestep", C.c_double),
+    ]
+
+
+def _bind_swarm():
+    L = lib()
+    if getattr(L, "_swarm_bound", False):
+        return L
+    P = C.c_void_p
+    L.apic_swarm_run.argtypes = [C.POINTER(SwarmConfig), C.POINTER(MccModel), C.POINTER(C.c_double), C.c_size_t,
+                                 C.POINTER(SwarmResult)]
+    L.apic_swarm_last_error.restype = C.c_char_p
+    L.apic_swarm_last_error.argtypes = [P]
+    L.apic_swarm_server_create.argtypes = [C.POINTER(SwarmServerConfig), C.POINTER(MccModel), C.POINTER(P)]
+    L.apic_swarm_server_destroy.argtypes = [P]
+    L.apic_swarm_server_submit.argtypes = [P, C.POINTER(SwarmRequest), C.POINTER(C.c_uint64)]
+    L.apic_swarm_server_advance.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.apic_swarm_server_poll.argtypes = [P, C.c_uint64, C.POINTER(SwarmResult), C.POINTER(C.c_int)]
+    L.apic_swarm_server_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)]
+    L.apic_swarm_server_cuda_stream.argtypes = [P, C.POINTER(P)]
+    L._swarm_bound = True
+    return L
+
+
+def _check_swarm(rc, handle=None):
+    if rc != 0:
+        raise ApicError(rc, _bind_swarm().apic_swarm_last_error(handle).decode(errors="replace"))
+
+
+def swarm_run(cfg: SwarmConfig, gas: MccModel, fields_td):
+    """run_swarm_benchmark on the device: one SwarmResult per reduced field."""
+    L = _bind_swarm()
+    f = np.ascontiguousarray(fields_td, dtype=np.float64)
+    out = (SwarmResult * len(f))()
+    _check_swarm(L.apic_swarm_run(C.byref(cfg), C.byref(gas), f.ctypes.data_as(C.POINTER(C.c_double)), len(f), out))
+    return list(out)
+
+
+class SwarmServer:
+    """The batched swarm server (admission by memory budget and run slots,
+    graph-launched steps, retirement on convergence)."""
+
+    def __init__(self, gas: MccModel, memory_budget_bytes, max_runs=64, precision=FP32, steps_per_launch=64):
+        L = _bind_swarm()
+        self.conf = SwarmServerConfig(memory_budget_bytes, max_runs, precision, steps_per_launch)
+        h = C.c_void_p()
+        _check_swarm(L.apic_swarm_server_create(C.byref(self.conf), C.byref(gas), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _bind_swarm().apic_swarm_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, req: SwarmRequest) -> int:
+        i = C.c_uint64()
+        _check_swarm(_bind_swarm().apic_swarm_server_submit(self.h, C.byref(req), C.byref(i)), self.h)
+        return i.value
+
+    def advance(self):
+        a, q = C.c_int(), C.c_int()
+        _check_swarm(_bind_swarm().apic_swarm_server_advance(self.h, C.byref(a), C.byref(q)), self.h)
+        return a.value, q.value
+
+    def poll(self, rid):
+        out, done = SwarmResult(), C.c_int()
+        _check_swarm(_bind_swarm().apic_swarm_server_poll(self.h, rid, C.byref(out), C.byref(done)), self.h)
+        return out if done.value else None
+
+    def stats(self):
+        g, p, f = C.c_uint64(), C.c_uint64(), C.c_size_t()
+        _check_swarm(_bind_swarm().apic_swarm_server_stats(self.h, C.byref(g), C.byref(p), C.byref(f)), self.h)
+        return g.value, p.value, f.value
+
+    def cuda_stream(self) -> int:
+        s = C.c_void_p()
+        _check_swarm(_bind_swarm().apic_swarm_server_cuda_stream(self.h, C.byref(s)), self.h)
+        return s.value or 0

@@ -403,3 +403,27 @@ def swarm_c5(fields_td=(10.0, 100.0, 1000.0), particles=100_000, steps=2000, bur
     return SwarmSpec("swarm_4process", ch, mn, ng, T, nu, 0.1 / nu, steps, burn_in_steps, particles,
                      list(fields_td), branching=branching, initial_mean_energy_ev=1.0,
                      max_energy_ev=max_energy_ev, seed=seed)
+
+
+def to_device_swarm(spec: SwarmSpec, precision=0):
+    """(apic.SwarmConfig, apic.MccModel, Tables) of a swarm deck."""
+    from . import SWARM_BRANCHING, SWARM_FIXED, SwarmConfig, Tables, mcc_model
+    tabs = Tables()
+    chans = [tabs.channel(c.process, c.energy, c.sigma, c.threshold, c.secondary, c.ion, angular=c.angular,
+                          mu_energy=c.mu_energy, mu=c.mu) for c in spec.channels]
+    gas = mcc_model(0, chans, spec.neutral_density, spec.max_frequency, spec.neutral_mass, spec.neutral_temperature,
+                    1, spec.max_candidates)
+    cfg = SwarmConfig(spec.neutral_density, spec.neutral_temperature, spec.max_frequency, spec.timestep,
+                      spec.steps, spec.burn_in_steps, spec.particles,
+                      SWARM_BRANCHING if spec.branching else SWARM_FIXED, spec.population_limit,
+                      spec.uncertainty_blocks, 0, spec.initial_mean_energy_ev, spec.max_energy_ev, spec.seed,
+                      precision)
+    return cfg, gas, tabs
+
+
+def swarm_request(spec: SwarmSpec, td, particles=None, seed=None, steps=None, burn_in_steps=None, tolerance=0.0):
+    from . import SWARM_BRANCHING, SWARM_FIXED, SwarmRequest
+    return SwarmRequest(td, particles or spec.particles, spec.seed if seed is None else seed, steps or spec.steps,
+                        spec.burn_in_steps if burn_in_steps is None else burn_in_steps, spec.uncertainty_blocks,
+                        tolerance, SWARM_BRANCHING if spec.branching else SWARM_FIXED, spec.population_limit,
+                        spec.initial_mean_energy_ev, spec.max_energy_ev, spec.timestep)

@@ -24,7 +24,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
           "--expt-relaxed-constexpr", "--extended-lambda", "-I", os.path.join(ROOT, "include")]
 # Files whose FP64 arithmetic mirrors the reference operation by operation.
-NO_FMA = {"pic1d.cu", "pic2d3d.cu"}
+NO_FMA = {"pic1d.cu", "pic2d3d.cu", "swarm.cu"}
 
 
 def nvcc() -> str:

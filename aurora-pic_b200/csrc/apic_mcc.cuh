@@ -47,6 +47,9 @@ struct MccChannelDev {
     const double* energy;
     const double* sigma;
     TableIndex index;
+    int mu_rows;              // Henyey-Greenstein mean-cosine table (0: none)
+    const double* mu_energy;
+    const double* mu;
 };
 
 struct MccModelDev {
@@ -195,6 +198,53 @@ __device__ inline void isotropic(double speed, S& s, double out[3]) {
     out[2] = speed * cosine;
 }
 
+// MeanCosineTable::evaluate, src/Collision.cpp:296-313
+__device__ inline double mean_cosine(const MccChannelDev& c, double energy) {
+    const double* e = c.mu_energy;
+    const int n = c.mu_rows;
+    if (energy <= e[0]) return c.mu[0];
+    if (energy >= e[n - 1]) return c.mu[n - 1];
+    int lo = 0, hi = n;  // upper_bound
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (energy < e[mid]) hi = mid; else lo = mid + 1;
+    }
+    const int high = lo, low = high - 1;
+    const double fraction = (energy - e[low]) / (e[high] - e[low]);
+    return c.mu[low] + fraction * (c.mu[high] - c.mu[low]);
+}
+
+// angular_velocity: Henyey-Greenstein deflection about the incoming relative
+// velocity, src/Collision.cpp:66-129
+template <class S>
+__device__ inline void angular_velocity(const double in[3], double speed, double g, S& s, double out[3]) {
+    const double in_speed = norm3(in[0], in[1], in[2]);
+    if (!(in_speed > 0.0)) { isotropic(speed, s, out); return; }
+    const double sample = uniform01(s);
+    double cosine = 2.0 * sample - 1.0;
+    if (g != 0.0) {
+        const double numerator = 1.0 - g * g;
+        const double denominator = 1.0 - g + 2.0 * g * sample;
+        const double ratio = numerator / denominator;
+        cosine = (1.0 + g * g - ratio * ratio) / (2.0 * g);
+        cosine = cosine < -1.0 ? -1.0 : (cosine > 1.0 ? 1.0 : cosine);
+    }
+    const double t = 1.0 - cosine * cosine;
+    const double sine = sqrt(0.0 > t ? 0.0 : t);
+    const double azimuth = 2.0 * 3.141592653589793 * uniform01(s);
+    const double d[3] = {in[0] / in_speed, in[1] / in_speed, in[2] / in_speed};
+    const bool low = fabs(d[2]) < 0.9;
+    const double h[3] = {0.0, low ? 0.0 : 1.0, low ? 1.0 : 0.0};
+    double tg[3] = {h[1] * d[2] - h[2] * d[1], h[2] * d[0] - h[0] * d[2], h[0] * d[1] - h[1] * d[0]};
+    const double tn = norm3(tg[0], tg[1], tg[2]);
+    tg[0] /= tn; tg[1] /= tn; tg[2] /= tn;
+    const double bt[3] = {d[1] * tg[2] - d[2] * tg[1], d[2] * tg[0] - d[0] * tg[2], d[0] * tg[1] - d[1] * tg[0]};
+    double sn, cs;
+    sincos(azimuth, &sn, &cs);
+    const double tf = sine * cs, bf = sine * sn;
+    for (int k = 0; k < 3; ++k) out[k] = speed * (cosine * d[k] + tf * tg[k] + bf * bt[k]);
+}
+
 struct CollideResult {
     unsigned candidates = 0, nulls = 0;
     unsigned channel[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -274,6 +324,8 @@ __device__ inline void collide3(const MccModelDev& m, double v[3], double dt, S&
                     const double speed = sqrt(2.0 * energy / m.particle_mass);
                     double sc[3];
                     if (c.angular == 1) { sc[0] = -rel[0]; sc[1] = -rel[1]; sc[2] = -rel[2]; }
+                    else if (c.angular == 2 && c.mu_rows)
+                        angular_velocity(rel, speed, mean_cosine(c, collision_energy(m, c, initial_speed)), s, sc);
                     else isotropic(speed, s, sc);
                     if (c.process == kElastic && m.neutral_mass > 0.0) {
                         const double total = m.particle_mass + m.neutral_mass;

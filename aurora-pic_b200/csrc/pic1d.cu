@@ -39,6 +39,7 @@
 
 #include "apic_common.cuh"
 #include "apic_mcc.cuh"
+#include "apic_mcc_host.h"
 #include "apic_rng.cuh"
 
 namespace apic {
@@ -955,84 +956,6 @@ std::string describe_device_error(unsigned w) {
     return s;
 }
 
-// Largest speed below which the reference's frequency-bound check
-// (validate_frequency_bound, src/Collision.cpp:627-685) cannot fail.  Each
-// channel's cross section is piecewise linear in energy and energy is
-// quadratic in speed, so between breakpoints the total rate is
-// n v (A + B v^2); its maximum per interval is exact.  Thermal neutrals use
-// the monotone majorant n (v + 8 sigma) sum_c max_{E <= E(v + 8 sigma)} sigma_c.
-static double safe_speed(const apic_mcc_model& m, double particle_mass, double neutral_stddev) {
-    const double margin = 1.0 - 1e-9;
-    const double target = m.max_frequency * margin;
-    const double com = m.neutral_mass > 0 ? particle_mass * m.neutral_mass / (particle_mass + m.neutral_mass) : 0;
-    auto mass_of = [&](const apic_mcc_channel& c) { return c.energy_frame == APIC_FRAME_CENTER_OF_MASS ? com : particle_mass; };
-    auto sigma_at = [&](const apic_mcc_channel& c, double e) {
-        if (e <= c.energy[0]) return c.sigma[0];
-        if (e >= c.energy[c.rows - 1]) return c.sigma[c.rows - 1];
-        const double* up = std::upper_bound(c.energy, c.energy + c.rows, e);
-        const size_t hi = (size_t)(up - c.energy), lo = hi - 1;
-        const double f = (e - c.energy[lo]) / (c.energy[hi] - c.energy[lo]);
-        return c.sigma[lo] + f * (c.sigma[hi] - c.sigma[lo]);
-    };
-    if (neutral_stddev == 0.0) {
-        // speed breakpoints of every channel
-        std::vector<double> br{0.0};
-        for (int i = 0; i < m.nch; ++i) {
-            const auto& c = m.ch[i];
-            const double ms = mass_of(c);
-            for (size_t k = 0; k < c.rows; ++k) br.push_back(std::sqrt(2.0 * c.energy[k] / ms));
-            if (c.threshold_energy > 0) br.push_back(std::sqrt(2.0 * c.threshold_energy / ms));
-        }
-        std::sort(br.begin(), br.end());
-        auto total = [&](double v) {
-            double t = 0;
-            for (int i = 0; i < m.nch; ++i) {
-                const auto& c = m.ch[i];
-                const double e = 0.5 * mass_of(c) * v * v;
-                if (e >= c.threshold_energy) t += m.neutral_density * sigma_at(c, e) * v;
-            }
-            return t;
-        };
-        for (size_t k = 0; k + 1 < br.size(); ++k) {
-            const double v1 = br[k], v2 = br[k + 1];
-            if (!(v2 > v1)) continue;
-            // sample the cubic densely enough to bound it (endpoints + interior extremum)
-            double mx = std::max(total(v1 * (1 + 1e-12) + 1e-300), total(v2 * (1 - 1e-12)));
-            for (int q = 1; q < 16; ++q) mx = std::max(mx, total(v1 + (v2 - v1) * q / 16.0));
-            if (mx * (1 + 1e-6) > target) return v1;
-        }
-        // beyond the last breakpoint every sigma is constant: rate = n v sum sigma_last
-        double s_last = 0;
-        for (int i = 0; i < m.nch; ++i) s_last += m.ch[i].sigma[m.ch[i].rows - 1];
-        if (s_last <= 0) return 1e300;
-        return std::min(std::max(br.back(), 0.0) == br.back() ? 1e300 : 0.0,
-                        target / (m.neutral_density * s_last) * (1 - 1e-6));
-    }
-    const double limit = kThermalSigma * neutral_stddev;
-    auto majorant = [&](double v) {
-        double b = 0;
-        for (int i = 0; i < m.nch; ++i) {
-            const auto& c = m.ch[i];
-            const double emax = 0.5 * mass_of(c) * (v + limit) * (v + limit);
-            if (emax < c.threshold_energy) continue;
-            double smax = sigma_at(c, 0.0);
-            for (size_t k = 0; k < c.rows && c.energy[k] <= emax; ++k) smax = std::max(smax, c.sigma[k]);
-            smax = std::max(smax, sigma_at(c, emax));
-            b += m.neutral_density * smax * (v + limit);
-        }
-        return b;
-    };
-    if (majorant(0.0) * (1 + 1e-6) > target) return -1.0;  // always check exactly
-    double lo = 0.0, hi = 1.0;
-    while (majorant(hi) * (1 + 1e-6) <= target && hi < 1e12) hi *= 2;
-    if (hi >= 1e12) return 1e300;
-    for (int it = 0; it < 200; ++it) {
-        const double mid = 0.5 * (lo + hi);
-        if (majorant(mid) * (1 + 1e-6) <= target) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
 struct Sim1D {
     apic_config1d cfg{};
     std::string last_error;
@@ -1062,32 +985,6 @@ struct Sim1D {
         if (stream) cudaStreamSynchronize(stream);
         for (void* a : allocations) cudaFree(a);
         if (stream) cudaStreamDestroy(stream);
-    }
-
-    // Bracket index over log2(energy) for a strictly increasing table.
-    TableIndex build_index(const double* e, size_t rows) {
-        TableIndex ix{};
-        size_t first_pos = 0;
-        while (first_pos < rows && !(e[first_pos] > 0.0)) ++first_pos;
-        if (first_pos + 1 >= rows) return ix;  // no usable positive range: plain binary search
-        const double lmin = std::log2(e[first_pos]);
-        const double lmax = std::log2(e[rows - 1]);
-        if (!(lmax > lmin)) return ix;
-        const int nbins = (int)std::min<size_t>(std::max<size_t>(rows, 256), 8192);
-        std::vector<unsigned> first(nbins + 1);
-        for (int b = 0; b <= nbins; ++b) {
-            const double edge = std::exp2(lmin + (lmax - lmin) * (double)b / (double)nbins);
-            first[b] = (unsigned)(std::upper_bound(e, e + rows, edge) - e);
-        }
-        first[nbins] = (unsigned)rows;
-        unsigned* d = dalloc<unsigned>(first.size());
-        APIC_CUDA(cudaMemcpyAsync(d, first.data(), first.size() * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
-        APIC_CUDA(cudaStreamSynchronize(stream));
-        ix.first_gt = d;
-        ix.nbins = nbins;
-        ix.lmin = lmin;
-        ix.inv_width = (double)nbins / (lmax - lmin);
-        return ix;
     }
 
     void create(const apic_config1d& c) {
@@ -1175,37 +1072,8 @@ struct Sim1D {
             require(p.sp[m.species].model < 0, "one MCC model per species is supported", APIC_ERR_UNSUPPORTED);
             require(c.velocity_dimensions == 3, "1D MCC on the device requires velocity_dimensions = 3",
                     APIC_ERR_UNSUPPORTED);
-            require(std::isfinite(m.neutral_density) && m.neutral_density > 0, "MCC neutral_density must be positive and finite");
-            require(std::isfinite(m.max_frequency) && m.max_frequency > 0, "MCC max_frequency must be positive and finite");
-            require(m.max_candidates > 0, "MCC max_candidates_per_particle must be positive");
-            require(m.nch >= 1 && m.nch <= kMaxChannels, "MCC requires at least one collision channel");
-            const double mass = c.species[m.species].mass;
-            MccModelDev& D = p.model[mi];
-            D.nch = m.nch;
-            D.species = m.species;
-            D.particle_mass = mass;
-            D.neutral_mass = m.neutral_mass;
-            D.neutral_density = m.neutral_density;
-            D.max_frequency = m.max_frequency;
-            D.max_candidates = (unsigned)std::min<size_t>(m.max_candidates, 0xFFFFFFFFu);
-            D.com_mass = m.neutral_mass > 0 ? mass * m.neutral_mass / (mass + m.neutral_mass) : 0.0;
-            double sd = 0.0;
-            if (m.gas_units_si && m.neutral_temperature > 0) {
-                require(m.neutral_mass > 0, "thermal-neutral MCC requires positive neutral_mass");
-                sd = std::sqrt(1.380649e-23 * m.neutral_temperature / m.neutral_mass);
-            }
-            D.neutral_stddev = sd;
-            neutral_stddev[mi] = sd;
-            for (int ci = 0; ci < m.nch; ++ci) {
+            for (int ci = 0; ci < m.nch && ci < kMaxChannels; ++ci) {
                 const apic_mcc_channel& ch = m.ch[ci];
-                require(ch.rows >= 2 && ch.energy && ch.sigma, "collision cross-section table requires at least two rows");
-                for (size_t k = 0; k < ch.rows; ++k) {
-                    require(std::isfinite(ch.energy[k]) && ch.energy[k] >= 0 && std::isfinite(ch.sigma[k]) && ch.sigma[k] >= 0,
-                            "collision table values must be finite and non-negative");
-                    require(k == 0 || ch.energy[k] > ch.energy[k - 1], "collision table energies must be strictly increasing");
-                }
-                require(ch.angular == APIC_ISOTROPIC || ch.angular == APIC_BACKWARD,
-                        "Henyey-Greenstein scattering is not supported", APIC_ERR_UNSUPPORTED);
                 require(ch.process != APIC_ATTACHMENT, "1D MCC does not support attachment");
                 if (ch.process == APIC_IONIZATION) {
                     require(ch.secondary_species >= 0 && ch.secondary_species < c.nspecies &&
@@ -1218,36 +1086,10 @@ struct Sim1D {
                                 tgt.mass == sec.mass && tgt.charge == sec.charge && ion.charge == -tgt.charge,
                             "1D ionization products violate the equal-weight charge-conservation contract");
                 }
-                if (ch.process == APIC_CHARGE_EXCHANGE) {
-                    const double tol = 64.0 * 2.220446049250313e-16 * std::max(mass, m.neutral_mass);
-                    require(m.neutral_mass > 0 && std::fabs(mass - m.neutral_mass) <= tol,
-                            "resonant charge exchange requires projectile mass equal to neutral_mass");
-                }
-                MccChannelDev& C = D.ch[ci];
-                C.process = ch.process;
-                C.angular = ch.angular;
-                C.frame = ch.energy_frame;
-                C.threshold = ch.threshold_energy;
-                C.secondary = ch.secondary_species;
-                C.ion = ch.ion_species;
-                C.rows = (int)ch.rows;
-                double* e = dalloc<double>(ch.rows);
-                double* s = dalloc<double>(ch.rows);
-                APIC_CUDA(cudaMemcpyAsync(e, ch.energy, ch.rows * sizeof(double), cudaMemcpyHostToDevice, stream));
-                APIC_CUDA(cudaMemcpyAsync(s, ch.sigma, ch.rows * sizeof(double), cudaMemcpyHostToDevice, stream));
-                C.energy = e;
-                C.sigma = s;
-                C.index = build_index(ch.energy, ch.rows);
             }
-            D.shared_grid = 1;
-            for (int ci = 0; ci < m.nch; ++ci) {
-                const apic_mcc_channel& a = m.ch[0];
-                const apic_mcc_channel& b = m.ch[ci];
-                if (b.energy_frame != APIC_FRAME_PROJECTILE || b.rows != a.rows ||
-                    std::memcmp(a.energy, b.energy, a.rows * sizeof(double)) != 0)
-                    D.shared_grid = 0;
-            }
-            D.v_safe = safe_speed(m, mass, sd);
+            DeviceArena arena{allocations, stream};
+            build_model(m, c.species[m.species].mass, arena, p.model[mi]);
+            neutral_stddev[mi] = p.model[mi].neutral_stddev;
             p.sp[m.species].model = mi;
             APIC_CUDA(cudaStreamSynchronize(stream));  // host tables may be freed after create
         }
@@ -1838,46 +1680,39 @@ int apic_collide3(const apic_mcc_model* model, double particle_mass, size_t n, d
         apic::require(model && v3 && stats, "null argument");
         apic::require(n > 0 && n < (1u << 30), "particle count out of range");
         apic::require(std::isfinite(dt) && dt > 0, "MCC timestep must be positive and finite");
-        apic_config1d c{};
-        c.boundary = APIC_DIRICHLET;
-        c.velocity_dimensions = 3;
-        c.units = APIC_SI;
-        c.nx = 3;
-        c.length = 1.0;
-        c.dt = dt;
-        // a projectile species plus an opposite-charge product species satisfy
-        // the model validation; the stateless form reports products in stats
-        c.nspecies = 2;
-        c.species[0].charge = 1.0;
-        c.species[0].mass = particle_mass;
-        c.species[0].weight = 1.0;
-        c.species[0].capacity = 1;
-        c.species[1] = c.species[0];
-        c.species[1].charge = -1.0;
-        c.nmodels = 1;
-        c.models[0] = *model;
-        c.models[0].species = 0;
-        for (int i = 0; i < model->nch; ++i) {
-            c.models[0].ch[i].secondary_species = 0;
-            c.models[0].ch[i].ion_species = 1;
-        }
-        apic::Sim1D S;
-        S.create(c);
-        cudaStream_t s = S.stream;
-        double* dv = S.dalloc<double>(3 * n);
-        apic_collide_stats* ds = S.dalloc<apic_collide_stats>(n);
+        // a standalone model: every channel kind (attachment and Henyey-Greenstein
+        // included); ionization products are reported in stats
+        std::vector<void*> allocs;
+        cudaStream_t s = nullptr;
+        APIC_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct Release {
+            std::vector<void*>& a;
+            cudaStream_t s;
+            ~Release() {
+                cudaStreamSynchronize(s);
+                for (void* p : a) cudaFree(p);
+                cudaStreamDestroy(s);
+            }
+        } release{allocs, s};
+        apic::DeviceArena arena{allocs, s};
+        apic_mcc_model mm = *model;
+        mm.species = 0;
+        apic::MccModelDev D{};
+        apic::build_model(mm, particle_mass, arena, D);
+        double* dv = arena.alloc<double>(3 * n);
+        apic_collide_stats* ds = arena.alloc<apic_collide_stats>(n);
         uint64_t* dd = nullptr;
         uint64_t* doff = nullptr;
         if (draws) {
             apic::require(offsets != nullptr, "replay draws need per-particle offsets");
             const uint64_t total = offsets[n];
-            dd = S.dalloc<uint64_t>(total);
-            doff = S.dalloc<uint64_t>(n + 1);
+            dd = arena.alloc<uint64_t>(total);
+            doff = arena.alloc<uint64_t>(n + 1);
             APIC_CUDA(cudaMemcpyAsync(dd, draws, total * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
             APIC_CUDA(cudaMemcpyAsync(doff, offsets, (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
         }
         APIC_CUDA(cudaMemcpyAsync(dv, v3, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-        apic::k_collide3<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(S.p.model[0], (int)n, dv, dt, dd, doff, seed,
+        apic::k_collide3<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(D, (int)n, dv, dt, dd, doff, seed,
                                                                     (uint32_t)step, stream, ds);
         APIC_CUDA(cudaGetLastError());
         APIC_CUDA(cudaMemcpyAsync(v3, dv, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));

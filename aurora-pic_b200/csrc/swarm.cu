@@ -1,0 +1,1377 @@
+// Homogeneous electron swarms on the device: run_field (src/Swarm.cpp:940-1250)
+// for many runs at once, and the serving loop that admits, steps and retires
+// them.
+//
+// Layout.  Every run owns structure-of-arrays electron state (velocity and
+// displacement since the sampling start, FP64 or FP32) in one device pool.
+// Runs are cut into chunks of kChunk electrons; a chunk table (run slot, first
+// electron) lists the chunks of every active run back to back, and one
+// persistent push kernel walks it, so runs of any size share one launch per
+// substep.  Per-chunk partial sums feed a per-run reduction whose summation
+// order depends on the run alone: a run's result is bit-identical whether it
+// runs alone or among others.
+//
+// Random numbers.  Philox4x32-10 streams keyed on (seed, electron index, step):
+// stream 0 for the collision loop, stream 1 (index 0xFFFFFFFF) for the
+// resampling offset, stream 2 (step 0xFFFFFFFF) for the initial Maxwellian.
+//
+// Per step (src/Swarm.cpp:994-1128): half kick, energy check, drift,
+// null-collision MCC, half kick, energy check, tallies; with branching, the
+// surviving electrons and the ionization secondaries are compacted in the
+// reference's order (survivors in order, then secondaries in parent order) and
+// systematically resampled back to the target population.  All electrons of a
+// run share one weight, so the resampling source of output s is the electron
+// ceil((u + s) M / N) - 1 of the M compacted ones.
+#include <cub/block/block_scan.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "aurorapic_b200.h"
+#include "apic_common.cuh"
+#include "apic_mcc.cuh"
+#include "apic_mcc_host.h"
+#include "apic_rng.cuh"
+
+namespace apic {
+cudaError_t bounded_wait(cudaStream_t stream, double seconds);
+
+namespace swarm {
+
+constexpr int kThreads = 256;
+constexpr int kChunk = 1024;
+constexpr int kItems = kChunk / kThreads;
+constexpr int kQueue = 384;                 // collision candidates buffered per chunk
+constexpr int kMaxBirthsPerElectron = 8;
+constexpr double kElectronMass = 9.1093837139e-31;  // src/Swarm.cpp:23
+constexpr double kEvToJ = 1.602176634e-19;          // src/Swarm.cpp:24-25
+constexpr double kTownsend = 1.0e-21;               // src/Swarm.cpp:26
+constexpr size_t kAllocationLimit = 10000000;        // src/Swarm.cpp:27
+
+enum : unsigned {
+    kErrMaxEnergyPre = 1u << 8,
+    kErrMaxEnergy = 1u << 9,
+    kErrPopulation = 1u << 10,
+    kErrExtinct = 1u << 11,
+};
+
+struct RunCfg {  // written by the host at admission, read-only on the device
+    double half_kick, dt, max_energy_ev, init_sd;
+    uint64_t seed;
+    uint32_t n, steps, burn_in, first_chunk, nchunks, limit;
+    int branching;
+    int pad;
+    void* v[3];
+    void* d[3];
+    void* bv[3];       // compacted population (branching), `limit` electrons
+    void* bd[3];
+    void* sv[3];       // secondaries staged per chunk (branching), nchunks * kChunk
+    uint32_t* skey;    // their keys: parent index within the chunk * 8 + secondary number
+    uint8_t* alive;    // survivors of the current step (branching)
+    double* samples;   // velocity, energy, log weight per sampling step
+};
+
+struct RunState {  // written by the device
+    uint32_t step, active;
+    unsigned error;
+    uint32_t m_prime, survivors, pad;
+    double weight, weight_next, u, exposure, max_ev;
+    unsigned long long candidates, nulls;
+    unsigned long long counts[kMaxChannels];
+    double wcoll[kMaxChannels], wcoll2[kMaxChannels];
+    double mean_d[3], var_l, var_t;
+};
+
+struct ChunkPartial {
+    double vsum, esum, emax;
+    unsigned long long cand, nulls;
+    unsigned counts[kMaxChannels];
+    unsigned surv, births, surv_off, birth_off;
+};
+
+struct Batch {
+    const RunCfg* cfg;
+    RunState* st;
+    const uint32_t* chunk_run;
+    const uint32_t* chunk_first;
+    const uint32_t* nchunks;
+    ChunkPartial* part;
+    int max_runs;
+    MccModelDev model;
+};
+
+struct QueueEntry {
+    double v[3];
+    double first_wait;
+    uint32_t local;
+    uint32_t draws;
+};
+
+template <class T>
+__device__ __forceinline__ T* arr(void* p) { return static_cast<T*>(p); }
+
+// kinetic_energy_ev, src/Swarm.cpp:95-101
+__device__ __forceinline__ double ke_ev(double x, double y, double z) {
+    const double s2 = x * x + y * y + z * z;
+    return 0.5 * kElectronMass * s2 / kEvToJ;
+}
+
+template <class T>
+__device__ __forceinline__ T store_as(double x) { return (T)x; }
+
+// Block-wide sum of one double per thread in a fixed tree order.
+__device__ double block_sum(double x, double* red) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+    return t;  // valid on thread 0
+}
+
+__device__ double block_max(double x, double* red) {
+    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) t = fmax(t, red[w]);
+    return t;
+}
+
+__device__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long* red) {
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = x;
+    __syncthreads();
+    unsigned long long t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+    return t;
+}
+
+// ---- initial Maxwellian (src/Swarm.cpp:948-956) --------------------------------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_swarm_init(RunCfg R) {
+    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= R.n) return;
+    PhiloxStream s(R.seed, i, 0xFFFFFFFFu, 2u);
+    NormalState ns;
+    for (int a = 0; a < 3; ++a) {
+        arr<T>(R.v[a])[i] = store_as<T>(normal(ns, s, 0.0, R.init_sd));
+        arr<T>(R.d[a])[i] = store_as<T>(0.0);
+    }
+}
+
+// ---- one step of every active run: kick, drift, MCC, kick, tallies -------------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, 2) k_swarm_push(Batch b) {
+    __shared__ QueueEntry s_queue[kQueue];
+    __shared__ unsigned char s_removed[kQueue];
+    __shared__ unsigned s_qlen, s_births;
+    __shared__ double s_red[kThreads / 32];
+    __shared__ unsigned long long s_redu[kThreads / 32];
+    const int tid = threadIdx.x;
+    const uint32_t nch_total = *b.nchunks;
+    const MccModelDev& M = b.model;
+
+    for (uint32_t c = blockIdx.x; c < nch_total; c += gridDim.x) {
+        const uint32_t slot = b.chunk_run[c];
+        const RunCfg& R = b.cfg[slot];
+        RunState& S = b.st[slot];
+        if (!S.active) continue;  // uniform over the CTA
+        const uint32_t first = b.chunk_first[c];
+        const uint32_t local_chunk = first / kChunk;
+        const uint32_t cnt = min((uint32_t)kChunk, R.n - first);
+        const uint32_t step = S.step;
+        const bool sampling = step >= R.burn_in;
+        if (tid == 0) { s_qlen = 0; s_births = 0; }
+        __syncthreads();
+
+        double v[kItems][3];
+        int queued[kItems];
+        unsigned err = 0;
+        double emax = 0.0;
+        unsigned cand = 0, nulls = 0, counts[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+        bool removed[kItems];
+        // -- phase A: half kick, energy check, drift, first waiting time --
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const uint32_t li = k * kThreads + tid;
+            const uint32_t i = first + li;
+            queued[k] = -1;
+            removed[k] = false;
+            v[k][0] = v[k][1] = v[k][2] = 0.0;
+            if (li >= cnt) continue;
+            for (int a = 0; a < 3; ++a) v[k][a] = (double)arr<T>(R.v[a])[i];
+            v[k][0] += R.half_kick;
+            const double pre = ke_ev(v[k][0], v[k][1], v[k][2]);
+            emax = fmax(emax, pre);
+            if (pre > R.max_energy_ev) err |= kErrMaxEnergyPre;
+            if (sampling) {
+                for (int a = 0; a < 3; ++a) {
+                    T* dp = arr<T>(R.d[a]) + i;
+                    *dp = store_as<T>((double)*dp + v[k][a] * R.dt);
+                }
+            }
+            // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
+            if (!frequency_bound_ok(M, norm3(v[k][0], v[k][1], v[k][2]))) err |= kErrMajorant;
+            PhiloxStream rng(R.seed, i, step, 0u);
+            double u = uniform01(rng);
+            for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
+            const double wait = -log(u) / M.max_frequency;
+            if (isfinite(wait) && wait < R.dt) {
+                const unsigned q = atomicAdd(&s_qlen, 1u);
+                if (q < (unsigned)kQueue) {
+                    QueueEntry& e = s_queue[q];
+                    e.v[0] = v[k][0]; e.v[1] = v[k][1]; e.v[2] = v[k][2];
+                    e.first_wait = wait;
+                    e.local = li;
+                    e.draws = rng.index;
+                    queued[k] = (int)q;
+                } else {
+                    queued[k] = -2;  // queue full: this thread runs the loop itself below
+                }
+            }
+        }
+        __syncthreads();
+        // -- phase B: the full collision loops, packed densely over the CTA --
+        auto run_collide = [&](QueueEntry& e) {
+            PhiloxStream rng(R.seed, first + e.local, step, 0u);
+            rng.seek(e.draws);
+            CollideResult r;
+            unsigned nsec = 0;
+            const uint32_t li = e.local;
+            collide3(M, e.v, R.dt, rng, r,
+                     [&](int, const double* vs, const double*) {
+                         if (!R.branching) return;  // fixed population: secondaries are not followed
+                         if (nsec >= (unsigned)kMaxBirthsPerElectron) { err |= kErrBirths; return; }
+                         const unsigned bi = atomicAdd(&s_births, 1u);
+                         if (bi >= (unsigned)kChunk) { err |= kErrBirths; return; }
+                         const size_t at = (size_t)local_chunk * kChunk + bi;
+                         for (int a = 0; a < 3; ++a) arr<T>(R.sv[a])[at] = store_as<T>(vs[a]);
+                         R.skey[at] = li * kMaxBirthsPerElectron + nsec;
+                         ++nsec;
+                     },
+                     true, e.first_wait);
+            err |= r.error;
+            cand += r.candidates;
+            nulls += r.nulls;
+            for (int ch = 0; ch < kMaxChannels; ++ch) counts[ch] += r.channel[ch];
+            return r.removed;
+        };
+        const unsigned qlen = min(s_qlen, (unsigned)kQueue);
+        for (unsigned q = tid; q < qlen; q += kThreads) s_removed[q] = run_collide(s_queue[q]) ? 1 : 0;
+        __syncthreads();
+        // -- phase C: second half kick, energy check, tallies, store --
+        double vsum = 0.0, esum = 0.0;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            const uint32_t li = k * kThreads + tid;
+            const uint32_t i = first + li;
+            if (li >= cnt) continue;
+            if (queued[k] >= 0) {
+                const QueueEntry& e = s_queue[queued[k]];
+                v[k][0] = e.v[0]; v[k][1] = e.v[1]; v[k][2] = e.v[2];
+                removed[k] = s_removed[queued[k]] != 0;
+            } else if (queued[k] == -2) {
+                QueueEntry e;
+                e.v[0] = v[k][0]; e.v[1] = v[k][1]; e.v[2] = v[k][2];
+                PhiloxStream rng(R.seed, i, step, 0u);
+                double u = uniform01(rng);
+                for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
+                e.first_wait = -log(u) / M.max_frequency;
+                e.local = li;
+                e.draws = rng.index;
+                removed[k] = run_collide(e);
+                v[k][0] = e.v[0]; v[k][1] = e.v[1]; v[k][2] = e.v[2];
+            }
+            v[k][0] += R.half_kick;
+            const double e = ke_ev(v[k][0], v[k][1], v[k][2]);
+            emax = fmax(emax, e);
+            if (e > R.max_energy_ev) err |= kErrMaxEnergy;
+            T vs[3];
+            for (int a = 0; a < 3; ++a) {
+                vs[a] = store_as<T>(v[k][a]);
+                arr<T>(R.v[a])[i] = vs[a];
+            }
+            if (R.branching) R.alive[i] = removed[k] ? 0 : 1;
+            // fixed population: the sample sums of this step (the stored values)
+            vsum += (double)vs[0];
+            esum += ke_ev((double)vs[0], (double)vs[1], (double)vs[2]);
+        }
+        if (err) atomicOr(&S.error, err);
+        // -- per-chunk partials, fixed reduction order --
+        unsigned surv = 0;
+        if (R.branching) {
+#pragma unroll
+            for (int k = 0; k < kItems; ++k) {
+                const uint32_t li = k * kThreads + tid;
+                if (li < cnt && !removed[k]) ++surv;
+            }
+        }
+        const double tv = block_sum(vsum, s_red);
+        const double te = block_sum(esum, s_red);
+        const double tm = block_max(emax, s_red);
+        const unsigned long long tc = block_sum_u64(cand, s_redu);
+        const unsigned long long tn = block_sum_u64(nulls, s_redu);
+        const unsigned long long ts = block_sum_u64(surv, s_redu);
+        unsigned long long tch[kMaxChannels];
+        for (int ch = 0; ch < M.nch; ++ch) tch[ch] = block_sum_u64(counts[ch], s_redu);
+        if (tid == 0) {
+            ChunkPartial& P = b.part[c];
+            P.vsum = tv;
+            P.esum = te;
+            P.emax = tm;
+            P.cand = tc;
+            P.nulls = tn;
+            for (int ch = 0; ch < kMaxChannels; ++ch) P.counts[ch] = ch < M.nch ? (unsigned)tch[ch] : 0u;
+            P.surv = (unsigned)ts;
+            P.births = min(s_births, (unsigned)kChunk);
+        }
+        __syncthreads();
+    }
+}
+
+// ---- branching: scan of survivors and secondaries per run ------------------------
+
+__global__ void __launch_bounds__(kThreads) k_swarm_branch_scan(Batch b) {
+    using Scan = cub::BlockScan<unsigned long long, kThreads>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ unsigned long long s_carry_s, s_carry_b;
+    const int slot = blockIdx.x;
+    if (slot >= b.max_runs) return;
+    const RunCfg& R = b.cfg[slot];
+    RunState& S = b.st[slot];
+    if (!S.active || !R.branching) return;
+    if (threadIdx.x == 0) { s_carry_s = 0; s_carry_b = 0; }
+    __syncthreads();
+    for (uint32_t base = 0; base < R.nchunks; base += kThreads) {
+        const uint32_t lc = base + threadIdx.x;
+        const bool ok = lc < R.nchunks;
+        ChunkPartial* P = ok ? &b.part[R.first_chunk + lc] : nullptr;
+        // survivors and births packed in one 64-bit scan (each < 2^32 per run)
+        const unsigned long long x = ok ? (((unsigned long long)P->surv << 32) | P->births) : 0ull;
+        unsigned long long ex, tot;
+        Scan(tmp).ExclusiveSum(x, ex, tot);
+        if (ok) {
+            P->surv_off = (unsigned)(s_carry_s + (ex >> 32));
+            P->birth_off = (unsigned)(s_carry_b + (ex & 0xFFFFFFFFull));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_carry_s += tot >> 32;
+            s_carry_b += tot & 0xFFFFFFFFull;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const unsigned long long mp = s_carry_s + s_carry_b;
+        S.survivors = (uint32_t)s_carry_s;
+        S.m_prime = (uint32_t)min(mp, 0xFFFFFFFFull);
+        if (mp > R.limit) atomicOr(&S.error, kErrPopulation);
+        if (mp == 0) atomicOr(&S.error, kErrExtinct);
+        // systematic_resample, src/Swarm.cpp:616-643: offset and output weight
+        PhiloxStream rng(R.seed, 0xFFFFFFFFu, S.step, 1u);
+        S.u = uniform01(rng);
+        S.weight_next = mp == R.n ? S.weight : (double)mp * S.weight / (double)R.n;
+    }
+}
+
+// Survivors in order, then the secondaries in parent order, into the
+// compacted population.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_swarm_branch_compact(Batch b) {
+    using Scan = cub::BlockScan<unsigned, kThreads>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ uint32_t s_key[kChunk];
+    __shared__ unsigned s_carry;
+    const uint32_t nch_total = *b.nchunks;
+    for (uint32_t c = blockIdx.x; c < nch_total; c += gridDim.x) {
+        const uint32_t slot = b.chunk_run[c];
+        const RunCfg& R = b.cfg[slot];
+        const RunState& S = b.st[slot];
+        if (!S.active || !R.branching || S.error) continue;
+        const ChunkPartial& P = b.part[c];
+        const uint32_t first = b.chunk_first[c];
+        const uint32_t local_chunk = first / kChunk;
+        const uint32_t cnt = min((uint32_t)kChunk, R.n - first);
+        if (threadIdx.x == 0) s_carry = 0;
+        __syncthreads();
+        for (uint32_t base = 0; base < cnt; base += kThreads) {
+            const uint32_t li = base + threadIdx.x;
+            const unsigned a = li < cnt ? R.alive[first + li] : 0u;
+            unsigned ex, tot;
+            Scan(tmp).ExclusiveSum(a, ex, tot);
+            if (a) {
+                const size_t dst = (size_t)P.surv_off + s_carry + ex;
+                for (int k = 0; k < 3; ++k) {
+                    arr<T>(R.bv[k])[dst] = arr<T>(R.v[k])[first + li];
+                    arr<T>(R.bd[k])[dst] = arr<T>(R.d[k])[first + li];
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_carry += tot;
+            __syncthreads();
+        }
+        const unsigned nb = P.births;
+        const size_t sbase = (size_t)local_chunk * kChunk;
+        for (unsigned j = threadIdx.x; j < nb; j += kThreads) s_key[j] = R.skey[sbase + j];
+        __syncthreads();
+        for (unsigned j = threadIdx.x; j < nb; j += kThreads) {
+            const uint32_t key = s_key[j];
+            unsigned rank = 0;
+            for (unsigned q = 0; q < nb; ++q) rank += s_key[q] < key ? 1u : 0u;
+            const size_t dst = (size_t)S.survivors + P.birth_off + rank;
+            const uint32_t parent = first + key / kMaxBirthsPerElectron;
+            for (int k = 0; k < 3; ++k) {
+                arr<T>(R.bv[k])[dst] = arr<T>(R.sv[k])[sbase + j];
+                arr<T>(R.bd[k])[dst] = arr<T>(R.d[k])[parent];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Systematic resampling back to N electrons, and the sample sums of the step.
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_swarm_branch_resample(Batch b) {
+    __shared__ double s_red[kThreads / 32];
+    const uint32_t nch_total = *b.nchunks;
+    for (uint32_t c = blockIdx.x; c < nch_total; c += gridDim.x) {
+        const uint32_t slot = b.chunk_run[c];
+        const RunCfg& R = b.cfg[slot];
+        const RunState& S = b.st[slot];
+        if (!S.active || !R.branching || S.error) continue;
+        const uint32_t first = b.chunk_first[c];
+        const uint32_t cnt = min((uint32_t)kChunk, R.n - first);
+        const uint32_t mp = S.m_prime;
+        double vsum = 0.0, esum = 0.0;
+        for (uint32_t li = threadIdx.x; li < cnt; li += kThreads) {
+            const uint32_t s = first + li;
+            uint32_t j = s;
+            if (mp != R.n) {
+                const double t = (S.u + (double)s) * (double)mp / (double)R.n;
+                const double cj = ceil(t) - 1.0;
+                j = cj < 0.0 ? 0u : (uint32_t)cj;
+                if (j > mp - 1) j = mp - 1;
+            }
+            T vs[3];
+            for (int k = 0; k < 3; ++k) {
+                vs[k] = arr<T>(R.bv[k])[j];
+                arr<T>(R.v[k])[s] = vs[k];
+                arr<T>(R.d[k])[s] = arr<T>(R.bd[k])[j];
+            }
+            vsum += (double)vs[0];
+            esum += ke_ev((double)vs[0], (double)vs[1], (double)vs[2]);
+        }
+        const double tv = block_sum(vsum, s_red);
+        const double te = block_sum(esum, s_red);
+        if (threadIdx.x == 0) {
+            b.part[c].vsum = tv;
+            b.part[c].esum = te;
+        }
+        __syncthreads();
+    }
+}
+
+// ---- per run: tallies and the samples of the step --------------------------------
+
+__global__ void __launch_bounds__(kThreads) k_swarm_reduce(Batch b) {
+    __shared__ double s_red[kThreads / 32];
+    __shared__ unsigned long long s_redu[kThreads / 32];
+    const int slot = blockIdx.x;
+    if (slot >= b.max_runs) return;
+    const RunCfg& R = b.cfg[slot];
+    RunState& S = b.st[slot];
+    if (!S.active) return;
+    const int nch = b.model.nch;
+    double vsum = 0.0, esum = 0.0, emax = 0.0;
+    unsigned long long cand = 0, nulls = 0, cnt[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t lc = threadIdx.x; lc < R.nchunks; lc += kThreads) {
+        const ChunkPartial& P = b.part[R.first_chunk + lc];
+        vsum += P.vsum;
+        esum += P.esum;
+        emax = fmax(emax, P.emax);
+        cand += P.cand;
+        nulls += P.nulls;
+        for (int ch = 0; ch < nch; ++ch) cnt[ch] += P.counts[ch];
+    }
+    const double tv = block_sum(vsum, s_red);
+    const double te = block_sum(esum, s_red);
+    const double tm = block_max(emax, s_red);
+    const unsigned long long tc = block_sum_u64(cand, s_redu);
+    const unsigned long long tn = block_sum_u64(nulls, s_redu);
+    unsigned long long tch[kMaxChannels];
+    for (int ch = 0; ch < nch; ++ch) tch[ch] = block_sum_u64(cnt[ch], s_redu);
+    if (threadIdx.x != 0) return;
+    const uint32_t step = S.step;
+    const double w = S.weight;
+    S.max_ev = fmax(S.max_ev, tm);
+    if (step >= R.burn_in) {
+        S.exposure += (double)R.n * w * R.dt;
+        S.candidates += tc;
+        S.nulls += tn;
+        for (int ch = 0; ch < nch; ++ch) {
+            S.counts[ch] += tch[ch];
+            S.wcoll[ch] += w * (double)tch[ch];
+            S.wcoll2[ch] += w * w * (double)tch[ch];
+        }
+    }
+    if (R.branching && !S.error) S.weight = S.weight_next;
+    if (step >= R.burn_in) {
+        const size_t ns = R.steps - R.burn_in;
+        const size_t k = step - R.burn_in;
+        R.samples[k] = tv / (double)R.n;
+        R.samples[ns + k] = te / (double)R.n;
+        R.samples[2 * ns + k] = log((double)R.n * S.weight);
+    }
+    S.step = step + 1;
+    if (S.step >= R.steps || S.error) S.active = 0;
+}
+
+// ---- per run: displacement statistics for the diffusion coefficients -------------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_swarm_moments(RunCfg R, RunState* S) {
+    __shared__ double s_red[kThreads / 32];
+    __shared__ double s_mean[3];
+    double m[3] = {0.0, 0.0, 0.0};
+    for (uint32_t i = threadIdx.x; i < R.n; i += kThreads)
+        for (int a = 0; a < 3; ++a) m[a] += (double)arr<T>(R.d[a])[i];
+    for (int a = 0; a < 3; ++a) {
+        const double t = block_sum(m[a], s_red);
+        if (threadIdx.x == 0) s_mean[a] = t / (double)R.n;
+        __syncthreads();
+    }
+    double vl = 0.0, vt = 0.0;
+    for (uint32_t i = threadIdx.x; i < R.n; i += kThreads) {
+        const double dx = (double)arr<T>(R.d[0])[i] - s_mean[0];
+        const double dy = (double)arr<T>(R.d[1])[i] - s_mean[1];
+        const double dz = (double)arr<T>(R.d[2])[i] - s_mean[2];
+        vl += dx * dx;
+        vt += dy * dy + dz * dz;
+    }
+    const double tl = block_sum(vl, s_red);
+    const double tt = block_sum(vt, s_red);
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) S->mean_d[a] = s_mean[a];
+        S->var_l = tl / (double)R.n;
+        S->var_t = tt / (double)R.n;
+    }
+}
+
+// ---- host side -------------------------------------------------------------------
+
+// block_mean_and_error, src/Swarm.cpp:103-134
+static bool block_mean_and_error(const double* x, size_t n, size_t blocks, double& mean, double& se) {
+    if (n == 0 || blocks == 0 || blocks > n) return false;
+    std::vector<double> means(blocks);
+    for (size_t b = 0; b < blocks; ++b) {
+        const size_t begin = b * n / blocks, end = (b + 1) * n / blocks;
+        double total = 0.0;
+        for (size_t i = begin; i < end; ++i) total += x[i];
+        means[b] = total / (double)(end - begin);
+    }
+    double m = 0.0;
+    for (double v : means) m += v;
+    m /= (double)blocks;
+    double e = 0.0;
+    if (blocks > 1) {
+        double sq = 0.0;
+        for (double v : means) sq += (v - m) * (v - m);
+        e = std::sqrt(sq / ((double)blocks * (double)(blocks - 1)));
+    }
+    mean = m;
+    se = e;
+    return true;
+}
+
+// block_slope_and_error / linear_slope, src/Swarm.cpp:136-197
+static bool block_slope_and_error(const double* x, size_t n, double dt, size_t blocks, double& slope, double& se) {
+    if (blocks == 0 || n % blocks != 0 || n / blocks < 2) return false;
+    const size_t bs = n / blocks;
+    std::vector<double> slopes(blocks);
+    for (size_t b = 0; b < blocks; ++b) {
+        const size_t begin = b * bs, count = bs;
+        const double mean_index = 0.5 * (double)(count - 1);
+        double cov = 0.0, iv = 0.0, mv = 0.0;
+        for (size_t i = begin; i < begin + count; ++i) mv += x[i];
+        mv /= (double)count;
+        for (size_t l = 0; l < count; ++l) {
+            const double ci = (double)l - mean_index;
+            cov += ci * (x[begin + l] - mv);
+            iv += ci * ci;
+        }
+        slopes[b] = cov / (iv * dt);
+    }
+    double m = 0.0;
+    for (double v : slopes) m += v;
+    m /= (double)blocks;
+    double e = 0.0;
+    if (blocks > 1) {
+        double sq = 0.0;
+        for (double v : slopes) sq += (v - m) * (v - m);
+        e = std::sqrt(sq / ((double)blocks * (double)(blocks - 1)));
+    }
+    slope = m;
+    se = e;
+    return true;
+}
+
+// effective_population_limit, src/Swarm.cpp:237-260
+static size_t population_limit(size_t particles, size_t requested) {
+    if (requested != 0) return requested;
+    if (particles >= kAllocationLimit) return particles;
+    const size_t source = kAllocationLimit - particles;
+    const size_t doubled = particles > source / 2 ? source : 2 * particles;
+    const size_t buffer = std::min<size_t>(source, 1024);
+    const size_t buffered = particles > source - buffer ? source : particles + 1024;
+    return std::min(source, std::max(doubled, buffered));
+}
+
+// First-fit allocator over one device block (offsets aligned to 256 bytes).
+struct Pool {
+    char* base = nullptr;
+    size_t size = 0;
+    std::map<size_t, size_t> free_;  // offset -> length
+
+    void init(char* b, size_t s) {
+        base = b;
+        size = s;
+        free_.clear();
+        free_[0] = s;
+    }
+    static size_t round(size_t x) { return (x + 255) & ~(size_t)255; }
+    char* alloc(size_t bytes) {
+        bytes = round(std::max<size_t>(bytes, 1));
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= bytes) {
+                const size_t off = it->first, len = it->second;
+                free_.erase(it);
+                if (len > bytes) free_[off + bytes] = len - bytes;
+                return base + off;
+            }
+        }
+        return nullptr;
+    }
+    void release(char* p, size_t bytes) {
+        bytes = round(std::max<size_t>(bytes, 1));
+        size_t off = (size_t)(p - base);
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && off + bytes == next->first) {
+            bytes += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                prev->second += bytes;
+                return;
+            }
+        }
+        free_[off] = bytes;
+    }
+};
+
+struct Request {
+    uint64_t id;
+    apic_swarm_request req;
+    double submitted;      // host clock, seconds
+};
+
+struct Run {
+    bool used = false;
+    uint64_t id = 0;
+    apic_swarm_request req{};
+    RunCfg cfg{};
+    std::vector<std::pair<char*, size_t>> blocks;
+    size_t last_check_step = 0;
+    std::vector<double> hv, he;  // host copies of the velocity and energy samples so far
+    double submitted = 0.0;
+    double admitted = 0.0;
+};
+
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Server {
+    apic_swarm_server_config conf{};
+    std::string last_error;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> allocations;
+    MccModelDev model{};
+    double neutral_density = 0.0, max_frequency = 0.0;
+    bool fp32 = false;
+    Pool pool;
+    size_t max_chunks = 0;
+    // device tables
+    RunCfg* d_cfg = nullptr;
+    RunState* d_st = nullptr;
+    uint32_t* d_chunk_run = nullptr;
+    uint32_t* d_chunk_first = nullptr;
+    uint32_t* d_nchunks = nullptr;
+    ChunkPartial* d_part = nullptr;
+    // host mirrors
+    std::vector<Run> runs;
+    std::vector<RunState> h_st;
+    std::vector<uint32_t> h_chunk_run, h_chunk_first;
+    std::deque<Request> queue;
+    std::map<uint64_t, apic_swarm_result> done;
+    uint64_t next_id = 1;
+    bool tables_dirty = true;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int push_grid = 0;
+    uint64_t launches = 0;
+    uint64_t particle_steps = 0;
+
+    ~Server() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void* a : allocations) cudaFree(a);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    Batch batch() const {
+        Batch b;
+        b.cfg = d_cfg;
+        b.st = d_st;
+        b.chunk_run = d_chunk_run;
+        b.chunk_first = d_chunk_first;
+        b.nchunks = d_nchunks;
+        b.part = d_part;
+        b.max_runs = conf.max_runs;
+        b.model = model;
+        return b;
+    }
+
+    void create(const apic_swarm_server_config& c, const apic_mcc_model& gas) {
+        conf = c;
+        require(c.max_runs >= 1 && c.max_runs <= 4096, "max_runs must be between 1 and 4096");
+        require(c.memory_budget_bytes >= (size_t)1 << 20, "memory_budget_bytes must be at least 1 MiB");
+        require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
+        require(c.steps_per_launch >= 1 && c.steps_per_launch <= 4096, "steps_per_launch must be between 1 and 4096");
+        fp32 = c.precision == APIC_FP32;
+        APIC_CUDA(cudaGetDevice(&device));
+        APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        // collision_config, src/Swarm.cpp:520-557: electrons on the dataset's channels
+        require(gas.nch >= 1, "swarm gas dataset has no collision channels");
+        bool has_elastic = false;
+        for (int i = 0; i < gas.nch && i < kMaxChannels; ++i) {
+            require(gas.ch[i].process != APIC_CHARGE_EXCHANGE,
+                    "electron swarm benchmark does not support charge-exchange channels");
+            require(gas.ch[i].energy_frame == APIC_FRAME_PROJECTILE,
+                    "electron swarm benchmark requires projectile-frame cross-section energy");
+            has_elastic = has_elastic || gas.ch[i].process == APIC_ELASTIC;
+        }
+        require(has_elastic, "electron swarm benchmark requires an elastic channel");
+        require(std::isfinite(gas.neutral_density) && gas.neutral_density > 0,
+                "swarm neutral_density must be positive and finite");
+        require(std::isfinite(gas.max_frequency) && gas.max_frequency > 0,
+                "swarm max_frequency must be positive and finite");
+        require(std::isfinite(gas.neutral_temperature) && gas.neutral_temperature >= 0,
+                "swarm neutral_temperature must be finite and non-negative");
+        apic_mcc_model m = gas;
+        m.species = 0;
+        m.gas_units_si = 1;
+        if (m.max_candidates == 0) m.max_candidates = 64;
+        DeviceArena arena{allocations, stream};
+        build_model(m, kElectronMass, arena, model);
+        neutral_density = m.neutral_density;
+        max_frequency = m.max_frequency;
+        char* pool_base = arena.alloc<char>(c.memory_budget_bytes);
+        pool.init(pool_base, c.memory_budget_bytes);
+        const size_t min_bytes = (fp32 ? 4 : 8) * 6 * (size_t)kChunk;
+        max_chunks = c.memory_budget_bytes / min_bytes + (size_t)c.max_runs + 1;
+        d_cfg = arena.alloc<RunCfg>(c.max_runs);
+        d_st = arena.alloc<RunState>(c.max_runs);
+        d_chunk_run = arena.alloc<uint32_t>(max_chunks);
+        d_chunk_first = arena.alloc<uint32_t>(max_chunks);
+        d_nchunks = arena.alloc<uint32_t>(1);
+        d_part = arena.alloc<ChunkPartial>(max_chunks);
+        runs.resize(c.max_runs);
+        h_st.resize(c.max_runs);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        push_grid = sms * 2;
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void validate(const apic_swarm_request& r) const {
+        auto pf = [](double x) { return std::isfinite(x) && x > 0.0; };
+        require(pf(r.timestep), "swarm timestep must be positive and finite");
+        require(max_frequency * r.timestep <= 0.1, "swarm max_frequency * timestep must not exceed 0.1");
+        require(r.steps > 0 && r.burn_in_steps < r.steps, "swarm steps must exceed burn_in_steps");
+        require(r.particles > 0, "swarm particles must be positive");
+        require(r.particles <= kAllocationLimit, "swarm particles exceeds the safety limit of 10000000");
+        require(r.steps <= 0xFFFFFF00u, "swarm steps out of range");
+        const size_t sampling = r.steps - r.burn_in_steps;
+        require(r.uncertainty_blocks >= 1 && r.uncertainty_blocks <= sampling,
+                "swarm uncertainty_blocks must be between 1 and the number of sampling steps");
+        require(sampling % r.uncertainty_blocks == 0, "swarm sampling steps must be divisible by uncertainty_blocks");
+        require(r.population_model == APIC_SWARM_FIXED || r.population_model == APIC_SWARM_BRANCHING,
+                "unknown swarm population_model");
+        bool has_ion = false, has_att = false;
+        for (int i = 0; i < model.nch; ++i) {
+            has_ion = has_ion || model.ch[i].process == kIonization;
+            has_att = has_att || model.ch[i].process == kAttachment;
+        }
+        if (r.population_model == APIC_SWARM_FIXED) {
+            require(r.population_limit == 0,
+                    "swarm population_limit is valid only for population_model = branching_resampled");
+            require(!has_att, "fixed-population swarm does not support attachment; use population_model = "
+                              "branching_resampled");
+        } else {
+            const size_t lim = population_limit(r.particles, r.population_limit);
+            require(lim > r.particles && lim <= kAllocationLimit - r.particles,
+                    "branching swarm population_limit must exceed particles and population_limit + particles must "
+                    "not exceed the allocation safety limit of 10000000");
+            require(sampling / r.uncertainty_blocks >= 2,
+                    "branching swarm requires at least two sampling steps per uncertainty block");
+            require(has_ion || has_att, "branching swarm requires an ionization or attachment channel");
+        }
+        require(std::isfinite(r.initial_mean_energy_ev) && r.initial_mean_energy_ev >= 0,
+                "swarm initial_mean_energy_ev must be finite and non-negative");
+        require(pf(r.max_energy_ev), "swarm max_energy_ev must be positive and finite");
+        for (int i = 0; i < model.nch; ++i) {  // src/Swarm.cpp:455-477
+            require(!(r.max_energy_ev > host_table_max_[i] / kEvToJ),
+                    "swarm max_energy_ev exceeds channel table coverage");
+            require(!(host_mu_max_[i] > 0.0 && r.max_energy_ev > host_mu_max_[i] / kEvToJ),
+                    "swarm max_energy_ev exceeds channel angular table coverage");
+        }
+        require(std::isfinite(r.reduced_field_td) && r.reduced_field_td >= 0,
+                "swarm reduced fields must be finite and non-negative");
+        require(std::isfinite(r.reduced_field_td * kTownsend * neutral_density),
+                "swarm reduced field and neutral density overflow the electric field");
+        require(std::isfinite(r.tolerance) && r.tolerance >= 0, "swarm tolerance must be finite and non-negative");
+    }
+    double host_table_max_[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double host_mu_max_[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+    size_t run_bytes(const apic_swarm_request& r) const {
+        const size_t es = fp32 ? 4 : 8;
+        const size_t n = r.particles;
+        const size_t nch = (n + kChunk - 1) / kChunk;
+        size_t bytes = Pool::round(6 * n * es) + Pool::round(3 * (r.steps - r.burn_in_steps) * sizeof(double));
+        if (r.population_model == APIC_SWARM_BRANCHING) {
+            const size_t lim = population_limit(n, r.population_limit);
+            bytes += Pool::round(6 * lim * es) + Pool::round(3 * nch * kChunk * es) +
+                     Pool::round(nch * kChunk * sizeof(uint32_t)) + Pool::round(n);
+        }
+        return bytes;
+    }
+
+    // Admits queued requests (first that fits, in arrival order) while slots,
+    // chunk-table room and pool memory allow.
+    int admit() {
+        int admitted = 0;
+        size_t used_chunks = h_chunk_run.size();
+        for (auto it = queue.begin(); it != queue.end();) {
+            int slot = -1;
+            for (int s = 0; s < conf.max_runs; ++s)
+                if (!runs[s].used) { slot = s; break; }
+            if (slot < 0) break;
+            const apic_swarm_request& r = it->req;
+            const size_t nch = (r.particles + kChunk - 1) / kChunk;
+            if (used_chunks + nch > max_chunks || run_bytes(r) > pool.size) { ++it; continue; }
+            if (!place(slot, *it)) { ++it; continue; }
+            used_chunks += nch;
+            it = queue.erase(it);
+            ++admitted;
+        }
+        return admitted;
+    }
+
+    bool place(int slot, const Request& q) {
+        const apic_swarm_request& r = q.req;
+        Run& run = runs[slot];
+        const size_t es = fp32 ? 4 : 8;
+        const size_t n = r.particles;
+        const size_t nch = (n + kChunk - 1) / kChunk;
+        const bool br = r.population_model == APIC_SWARM_BRANCHING;
+        const size_t lim = br ? population_limit(n, r.population_limit) : n;
+        std::vector<std::pair<char*, size_t>> blocks;
+        auto take = [&](size_t bytes) -> char* {
+            char* p = pool.alloc(bytes);
+            if (p) blocks.push_back({p, bytes});
+            return p;
+        };
+        char* a = take(6 * n * es);
+        char* smp = take(3 * (r.steps - r.burn_in_steps) * sizeof(double));
+        char *bb = nullptr, *sb = nullptr, *kb = nullptr, *al = nullptr;
+        if (br) {
+            bb = take(6 * lim * es);
+            sb = take(3 * nch * kChunk * es);
+            kb = take(nch * kChunk * sizeof(uint32_t));
+            al = take(n);
+        }
+        if (!a || !smp || (br && (!bb || !sb || !kb || !al))) {
+            for (auto& blk : blocks) pool.release(blk.first, blk.second);
+            return false;
+        }
+        RunCfg& C = run.cfg;
+        C = RunCfg{};
+        const double E = r.reduced_field_td * kTownsend * neutral_density;
+        const double acceleration = -kEvToJ * E / kElectronMass;
+        C.half_kick = 0.5 * acceleration * r.timestep;
+        C.dt = r.timestep;
+        C.max_energy_ev = r.max_energy_ev;
+        C.init_sd = std::sqrt(2.0 * r.initial_mean_energy_ev * kEvToJ / (3.0 * kElectronMass));
+        C.seed = r.seed;
+        C.n = (uint32_t)n;
+        C.steps = (uint32_t)r.steps;
+        C.burn_in = (uint32_t)r.burn_in_steps;
+        C.nchunks = (uint32_t)nch;
+        C.limit = (uint32_t)lim;
+        C.branching = br ? 1 : 0;
+        for (int k = 0; k < 3; ++k) {
+            C.v[k] = a + (size_t)k * n * es;
+            C.d[k] = a + (size_t)(3 + k) * n * es;
+            if (br) {
+                C.bv[k] = bb + (size_t)k * lim * es;
+                C.bd[k] = bb + (size_t)(3 + k) * lim * es;
+                C.sv[k] = sb + (size_t)k * nch * kChunk * es;
+            }
+        }
+        C.skey = reinterpret_cast<uint32_t*>(kb);
+        C.alive = reinterpret_cast<uint8_t*>(al);
+        C.samples = reinterpret_cast<double*>(smp);
+        run.used = true;
+        run.id = q.id;
+        run.req = r;
+        run.blocks = std::move(blocks);
+        run.last_check_step = 0;
+        run.submitted = q.submitted;
+        run.admitted = now_s();
+        RunState S{};
+        S.active = 1;
+        S.weight = 1.0;
+        h_st[slot] = S;
+        APIC_CUDA(cudaMemcpyAsync(d_st + slot, &h_st[slot], sizeof S, cudaMemcpyHostToDevice, stream));
+        if (fp32) k_swarm_init<float><<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, stream>>>(C);
+        else k_swarm_init<double><<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, stream>>>(C);
+        APIC_CUDA(cudaGetLastError());
+        tables_dirty = true;
+        return true;
+    }
+
+    void rebuild_tables() {
+        h_chunk_run.clear();
+        h_chunk_first.clear();
+        for (int s = 0; s < conf.max_runs; ++s) {
+            Run& r = runs[s];
+            if (!r.used) continue;
+            r.cfg.first_chunk = (uint32_t)h_chunk_run.size();
+            for (uint32_t k = 0; k < r.cfg.nchunks; ++k) {
+                h_chunk_run.push_back((uint32_t)s);
+                h_chunk_first.push_back(k * kChunk);
+            }
+            APIC_CUDA(cudaMemcpyAsync(d_cfg + s, &r.cfg, sizeof(RunCfg), cudaMemcpyHostToDevice, stream));
+        }
+        const uint32_t nc = (uint32_t)h_chunk_run.size();
+        if (nc) {
+            APIC_CUDA(cudaMemcpyAsync(d_chunk_run, h_chunk_run.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                      stream));
+            APIC_CUDA(cudaMemcpyAsync(d_chunk_first, h_chunk_first.data(), nc * sizeof(uint32_t),
+                                      cudaMemcpyHostToDevice, stream));
+        }
+        nchunks_host_ = nc;
+        APIC_CUDA(cudaMemcpyAsync(d_nchunks, &nchunks_host_, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        // the host copies above read pageable host memory: wait before it changes
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        tables_dirty = false;
+    }
+    uint32_t nchunks_host_ = 0;
+
+    template <class T>
+    void enqueue_step(const Batch& b) {
+        k_swarm_push<T><<<push_grid, kThreads, 0, stream>>>(b);
+        k_swarm_branch_scan<<<conf.max_runs, kThreads, 0, stream>>>(b);
+        k_swarm_branch_compact<T><<<push_grid, kThreads, 0, stream>>>(b);
+        k_swarm_branch_resample<T><<<push_grid, kThreads, 0, stream>>>(b);
+        k_swarm_reduce<<<conf.max_runs, kThreads, 0, stream>>>(b);
+    }
+
+    void ensure_graph() {
+        if (graph_exec) return;
+        const Batch b = batch();
+        APIC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        for (size_t k = 0; k < conf.steps_per_launch; ++k) {
+            if (fp32) enqueue_step<float>(b);
+            else enqueue_step<double>(b);
+        }
+        APIC_CUDA(cudaStreamEndCapture(stream, &graph));
+        APIC_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+    }
+
+    // Finishes a run whose device state says it stopped (steps done, converged
+    // or failed): statistics from its samples, diffusion from its displacements.
+    void retire(int slot, bool converged) {
+        Run& run = runs[slot];
+        RunState& S = h_st[slot];
+        const apic_swarm_request& r = run.req;
+        apic_swarm_result out{};
+        out.id = run.id;
+        out.reduced_field_td = r.reduced_field_td;
+        const double E = r.reduced_field_td * kTownsend * neutral_density;
+        out.electric_field_v_m = E;
+        out.steps_done = S.step;
+        out.converged = converged ? 1 : 0;
+        out.initial_weight = (double)r.particles;
+        out.diffusion_available = r.population_model == APIC_SWARM_FIXED;
+        out.nch = model.nch;
+        out.status = APIC_OK;
+        if (S.error) {
+            out.status = (S.error & (kErrMajorant)) ? APIC_ERR_MAJORANT
+                         : (S.error & kErrCandidates) ? APIC_ERR_CANDIDATES
+                         : (S.error & (kErrPopulation | kErrBirths)) ? APIC_ERR_CAPACITY
+                         : (S.error & kErrNonFinite) ? APIC_ERR_NONFINITE
+                                                     : APIC_ERR_INVALID;
+            std::string msg;
+            if (S.error & kErrMaxEnergyPre) msg += "swarm particle energy exceeded max_energy_ev before collision lookup; ";
+            if (S.error & kErrMaxEnergy) msg += "swarm particle energy exceeded max_energy_ev; ";
+            if (S.error & kErrMajorant) msg += "MCC total collision frequency exceeds configured max_frequency; ";
+            if (S.error & kErrCandidates) msg += "MCC candidate limit exceeded; ";
+            if (S.error & kErrPopulation) msg += "branching swarm exceeded population_limit before resampling; ";
+            if (S.error & kErrExtinct) msg += "branching swarm electron ensemble became extinct; ";
+            if (S.error & kErrBirths) msg += "ionization secondaries exceeded the per-chunk staging buffer; ";
+            if (S.error & kErrNonFinite) msg += "electron velocity became non-finite; ";
+            std::snprintf(out.message, sizeof out.message, "%s", msg.c_str());
+        }
+        const size_t steps_done = S.step;
+        const size_t ns = steps_done > r.burn_in_steps ? steps_done - r.burn_in_steps : 0;
+        const size_t total_ns = r.steps - r.burn_in_steps;
+        if (out.status == APIC_OK && ns > 0) {
+            std::vector<double> smp(3 * total_ns);
+            APIC_CUDA(cudaMemcpyAsync(smp.data(), run.cfg.samples, smp.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                      stream));
+            if (r.population_model == APIC_SWARM_FIXED) {
+                if (fp32) k_swarm_moments<float><<<1, kThreads, 0, stream>>>(run.cfg, d_st + slot);
+                else k_swarm_moments<double><<<1, kThreads, 0, stream>>>(run.cfg, d_st + slot);
+                APIC_CUDA(cudaGetLastError());
+            }
+            APIC_CUDA(cudaMemcpyAsync(&S, d_st + slot, sizeof S, cudaMemcpyDeviceToHost, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            const double* vs = smp.data();
+            const double* es = smp.data() + total_ns;
+            const double* ls = smp.data() + 2 * total_ns;
+            const size_t blocks = std::min(r.uncertainty_blocks, ns);
+            double m = 0, e = 0;
+            block_mean_and_error(vs, ns, blocks, m, e);
+            out.mean_velocity_x = m;
+            out.mean_velocity_x_se = e;
+            out.drift_velocity = -m;
+            out.reduced_mobility = E == 0.0 ? 0.0 : out.drift_velocity * neutral_density / E;
+            block_mean_and_error(es, ns, blocks, m, e);
+            out.mean_energy_ev = m;
+            out.mean_energy_se_ev = e;
+            const double sampling_time = (double)ns * r.timestep;
+            if (out.diffusion_available) {
+                out.diffusion_longitudinal = S.var_l / (2.0 * sampling_time);
+                out.diffusion_transverse = S.var_t / (4.0 * sampling_time);
+            }
+            for (int c = 0; c < model.nch; ++c) {
+                out.channel_collisions[c] = S.counts[c];
+                out.channel_rate[c] = S.wcoll[c] / S.exposure;
+                out.channel_rate_se[c] = std::sqrt(S.wcoll2[c]) / S.exposure;
+                if (model.ch[c].process == kIonization) {
+                    out.ionization_rate += out.channel_rate[c];
+                    out.ionization_rate_se = std::hypot(out.ionization_rate_se, out.channel_rate_se[c]);
+                } else if (model.ch[c].process == kAttachment) {
+                    out.attachment_rate += out.channel_rate[c];
+                    out.attachment_rate_se = std::hypot(out.attachment_rate_se, out.channel_rate_se[c]);
+                }
+            }
+            out.net_rate = out.ionization_rate - out.attachment_rate;
+            out.net_rate_se = std::hypot(out.ionization_rate_se, out.attachment_rate_se);
+            out.final_weight = (double)r.particles * S.weight;
+            out.final_particles = r.particles;
+            if (r.population_model == APIC_SWARM_BRANCHING) {
+                double g = 0, ge = 0;
+                if (block_slope_and_error(ls, ns, r.timestep, blocks, g, ge)) {
+                    out.growth_rate = g;
+                    out.growth_rate_se = ge;
+                    if (out.drift_velocity > 0.0) {
+                        const double drift = out.drift_velocity, de = out.mean_velocity_x_se;
+                        out.townsend_available = 1;
+                        out.townsend_growth = g / drift;
+                        out.townsend_growth_se = std::hypot(ge / drift, g * de / (drift * drift));
+                        out.townsend_rate = out.net_rate / drift;
+                        out.townsend_rate_se =
+                            std::hypot(out.net_rate_se / drift, out.net_rate * de / (drift * drift));
+                    }
+                }
+            }
+            out.candidates = S.candidates;
+            out.null_collisions = S.nulls;
+        }
+        out.max_observed_energy_ev = S.max_ev;
+        const double t = now_s();
+        out.latency_s = t - run.submitted;
+        out.queue_s = run.admitted - run.submitted;
+        done[run.id] = out;
+        for (auto& blk : run.blocks) pool.release(blk.first, blk.second);
+        run = Run{};
+        RunState off{};
+        h_st[slot] = off;
+        APIC_CUDA(cudaMemcpyAsync(d_st + slot, &h_st[slot], sizeof(RunState), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        tables_dirty = true;
+    }
+
+    // Convergence: the relative block standard errors of drift velocity and
+    // mean energy over the samples so far at most `tolerance`.
+    bool converged(int slot) {
+        const Run& run = runs[slot];
+        const apic_swarm_request& r = run.req;
+        if (!(r.tolerance > 0.0)) return false;
+        const size_t step = h_st[slot].step;
+        if (step <= r.burn_in_steps) return false;
+        const size_t ns = step - r.burn_in_steps;
+        if (ns < 4 * r.uncertainty_blocks) return false;
+        const size_t total_ns = r.steps - r.burn_in_steps;
+        Run& rw = runs[slot];
+        const size_t have = rw.hv.size();
+        rw.hv.resize(ns);
+        rw.he.resize(ns);
+        APIC_CUDA(cudaMemcpyAsync(rw.hv.data() + have, run.cfg.samples + have, (ns - have) * sizeof(double),
+                                  cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaMemcpyAsync(rw.he.data() + have, run.cfg.samples + total_ns + have,
+                                  (ns - have) * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        double mv, sv, me, se;
+        block_mean_and_error(rw.hv.data(), ns, r.uncertainty_blocks, mv, sv);
+        block_mean_and_error(rw.he.data(), ns, r.uncertainty_blocks, me, se);
+        return sv <= r.tolerance * std::fabs(mv) && se <= r.tolerance * std::fabs(me);
+    }
+
+    // One serving iteration: admit, run steps_per_launch steps of every active
+    // run (one graph launch), read the run states, retire finished runs.
+    void advance(int* active_out, int* queued_out) {
+        admit();
+        if (tables_dirty) rebuild_tables();
+        int active = 0;
+        for (int s = 0; s < conf.max_runs; ++s) active += runs[s].used ? 1 : 0;
+        if (active) {
+            ensure_graph();
+            APIC_CUDA(cudaGraphLaunch(graph_exec, stream));
+            ++launches;
+            APIC_CUDA(cudaMemcpyAsync(h_st.data(), d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
+                                      stream));
+            const cudaError_t w = bounded_wait(stream, 600.0);
+            if (w == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "swarm step did not complete in time");
+            APIC_CUDA(w);
+            for (int s = 0; s < conf.max_runs; ++s) {
+                Run& run = runs[s];
+                if (!run.used) continue;
+                const size_t advanced = h_st[s].step - run.last_check_step;
+                particle_steps += advanced * run.req.particles;
+                run.last_check_step = h_st[s].step;
+                if (!h_st[s].active) {
+                    retire(s, false);
+                } else if (converged(s)) {
+                    retire(s, true);
+                }
+            }
+        }
+        active = 0;
+        for (int s = 0; s < conf.max_runs; ++s) active += runs[s].used ? 1 : 0;
+        if (active_out) *active_out = active;
+        if (queued_out) *queued_out = (int)queue.size();
+    }
+
+    uint64_t submit(const apic_swarm_request& r) {
+        validate(r);
+        require(run_bytes(r) <= pool.size, "swarm request does not fit the server's memory budget", APIC_ERR_CAPACITY);
+        require((r.particles + kChunk - 1) / kChunk + 1 <= max_chunks, "swarm request exceeds the chunk table",
+                APIC_ERR_CAPACITY);
+        Request q;
+        q.id = next_id++;
+        q.req = r;
+        q.submitted = now_s();
+        queue.push_back(q);
+        return q.id;
+    }
+};
+
+}  // namespace swarm
+}  // namespace apic
+
+struct apic_swarm_server {
+    apic::swarm::Server impl;
+};
+
+namespace {
+thread_local std::string g_swarm_error;
+
+template <class F>
+int guarded_swarm(apic_swarm_server* h, F&& f) {
+    try {
+        f();
+        return APIC_OK;
+    } catch (const apic::Error& e) {
+        (h ? h->impl.last_error : g_swarm_error) = e.what();
+        return e.status;
+    } catch (const std::exception& e) {
+        (h ? h->impl.last_error : g_swarm_error) = e.what();
+        return APIC_ERR_INVALID;
+    }
+}
+}  // namespace
+
+extern "C" {
+
+int apic_swarm_server_create(const apic_swarm_server_config* cfg, const apic_mcc_model* gas,
+                             apic_swarm_server** out) {
+    if (!cfg || !gas || !out) {
+        g_swarm_error = "null argument";
+        return APIC_ERR_INVALID;
+    }
+    *out = nullptr;
+    auto h = std::make_unique<apic_swarm_server>();
+    const int rc = guarded_swarm(h.get(), [&] {
+        h->impl.create(*cfg, *gas);
+        for (int i = 0; i < gas->nch && i < apic::kMaxChannels; ++i) {
+            h->impl.host_table_max_[i] = gas->ch[i].energy[gas->ch[i].rows - 1];
+            if (gas->ch[i].angular == APIC_HENYEY_GREENSTEIN)
+                h->impl.host_mu_max_[i] = gas->ch[i].mean_cosine_energy[gas->ch[i].mean_cosine_rows - 1];
+        }
+    });
+    if (rc != APIC_OK) {
+        g_swarm_error = h->impl.last_error;
+        return rc;
+    }
+    *out = h.release();
+    return APIC_OK;
+}
+
+void apic_swarm_server_destroy(apic_swarm_server* srv) { delete srv; }
+
+const char* apic_swarm_last_error(const apic_swarm_server* srv) {
+    return srv ? srv->impl.last_error.c_str() : g_swarm_error.c_str();
+}
+
+int apic_swarm_server_submit(apic_swarm_server* srv, const apic_swarm_request* req, uint64_t* id) {
+    if (!srv || !req || !id) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] { *id = srv->impl.submit(*req); });
+}
+
+int apic_swarm_server_advance(apic_swarm_server* srv, int* active, int* queued) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] { srv->impl.advance(active, queued); });
+}
+
+int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic_swarm_result* out, int* done) {
+    if (!srv || !out || !done) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] {
+        auto it = srv->impl.done.find(id);
+        *done = it != srv->impl.done.end() ? 1 : 0;
+        if (*done) {
+            *out = it->second;
+            srv->impl.done.erase(it);
+        }
+    });
+}
+
+int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,
+                            size_t* pool_bytes_free) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] {
+        if (graph_launches) *graph_launches = srv->impl.launches;
+        if (particle_steps) *particle_steps = srv->impl.particle_steps;
+        if (pool_bytes_free) {
+            size_t f = 0;
+            for (auto& kv : srv->impl.pool.free_) f += kv.second;
+            *pool_bytes_free = f;
+        }
+    });
+}
+
+int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream) {
+    if (!srv || !stream) return APIC_ERR_INVALID;
+    *stream = srv->impl.stream;
+    return APIC_OK;
+}
+
+int apic_swarm_run(const apic_swarm_config* cfg, const apic_mcc_model* gas, const double* fields_td, size_t nfields,
+                   apic_swarm_result* results) {
+    if (!cfg || !gas || !fields_td || !results || nfields == 0) {
+        g_swarm_error = "null argument";
+        return APIC_ERR_INVALID;
+    }
+    return guarded_swarm(nullptr, [&] {
+        for (size_t a = 0; a < nfields; ++a)
+            for (size_t b = a + 1; b < nfields; ++b)
+                apic::require(fields_td[a] != fields_td[b], "swarm reduced fields must not contain duplicates");
+        const uint64_t limit = cfg->work_item_limit ? cfg->work_item_limit : 100000000ull;
+        auto over = [](uint64_t a, uint64_t b, uint64_t lim) { return a != 0 && b > lim / a; };
+        apic::require(!over(nfields, cfg->particles, limit) && !over(nfields * cfg->particles, cfg->steps, limit),
+                      "swarm scan exceeds work_item_limit; raise it explicitly only on an appropriate compute host");
+        apic_mcc_model m = *gas;
+        m.neutral_density = cfg->neutral_density;
+        m.neutral_temperature = cfg->neutral_temperature;
+        m.max_frequency = cfg->max_frequency;
+        apic_swarm_request r{};
+        r.particles = cfg->particles;
+        r.steps = cfg->steps;
+        r.burn_in_steps = cfg->burn_in_steps;
+        r.uncertainty_blocks = cfg->uncertainty_blocks;
+        r.population_model = cfg->population_model;
+        r.population_limit = cfg->population_limit;
+        r.initial_mean_energy_ev = cfg->initial_mean_energy_ev;
+        r.max_energy_ev = cfg->max_energy_ev;
+        r.timestep = cfg->timestep;
+        r.tolerance = 0.0;
+        apic_swarm_server_config sc{};
+        sc.max_runs = (int)nfields;
+        sc.precision = cfg->precision;
+        sc.steps_per_launch = std::min<size_t>(cfg->steps, 64);
+        // every field resident at once
+        apic::swarm::Server probe;
+        probe.fp32 = cfg->precision == APIC_FP32;
+        size_t bytes = 0;
+        for (size_t f = 0; f < nfields; ++f) bytes += probe.run_bytes(r) + 4096;
+        sc.memory_budget_bytes = std::max<size_t>(bytes, (size_t)1 << 20);
+        apic_swarm_server* srv = nullptr;
+        int rc = apic_swarm_server_create(&sc, &m, &srv);
+        if (rc != APIC_OK) throw apic::Error(rc, g_swarm_error);
+        std::unique_ptr<apic_swarm_server> hold(srv);
+        std::vector<uint64_t> ids(nfields);
+        for (size_t f = 0; f < nfields; ++f) {
+            r.reduced_field_td = fields_td[f];
+            r.seed = cfg->seed + f;  // src/Swarm.cpp:1513-1515
+            ids[f] = srv->impl.submit(r);
+        }
+        int active = 1, queued = 1;
+        while (active || queued) srv->impl.advance(&active, &queued);
+        for (size_t f = 0; f < nfields; ++f) {
+            auto it = srv->impl.done.find(ids[f]);
+            apic::require(it != srv->impl.done.end(), "swarm run did not finish");
+            results[f] = it->second;
+        }
+        for (size_t f = 0; f < nfields; ++f)
+            if (results[f].status != APIC_OK) throw apic::Error(results[f].status, results[f].message);
+    });
+}
+
+}  // extern "C"

@@ -68,9 +68,8 @@ typedef enum {
     APIC_ATTACHMENT = 3,
     APIC_CHARGE_EXCHANGE = 4
 } apic_process;
-/* AngularScatteringKind, include/pic/Config.hpp:33-37 (Henyey-Greenstein is
- * not supported by this build and is rejected with APIC_ERR_UNSUPPORTED). */
-typedef enum { APIC_ISOTROPIC = 0, APIC_BACKWARD = 1 } apic_angular;
+/* AngularScatteringKind, include/pic/Config.hpp:33-37 */
+typedef enum { APIC_ISOTROPIC = 0, APIC_BACKWARD = 1, APIC_HENYEY_GREENSTEIN = 2 } apic_angular;
 /* CollisionEnergyFrame, include/pic/Config.hpp:38-41 */
 typedef enum { APIC_FRAME_PROJECTILE = 0, APIC_FRAME_CENTER_OF_MASS = 1 } apic_frame;
 
@@ -87,6 +86,12 @@ typedef struct {
     size_t rows;
     const double* energy;
     const double* sigma;
+    /* Henyey-Greenstein only: MeanCosineTable (include/pic/Collision.hpp:33-48),
+     * energies already multiplied by mean_cosine_energy_scale, strictly
+     * increasing, covering the cross-section table; mean cosines in (-1, 1). */
+    size_t mean_cosine_rows;
+    const double* mean_cosine_energy;
+    const double* mean_cosine;
 } apic_mcc_channel;
 
 /* CollisionConfig (null_collision), include/pic/Config.hpp:110-132 */
@@ -369,6 +374,111 @@ APIC_EXPORT int apic_field_solve_periodic_nd(int dims, const size_t* n, const do
 APIC_EXPORT int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, const double* length,
                                                      double permittivity, const double* d_rho, double* d_phi,
                                                      double* d_electric, void* stream);
+
+/* ======================================================================
+ * Homogeneous electron swarms (src/Swarm.cpp)
+ * ====================================================================== */
+
+/* SwarmPopulationModel, include/pic/Swarm.hpp:14-17 */
+typedef enum { APIC_SWARM_FIXED = 0, APIC_SWARM_BRANCHING = 1 } apic_swarm_population;
+
+/* SwarmBenchmarkConfig, include/pic/Swarm.hpp:29-59, minus the file and
+ * spatial-Townsend controls.  The gas dataset arrives as an apic_mcc_model
+ * (channels with tables in joules / m^2, neutral_mass); its density,
+ * temperature and max_frequency are taken from this struct. */
+typedef struct {
+    double neutral_density, neutral_temperature, max_frequency, timestep;
+    size_t steps, burn_in_steps, particles;
+    int population_model;          /* apic_swarm_population */
+    size_t population_limit;       /* 0: the reference's default (src/Swarm.cpp:237-260) */
+    size_t uncertainty_blocks;
+    uint64_t work_item_limit;      /* 0: 100000000 */
+    double initial_mean_energy_ev, max_energy_ev;
+    uint64_t seed;
+    int precision;                 /* electron storage: APIC_FP64 or APIC_FP32 */
+} apic_swarm_config;
+
+/* SwarmBenchmarkResult, include/pic/Swarm.hpp:73-115, minus the spatial
+ * Townsend fields, plus the serving bookkeeping (id .. queue_s). */
+typedef struct {
+    uint64_t id;
+    int status;                    /* APIC_OK or the run's error */
+    char message[256];
+    uint64_t steps_done;
+    int converged;                 /* stopped by the tolerance test */
+    double latency_s, queue_s;     /* submit -> result, submit -> admission */
+    double reduced_field_td, electric_field_v_m;
+    double mean_velocity_x, mean_velocity_x_se, drift_velocity, reduced_mobility;
+    double mean_energy_ev, mean_energy_se_ev;
+    int diffusion_available;
+    double diffusion_longitudinal, diffusion_transverse;
+    double max_observed_energy_ev;
+    double initial_weight, final_weight;
+    uint64_t final_particles;
+    double growth_rate, growth_rate_se;
+    double ionization_rate, ionization_rate_se, attachment_rate, attachment_rate_se;
+    double net_rate, net_rate_se;
+    int townsend_available;
+    double townsend_growth, townsend_growth_se, townsend_rate, townsend_rate_se;
+    uint64_t candidates, null_collisions;
+    int nch;
+    uint64_t channel_collisions[APIC_MAX_CHANNELS];
+    double channel_rate[APIC_MAX_CHANNELS], channel_rate_se[APIC_MAX_CHANNELS];
+} apic_swarm_result;
+
+/* run_swarm_benchmark (src/Swarm.cpp:1503-1524) without the spatial Townsend
+ * pass: every reduced field runs as one device run (seed cfg->seed + f), all of
+ * them at once; results[f] receives field f.  Same validation and messages as
+ * validate_config (src/Swarm.cpp:262-518). */
+APIC_EXPORT int apic_swarm_run(const apic_swarm_config* cfg, const apic_mcc_model* gas, const double* fields_td,
+                               size_t nfields, apic_swarm_result* results);
+
+/* Serving: a persistent batch of swarm runs on one GPU.  No reference
+ * counterpart (the reference runs fields one after another): requests are
+ * admitted while run slots and the device memory budget allow, every active
+ * run advances steps_per_launch steps per apic_swarm_server_advance (one CUDA
+ * graph launch for the whole batch), and runs retire when their steps are done
+ * or their drift velocity and mean energy have converged. */
+typedef struct apic_swarm_server apic_swarm_server;
+/* Message of the last failed call on srv, or of the last failed call without
+ * a server (srv NULL: apic_swarm_run, apic_swarm_server_create). */
+APIC_EXPORT const char* apic_swarm_last_error(const apic_swarm_server* srv);
+typedef struct {
+    size_t memory_budget_bytes;    /* device pool for electron state and samples */
+    int max_runs;                  /* concurrent run slots */
+    int precision;                 /* APIC_FP64 or APIC_FP32 */
+    size_t steps_per_launch;       /* steps per advance (graph length) */
+} apic_swarm_server_config;
+
+/* One run_field request on the server's gas. */
+typedef struct {
+    double reduced_field_td;
+    size_t particles;
+    uint64_t seed;
+    size_t steps;                  /* at most this many steps */
+    size_t burn_in_steps;
+    size_t uncertainty_blocks;
+    double tolerance;              /* > 0: stop once the relative block standard errors of drift
+                                      velocity and mean energy are <= tolerance (checked after each
+                                      advance, at least 4 samples per block) */
+    int population_model;
+    size_t population_limit;
+    double initial_mean_energy_ev, max_energy_ev, timestep;
+} apic_swarm_request;
+
+/* gas: channels, neutral_density, neutral_temperature, max_frequency and
+ * neutral_mass of every run on this server. */
+APIC_EXPORT int apic_swarm_server_create(const apic_swarm_server_config* cfg, const apic_mcc_model* gas,
+                                         apic_swarm_server** out);
+APIC_EXPORT void apic_swarm_server_destroy(apic_swarm_server* srv);
+APIC_EXPORT int apic_swarm_server_submit(apic_swarm_server* srv, const apic_swarm_request* req, uint64_t* id);
+/* Admit, step every active run, retire finished runs; waits for the device. */
+APIC_EXPORT int apic_swarm_server_advance(apic_swarm_server* srv, int* active, int* queued);
+/* done = 1 and *out filled (once) when request id has finished. */
+APIC_EXPORT int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic_swarm_result* out, int* done);
+APIC_EXPORT int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,
+                                        size_t* pool_bytes_free);
+APIC_EXPORT int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream);
 
 #ifdef __cplusplus
 }

@@ -52,3 +52,27 @@ SWARM_KEYS = ("mean_velocity_x", "mean_velocity_x_se", "drift_velocity", "reduce
               "final_weight", "final_particles", "growth_rate", "growth_rate_se", "ionization_rate",
               "ionization_rate_se", "attachment_rate", "attachment_rate_se", "net_rate", "townsend_growth",
               "townsend_rate", "candidates", "null_collisions")
+
+
+ENSEMBLE_SEEDS = 12
+
+
+def swarm_ensemble_cases():
+    """Decks whose seed ensembles (ENSEMBLE_SEEDS reference runs each, in
+    tests/golden/swarm_ensemble_*.npz) pin the device statistically: the
+    anisotropic gas at 1e24 m^-3 relaxes within the burn-in, and ensemble
+    averages over independent seeds carry honest standard errors (block errors
+    of one branching run understate the step-to-step correlation that
+    resampling creates)."""
+    out = {}
+    for name, att in (("ens_fixed", False), ("ens_branching", True)):
+        ch, mn = W.swarm_gas_anisotropic(attachment=att)
+        ng, T = 1e24, 300.0
+        nu = W.swarm_max_frequency(ch, ng, mn, T, 199.0)
+        out[name] = W.SwarmSpec(name, ch, mn, ng, T, nu, 0.08 / nu, 600, 300, 2000, [50.0, 250.0],
+                                branching=att, uncertainty_blocks=10, initial_mean_energy_ev=2.0,
+                                max_energy_ev=199.0, seed=1000)
+    return out
+
+
+ENSEMBLE_KEYS = ("mean_velocity_x", "mean_energy_ev", "ionization_rate", "attachment_rate")

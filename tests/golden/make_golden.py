@@ -193,7 +193,24 @@ def swarm_fixture():
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
+def swarm_ensemble_fixture():
+    """run_swarm_benchmark over ENSEMBLE_SEEDS seeds of each ensemble deck."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from common import ENSEMBLE_KEYS, ENSEMBLE_SEEDS, swarm_ensemble_cases
+    for name, spec in swarm_ensemble_cases().items():
+        T = po.TableSet()
+        cfg, gas = po.swarm_from_spec(spec, T)
+        rows = []
+        for k in range(ENSEMBLE_SEEDS):
+            cfg.seed = spec.seed + 100 * k
+            rows.append(po.ref_swarm_run(cfg, gas, spec.fields_td, tempfile.mkdtemp()))
+        out = {key: np.array([[getattr(r, key) for r in row] for row in rows]) for key in ENSEMBLE_KEYS}
+        out["fields_td"] = np.array(spec.fields_td)
+        np.savez_compressed(os.path.join(HERE, f"swarm_ensemble_{name}.npz"), **out)
+
+
 def main():
+    swarm_ensemble_fixture()
     swarm_fixture()
     collide_hg_fixture()
     for name in ND_CASES:

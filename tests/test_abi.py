@@ -58,3 +58,31 @@ def test_workload_shapes():
     ts = W.two_stream()
     assert ts.nx == 256 and sum(len(s.x) for s in ts.species) == 32768
     assert np.all((ts.species[0].x >= 0) & (ts.species[0].x < ts.length))
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """Every struct the Python binding passes across the ABI has the C size."""
+    names = {"apic_mcc_channel": apic.McChannel, "apic_mcc_model": apic.MccModel, "apic_config1d": apic.Config1D,
+             "apic_config_nd": apic.ConfigND, "apic_sample_nd": apic.SampleND,
+             "apic_swarm_config": apic.SwarmConfig, "apic_swarm_result": apic.SwarmResult,
+             "apic_swarm_request": apic.SwarmRequest, "apic_swarm_server_config": apic.SwarmServerConfig}
+    src = tmp_path / "sizes.c"
+    body = "".join(f'    printf("{n} %zu\\n", sizeof({n}));\n' for n in names)
+    src.write_text('#include <stdio.h>\n#include "aurorapic_b200.h"\nint main(void) {\n' + body + "    return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    import subprocess
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    got = dict(zip(out[0::2], map(int, out[1::2])))
+    for n, cls in names.items():
+        assert got[n] == C.sizeof(cls), (n, got[n], C.sizeof(cls))
+
+
+def test_swarm_request_validation_on_cpu():
+    """Server creation needs a device; its absence is reported, never hidden."""
+    spec = W.swarm_c5(particles=1000, steps=100, burn_in_steps=50)
+    cfg, gas, tabs = W.to_device_swarm(spec)
+    if apic.lib().apic_device_count() > 0:
+        pytest.skip("checks the no-device path")
+    with pytest.raises(apic.ApicError):
+        apic.swarm_run(cfg, gas, [10.0])
