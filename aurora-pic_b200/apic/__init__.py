@@ -621,6 +621,9 @@ def _bind_swarm():
     L.apic_swarm_server_poll.argtypes = [P, C.c_uint64, C.POINTER(SwarmResult), C.POINTER(C.c_int)]
     L.apic_swarm_server_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)]
     L.apic_swarm_server_cuda_stream.argtypes = [P, C.POINTER(P)]
+    L.apic_swarm_server_set_kernel_timing.argtypes = [P, C.c_int]
+    L.apic_swarm_server_kernel_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                 C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
     L._swarm_bound = True
     return L
 
@@ -685,3 +688,13 @@ class SwarmServer:
         s = C.c_void_p()
         _check_swarm(_bind_swarm().apic_swarm_server_cuda_stream(self.h, C.byref(s)), self.h)
         return s.value or 0
+
+    def set_kernel_timing(self, enable: bool):
+        _check_swarm(_bind_swarm().apic_swarm_server_set_kernel_timing(self.h, int(enable)), self.h)
+
+    def kernel_times(self):
+        """(push ms, collision ms, steps timed, push algorithmic bytes) since timing was enabled."""
+        ms, cms, n, b = C.c_double(), C.c_double(), C.c_uint64(), C.c_double()
+        _check_swarm(_bind_swarm().apic_swarm_server_kernel_times(self.h, C.byref(ms), C.byref(cms), C.byref(n),
+                                                                  C.byref(b)), self.h)
+        return ms.value, cms.value, n.value, b.value

@@ -58,8 +58,15 @@ struct MccModelDev {
     double particle_mass, neutral_mass, neutral_density, max_frequency, neutral_stddev;
     double com_mass;      // particle_mass * neutral_mass / (particle_mass + neutral_mass)
     double v_safe;        // |v| <= v_safe passes the frequency-bound check without evaluation
+    double v_safe2;       // |v|^2 <= v_safe2 implies |v| <= v_safe (negative: always evaluate)
     unsigned max_candidates;
     int shared_grid;      // every channel uses the same energy rows and the projectile frame
+    // speed bins of width 1 / safe_inv_dv whose every speed provably passes the
+    // frequency-bound check (1) or may not (0); speeds past the last bin take
+    // the exact check
+    const unsigned char* safe_bins;
+    int nsafe;
+    double safe_inv_dv;
     MccChannelDev ch[kMaxChannels];
 };
 
@@ -143,8 +150,19 @@ __device__ inline bool rates_for_speed(const MccModelDev& m, double speed, doubl
 
 // validate_frequency_bound, src/Collision.cpp:627-685 (exact form, run only
 // above the precomputed safe speed).
-__device__ inline bool frequency_bound_ok(const MccModelDev& m, double speed) {
+static __device__ __noinline__ bool frequency_bound_exact(const MccModelDev& m, double speed);
+
+__device__ __forceinline__ bool frequency_bound_ok(const MccModelDev& m, double speed) {
     if (speed <= m.v_safe) return true;
+    if (m.safe_bins) {
+        const double f = speed * m.safe_inv_dv;
+        if (f < (double)m.nsafe && __ldg(m.safe_bins + (int)f)) return true;
+    }
+    return frequency_bound_exact(m, speed);
+}
+
+// validate_frequency_bound, src/Collision.cpp:627-685, evaluated
+static __device__ __noinline__ bool frequency_bound_exact(const MccModelDev& m, double speed) {
     double rates[kMaxChannels];
     if (m.neutral_stddev == 0.0) return rates_for_speed(m, speed, rates);
     const double limit = kThermalSigma * m.neutral_stddev;

@@ -140,6 +140,79 @@ inline TableIndex build_index(const double* e, size_t rows, DeviceArena& arena) 
     return ix;
 }
 
+// Range maxima of a table column in O(1) after an O(n log n) build.
+struct SparseMax {
+    std::vector<std::vector<double>> t;
+    explicit SparseMax(const double* x, size_t n) {
+        t.push_back(std::vector<double>(x, x + n));
+        for (size_t w = 1; 2 * w <= n; w *= 2) {
+            const auto& p = t.back();
+            std::vector<double> q(n - 2 * w + 1);
+            for (size_t i = 0; i < q.size(); ++i) q[i] = std::max(p[i], p[i + w]);
+            t.push_back(std::move(q));
+        }
+    }
+    double max(size_t a, size_t b) const {  // [a, b), a < b
+        int k = 0;
+        while (((size_t)2 << k) <= b - a) ++k;
+        return std::max(t[k][a], t[k][b - ((size_t)1 << k)]);
+    }
+};
+
+// Speed bins whose every speed passes the frequency-bound check.  For a bin
+// [v_a, v_b] the check's value at any speed inside is at most
+// n (v_b + 8 sigma) sum_c max{ sigma_c(E) : E(v_a - 8 sigma) <= E <= E(v_b + 8 sigma) }
+// (without thermal neutrals: n v_b sum_c max over [E(v_a), E(v_b)]); the
+// cross sections are piecewise linear, so that maximum is attained at a table
+// row or at an end of the window.  Bins are marked safe when this bound stays
+// below max_frequency (1 - 1e-9).
+inline void build_safe_bins(const apic_mcc_model& m, double mass, double sd, DeviceArena& arena, MccModelDev& D) {
+    const double com = m.neutral_mass > 0 ? mass * m.neutral_mass / (mass + m.neutral_mass) : 0.0;
+    double vtop = 0.0;  // speed of the highest table energy, over channels
+    for (int i = 0; i < m.nch; ++i) {
+        const auto& c = m.ch[i];
+        const double ms = c.energy_frame == APIC_FRAME_CENTER_OF_MASS ? com : mass;
+        vtop = std::max(vtop, std::sqrt(2.0 * c.energy[c.rows - 1] / ms));
+    }
+    const int nbins = 16384;
+    const double limit = kThermalSigma * sd;
+    if (!(vtop > 0.0) || !std::isfinite(vtop)) return;
+    const double dv = vtop / nbins;
+    std::vector<SparseMax> rm;
+    for (int i = 0; i < m.nch; ++i) rm.emplace_back(m.ch[i].sigma, m.ch[i].rows);
+    auto sigma_at = [](const apic_mcc_channel& c, double e) {
+        if (e <= c.energy[0]) return c.sigma[0];
+        if (e >= c.energy[c.rows - 1]) return c.sigma[c.rows - 1];
+        const double* up = std::upper_bound(c.energy, c.energy + c.rows, e);
+        const size_t hi = (size_t)(up - c.energy), lo = hi - 1;
+        const double f = (e - c.energy[lo]) / (c.energy[hi] - c.energy[lo]);
+        return c.sigma[lo] + f * (c.sigma[hi] - c.sigma[lo]);
+    };
+    const double target = m.max_frequency * (1.0 - 1e-9);
+    std::vector<unsigned char> safe(nbins, 0);
+    for (int b = 0; b < nbins; ++b) {
+        const double va = dv * b, vb = dv * (b + 1) * (1.0 + 1e-12);
+        const double lo_v = std::max(va - limit, 0.0), hi_v = vb + limit;
+        double bound = 0.0;
+        for (int i = 0; i < m.nch; ++i) {
+            const auto& c = m.ch[i];
+            const double ms = c.energy_frame == APIC_FRAME_CENTER_OF_MASS ? com : mass;
+            const double e_hi = 0.5 * ms * hi_v * hi_v;
+            if (e_hi < c.threshold_energy) continue;
+            const double e_lo = std::max(0.5 * ms * lo_v * lo_v, c.threshold_energy);
+            double smax = std::max(sigma_at(c, e_lo), sigma_at(c, e_hi));
+            const size_t k0 = (size_t)(std::lower_bound(c.energy, c.energy + c.rows, e_lo) - c.energy);
+            const size_t k1 = (size_t)(std::upper_bound(c.energy, c.energy + c.rows, e_hi) - c.energy);
+            if (k0 < k1) smax = std::max(smax, rm[i].max(k0, k1));
+            bound += m.neutral_density * smax * hi_v;
+        }
+        safe[b] = bound * (1.0 + 1e-9) <= target ? 1 : 0;
+    }
+    D.safe_bins = arena.upload(safe.data(), safe.size());
+    D.nsafe = nbins;
+    D.safe_inv_dv = 1.0 / dv;
+}
+
 // Validates one model (the checks that do not depend on the caller's species
 // layout) and fills D with device copies of its tables.  The host tables may be
 // released when this returns.
@@ -228,6 +301,8 @@ inline void build_model(const apic_mcc_model& m, double mass, DeviceArena& arena
             D.shared_grid = 0;
     }
     D.v_safe = safe_speed(m, mass, sd);
+    D.v_safe2 = D.v_safe < 0.0 ? -1.0 : std::nextafter(D.v_safe * D.v_safe, 0.0);
+    build_safe_bins(m, mass, sd, arena, D);
     APIC_CUDA(cudaStreamSynchronize(arena.stream));  // host tables may be freed after this
 }
 

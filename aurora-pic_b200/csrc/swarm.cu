@@ -49,7 +49,6 @@ namespace swarm {
 constexpr int kThreads = 256;
 constexpr int kChunk = 1024;
 constexpr int kItems = kChunk / kThreads;
-constexpr int kQueue = 384;                 // collision candidates buffered per chunk
 constexpr int kMaxBirthsPerElectron = 8;
 constexpr double kElectronMass = 9.1093837139e-31;  // src/Swarm.cpp:23
 constexpr double kEvToJ = 1.602176634e-19;          // src/Swarm.cpp:24-25
@@ -65,6 +64,16 @@ enum : unsigned {
 
 struct RunCfg {  // written by the host at admission, read-only on the device
     double half_kick, dt, max_energy_ev, init_sd;
+    double vscale, escale;  // fixed-point scales (powers of two) of the v_x and |v|^2 sums
+    // kinetic_energy_ev(v) > max_energy_ev exactly when |v|^2 > s2_max (the
+    // energy is a monotone function of |v|^2 in floating point)
+    double s2_max;
+    // -log(u) / max_frequency < dt exactly when the first 64-bit draw is at
+    // least cand_draw_min (u = draw / 2^64; a zero draw is redrawn and takes
+    // the evaluated path); no_candidates when no draw qualifies
+    uint64_t cand_draw_min;
+    int no_candidates;
+    int pad0;
     uint64_t seed;
     uint32_t n, steps, burn_in, first_chunk, nchunks, limit;
     int branching;
@@ -90,11 +99,25 @@ struct RunState {  // written by the device
     double mean_d[3], var_l, var_t;
 };
 
+// Per-chunk tallies of one step.  The sums are fixed point (each electron's
+// contribution rounded once), so they do not depend on the order in which the
+// push and collision kernels add them.
 struct ChunkPartial {
-    double vsum, esum, emax;
+    unsigned long long vsum, esum;  // two's-complement fixed point
+    unsigned long long emax_bits;   // largest |v|^2 (bits of a non-negative double)
     unsigned long long cand, nulls;
     unsigned counts[kMaxChannels];
     unsigned surv, births, surv_off, birth_off;
+};
+
+// An electron whose first waiting time falls inside the step.  Its stored
+// velocity is still the one from the start of the step; the collision kernel
+// repeats the first half kick and the first draw.
+struct Candidate {
+    uint32_t particle;  // index within its run
+    uint32_t chunk;     // chunk-table position
+    uint32_t slot;
+    uint32_t pad;
 };
 
 struct Batch {
@@ -104,15 +127,11 @@ struct Batch {
     const uint32_t* chunk_first;
     const uint32_t* nchunks;
     ChunkPartial* part;
+    Candidate* queue;
+    unsigned* qlen;
+    unsigned qcap;
     int max_runs;
-    MccModelDev model;
-};
-
-struct QueueEntry {
-    double v[3];
-    double first_wait;
-    uint32_t local;
-    uint32_t draws;
+    const MccModelDev* model;  // in device memory: the kernels take references into it
 };
 
 template <class T>
@@ -127,7 +146,13 @@ __device__ __forceinline__ double ke_ev(double x, double y, double z) {
 template <class T>
 __device__ __forceinline__ T store_as(double x) { return (T)x; }
 
-// Block-wide sum of one double per thread in a fixed tree order.
+__device__ __forceinline__ double sq3(double x, double y, double z) { return x * x + y * y + z * z; }
+
+__device__ __forceinline__ unsigned long long to_fixed(double x, double scale) {
+    return (unsigned long long)__double2ll_rn(x * scale);
+}
+
+// Block-wide sum of one double per thread in a fixed tree order (valid on thread 0).
 __device__ double block_sum(double x, double* red) {
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -137,31 +162,20 @@ __device__ double block_sum(double x, double* red) {
     double t = 0.0;
     if (threadIdx.x == 0)
         for (int w = 0; w < kThreads / 32; ++w) t += red[w];
-    return t;  // valid on thread 0
-}
-
-__device__ double block_max(double x, double* red) {
-    for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[warp] = x;
-    __syncthreads();
-    double t = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < kThreads / 32; ++w) t = fmax(t, red[w]);
     return t;
 }
 
-__device__ unsigned long long block_sum_u64(unsigned long long x, unsigned long long* red) {
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) red[warp] = x;
-    __syncthreads();
-    unsigned long long t = 0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
-    return t;
+    return x;
+}
+
+__device__ __forceinline__ unsigned long long warp_max_u64(unsigned long long x) {
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, o);
+        x = y > x ? y : x;
+    }
+    return x;
 }
 
 // ---- initial Maxwellian (src/Swarm.cpp:948-956) --------------------------------
@@ -178,174 +192,221 @@ __global__ void __launch_bounds__(kThreads) k_swarm_init(RunCfg R) {
     }
 }
 
-// ---- one step of every active run: kick, drift, MCC, kick, tallies -------------
+// Tally destinations of one chunk: shared memory in the push kernel, the
+// chunk's global partial in the collision kernel (atomics on generic addresses).
+struct Tally {
+    unsigned long long* vsum;
+    unsigned long long* esum;
+    unsigned long long* emax;
+    unsigned long long* cand;
+    unsigned long long* nulls;
+    unsigned* counts;
+    unsigned* surv;
+    unsigned* births;
+    unsigned* err;
+};
+
+// The rest of one electron's step after its first waiting time fell inside
+// the step: the collision loop (src/Collision.cpp:907-993), the second half
+// kick and energy check, the store, and the tallies.
+template <class T>
+__device__ __forceinline__ void finish_candidate(const MccModelDev& M, const RunCfg& R, uint32_t step,
+                                                 uint32_t first, const Candidate& e, const Tally& t) {
+    double v[3];
+    for (int a = 0; a < 3; ++a) v[a] = (double)arr<T>(R.v[a])[e.particle];
+    v[0] += R.half_kick;  // the push kernel's first half kick, repeated
+    PhiloxStream rng(R.seed, e.particle, step, 0u);
+    double u = uniform01(rng);
+    for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
+    const double first_wait = -log(u) / M.max_frequency;
+    CollideResult r;
+    unsigned nsec = 0;
+    const uint32_t li = e.particle - first;
+    const uint32_t local_chunk = first / kChunk;
+    unsigned err = 0;
+    collide3(M, v, R.dt, rng, r,
+             [&](int, const double* vs, const double*) {
+                 if (!R.branching) return;  // fixed population: secondaries are not followed
+                 if (nsec >= (unsigned)kMaxBirthsPerElectron) { err |= kErrBirths; return; }
+                 const unsigned bi = atomicAdd(t.births, 1u);
+                 if (bi >= (unsigned)kChunk) { err |= kErrBirths; return; }
+                 const size_t at = (size_t)local_chunk * kChunk + bi;
+                 for (int a = 0; a < 3; ++a) arr<T>(R.sv[a])[at] = store_as<T>(vs[a]);
+                 R.skey[at] = li * kMaxBirthsPerElectron + nsec;
+                 ++nsec;
+             },
+             true, first_wait);
+    err |= r.error;
+    v[0] += R.half_kick;
+    const double s2 = sq3(v[0], v[1], v[2]);
+    if (s2 > R.s2_max) err |= kErrMaxEnergy;
+    T vs[3];
+    for (int a = 0; a < 3; ++a) {
+        vs[a] = store_as<T>(v[a]);
+        arr<T>(R.v[a])[e.particle] = vs[a];
+    }
+    if (R.branching) R.alive[e.particle] = r.removed ? 0 : 1;
+    atomicMax(t.emax, (unsigned long long)__double_as_longlong(s2));
+    atomicAdd(t.cand, (unsigned long long)r.candidates);
+    if (r.nulls) atomicAdd(t.nulls, (unsigned long long)r.nulls);
+    for (int ch = 0; ch < M.nch; ++ch)
+        if (r.channel[ch]) atomicAdd(&t.counts[ch], r.channel[ch]);
+    if (!r.removed) atomicAdd(t.surv, 1u);
+    atomicAdd(t.vsum, to_fixed((double)vs[0], R.vscale));
+    atomicAdd(t.esum, to_fixed(sq3((double)vs[0], (double)vs[1], (double)vs[2]), R.escale));
+    if (err) atomicOr(t.err, err);
+}
+
+// ---- one step, streaming part: every electron of every active run --------------
+// Half kick, energy check, drift, first waiting time; electrons without a
+// collision candidate finish the step here, the others go to the candidate
+// queue (one global reservation per chunk).
 
 template <class T>
 __global__ void __launch_bounds__(kThreads, 2) k_swarm_push(Batch b) {
-    __shared__ QueueEntry s_queue[kQueue];
-    __shared__ unsigned char s_removed[kQueue];
-    __shared__ unsigned s_qlen, s_births;
-    __shared__ double s_red[kThreads / 32];
-    __shared__ unsigned long long s_redu[kThreads / 32];
-    const int tid = threadIdx.x;
+    __shared__ unsigned long long s_vsum, s_esum, s_emax, s_cand, s_nulls;
+    __shared__ unsigned s_counts[kMaxChannels];
+    __shared__ unsigned s_surv, s_births, s_err, s_ncand, s_base;
+    const int tid = threadIdx.x, lane = tid & 31;
     const uint32_t nch_total = *b.nchunks;
-    const MccModelDev& M = b.model;
+    const MccModelDev& M = *b.model;
 
     for (uint32_t c = blockIdx.x; c < nch_total; c += gridDim.x) {
         const uint32_t slot = b.chunk_run[c];
         const RunCfg& R = b.cfg[slot];
-        RunState& S = b.st[slot];
+        const RunState& S = b.st[slot];
         if (!S.active) continue;  // uniform over the CTA
         const uint32_t first = b.chunk_first[c];
-        const uint32_t local_chunk = first / kChunk;
         const uint32_t cnt = min((uint32_t)kChunk, R.n - first);
         const uint32_t step = S.step;
         const bool sampling = step >= R.burn_in;
-        if (tid == 0) { s_qlen = 0; s_births = 0; }
+        if (tid == 0) {
+            s_vsum = s_esum = s_emax = s_cand = s_nulls = 0ull;
+            s_surv = s_births = s_err = s_ncand = 0u;
+        }
+        if (tid < kMaxChannels) s_counts[tid] = 0u;
         __syncthreads();
 
-        double v[kItems][3];
-        int queued[kItems];
-        unsigned err = 0;
-        double emax = 0.0;
-        unsigned cand = 0, nulls = 0, counts[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
-        bool removed[kItems];
-        // -- phase A: half kick, energy check, drift, first waiting time --
+        unsigned long long vsum = 0ull, esum = 0ull, emax = 0ull;
+        unsigned err = 0, surv = 0;
+        unsigned cand_mask = 0;
+        int qslot[kItems];
+        // loads of the thread's electrons, then their first 64-bit draws (four
+        // independent Philox chains that run while the loads are in flight)
+        T vl[kItems][3], dl[kItems][3];
+        uint64_t d0[kItems];
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const uint32_t li = k * kThreads + tid;
             const uint32_t i = first + li;
-            queued[k] = -1;
-            removed[k] = false;
-            v[k][0] = v[k][1] = v[k][2] = 0.0;
-            if (li >= cnt) continue;
-            for (int a = 0; a < 3; ++a) v[k][a] = (double)arr<T>(R.v[a])[i];
-            v[k][0] += R.half_kick;
-            const double pre = ke_ev(v[k][0], v[k][1], v[k][2]);
-            emax = fmax(emax, pre);
-            if (pre > R.max_energy_ev) err |= kErrMaxEnergyPre;
-            if (sampling) {
-                for (int a = 0; a < 3; ++a) {
-                    T* dp = arr<T>(R.d[a]) + i;
-                    *dp = store_as<T>((double)*dp + v[k][a] * R.dt);
-                }
-            }
-            // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
-            if (!frequency_bound_ok(M, norm3(v[k][0], v[k][1], v[k][2]))) err |= kErrMajorant;
-            PhiloxStream rng(R.seed, i, step, 0u);
-            double u = uniform01(rng);
-            for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
-            const double wait = -log(u) / M.max_frequency;
-            if (isfinite(wait) && wait < R.dt) {
-                const unsigned q = atomicAdd(&s_qlen, 1u);
-                if (q < (unsigned)kQueue) {
-                    QueueEntry& e = s_queue[q];
-                    e.v[0] = v[k][0]; e.v[1] = v[k][1]; e.v[2] = v[k][2];
-                    e.first_wait = wait;
-                    e.local = li;
-                    e.draws = rng.index;
-                    queued[k] = (int)q;
-                } else {
-                    queued[k] = -2;  // queue full: this thread runs the loop itself below
-                }
+            const bool ok = li < cnt;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                vl[k][a] = ok ? arr<T>(R.v[a])[i] : T(0);
+                dl[k][a] = ok && sampling ? arr<T>(R.d[a])[i] : T(0);
             }
         }
-        __syncthreads();
-        // -- phase B: the full collision loops, packed densely over the CTA --
-        auto run_collide = [&](QueueEntry& e) {
-            PhiloxStream rng(R.seed, first + e.local, step, 0u);
-            rng.seek(e.draws);
-            CollideResult r;
-            unsigned nsec = 0;
-            const uint32_t li = e.local;
-            collide3(M, e.v, R.dt, rng, r,
-                     [&](int, const double* vs, const double*) {
-                         if (!R.branching) return;  // fixed population: secondaries are not followed
-                         if (nsec >= (unsigned)kMaxBirthsPerElectron) { err |= kErrBirths; return; }
-                         const unsigned bi = atomicAdd(&s_births, 1u);
-                         if (bi >= (unsigned)kChunk) { err |= kErrBirths; return; }
-                         const size_t at = (size_t)local_chunk * kChunk + bi;
-                         for (int a = 0; a < 3; ++a) arr<T>(R.sv[a])[at] = store_as<T>(vs[a]);
-                         R.skey[at] = li * kMaxBirthsPerElectron + nsec;
-                         ++nsec;
-                     },
-                     true, e.first_wait);
-            err |= r.error;
-            cand += r.candidates;
-            nulls += r.nulls;
-            for (int ch = 0; ch < kMaxChannels; ++ch) counts[ch] += r.channel[ch];
-            return r.removed;
-        };
-        const unsigned qlen = min(s_qlen, (unsigned)kQueue);
-        for (unsigned q = tid; q < qlen; q += kThreads) s_removed[q] = run_collide(s_queue[q]) ? 1 : 0;
-        __syncthreads();
-        // -- phase C: second half kick, energy check, tallies, store --
-        double vsum = 0.0, esum = 0.0;
+#pragma unroll
+        for (int k = 0; k < kItems; ++k) {
+            uint32_t o[4];
+            philox4x32_10(0u, first + k * kThreads + tid, step, 0u, (uint32_t)R.seed, (uint32_t)(R.seed >> 32), o);
+            d0[k] = (uint64_t)o[1] << 32 | o[0];  // PhiloxStream's first draw
+        }
 #pragma unroll
         for (int k = 0; k < kItems; ++k) {
             const uint32_t li = k * kThreads + tid;
             const uint32_t i = first + li;
+            qslot[k] = -1;
             if (li >= cnt) continue;
-            if (queued[k] >= 0) {
-                const QueueEntry& e = s_queue[queued[k]];
-                v[k][0] = e.v[0]; v[k][1] = e.v[1]; v[k][2] = e.v[2];
-                removed[k] = s_removed[queued[k]] != 0;
-            } else if (queued[k] == -2) {
-                QueueEntry e;
-                e.v[0] = v[k][0]; e.v[1] = v[k][1]; e.v[2] = v[k][2];
+            double v[3];
+            for (int a = 0; a < 3; ++a) v[a] = (double)vl[k][a];
+            v[0] += R.half_kick;
+            const double pre = sq3(v[0], v[1], v[2]);
+            emax = max(emax, (unsigned long long)__double_as_longlong(pre));
+            if (pre > R.s2_max) err |= kErrMaxEnergyPre;
+            if (sampling)
+                for (int a = 0; a < 3; ++a) arr<T>(R.d[a])[i] = store_as<T>((double)dl[k][a] + v[a] * R.dt);
+            // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
+            if (!(pre <= M.v_safe2) && !frequency_bound_ok(M, sqrt(pre))) err |= kErrMajorant;
+            bool candidate;
+            if (d0[k] != 0ull) {
+                candidate = !R.no_candidates && d0[k] >= R.cand_draw_min;
+            } else {  // open_unit_interval draws again
                 PhiloxStream rng(R.seed, i, step, 0u);
-                double u = uniform01(rng);
+                double u = 0.0;
                 for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
-                e.first_wait = -log(u) / M.max_frequency;
-                e.local = li;
-                e.draws = rng.index;
-                removed[k] = run_collide(e);
-                v[k][0] = e.v[0]; v[k][1] = e.v[1]; v[k][2] = e.v[2];
+                const double wait = -log(u) / M.max_frequency;
+                candidate = isfinite(wait) && wait < R.dt;
             }
-            v[k][0] += R.half_kick;
-            const double e = ke_ev(v[k][0], v[k][1], v[k][2]);
-            emax = fmax(emax, e);
-            if (e > R.max_energy_ev) err |= kErrMaxEnergy;
+            if (candidate) {
+                cand_mask |= 1u << k;
+                qslot[k] = (int)atomicAdd(&s_ncand, 1u);
+                continue;
+            }
+            // no candidate this step: second half kick, check, store, tallies
+            v[0] += R.half_kick;
+            const double en = sq3(v[0], v[1], v[2]);
+            emax = max(emax, (unsigned long long)__double_as_longlong(en));
+            if (en > R.s2_max) err |= kErrMaxEnergy;
             T vs[3];
             for (int a = 0; a < 3; ++a) {
-                vs[a] = store_as<T>(v[k][a]);
+                vs[a] = store_as<T>(v[a]);
                 arr<T>(R.v[a])[i] = vs[a];
             }
-            if (R.branching) R.alive[i] = removed[k] ? 0 : 1;
-            // fixed population: the sample sums of this step (the stored values)
-            vsum += (double)vs[0];
-            esum += ke_ev((double)vs[0], (double)vs[1], (double)vs[2]);
+            if (R.branching) R.alive[i] = 1;
+            ++surv;
+            vsum += to_fixed((double)vs[0], R.vscale);
+            esum += to_fixed(sizeof(T) == sizeof(double) ? en : sq3((double)vs[0], (double)vs[1], (double)vs[2]),
+                             R.escale);
         }
-        if (err) atomicOr(&S.error, err);
-        // -- per-chunk partials, fixed reduction order --
-        unsigned surv = 0;
-        if (R.branching) {
+        vsum = warp_sum_u64(vsum);
+        esum = warp_sum_u64(esum);
+        emax = warp_max_u64(emax);
+        if (lane == 0) {
+            atomicAdd(&s_vsum, vsum);
+            atomicAdd(&s_esum, esum);
+            atomicMax(&s_emax, emax);
+        }
+        if (surv) atomicAdd(&s_surv, surv);
+        if (err) atomicOr(&s_err, err);
+        __syncthreads();
+        if (tid == 0) s_base = s_ncand ? atomicAdd(b.qlen, s_ncand) : 0u;
+        __syncthreads();
+        // the queue holds one entry per active electron, so it cannot overflow
 #pragma unroll
-            for (int k = 0; k < kItems; ++k) {
-                const uint32_t li = k * kThreads + tid;
-                if (li < cnt && !removed[k]) ++surv;
-            }
-        }
-        const double tv = block_sum(vsum, s_red);
-        const double te = block_sum(esum, s_red);
-        const double tm = block_max(emax, s_red);
-        const unsigned long long tc = block_sum_u64(cand, s_redu);
-        const unsigned long long tn = block_sum_u64(nulls, s_redu);
-        const unsigned long long ts = block_sum_u64(surv, s_redu);
-        unsigned long long tch[kMaxChannels];
-        for (int ch = 0; ch < M.nch; ++ch) tch[ch] = block_sum_u64(counts[ch], s_redu);
+        for (int k = 0; k < kItems; ++k)
+            if (cand_mask >> k & 1u)
+                b.queue[s_base + (unsigned)qslot[k]] = Candidate{first + k * kThreads + tid, c, slot, 0u};
+        __syncthreads();
         if (tid == 0) {
             ChunkPartial& P = b.part[c];
-            P.vsum = tv;
-            P.esum = te;
-            P.emax = tm;
-            P.cand = tc;
-            P.nulls = tn;
-            for (int ch = 0; ch < kMaxChannels; ++ch) P.counts[ch] = ch < M.nch ? (unsigned)tch[ch] : 0u;
-            P.surv = (unsigned)ts;
-            P.births = min(s_births, (unsigned)kChunk);
+            P.vsum = s_vsum;
+            P.esum = s_esum;
+            P.emax_bits = s_emax;
+            P.cand = s_cand;
+            P.nulls = s_nulls;
+            for (int ch = 0; ch < kMaxChannels; ++ch) P.counts[ch] = s_counts[ch];
+            P.surv = s_surv;
+            P.births = s_births;
+            if (s_err) atomicOr(&b.st[slot].error, s_err);
         }
         __syncthreads();
+    }
+}
+
+// ---- one step, collision part: the queued candidates, packed densely -----------
+
+template <class T>
+__global__ void __launch_bounds__(kThreads, 3) k_swarm_collide(Batch b) {
+    const unsigned qn = *b.qlen;
+    for (unsigned q = blockIdx.x * kThreads + threadIdx.x; q < qn; q += gridDim.x * kThreads) {
+        const Candidate e = b.queue[q];
+        const RunCfg& R = b.cfg[e.slot];
+        RunState& S = b.st[e.slot];
+        ChunkPartial& P = b.part[e.chunk];
+        const uint32_t first = b.chunk_first[e.chunk];
+        const Tally tl{&P.vsum, &P.esum, &P.emax_bits, &P.cand, &P.nulls, P.counts, &P.surv, &P.births, &S.error};
+        finish_candidate<T>(*b.model, R, S.step, first, e, tl);
     }
 }
 
@@ -367,7 +428,8 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_scan(Batch b) {
         const bool ok = lc < R.nchunks;
         ChunkPartial* P = ok ? &b.part[R.first_chunk + lc] : nullptr;
         // survivors and births packed in one 64-bit scan (each < 2^32 per run)
-        const unsigned long long x = ok ? (((unsigned long long)P->surv << 32) | P->births) : 0ull;
+        const unsigned long long x =
+            ok ? (((unsigned long long)P->surv << 32) | min(P->births, (unsigned)kChunk)) : 0ull;
         unsigned long long ex, tot;
         Scan(tmp).ExclusiveSum(x, ex, tot);
         if (ok) {
@@ -430,7 +492,7 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_compact(Batch b) {
             if (threadIdx.x == 0) s_carry += tot;
             __syncthreads();
         }
-        const unsigned nb = P.births;
+        const unsigned nb = min(P.births, (unsigned)kChunk);
         const size_t sbase = (size_t)local_chunk * kChunk;
         for (unsigned j = threadIdx.x; j < nb; j += kThreads) s_key[j] = R.skey[sbase + j];
         __syncthreads();
@@ -452,7 +514,7 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_compact(Batch b) {
 // Systematic resampling back to N electrons, and the sample sums of the step.
 template <class T>
 __global__ void __launch_bounds__(kThreads) k_swarm_branch_resample(Batch b) {
-    __shared__ double s_red[kThreads / 32];
+    __shared__ unsigned long long s_vsum, s_esum;
     const uint32_t nch_total = *b.nchunks;
     for (uint32_t c = blockIdx.x; c < nch_total; c += gridDim.x) {
         const uint32_t slot = b.chunk_run[c];
@@ -462,7 +524,9 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_resample(Batch b) {
         const uint32_t first = b.chunk_first[c];
         const uint32_t cnt = min((uint32_t)kChunk, R.n - first);
         const uint32_t mp = S.m_prime;
-        double vsum = 0.0, esum = 0.0;
+        if (threadIdx.x == 0) s_vsum = s_esum = 0ull;
+        __syncthreads();
+        unsigned long long vsum = 0ull, esum = 0ull;
         for (uint32_t li = threadIdx.x; li < cnt; li += kThreads) {
             const uint32_t s = first + li;
             uint32_t j = s;
@@ -478,14 +542,19 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_resample(Batch b) {
                 arr<T>(R.v[k])[s] = vs[k];
                 arr<T>(R.d[k])[s] = arr<T>(R.bd[k])[j];
             }
-            vsum += (double)vs[0];
-            esum += ke_ev((double)vs[0], (double)vs[1], (double)vs[2]);
+            vsum += to_fixed((double)vs[0], R.vscale);
+            esum += to_fixed(sq3((double)vs[0], (double)vs[1], (double)vs[2]), R.escale);
         }
-        const double tv = block_sum(vsum, s_red);
-        const double te = block_sum(esum, s_red);
+        vsum = warp_sum_u64(vsum);
+        esum = warp_sum_u64(esum);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&s_vsum, vsum);
+            atomicAdd(&s_esum, esum);
+        }
+        __syncthreads();
         if (threadIdx.x == 0) {
-            b.part[c].vsum = tv;
-            b.part[c].esum = te;
+            b.part[c].vsum = s_vsum;
+            b.part[c].esum = s_esum;
         }
         __syncthreads();
     }
@@ -494,52 +563,66 @@ __global__ void __launch_bounds__(kThreads) k_swarm_branch_resample(Batch b) {
 // ---- per run: tallies and the samples of the step --------------------------------
 
 __global__ void __launch_bounds__(kThreads) k_swarm_reduce(Batch b) {
-    __shared__ double s_red[kThreads / 32];
-    __shared__ unsigned long long s_redu[kThreads / 32];
+    __shared__ unsigned long long s_v, s_e, s_m, s_c, s_n;
+    __shared__ unsigned long long s_ch[kMaxChannels];
     const int slot = blockIdx.x;
+    if (slot == 0 && threadIdx.x == 0) *b.qlen = 0u;  // the candidate queue of the next step starts empty
     if (slot >= b.max_runs) return;
     const RunCfg& R = b.cfg[slot];
     RunState& S = b.st[slot];
     if (!S.active) return;
-    const int nch = b.model.nch;
-    double vsum = 0.0, esum = 0.0, emax = 0.0;
-    unsigned long long cand = 0, nulls = 0, cnt[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int nch = b.model->nch;
+    if (threadIdx.x == 0) s_v = s_e = s_m = s_c = s_n = 0ull;
+    if (threadIdx.x < kMaxChannels) s_ch[threadIdx.x] = 0ull;
+    __syncthreads();
+    unsigned long long v = 0, e = 0, m = 0, cand = 0, nulls = 0, cnt[kMaxChannels] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t lc = threadIdx.x; lc < R.nchunks; lc += kThreads) {
         const ChunkPartial& P = b.part[R.first_chunk + lc];
-        vsum += P.vsum;
-        esum += P.esum;
-        emax = fmax(emax, P.emax);
+        v += P.vsum;
+        e += P.esum;
+        m = max(m, P.emax_bits);
         cand += P.cand;
         nulls += P.nulls;
-        for (int ch = 0; ch < nch; ++ch) cnt[ch] += P.counts[ch];
+#pragma unroll
+        for (int ch = 0; ch < kMaxChannels; ++ch) cnt[ch] += P.counts[ch];
     }
-    const double tv = block_sum(vsum, s_red);
-    const double te = block_sum(esum, s_red);
-    const double tm = block_max(emax, s_red);
-    const unsigned long long tc = block_sum_u64(cand, s_redu);
-    const unsigned long long tn = block_sum_u64(nulls, s_redu);
-    unsigned long long tch[kMaxChannels];
-    for (int ch = 0; ch < nch; ++ch) tch[ch] = block_sum_u64(cnt[ch], s_redu);
+    v = warp_sum_u64(v);
+    e = warp_sum_u64(e);
+    m = warp_max_u64(m);
+    cand = warp_sum_u64(cand);
+    nulls = warp_sum_u64(nulls);
+#pragma unroll
+    for (int ch = 0; ch < kMaxChannels; ++ch) cnt[ch] = warp_sum_u64(cnt[ch]);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&s_v, v);
+        atomicAdd(&s_e, e);
+        atomicMax(&s_m, m);
+        atomicAdd(&s_c, cand);
+        atomicAdd(&s_n, nulls);
+        for (int ch = 0; ch < nch; ++ch) atomicAdd(&s_ch[ch], cnt[ch]);
+    }
+    __syncthreads();
     if (threadIdx.x != 0) return;
     const uint32_t step = S.step;
     const double w = S.weight;
-    S.max_ev = fmax(S.max_ev, tm);
+    // kinetic_energy_ev of the largest |v|^2: the energy is monotone in |v|^2
+    S.max_ev = fmax(S.max_ev, 0.5 * kElectronMass * __longlong_as_double((long long)s_m) / kEvToJ);
     if (step >= R.burn_in) {
         S.exposure += (double)R.n * w * R.dt;
-        S.candidates += tc;
-        S.nulls += tn;
+        S.candidates += s_c;
+        S.nulls += s_n;
         for (int ch = 0; ch < nch; ++ch) {
-            S.counts[ch] += tch[ch];
-            S.wcoll[ch] += w * (double)tch[ch];
-            S.wcoll2[ch] += w * w * (double)tch[ch];
+            S.counts[ch] += s_ch[ch];
+            S.wcoll[ch] += w * (double)s_ch[ch];
+            S.wcoll2[ch] += w * w * (double)s_ch[ch];
         }
     }
     if (R.branching && !S.error) S.weight = S.weight_next;
     if (step >= R.burn_in) {
         const size_t ns = R.steps - R.burn_in;
         const size_t k = step - R.burn_in;
-        R.samples[k] = tv / (double)R.n;
-        R.samples[ns + k] = te / (double)R.n;
+        R.samples[k] = (double)(long long)s_v / R.vscale / (double)R.n;
+        R.samples[ns + k] = 0.5 * kElectronMass * ((double)(long long)s_e / R.escale) / kEvToJ / (double)R.n;
         R.samples[2 * ns + k] = log((double)R.n * S.weight);
     }
     S.step = step + 1;
@@ -633,6 +716,62 @@ static bool block_slope_and_error(const double* x, size_t n, double dt, size_t b
     slope = m;
     se = e;
     return true;
+}
+
+// Largest |v|^2 whose kinetic_energy_ev (0.5 m |v|^2 / e, src/Swarm.cpp:95-101)
+// does not exceed e_max: the energy checks of src/Swarm.cpp:1011-1037 become
+// comparisons of |v|^2 with this value.
+static double s2_threshold(double e_max) {
+    auto f = [](double s2) { return 0.5 * kElectronMass * s2 / kEvToJ; };
+    uint64_t lo = 0, hi = 0x7FF0000000000000ull;  // f(0) <= e_max < f(inf)
+    while (hi - lo > 1) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        double x;
+        std::memcpy(&x, &mid, 8);
+        if (f(x) <= e_max) lo = mid; else hi = mid;
+    }
+    double r;
+    std::memcpy(&r, &lo, 8);
+    return r;
+}
+
+// The first waiting time -log(u) / nu (src/Collision.cpp:926-933) falls inside
+// the step (< dt) exactly when u >= u*, and u = draw / 2^64 (libstdc++'s
+// generate_canonical on a 64-bit draw, values rounding to 1 replaced by the
+// largest double below 1) is at least u* exactly when the draw is at least
+// D*.  Both thresholds are found by bisection with the host's log, the one
+// the CPU restatement uses.
+static void draw_threshold(double nu, double dt, uint64_t& dmin, int& none) {
+    auto wait = [nu](double u) { return -std::log(u) / nu; };
+    const double umax = std::nextafter(1.0, 0.0);
+    none = 0;
+    dmin = 0;
+    if (!(wait(umax) < dt)) { none = 1; return; }
+    uint64_t lo = 1, hi;  // bit patterns: wait(lo) >= dt > wait(hi)
+    std::memcpy(&hi, &umax, 8);
+    {
+        double x;
+        std::memcpy(&x, &lo, 8);
+        if (wait(x) < dt) { dmin = 1; return; }
+    }
+    while (hi - lo > 1) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        double x;
+        std::memcpy(&x, &mid, 8);
+        if (wait(x) < dt) hi = mid; else lo = mid;
+    }
+    double ustar;
+    std::memcpy(&ustar, &hi, 8);
+    auto canon = [umax](uint64_t d) {
+        double r = (double)d / 18446744073709551616.0;
+        return r >= 1.0 ? umax : r;
+    };
+    uint64_t a = 0, b = ~0ull;  // canon(a) < u* <= canon(b)
+    while (b - a > 1) {
+        const uint64_t mid = a + (b - a) / 2;
+        if (canon(mid) >= ustar) b = mid; else a = mid;
+    }
+    dmin = b;
 }
 
 // effective_population_limit, src/Swarm.cpp:237-260
@@ -730,6 +869,10 @@ struct Server {
     uint32_t* d_chunk_first = nullptr;
     uint32_t* d_nchunks = nullptr;
     ChunkPartial* d_part = nullptr;
+    Candidate* d_queue = nullptr;
+    MccModelDev* d_model = nullptr;
+    unsigned* d_qlen = nullptr;
+    size_t qcap = 0;
     // host mirrors
     std::vector<Run> runs;
     std::vector<RunState> h_st;
@@ -743,6 +886,10 @@ struct Server {
     int push_grid = 0;
     uint64_t launches = 0;
     uint64_t particle_steps = 0;
+    // optional timing of the push kernel (kernels launched one by one, no graph)
+    bool timing = false;
+    double push_ms = 0.0, collide_ms = 0.0, push_bytes = 0.0;
+    uint64_t push_launches = 0;
 
     ~Server() {
         if (stream) cudaStreamSynchronize(stream);
@@ -760,8 +907,11 @@ struct Server {
         b.chunk_first = d_chunk_first;
         b.nchunks = d_nchunks;
         b.part = d_part;
+        b.queue = d_queue;
+        b.qlen = d_qlen;
+        b.qcap = (unsigned)qcap;
         b.max_runs = conf.max_runs;
-        b.model = model;
+        b.model = d_model;
         return b;
     }
 
@@ -799,10 +949,18 @@ struct Server {
         build_model(m, kElectronMass, arena, model);
         neutral_density = m.neutral_density;
         max_frequency = m.max_frequency;
-        char* pool_base = arena.alloc<char>(c.memory_budget_bytes);
-        pool.init(pool_base, c.memory_budget_bytes);
+        d_model = arena.upload(&model, 1);
+        // the collision-candidate queue has one entry per electron the pool can
+        // hold (every electron of a step may be a candidate)
+        const size_t per_electron = 6 * (fp32 ? 4 : 8);
+        qcap = std::min<size_t>(c.memory_budget_bytes / (per_electron + sizeof(Candidate)), 0xFFFFFFF0u);
+        d_queue = arena.alloc<Candidate>(qcap);
+        d_qlen = arena.alloc<unsigned>(1);
+        const size_t pool_bytes = c.memory_budget_bytes - qcap * sizeof(Candidate);
+        char* pool_base = arena.alloc<char>(pool_bytes);
+        pool.init(pool_base, pool_bytes);
         const size_t min_bytes = (fp32 ? 4 : 8) * 6 * (size_t)kChunk;
-        max_chunks = c.memory_budget_bytes / min_bytes + (size_t)c.max_runs + 1;
+        max_chunks = pool_bytes / min_bytes + (size_t)c.max_runs + 1;
         d_cfg = arena.alloc<RunCfg>(c.max_runs);
         d_st = arena.alloc<RunState>(c.max_runs);
         d_chunk_run = arena.alloc<uint32_t>(max_chunks);
@@ -813,7 +971,7 @@ struct Server {
         h_st.resize(c.max_runs);
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        push_grid = sms * 2;
+        push_grid = sms * 4;
         APIC_CUDA(cudaStreamSynchronize(stream));
     }
 
@@ -886,6 +1044,9 @@ struct Server {
     int admit() {
         int admitted = 0;
         size_t used_chunks = h_chunk_run.size();
+        size_t electrons = 0;  // the candidate queue holds one entry per active electron
+        for (int s = 0; s < conf.max_runs; ++s)
+            if (runs[s].used) electrons += runs[s].req.particles;
         for (auto it = queue.begin(); it != queue.end();) {
             int slot = -1;
             for (int s = 0; s < conf.max_runs; ++s)
@@ -893,9 +1054,10 @@ struct Server {
             if (slot < 0) break;
             const apic_swarm_request& r = it->req;
             const size_t nch = (r.particles + kChunk - 1) / kChunk;
-            if (used_chunks + nch > max_chunks || run_bytes(r) > pool.size) { ++it; continue; }
+            if (used_chunks + nch > max_chunks || electrons + r.particles > qcap) { ++it; continue; }
             if (!place(slot, *it)) { ++it; continue; }
             used_chunks += nch;
+            electrons += r.particles;
             it = queue.erase(it);
             ++admitted;
         }
@@ -934,6 +1096,13 @@ struct Server {
         const double E = r.reduced_field_td * kTownsend * neutral_density;
         const double acceleration = -kEvToJ * E / kElectronMass;
         C.half_kick = 0.5 * acceleration * r.timestep;
+        // fixed-point scales: |v_x| <= v(max_energy_ev) and energy <= max_energy_ev
+        // for every electron of a healthy run, so n such terms stay below 2^61
+        const double vmax = std::sqrt(2.0 * r.max_energy_ev * kEvToJ / kElectronMass);
+        C.s2_max = s2_threshold(r.max_energy_ev);
+        C.vscale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 61) / ((double)n * vmax))));
+        C.escale = std::ldexp(1.0, (int)std::floor(std::log2(std::ldexp(1.0, 61) / ((double)n * C.s2_max))));
+        draw_threshold(max_frequency, r.timestep, C.cand_draw_min, C.no_candidates);
         C.dt = r.timestep;
         C.max_energy_ev = r.max_energy_ev;
         C.init_sd = std::sqrt(2.0 * r.initial_mean_energy_ev * kEvToJ / (3.0 * kElectronMass));
@@ -1006,6 +1175,7 @@ struct Server {
     template <class T>
     void enqueue_step(const Batch& b) {
         k_swarm_push<T><<<push_grid, kThreads, 0, stream>>>(b);
+        k_swarm_collide<T><<<push_grid, kThreads, 0, stream>>>(b);
         k_swarm_branch_scan<<<conf.max_runs, kThreads, 0, stream>>>(b);
         k_swarm_branch_compact<T><<<push_grid, kThreads, 0, stream>>>(b);
         k_swarm_branch_resample<T><<<push_grid, kThreads, 0, stream>>>(b);
@@ -1172,9 +1342,60 @@ struct Server {
         if (tables_dirty) rebuild_tables();
         int active = 0;
         for (int s = 0; s < conf.max_runs; ++s) active += runs[s].used ? 1 : 0;
+        if (active && timing) {
+            // algorithmic bytes of each push: velocity read + write, and the
+            // displacement read + write during sampling steps
+            const size_t es = fp32 ? 4 : 8;
+            const Batch b = batch();
+            struct Ev3 { cudaEvent_t first, second, third; };
+            std::vector<Ev3> ev(conf.steps_per_launch);
+            for (size_t k = 0; k < conf.steps_per_launch; ++k) {
+                for (int s = 0; s < conf.max_runs; ++s) {
+                    const Run& run = runs[s];
+                    if (!run.used || !h_st[s].active) continue;
+                    const size_t st = h_st[s].step + k;
+                    if (st >= run.req.steps) continue;
+                    push_bytes += (double)run.req.particles * es * (st >= run.req.burn_in_steps ? 12 : 6);
+                }
+                APIC_CUDA(cudaEventCreate(&ev[k].first));
+                APIC_CUDA(cudaEventCreate(&ev[k].second));
+                APIC_CUDA(cudaEventCreate(&ev[k].third));
+                APIC_CUDA(cudaEventRecord(ev[k].first, stream));
+                if (fp32) k_swarm_push<float><<<push_grid, kThreads, 0, stream>>>(b);
+                else k_swarm_push<double><<<push_grid, kThreads, 0, stream>>>(b);
+                APIC_CUDA(cudaEventRecord(ev[k].second, stream));
+                if (fp32) k_swarm_collide<float><<<push_grid, kThreads, 0, stream>>>(b);
+                else k_swarm_collide<double><<<push_grid, kThreads, 0, stream>>>(b);
+                APIC_CUDA(cudaEventRecord(ev[k].third, stream));
+                k_swarm_branch_scan<<<conf.max_runs, kThreads, 0, stream>>>(b);
+                if (fp32) {
+                    k_swarm_branch_compact<float><<<push_grid, kThreads, 0, stream>>>(b);
+                    k_swarm_branch_resample<float><<<push_grid, kThreads, 0, stream>>>(b);
+                } else {
+                    k_swarm_branch_compact<double><<<push_grid, kThreads, 0, stream>>>(b);
+                    k_swarm_branch_resample<double><<<push_grid, kThreads, 0, stream>>>(b);
+                }
+                k_swarm_reduce<<<conf.max_runs, kThreads, 0, stream>>>(b);
+                APIC_CUDA(cudaGetLastError());
+            }
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            for (auto& e : ev) {
+                float ms = 0.f, ms2 = 0.f;
+                APIC_CUDA(cudaEventElapsedTime(&ms, e.first, e.second));
+                APIC_CUDA(cudaEventElapsedTime(&ms2, e.second, e.third));
+                push_ms += ms;
+                collide_ms += ms2;
+                ++push_launches;
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+                cudaEventDestroy(e.third);
+            }
+        }
         if (active) {
-            ensure_graph();
-            APIC_CUDA(cudaGraphLaunch(graph_exec, stream));
+            if (!timing) {
+                ensure_graph();
+                APIC_CUDA(cudaGraphLaunch(graph_exec, stream));
+            }
             ++launches;
             APIC_CUDA(cudaMemcpyAsync(h_st.data(), d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
                                       stream));
@@ -1202,7 +1423,8 @@ struct Server {
 
     uint64_t submit(const apic_swarm_request& r) {
         validate(r);
-        require(run_bytes(r) <= pool.size, "swarm request does not fit the server's memory budget", APIC_ERR_CAPACITY);
+        require(run_bytes(r) <= pool.size && r.particles <= qcap,
+                "swarm request does not fit the server's memory budget", APIC_ERR_CAPACITY);
         require((r.particles + kChunk - 1) / kChunk + 1 <= max_chunks, "swarm request exceeds the chunk table",
                 APIC_ERR_CAPACITY);
         Request q;
@@ -1304,6 +1526,28 @@ int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, ui
             for (auto& kv : srv->impl.pool.free_) f += kv.second;
             *pool_bytes_free = f;
         }
+    });
+}
+
+int apic_swarm_server_set_kernel_timing(apic_swarm_server* srv, int enable) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] {
+        srv->impl.timing = enable != 0;
+        srv->impl.push_ms = 0.0;
+        srv->impl.collide_ms = 0.0;
+        srv->impl.push_bytes = 0.0;
+        srv->impl.push_launches = 0;
+    });
+}
+
+int apic_swarm_server_kernel_times(apic_swarm_server* srv, double* push_ms, double* collide_ms,
+                                   uint64_t* push_launches, double* push_bytes) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] {
+        if (push_ms) *push_ms = srv->impl.push_ms;
+        if (collide_ms) *collide_ms = srv->impl.collide_ms;
+        if (push_launches) *push_launches = srv->impl.push_launches;
+        if (push_bytes) *push_bytes = srv->impl.push_bytes;
     });
 }
 

@@ -43,6 +43,10 @@ WORKLOAD_2D = "plasma_2d3v_bz: periodic 512x512 cells (cell = lambda_D at 1e16 m
               "ions (33,554,432 particles), Bz 0.01 T, Te 2 eV, Ti 0.03 eV, m_i/m_e 1836, dt 0.1/omega_pe"
 WORKLOAD_3D = "plasma_3d3v_bx: periodic 256^3 cells, 8 ppc e- + 8 ppc ions (268,435,456 particles), " \
               "Bx 0.005 T, Te 1 eV, Ti 0.025 eV, m_i/m_e 1836, dt 0.1/omega_pe"
+WORKLOAD_SWARM = "swarm_serving: electron swarms in a 4-process gas (elastic, excitations 11.5 / 13.0 eV, " \
+                 "ionization 15.8 eV) at 2.45e25 m^-3, 300 K; E/N log-uniform 10-1000 Td, electrons log-normal " \
+                 "(median 100k, sigma 1, clipped 10k-4M), Poisson arrivals at 80% of measured capacity, each run " \
+                 "until drift velocity and mean energy converge to 1% or 20k steps"
 # algorithmic bytes per particle-step: read + write of the persistent state once
 BYTES_PER_PSTEP = {("plasma2d", "fp64"): 80, ("plasma3d", "fp64"): 96,
                    ("plasma2d", "fp32"): 48, ("plasma3d", "fp32"): 56}
@@ -54,7 +58,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ccp1d", choices=["ccp1d", "plasma2d", "plasma3d"])
+    ap.add_argument("--workload", default="ccp1d", choices=["ccp1d", "plasma2d", "plasma3d", "swarm"])
+    ap.add_argument("--requests", type=int, default=96, help="swarm: requests in the Poisson serving phase")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--cells", type=int, default=None, help="cells per axis")
@@ -63,9 +68,11 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
-    big = a.workload != "ccp1d"
+    big = a.workload in ("plasma2d", "plasma3d")
+    if a.workload == "swarm":
+        a.precision = a.precision or "fp32"
     if a.steps is None:
-        a.steps = {"ccp1d": 200, "plasma2d": 100, "plasma3d": 20}[a.workload]
+        a.steps = {"ccp1d": 200, "plasma2d": 100, "plasma3d": 20, "swarm": 48}[a.workload]
     if a.warmup is None:
         a.warmup = 5 if big else 20
     if a.e2e_steps is None:
@@ -180,8 +187,43 @@ def _prod(t):
     return r
 
 
+def _swarm_cpu_sample(seconds, threads):
+    """The reference's run_swarm_benchmark on this host: one serial run per
+    core (the reference runs fields one after another), each sized to about
+    `seconds` of work, on the serving deck's gas and timestep."""
+    import concurrent.futures as cf
+    import pyoracle as po
+    from apic import workloads as W
+    if not po.reference_available():
+        raise RuntimeError("the reference library was not built on this host")
+    spec = W.swarm_c5()
+    T = po.TableSet()
+    cfg, gas = po.swarm_from_spec(spec, T)
+    cfg.particles, cfg.steps, cfg.burn_in_steps = 2000, 100, 50
+    t0 = time.perf_counter()
+    po.ref_swarm_run(cfg, gas, [100.0], tempfile.mkdtemp())
+    rate = cfg.particles * cfg.steps / (time.perf_counter() - t0)
+    steps = 200
+    cfg.steps, cfg.burn_in_steps = steps, 100
+    cfg.particles = int(min(max(rate * seconds / steps, 1000), 200_000))
+
+    def one(k):
+        return po.ref_swarm_run(cfg, gas, [100.0 + 10.0 * k], tempfile.mkdtemp())
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:  # ctypes calls release the GIL
+        list(ex.map(one, range(threads)))
+    dt = time.perf_counter() - t0
+    return threads * cfg.particles * steps / dt, dt, cfg.particles, steps
+
+
 def cpu_reference_sample(args, wl, seconds, threads):
     """A bounded sample of the reference's CPU step on this host's cores."""
+    if args.workload == "swarm":
+        v, dt, n, steps = _swarm_cpu_sample(seconds, threads)
+        return {"value": v, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                "sample": f"{threads} concurrent run_swarm_benchmark runs (one field each, {n} electrons x {steps} "
+                          f"steps, 100-{100 + 10 * (threads - 1)} Td) in {dt:.1f} s"}
     if args.workload == "ccp1d":
         sim, kind, cores, _ = _ccp_cpu_sim(wl, threads)
         n = sum(len(s.x) for s in wl.species)
@@ -207,6 +249,18 @@ def run_reference(args):
         return
     from apic import workloads as W
     threads = os.cpu_count() or 1
+    if args.workload == "swarm":
+        value, dt, n, steps = _swarm_cpu_sample(min(20.0, 2.0 * max(1, min(args.steps, 10))), threads)
+        line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * dt / steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOAD_SWARM, "parallelism": "one serial run per host thread"},
+                "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "reference",
+                                 "sample": f"{threads} concurrent runs of {n} electrons x {steps} steps"},
+                "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     if args.workload == "ccp1d":
         wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7)
         sim, kind, threads, _ = _ccp_cpu_sim(wl, threads)
@@ -477,6 +531,129 @@ def bench_plasma(args, rank, dist):
     }
 
 
+def _swarm_draw(rng, spec, W, k, seed_base):
+    """One serving request: E/N log-uniform in 10-1000 Td, electrons
+    log-normal (median 100k, sigma 1) clipped to 10k-4M, 1% tolerance or 20k
+    steps, 2000 burn-in steps."""
+    import numpy as np
+    td = float(np.exp(rng.uniform(np.log(10.0), np.log(1000.0))))
+    n = int(np.clip(np.exp(rng.normal(np.log(1e5), 1.0)), 1e4, 4e6))
+    return W.swarm_request(spec, td, particles=n, seed=seed_base + k, steps=20000, burn_in_steps=2000, tolerance=0.01)
+
+
+def bench_swarm(args, rank, dist):
+    """Batched swarm serving: saturation throughput, then Poisson arrivals at
+    80% of the measured capacity with p50 / p99 request latency."""
+    import numpy as np
+    import torch
+    import apic
+    from apic import workloads as W
+
+    spec = W.swarm_c5()
+    prec = apic.FP32 if args.precision == "fp32" else apic.FP64
+    cfg, gas, tabs = W.to_device_swarm(spec, prec)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(min(64 << 30, 0.6 * free))
+    spl = 200
+    srv = apic.SwarmServer(gas, budget, max_runs=256, precision=prec, steps_per_launch=spl)
+    ext = torch.cuda.ExternalStream(srv.cuda_stream())
+    rng = np.random.default_rng(5 + rank)
+
+    def drain(ids, submit_at=None, pending=None):
+        done = {}
+        while len(done) < len(ids):
+            srv.advance()
+            for i in ids:
+                if i not in done:
+                    r = srv.poll(i)
+                    if r is not None:
+                        done[i] = r
+        return done
+
+    # warm-up: graph capture and first-touch of the pool
+    drain([srv.submit(_swarm_draw(rng, spec, W, k, 10_000_000)) for k in range(max(args.warmup, 3))])
+
+    # -- saturation: a full queue, device time over the whole batch --
+    batch = [_swarm_draw(rng, spec, W, k, 20_000_000 + 1000 * rank) for k in range(args.steps)]
+    _, ps0, _ = srv.stats()
+    ids = [srv.submit(r) for r in batch]
+    srv.set_kernel_timing(True)  # the first two advances time the push kernel one launch at a time
+    srv.advance()
+    srv.advance()
+    push_ms, collide_ms, push_launches, push_bytes = srv.kernel_times()
+    srv.set_kernel_timing(False)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(ext)
+        g0 = srv.stats()[0]
+        res = drain(ids)
+        e1.record(ext)
+        e1.synchronize()
+    t_sat = e0.elapsed_time(e1) * 1e-3
+    g1, ps1, _ = srv.stats()
+    sat_psteps = ps1 - ps0
+    # the two timed advances ran before e0: count only the work inside the region
+    ms_max, total = _reduce(dist, t_sat * 1e3, float(sat_psteps))
+    value = total / (ms_max * 1e-3)
+    capacity = len(batch) / t_sat
+    assert all(r.status == 0 for r in res.values()), [r.message for r in res.values() if r.status]
+
+    # -- serving: Poisson arrivals at 80% of capacity --
+    rate = 0.8 * capacity
+    gaps = rng.exponential(1.0 / rate, args.requests)
+    arrivals = np.cumsum(gaps)
+    reqs = [_swarm_draw(rng, spec, W, k, 30_000_000 + 1000 * rank) for k in range(args.requests)]
+    _, ps2, _ = srv.stats()
+    t0 = time.perf_counter()
+    sub, lat, results = {}, [], []
+    nxt = 0
+    while len(lat) < args.requests:
+        now = time.perf_counter() - t0
+        while nxt < args.requests and arrivals[nxt] <= now:
+            sub[srv.submit(reqs[nxt])] = arrivals[nxt]
+            nxt += 1
+        active, queued = srv.advance()
+        now = time.perf_counter() - t0
+        for i in list(sub):
+            r = srv.poll(i)
+            if r is not None:
+                lat.append(now - sub.pop(i))
+                results.append(r)
+        if not active and not queued and nxt < args.requests:
+            time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
+    t_serve = time.perf_counter() - t0
+    _, ps3, _ = srv.stats()
+    serve_value = (ps3 - ps2) / t_serve
+    srv.close()
+    lat = np.array(lat)
+    hbm, peak_kind = peaks()
+    achieved = push_bytes / (push_ms * 1e-3) / 1e9 if push_ms > 0 else None
+    steps_done = np.array([r.steps_done for r in results])
+    return {
+        "value": value, "ms_per_step": 1e3 * t_sat / max(1, (g1 - g0) * spl), "dtype": "f32" if prec == apic.FP32 else "f64",
+        "config": {"workload": WORKLOAD_SWARM, "form": ("FP32 electron velocity + displacement, FP64 collision "
+                                                        "arithmetic and tallies") if prec == apic.FP32 else
+                   "FP64 electrons", "saturation_requests": len(batch), "steps_per_launch": spl,
+                   "l2": "electron state of the batch larger than L2"},
+        "e2e": {"value": serve_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                "note": "Poisson serving phase through the swarm server API: requests and results are host structs"},
+        "swarm": {"p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                  "capacity_requests_per_s": capacity, "arrival_rate_requests_per_s": rate,
+                  "requests": int(args.requests), "converged_fraction": float(np.mean([r.converged for r in results])),
+                  "mean_steps": float(steps_done.mean()), "serving_particle_steps_per_s": serve_value},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm if achieved else None, "traffic": _profiled_traffic("k_swarm_push_c5_fp32.md"),
+                     "peak_kind": peak_kind, "kernel": "k_swarm_push<float>",
+                     "bytes_per_particle_step": "24 (burn-in) / 48 (sampling)",
+                     "push_ms_per_launch": push_ms / max(push_launches, 1),
+                     "collide_ms_per_launch": collide_ms / max(push_launches, 1)},
+        "gpu_launches": int((g1 - g0) * spl * 6),
+        "clocks": clk.summary(),
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -494,7 +671,12 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    part = bench_ccp1d(args, rank, dist) if args.workload == "ccp1d" else bench_plasma(args, rank, dist)
+    if args.workload == "ccp1d":
+        part = bench_ccp1d(args, rank, dist)
+    elif args.workload == "swarm":
+        part = bench_swarm(args, rank, dist)
+    else:
+        part = bench_plasma(args, rank, dist)
 
     if rank == 0:
         cpu = None
@@ -502,7 +684,8 @@ def main():
             try:
                 from apic import workloads as W
                 wl = (W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7)
-                      if args.workload == "ccp1d" else W.plasma_plan(2 if args.workload == "plasma2d" else 3))
+                      if args.workload == "ccp1d" else None if args.workload == "swarm"
+                      else W.plasma_plan(2 if args.workload == "plasma2d" else 3))
                 cpu = cpu_reference_sample(args, wl, args.cpu_seconds, os.cpu_count() or 1)
             except Exception as e:  # reported, never fatal
                 cpu = {"value": None, "error": str(e)}
@@ -515,6 +698,8 @@ def main():
             "data": "synthetic", "config": cfg, "e2e": part["e2e"], "roofline": part["roofline"],
             "gpu_launches": part["gpu_launches"], "clocks": part["clocks"], "cpu_baseline": cpu,
         }
+        if "swarm" in part:
+            line["swarm"] = part["swarm"]
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -479,6 +479,15 @@ APIC_EXPORT int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic
 APIC_EXPORT int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,
                                         size_t* pool_bytes_free);
 APIC_EXPORT int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream);
+/* Diagnostics: with timing on, advance launches the step kernels one by one
+ * (no graph) and times every streaming push and collision launch with CUDA
+ * events; kernel_times reports the summed milliseconds of each, the number of
+ * steps timed, and the push's algorithmic bytes (electron velocity read +
+ * write, plus displacement read + write in sampling steps).  Enabling resets
+ * the sums. */
+APIC_EXPORT int apic_swarm_server_set_kernel_timing(apic_swarm_server* srv, int enable);
+APIC_EXPORT int apic_swarm_server_kernel_times(apic_swarm_server* srv, double* push_ms, double* collide_ms,
+                                               uint64_t* push_launches, double* push_bytes);
 
 #ifdef __cplusplus
 }
