@@ -6,7 +6,7 @@
 #include <stdexcept>
 #include <string>
 
-#include "../../include/aurorapic_b200.h"
+#include "aurorapic_b200.h"
 
 namespace apic {
 

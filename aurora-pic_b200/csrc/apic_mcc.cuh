@@ -150,19 +150,34 @@ __device__ inline bool rates_for_speed(const MccModelDev& m, double speed, doubl
 
 // validate_frequency_bound, src/Collision.cpp:627-685 (exact form, run only
 // above the precomputed safe speed).
-static __device__ __noinline__ bool frequency_bound_exact(const MccModelDev& m, double speed);
+__device__ inline bool frequency_bound_exact(const MccModelDev& m, double speed);
 
-__device__ __forceinline__ bool frequency_bound_ok(const MccModelDev& m, double speed) {
+__device__ __forceinline__ bool frequency_bound_binned(const MccModelDev& m, double speed) {
     if (speed <= m.v_safe) return true;
     if (m.safe_bins) {
         const double f = speed * m.safe_inv_dv;
         if (f < (double)m.nsafe && __ldg(m.safe_bins + (int)f)) return true;
     }
+    return false;
+}
+
+__device__ __forceinline__ bool frequency_bound_ok(const MccModelDev& m, double speed) {
+    return frequency_bound_binned(m, speed) || frequency_bound_exact(m, speed);
+}
+
+// The same check with the evaluated part out of line, for kernels whose model
+// lives in global memory (an out-of-line call on a kernel-parameter model
+// would copy it to local memory).
+static __device__ __noinline__ bool frequency_bound_exact_far(const MccModelDev& m, double speed) {
     return frequency_bound_exact(m, speed);
 }
 
+__device__ __forceinline__ bool frequency_bound_ok_far(const MccModelDev& m, double speed) {
+    return frequency_bound_binned(m, speed) || frequency_bound_exact_far(m, speed);
+}
+
 // validate_frequency_bound, src/Collision.cpp:627-685, evaluated
-static __device__ __noinline__ bool frequency_bound_exact(const MccModelDev& m, double speed) {
+__device__ inline bool frequency_bound_exact(const MccModelDev& m, double speed) {
     double rates[kMaxChannels];
     if (m.neutral_stddev == 0.0) return rates_for_speed(m, speed, rates);
     const double limit = kThermalSigma * m.neutral_stddev;

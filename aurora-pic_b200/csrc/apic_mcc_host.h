@@ -140,6 +140,45 @@ inline TableIndex build_index(const double* e, size_t rows, DeviceArena& arena) 
     return ix;
 }
 
+// The first waiting time -log(u) / nu (src/Collision.cpp:926-933) falls inside
+// the step (< dt) exactly when u >= u*, and u = draw / 2^64 (libstdc++'s
+// generate_canonical on a 64-bit draw, values rounding to 1 replaced by the
+// largest double below 1) is at least u* exactly when the draw is at least
+// D*.  Both thresholds are found by bisection with the host's log, the one
+// the CPU restatement uses.
+inline void draw_threshold(double nu, double dt, uint64_t& dmin, int& none) {
+    auto wait = [nu](double u) { return -std::log(u) / nu; };
+    const double umax = std::nextafter(1.0, 0.0);
+    none = 0;
+    dmin = 0;
+    if (!(wait(umax) < dt)) { none = 1; return; }
+    uint64_t lo = 1, hi;  // bit patterns: wait(lo) >= dt > wait(hi)
+    std::memcpy(&hi, &umax, 8);
+    {
+        double x;
+        std::memcpy(&x, &lo, 8);
+        if (wait(x) < dt) { dmin = 1; return; }
+    }
+    while (hi - lo > 1) {
+        const uint64_t mid = lo + (hi - lo) / 2;
+        double x;
+        std::memcpy(&x, &mid, 8);
+        if (wait(x) < dt) hi = mid; else lo = mid;
+    }
+    double ustar;
+    std::memcpy(&ustar, &hi, 8);
+    auto canon = [umax](uint64_t d) {
+        double r = (double)d / 18446744073709551616.0;
+        return r >= 1.0 ? umax : r;
+    };
+    uint64_t a = 0, b = ~0ull;  // canon(a) < u* <= canon(b)
+    while (b - a > 1) {
+        const uint64_t mid = a + (b - a) / 2;
+        if (canon(mid) >= ustar) b = mid; else a = mid;
+    }
+    dmin = b;
+}
+
 // Range maxima of a table column in O(1) after an O(n log n) build.
 struct SparseMax {
     std::vector<std::vector<double>> t;

@@ -69,6 +69,13 @@ struct ReplayStream {
 // generate_canonical<double, 53|64> on a 64-bit engine (libstdc++
 // <bits/random.tcc>): one draw, divided by 2^64, results that round to 1
 // become nextafter(1, 0).
+// generate_canonical of one given 64-bit draw
+__device__ inline double canonical_of(uint64_t draw) {
+    double ret = (double)draw / 18446744073709551616.0;
+    if (ret >= 1.0) ret = 0x1.fffffffffffffp-1;
+    return ret;
+}
+
 template <class S>
 __device__ inline double canonical(S& s) {
     const double sum = (double)s.next();

@@ -93,6 +93,10 @@ struct SpeciesDev {
     double qm, hqm, qw, qwdx, mass, weight;
     int model;
     unsigned capacity;
+    // MCC first waiting time inside the step exactly when the first 64-bit
+    // draw is >= cand_draw_min (see draw_threshold); no_candidates: never
+    uint64_t cand_draw_min;
+    int no_candidates;
     // Layout: the live particles, in logical order, are the concatenation of
     // ranges r = 0..nranges-1 of physical slots [start[r], start[r] + count[r]);
     // lstart[r] is the logical index of a range's first particle.
@@ -236,7 +240,7 @@ struct CandidateEntry {
 constexpr int kQueue = 384;
 
 template <int VDIM, bool DIRICHLET>
-__global__ void __launch_bounds__(kThreads, 3) k_pass1d(Params1D p) {
+__global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
     unsigned long long* sRho = reinterpret_cast<unsigned long long*>(sE + p.nx);
@@ -306,12 +310,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_pass1d(Params1D p) {
                 if (mcc) {
                     const MccModelDev& M = p.model[S.model];
                     // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
-                    if (!frequency_bound_ok(M, norm3(vc[k], vy[k], vz[k]))) atomicOr(&st->error, kErrMajorant);
+                    const double s2 = vc[k] * vc[k] + vy[k] * vy[k] + vz[k] * vz[k];
+                    if (!(s2 <= M.v_safe2) && !frequency_bound_ok(M, sqrt(s2))) atomicOr(&st->error, kErrMajorant);
                     PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
-                    double u = uniform01(rng);
-                    for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
-                    const double wait = -log(u) / M.max_frequency;
-                    if (isfinite(wait) && wait < p.dt) {
+                    const uint64_t d0 = rng.next();
+                    // the raw-draw threshold decides exactly as -log(u)/nu < dt would
+                    bool cand = d0 != 0ull ? (!S.no_candidates && d0 >= S.cand_draw_min) : true;
+                    double wait = 0.0;
+                    if (cand) {
+                        double u = d0 != 0ull ? canonical_of(d0) : 0.0;
+                        for (int guard = 0; !(u > 0.0) && guard < 64; ++guard) u = uniform01(rng);
+                        wait = -log(u) / M.max_frequency;
+                        cand = isfinite(wait) && wait < p.dt;
+                    }
+                    if (cand) {
                         const unsigned q = atomicAdd(&s_qlen, 1u);
                         if (q < (unsigned)kQueue) {
                             CandidateEntry& ce = s_queue[q];
@@ -580,15 +592,39 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         nb = kMaxBirths;
     }
     if (nb > 0) {
-        unsigned long long keys[kPostItems];
         int idx[kPostItems];
+        if (nb <= (unsigned)kPostThreads) {
+            // a few products (the usual case): each finds its rank by counting
+            // the smaller keys, one key per thread
+            __shared__ unsigned long long s_keys[kPostThreads];
+            __shared__ int s_order[kPostThreads];
+            if (tid < (int)nb) s_keys[tid] = p.births[tid].key;
+            __syncthreads();
+            if (tid < (int)nb) {
+                const unsigned long long key = s_keys[tid];
+                unsigned r = 0;
+                for (unsigned q = 0; q < nb; ++q) {
+                    const unsigned long long o = s_keys[q];
+                    r += (o < key || (o == key && q < (unsigned)tid)) ? 1u : 0u;
+                }
+                s_order[r] = tid;
+            }
+            __syncthreads();
 #pragma unroll
-        for (int k = 0; k < kPostItems; ++k) {
-            const unsigned i = tid * kPostItems + k;
-            keys[k] = i < nb ? p.births[i].key : ~0ull;
-            idx[k] = (int)i;
+            for (int k = 0; k < kPostItems; ++k) {
+                const unsigned rank = tid * kPostItems + k;
+                idx[k] = rank < nb ? s_order[rank] : 0;
+            }
+        } else {
+            unsigned long long keys[kPostItems];
+#pragma unroll
+            for (int k = 0; k < kPostItems; ++k) {
+                const unsigned i = tid * kPostItems + k;
+                keys[k] = i < nb ? p.births[i].key : ~0ull;
+                idx[k] = (int)i;
+            }
+            Sort(tmp.sort).Sort(keys, idx);
         }
-        Sort(tmp.sort).Sort(keys, idx);
         __syncthreads();
         double bx[kPostItems], bvh[kPostItems], bv[kPostItems][3];
         int bs[kPostItems];
@@ -1091,6 +1127,7 @@ struct Sim1D {
             build_model(m, c.species[m.species].mass, arena, p.model[mi]);
             neutral_stddev[mi] = p.model[mi].neutral_stddev;
             p.sp[m.species].model = mi;
+            draw_threshold(m.max_frequency, c.dt, p.sp[m.species].cand_draw_min, p.sp[m.species].no_candidates);
             APIC_CUDA(cudaStreamSynchronize(stream));  // host tables may be freed after create
         }
         p.E = dalloc<double>(c.nx);
