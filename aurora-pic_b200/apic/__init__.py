@@ -330,6 +330,18 @@ class Simulation1D:
         return lib().apic_sim1d_step_count(self.h)
 
 
+def step_group(sims, nsteps=1):
+    """Steps several Simulation1D runs together (their work overlaps on the GPU)."""
+    arr = (C.c_void_p * len(sims))(*[s.h for s in sims])
+    rc = lib().apic_sim1d_step_group(arr, len(sims), nsteps)
+    if rc != 0:
+        for s in sims:
+            msg = lib().apic_sim1d_last_error(s.h)
+            if msg:
+                raise ApicError(rc, msg.decode())
+        raise ApicError(rc, "step_group failed")
+
+
 def deposit_solve_gather_1d(boundary, nx, length, permittivity, phi_left, phi_right, charges, weights, xs, xq=None):
     ns = len(xs)
     xs = [np.ascontiguousarray(x, dtype=np.float64) for x in xs]

@@ -1017,8 +1017,18 @@ struct Sim1D {
         return static_cast<T*>(ptr);
     }
 
+    // graphs of two steady steps (collision part pending), one per buffer parity
+    cudaGraphExec_t pair_exec[2] = {nullptr, nullptr};
+    int blocks_cache = 0;
+
+    void drop_graphs() {
+        for (auto& g : pair_exec)
+            if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    }
+
     ~Sim1D() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (void* a : allocations) cudaFree(a);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1209,12 +1219,14 @@ struct Sim1D {
         return q;
     }
 
-    int grid_blocks() const {
+    int grid_blocks() {
+        if (blocks_cache) return blocks_cache;
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         size_t tiles = 0;
         for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
-        return (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 4));
+        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 4));
+        return blocks_cache;
     }
 
     // Optional per-kernel timing (CUDA events on the handle's stream).
@@ -1350,6 +1362,29 @@ struct Sim1D {
         launch_pass(kModeDeposit, kPostSolve);
         pending = false;
         initialized = true;
+    }
+
+    // Two steps with the collision part of the previous step pending, as one
+    // CUDA graph launch (kernel parameters depend only on the buffer parity).
+    void steady_pair() {
+        const int par = parity;
+        if (!pair_exec[par]) {
+            const bool t = timing;
+            timing = false;
+            cudaGraph_t g = nullptr;
+            APIC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            const unsigned mode = kModeSyncMcc | kModeKickDrift | kModeDeposit;
+            launch_pass(mode, kPostSolve | kPostAdvance | kPostPushBirths);
+            launch_pass(mode, kPostSolve | kPostAdvance | kPostPushBirths);
+            timing = t;
+            APIC_CUDA(cudaStreamEndCapture(stream, &g));
+            const cudaError_t e = cudaGraphInstantiate(&pair_exec[par], g, 0);
+            cudaGraphDestroy(g);
+            APIC_CUDA(e);
+        }
+        APIC_CUDA(cudaGraphLaunch(pair_exec[par], stream));
+        time += 2.0 * cfg.dt;
+        step += 2;
     }
 
     void do_steps(size_t nsteps) {
@@ -1552,6 +1587,41 @@ int apic_sim1d_resume(apic_sim1d* sim, double time, uint64_t step) {
 int apic_sim1d_step(apic_sim1d* sim, size_t nsteps) {
     if (!sim) return APIC_ERR_INVALID;
     return guarded(sim, [&] { sim->impl.do_steps(nsteps); });
+}
+
+int apic_sim1d_step_group(apic_sim1d* const* sims, size_t n, size_t nsteps) {
+    if (!sims) return APIC_ERR_INVALID;
+    for (size_t i = 0; i < n; ++i)
+        if (!sims[i]) return APIC_ERR_INVALID;
+    std::vector<size_t> left(n, nsteps);
+    // bring every run to the steady state (collision part pending) one step at a time
+    for (size_t i = 0; i < n; ++i) {
+        if (!left[i] || sims[i]->impl.pending) continue;
+        const int rc = guarded(sims[i], [&] { sims[i]->impl.do_steps(1); });
+        if (rc != APIC_OK) return rc;
+        --left[i];
+    }
+    // then two steps per graph launch, round robin over the runs' streams
+    for (bool more = true; more;) {
+        more = false;
+        for (size_t i = 0; i < n; ++i) {
+            if (left[i] < 2) continue;
+            const int rc = guarded(sims[i], [&] {
+                apic::Sim1D& S = sims[i]->impl;
+                apic::require(S.initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
+                if (S.timing) S.do_steps(2); else S.steady_pair();
+            });
+            if (rc != APIC_OK) return rc;
+            left[i] -= 2;
+            more = more || left[i] >= 2;
+        }
+    }
+    for (size_t i = 0; i < n; ++i) {
+        if (!left[i]) continue;
+        const int rc = guarded(sims[i], [&] { sims[i]->impl.do_steps(left[i]); });
+        if (rc != APIC_OK) return rc;
+    }
+    return APIC_OK;
 }
 
 int apic_sim1d_synchronize(apic_sim1d* sim) {

@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ccp1d", choices=["ccp1d", "plasma2d", "plasma3d", "swarm"])
     ap.add_argument("--requests", type=int, default=96, help="swarm: requests in the Poisson serving phase")
+    ap.add_argument("--batch", type=int, default=8, help="ccp1d: discharges stepped together for the batched line")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--cells", type=int, default=None, help="cells per axis")
@@ -412,7 +413,9 @@ def bench_ccp1d(args, rank, dist):
     achieved = bytes_per_pstep * mean_n / (per_pass_ms * 1e-3) / 1e9
     traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md")
     sim.close()
+    batched = _batched_ccp(args, rank) if args.batch > 1 else None
     return {
+        "batched": batched,
         "value": value, "ms_per_step": ms_max / args.steps, "dtype": "f64",
         "config": {"workload": WORKLOAD_CCP, "particles": int(mean_n),
                    "form": "FP64 particles (bit-faithful arithmetic)", "l2": "flushed between timed steps"},
@@ -425,6 +428,48 @@ def bench_ccp1d(args, rank, dist):
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
     }
+
+
+def _batched_ccp(args, rank):
+    """`args.batch` independent discharges stepped together through
+    apic_sim1d_step_group (their kernels overlap on the GPU): aggregate
+    particle-steps/s, device time from one event before the launches to the
+    last run's end event (host launch time included)."""
+    import torch
+    import apic
+    from apic import workloads as W
+    sims = []
+    for k in range(args.batch):
+        wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=100 + 31 * rank + k)
+        cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=5000 + 31 * rank + k)
+        sim = apic.Simulation1D(cfg, tabs)
+        for i, s in enumerate(wl.species):
+            sim.load(i, s.x, s.v, None, s.vy, s.vz)
+        sim.initialize()
+        sims.append((sim, tabs))
+    group = [s for s, _ in sims]
+    apic.step_group(group, max(args.warmup, 4))
+    for s in group:
+        s.synchronize()
+    n0 = sum(s.count(i) for s in group for i in range(2))
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    start.record()
+    apic.step_group(group, args.steps)
+    ends = []
+    for s in group:
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(torch.cuda.ExternalStream(s.cuda_stream()))
+        ends.append(e)
+    torch.cuda.synchronize()
+    ms = max(start.elapsed_time(e) for e in ends)
+    n1 = sum(s.count(i) for s in group for i in range(2))
+    for s in group:
+        s.close()
+    psteps = args.steps * 0.5 * (n0 + n1)
+    return {"decks": args.batch, "value": psteps / (ms * 1e-3), "unit": "particle-steps/s",
+            "ms_per_step": ms / args.steps, "form": "FP64 particles, runs stepped together (apic_sim1d_step_group)",
+            "l2": f"{args.batch} discharges' state larger than L2"}
 
 
 def bench_plasma(args, rank, dist):
@@ -700,6 +745,10 @@ def main():
         }
         if "swarm" in part:
             line["swarm"] = part["swarm"]
+        if part.get("batched"):
+            b = dict(part["batched"])
+            b["vs_single_run"] = b["value"] / part["value"]
+            line["batched"] = b
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

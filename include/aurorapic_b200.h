@@ -215,6 +215,12 @@ APIC_EXPORT int apic_sim1d_resume(apic_sim1d* sim, double time, uint64_t step);
  * Asynchronous: returns after enqueueing; errors surface at the next
  * synchronising call. */
 APIC_EXPORT int apic_sim1d_step(apic_sim1d* sim, size_t nsteps);
+/* Steps n independent runs nsteps each, their work overlapping on the GPU:
+ * every run has its own stream, and steady steps go out two per CUDA graph
+ * launch, round robin over the runs.  No reference counterpart (the
+ * reference steps one Simulation at a time); each run's result is the one
+ * apic_sim1d_step would give.  Asynchronous, like apic_sim1d_step. */
+APIC_EXPORT int apic_sim1d_step_group(apic_sim1d* const* sims, size_t n, size_t nsteps);
 
 /* Waits (bounded) for the handle's stream and returns the device error word. */
 APIC_EXPORT int apic_sim1d_synchronize(apic_sim1d* sim);
