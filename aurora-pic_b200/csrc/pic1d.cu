@@ -211,16 +211,24 @@ __device__ __forceinline__ void deposit_contrib(const Cic& c, const SpeciesDev& 
 
 // ---- range-table layout -----------------------------------------------------
 
-// Physical slot of logical particle `idx`: the range containing it is found by
-// binary search over the ranges' logical starts.
-__device__ __forceinline__ unsigned physical_slot(const unsigned* lstart, const unsigned* start, unsigned nr,
-                                                  unsigned idx) {
-    unsigned lo = 0, hi = nr;  // last range with lstart <= idx
+// The range holding logical particle `idx`: the last range whose logical
+// start is <= idx, by binary search over the ranges' logical starts.
+__device__ __forceinline__ unsigned range_of(const unsigned* lstart, unsigned nr, unsigned idx) {
+    unsigned lo = 0, hi = nr;
     while (hi - lo > 1) {
         const unsigned mid = (lo + hi) >> 1;
         if (__ldg(lstart + mid) <= idx) lo = mid; else hi = mid;
     }
-    return __ldg(start + lo) + (idx - __ldg(lstart + lo));
+    return lo;
+}
+
+// Physical slot of logical particle `idx`, walking forward from range r0
+// (a range at or before the one holding idx): a tile spans few ranges.
+__device__ __forceinline__ unsigned physical_slot_from(const unsigned* lstart, const unsigned* start, unsigned nr,
+                                                       unsigned r0, unsigned idx) {
+    unsigned r = r0;
+    while (r + 1 < nr && __ldg(lstart + r + 1) <= idx) ++r;
+    return __ldg(start + r) + (idx - __ldg(lstart + r));
 }
 
 // ---- the fused particle pass -----------------------------------------------
@@ -274,6 +282,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
         const unsigned nr = st->nranges[s];
         const unsigned base = tile * kTile;
         const bool mcc = (mode & kModeSyncMcc) && S.model >= 0 && VDIM == 3;
+        // one search per warp for the range of its first particle
+        const unsigned wfirst = base + (unsigned)(tid & ~31);
+        unsigned r0 = 0;
+        if (lane == 0 && wfirst < n) r0 = range_of(S.rlstart[0], nr, wfirst);
+        r0 = __shfl_sync(0xffffffffu, r0, 0);
 
         double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems], Ek[kItems];
         bool keep[kItems];
@@ -284,7 +297,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
             const bool live = idx < n;
             keep[k] = live;
             queued[k] = -1;
-            const unsigned ph = live ? physical_slot(S.rlstart[0], S.rstart[0], nr, idx) : 0u;
+            const unsigned ph = live ? physical_slot_from(S.rlstart[0], S.rstart[0], nr, r0, idx) : 0u;
             x[k] = live ? S.x[0][ph] : 0.0;
             vh[k] = live ? S.vh[0][ph] : 0.0;
             vy[k] = (VDIM == 3 && live) ? S.vy[0][ph] : 0.0;
@@ -1225,7 +1238,8 @@ struct Sim1D {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         size_t tiles = 0;
         for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
-        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 4));
+        // one resident wave: k_pass1d runs two CTAs per SM
+        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 2));
         return blocks_cache;
     }
 
