@@ -340,7 +340,8 @@ __device__ __forceinline__ void gather32(const ParamsND& p, int ix, int iy, int 
     const float wx[2] = {1.0f - f[0], f[0]}, wy[2] = {1.0f - f[1], f[1]};
     if (DIM == 2) {
         const float2* E = reinterpret_cast<const float2*>(p.E32);
-        const float2 a = E[iy * nx + ix], b = E[iy * nx + ix1], c = E[iy1 * nx + ix], d = E[iy1 * nx + ix1];
+        const float2 a = __ldg(E + iy * nx + ix), b = __ldg(E + iy * nx + ix1), c = __ldg(E + iy1 * nx + ix),
+                     d = __ldg(E + iy1 * nx + ix1);
         const float w00 = wx[0] * wy[0], w10 = wx[1] * wy[0], w01 = wx[0] * wy[1], w11 = wx[1] * wy[1];
         e[0] = fmaf(a.x, w00, fmaf(b.x, w10, fmaf(c.x, w01, d.x * w11)));
         e[1] = fmaf(a.y, w00, fmaf(b.y, w10, fmaf(c.y, w01, d.y * w11)));
@@ -360,7 +361,7 @@ __device__ __forceinline__ void gather32(const ParamsND& p, int ix, int iy, int 
 #pragma unroll
                 for (int a = 0; a < 2; ++a) {
                     const float w = wx[a] * wyz;
-                    const float4 v = E[row + xx[a]];
+                    const float4 v = __ldg(E + row + xx[a]);
                     e[0] = fmaf(v.x, w, e[0]);
                     e[1] = fmaf(v.y, w, e[1]);
                     e[2] = fmaf(v.z, w, e[2]);
@@ -393,16 +394,19 @@ __device__ __forceinline__ void advance(float& f, int& i, float disp, int n) {
 
 // Runs of lanes that share a cell (particles are sorted by cell) add their
 // 2^-25-quantised weights with a converged segmented shuffle scan; runs are
-// capped at 8 lanes so three shuffle steps suffice.  The last lane of each run
-// commits its sums with one 64-bit atomic per node.
+// capped at SEG lanes (32 x 2^25 < 2^32, so a run's sum fits 32 bits): SEG = 32
+// where a warp usually sits in one or two cells (2D, 64 particles per cell),
+// 8 where it spans several (3D).  The last lane of each run commits its sums
+// with one 64-bit atomic per node.
 template <int DIM>
 __device__ __forceinline__ void deposit32_warp(const ParamsND& p, unsigned long long* acc, bool valid, int ix, int iy,
                                                int iz, const float f[3]) {
+    constexpr int SEG = DIM == 2 ? 32 : 8;
     const int lane = threadIdx.x & 31;
     const int nx = p.n[0], ny = p.n[1];
     const unsigned key = valid ? (((unsigned)iz * ny + iy) * nx + ix) : 0xFFFFFFFFu;
     const unsigned prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const bool head = (lane & 7) == 0 || prev != key;
+    const bool head = (lane & (SEG - 1)) == 0 || prev != key;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
     const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
     const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
@@ -419,7 +423,7 @@ __device__ __forceinline__ void deposit32_warp(const ParamsND& p, unsigned long 
             for (int a = 0; a < 2; ++a) {
                 unsigned q = valid ? (unsigned)__float2int_rn(wx[a] * wy[b] * wz[c] * kWeightScale) : 0u;
 #pragma unroll
-                for (int d = 1; d < 8; d <<= 1) {
+                for (int d = 1; d < SEG; d <<= 1) {
                     const unsigned t = __shfl_up_sync(0xffffffffu, q, d);
                     if (lane - d >= start) q += t;
                 }
@@ -436,10 +440,10 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
         return;  // whole warp past the end
     int ix = 0, iy = 0, iz = 0;
     float f[3] = {0.0f, 0.0f, 0.0f}, v[3] = {0.0f, 0.0f, 0.0f};
-    if (valid) {
-        unpack_cell(S.cell[buf][i], ix, iy, iz);
-        for (int a = 0; a < DIM; ++a) f[a] = S.off[buf][a][i];
-        for (int a = 0; a < 3; ++a) v[a] = S.vel[buf][a][i];
+    if (valid) {  // streamed once per step: evict-first, so L1 keeps the field
+        unpack_cell(__ldcs(&S.cell[buf][i]), ix, iy, iz);
+        for (int a = 0; a < DIM; ++a) f[a] = __ldcs(&S.off[buf][a][i]);
+        for (int a = 0; a < 3; ++a) v[a] = __ldcs(&S.vel[buf][a][i]);
     }
     if (MODE == kPushStep || MODE == kPushInitHalf || MODE == kPushSync) {
         float e[3] = {0.0f, 0.0f, 0.0f};
@@ -474,9 +478,9 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
         int* idx[3] = {&ix, &iy, &iz};
         for (int a = 0; a < DIM; ++a) advance(f[a], *idx[a], v[a] * S.drift[a], p.n[a]);
         if (valid) {
-            S.cell[buf][i] = pack_cell(ix, iy, iz);
-            for (int a = 0; a < DIM; ++a) S.off[buf][a][i] = f[a];
-            for (int a = 0; a < 3; ++a) S.vel[buf][a][i] = v[a];
+            __stcs(&S.cell[buf][i], pack_cell(ix, iy, iz));
+            for (int a = 0; a < DIM; ++a) __stcs(&S.off[buf][a][i], f[a]);
+            for (int a = 0; a < 3; ++a) __stcs(&S.vel[buf][a][i], v[a]);
         }
     }
     // ---- deposit ----
