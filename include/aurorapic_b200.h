@@ -2,7 +2,7 @@
  * aurorapic_b200.h - C ABI of the B200-native electrostatic PIC particle step.
  *
  * Drop-in boundary for AuroraPIC's structured-grid particle step.  The
- * reference is a C++ library (include/pic/*.hpp); each entry point below names
+ * reference is a C++ library (the headers under include/pic/); each entry point below names
  * the reference interface it replaces.  All entry points:
  *   - take plain pointers and sizes (host memory unless stated otherwise),
  *   - never throw and never retain caller memory after returning,

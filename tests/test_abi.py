@@ -86,3 +86,25 @@ def test_swarm_request_validation_on_cpu():
         pytest.skip("checks the no-device path")
     with pytest.raises(apic.ApicError):
         apic.swarm_run(cfg, gas, [10.0])
+
+
+def build_facade_check(tmp_path):
+    import subprocess
+    exe = tmp_path / "facade_check"
+    subprocess.run(["g++", "-std=c++20", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "facade_check.cpp"), "-L", os.path.dirname(apic.library_path()),
+                    "-laurorapic_b200", "-Wl,-rpath," + os.path.dirname(apic.library_path()), "-o", str(exe)],
+                   check=True)
+    return exe
+
+
+def test_cpp20_facade_compiles_and_maps_errors(tmp_path):
+    """The C++20 facade (include/aurorapic_b200.hpp) builds against the
+    library; without a device, creation raises runtime_error and a bad
+    configuration keeps the reference's invalid_argument."""
+    import subprocess
+    if apic.lib().apic_device_count() > 0:
+        pytest.skip("checks the no-device path")
+    out = subprocess.run([str(build_facade_check(tmp_path))], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "invalid_argument: simulation dt must be positive and finite" in out.stdout

@@ -222,3 +222,11 @@ def test_step_group_matches_individual_steps():
                 assert np.array_equal(a[key], b[key]), key
         for x, y in zip(g.fields(), s.fields()):
             assert np.array_equal(x, y)
+
+
+def test_cpp20_facade_on_the_device(tmp_path):
+    import subprocess
+    from test_abi import build_facade_check
+    out = subprocess.run([str(build_facade_check(tmp_path))], capture_output=True, text=True)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "device step=3 live=8" in out.stdout
