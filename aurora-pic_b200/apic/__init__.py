@@ -631,6 +631,8 @@ def _bind_swarm():
     L.apic_swarm_server_submit.argtypes = [P, C.POINTER(SwarmRequest), C.POINTER(C.c_uint64)]
     L.apic_swarm_server_advance.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.apic_swarm_server_poll.argtypes = [P, C.c_uint64, C.POINTER(SwarmResult), C.POINTER(C.c_int)]
+    L.apic_swarm_server_launch.argtypes = [P]
+    L.apic_swarm_server_complete.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.apic_swarm_server_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)]
     L.apic_swarm_server_cuda_stream.argtypes = [P, C.POINTER(P)]
     L.apic_swarm_server_set_kernel_timing.argtypes = [P, C.c_int]
@@ -684,6 +686,16 @@ class SwarmServer:
     def advance(self):
         a, q = C.c_int(), C.c_int()
         _check_swarm(_bind_swarm().apic_swarm_server_advance(self.h, C.byref(a), C.byref(q)), self.h)
+        return a.value, q.value
+
+    def launch(self):
+        """First half of advance(): enqueue the batch's steps and return."""
+        _check_swarm(_bind_swarm().apic_swarm_server_launch(self.h), self.h)
+
+    def complete(self):
+        """Second half: wait, retire finished runs; returns (active, queued)."""
+        a, q = C.c_int(), C.c_int()
+        _check_swarm(_bind_swarm().apic_swarm_server_complete(self.h, C.byref(a), C.byref(q)), self.h)
         return a.value, q.value
 
     def poll(self, rid):

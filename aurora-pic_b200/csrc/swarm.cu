@@ -854,6 +854,7 @@ struct Server {
 
     ~Server() {
         if (stream) cudaStreamSynchronize(stream);
+        if (h_st_pinned) cudaFreeHost(h_st_pinned);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
         for (void* a : allocations) cudaFree(a);
@@ -1298,7 +1299,18 @@ struct Server {
 
     // One serving iteration: admit, run steps_per_launch steps of every active
     // run (one graph launch), read the run states, retire finished runs.
+    // advance = launch + complete; between the two the host may queue other
+    // work (other streams) that overlaps this batch on the GPU.
     void advance(int* active_out, int* queued_out) {
+        launch();
+        complete(active_out, queued_out);
+    }
+
+    RunState* h_st_pinned = nullptr;  // async read-back target of the run states
+    bool launched = false;
+
+    void launch() {
+        require(!launched, "launch() while a launched batch has not completed", APIC_ERR_STATE);
         admit();
         if (tables_dirty) rebuild_tables();
         int active = 0;
@@ -1358,11 +1370,20 @@ struct Server {
                 APIC_CUDA(cudaGraphLaunch(graph_exec, stream));
             }
             ++launches;
-            APIC_CUDA(cudaMemcpyAsync(h_st.data(), d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
+            if (!h_st_pinned) APIC_CUDA(cudaMallocHost(&h_st_pinned, h_st.size() * sizeof(RunState)));
+            APIC_CUDA(cudaMemcpyAsync(h_st_pinned, d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
                                       stream));
+            launched = true;
+        }
+    }
+
+    void complete(int* active_out, int* queued_out) {
+        if (launched) {
+            launched = false;
             const cudaError_t w = bounded_wait(stream, 600.0);
             if (w == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "swarm step did not complete in time");
             APIC_CUDA(w);
+            std::memcpy(h_st.data(), h_st_pinned, h_st.size() * sizeof(RunState));
             for (int s = 0; s < conf.max_runs; ++s) {
                 Run& run = runs[s];
                 if (!run.used) continue;
@@ -1376,7 +1397,7 @@ struct Server {
                 }
             }
         }
-        active = 0;
+        int active = 0;
         for (int s = 0; s < conf.max_runs; ++s) active += runs[s].used ? 1 : 0;
         if (active_out) *active_out = active;
         if (queued_out) *queued_out = (int)queue.size();
@@ -1462,6 +1483,16 @@ int apic_swarm_server_submit(apic_swarm_server* srv, const apic_swarm_request* r
 int apic_swarm_server_advance(apic_swarm_server* srv, int* active, int* queued) {
     if (!srv) return APIC_ERR_INVALID;
     return guarded_swarm(srv, [&] { srv->impl.advance(active, queued); });
+}
+
+int apic_swarm_server_launch(apic_swarm_server* srv) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] { srv->impl.launch(); });
+}
+
+int apic_swarm_server_complete(apic_swarm_server* srv, int* active, int* queued) {
+    if (!srv) return APIC_ERR_INVALID;
+    return guarded_swarm(srv, [&] { srv->impl.complete(active, queued); });
 }
 
 int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic_swarm_result* out, int* done) {

@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ccp1d", choices=["ccp1d", "plasma2d", "plasma3d", "swarm"])
     ap.add_argument("--requests", type=int, default=96, help="swarm: requests in the Poisson serving phase")
+    ap.add_argument("--mixed-requests", type=int, default=64,
+                    help="swarm: swarm requests of the mixed phase (two-stream decks arrive at half that rate)")
     ap.add_argument("--batch", type=int, default=8, help="ccp1d: discharges stepped together for the batched line")
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--ppc", type=int, default=None)
@@ -586,6 +588,95 @@ def _swarm_draw(rng, spec, W, k, seed_base):
     return W.swarm_request(spec, td, particles=n, seed=seed_base + k, steps=20000, burn_in_steps=2000, tolerance=0.01)
 
 
+def _mixed_serving(args, srv, spec, rng, rate, rank):
+    """Swarm requests (Poisson, `rate`) mixed with small 1D two-stream decks
+    (Poisson at rate / 2; Nx log-uniform over 64..1024, 64 particles per cell
+    per beam, 2000 steps).  The swarm batch's graph and the decks' steps
+    overlap on the GPU: each iteration launches the swarm batch, steps the
+    active decks (apic_sim1d_step_group on their own streams), then completes
+    the swarm batch.  Decks come from a pool created up front (no device
+    allocation while serving)."""
+    import numpy as np
+    import apic
+    from apic import workloads as W
+    nxs = (64, 128, 256, 512, 1024)
+    pool = {nx: [] for nx in nxs}
+    for nx in nxs:
+        for k in range(4):
+            wl = W.two_stream(particles_per_beam=64 * nx, nx=nx, seed=1)
+            cfg, tabs = W.to_device_config(wl, seed=9000 + k)
+            pool[nx].append((apic.Simulation1D(cfg, tabs), tabs))
+    free = {nx: list(range(4)) for nx in nxs}
+    n_sw = args.mixed_requests
+    n_dk = max(1, n_sw // 2)
+    sw_arr = np.cumsum(rng.exponential(1.0 / rate, n_sw))
+    dk_arr = np.cumsum(rng.exponential(2.0 / rate, n_dk))
+    sw_req = [_swarm_draw(rng, spec, W, k, 40_000_000 + 1000 * rank) for k in range(n_sw)]
+    dk_nx = [nxs[int(rng.integers(0, len(nxs)))] for _ in range(n_dk)]
+    deck_steps, per_iter = 2000, 100
+    _, ps0, _ = srv.stats()
+    t0 = time.perf_counter()
+    sw_sub, dk_wait, active = {}, [], []  # active: [sim, nx, slot, arrival, steps]
+    sw_lat, dk_lat = [], []
+    i_sw = i_dk = 0
+    deck_psteps = 0
+    while len(sw_lat) < n_sw or len(dk_lat) < n_dk:
+        now = time.perf_counter() - t0
+        while i_sw < n_sw and sw_arr[i_sw] <= now:
+            sw_sub[srv.submit(sw_req[i_sw])] = sw_arr[i_sw]
+            i_sw += 1
+        while i_dk < n_dk and dk_arr[i_dk] <= now:
+            dk_wait.append((dk_nx[i_dk], dk_arr[i_dk], i_dk))
+            i_dk += 1
+        for item in list(dk_wait):  # admit decks into free pool slots
+            nx, arr, k = item
+            if free[nx]:
+                slot = free[nx].pop()
+                sim = pool[nx][slot][0]
+                wl = W.two_stream(particles_per_beam=64 * nx, nx=nx, seed=500 + k)
+                for sp_i, sp in enumerate(wl.species):
+                    sim.load(sp_i, sp.x, sp.v)
+                sim.initialize()
+                active.append([sim, nx, slot, arr, 0, 2 * 64 * nx])
+                dk_wait.remove(item)
+        srv.launch()
+        if active:
+            apic.step_group([a[0] for a in active], per_iter)
+        srv.complete()
+        now = time.perf_counter() - t0
+        for i in list(sw_sub):
+            r = srv.poll(i)
+            if r is not None:
+                sw_lat.append(now - sw_sub.pop(i))
+        for a in list(active):
+            a[4] += per_iter
+            deck_psteps += per_iter * a[5]
+            if a[4] >= deck_steps:
+                a[0].sample()  # waits for the deck and reads its diagnostics
+                dk_lat.append(time.perf_counter() - t0 - a[3])
+                free[a[1]].append(a[2])
+                active.remove(a)
+        if not sw_sub and not active and not dk_wait:
+            nxt = []
+            if i_sw < n_sw:
+                nxt.append(sw_arr[i_sw])
+            if i_dk < n_dk:
+                nxt.append(dk_arr[i_dk])
+            if nxt:
+                time.sleep(max(0.0, min(nxt) - (time.perf_counter() - t0)))
+    wall = time.perf_counter() - t0
+    _, ps1, _ = srv.stats()
+    for nx in nxs:
+        for sim, _ in pool[nx]:
+            sim.close()
+    sw_lat, dk_lat = np.array(sw_lat), np.array(dk_lat)
+    return {"swarm_requests": n_sw, "deck_requests": n_dk,
+            "swarm_p50_latency_s": float(np.percentile(sw_lat, 50)), "swarm_p99_latency_s": float(np.percentile(sw_lat, 99)),
+            "deck_p50_latency_s": float(np.percentile(dk_lat, 50)), "deck_p99_latency_s": float(np.percentile(dk_lat, 99)),
+            "particle_steps_per_s": ((ps1 - ps0) + deck_psteps) / wall,
+            "decks": "two-stream 1D1V, Nx in 64..1024 (64 particles per cell per beam), 2000 steps, FP64"}
+
+
 def bench_swarm(args, rank, dist):
     """Batched swarm serving: saturation throughput, then Poisson arrivals at
     80% of the measured capacity with p50 / p99 request latency."""
@@ -671,6 +762,7 @@ def bench_swarm(args, rank, dist):
     t_serve = time.perf_counter() - t0
     _, ps3, _ = srv.stats()
     serve_value = (ps3 - ps2) / t_serve
+    mixed = _mixed_serving(args, srv, spec, rng, rate, rank) if args.mixed_requests > 0 else None
     srv.close()
     lat = np.array(lat)
     hbm, peak_kind = peaks()
@@ -687,7 +779,8 @@ def bench_swarm(args, rank, dist):
         "swarm": {"p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                   "capacity_requests_per_s": capacity, "arrival_rate_requests_per_s": rate,
                   "requests": int(args.requests), "converged_fraction": float(np.mean([r.converged for r in results])),
-                  "mean_steps": float(steps_done.mean()), "serving_particle_steps_per_s": serve_value},
+                  "mean_steps": float(steps_done.mean()), "serving_particle_steps_per_s": serve_value,
+                  "mixed": mixed},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm if achieved else None, "traffic": _profiled_traffic("k_swarm_push_c5_fp32.md"),
                      "peak_kind": peak_kind, "kernel": "k_swarm_push<float>",

@@ -480,6 +480,11 @@ APIC_EXPORT void apic_swarm_server_destroy(apic_swarm_server* srv);
 APIC_EXPORT int apic_swarm_server_submit(apic_swarm_server* srv, const apic_swarm_request* req, uint64_t* id);
 /* Admit, step every active run, retire finished runs; waits for the device. */
 APIC_EXPORT int apic_swarm_server_advance(apic_swarm_server* srv, int* active, int* queued);
+/* advance in two halves: launch admits and enqueues the batch's steps and
+ * returns at once; complete waits for them and retires finished runs.  Work
+ * the caller enqueues on other streams in between overlaps the batch. */
+APIC_EXPORT int apic_swarm_server_launch(apic_swarm_server* srv);
+APIC_EXPORT int apic_swarm_server_complete(apic_swarm_server* srv, int* active, int* queued);
 /* done = 1 and *out filled (once) when request id has finished. */
 APIC_EXPORT int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic_swarm_result* out, int* done);
 APIC_EXPORT int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,

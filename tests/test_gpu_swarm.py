@@ -212,3 +212,43 @@ def test_collide_henyey_greenstein_attachment_replay_against_reference():
         assert list(s.channel_collisions)[:4] == list(f["channels"][i])[:4]
         assert s.removed == f["removed"][i]
         assert (s.draws & 0x7FFFFFFF) == f["draws"][i]
+
+
+def test_launch_complete_overlapping_1d_decks_keeps_results():
+    """Launching the swarm batch, stepping 1D decks on their own streams, then
+    completing the batch changes neither the swarm result nor the decks'."""
+    spec = W.swarm_c5(particles=3000, steps=400, burn_in_steps=200)
+    req = W.swarm_request(spec, 150.0, seed=5)
+    alone = _server(spec, spl=40)
+    a_id = alone.submit(req)
+    a = _drain(alone, [a_id])[a_id]
+    alone.close()
+    wl = W.two_stream(particles_per_beam=4096, nx=128, seed=9)
+    decks = []
+    for k in range(2):
+        cfg, tabs = W.to_device_config(wl, seed=3 + k)
+        d = apic.Simulation1D(cfg, tabs)
+        for i, sp in enumerate(wl.species):
+            d.load(i, sp.x, sp.v)
+        d.initialize()
+        decks.append((d, tabs))
+    ref = apic.Simulation1D(*W.to_device_config(wl, seed=3))
+    for i, sp in enumerate(wl.species):
+        ref.load(i, sp.x, sp.v)
+    ref.initialize()
+    mix = _server(spec, spl=40)
+    m_id = mix.submit(req)
+    done, steps = None, 0
+    while done is None:
+        mix.launch()
+        apic.step_group([d for d, _ in decks], 10)
+        steps += 10
+        mix.complete()
+        done = mix.poll(m_id)
+    mix.close()
+    assert _result_tuple(done) == _result_tuple(a)
+    ref.step(steps)
+    for k in range(2):
+        x, y = decks[0][0].particles(k), ref.particles(k)
+        for key in x:
+            assert np.array_equal(x[key], y[key])
