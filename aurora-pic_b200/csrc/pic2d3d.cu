@@ -487,6 +487,57 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
     deposit32_warp<DIM>(p, acc, valid, ix, iy, iz, f);
 }
 
+// The step push of the FP32 form with ITEMS particles per thread: all of the
+// thread's particle loads are issued before the first gather, so each warp
+// keeps ITEMS times the bytes in flight (the single-particle form leaves HBM
+// latency-bound).  Slice k of the CTA is the contiguous block of kThreads
+// particles at base + k * kThreads, so each warp still deposits runs of
+// consecutive (cell-sorted) particles.
+template <int DIM, bool BORIS, int ITEMS>
+__global__ void __launch_bounds__(kThreads) k_push32_step(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
+    const unsigned base = blockIdx.x * (ITEMS * kThreads);
+    const unsigned tid = threadIdx.x;
+    unsigned cl[ITEMS];
+    float fo[ITEMS][3], vv[ITEMS][3];
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        const unsigned i = base + k * kThreads + tid;
+        const bool ok = i < S.n;
+        cl[k] = ok ? __ldcs(&S.cell[buf][i]) : 0u;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            fo[k][a] = (ok && a < DIM) ? __ldcs(&S.off[buf][a][i]) : 0.0f;
+            vv[k][a] = ok ? __ldcs(&S.vel[buf][a][i]) : 0.0f;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        const unsigned i = base + k * kThreads + tid;
+        if (base + k * kThreads + (tid & ~31u) >= S.n) continue;  // whole warp past the end
+        const bool valid = i < S.n;
+        int ix = 0, iy = 0, iz = 0;
+        unpack_cell(cl[k], ix, iy, iz);
+        float* f = fo[k];
+        float* v = vv[k];
+        float e[3] = {0.0f, 0.0f, 0.0f};
+        if (valid) gather32<DIM>(p, ix, iy, iz, f, e);
+        // kick + drift, src/Pusher.cpp:109-128, :162-174
+        if (BORIS) {
+            boris32(v, e, S.hqmdt, S.tb, S.sb);
+        } else {
+            for (int a = 0; a < DIM; ++a) v[a] = fmaf(S.qmdt, e[a], v[a]);
+        }
+        int* idx[3] = {&ix, &iy, &iz};
+        for (int a = 0; a < DIM; ++a) advance(f[a], *idx[a], v[a] * S.drift[a], p.n[a]);
+        if (valid) {
+            __stcs(&S.cell[buf][i], pack_cell(ix, iy, iz));
+            for (int a = 0; a < DIM; ++a) __stcs(&S.off[buf][a][i], f[a]);
+            for (int a = 0; a < 3; ++a) __stcs(&S.vel[buf][a][i], v[a]);
+        }
+        deposit32_warp<DIM>(p, acc, valid, ix, iy, iz, f);
+    }
+}
+
 // FP64 staging <-> FP32 state.  The cell/offset split follows the periodic CIC
 // index of the reference (wrap, divide by the cell size, floor).
 template <int DIM>
@@ -1331,6 +1382,20 @@ struct SimND {
         if (S.n == 0) return;
         const unsigned blocks = (S.n + kThreads - 1) / kThreads;
         const int b = buf[s];
+        if (fp32 && MODE == kPushStep) {
+            constexpr int I2 = 4, I3 = 2;  // particles per thread of the step push
+            const unsigned g2 = (S.n + I2 * kThreads - 1) / (I2 * kThreads);
+            const unsigned g3 = (S.n + I3 * kThreads - 1) / (I3 * kThreads);
+            if (cfg.dims == 2) {
+                if (boris) k_push32_step<2, true, I2><<<g2, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                else k_push32_step<2, false, I2><<<g2, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+            } else {
+                if (boris) k_push32_step<3, true, I3><<<g3, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                else k_push32_step<3, false, I3><<<g3, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+            }
+            APIC_CUDA(cudaGetLastError());
+            return;
+        }
         if (fp32) {
             if (cfg.dims == 2) {
                 if (boris) k_push32<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
