@@ -1383,7 +1383,7 @@ struct SimND {
         const unsigned blocks = (S.n + kThreads - 1) / kThreads;
         const int b = buf[s];
         if (fp32 && MODE == kPushStep) {
-            constexpr int I2 = 4, I3 = 2;  // particles per thread of the step push
+            constexpr int I2 = 4, I3 = 2;  // particles per thread of the step push (measured best)
             const unsigned g2 = (S.n + I2 * kThreads - 1) / (I2 * kThreads);
             const unsigned g3 = (S.n + I3 * kThreads - 1) / (I3 * kThreads);
             if (cfg.dims == 2) {
