@@ -713,6 +713,13 @@ class SwarmServer:
         _check_swarm(_bind_swarm().apic_swarm_server_cuda_stream(self.h, C.byref(s)), self.h)
         return s.value or 0
 
+    def kernel_launches(self) -> int:
+        n = C.c_uint64()
+        L = _bind_swarm()
+        L.apic_swarm_server_kernel_launches.argtypes = [C.c_void_p, C.POINTER(C.c_uint64)]
+        _check_swarm(L.apic_swarm_server_kernel_launches(self.h, C.byref(n)), self.h)
+        return n.value
+
     def set_kernel_timing(self, enable: bool):
         _check_swarm(_bind_swarm().apic_swarm_server_set_kernel_timing(self.h, int(enable)), self.h)
 

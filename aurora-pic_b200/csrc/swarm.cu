@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_swarm_push(Batch b) {
 // ---- one step, collision part: the queued candidates, packed densely -----------
 
 template <class T>
-__global__ void __launch_bounds__(kThreads, 3) k_swarm_collide(Batch b) {
+__global__ void __launch_bounds__(kThreads, 4) k_swarm_collide(Batch b) {
     const unsigned qn = *b.qlen;
     for (unsigned q = blockIdx.x * kThreads + threadIdx.x; q < qn; q += gridDim.x * kThreads) {
         const Candidate e = b.queue[q];
@@ -846,6 +846,7 @@ struct Server {
     cudaGraphExec_t graph_exec = nullptr;
     int push_grid = 0;
     uint64_t launches = 0;
+    uint64_t kernel_launches = 0;  // step kernels launched (graph nodes included)
     uint64_t particle_steps = 0;
     // optional timing of the push kernel (kernels launched one by one, no graph)
     bool timing = false;
@@ -857,6 +858,8 @@ struct Server {
         if (h_st_pinned) cudaFreeHost(h_st_pinned);
         if (graph_exec) cudaGraphExecDestroy(graph_exec);
         if (graph) cudaGraphDestroy(graph);
+        if (graph_exec_fixed) cudaGraphExecDestroy(graph_exec_fixed);
+        if (graph_fixed) cudaGraphDestroy(graph_fixed);
         for (void* a : allocations) cudaFree(a);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -1135,25 +1138,35 @@ struct Server {
     uint32_t nchunks_host_ = 0;
 
     template <class T>
-    void enqueue_step(const Batch& b) {
+    void enqueue_step(const Batch& b, bool branching) {
         k_swarm_push<T><<<push_grid, kThreads, 0, stream>>>(b);
         k_swarm_collide<T><<<push_grid, kThreads, 0, stream>>>(b);
-        k_swarm_branch_scan<<<conf.max_runs, kThreads, 0, stream>>>(b);
-        k_swarm_branch_compact<T><<<push_grid, kThreads, 0, stream>>>(b);
-        k_swarm_branch_resample<T><<<push_grid, kThreads, 0, stream>>>(b);
+        if (branching) {
+            k_swarm_branch_scan<<<conf.max_runs, kThreads, 0, stream>>>(b);
+            k_swarm_branch_compact<T><<<push_grid, kThreads, 0, stream>>>(b);
+            k_swarm_branch_resample<T><<<push_grid, kThreads, 0, stream>>>(b);
+        }
         k_swarm_reduce<<<conf.max_runs, kThreads, 0, stream>>>(b);
     }
 
-    void ensure_graph() {
-        if (graph_exec) return;
+    // Two step graphs: with the branching kernels, for batches holding a
+    // branching run, and without them.
+    cudaGraph_t graph_fixed = nullptr;
+    cudaGraphExec_t graph_exec_fixed = nullptr;
+
+    cudaGraphExec_t ensure_graph(bool branching) {
+        cudaGraph_t& g = branching ? graph : graph_fixed;
+        cudaGraphExec_t& ge = branching ? graph_exec : graph_exec_fixed;
+        if (ge) return ge;
         const Batch b = batch();
         APIC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         for (size_t k = 0; k < conf.steps_per_launch; ++k) {
-            if (fp32) enqueue_step<float>(b);
-            else enqueue_step<double>(b);
+            if (fp32) enqueue_step<float>(b, branching);
+            else enqueue_step<double>(b, branching);
         }
-        APIC_CUDA(cudaStreamEndCapture(stream, &graph));
-        APIC_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+        APIC_CUDA(cudaStreamEndCapture(stream, &g));
+        APIC_CUDA(cudaGraphInstantiate(&ge, g, 0));
+        return ge;
     }
 
     // Finishes a run whose device state says it stopped (steps done, converged
@@ -1365,10 +1378,11 @@ struct Server {
             }
         }
         if (active) {
-            if (!timing) {
-                ensure_graph();
-                APIC_CUDA(cudaGraphLaunch(graph_exec, stream));
-            }
+            bool branching = false;
+            for (int s = 0; s < conf.max_runs; ++s)
+                branching = branching || (runs[s].used && runs[s].cfg.branching);
+            if (!timing) APIC_CUDA(cudaGraphLaunch(ensure_graph(branching), stream));
+            kernel_launches += conf.steps_per_launch * (timing || branching ? 6 : 3);
             ++launches;
             if (!h_st_pinned) APIC_CUDA(cudaMallocHost(&h_st_pinned, h_st.size() * sizeof(RunState)));
             APIC_CUDA(cudaMemcpyAsync(h_st_pinned, d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
@@ -1541,6 +1555,12 @@ int apic_swarm_server_kernel_times(apic_swarm_server* srv, double* push_ms, doub
         if (push_launches) *push_launches = srv->impl.push_launches;
         if (push_bytes) *push_bytes = srv->impl.push_bytes;
     });
+}
+
+int apic_swarm_server_kernel_launches(apic_swarm_server* srv, uint64_t* launches) {
+    if (!srv || !launches) return APIC_ERR_INVALID;
+    *launches = srv->impl.kernel_launches;
+    return APIC_OK;
 }
 
 int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream) {

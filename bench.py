@@ -724,7 +724,9 @@ def bench_swarm(args, rank, dist):
     with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         e0.record(ext)
         g0 = srv.stats()[0]
+        k0 = srv.kernel_launches()
         res = drain(ids)
+        k1 = srv.kernel_launches()
         e1.record(ext)
         e1.synchronize()
     t_sat = e0.elapsed_time(e1) * 1e-3
@@ -787,7 +789,7 @@ def bench_swarm(args, rank, dist):
                      "bytes_per_particle_step": "24 (burn-in) / 48 (sampling)",
                      "push_ms_per_launch": push_ms / max(push_launches, 1),
                      "collide_ms_per_launch": collide_ms / max(push_launches, 1)},
-        "gpu_launches": int((g1 - g0) * spl * 6),
+        "gpu_launches": int(k1 - k0),
         "clocks": clk.summary(),
     }
 

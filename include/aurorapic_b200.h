@@ -490,6 +490,8 @@ APIC_EXPORT int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic
 APIC_EXPORT int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,
                                         size_t* pool_bytes_free);
 APIC_EXPORT int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream);
+/* Step kernels the server has launched (inside its graphs included). */
+APIC_EXPORT int apic_swarm_server_kernel_launches(apic_swarm_server* srv, uint64_t* launches);
 /* Diagnostics: with timing on, advance launches the step kernels one by one
  * (no graph) and times every streaming push and collision launch with CUDA
  * events; kernel_times reports the summed milliseconds of each, the number of
