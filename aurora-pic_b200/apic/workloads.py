@@ -115,6 +115,21 @@ def two_stream(particles_per_beam=16384, nx=256, seed=1, steps=2000) -> Workload
     return Workload1D("two_stream_1d1v", False, 1, False, nx, L, 0.1, sp, steps=steps)
 
 
+def landau(particles=1 << 20, nx=64, k=0.5, alpha=0.05, seed=3, steps=400) -> Workload1D:
+    """1D1V Landau damping in normalized units: Maxwellian electrons (v_th = 1)
+    over an immobile neutralising background, L = 2 pi / k, density
+    1 + alpha cos(k x) from a position displacement, dt = 0.1.  Linear theory at
+    k lambda_D = 0.5: omega = 1.4156 - 0.1533 i."""
+    L = 2 * math.pi / k
+    w = L / particles
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, L, particles)
+    x = np.mod(x + alpha / k * np.sin(k * x), L)
+    v = rng.standard_normal(particles)
+    sp = [SpeciesSpec(-1.0, 1.0, w, particles, x, v, thermal=1.0)]
+    return Workload1D("landau_1d1v", False, 1, False, nx, L, 0.1, sp, steps=steps)
+
+
 def _rate_bound(mass, channels, e_max_ev, neutral_density, neutral_mass, temperature, grid=20001):
     s_max = math.sqrt(2 * e_max_ev * E_CHARGE / mass)
     v = np.linspace(0.0, s_max, grid)
