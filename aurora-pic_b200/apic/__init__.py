@@ -383,6 +383,7 @@ class ConfigND(C.Structure):
         ("units", C.c_int), ("relative_permittivity", C.c_double), ("magnetic_field", C.c_double * 3),
         ("out_of_plane_depth", C.c_double), ("precision", C.c_int), ("sort_interval", C.c_size_t),
         ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
+        ("push_items", C.c_int),
     ]
 
 
@@ -431,7 +432,8 @@ def _check_nd(rc, handle=None):
 
 
 def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), units=NORMALIZED,
-              relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16) -> ConfigND:
+              relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16,
+              push_items=0) -> ConfigND:
     c = ConfigND()
     c.dims = dims
     c.n[:] = list(n) + [1] * (3 - len(n))
@@ -439,6 +441,7 @@ def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), u
     c.dt, c.units, c.relative_permittivity = dt, units, relative_permittivity
     c.magnetic_field[:] = list(magnetic_field)
     c.out_of_plane_depth, c.precision, c.sort_interval = out_of_plane_depth, precision, sort_interval
+    c.push_items = push_items
     c.nspecies = len(species)
     for i, (q, m, w, cap) in enumerate(species):
         c.species[i] = SpeciesCfg(q, m, w, cap)

@@ -1285,6 +1285,9 @@ struct SimND {
         }
         require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
         require(c.nspecies >= 1 && c.nspecies <= APIC_MAX_SPECIES, "species count out of range");
+        require(c.push_items == 0 || c.push_items == 1 || c.push_items == 2 || c.push_items == 4 ||
+                    c.push_items == 8,
+                "push_items must be 0, 1, 2, 4 or 8");
         const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
         require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
         const double depth = c.out_of_plane_depth == 0.0 ? 1.0 : c.out_of_plane_depth;
@@ -1376,6 +1379,18 @@ struct SimND {
 
     SpeciesND view(int s) const { return sp[s]; }
 
+    template <int DIM, bool BORIS>
+    void launch_step32(int items, const SpeciesND& S, int b, int s) {
+        const unsigned g = (unsigned)((S.n + (unsigned)items * kThreads - 1) / ((unsigned)items * kThreads));
+        unsigned long long* acc = solver.F.acc[s];
+        switch (items) {
+            case 1: k_push32_step<DIM, BORIS, 1><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 2: k_push32_step<DIM, BORIS, 2><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 4: k_push32_step<DIM, BORIS, 4><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            default: k_push32_step<DIM, BORIS, 8><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+        }
+    }
+
     template <int MODE>
     void launch_push(int s) {
         const SpeciesND& S = sp[s];
@@ -1383,15 +1398,14 @@ struct SimND {
         const unsigned blocks = (S.n + kThreads - 1) / kThreads;
         const int b = buf[s];
         if (fp32 && MODE == kPushStep) {
-            constexpr int I2 = 4, I3 = 2;  // particles per thread of the step push (measured best)
-            const unsigned g2 = (S.n + I2 * kThreads - 1) / (I2 * kThreads);
-            const unsigned g3 = (S.n + I3 * kThreads - 1) / (I3 * kThreads);
+            // particles per thread: configured, else the measured best (4 in 2D, 2 in 3D)
+            const int items = cfg.push_items ? cfg.push_items : (cfg.dims == 2 ? 4 : 2);
             if (cfg.dims == 2) {
-                if (boris) k_push32_step<2, true, I2><<<g2, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
-                else k_push32_step<2, false, I2><<<g2, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                if (boris) launch_step32<2, true>(items, S, b, s);
+                else launch_step32<2, false>(items, S, b, s);
             } else {
-                if (boris) k_push32_step<3, true, I3><<<g3, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
-                else k_push32_step<3, false, I3><<<g3, kThreads, 0, stream>>>(p, S, b, solver.F.acc[s]);
+                if (boris) launch_step32<3, true>(items, S, b, s);
+                else launch_step32<3, false>(items, S, b, s);
             }
             APIC_CUDA(cudaGetLastError());
             return;

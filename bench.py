@@ -66,7 +66,8 @@ def parse():
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"])
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--cells", type=int, default=None, help="cells per axis")
-    ap.add_argument("--sort-interval", type=int, default=16)
+    ap.add_argument("--sort-interval", type=int, default=0, help="plasma: 0 = chosen by the autotuner")
+    ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner (fixed defaults)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -440,8 +441,24 @@ def _batched_ccp(args, rank):
     import torch
     import apic
     from apic import workloads as W
+    batch = args.batch
+    tuned = None
+    if not args.no_autotune:
+        from apic import autotune
+
+        def make(k):
+            wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=200 + k)
+            cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=7000 + k)
+            sim = apic.Simulation1D(cfg, tabs)
+            for i, s in enumerate(wl.species):
+                sim.load(i, s.x, s.v, None, s.vy, s.vz)
+            sim.initialize()
+            return sim, tabs
+
+        tuned = autotune.tune_group(make, sizes=(2, 4, 8, 16))
+        batch = tuned["runs"]
     sims = []
-    for k in range(args.batch):
+    for k in range(batch):
         wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=100 + 31 * rank + k)
         cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=5000 + 31 * rank + k)
         sim = apic.Simulation1D(cfg, tabs)
@@ -469,9 +486,10 @@ def _batched_ccp(args, rank):
     for s in group:
         s.close()
     psteps = args.steps * 0.5 * (n0 + n1)
-    return {"decks": args.batch, "value": psteps / (ms * 1e-3), "unit": "particle-steps/s",
+    return {"decks": batch, "autotuned": tuned["table"] if tuned else None,
+            "value": psteps / (ms * 1e-3), "unit": "particle-steps/s",
             "ms_per_step": ms / args.steps, "form": "FP64 particles, runs stepped together (apic_sim1d_step_group)",
-            "l2": f"{args.batch} discharges' state larger than L2"}
+            "l2": f"{batch} discharges' state larger than L2"}
 
 
 def bench_plasma(args, rank, dist):
@@ -485,7 +503,13 @@ def bench_plasma(args, rank, dist):
     cells = None if args.cells is None else (args.cells,) * dims
     plan = W.plasma_plan(dims, cells=cells, ppc=args.ppc, seed=11 + 2 * rank)
     prec = apic.FP32 if args.precision == "fp32" else apic.FP64
-    sim = apic.SimulationND(plan.config(precision=prec, sort_interval=args.sort_interval))
+    tuned = None
+    sort_interval, push_items = args.sort_interval or 16, 0
+    if not args.no_autotune and not args.sort_interval:
+        from apic import autotune
+        tuned = autotune.tune_plasma(plan, prec, steps=32)
+        sort_interval, push_items = tuned["sort_interval"], tuned["push_items"]
+    sim = apic.SimulationND(plan.config(precision=prec, sort_interval=sort_interval, push_items=push_items))
     plan.load(sim)
     sim.initialize()
     sim.step(args.warmup)
@@ -559,12 +583,15 @@ def bench_plasma(args, rank, dist):
     per_step_push = push_ms / max(nsteps, 1)
     achieved = bpp * P / (per_step_push * 1e-3) / 1e9
     form = ("FP32 particles: packed int32 cell + FP32 offsets + FP32 velocities; FP64 fixed-point deposit, "
-            "FP64 spectral solve") if prec == apic.FP32 else "FP64 particles (bit-faithful arithmetic)"
+            "FP64 spectral solve; error against the FP64 oracle after 10 steps (tests/test_gpu_nd.py): positions "
+            "< 1e-5 cell, velocities < 1e-5 thermal, fields < 1e-4") if prec == apic.FP32 else \
+        "FP64 particles (bit-faithful arithmetic)"
     sim.close()
     return {
         "value": value, "ms_per_step": ms_max / args.steps, "dtype": "f32" if prec == apic.FP32 else "f64",
         "config": {"workload": WORKLOAD_2D if dims == 2 else WORKLOAD_3D, "particles": P, "form": form,
-                   "sort_interval": args.sort_interval,
+                   "sort_interval": sort_interval, "push_items": push_items or ("4" if dims == 2 else "2"),
+                   "autotuned": tuned["table"] if tuned else None,
                    "l2": f"inputs larger than L2 ({bpp // 2 * P / 1e9:.1f} GB of particle state)"},
         "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
@@ -690,10 +717,15 @@ def bench_swarm(args, rank, dist):
     cfg, gas, tabs = W.to_device_swarm(spec, prec)
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(64 << 30, 0.6 * free))
-    spl = 200
+    rng = np.random.default_rng(5 + rank)
+    spl, tuned = 200, None
+    if not args.no_autotune:
+        from apic import autotune
+        sample = [_swarm_draw(rng, spec, W, k, 5_000_000) for k in range(12)]
+        tuned = autotune.tune_swarm_server(gas, sample, prec, min(budget, 16 << 30))
+        spl = tuned["steps_per_launch"]
     srv = apic.SwarmServer(gas, budget, max_runs=256, precision=prec, steps_per_launch=spl)
     ext = torch.cuda.ExternalStream(srv.cuda_stream())
-    rng = np.random.default_rng(5 + rank)
 
     def drain(ids, submit_at=None, pending=None):
         done = {}
@@ -775,6 +807,7 @@ def bench_swarm(args, rank, dist):
         "config": {"workload": WORKLOAD_SWARM, "form": ("FP32 electron velocity + displacement, FP64 collision "
                                                         "arithmetic and tallies") if prec == apic.FP32 else
                    "FP64 electrons", "saturation_requests": len(batch), "steps_per_launch": spl,
+                   "autotuned": tuned["table"] if tuned else None,
                    "l2": "electron state of the batch larger than L2"},
         "e2e": {"value": serve_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                 "note": "Poisson serving phase through the swarm server API: requests and results are host structs"},

@@ -128,3 +128,28 @@ def test_fp32_energy_conservation_2d():
     drift32 = abs(res[apic.FP32][1] - res[apic.FP32][0]) / res[apic.FP32][0]
     assert abs(res[apic.FP32][0] - res[apic.FP64][0]) < 1e-5 * res[apic.FP64][0]
     assert drift32 < max(2 * drift64, 1e-4), (drift32, drift64)
+
+
+def test_push_items_and_autotuner_leave_results_unchanged():
+    """The FP32 push's particles-per-thread knob changes only speed: every
+    setting gives the same particles and fields; the autotuner returns one of
+    the candidates with its timing table."""
+    from apic import autotune
+    plan = W.plasma_plan(2, cells=(64, 64), ppc=16, seed=4)
+    ref = None
+    for items in (1, 2, 4, 8):
+        sim = apic.SimulationND(plan.config(precision=apic.FP32, sort_interval=4, push_items=items))
+        plan.load(sim)
+        sim.initialize()
+        sim.step(9)
+        got = [sim.particles(k) for k in range(2)] + [sim.fields()]
+        sim.close()
+        if ref is None:
+            ref = got
+        else:
+            for a, b in zip(got, ref):
+                for x, y in zip(a, b):
+                    assert np.array_equal(x, y), items
+    out = autotune.tune_plasma(plan, apic.FP32, sort_intervals=(4, 8), push_items=(1, 4), steps=8)
+    assert out["sort_interval"] in (4, 8) and out["push_items"] in (1, 4)
+    assert len(out["table"]) == 4 and all(r["ms_per_step"] > 0 for r in out["table"])
