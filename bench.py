@@ -582,6 +582,16 @@ def bench_plasma(args, rank, dist):
     bpp = BYTES_PER_PSTEP[(args.workload, args.precision)]
     per_step_push = push_ms / max(nsteps, 1)
     achieved = bpp * P / (per_step_push * 1e-3) / 1e9
+    # DRAM bytes per push launch from the committed ncu capture of a smaller
+    # case of the same deck, scaled by the particles per launch (the state is
+    # streamed once per launch, so traffic grows in proportion)
+    traffic, traffic_note = None, None
+    if prec == apic.FP32:
+        captured = {2: 4194304, 3: 16777216}[dims]
+        t = _profiled_traffic(f"k_push32_plasma{dims}d_fp32.md")
+        if t:
+            traffic = t * (P / 2) / captured
+            traffic_note = f"ncu capture of {captured} particles per launch scaled to {P // 2}"
     form = ("FP32 particles: packed int32 cell + FP32 offsets + FP32 velocities; FP64 fixed-point deposit, "
             "FP64 spectral solve; error against the FP64 oracle after 10 steps (tests/test_gpu_nd.py): positions "
             "< 1e-5 cell, velocities < 1e-5 thermal, fields < 1e-4") if prec == apic.FP32 else \
@@ -596,7 +606,7 @@ def bench_plasma(args, rank, dist):
         "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
                      "kernel": ("k_push32" if prec == apic.FP32 else "k_push") + f"<{dims}, boris>",
                      "bytes_per_particle_step": bpp, "push_ms": per_step_push,
                      "solve_ms": solve_ms / max(nsteps, 1), "sort_ms_per_step": sort_ms / max(nsteps, 1)},
