@@ -384,6 +384,7 @@ class ConfigND(C.Structure):
         ("out_of_plane_depth", C.c_double), ("precision", C.c_int), ("sort_interval", C.c_size_t),
         ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
         ("push_items", C.c_int),
+        ("species_sort_interval", C.c_size_t * MAX_SPECIES),
     ]
 
 
@@ -433,7 +434,7 @@ def _check_nd(rc, handle=None):
 
 def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), units=NORMALIZED,
               relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16,
-              push_items=0) -> ConfigND:
+              push_items=0, species_sort_interval=None) -> ConfigND:
     c = ConfigND()
     c.dims = dims
     c.n[:] = list(n) + [1] * (3 - len(n))
@@ -442,6 +443,8 @@ def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), u
     c.magnetic_field[:] = list(magnetic_field)
     c.out_of_plane_depth, c.precision, c.sort_interval = out_of_plane_depth, precision, sort_interval
     c.push_items = push_items
+    if species_sort_interval:
+        c.species_sort_interval[:] = list(species_sort_interval) + [0] * (MAX_SPECIES - len(species_sort_interval))
     c.nspecies = len(species)
     for i, (q, m, w, cap) in enumerate(species):
         c.species[i] = SpeciesCfg(q, m, w, cap)

@@ -291,12 +291,15 @@ class PlasmaPlan:
     def particles(self) -> int:
         return sum(s[3] for s in self.species)
 
-    def config(self, precision=0, sort_interval=16, capacity_factor=1.0, push_items=0):
+    def config(self, precision=0, sort_interval=16, capacity_factor=1.0, push_items=0, ion_sort_factor=16):
+        """The ions (thermal speed 40-270x below the electrons') are re-sorted
+        ion_sort_factor times less often than the electrons."""
         from . import SI, config_nd
         sp = [(q, m, w, int(n * capacity_factor) + 1) for (q, m, w, n, vt, seed) in self.species]
         return config_nd(dims=self.dims, n=self.n, length=self.length, dt=self.dt, species=sp,
                          magnetic_field=self.B, units=SI, precision=precision, sort_interval=sort_interval,
-                         push_items=push_items)
+                         push_items=push_items,
+                         species_sort_interval=[sort_interval, sort_interval * ion_sort_factor])
 
     def load(self, sim):
         for k, (q, m, w, n, vt, seed) in enumerate(self.species):

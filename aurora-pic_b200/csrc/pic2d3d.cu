@@ -573,18 +573,31 @@ __device__ __forceinline__ unsigned linear_cell(const ParamsND& p, unsigned c) {
     return ((unsigned)z * p.n[1] + y) * p.n[0] + x;
 }
 
+// Lanes of a warp that share a cell (particles are nearly sorted, so a warp
+// spans few cells) take one atomic per cell: the group's leader adds the
+// group's size and the lanes take consecutive slots in lane order.
 __global__ void k_cell_hist32(ParamsND p, SpeciesND S, int buf, unsigned* count) {
     const unsigned i = blockIdx.x * kThreads + threadIdx.x;
-    if (i < S.n) atomicAdd(count + linear_cell(p, S.cell[buf][i]), 1u);
+    const bool valid = i < S.n;
+    const unsigned key = valid ? linear_cell(p, S.cell[buf][i]) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + key, (unsigned)__popc(peers));
 }
 
 template <int DIM>
 __global__ void k_cell_scatter32(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
     const unsigned i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= S.n) return;
+    const bool valid = i < S.n;
     const int to = from ^ 1;
-    const unsigned c = S.cell[from][i];
-    const unsigned o = atomicAdd(cursor + linear_cell(p, c), 1u);
+    const unsigned c = valid ? S.cell[from][i] : 0u;
+    const unsigned key = valid ? linear_cell(p, c) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (valid && lane == leader) base = atomicAdd(cursor + key, (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!valid) return;
+    const unsigned o = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
     S.cell[to][o] = c;
     for (int a = 0; a < DIM; ++a) S.off[to][a][o] = S.off[from][a][i];
     for (int a = 0; a < 3; ++a) S.vel[to][a][o] = S.vel[from][a][i];
@@ -1242,7 +1255,9 @@ struct SimND {
     uint64_t step_count = 0;
     size_t sort_interval = 16;
     uint64_t launches = 0;  // kernels launched by step()
-    size_t steps_since_sort = 0;
+    size_t steps_since_sort = 0;                   // of the most frequently sorted species
+    size_t since_sort[APIC_MAX_SPECIES] = {0, 0, 0, 0};
+    size_t species_interval[APIC_MAX_SPECIES] = {16, 16, 16, 16};
     unsigned* cell_count = nullptr;
     unsigned* cell_offset = nullptr;
     unsigned* block_sums = nullptr;
@@ -1297,6 +1312,8 @@ struct SimND {
             throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
         APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         sort_interval = c.sort_interval ? c.sort_interval : 16;
+        for (int k = 0; k < APIC_MAX_SPECIES; ++k)
+            species_interval[k] = c.species_sort_interval[k] ? c.species_sort_interval[k] : sort_interval;
 
         p.dims = c.dims;
         size_t N = 1;
@@ -1523,6 +1540,7 @@ struct SimND {
         for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushInitHalf>(s);
         initialized = true;
         steps_since_sort = sort_interval;  // sort before the first step
+        for (int k = 0; k < APIC_MAX_SPECIES; ++k) since_sort[k] = species_interval[k];
     }
 
     void resume(double t, uint64_t k) {
@@ -1531,23 +1549,27 @@ struct SimND {
         deposit_and_solve();
         initialized = true;
         steps_since_sort = sort_interval;
+        for (int k = 0; k < APIC_MAX_SPECIES; ++k) since_sort[k] = species_interval[k];
     }
 
     void do_steps(size_t nsteps) {
         require(initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
         for (size_t it = 0; it < nsteps; ++it) {
             Ev ev{};
-            const bool sort_now = steps_since_sort >= sort_interval;
             if (timing) {
                 APIC_CUDA(cudaEventCreate(&ev.a)); APIC_CUDA(cudaEventCreate(&ev.b));
                 APIC_CUDA(cudaEventCreate(&ev.c)); APIC_CUDA(cudaEventCreate(&ev.d));
                 APIC_CUDA(cudaEventRecord(ev.a, stream));
             }
-            if (sort_now) {
-                for (int s = 0; s < cfg.nspecies; ++s) sort_species(s);
-                steps_since_sort = 0;
-                launches += 5 * (uint64_t)cfg.nspecies;  // histogram, three scan passes, scatter
+            bool any_sorted = false;
+            for (int s = 0; s < cfg.nspecies; ++s) {
+                if (since_sort[s] < species_interval[s]) continue;
+                sort_species(s);
+                since_sort[s] = 0;
+                any_sorted = true;
+                launches += 5;  // histogram, three scan passes, scatter
             }
+            if (any_sorted) steps_since_sort = 0;
             if (timing) APIC_CUDA(cudaEventRecord(ev.b, stream));
             for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
             if (timing) APIC_CUDA(cudaEventRecord(ev.c, stream));
@@ -1555,10 +1577,11 @@ struct SimND {
             launches += (uint64_t)cfg.nspecies + (cfg.dims == 2 ? 3 : 5);  // pushes, FFT passes
             if (timing) {
                 APIC_CUDA(cudaEventRecord(ev.d, stream));
-                ev.sorted = sort_now;
+                ev.sorted = any_sorted;
                 events.push_back(ev);
             }
             ++steps_since_sort;
+            for (int s = 0; s < cfg.nspecies; ++s) ++since_sort[s];
             time += cfg.dt;
             ++step_count;
         }

@@ -297,6 +297,8 @@ typedef struct {
     apic_species species[APIC_MAX_SPECIES];
     int push_items;             /* FP32 form: particles per thread of the step push, 1, 2, 4 or 8
                                    (0 = default: 4 in 2D, 2 in 3D); a tuning knob, no effect on results */
+    size_t species_sort_interval[APIC_MAX_SPECIES];  /* per species (0 = sort_interval): slow heavy
+                                   species keep their cell order far longer; no effect on results */
 } apic_config_nd;
 
 /* DiagnosticSample2D / DiagnosticSample3D, src/Diagnostics.cpp:111-137, :205-232 */
