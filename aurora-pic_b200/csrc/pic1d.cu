@@ -110,10 +110,17 @@ struct SpeciesDev {
     double* vy[2];
     double* vz[2];
     double* v;  // time-centred velocity (valid after a read-back pass)
+    // FP32 form: v_half, v_y, v_z stored as float (x stays FP64: the int32
+    // cell + FP32 offset pair would take the same 8 bytes); null in FP64 form
+    float* vh32[2];
+    float* vy32[2];
+    float* vz32[2];
+    double* stage;  // FP32 form: FP64 staging for host copies (capacity)
 };
 
 struct Params1D {
     int nspecies, vdim, dirichlet, nx;
+    int f32;  // FP32 particle form
     double L, dx, inv_dx, dt, eps, rho_scale, inv_rho_scale;
     unsigned mode;
     uint64_t seed;
@@ -247,7 +254,19 @@ struct CandidateEntry {
 };
 constexpr int kQueue = 384;
 
-template <int VDIM, bool DIRICHLET>
+// Velocity components of the two storage forms: FP64, or FP32 (rounded to
+// nearest when stored, widened exactly when loaded; the arithmetic is FP64).
+template <bool F32>
+__device__ __forceinline__ double ld_comp(const double* d, const float* f, unsigned i) {
+    return F32 ? (double)f[i] : d[i];
+}
+template <bool F32>
+__device__ __forceinline__ void st_comp(double* d, float* f, unsigned long long i, double v) {
+    if (F32) f[i] = (float)v;
+    else d[i] = v;
+}
+
+template <int VDIM, bool DIRICHLET, bool F32>
 __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
@@ -299,9 +318,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
             queued[k] = -1;
             const unsigned ph = live ? physical_slot_from(S.rlstart[0], S.rstart[0], nr, r0, idx) : 0u;
             x[k] = live ? S.x[0][ph] : 0.0;
-            vh[k] = live ? S.vh[0][ph] : 0.0;
-            vy[k] = (VDIM == 3 && live) ? S.vy[0][ph] : 0.0;
-            vz[k] = (VDIM == 3 && live) ? S.vz[0][ph] : 0.0;
+            vh[k] = live ? ld_comp<F32>(S.vh[0], S.vh32[0], ph) : 0.0;
+            vy[k] = (VDIM == 3 && live) ? ld_comp<F32>(S.vy[0], S.vy32[0], ph) : 0.0;
+            vz[k] = (VDIM == 3 && live) ? ld_comp<F32>(S.vz[0], S.vz32[0], ph) : 0.0;
             vc[k] = 0.0;
             if ((mode & kModeInitHalf) && live) vc[k] = S.v[ph];
         }
@@ -478,10 +497,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
                 out_base + s_cnt[k * (kThreads / 32) + warp] + __popc(ballots[k] & lt);
             if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
             S.x[1][o] = x[k];
-            S.vh[1][o] = vh[k];
+            st_comp<F32>(S.vh[1], S.vh32[1], o, vh[k]);
             if (VDIM == 3) {
-                S.vy[1][o] = vy[k];
-                S.vz[1][o] = vz[k];
+                st_comp<F32>(S.vy[1], S.vy32[1], o, vy[k]);
+                st_comp<F32>(S.vz[1], S.vz32[1], o, vz[k]);
             }
             if (mode & (kModeWriteV | kModeInitHalf)) S.v[o] = vc[k];
         }
@@ -519,7 +538,7 @@ __host__ __device__ inline size_t post_smem_bytes(int nx, bool dirichlet) {
            (dirichlet ? (size_t)2 * nx * 8 : (size_t)2 * nx * 8 /* twiddles */ + (size_t)4 * nx * 8 /* spectra */);
 }
 
-template <int VDIM, bool DIRICHLET>
+template <int VDIM, bool DIRICHLET, bool F32>
 __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned post) {
     using Sort = cub::BlockRadixSort<unsigned long long, kPostThreads, kPostItems, int>;
     using ScanU = cub::BlockScan<unsigned, kPostThreads>;
@@ -692,10 +711,10 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                 const unsigned long long o = (unsigned long long)s_bstart[s] + ranks[k];
                 if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
                 S.x[1][o] = bx[k];
-                S.vh[1][o] = bvh[k];
+                st_comp<F32>(S.vh[1], S.vh32[1], o, bvh[k]);
                 if (VDIM == 3) {
-                    S.vy[1][o] = bv[k][1];
-                    S.vz[1][o] = bv[k][2];
+                    st_comp<F32>(S.vy[1], S.vy32[1], o, bv[k][1]);
+                    st_comp<F32>(S.vz[1], S.vz32[1], o, bv[k][2]);
                 }
                 S.v[o] = bv[k][0];
             }
@@ -860,6 +879,14 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
     }
 }
 
+// FP32 form: host copies go through an FP64 staging array.
+__global__ void k_narrow1d(const double* __restrict__ in, float* __restrict__ out, unsigned n) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (float)in[i];
+}
+__global__ void k_widen1d(const float* __restrict__ in, double* __restrict__ out, unsigned n) {
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)in[i];
+}
+
 // Simulation::sample reductions (src/Simulation.cpp:1140-1161,
 // src/Species.cpp:338-351): per-block partial sums, then the last block adds
 // the partials in block order, so the result does not depend on scheduling.
@@ -876,7 +903,11 @@ __global__ void __launch_bounds__(256) k_sample1d(Params1D p, double* partial, u
         for (unsigned i = blockIdx.x * 256 + tid; i < n; i += gridDim.x * 256) {
             const double v = S.v[i];
             double sq = v * v;
-            if (p.vdim == 3) sq += S.vy[0][i] * S.vy[0][i] + S.vz[0][i] * S.vz[0][i];
+            if (p.vdim == 3) {
+                const double vy = p.f32 ? (double)S.vy32[0][i] : S.vy[0][i];
+                const double vz = p.f32 ? (double)S.vz32[0][i] : S.vz[0][i];
+                sq += vy * vy + vz * vz;
+            }
             acc += hmw * sq;
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
@@ -1014,6 +1045,7 @@ struct Sim1D {
     DevState* st = nullptr;
     std::vector<void*> allocations;
     std::vector<std::vector<double>> tables;  // host copies (kept for safe_speed)
+    bool fp32 = false;      // FP32 particle form (APIC_FP32)
     bool pending = false;   // collision part of the last step not yet applied
     bool initialized = false;
     int parity = 0;         // which of the two buffers holds the current state
@@ -1058,7 +1090,8 @@ struct Sim1D {
         require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
         require(c.nspecies >= 1 && c.nspecies <= kMaxSpecies, "species count out of range");
         require(c.nmodels >= 0 && c.nmodels <= kMaxModels, "model count out of range");
-        require(c.precision == APIC_FP64, "this entry point builds the FP64 form", APIC_ERR_UNSUPPORTED);
+        require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
+        fp32 = c.precision == APIC_FP32;
         const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
         require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
         int ndev = 0;
@@ -1069,6 +1102,7 @@ struct Sim1D {
 
         const bool dir = c.boundary == APIC_DIRICHLET;
         p.nspecies = c.nspecies;
+        p.f32 = fp32 ? 1 : 0;
         p.vdim = c.velocity_dimensions;
         p.dirichlet = dir;
         p.nx = (int)c.nx;
@@ -1117,13 +1151,21 @@ struct Sim1D {
                 S.rlstart[b] = dalloc<unsigned>(maxr);
             }
             S.chunk_surv = dalloc<unsigned>(maxr);
+            const bool v3 = c.velocity_dimensions == 3;
             for (int b = 0; b < 2; ++b) {
                 S.x[b] = dalloc<double>(cap);
-                S.vh[b] = dalloc<double>(cap);
-                S.vy[b] = c.velocity_dimensions == 3 ? dalloc<double>(cap) : nullptr;
-                S.vz[b] = c.velocity_dimensions == 3 ? dalloc<double>(cap) : nullptr;
+                if (fp32) {
+                    S.vh32[b] = dalloc<float>(cap);
+                    S.vy32[b] = v3 ? dalloc<float>(cap) : nullptr;
+                    S.vz32[b] = v3 ? dalloc<float>(cap) : nullptr;
+                } else {
+                    S.vh[b] = dalloc<double>(cap);
+                    S.vy[b] = v3 ? dalloc<double>(cap) : nullptr;
+                    S.vz[b] = v3 ? dalloc<double>(cap) : nullptr;
+                }
             }
             S.v = dalloc<double>(cap);
+            if (fp32) S.stage = dalloc<double>(cap);
         }
         for (int mi = 0; mi < c.nmodels; ++mi) {
             const apic_mcc_model& m = c.models[mi];
@@ -1198,17 +1240,10 @@ struct Sim1D {
         APIC_CUDA(cudaStreamSynchronize(stream));
         static bool attr_done = false;
         if (!attr_done) {
-            const int smem = kMaxNx1D * 16;
-            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_pass1d<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            const int psm = (int)post_smem_bytes(kMaxNx1D, true);
-            const int psm_p = (int)post_smem_bytes(kMaxNx1DPeriodic, false);
-            APIC_CUDA(cudaFuncSetAttribute(k_post1d<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
-            APIC_CUDA(cudaFuncSetAttribute(k_post1d<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
-            APIC_CUDA(cudaFuncSetAttribute(k_post1d<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm_p));
-            APIC_CUDA(cudaFuncSetAttribute(k_post1d<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm_p));
+            set_attributes<1, false, false>(); set_attributes<1, true, false>();
+            set_attributes<3, false, false>(); set_attributes<3, true, false>();
+            set_attributes<1, false, true>(); set_attributes<1, true, true>();
+            set_attributes<3, false, true>(); set_attributes<3, true, true>();
             attr_done = true;
         }
     }
@@ -1225,6 +1260,9 @@ struct Sim1D {
             S.vh[0] = B.vh[in]; S.vh[1] = B.vh[out];
             S.vy[0] = B.vy[in]; S.vy[1] = B.vy[out];
             S.vz[0] = B.vz[in]; S.vz[1] = B.vz[out];
+            S.vh32[0] = B.vh32[in]; S.vh32[1] = B.vh32[out];
+            S.vy32[0] = B.vy32[in]; S.vy32[1] = B.vy32[out];
+            S.vz32[0] = B.vz32[in]; S.vz32[1] = B.vz32[out];
             S.rstart[0] = B.rstart[in]; S.rstart[1] = B.rstart[out];
             S.rcount[0] = B.rcount[in]; S.rcount[1] = B.rcount[out];
             S.rlstart[0] = B.rlstart[in]; S.rlstart[1] = B.rlstart[out];
@@ -1263,6 +1301,21 @@ struct Sim1D {
         events.clear();
     }
 
+    template <int VDIM, bool DIR, bool F32>
+    static void set_attributes() {
+        const int smem = kMaxNx1D * 16;
+        APIC_CUDA(cudaFuncSetAttribute(k_pass1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        const int psm = (int)post_smem_bytes(DIR ? kMaxNx1D : kMaxNx1DPeriodic, DIR);
+        APIC_CUDA(cudaFuncSetAttribute(k_post1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
+    }
+
+    template <int VDIM, bool DIR, bool F32>
+    void launch_kernels(const Params1D& q, int blocks, size_t smem, size_t post_smem, unsigned post, EvPair& ev) {
+        k_pass1d<VDIM, DIR, F32><<<blocks, kThreads, smem, stream>>>(q);
+        if (timing) cudaEventRecord(ev.b, stream);
+        k_post1d<VDIM, DIR, F32><<<1, kPostThreads, post_smem, stream>>>(q, post);
+    }
+
     void launch_pass(unsigned mode, unsigned post) {
         const Params1D q = pass_params(mode);
         const int blocks = grid_blocks();
@@ -1276,12 +1329,16 @@ struct Sim1D {
             APIC_CUDA(cudaEventCreate(&ev.c));
             APIC_CUDA(cudaEventRecord(ev.a, stream));
         }
-        if (cfg.velocity_dimensions == 3) {
-            if (dir) { k_pass1d<3, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, true><<<1, kPostThreads, post_smem, stream>>>(q, post); }
-            else { k_pass1d<3, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<3, false><<<1, kPostThreads, post_smem, stream>>>(q, post); }
-        } else {
-            if (dir) { k_pass1d<1, true><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, true><<<1, kPostThreads, post_smem, stream>>>(q, post); }
-            else { k_pass1d<1, false><<<blocks, kThreads, smem, stream>>>(q); if (timing) cudaEventRecord(ev.b, stream); k_post1d<1, false><<<1, kPostThreads, post_smem, stream>>>(q, post); }
+        const int form = (cfg.velocity_dimensions == 3 ? 4 : 0) | (dir ? 2 : 0) | (fp32 ? 1 : 0);
+        switch (form) {
+            case 0: launch_kernels<1, false, false>(q, blocks, smem, post_smem, post, ev); break;
+            case 1: launch_kernels<1, false, true>(q, blocks, smem, post_smem, post, ev); break;
+            case 2: launch_kernels<1, true, false>(q, blocks, smem, post_smem, post, ev); break;
+            case 3: launch_kernels<1, true, true>(q, blocks, smem, post_smem, post, ev); break;
+            case 4: launch_kernels<3, false, false>(q, blocks, smem, post_smem, post, ev); break;
+            case 5: launch_kernels<3, false, true>(q, blocks, smem, post_smem, post, ev); break;
+            case 6: launch_kernels<3, true, false>(q, blocks, smem, post_smem, post, ev); break;
+            default: launch_kernels<3, true, true>(q, blocks, smem, post_smem, post, ev); break;
         }
         if (timing) {
             APIC_CUDA(cudaEventRecord(ev.c, stream));
@@ -1289,6 +1346,31 @@ struct Sim1D {
         }
         APIC_CUDA(cudaGetLastError());
         parity ^= 1;
+    }
+
+    // One velocity component of species s between host doubles and the
+    // current device buffer (FP32 form: rounded to nearest on the way in).
+    void put_comp(int s, double* d, float* f, const double* host, size_t n) {
+        if (n == 0) return;
+        if (!fp32) {
+            APIC_CUDA(cudaMemcpyAsync(d, host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+            return;
+        }
+        double* stage = p.sp[s].stage;
+        APIC_CUDA(cudaMemcpyAsync(stage, host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        k_narrow1d<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, stream>>>(stage, f, (unsigned)n);
+        APIC_CUDA(cudaGetLastError());
+    }
+    void get_comp(int s, const double* d, const float* f, double* host, size_t n) {
+        if (n == 0) return;
+        if (!fp32) {
+            APIC_CUDA(cudaMemcpyAsync(host, d, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            return;
+        }
+        double* stage = p.sp[s].stage;
+        k_widen1d<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0, stream>>>(f, stage, (unsigned)n);
+        APIC_CUDA(cudaGetLastError());
+        APIC_CUDA(cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     }
 
     void load(int s, size_t n, const double* x, const double* v, const double* vh, const double* vy,
@@ -1302,11 +1384,11 @@ struct Sim1D {
             SpeciesDev& B = p.sp[s];
             const size_t bytes = n * sizeof(double);
             APIC_CUDA(cudaMemcpyAsync(B.x[parity], x, bytes, cudaMemcpyHostToDevice, stream));
-            APIC_CUDA(cudaMemcpyAsync(B.vh[parity], vh, bytes, cudaMemcpyHostToDevice, stream));
+            put_comp(s, B.vh[parity], B.vh32[parity], vh, n);
             APIC_CUDA(cudaMemcpyAsync(B.v, v, bytes, cudaMemcpyHostToDevice, stream));
             if (cfg.velocity_dimensions == 3) {
-                APIC_CUDA(cudaMemcpyAsync(B.vy[parity], vy, bytes, cudaMemcpyHostToDevice, stream));
-                APIC_CUDA(cudaMemcpyAsync(B.vz[parity], vz, bytes, cudaMemcpyHostToDevice, stream));
+                put_comp(s, B.vy[parity], B.vy32[parity], vy, n);
+                put_comp(s, B.vz[parity], B.vz32[parity], vz, n);
             }
             set_single_range(s, (unsigned)n);
             APIC_CUDA(cudaStreamSynchronize(stream));
@@ -1330,11 +1412,11 @@ struct Sim1D {
         SpeciesDev& B = p.sp[s];
         const size_t bytes = m * sizeof(double);
         APIC_CUDA(cudaMemcpyAsync(B.x[parity], hx.data(), bytes, cudaMemcpyHostToDevice, stream));
-        APIC_CUDA(cudaMemcpyAsync(B.vh[parity], hvh.data(), bytes, cudaMemcpyHostToDevice, stream));
+        put_comp(s, B.vh[parity], B.vh32[parity], hvh.data(), m);
         APIC_CUDA(cudaMemcpyAsync(B.v, hv.data(), bytes, cudaMemcpyHostToDevice, stream));
         if (cfg.velocity_dimensions == 3) {
-            APIC_CUDA(cudaMemcpyAsync(B.vy[parity], hvy.data(), bytes, cudaMemcpyHostToDevice, stream));
-            APIC_CUDA(cudaMemcpyAsync(B.vz[parity], hvz.data(), bytes, cudaMemcpyHostToDevice, stream));
+            put_comp(s, B.vy[parity], B.vy32[parity], hvy.data(), m);
+            put_comp(s, B.vz[parity], B.vz32[parity], hvz.data(), m);
         }
         set_single_range(s, (unsigned)m);
         APIC_CUDA(cudaStreamSynchronize(stream));
@@ -1461,10 +1543,10 @@ struct Sim1D {
         const size_t bytes = n * sizeof(double);
         if (x) APIC_CUDA(cudaMemcpyAsync(x, B.x[parity], bytes, cudaMemcpyDeviceToHost, stream));
         if (v) APIC_CUDA(cudaMemcpyAsync(v, B.v, bytes, cudaMemcpyDeviceToHost, stream));
-        if (vh) APIC_CUDA(cudaMemcpyAsync(vh, B.vh[parity], bytes, cudaMemcpyDeviceToHost, stream));
+        if (vh) get_comp(s, B.vh[parity], B.vh32[parity], vh, n);
         if (cfg.velocity_dimensions == 3) {
-            if (vy) APIC_CUDA(cudaMemcpyAsync(vy, B.vy[parity], bytes, cudaMemcpyDeviceToHost, stream));
-            if (vz) APIC_CUDA(cudaMemcpyAsync(vz, B.vz[parity], bytes, cudaMemcpyDeviceToHost, stream));
+            if (vy) get_comp(s, B.vy[parity], B.vy32[parity], vy, n);
+            if (vz) get_comp(s, B.vz[parity], B.vz32[parity], vz, n);
         } else {
             if (vy) std::memset(vy, 0, bytes);
             if (vz) std::memset(vz, 0, bytes);

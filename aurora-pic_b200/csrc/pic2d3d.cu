@@ -1282,6 +1282,7 @@ struct SimND {
 
     ~SimND() {
         if (stream) cudaStreamSynchronize(stream);
+        drop_graphs();
         for (auto& e : events) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); cudaEventDestroy(e.c); cudaEventDestroy(e.d); }
         for (void* a : allocations) cudaFree(a);
         if (stream) cudaStreamDestroy(stream);
@@ -1508,6 +1509,7 @@ struct SimND {
         for (size_t i = 0; i < n; ++i) ids[i] = (unsigned)i;
         APIC_CUDA(cudaMemcpyAsync(S.id[b], ids.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaStreamSynchronize(stream));
+        if (S.n != (unsigned)n) drop_graphs();  // captured launches carry the particle count
         S.n = (unsigned)n;
         to_fp32(s);
         initialized = false;
@@ -1523,6 +1525,7 @@ struct SimND {
         if (n) k_load_maxwellian<<<blocks, kThreads, 0, stream>>>(S, buf[s], cfg.dims, (unsigned)n, seed, p.L[0],
                                                                    p.L[1], p.L[2], vt, drift, axis, amp);
         APIC_CUDA(cudaGetLastError());
+        if (S.n != (unsigned)n) drop_graphs();  // captured launches carry the particle count
         S.n = (unsigned)n;
         to_fp32(s);
         initialized = false;
@@ -1552,32 +1555,83 @@ struct SimND {
         for (int k = 0; k < APIC_MAX_SPECIES; ++k) since_sort[k] = species_interval[k];
     }
 
+    // One step as a CUDA graph: its kernel parameters depend only on which
+    // species are sorted this step and on each species' buffer parity, so the
+    // graphs are cached under that key (at most a few per run).
+    struct StepGraph {
+        unsigned key;
+        cudaGraphExec_t exec;
+    };
+    std::vector<StepGraph> step_graphs;
+
+    void drop_graphs() {
+        for (auto& g : step_graphs) cudaGraphExecDestroy(g.exec);
+        step_graphs.clear();
+    }
+
+    void enqueue_step(unsigned sort_mask) {
+        for (int s = 0; s < cfg.nspecies; ++s)
+            if (sort_mask >> s & 1u) sort_species(s);
+        for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
+        solver.solve();
+    }
+
+    void launch_step_graph(unsigned sort_mask) {
+        unsigned key = sort_mask;
+        for (int s = 0; s < cfg.nspecies; ++s) key |= (unsigned)buf[s] << (APIC_MAX_SPECIES + s);
+        cudaGraphExec_t exec = nullptr;
+        for (const auto& g : step_graphs)
+            if (g.key == key) exec = g.exec;
+        if (!exec) {
+            int saved[APIC_MAX_SPECIES];
+            for (int s = 0; s < APIC_MAX_SPECIES; ++s) saved[s] = buf[s];
+            cudaGraph_t g = nullptr;
+            APIC_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            enqueue_step(sort_mask);
+            const cudaError_t ce = cudaStreamEndCapture(stream, &g);
+            for (int s = 0; s < APIC_MAX_SPECIES; ++s) buf[s] = saved[s];
+            APIC_CUDA(ce);
+            const cudaError_t ie = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            APIC_CUDA(ie);
+            step_graphs.push_back({key, exec});
+        }
+        APIC_CUDA(cudaGraphLaunch(exec, stream));
+        for (int s = 0; s < cfg.nspecies; ++s)
+            if (sort_mask >> s & 1u) buf[s] ^= 1;
+    }
+
     void do_steps(size_t nsteps) {
         require(initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
         for (size_t it = 0; it < nsteps; ++it) {
-            Ev ev{};
-            if (timing) {
+            unsigned sort_mask = 0;
+            for (int s = 0; s < cfg.nspecies; ++s)
+                if (since_sort[s] >= species_interval[s] && sp[s].n) sort_mask |= 1u << s;
+            for (int s = 0; s < cfg.nspecies; ++s) {
+                if (since_sort[s] < species_interval[s]) continue;
+                since_sort[s] = 0;
+                if (sp[s].n) launches += 5;  // histogram, three scan passes, scatter
+            }
+            if (sort_mask) steps_since_sort = 0;
+            for (int s = 0; s < cfg.nspecies; ++s)
+                if (sp[s].n) ++launches;
+            launches += cfg.dims == 2 ? 3 : 5;  // FFT passes
+            if (!timing) {
+                launch_step_graph(sort_mask);
+            } else {
+                // kernel by kernel, with events between the phases
+                Ev ev{};
                 APIC_CUDA(cudaEventCreate(&ev.a)); APIC_CUDA(cudaEventCreate(&ev.b));
                 APIC_CUDA(cudaEventCreate(&ev.c)); APIC_CUDA(cudaEventCreate(&ev.d));
                 APIC_CUDA(cudaEventRecord(ev.a, stream));
-            }
-            bool any_sorted = false;
-            for (int s = 0; s < cfg.nspecies; ++s) {
-                if (since_sort[s] < species_interval[s]) continue;
-                sort_species(s);
-                since_sort[s] = 0;
-                any_sorted = true;
-                launches += 5;  // histogram, three scan passes, scatter
-            }
-            if (any_sorted) steps_since_sort = 0;
-            if (timing) APIC_CUDA(cudaEventRecord(ev.b, stream));
-            for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
-            if (timing) APIC_CUDA(cudaEventRecord(ev.c, stream));
-            solver.solve();
-            launches += (uint64_t)cfg.nspecies + (cfg.dims == 2 ? 3 : 5);  // pushes, FFT passes
-            if (timing) {
+                for (int s = 0; s < cfg.nspecies; ++s)
+                    if (sort_mask >> s & 1u) sort_species(s);
+                APIC_CUDA(cudaEventRecord(ev.b, stream));
+                for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
+                APIC_CUDA(cudaEventRecord(ev.c, stream));
+                solver.solve();
                 APIC_CUDA(cudaEventRecord(ev.d, stream));
-                ev.sorted = any_sorted;
+                ev.sorted = sort_mask != 0;
                 events.push_back(ev);
             }
             ++steps_since_sort;

@@ -326,8 +326,9 @@ def bench_ccp1d(args, rank, dist):
     import apic
     from apic import workloads as W
 
+    prec = apic.FP32 if args.precision == "fp32" else apic.FP64
     wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7 + rank)
-    cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=1000 + rank)
+    cfg, tabs = W.to_device_config(wl, precision=prec, seed=1000 + rank)
     sim = apic.Simulation1D(cfg, tabs)
     for i, s in enumerate(wl.species):
         sim.load(i, s.x, s.v, None, s.vy, s.vz)
@@ -411,17 +412,29 @@ def bench_ccp1d(args, rank, dist):
     e_ms, e_total = _reduce(dist, e2e_ms, args.e2e_steps * mean_n)
 
     hbm, peak_kind = peaks()
-    bytes_per_pstep = 64  # FP64 1D3V: read + write x, v_half, v_y, v_z
+    # read + write x, v_half, v_y, v_z: FP64 8+8+8+8, FP32 form 8+4+4+4
+    bytes_per_pstep = 64 if prec == apic.FP64 else 40
     per_pass_ms = pass_ms / max(passes, 1)
     achieved = bytes_per_pstep * mean_n / (per_pass_ms * 1e-3) / 1e9
-    traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md")
+    traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md" if prec == apic.FP64 else "k_pass1d_ccp1d_fp32.md")
     sim.close()
+    # the other storage form of the same discharge, device-timed the same way
+    other = apic.FP32 if prec == apic.FP64 else apic.FP64
+    other_ps, other_ms = _single_ccp(args, rank, other, max(50, args.steps // 2))
+    forms = {("fp64" if prec == apic.FP64 else "fp32"): {"particle_steps_per_s": value, "ms_per_step": ms_max / args.steps},
+             ("fp32" if other == apic.FP32 else "fp64"): {"particle_steps_per_s": other_ps, "ms_per_step": other_ms},
+             "fp32_error": FP32_1D_ERROR}
     batched = _batched_ccp(args, rank) if args.batch > 1 else None
+    if batched:
+        batched["vs_plain_fp64_single_run"] = batched["value"] / forms["fp64"]["particle_steps_per_s"]
     return {
         "batched": batched,
+        "forms": forms,
         "value": value, "ms_per_step": ms_max / args.steps, "dtype": "f64",
         "config": {"workload": WORKLOAD_CCP, "particles": int(mean_n),
-                   "form": "FP64 particles (bit-faithful arithmetic)", "l2": "flushed between timed steps"},
+                   "form": "FP64 particles (bit-faithful arithmetic)" if prec == apic.FP64 else
+                   "FP32 particle form: FP64 x, FP32 v_half/v_y/v_z, FP64 arithmetic, fields and tallies; " + FP32_1D_ERROR,
+                   "l2": "flushed between timed steps"},
         "e2e": {"value": e_total / (e_ms * 1e-3), "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
@@ -433,11 +446,52 @@ def bench_ccp1d(args, rank, dist):
     }
 
 
+FP32_1D_ERROR = ("error against the FP64 oracle after 20 discharge steps / 50 two-stream steps "
+                 "(tests/test_gpu_1d_fp32.py): positions < 1e-6, velocities < 1e-5 relative, "
+                 "collision counts within 1%")
+
+
+def _single_ccp(args, rank, prec, steps):
+    """One discharge in the given storage form, device-timed over `steps`
+    steps with the L2 flushed between steps; (particle-steps/s, ms/step)."""
+    import torch
+    import apic
+    from apic import workloads as W
+    wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=7 + rank)
+    cfg, tabs = W.to_device_config(wl, precision=prec, seed=1000 + rank)
+    sim = apic.Simulation1D(cfg, tabs)
+    for i, s in enumerate(wl.species):
+        sim.load(i, s.x, s.v, None, s.vy, s.vz)
+    sim.initialize()
+    sim.step(args.warmup)
+    sim.synchronize()
+    ext = torch.cuda.ExternalStream(sim.cuda_stream())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    flush_sink = torch.empty((), dtype=torch.float32, device="cuda")
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    n0 = sum(sim.count(s) for s in range(len(wl.species)))
+    torch.cuda.synchronize()
+    with torch.cuda.stream(ext):
+        for i in range(steps):
+            flush.zero_()
+            flush_sink.copy_(flush.sum())
+            starts[i].record(ext)
+            sim.step(1)
+            ends[i].record(ext)
+    sim.synchronize()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+    n1 = sum(sim.count(s) for s in range(len(wl.species)))
+    sim.close()
+    return steps * 0.5 * (n0 + n1) / (ms * 1e-3), ms / steps
+
+
 def _batched_ccp(args, rank):
-    """`args.batch` independent discharges stepped together through
-    apic_sim1d_step_group (their kernels overlap on the GPU): aggregate
-    particle-steps/s, device time from one event before the launches to the
-    last run's end event (host launch time included)."""
+    """`args.batch` independent discharges in the FP32 particle form stepped
+    together through apic_sim1d_step_group (their kernels overlap on the GPU):
+    aggregate particle-steps/s, device time from one event before the launches
+    to the last run's end event (host launch time included)."""
     import torch
     import apic
     from apic import workloads as W
@@ -448,7 +502,7 @@ def _batched_ccp(args, rank):
 
         def make(k):
             wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=200 + k)
-            cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=7000 + k)
+            cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=7000 + k)
             sim = apic.Simulation1D(cfg, tabs)
             for i, s in enumerate(wl.species):
                 sim.load(i, s.x, s.v, None, s.vy, s.vz)
@@ -460,7 +514,7 @@ def _batched_ccp(args, rank):
     sims = []
     for k in range(batch):
         wl = W.ccp_helium(particles_per_cell=args.ppc or 512, cells=args.cells or 512, seed=100 + 31 * rank + k)
-        cfg, tabs = W.to_device_config(wl, precision=apic.FP64, seed=5000 + 31 * rank + k)
+        cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=5000 + 31 * rank + k)
         sim = apic.Simulation1D(cfg, tabs)
         for i, s in enumerate(wl.species):
             sim.load(i, s.x, s.v, None, s.vy, s.vz)
@@ -488,7 +542,8 @@ def _batched_ccp(args, rank):
     psteps = args.steps * 0.5 * (n0 + n1)
     return {"decks": batch, "autotuned": tuned["table"] if tuned else None,
             "value": psteps / (ms * 1e-3), "unit": "particle-steps/s",
-            "ms_per_step": ms / args.steps, "form": "FP64 particles, runs stepped together (apic_sim1d_step_group)",
+            "ms_per_step": ms / args.steps,
+            "form": "FP32 particle form, runs stepped together (apic_sim1d_step_group)",
             "l2": f"{batch} discharges' state larger than L2"}
 
 
@@ -518,14 +573,13 @@ def bench_plasma(args, rank, dist):
     ext = torch.cuda.ExternalStream(sim.cuda_stream())
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    sim.set_kernel_timing(True)
     launches0 = sim.launch_count()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
         e0.record(ext)
-        sim.step(args.steps)
+        sim.step(args.steps)  # one CUDA graph launch per step
         e1.record(ext)
         sim.synchronize()
         torch.cuda.synchronize()
@@ -533,6 +587,11 @@ def bench_plasma(args, rank, dist):
         dist.barrier()
     ms = e0.elapsed_time(e1)
     launches = sim.launch_count() - launches0
+    # per-kernel breakdown: the same number of steps again, kernel by kernel
+    # with events between sort, push and solve (outside the timed region)
+    sim.set_kernel_timing(True)
+    sim.step(args.steps)
+    sim.synchronize()
     push_ms, solve_ms, sort_ms, nsteps = sim.kernel_times()
     sim.set_kernel_timing(False)
     ms_max, total = _reduce(dist, ms, args.steps * P)
@@ -883,6 +942,8 @@ def main():
         }
         if "swarm" in part:
             line["swarm"] = part["swarm"]
+        if part.get("forms"):
+            line["forms"] = part["forms"]
         if part.get("batched"):
             b = dict(part["batched"])
             b["vs_single_run"] = b["value"] / part["value"]

@@ -558,6 +558,16 @@ static void store_reserve(ora_store* s, size_t cap) {
     s->cap = cap;
 }
 
+static double f32_round(double v) { return (double)(float)v; }
+
+static void round_stored(ora_store* st) {
+    for (size_t i = 0; i < st->n; ++i) {
+        st->vh[i] = f32_round(st->vh[i]);
+        st->vy[i] = f32_round(st->vy[i]);
+        st->vz[i] = f32_round(st->vz[i]);
+    }
+}
+
 ora_sim1d* ora_sim1d_create(const ora_config1d* cfg, int mode, uint64_t philox_seed) {
     ora_sim1d* s = calloc(1, sizeof *s);
     s->cfg = *cfg;
@@ -595,12 +605,22 @@ int ora_sim1d_load(ora_sim1d* s, int species, size_t n, const double* x, const d
     store_reserve(st, n + 16);
     st->n = 0;
     for (size_t i = 0; i < n; ++i) {
-        if (s->mode == 1 && alive && !alive[i]) continue; /* device layout holds live particles only */
+        if (s->mode != 0 && alive && !alive[i]) continue; /* device layout holds live particles only */
         const size_t k = st->n++;
         st->x[k] = x[i]; st->v[k] = v[i]; st->vh[k] = vh[i];
         st->vy[k] = vy ? vy[i] : 0.0; st->vz[k] = vz ? vz[i] : 0.0;
         st->alive[k] = alive ? alive[i] : 1;
     }
+    if (s->mode == 2) round_stored(st);
+    return 0;
+}
+
+/* Mode 2 (the device's FP32 particle form): v_half, v_y and v_z are stored as
+ * float, rounded to nearest each time a particle is stored (load, the end of
+ * initialize, after each drift, and whenever the state is read back); the
+ * position stays FP64 and all arithmetic is FP64. */
+int ora_sim1d_round_fp32(ora_sim1d* s) {
+    for (int k = 0; k < s->cfg.nspecies; ++k) round_stored(&s->sp[k]);
     return 0;
 }
 
@@ -633,6 +653,7 @@ int ora_sim1d_initialize(ora_sim1d* s) {
             if (st->alive[i])
                 st->vh[i] = st->v[i] - 0.5 * qm * ora_gather1d(s->E, s->cfg.nx, s->cfg.length, s->dx,
                                                               s->cfg.dirichlet, st->x[i]) * s->cfg.dt;
+        if (s->mode == 2) round_stored(st);
     }
     return 0;
 }
@@ -756,14 +777,19 @@ static int step_once(ora_sim1d* s) {
                 st->alive[i] = 0;
             }
             (void)mw;
-            if (s->mode == 1 && st->alive[i]) {
+            if (s->mode == 2 && st->alive[i]) {
+                st->vh[i] = f32_round(st->vh[i]);
+                st->vy[i] = f32_round(st->vy[i]);
+                st->vz[i] = f32_round(st->vz[i]);
+            }
+            if (s->mode != 0 && st->alive[i]) {
                 /* device layout: survivors compacted in order */
                 st->x[out] = st->x[i]; st->v[out] = st->v[i]; st->vh[out] = st->vh[i];
                 st->vy[out] = st->vy[i]; st->vz[out] = st->vz[i]; st->alive[out] = 1;
                 ++out;
             }
         }
-        if (s->mode == 1) st->n = out;
+        if (s->mode != 0) st->n = out;
     }
     deposit_and_solve(s, s->time + c->dt);
     for (int sid = 0; sid < c->nspecies; ++sid) {

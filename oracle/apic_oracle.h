@@ -64,7 +64,9 @@ typedef struct ora_sim1d ora_sim1d;
 /* mode 0: reference layout and one shared mt19937_64 stream (bit-exact with
  *         the reference's Simulation);
  * mode 1: device layout (survivors compacted in order, products appended in
- *         parent order) and per-(seed, species, slot, step) Philox streams. */
+ *         parent order) and per-(seed, species, slot, step) Philox streams;
+ * mode 2: mode 1 with v_half, v_y, v_z stored as float (the device's FP32
+ *         particle form), see ora_sim1d_round_fp32. */
 ora_sim1d* ora_sim1d_create(const ora_config1d* cfg, int mode, uint64_t philox_seed);
 void ora_sim1d_destroy(ora_sim1d* s);
 int ora_sim1d_load(ora_sim1d* s, int species, size_t n, const double* x, const double* v,
@@ -72,6 +74,9 @@ int ora_sim1d_load(ora_sim1d* s, int species, size_t n, const double* x, const d
 int ora_sim1d_initialize_fields(ora_sim1d* s, double time, uint64_t step);
 int ora_sim1d_initialize(ora_sim1d* s);
 int ora_sim1d_step(ora_sim1d* s, size_t steps);
+/* mode 2 only: round the stored velocities as the device stores them when its
+ * state is read back (a no-op on values already rounded) */
+int ora_sim1d_round_fp32(ora_sim1d* s);
 size_t ora_sim1d_count(const ora_sim1d* s, int species);
 int ora_sim1d_get(const ora_sim1d* s, int species, double* x, double* v, double* vh,
                   double* vy, double* vz, uint8_t* alive);

@@ -150,6 +150,7 @@ def oracle() -> C.CDLL:
         L.ora_sim1d_load.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _DP, _DP, _U8P]
         L.ora_sim1d_initialize_fields.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
         L.ora_sim1d_step.argtypes = [C.c_void_p, C.c_size_t]
+        L.ora_sim1d_round_fp32.argtypes = [C.c_void_p]
         L.ora_sim1d_initialize.argtypes = [C.c_void_p]
         L.ora_sim1d_count.restype = C.c_size_t
         L.ora_sim1d_count.argtypes = [C.c_void_p, C.c_int]
@@ -266,7 +267,8 @@ def config1d(*, dirichlet, vdim, si, nx, length, dt, species, models=(), phi_lef
 
 class Sim1D:
     """Oracle 1D simulation (mode 0 = reference layout and stream, mode 1 =
-    device layout with Philox streams)."""
+    device layout with Philox streams, mode 2 = mode 1 with FP32-stored
+    velocities, the device's FP32 particle form)."""
 
     def __init__(self, cfg: Config1D, mode: int, philox_seed: int = 0):
         L = oracle()
@@ -301,6 +303,10 @@ class Sim1D:
         rc = oracle().ora_sim1d_step(self.h, n)
         if rc:
             raise RuntimeError(oracle().ora_last_error().decode())
+
+    def round_fp32(self):
+        """Mode 2: round the stored velocities as a device read-back does."""
+        oracle().ora_sim1d_round_fp32(self.h)
 
     def particles(self, s):
         L = oracle()
