@@ -47,6 +47,9 @@ namespace apic {
 constexpr int kThreads = 256;
 constexpr int kItems = 4;
 constexpr int kTile = kThreads * kItems;
+constexpr int kMinBlocks = 2;  // resident CTAs of k_pass1d per SM (register budget)
+constexpr int kWarpCounts = kItems * (kThreads / 32);  // per-(item, warp) survivor counts of a tile
+static_assert(kWarpCounts <= 32, "the survivor scan runs in one warp");
 constexpr int kMaxSpecies = APIC_MAX_SPECIES;
 constexpr int kMaxModels = APIC_MAX_MODELS;
 constexpr int kPostThreads = 512;
@@ -165,9 +168,13 @@ __device__ __forceinline__ Cic cic_periodic(double x, double L, double dx, int n
     const double fl = floor(g);
     const unsigned long long i = (unsigned long long)fl;
     const double f = g - (double)i;
+    // i % nx and (i + 1) % nx; i <= nx after the wrap, so the remainders are
+    // single subtractions (the 64-bit division only for out-of-range input)
+    const unsigned long long n = (unsigned long long)nx;
+    const unsigned long long i1 = i + 1;
     Cic c;
-    c.i0 = (int)(i % (unsigned long long)nx);
-    c.i1 = (int)((i + 1) % (unsigned long long)nx);
+    c.i0 = (int)(i < n ? i : (i < 2 * n ? i - n : i % n));
+    c.i1 = (int)(i1 < n ? i1 : (i1 < 2 * n ? i1 - n : i1 % n));
     c.w0 = 1.0 - f;
     c.w1 = f;
     return c;
@@ -267,11 +274,11 @@ __device__ __forceinline__ void st_comp(double* d, float* f, unsigned long long 
 }
 
 template <int VDIM, bool DIRICHLET, bool F32>
-__global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
     unsigned long long* sRho = reinterpret_cast<unsigned long long*>(sE + p.nx);
-    __shared__ unsigned s_cnt[kItems * (kThreads / 32)];
+    __shared__ unsigned s_cnt[32];
     __shared__ unsigned s_qlen;
     __shared__ CandidateEntry s_queue[kQueue];
 
@@ -472,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_pass1d(Params1D p) {
         }
         __syncthreads();
         if (warp == 0) {
-            const unsigned c = s_cnt[lane];
+            const unsigned c = lane < kWarpCounts ? s_cnt[lane] : 0u;
             unsigned incl = c;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -1099,6 +1106,9 @@ struct Sim1D {
             throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
         APIC_CUDA(cudaGetDevice(&device));
         APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        int least_priority = 0, greatest_priority = 0;
+        APIC_CUDA(cudaDeviceGetStreamPriorityRange(&least_priority, &greatest_priority));
+        post_priority = greatest_priority;
 
         const bool dir = c.boundary == APIC_DIRICHLET;
         p.nspecies = c.nspecies;
@@ -1276,8 +1286,8 @@ struct Sim1D {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         size_t tiles = 0;
         for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
-        // one resident wave: k_pass1d runs two CTAs per SM
-        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * 2));
+        // one resident wave of k_pass1d: kMinBlocks CTAs per SM
+        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * kMinBlocks));
         return blocks_cache;
     }
 
@@ -1309,11 +1319,27 @@ struct Sim1D {
         APIC_CUDA(cudaFuncSetAttribute(k_post1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
     }
 
+    // The post kernel takes a whole SM's registers (one 512-thread CTA), so
+    // when several runs step together on the GPU it is launched at the
+    // highest stream priority: the CTA scheduler then gives it the next free
+    // SM instead of another run's pass CTA, and no run waits behind the others.
+    int post_priority = 0;
+
     template <int VDIM, bool DIR, bool F32>
     void launch_kernels(const Params1D& q, int blocks, size_t smem, size_t post_smem, unsigned post, EvPair& ev) {
         k_pass1d<VDIM, DIR, F32><<<blocks, kThreads, smem, stream>>>(q);
         if (timing) cudaEventRecord(ev.b, stream);
-        k_post1d<VDIM, DIR, F32><<<1, kPostThreads, post_smem, stream>>>(q, post);
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(1);
+        lc.blockDim = dim3(kPostThreads);
+        lc.dynamicSmemBytes = post_smem;
+        lc.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributePriority;
+        attr[0].val.priority = post_priority;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        APIC_CUDA(cudaLaunchKernelEx(&lc, k_post1d<VDIM, DIR, F32>, q, post));
     }
 
     void launch_pass(unsigned mode, unsigned post) {
