@@ -886,7 +886,8 @@ def bench_swarm(args, rank, dist):
                   "mean_steps": float(steps_done.mean()), "serving_particle_steps_per_s": serve_value,
                   "mixed": mixed},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm if achieved else None, "traffic": _profiled_traffic("k_swarm_push_c5_fp32.md"),
+                     "frac": achieved / hbm if achieved else None, "traffic": None,
+                     "traffic_note": "no ncu capture at the saturation size: the pool there spans tens of GB",
                      "peak_kind": peak_kind, "kernel": "k_swarm_push<float>",
                      "bytes_per_particle_step": "24 (burn-in) / 48 (sampling)",
                      "push_ms_per_launch": push_ms / max(push_launches, 1),
