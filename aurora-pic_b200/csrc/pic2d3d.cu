@@ -748,9 +748,12 @@ __global__ void k_unpermute(const unsigned* id, const double* src, double* dst, 
 // ---- spectral Poisson solve: line FFTs in shared memory -----------------------------
 
 enum : int { kFwdFromRho = 0, kFwdInPlace = 1, kFwdMulInv = 2, kInvInPlace = 3, kInvToFields = 4 };
+constexpr int kFftThreads = 256;             // threads per FFT tile
+constexpr size_t kFftTileBytes = 100 * 1024;  // shared-memory budget of one tile (lines per tile follow)
 
 struct FftPass {
     int n, log2n;
+    int log2T;              // log2 of T (every extent and T are powers of two)
     long long es, ls;       // element stride, stride between the tile's lines
     int T;                  // lines per tile
     long long tiles_inner;  // tiles per outer slab
@@ -761,6 +764,7 @@ struct FftPass {
 
 struct FieldsND {
     int dims, nx, ny, nz;
+    int lnx, lny;  // log2 nx, log2 ny (power-of-two extents)
     double L[3], eps, inv_scale, pack;  // pack: power of two that balances phi and E in one complex array
     unsigned long long* rho_acc;
     const double* rho_in;  // when set, the forward pass reads FP64 rho instead of the accumulator
@@ -858,10 +862,11 @@ __device__ __forceinline__ void dft_reg(Cplx (&a)[R], bool inv) { dft_small<R>(a
 template <int R>
 __device__ void stockham_stage(const Cplx* __restrict__ src, Cplx* __restrict__ dst, int lines, int n, int L,
                                const Cplx* tw, bool inv) {
-    const int nb = n / R;
+    const int nb = n / R;  // a power of two
+    const int lnb = __ffs(nb) - 1;
     const int tstep = n / (L * R);
     for (int b = threadIdx.x; b < lines * nb; b += blockDim.x) {
-        const int l = b / nb, j = b - l * nb;
+        const int l = b >> lnb, j = b & (nb - 1);
         const int k = j & (L - 1);
         const Cplx* s = src + l * n;
         Cplx a[R];
@@ -917,12 +922,12 @@ __device__ __forceinline__ long long tile_base(const FftPass& f, long long tile)
 
 // element b of the tile: (line l, element e) so that consecutive b are consecutive in memory
 __device__ __forceinline__ void tile_elem(const FftPass& f, int b, int& l, int& e) {
-    if (f.es == 1) { l = b / f.n; e = b % f.n; }
-    else { e = b / f.T; l = b % f.T; }
+    if (f.es == 1) { l = b >> f.log2n; e = b & (f.n - 1); }
+    else { e = b >> f.log2T; l = b & (f.T - 1); }
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
+__global__ void __launch_bounds__(kFftThreads) k_fft(FieldsND F, FftPass f) {
     extern __shared__ __align__(16) unsigned char fsm[];
     // shared memory: region0 (2 T lines) and region1 (2 T lines), then the
     // n twiddles; a single array ping-pongs inside region0, an (A, B) pair
@@ -989,9 +994,9 @@ __global__ void __launch_bounds__(kThreads) k_fft(FieldsND F, FftPass f) {
             int l, e;
             tile_elem(f, b, l, e);
             const long long g = base + l * f.ls + e * f.es;
-            const int ix = (int)(g % F.nx);
-            const int iy = (int)((g / F.nx) % F.ny);
-            const int iz = F.dims == 3 ? (int)(g / ((long long)F.nx * F.ny)) : 0;
+            const int ix = (int)(g & (F.nx - 1));
+            const int iy = (int)((g >> F.lnx) & (F.ny - 1));
+            const int iz = F.dims == 3 ? (int)(g >> (F.lnx + F.lny)) : 0;
             const Cplx r = X[l * ld + e];
             Cplx a = {0.0, 0.0}, bb = {0.0, 0.0};
             if (ix != 0 || iy != 0 || iz != 0) {
@@ -1164,6 +1169,7 @@ struct Solver {
             f.tiles_inner = nx / T; f.outer_stride = nx;
         }
         f.log2n = ilog2(f.n);
+        f.log2T = ilog2(T);
         return f;
     }
 
@@ -1175,6 +1181,8 @@ struct Solver {
     void setup(int dims, const size_t* n, const double* L, double eps, double inv_scale) {
         F.dims = dims;
         F.nx = (int)n[0]; F.ny = (int)n[1]; F.nz = dims == 3 ? (int)n[2] : 1;
+        F.lnx = ilog2(F.nx);
+        F.lny = ilog2(F.ny);
         for (int a = 0; a < 3; ++a) F.L[a] = a < dims ? L[a] : 1.0;
         F.eps = eps;
         F.inv_scale = inv_scale;
@@ -1195,7 +1203,7 @@ struct Solver {
         // so that two CTAs fit on an SM (about 100 KB of shared memory each)
         auto lines = [](int n, long long available, int buffers) {
             int T = 8;
-            while (T > 1 && (size_t)buffers * T * n * sizeof(Cplx) + n * sizeof(Cplx) > 100 * 1024) T >>= 1;
+            while (T > 1 && (size_t)buffers * T * n * sizeof(Cplx) + n * sizeof(Cplx) > kFftTileBytes) T >>= 1;
             while (T > 1 && available % T) T >>= 1;
             return T;
         };
@@ -1225,15 +1233,15 @@ struct Solver {
     // rho_acc -> rho, phi, E (the fixed-point accumulator is cleared)
     void solve() {
         if (F.dims == 2) {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
-            k_fft<kFwdMulInv><<<(unsigned)tiles(py), kThreads, smem_of(py, kFwdMulInv), stream>>>(F, py);
-            k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kFftThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
+            k_fft<kFwdMulInv><<<(unsigned)tiles(py), kFftThreads, smem_of(py, kFwdMulInv), stream>>>(F, py);
+            k_fft<kInvToFields><<<(unsigned)tiles(px), kFftThreads, smem_of(px, kInvToFields), stream>>>(F, px);
         } else {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
-            k_fft<kFwdInPlace><<<(unsigned)tiles(pys), kThreads, smem_of(pys, kFwdInPlace), stream>>>(F, pys);
-            k_fft<kFwdMulInv><<<(unsigned)tiles(pz), kThreads, smem_of(pz, kFwdMulInv), stream>>>(F, pz);
-            k_fft<kInvInPlace><<<(unsigned)tiles(py), kThreads, smem_of(py, kInvInPlace), stream>>>(F, py);
-            k_fft<kInvToFields><<<(unsigned)tiles(px), kThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kFftThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
+            k_fft<kFwdInPlace><<<(unsigned)tiles(pys), kFftThreads, smem_of(pys, kFwdInPlace), stream>>>(F, pys);
+            k_fft<kFwdMulInv><<<(unsigned)tiles(pz), kFftThreads, smem_of(pz, kFwdMulInv), stream>>>(F, pz);
+            k_fft<kInvInPlace><<<(unsigned)tiles(py), kFftThreads, smem_of(py, kInvInPlace), stream>>>(F, py);
+            k_fft<kInvToFields><<<(unsigned)tiles(px), kFftThreads, smem_of(px, kInvToFields), stream>>>(F, px);
         }
         APIC_CUDA(cudaGetLastError());
     }
@@ -2008,6 +2016,8 @@ extern "C" int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, c
         F.nx = (int)n[0];
         F.ny = (int)n[1];
         F.nz = dims == 3 ? (int)n[2] : 1;
+        F.lnx = ilog2(F.nx);
+        F.lny = ilog2(F.ny);
         for (int a = 0; a < 3; ++a) F.L[a] = a < dims ? length[a] : 1.0;
         F.eps = permittivity;
         F.inv_scale = 1.0;
@@ -2023,7 +2033,7 @@ extern "C" int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, c
         F.E = E;
         auto lines = [](int len, long long available, int buffers) {
             int T = 8;
-            while (T > 1 && (size_t)buffers * T * len * sizeof(Cplx) + len * sizeof(Cplx) > 100 * 1024) T >>= 1;
+            while (T > 1 && (size_t)buffers * T * len * sizeof(Cplx) + len * sizeof(Cplx) > kFftTileBytes) T >>= 1;
             while (T > 1 && available % T) T >>= 1;
             return T;
         };
