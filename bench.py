@@ -311,9 +311,12 @@ def _profiled_traffic(name):
         return None
 
 
-def _reduce(dist, t_ms, work):
+def _reduce(dist, t_ms, work, device="cuda"):
+    """Whole-job figures of the replicas: the slowest rank's device time (the
+    job ends when it does) and the work summed over ranks.  `device` is the
+    process group's tensor device ("cuda" for NCCL, "cpu" for gloo)."""
     import torch
-    t = torch.tensor([t_ms, work], dtype=torch.float64, device="cuda")
+    t = torch.tensor([t_ms, work], dtype=torch.float64, device=device)
     if dist:
         dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
         dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
