@@ -641,6 +641,7 @@ def _bind_swarm():
     L.apic_swarm_server_complete.argtypes = [P, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.apic_swarm_server_stats.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_size_t)]
     L.apic_swarm_server_cuda_stream.argtypes = [P, C.POINTER(P)]
+    L.apic_swarm_server_copy_bytes.argtypes = [P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.apic_swarm_server_set_kernel_timing.argtypes = [P, C.c_int]
     L.apic_swarm_server_kernel_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                  C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
@@ -718,6 +719,12 @@ class SwarmServer:
         s = C.c_void_p()
         _check_swarm(_bind_swarm().apic_swarm_server_cuda_stream(self.h, C.byref(s)), self.h)
         return s.value or 0
+
+    def copy_bytes(self):
+        """(host -> device, device -> host) bytes the server has copied."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check_swarm(_bind_swarm().apic_swarm_server_copy_bytes(self.h, C.byref(a), C.byref(b)), self.h)
+        return a.value, b.value
 
     def kernel_launches(self) -> int:
         n = C.c_uint64()

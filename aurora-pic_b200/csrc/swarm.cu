@@ -817,6 +817,16 @@ struct Server {
     std::string last_error;
     int device = 0;
     cudaStream_t stream = nullptr;
+    // host <-> device bytes of the serving loop (run set-up, tables, samples, results)
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    void copy_h2d(void* dst, const void* src, size_t bytes) {
+        APIC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        h2d_bytes += bytes;
+    }
+    void copy_d2h(void* dst, const void* src, size_t bytes) {
+        APIC_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+        d2h_bytes += bytes;
+    }
     std::vector<void*> allocations;
     MccModelDev model{};
     double neutral_density = 0.0, max_frequency = 0.0;
@@ -1101,7 +1111,7 @@ struct Server {
         S.active = 1;
         S.weight = 1.0;
         h_st[slot] = S;
-        APIC_CUDA(cudaMemcpyAsync(d_st + slot, &h_st[slot], sizeof S, cudaMemcpyHostToDevice, stream));
+        copy_h2d(d_st + slot, &h_st[slot], sizeof S);
         if (fp32) k_swarm_init<float><<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, stream>>>(C);
         else k_swarm_init<double><<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, stream>>>(C);
         APIC_CUDA(cudaGetLastError());
@@ -1120,17 +1130,15 @@ struct Server {
                 h_chunk_run.push_back((uint32_t)s);
                 h_chunk_first.push_back(k * kChunk);
             }
-            APIC_CUDA(cudaMemcpyAsync(d_cfg + s, &r.cfg, sizeof(RunCfg), cudaMemcpyHostToDevice, stream));
+            copy_h2d(d_cfg + s, &r.cfg, sizeof(RunCfg));
         }
         const uint32_t nc = (uint32_t)h_chunk_run.size();
         if (nc) {
-            APIC_CUDA(cudaMemcpyAsync(d_chunk_run, h_chunk_run.data(), nc * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                                      stream));
-            APIC_CUDA(cudaMemcpyAsync(d_chunk_first, h_chunk_first.data(), nc * sizeof(uint32_t),
-                                      cudaMemcpyHostToDevice, stream));
+            copy_h2d(d_chunk_run, h_chunk_run.data(), nc * sizeof(uint32_t));
+            copy_h2d(d_chunk_first, h_chunk_first.data(), nc * sizeof(uint32_t));
         }
         nchunks_host_ = nc;
-        APIC_CUDA(cudaMemcpyAsync(d_nchunks, &nchunks_host_, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
+        copy_h2d(d_nchunks, &nchunks_host_, sizeof(uint32_t));
         // the host copies above read pageable host memory: wait before it changes
         APIC_CUDA(cudaStreamSynchronize(stream));
         tables_dirty = false;
@@ -1208,14 +1216,13 @@ struct Server {
         const size_t total_ns = r.steps - r.burn_in_steps;
         if (out.status == APIC_OK && ns > 0) {
             std::vector<double> smp(3 * total_ns);
-            APIC_CUDA(cudaMemcpyAsync(smp.data(), run.cfg.samples, smp.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                      stream));
+            copy_d2h(smp.data(), run.cfg.samples, smp.size() * sizeof(double));
             if (r.population_model == APIC_SWARM_FIXED) {
                 if (fp32) k_swarm_moments<float><<<1, kThreads, 0, stream>>>(run.cfg, d_st + slot);
                 else k_swarm_moments<double><<<1, kThreads, 0, stream>>>(run.cfg, d_st + slot);
                 APIC_CUDA(cudaGetLastError());
             }
-            APIC_CUDA(cudaMemcpyAsync(&S, d_st + slot, sizeof S, cudaMemcpyDeviceToHost, stream));
+            copy_d2h(&S, d_st + slot, sizeof S);
             APIC_CUDA(cudaStreamSynchronize(stream));
             const double* vs = smp.data();
             const double* es = smp.data() + total_ns;
@@ -1279,7 +1286,7 @@ struct Server {
         run = Run{};
         RunState off{};
         h_st[slot] = off;
-        APIC_CUDA(cudaMemcpyAsync(d_st + slot, &h_st[slot], sizeof(RunState), cudaMemcpyHostToDevice, stream));
+        copy_h2d(d_st + slot, &h_st[slot], sizeof(RunState));
         APIC_CUDA(cudaStreamSynchronize(stream));
         tables_dirty = true;
     }
@@ -1299,10 +1306,8 @@ struct Server {
         const size_t have = rw.hv.size();
         rw.hv.resize(ns);
         rw.he.resize(ns);
-        APIC_CUDA(cudaMemcpyAsync(rw.hv.data() + have, run.cfg.samples + have, (ns - have) * sizeof(double),
-                                  cudaMemcpyDeviceToHost, stream));
-        APIC_CUDA(cudaMemcpyAsync(rw.he.data() + have, run.cfg.samples + total_ns + have,
-                                  (ns - have) * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        copy_d2h(rw.hv.data() + have, run.cfg.samples + have, (ns - have) * sizeof(double));
+        copy_d2h(rw.he.data() + have, run.cfg.samples + total_ns + have, (ns - have) * sizeof(double));
         APIC_CUDA(cudaStreamSynchronize(stream));
         double mv, sv, me, se;
         block_mean_and_error(rw.hv.data(), ns, r.uncertainty_blocks, mv, sv);
@@ -1385,8 +1390,7 @@ struct Server {
             kernel_launches += conf.steps_per_launch * (timing || branching ? 6 : 3);
             ++launches;
             if (!h_st_pinned) APIC_CUDA(cudaMallocHost(&h_st_pinned, h_st.size() * sizeof(RunState)));
-            APIC_CUDA(cudaMemcpyAsync(h_st_pinned, d_st, h_st.size() * sizeof(RunState), cudaMemcpyDeviceToHost,
-                                      stream));
+            copy_d2h(h_st_pinned, d_st, h_st.size() * sizeof(RunState));
             launched = true;
         }
     }
@@ -1519,6 +1523,13 @@ int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic_swarm_resul
             srv->impl.done.erase(it);
         }
     });
+}
+
+int apic_swarm_server_copy_bytes(apic_swarm_server* srv, uint64_t* h2d, uint64_t* d2h) {
+    if (!srv) return APIC_ERR_INVALID;
+    if (h2d) *h2d = srv->impl.h2d_bytes;
+    if (d2h) *d2h = srv->impl.d2h_bytes;
+    return APIC_OK;
 }
 
 int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,

@@ -847,7 +847,8 @@ def bench_swarm(args, rank, dist):
     gaps = rng.exponential(1.0 / rate, args.requests)
     arrivals = np.cumsum(gaps)
     reqs = [_swarm_draw(rng, spec, W, k, 30_000_000 + 1000 * rank) for k in range(args.requests)]
-    _, ps2, _ = srv.stats()
+    g2, ps2, _ = srv.stats()
+    h2d0, d2h0 = srv.copy_bytes()
     t0 = time.perf_counter()
     sub, lat, results = {}, [], []
     nxt = 0
@@ -866,7 +867,9 @@ def bench_swarm(args, rank, dist):
         if not active and not queued and nxt < args.requests:
             time.sleep(max(0.0, arrivals[nxt] - (time.perf_counter() - t0)))
     t_serve = time.perf_counter() - t0
-    _, ps3, _ = srv.stats()
+    g3, ps3, _ = srv.stats()
+    h2d1, d2h1 = srv.copy_bytes()
+    serve_steps = max(1, (g3 - g2) * spl)  # device steps of the serving phase
     serve_value = (ps3 - ps2) / t_serve
     mixed = _mixed_serving(args, srv, spec, rng, rate, rank) if args.mixed_requests > 0 else None
     srv.close()
@@ -881,8 +884,11 @@ def bench_swarm(args, rank, dist):
                    "FP64 electrons", "saturation_requests": len(batch), "steps_per_launch": spl,
                    "autotuned": tuned["table"] if tuned else None,
                    "l2": "electron state of the batch larger than L2"},
-        "e2e": {"value": serve_value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
-                "note": "Poisson serving phase through the swarm server API: requests and results are host structs"},
+        "e2e": {"value": serve_value, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": (h2d1 - h2d0) / serve_steps, "d2h_bytes_per_step": (d2h1 - d2h0) / serve_steps,
+                "note": ("Poisson serving phase through the swarm server API, host wall clock: requests and "
+                         "results are host structs; bytes per device step are the server's own copies (run "
+                         "set-up, chunk tables, samples read for the convergence test, results)")},
         "swarm": {"p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
                   "capacity_requests_per_s": capacity, "arrival_rate_requests_per_s": rate,
                   "requests": int(args.requests), "converged_fraction": float(np.mean([r.converged for r in results])),

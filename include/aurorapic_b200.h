@@ -494,6 +494,10 @@ APIC_EXPORT int apic_swarm_server_poll(apic_swarm_server* srv, uint64_t id, apic
 APIC_EXPORT int apic_swarm_server_stats(apic_swarm_server* srv, uint64_t* graph_launches, uint64_t* particle_steps,
                                         size_t* pool_bytes_free);
 APIC_EXPORT int apic_swarm_server_cuda_stream(apic_swarm_server* srv, void** stream);
+/* Bytes the server has copied host -> device (run set-up, chunk tables) and
+ * device -> host (samples for the convergence test, finished runs' results)
+ * since it was created.  No counterpart in the reference, which has no server. */
+APIC_EXPORT int apic_swarm_server_copy_bytes(apic_swarm_server* srv, uint64_t* h2d, uint64_t* d2h);
 /* Step kernels the server has launched (inside its graphs included). */
 APIC_EXPORT int apic_swarm_server_kernel_launches(apic_swarm_server* srv, uint64_t* launches);
 /* Diagnostics: with timing on, advance launches the step kernels one by one

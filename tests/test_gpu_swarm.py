@@ -142,8 +142,12 @@ def test_result_identical_alone_and_in_the_mix():
     alone = _server(spec)
     a_id = alone.submit(probe)
     a = _drain(alone, [a_id])[a_id]
+    h2d, d2h = alone.copy_bytes()
     alone.close()
     assert a.status == 0, a.message
+    # the server's own traffic: at least the run's state record in, and the
+    # sampled drift and energy series (steps after burn-in, 8 B each) out
+    assert h2d > 0 and d2h >= 2 * (640 - 320) * 8
     mix = _server(spec, max_runs=4)
     ids = [mix.submit(W.swarm_request(spec, td, particles=n, seed=s))
            for td, n, s in ((30.0, 3000, 1), (500.0, 12000, 2), (80.0, 2500, 3))]
