@@ -553,6 +553,25 @@ def field_solve_periodic_nd(dims, n, length, permittivity, rho):
     return phi, E.reshape(dims, N)
 
 
+def field_solve_mixed_2d(n, length, periodic_axis, permittivity, lower_potential, upper_potential, rho):
+    """FieldSolver::solve(Mesh2D&) with one periodic axis (0: x, 1: y) and wall
+    potentials on the other; returns (phi, E[2]) on the nx * ny mesh."""
+    L = _bind_nd()
+    L.apic_field_solve_mixed_2d.argtypes = [C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.c_int, C.c_double,
+                                            C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]
+    N = int(n[0] * n[1])
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    if rho.size != N:
+        raise ValueError("rho must hold nx * ny values")
+    phi, E = np.zeros(N), np.zeros(2 * N)
+    ns = (C.c_size_t * 2)(int(n[0]), int(n[1]))
+    Lv = np.ascontiguousarray(length, dtype=np.float64)
+    _check_nd(L.apic_field_solve_mixed_2d(ns, dptr(Lv), periodic_axis, permittivity, lower_potential,
+                                          upper_potential, dptr(rho), dptr(phi), dptr(E)))
+    return phi, E.reshape(2, N)
+
+
 def _simnd_load_maxwellian(self, species, n, seed, thermal_speed, drift_x=0.0, perturb_axis=0, perturb_amplitude=0.0):
     L = _bind_nd()
     L.apic_simnd_load_maxwellian.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_double, C.c_double,

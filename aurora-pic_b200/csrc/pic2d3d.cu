@@ -1747,6 +1747,196 @@ struct SimND {
 }  // namespace nd
 }  // namespace apic
 
+// ---- 2D solve with one periodic axis ------------------------------------------------
+//
+// FieldSolver::solve(Mesh2D&) for a mesh with exactly one periodic axis
+// (solve_mixed_spectral_tridiagonal, src/FieldSolver.cpp:501-657): every row
+// along the periodic axis is Fourier transformed, each mode solves a
+// tridiagonal system across the wall axis (discrete eigenvalue
+// 4 sin^2(pi m / N) / h^2 of the periodic second difference, wall potentials on
+// mode 0 scaled by N), the rows are transformed back, and E follows from the
+// finite differences of compute_electric_field (src/FieldSolver.cpp:298-346).
+// The spectra are stored wall-row-major (hat[d * np + m]) so that the one
+// thread per mode of the tridiagonal kernel reads and writes coalesced rows.
+
+namespace apic {
+namespace nd {
+
+__device__ __forceinline__ size_t mixed_index(int d, int q, int nx, int periodic_y) {
+    return periodic_y ? (size_t)q * nx + d : (size_t)d * nx + q;
+}
+
+__global__ void __launch_bounds__(kFftThreads) k_mixed_forward(const double* __restrict__ rho, Cplx* __restrict__ hat,
+                                                               int nx, int np, int periodic_y, const Cplx* tw) {
+    extern __shared__ __align__(16) unsigned char msm[];
+    Cplx* a = reinterpret_cast<Cplx*>(msm);
+    Cplx* b = a + np;
+    Cplx* tws = b + np;
+    const int d = blockIdx.x;
+    for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        tws[q] = tw[q];
+        a[q] = {rho[mixed_index(d, q, nx, periodic_y)], 0.0};
+    }
+    __syncthreads();
+    const Cplx* r = fft_lines(a, b, 1, np, tws, false);
+    for (int m = threadIdx.x; m < np; m += blockDim.x) hat[(size_t)d * np + m] = r[m];
+}
+
+// One thread per mode: the forward sweep keeps modified_rhs in place of
+// rho_hat and modified_upper (real for these real coefficients) in mu; the
+// back substitution leaves phi_hat in hat.
+__global__ void k_mixed_tridiag(Cplx* __restrict__ hat, double* __restrict__ mu, int nd, int np, double inv_dsq,
+                                double inv_psq, double eps, double lower, double upper) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= np) return;
+    const int ni = nd - 2;
+    const double angle = 3.141592653589793 * (double)m / (double)np;
+    const double eig = 4.0 * sin(angle) * sin(angle) * inv_psq;
+    const double diag = 2.0 * inv_dsq + eig;
+    const double off = -inv_dsq;
+    const double scale = (double)np;
+    const double lb = m == 0 ? lower * scale : 0.0, ub = m == 0 ? upper * scale : 0.0;
+    double pr = 0.0, pi = 0.0, pu = 0.0;  // modified_rhs and modified_upper of the previous row
+    for (int k = 0; k < ni; ++k) {
+        const Cplx rh = hat[(size_t)(k + 1) * np + m];
+        double rr = rh.re / eps, ri = rh.im / eps;
+        if (k == 0) rr += inv_dsq * lb;
+        if (k + 1 == ni) rr += inv_dsq * ub;
+        double u, xr, xi;
+        if (k == 0) {
+            u = off / diag;
+            xr = rr / diag;
+            xi = ri / diag;
+        } else {
+            const double den = diag - off * pu;
+            u = k + 1 == ni ? 0.0 : off / den;
+            xr = (rr - off * pr) / den;
+            xi = (ri - off * pi) / den;
+        }
+        hat[(size_t)(k + 1) * np + m] = {xr, xi};
+        mu[(size_t)k * np + m] = u;
+        pr = xr; pi = xi; pu = u;
+    }
+    hat[m] = {lb, 0.0};
+    hat[(size_t)(nd - 1) * np + m] = {ub, 0.0};
+    for (int k = ni - 2; k >= 0; --k) {
+        const Cplx nxt = hat[(size_t)(k + 2) * np + m];
+        const Cplx cur = hat[(size_t)(k + 1) * np + m];
+        const double u = mu[(size_t)k * np + m];
+        hat[(size_t)(k + 1) * np + m] = {cur.re - u * nxt.re, cur.im - u * nxt.im};
+    }
+}
+
+__global__ void __launch_bounds__(kFftThreads) k_mixed_inverse(const Cplx* __restrict__ hat, double* __restrict__ phi,
+                                                               int nx, int np, int periodic_y, const Cplx* tw) {
+    extern __shared__ __align__(16) unsigned char msm[];
+    Cplx* a = reinterpret_cast<Cplx*>(msm);
+    Cplx* b = a + np;
+    Cplx* tws = b + np;
+    const int d = blockIdx.x;
+    for (int m = threadIdx.x; m < np; m += blockDim.x) {
+        tws[m] = tw[m];
+        a[m] = hat[(size_t)d * np + m];
+    }
+    __syncthreads();
+    const Cplx* r = fft_lines(a, b, 1, np, tws, true);
+    for (int q = threadIdx.x; q < np; q += blockDim.x) phi[mixed_index(d, q, nx, periodic_y)] = r[q].re;
+}
+
+// compute_electric_field(Mesh2D&), src/FieldSolver.cpp:298-346
+__global__ void k_mixed_efield(const double* __restrict__ phi, double* __restrict__ E, int nx, int ny, double dx,
+                               double dy, int periodic_x, int periodic_y) {
+    const size_t N = (size_t)nx * ny;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < N; idx += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx), j = (int)(idx / nx);
+        const size_t row = (size_t)j * nx;
+        double ex, ey;
+        if (periodic_x) ex = -(phi[row + (i + 1) % nx] - phi[row + (i + nx - 1) % nx]) / (2.0 * dx);
+        else if (i == 0) ex = -(phi[row + 1] - phi[idx]) / dx;
+        else if (i + 1 == nx) ex = -(phi[idx] - phi[row + i - 1]) / dx;
+        else ex = -(phi[row + i + 1] - phi[row + i - 1]) / (2.0 * dx);
+        if (periodic_y) ey = -(phi[(size_t)((j + 1) % ny) * nx + i] - phi[(size_t)((j + ny - 1) % ny) * nx + i]) / (2.0 * dy);
+        else if (j == 0) ey = -(phi[(size_t)nx + i] - phi[idx]) / dy;
+        else if (j + 1 == ny) ey = -(phi[idx] - phi[row - nx + i]) / dy;
+        else ey = -(phi[row + nx + i] - phi[row - nx + i]) / (2.0 * dy);
+        E[idx] = ex;
+        E[N + idx] = ey;
+    }
+}
+
+// device arrays and stream of one call, released on every exit path
+struct MixedScratch {
+    cudaStream_t s = nullptr;
+    std::vector<void*> a;
+    ~MixedScratch() {
+        if (s) cudaStreamSynchronize(s);
+        for (void* p : a) cudaFree(p);
+        if (s) cudaStreamDestroy(s);
+    }
+    template <class T>
+    T* get(size_t count) {
+        void* p = nullptr;
+        APIC_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+        a.push_back(p);
+        return static_cast<T*>(p);
+    }
+};
+
+static void solve_mixed_2d(const size_t* n, const double* length, int periodic_axis, double permittivity,
+                           double lower, double upper, const double* rho, double* phi, double* electric) {
+    require(n && length && rho && phi && electric, "null argument");
+    require(periodic_axis == 0 || periodic_axis == 1, "periodic_axis must be 0 (x) or 1 (y)");
+    require(std::isfinite(permittivity) && permittivity > 0, "field-solver permittivity must be positive and finite");
+    require(std::isfinite(lower) && std::isfinite(upper), "wall potentials must be finite");
+    const int periodic_y = periodic_axis == 1;
+    const size_t nx = n[0], ny = n[1];
+    const size_t nd = periodic_y ? nx : ny, np = periodic_y ? ny : nx;
+    require(nd >= 3, "the wall axis needs at least 3 nodes");
+    require(pow2(np) && np <= (size_t)kMaxLine, "the periodic extent must be a power of two up to 1024",
+            APIC_ERR_UNSUPPORTED);
+    for (int a = 0; a < 2; ++a)
+        require(std::isfinite(length[a]) && length[a] > 0, "domain lengths must be positive and finite");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
+    // Mesh2D spacings, src/Mesh2D.cpp:57-60
+    const double dx = length[0] / (double)(periodic_y ? nx - 1 : nx);
+    const double dy = length[1] / (double)(periodic_y ? ny : ny - 1);
+    const double hd = periodic_y ? dx : dy, hp = periodic_y ? dy : dx;
+    const size_t N = nx * ny;
+    MixedScratch S;
+    APIC_CUDA(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
+    double* d_rho = S.get<double>(N);
+    double* d_phi = S.get<double>(N);
+    double* d_E = S.get<double>(2 * N);
+    double* d_mu = S.get<double>(N);
+    Cplx* d_hat = S.get<Cplx>(N);
+    Cplx* d_tw = S.get<Cplx>(np);
+    std::vector<Cplx> tw(np);
+    const double twopi = 2.0 * 3.141592653589793;
+    for (size_t k = 0; k < np; ++k) tw[k] = {std::cos(twopi * k / np), -std::sin(twopi * k / np)};
+    APIC_CUDA(cudaMemcpyAsync(d_tw, tw.data(), np * sizeof(Cplx), cudaMemcpyHostToDevice, S.s));
+    APIC_CUDA(cudaMemcpyAsync(d_rho, rho, N * sizeof(double), cudaMemcpyHostToDevice, S.s));
+    const size_t smem = 3 * np * sizeof(Cplx);
+    APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_mixed_forward<<<(unsigned)nd, kFftThreads, smem, S.s>>>(d_rho, d_hat, (int)nx, (int)np, periodic_y, d_tw);
+    k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, S.s>>>(d_hat, d_mu, (int)nd, (int)np, 1.0 / (hd * hd),
+                                                                     1.0 / (hp * hp), permittivity, lower, upper);
+    k_mixed_inverse<<<(unsigned)nd, kFftThreads, smem, S.s>>>(d_hat, d_phi, (int)nx, (int)np, periodic_y, d_tw);
+    k_mixed_efield<<<(unsigned)std::min<size_t>((N + 255) / 256, 4096), 256, 0, S.s>>>(
+        d_phi, d_E, (int)nx, (int)ny, dx, dy, periodic_y ? 0 : 1, periodic_y);
+    APIC_CUDA(cudaGetLastError());
+    APIC_CUDA(cudaMemcpyAsync(phi, d_phi, N * sizeof(double), cudaMemcpyDeviceToHost, S.s));
+    APIC_CUDA(cudaMemcpyAsync(electric, d_E, 2 * N * sizeof(double), cudaMemcpyDeviceToHost, S.s));
+    const cudaError_t e = bounded_wait(S.s, 600.0);
+    if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
+    APIC_CUDA(e);
+}
+
+}  // namespace nd
+}  // namespace apic
+
 // ---- C ABI ---------------------------------------------------------------------------
 
 struct apic_sim_nd {
@@ -1907,6 +2097,13 @@ int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length
         S.solver.solve();
         S.read_fields(nullptr, phi, electric);
     });
+}
+
+int apic_field_solve_mixed_2d(const size_t* n, const double* length, int periodic_axis, double permittivity,
+                              double lower_potential, double upper_potential, const double* rho, double* phi,
+                              double* electric) {
+    return guarded_nd(nullptr, [&] { apic::nd::solve_mixed_2d(n, length, periodic_axis, permittivity,
+                                                              lower_potential, upper_potential, rho, phi, electric); });
 }
 
 }  // extern "C"

@@ -367,6 +367,21 @@ APIC_EXPORT int apic_simnd_launch_count(apic_sim_nd* sim, uint64_t* launches);
 APIC_EXPORT int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,
                                              const double* rho, double* phi, double* electric);
 
+/* FieldSolver::solve(Mesh2D&) for a mesh with exactly one periodic axis
+ * (solve_mixed_spectral_tridiagonal, src/FieldSolver.cpp:501-657, and
+ * compute_electric_field, :298-346): Fourier transform along the periodic axis,
+ * one tridiagonal solve per mode across the wall axis, wall potentials on mode
+ * 0.  periodic_axis 0: x periodic, walls at y = 0 (lower_potential, the
+ * reference's bottom) and y = Ly (upper, top); 1: y periodic, walls at x = 0
+ * (left) and x = Lx (right).  Mesh spacings follow Mesh2D (L / n along the
+ * periodic axis, L / (n - 1) across the walls).  rho, phi: nx * ny values
+ * (index j * nx + i); electric: [2][nx * ny].  The periodic extent must be a
+ * power of two up to 1024 (APIC_ERR_UNSUPPORTED otherwise), the wall extent at
+ * least 3.  Host arrays; the call returns when the results are copied back. */
+APIC_EXPORT int apic_field_solve_mixed_2d(const size_t* n, const double* length, int periodic_axis,
+                                          double permittivity, double lower_potential, double upper_potential,
+                                          const double* rho, double* phi, double* electric);
+
 /* Allocation-free variant of apic_field_solve_periodic_nd.  No counterpart in
  * the reference: it exists for callers that cannot call cudaMalloc - hosts that
  * manage all device memory through their own pool, and stepping loops that must

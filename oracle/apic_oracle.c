@@ -995,6 +995,94 @@ void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const siz
     free(rh);
 }
 
+/* solve_mixed_spectral_tridiagonal(Mesh2D&), src/FieldSolver.cpp:501-657, for a
+ * power-of-two periodic extent (transform_1d is then fft_radix2), followed by
+ * compute_electric_field(Mesh2D&), src/FieldSolver.cpp:298-346.  Mesh index
+ * j * nx + i; periodic_axis 0: x periodic, walls along y (bottom = lower,
+ * top = upper); 1: y periodic, walls along x (left = lower, right = upper).
+ * E holds [2][nx * ny].  Returns nonzero for an unsupported shape. */
+int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* n, const double* L,
+                       int periodic_axis, double eps, double lower, double upper) {
+    const size_t nx = n[0], ny = n[1];
+    const int periodic_y = periodic_axis == 1;
+    const size_t nd = periodic_y ? nx : ny;  /* direct (wall) extent */
+    const size_t np = periodic_y ? ny : nx;  /* periodic extent */
+    if (nd < 3 || np < 2 || (np & (np - 1))) return seterr(1, "mixed solve needs a power-of-two periodic extent");
+    /* Mesh2D spacings, src/Mesh2D.cpp:57-60 */
+    const double dx = L[0] / (double)(periodic_y ? nx - 1 : nx);
+    const double dy = L[1] / (double)(periodic_y ? ny : ny - 1);
+    const double hd = periodic_y ? dx : dy, hp = periodic_y ? dy : dx;
+    const double inv_dsq = 1.0 / (hd * hd), inv_psq = 1.0 / (hp * hp);
+    const size_t ni = nd - 2;
+#define MIDX(d, q) (periodic_y ? (q) * nx + (d) : (d) * nx + (q))
+    ora_cplx* rho_hat = calloc(nd * np, sizeof(ora_cplx));
+    ora_cplx* phi_hat = calloc(nd * np, sizeof(ora_cplx));
+    ora_cplx* line = malloc(np * sizeof(ora_cplx));
+    double* mu = calloc(ni, sizeof(double)); /* modified_upper: real for real coefficients */
+    ora_cplx* mr = calloc(ni, sizeof(ora_cplx));
+    for (size_t d = 0; d < nd; ++d) {
+        for (size_t q = 0; q < np; ++q) { line[q].re = rho[MIDX(d, q)]; line[q].im = 0.0; }
+        fft_radix2(line, np, 0);
+        for (size_t m = 0; m < np; ++m) rho_hat[m * nd + d] = line[m];
+    }
+    const double off = -inv_dsq;
+    const double bscale = (double)np;
+    for (size_t m = 0; m < np; ++m) {
+        const double angle = 3.14159265358979323846 * (double)m / (double)np;
+        const double eig = 4.0 * sin(angle) * sin(angle) * inv_psq;
+        const double diag = 2.0 * inv_dsq + eig;
+        const double lb = m == 0 ? lower * bscale : 0.0, ub = m == 0 ? upper * bscale : 0.0;
+        phi_hat[m * nd + 0].re = lb; phi_hat[m * nd + 0].im = 0.0;
+        phi_hat[m * nd + nd - 1].re = ub; phi_hat[m * nd + nd - 1].im = 0.0;
+        for (size_t k = 0; k < ni; ++k) {
+            const ora_cplx rh = rho_hat[m * nd + k + 1];
+            double rr = rh.re / eps, ri = rh.im / eps;
+            if (k == 0) rr += inv_dsq * lb;  /* the boundary terms are real */
+            if (k + 1 == ni) rr += inv_dsq * ub;
+            if (k == 0) {
+                mu[k] = off / diag;
+                mr[k].re = rr / diag; mr[k].im = ri / diag;
+            } else {
+                const double den = diag - off * mu[k - 1];
+                mu[k] = k + 1 == ni ? 0.0 : off / den;
+                mr[k].re = (rr - off * mr[k - 1].re) / den;
+                mr[k].im = (ri - off * mr[k - 1].im) / den;
+            }
+        }
+        phi_hat[m * nd + nd - 2] = mr[ni - 1];
+        for (size_t k = ni - 1; k-- > 0;) {
+            const ora_cplx nxt = phi_hat[m * nd + k + 2];
+            phi_hat[m * nd + k + 1].re = mr[k].re - mu[k] * nxt.re;
+            phi_hat[m * nd + k + 1].im = mr[k].im - mu[k] * nxt.im;
+        }
+    }
+    for (size_t d = 0; d < nd; ++d) {
+        for (size_t m = 0; m < np; ++m) line[m] = phi_hat[m * nd + d];
+        fft_radix2(line, np, 1);
+        for (size_t q = 0; q < np; ++q) phi[MIDX(d, q)] = line[q].re;
+    }
+#undef MIDX
+    /* compute_electric_field(Mesh2D&), src/FieldSolver.cpp:298-346 */
+    const size_t N = nx * ny;
+    for (size_t j = 0; j < ny; ++j)
+        for (size_t i = 0; i < nx; ++i) {
+            const size_t idx = j * nx + i;
+            double ex, ey;
+            if (!periodic_y) ex = -(phi[j * nx + (i + 1) % nx] - phi[j * nx + (i + nx - 1) % nx]) / (2.0 * dx);
+            else if (i == 0) ex = -(phi[j * nx + 1] - phi[idx]) / dx;
+            else if (i + 1 == nx) ex = -(phi[idx] - phi[j * nx + i - 1]) / dx;
+            else ex = -(phi[j * nx + i + 1] - phi[j * nx + i - 1]) / (2.0 * dx);
+            if (periodic_y) ey = -(phi[((j + 1) % ny) * nx + i] - phi[((j + ny - 1) % ny) * nx + i]) / (2.0 * dy);
+            else if (j == 0) ey = -(phi[nx + i] - phi[idx]) / dy;
+            else if (j + 1 == ny) ey = -(phi[idx] - phi[(j - 1) * nx + i]) / dy;
+            else ey = -(phi[(j + 1) * nx + i] - phi[(j - 1) * nx + i]) / (2.0 * dy);
+            E[idx] = ex;
+            E[N + idx] = ey;
+        }
+    free(rho_hat); free(phi_hat); free(line); free(mu); free(mr);
+    return 0;
+}
+
 /* Periodic CIC stencil of one axis, src/Mesh2D.cpp:96-129, src/FieldSolver.cpp:936-960 */
 static void cic_axis(double x, double L, double d, size_t n, size_t* i0, size_t* i1, double* f) {
     const double xp = wrap(x, L);

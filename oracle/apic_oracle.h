@@ -95,6 +95,9 @@ const char* ora_last_error(void);
 /* ---- structured 2D3V / 3D3V periodic -------------------------------------- */
 void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
                   double eps);
+/* FieldSolver::solve(Mesh2D&) with exactly one periodic axis (power of two). */
+int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* n, const double* L,
+                       int periodic_axis, double eps, double lower, double upper);
 void ora_gather_nd(const double* E, int dims, const size_t* n, const double* L, const double* pos, double* out);
 void ora_deposit_nd(double* rho, int dims, const size_t* n, const double* L, double q, size_t np,
                     const double* pos);

@@ -467,6 +467,36 @@ def _nd_bind():
     return L
 
 
+def solve_mixed_2d(rho, n, L, periodic_axis, eps, lower, upper):
+    """Oracle FieldSolver::solve(Mesh2D&) with one periodic axis: (phi, E[2])."""
+    Lb = oracle()
+    Lb.ora_solve_mixed_2d.argtypes = [_DP, _DP, _DP, _SZP, _DP, C.c_int, C.c_double, C.c_double, C.c_double]
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    N = int(n[0] * n[1])
+    phi, E = np.zeros(N), np.zeros(2 * N)
+    nn = (C.c_size_t * 2)(*[int(v) for v in n])
+    Lv = np.ascontiguousarray(L, dtype=np.float64)
+    rc = Lb.ora_solve_mixed_2d(dptr(rho), dptr(phi), dptr(E), nn, dptr(Lv), periodic_axis, eps, lower, upper)
+    if rc:
+        raise RuntimeError(Lb.ora_last_error().decode())
+    return phi, E.reshape(2, N)
+
+
+def ref_solve_mixed_2d(rho, n, L, periodic_axis, eps, lower, upper):
+    """The reference's own FieldSolver on a mixed Mesh2D, through the harness."""
+    Lb = ref()
+    Lb.ref_solve_mixed_2d.argtypes = [_SZP, _DP, C.c_int, C.c_double, C.c_double, C.c_double, _DP, _DP, _DP]
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    N = int(n[0] * n[1])
+    phi, E = np.zeros(N), np.zeros(2 * N)
+    nn = (C.c_size_t * 2)(*[int(v) for v in n])
+    Lv = np.ascontiguousarray(L, dtype=np.float64)
+    rc = Lb.ref_solve_mixed_2d(nn, dptr(Lv), periodic_axis, eps, lower, upper, dptr(rho), dptr(phi), dptr(E))
+    if rc:
+        raise RuntimeError("reference mixed solve failed")
+    return phi, E.reshape(2, N)
+
+
 def sizes3(n):
     n = list(n) + [1] * (3 - len(n))
     return (C.c_size_t * 3)(*n)

@@ -493,6 +493,29 @@ double refnd_time(void* h) {
 }
 
 // FieldSolver::solve(Mesh2D&/Mesh3D&) on a given charge density (periodic).
+/* FieldSolver::solve(Mesh2D&) on a mesh with one periodic axis: periodic_axis
+ * 0 = x periodic with walls bottom (lower) / top (upper); 1 = y periodic with
+ * walls left (lower) / right (upper). */
+int ref_solve_mixed_2d(const size_t* n, const double* L, int periodic_axis, double eps, double lower, double upper,
+                       const double* rho, double* phi, double* E) {
+    try {
+        pic::FieldSolver solver(eps);
+        pic::BoundaryConfig2D bc;
+        if (periodic_axis == 0) { bc.bottom.potential = lower; bc.top.potential = upper; }
+        else { bc.left.potential = lower; bc.right.potential = upper; }
+        const pic::Boundary px = periodic_axis == 0 ? pic::Boundary::Periodic : pic::Boundary::Dirichlet;
+        const pic::Boundary py = periodic_axis == 0 ? pic::Boundary::Dirichlet : pic::Boundary::Periodic;
+        pic::Mesh2D mesh(n[0], n[1], L[0], L[1], px, py, bc);
+        const size_t N = n[0] * n[1];
+        std::memcpy(mesh.rho().data(), rho, N * 8);
+        solver.solve(mesh);
+        std::memcpy(phi, mesh.phi().data(), N * 8);
+        std::memcpy(E, mesh.electric_x().data(), N * 8);
+        std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
 int ref_solve_nd(int dims, const size_t* n, const double* L, double eps, const double* rho, double* phi, double* E) {
     try {
         pic::FieldSolver solver(eps);

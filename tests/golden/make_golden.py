@@ -2,7 +2,9 @@
 itself (its library compiled from the reference sources by oracle/Makefile,
 driven through oracle/ref_harness.cpp).  Run from the repository root:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [fixture ...]
+
+(no names: every fixture; a name such as `mixed` writes only that one).
 
 The fixtures pin the CPU oracle (oracle/apic_oracle.c) in
 tests/test_oracle_golden.py; the GPU parity tests then compare the device
@@ -209,7 +211,35 @@ def swarm_ensemble_fixture():
         np.savez_compressed(os.path.join(HERE, f"swarm_ensemble_{name}.npz"), **out)
 
 
-def main():
+MIXED_CASES = {
+    # name: (n, L, periodic axis, lower / upper wall potentials)
+    "mixed2d_xperiodic": ((64, 33), (0.02, 0.015), 0, (0.0, 12.5)),
+    "mixed2d_yperiodic": ((17, 32), (0.01, 0.03), 1, (-3.0, 7.0)),
+}
+
+
+def mixed_fixture():
+    """FieldSolver::solve(Mesh2D&) on meshes with one periodic axis (the
+    spectral-tridiagonal solve), from seeded charge densities."""
+    eps = 8.8541878128e-12
+    for k, (name, (n, L, axis, (lo, hi))) in enumerate(MIXED_CASES.items()):
+        rng = np.random.default_rng(90 + k)
+        nx, ny = n
+        x = np.arange(nx)[None, :] / nx
+        y = np.arange(ny)[:, None] / ny
+        rho = 1e-6 * (1.0 + 0.3 * np.sin(2 * np.pi * x) * np.cos(np.pi * y) + 0.05 * rng.standard_normal((ny, nx)))
+        phi, E = po.ref_solve_mixed_2d(rho, n, L, axis, eps, lo, hi)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), n=np.array(n), L=np.array(L), axis=axis, eps=eps,
+                            lower=lo, upper=hi, rho=rho.ravel(), phi=phi, E=E)
+
+
+def main(names=None):
+    if names:
+        for n in names:
+            globals()[f"{n}_fixture"]()
+        print("golden vectors written to", HERE)
+        return
+    mixed_fixture()
     swarm_ensemble_fixture()
     swarm_fixture()
     collide_hg_fixture()
@@ -229,4 +259,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -63,6 +63,31 @@ def test_periodic_solve_against_oracle(dims, n):
     assert rel_max(E, Er[: dims * N].reshape(dims, N)) < TOL
 
 
+@pytest.mark.parametrize("n,L,axis,walls", [((64, 33), (0.02, 0.015), 0, (0.0, 12.5)),
+                                             ((17, 32), (0.01, 0.03), 1, (-3.0, 7.0)),
+                                             ((256, 3), (1.0, 0.5), 0, (1.0, -1.0)),
+                                             ((129, 512), (0.2, 0.1), 1, (0.0, 0.0))])
+def test_mixed_periodic_wall_solve_against_oracle(n, L, axis, walls):
+    """FieldSolver::solve(Mesh2D&) with one periodic axis (spectral along it,
+    tridiagonal across the walls): phi and E within 1e-12 of the oracle, which
+    is bit-exact with the reference on the golden meshes."""
+    rng = np.random.default_rng(sum(n) + axis)
+    nx, ny = n
+    rho = 1e-6 * (1.0 + 0.3 * rng.standard_normal((ny, nx)))
+    eps = 8.8541878128e-12
+    phi, E = apic.field_solve_mixed_2d(n, L, axis, eps, walls[0], walls[1], rho)
+    pr, Er = po.solve_mixed_2d(rho, n, L, axis, eps, walls[0], walls[1])
+    assert rel_max(phi, pr) < TOL
+    assert rel_max(E, Er) < TOL
+
+
+def test_mixed_solve_rejects_unsupported_meshes():
+    with pytest.raises(apic.ApicError):
+        apic.field_solve_mixed_2d((24, 9), (1.0, 1.0), 0, 1.0, 0.0, 0.0, np.zeros(24 * 9))  # periodic 24
+    with pytest.raises(apic.ApicError):
+        apic.field_solve_mixed_2d((16, 2), (1.0, 1.0), 0, 1.0, 0.0, 0.0, np.zeros(32))  # two wall nodes
+
+
 def test_sort_keeps_identity_and_fields():
     """Sorting every step versus never: identical particles (by load order) and fields."""
     wl = W.plasma_2d(cells=(32, 32), ppc=4, seed=8)

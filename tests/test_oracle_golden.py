@@ -169,3 +169,14 @@ def test_structured_periodic_run_bit_exact(name):
             assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
     rho, phi, E = sim.fields()
     assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
+
+
+@pytest.mark.parametrize("name", ["mixed2d_xperiodic", "mixed2d_yperiodic"])
+def test_mixed_spectral_tridiagonal_solve_bit_exact(name):
+    """FieldSolver::solve(Mesh2D&) with one periodic axis and wall potentials on
+    the other (FFT along the periodic axis, one tridiagonal solve per mode,
+    finite-difference E): phi and E bit-exact."""
+    f = load(f"{name}.npz")
+    phi, E = po.solve_mixed_2d(f["rho"], tuple(int(v) for v in f["n"]), f["L"], int(f["axis"]), float(f["eps"]),
+                               float(f["lower"]), float(f["upper"]))
+    assert np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
