@@ -385,6 +385,8 @@ class ConfigND(C.Structure):
         ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
         ("push_items", C.c_int),
         ("species_sort_interval", C.c_size_t * MAX_SPECIES),
+        ("profile_axis", C.c_int), ("profile_rows", C.c_size_t),
+        ("profile_coordinates", C.POINTER(C.c_double)), ("profile_values", C.POINTER(C.c_double)),
     ]
 
 
@@ -434,7 +436,10 @@ def _check_nd(rc, handle=None):
 
 def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), units=NORMALIZED,
               relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16,
-              push_items=0, species_sort_interval=None) -> ConfigND:
+              push_items=0, species_sort_interval=None, magnetic_field_profile=None) -> ConfigND:
+    """magnetic_field_profile: optional (axis, coordinates, values[rows][3]), B
+    tabulated along one axis (the arrays are kept on the returned config until
+    the simulation is created, which copies them)."""
     c = ConfigND()
     c.dims = dims
     c.n[:] = list(n) + [1] * (3 - len(n))
@@ -448,6 +453,16 @@ def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), u
     c.nspecies = len(species)
     for i, (q, m, w, cap) in enumerate(species):
         c.species[i] = SpeciesCfg(q, m, w, cap)
+    if magnetic_field_profile is not None:
+        ax, coords, values = magnetic_field_profile
+        pc = np.ascontiguousarray(coords, dtype=np.float64)
+        pv = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        if pv.size != 3 * pc.size:
+            raise ValueError("magnetic_field_profile values must be rows x 3")
+        c._profile_keep = (pc, pv)
+        c.profile_axis, c.profile_rows = int(ax), int(pc.size)
+        c.profile_coordinates = pc.ctypes.data_as(C.POINTER(C.c_double))
+        c.profile_values = pv.ctypes.data_as(C.POINTER(C.c_double))
     return c
 
 

@@ -70,7 +70,49 @@ struct ParamsND {
     const double* E;  // interleaved: 2 doubles per node (2D) or 4 (3D)
     const float* E32; // FP32 form: float copy of E
     unsigned long long* rho_acc;
+    // magnetic_field_profile: B piecewise linear along prof_axis (prof_rows = 0: uniform B)
+    int prof_axis, prof_rows;
+    const double* prof_c;  // coordinates
+    const double* prof_v;  // rows x 3
 };
+
+// TabulatedVectorField1D::evaluate, src/PrescribedField.cpp:89-113, at coordinate
+// q inside the table (create checks that the table covers the domain).
+__device__ __forceinline__ void profile_b(const ParamsND& p, double q, double B[3]) {
+    const double* c = p.prof_c;
+    const int n = p.prof_rows;
+    int right;
+    if (q == __ldg(c)) {
+        for (int a = 0; a < 3; ++a) B[a] = __ldg(p.prof_v + a);
+        return;
+    }
+    if (q == __ldg(c + n - 1)) {
+        for (int a = 0; a < 3; ++a) B[a] = __ldg(p.prof_v + 3 * (n - 1) + a);
+        return;
+    }
+    int lo = 0, hi = n;  // std::upper_bound
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (q < __ldg(c + mid)) hi = mid; else lo = mid + 1;
+    }
+    right = lo;
+    const int left = right - 1;
+    const double f = (q - __ldg(c + left)) / (__ldg(c + right) - __ldg(c + left));
+    for (int a = 0; a < 3; ++a) {
+        const double l = __ldg(p.prof_v + 3 * left + a), r = __ldg(p.prof_v + 3 * right + a);
+        B[a] = l + f * (r - l);
+    }
+}
+
+// magnetic_field(cfg, position), src/Simulation2D.cpp:121-132, src/Simulation3D.cpp:109-118
+__device__ __forceinline__ void field_b(const ParamsND& p, const double pos[3], double B[3]) {
+    if (!p.prof_rows) {
+        B[0] = p.B[0]; B[1] = p.B[1]; B[2] = p.B[2];
+        return;
+    }
+    const int a = p.prof_axis;
+    profile_b(p, a < p.dims ? (a == 0 ? pos[0] : (a == 1 ? pos[1] : pos[2])) : 0.0, B);
+}
 
 // FP32 form: each CIC weight is rounded to a multiple of 2^-25 and summed per
 // species in 64-bit integers (runs of lanes in one cell first add theirs with a
@@ -279,7 +321,9 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     if (MODE == kPushInitHalf) {
         double v[3] = {S.v[0][i], S.v[1][i], S.v[2][i]};
         if (BORIS) {
-            boris(v, e, p.B, S.qm, -0.5 * p.dt);
+            double Bp[3];
+            field_b(p, pos, Bp);
+            boris(v, e, Bp, S.qm, -0.5 * p.dt);
         } else {
             // initialize_leapfrog_half_step, src/Pusher.cpp:88-92, :152-156
             for (int a = 0; a < DIM; ++a) v[a] = v[a] - 0.5 * S.qm * e[a] * p.dt;
@@ -290,7 +334,9 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     double vh[3] = {S.vh[buf][0][j], S.vh[buf][1][j], S.vh[buf][2][j]};
     if (MODE == kPushSync) {
         if (BORIS) {
-            boris(vh, e, p.B, S.qm, 0.5 * p.dt);
+            double Bp[3];
+            field_b(p, pos, Bp);
+            boris(vh, e, Bp, S.qm, 0.5 * p.dt);
         } else {
             // synchronize_leapfrog, src/Pusher.cpp:131-135, :176-180
             for (int a = 0; a < DIM; ++a) vh[a] = vh[a] + 0.5 * S.qm * e[a] * p.dt;
@@ -300,7 +346,9 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     }
     // kick_boris / kick_leapfrog + drift_leapfrog, src/Pusher.cpp:109-128, :162-174
     if (BORIS) {
-        boris(vh, e, p.B, S.qm, p.dt);
+        double Bp[3];
+        field_b(p, pos, Bp);
+        boris(vh, e, Bp, S.qm, p.dt);
     } else {
         for (int a = 0; a < DIM; ++a) vh[a] += S.qm * e[a] * p.dt;
     }
@@ -381,6 +429,33 @@ __device__ __forceinline__ void boris32(float v[3], const float e[3], float h, c
     v[2] = fmaf(h, e[2], vm2 + fmaf(vp0, s[1], -vp1 * s[0]));
 }
 
+// FP32 form: the Boris rotation vectors t = (q/m dt/2) B and s = 2 t / (1 + t^2)
+// of a particle, from its cell and offset when B is tabulated (the species'
+// precomputed pair otherwise), in the same FP64 expression as the species' pair.
+__device__ __forceinline__ void boris_ts32(const ParamsND& p, const SpeciesND& S, int ix, int iy, int iz,
+                                           const float f[3], float tb[3], float sb[3]) {
+    if (!p.prof_rows) {
+        for (int a = 0; a < 3; ++a) { tb[a] = S.tb[a]; sb[a] = S.sb[a]; }
+        return;
+    }
+    const int a = p.prof_axis;
+    double q = 0.0;
+    if (a < p.dims) {
+        const int cell = a == 0 ? ix : (a == 1 ? iy : iz);
+        const float off = a == 0 ? f[0] : (a == 1 ? f[1] : f[2]);
+        q = ((double)cell + (double)off) * p.d[a];
+    }
+    double B[3];
+    profile_b(p, q, B);
+    const double hq = 0.5 * S.qm * p.dt;
+    double t2 = 0.0;
+    for (int c = 0; c < 3; ++c) t2 += (hq * B[c]) * (hq * B[c]);
+    for (int c = 0; c < 3; ++c) {
+        tb[c] = (float)(hq * B[c]);
+        sb[c] = (float)(2.0 * hq * B[c] / (1.0 + t2));
+    }
+}
+
 // Moves one axis by `disp` cells: integer carry into the periodic cell index.
 __device__ __forceinline__ void advance(float& f, int& i, float disp, int n) {
     float g = f + disp;
@@ -454,9 +529,10 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
             float* vv = MODE == kPushInitHalf ? w : v;
             const float h = MODE == kPushInitHalf ? -0.5f * S.hqmdt : 0.5f * S.hqmdt;
             if (BORIS) {
-                float t[3], sb[3];
+                float t[3], sb[3], tp[3], sp[3];
+                boris_ts32(p, S, ix, iy, iz, f, tp, sp);
                 float t2 = 0.0f;
-                for (int a = 0; a < 3; ++a) { t[a] = S.tb[a] * (MODE == kPushInitHalf ? -0.5f : 0.5f); t2 = fmaf(t[a], t[a], t2); }
+                for (int a = 0; a < 3; ++a) { t[a] = tp[a] * (MODE == kPushInitHalf ? -0.5f : 0.5f); t2 = fmaf(t[a], t[a], t2); }
                 for (int a = 0; a < 3; ++a) sb[a] = 2.0f * t[a] / (1.0f + t2);
                 boris32(vv, e, h, t, sb);
             } else {
@@ -471,7 +547,9 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
         }
         // kick + drift
         if (BORIS) {
-            boris32(v, e, S.hqmdt, S.tb, S.sb);
+            float tp[3], sp[3];
+            boris_ts32(p, S, ix, iy, iz, f, tp, sp);
+            boris32(v, e, S.hqmdt, tp, sp);
         } else {
             for (int a = 0; a < DIM; ++a) v[a] = fmaf(S.qmdt, e[a], v[a]);
         }
@@ -493,7 +571,9 @@ __global__ void __launch_bounds__(kThreads) k_push32(ParamsND p, SpeciesND S, in
 // latency-bound).  Slice k of the CTA is the contiguous block of kThreads
 // particles at base + k * kThreads, so each warp still deposits runs of
 // consecutive (cell-sorted) particles.
-template <int DIM, bool BORIS, int ITEMS>
+// PROF: B tabulated along one axis (a separate instantiation, so the uniform-B
+// kernels keep their register budget).
+template <int DIM, bool BORIS, int ITEMS, bool PROF>
 __global__ void __launch_bounds__(kThreads) k_push32_step(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
     const unsigned base = blockIdx.x * (ITEMS * kThreads);
     const unsigned tid = threadIdx.x;
@@ -522,7 +602,11 @@ __global__ void __launch_bounds__(kThreads) k_push32_step(ParamsND p, SpeciesND 
         float e[3] = {0.0f, 0.0f, 0.0f};
         if (valid) gather32<DIM>(p, ix, iy, iz, f, e);
         // kick + drift, src/Pusher.cpp:109-128, :162-174
-        if (BORIS) {
+        if (BORIS && PROF) {
+            float tp[3], sp[3];
+            boris_ts32(p, S, ix, iy, iz, f, tp, sp);
+            boris32(v, e, S.hqmdt, tp, sp);
+        } else if (BORIS) {
             boris32(v, e, S.hqmdt, S.tb, S.sb);
         } else {
             for (int a = 0; a < DIM; ++a) v[a] = fmaf(S.qmdt, e[a], v[a]);
@@ -1337,6 +1421,26 @@ struct SimND {
         }
         ncells = N;
         boris = c.magnetic_field[0] != 0.0 || c.magnetic_field[1] != 0.0 || c.magnetic_field[2] != 0.0;
+        if (c.profile_rows) {
+            // Simulation2D / Simulation3D constructor checks, src/Simulation3D.cpp:184-196
+            require(!boris, std::string(c.dims == 2 ? "2D" : "3D") +
+                                " uniform magnetic_field components and magnetic_field_profile are mutually exclusive");
+            require(c.profile_axis >= 0 && c.profile_axis <= 2, "coordinate axis must be x, y, or z");
+            require(c.profile_rows >= 2, "tabulated vector field requires at least two rows");
+            require(c.profile_coordinates && c.profile_values, "tabulated vector field arrays are required");
+            for (size_t k = 0; k < c.profile_rows; ++k) {
+                require(std::isfinite(c.profile_coordinates[k]) && std::isfinite(c.profile_values[3 * k]) &&
+                            std::isfinite(c.profile_values[3 * k + 1]) && std::isfinite(c.profile_values[3 * k + 2]),
+                        "tabulated vector field values must be finite");
+                require(k == 0 || c.profile_coordinates[k] > c.profile_coordinates[k - 1],
+                        "tabulated vector field coordinates must be strictly increasing");
+            }
+            const double hi = c.profile_axis < c.dims ? c.length[c.profile_axis] : 0.0;
+            require(c.profile_coordinates[0] <= 0.0 && c.profile_coordinates[c.profile_rows - 1] >= hi,
+                    "tabulated magnetic field does not cover the simulation domain");
+            require(c.profile_rows < (1u << 30), "tabulated vector field too long");
+            boris = true;
+        }
         p.dt = c.dt;
         p.eps = (c.units == APIC_SI ? 8.8541878128e-12 : 1.0) * rel;
         double bound = 0.0;
@@ -1385,6 +1489,20 @@ struct SimND {
         solver.setup(c.dims, c.n, c.length, p.eps, p.inv_rho_scale);
         p.E = solver.F.E;
         p.rho_acc = solver.F.rho_acc;
+        if (c.profile_rows) {  // copied: the caller's arrays may go away after create
+            double* pc = dalloc<double>(c.profile_rows);
+            double* pv = dalloc<double>(3 * c.profile_rows);
+            APIC_CUDA(cudaMemcpyAsync(pc, c.profile_coordinates, c.profile_rows * sizeof(double),
+                                      cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaMemcpyAsync(pv, c.profile_values, 3 * c.profile_rows * sizeof(double),
+                                      cudaMemcpyHostToDevice, stream));
+            p.prof_axis = c.profile_axis;
+            p.prof_rows = (int)c.profile_rows;
+            p.prof_c = pc;
+            p.prof_v = pv;
+            cfg.profile_coordinates = nullptr;  // not kept
+            cfg.profile_values = nullptr;
+        }
         if (fp32) {
             solver.F.E32 = dalloc<float>(N * (c.dims == 2 ? 2 : 4));
             p.E32 = solver.F.E32;
@@ -1409,11 +1527,20 @@ struct SimND {
     void launch_step32(int items, const SpeciesND& S, int b, int s) {
         const unsigned g = (unsigned)((S.n + (unsigned)items * kThreads - 1) / ((unsigned)items * kThreads));
         unsigned long long* acc = solver.F.acc[s];
+        if (BORIS && p.prof_rows) {
+            switch (items) {
+                case 1: k_push32_step<DIM, BORIS, 1, true><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+                case 2: k_push32_step<DIM, BORIS, 2, true><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+                case 4: k_push32_step<DIM, BORIS, 4, true><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+                default: k_push32_step<DIM, BORIS, 8, true><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            }
+            return;
+        }
         switch (items) {
-            case 1: k_push32_step<DIM, BORIS, 1><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
-            case 2: k_push32_step<DIM, BORIS, 2><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
-            case 4: k_push32_step<DIM, BORIS, 4><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
-            default: k_push32_step<DIM, BORIS, 8><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 1: k_push32_step<DIM, BORIS, 1, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 2: k_push32_step<DIM, BORIS, 2, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 4: k_push32_step<DIM, BORIS, 4, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            default: k_push32_step<DIM, BORIS, 8, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
         }
     }
 

@@ -299,6 +299,15 @@ typedef struct {
                                    (0 = default: 4 in 2D, 2 in 3D); a tuning knob, no effect on results */
     size_t species_sort_interval[APIC_MAX_SPECIES];  /* per species (0 = sort_interval): slow heavy
                                    species keep their cell order far longer; no effect on results */
+    /* magnetic_field_profile (TabulatedVectorField1D, src/PrescribedField.cpp:89-113): B piecewise
+       linear along one axis, evaluated at each particle's position in every Boris kick.
+       profile_rows = 0 keeps the uniform magnetic_field; otherwise magnetic_field must be zero
+       (mutually exclusive, as in the reference), the coordinates strictly increasing and covering
+       [0, length] of that axis (a 2D run queries z = 0).  The arrays are copied at create. */
+    int profile_axis;                   /* 0 = x, 1 = y, 2 = z */
+    size_t profile_rows;
+    const double* profile_coordinates;  /* profile_rows values */
+    const double* profile_values;       /* profile_rows x (Bx, By, Bz) */
 } apic_config_nd;
 
 /* DiagnosticSample2D / DiagnosticSample3D, src/Diagnostics.cpp:111-137, :205-232 */

@@ -1174,6 +1174,10 @@ void ora_boris(double v[3], const double E[3], const double B[3], double qm, dou
 
 struct ora_simnd {
     int dims, nspecies, boris;
+    /* magnetic_field_profile (TabulatedVectorField1D): rows > 0 replaces B */
+    int prof_axis;
+    size_t prof_rows;
+    double *prof_c, *prof_v; /* rows, rows x 3 */
     size_t n[3];
     double L[3], d[3], dt, eps, B[3], q[ORA_MAX_SPECIES], m[ORA_MAX_SPECIES], w[ORA_MAX_SPECIES];
     size_t np[ORA_MAX_SPECIES];
@@ -1207,6 +1211,7 @@ ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double d
 
 void ora_simnd_destroy(ora_simnd* s) {
     if (!s) return;
+    free(s->prof_c); free(s->prof_v);
     for (int k = 0; k < ORA_MAX_SPECIES; ++k) { free(s->pos[k]); free(s->v[k]); free(s->vh[k]); }
     free(s->rho); free(s->phi); free(s->E); free(s);
 }
@@ -1239,6 +1244,39 @@ static void simnd_gather(const ora_simnd* s, const double* pos, size_t np, size_
 
 void ora_simnd_initialize_fields(ora_simnd* s) { simnd_deposit_solve(s); }
 
+/* magnetic_field_profile: B(position) = TabulatedVectorField1D::evaluate,
+ * src/PrescribedField.cpp:89-113 (piecewise linear along one axis; the query
+ * is the particle position, z = 0 in 2D). */
+int ora_simnd_set_profile(ora_simnd* s, int axis, size_t rows, const double* coords, const double* values) {
+    if (rows < 2 || axis < 0 || axis > 2) return seterr(1, "tabulated vector field requires at least two rows");
+    free(s->prof_c); free(s->prof_v);
+    s->prof_c = malloc(rows * sizeof(double));
+    s->prof_v = malloc(3 * rows * sizeof(double));
+    memcpy(s->prof_c, coords, rows * sizeof(double));
+    memcpy(s->prof_v, values, 3 * rows * sizeof(double));
+    s->prof_axis = axis;
+    s->prof_rows = rows;
+    s->boris = 1;
+    return 0;
+}
+
+static void simnd_b(const ora_simnd* s, const double* pos, size_t np, size_t i, double B[3]) {
+    if (!s->prof_rows) { B[0] = s->B[0]; B[1] = s->B[1]; B[2] = s->B[2]; return; }
+    const double q = s->prof_axis < s->dims ? pos[s->prof_axis * np + i] : 0.0;
+    const double* c = s->prof_c;
+    const size_t n = s->prof_rows;
+    if (q == c[0]) { for (int a = 0; a < 3; ++a) B[a] = s->prof_v[a]; return; }
+    if (q == c[n - 1]) { for (int a = 0; a < 3; ++a) B[a] = s->prof_v[3 * (n - 1) + a]; return; }
+    size_t lo = 0, hi = n; /* upper_bound */
+    while (lo < hi) { const size_t mid = (lo + hi) / 2; if (q < c[mid]) hi = mid; else lo = mid + 1; }
+    const size_t right = lo, left = right - 1;
+    const double f = (q - c[left]) / (c[right] - c[left]);
+    for (int a = 0; a < 3; ++a) {
+        const double l = s->prof_v[3 * left + a], r = s->prof_v[3 * right + a];
+        B[a] = l + f * (r - l);
+    }
+}
+
 /* initialize(): deposit_and_solve + initialize_{boris,leapfrog}_half_step */
 void ora_simnd_initialize(ora_simnd* s) {
     simnd_deposit_solve(s);
@@ -1250,7 +1288,9 @@ void ora_simnd_initialize(ora_simnd* s) {
             simnd_gather(s, s->pos[k], np, i, e);
             double v[3] = {s->v[k][i], s->v[k][np + i], s->v[k][2 * np + i]};
             if (s->boris) {
-                ora_boris(v, e, s->B, qm, -0.5 * s->dt);
+                double B[3];
+                simnd_b(s, s->pos[k], np, i, B);
+                ora_boris(v, e, B, qm, -0.5 * s->dt);
             } else {
                 for (int a = 0; a < s->dims; ++a) v[a] = v[a] - 0.5 * qm * e[a] * s->dt;
             }
@@ -1271,7 +1311,9 @@ void ora_simnd_step(ora_simnd* s, size_t steps) {
                 double e[3];
                 simnd_gather(s, s->pos[k], np, i, e);
                 double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};
-                if (s->boris) ora_boris(v, e, s->B, qm, s->dt);
+                double B[3];
+                if (s->boris) simnd_b(s, s->pos[k], np, i, B);
+                if (s->boris) ora_boris(v, e, B, qm, s->dt);
                 else for (int a = 0; a < s->dims; ++a) v[a] += qm * e[a] * s->dt;
                 for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
                 for (int a = 0; a < s->dims; ++a) {
@@ -1288,7 +1330,9 @@ void ora_simnd_step(ora_simnd* s, size_t steps) {
                 double e[3];
                 simnd_gather(s, s->pos[k], np, i, e);
                 double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};
-                if (s->boris) ora_boris(v, e, s->B, qm, 0.5 * s->dt);
+                double B[3];
+                if (s->boris) simnd_b(s, s->pos[k], np, i, B);
+                if (s->boris) ora_boris(v, e, B, qm, 0.5 * s->dt);
                 else for (int a = 0; a < s->dims; ++a) v[a] = v[a] + 0.5 * qm * e[a] * s->dt;
                 for (int a = 0; a < 3; ++a) s->v[k][a * np + i] = v[a];
             }

@@ -108,6 +108,8 @@ ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double d
                             int nspecies, const double* q, const double* m, const double* w_eff);
 void ora_simnd_destroy(ora_simnd* s);
 void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const double* v, const double* vh);
+/* magnetic_field_profile: B piecewise linear along `axis` (values rows x 3) */
+int ora_simnd_set_profile(ora_simnd* s, int axis, size_t rows, const double* coords, const double* values);
 void ora_simnd_initialize_fields(ora_simnd* s);
 void ora_simnd_initialize(ora_simnd* s);
 void ora_simnd_step(ora_simnd* s, size_t steps);

@@ -523,6 +523,15 @@ class SimND:
                                      dptr(m), dptr(w))
         self.np = [0] * self.ns
 
+    def set_profile(self, axis, coordinates, values):
+        """magnetic_field_profile: B piecewise linear along `axis`."""
+        Lb = _nd_bind()
+        Lb.ora_simnd_set_profile.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP]
+        self._prof = (np.ascontiguousarray(coordinates, dtype=np.float64),
+                      np.ascontiguousarray(values, dtype=np.float64).ravel())
+        if Lb.ora_simnd_set_profile(self.h, axis, len(self._prof[0]), dptr(self._prof[0]), dptr(self._prof[1])):
+            raise RuntimeError(Lb.ora_last_error().decode())
+
     def __del__(self):
         if getattr(self, "h", None):
             _nd_bind().ora_simnd_destroy(self.h)
@@ -579,8 +588,9 @@ def _refnd_bind():
 class RefND:
     """The reference's Simulation2D / Simulation3D (periodic) through the harness."""
 
-    def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0):
-        """species: list of (q, m, w, count, drift_x, thermal)."""
+    def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0, profile=None):
+        """species: list of (q, m, w, count, drift_x, thermal); profile: optional
+        (axis, coordinates, values[rows][3]) magnetic_field_profile."""
         Lb = _refnd_bind()
         self.dims, self.n, self.N = dims, list(n), int(np.prod(n))
         cols = [np.array([s[i] for s in species], dtype=np.float64) for i in (0, 1, 2, 4, 5)]
@@ -589,8 +599,21 @@ class RefND:
         Bv = np.ascontiguousarray(B, dtype=np.float64)
         Lv = arr3(L)
         h = C.c_void_p()
-        rc = Lb.refnd_create(dims, sizes3(n), dptr(Lv), dt, si, dptr(Bv), len(species), dptr(cols[0]), dptr(cols[1]),
-                             dptr(cols[2]), counts, dptr(cols[3]), dptr(cols[4]), seed, threads, C.byref(h))
+        if profile is None:
+            rc = Lb.refnd_create(dims, sizes3(n), dptr(Lv), dt, si, dptr(Bv), len(species), dptr(cols[0]),
+                                 dptr(cols[1]), dptr(cols[2]), counts, dptr(cols[3]), dptr(cols[4]), seed, threads,
+                                 C.byref(h))
+        else:
+            ax, pc, pv = profile
+            pc = np.ascontiguousarray(pc, dtype=np.float64)
+            pv = np.ascontiguousarray(pv, dtype=np.float64).ravel()
+            self._keep_prof = (pc, pv)
+            Lb.refnd_create_profile.argtypes = [C.c_int, _SZP, _DP, C.c_double, C.c_int, _DP, C.c_int, _DP, _DP, _DP,
+                                                _SZP, _DP, _DP, C.c_uint, C.c_int, C.c_int, C.c_size_t, _DP, _DP,
+                                                C.POINTER(C.c_void_p)]
+            rc = Lb.refnd_create_profile(dims, sizes3(n), dptr(Lv), dt, si, dptr(Bv), len(species), dptr(cols[0]),
+                                         dptr(cols[1]), dptr(cols[2]), counts, dptr(cols[3]), dptr(cols[4]), seed,
+                                         threads, ax, len(pc), dptr(pc), dptr(pv), C.byref(h))
         if rc:
             raise RuntimeError(Lb.ref_last_error().decode())
         self.h = h

@@ -374,10 +374,20 @@ struct RefND {
 extern "C" {
 
 // species: q, m, w, count, drift_x, thermal (isotropic) per species
-int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, const double* B, int nspecies,
-                 const double* q, const double* m, const double* w, const size_t* count, const double* drift,
-                 const double* thermal, unsigned seed, int threads, void** out) {
+int refnd_create_profile(int dims, const size_t* n, const double* L, double dt, int si, const double* B,
+                         int nspecies, const double* q, const double* m, const double* w, const size_t* count,
+                         const double* drift, const double* thermal, unsigned seed, int threads, int prof_axis,
+                         size_t prof_rows, const double* prof_c, const double* prof_v, void** out) {
     try {
+        std::optional<pic::TabulatedVectorField1D> profile;
+        if (prof_rows) {
+            std::vector<double> cs(prof_c, prof_c + prof_rows);
+            std::vector<pic::Vec3> vs(prof_rows);
+            for (size_t k = 0; k < prof_rows; ++k) vs[k] = {prof_v[3 * k], prof_v[3 * k + 1], prof_v[3 * k + 2]};
+            const pic::CoordinateAxis ax = prof_axis == 0 ? pic::CoordinateAxis::X
+                                         : prof_axis == 1 ? pic::CoordinateAxis::Y : pic::CoordinateAxis::Z;
+            profile.emplace(ax, std::move(cs), std::move(vs));
+        }
         auto r = std::make_unique<RefND>();
         r->dims = dims;
         pic::RuntimePolicy rt;
@@ -388,6 +398,7 @@ int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, 
             c.nx = n[0]; c.ny = n[1]; c.length_x = L[0]; c.length_y = L[1];
             c.dt = dt; c.boundary = pic::Boundary::Periodic;
             c.magnetic_field_x = B[0]; c.magnetic_field_y = B[1]; c.magnetic_field_z = B[2];
+            c.magnetic_field_profile = profile;
             c.seed = seed; c.runtime = rt;
             c.output_dir = std::filesystem::temp_directory_path() / "apic_ref2d";
             size_t mx = 0;
@@ -408,6 +419,7 @@ int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, 
             c.length_x = L[0]; c.length_y = L[1]; c.length_z = L[2];
             c.dt = dt; c.boundary = pic::Boundary::Periodic;
             c.magnetic_field = {B[0], B[1], B[2]};
+            c.magnetic_field_profile = profile;
             c.seed = seed; c.runtime = rt;
             c.output_dir = std::filesystem::temp_directory_path() / "apic_ref3d";
             for (int s = 0; s < nspecies; ++s) {
@@ -422,6 +434,13 @@ int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, 
         *out = r.release();
         return 0;
     } catch (const std::exception& e) { return fail(e); }
+}
+
+int refnd_create(int dims, const size_t* n, const double* L, double dt, int si, const double* B, int nspecies,
+                 const double* q, const double* m, const double* w, const size_t* count, const double* drift,
+                 const double* thermal, unsigned seed, int threads, void** out) {
+    return refnd_create_profile(dims, n, L, dt, si, B, nspecies, q, m, w, count, drift, thermal, seed, threads, 0, 0,
+                                nullptr, nullptr, out);
 }
 
 void refnd_destroy(void* h) { delete static_cast<RefND*>(h); }

@@ -132,10 +132,37 @@ ND_CASES = {
 ND_SPECIES = [(-1.0, 1.0, 0.05, 400, 0.3, 0.4), (1.0, 50.0, 0.05, 400, 0.0, 0.05)]
 
 
+# magnetic_field_profile cases: B tabulated along one axis (uniform B zero)
+PROFILE_CASES = {
+    # name: dims, cells, axis, steps
+    "sim2d_bprofile": (2, (16, 8), 0, 25),
+    "sim3d_bprofile": (3, (8, 4, 8), 2, 25),
+}
+
+
+def bprofile_table(axis_length, rows=9):
+    """A smooth B(s) table covering [0, axis_length] (rows unevenly spaced)."""
+    c = axis_length * (np.linspace(0.0, 1.0, rows) ** 1.3)
+    v = np.stack([0.2 * np.sin(3.0 * c / axis_length), 0.1 + 0.0 * c, 0.8 + 0.4 * np.cos(2.0 * c / axis_length)],
+                 axis=1)
+    return c, v
+
+
+def bprofile_fixture():
+    for name, (dims, n, axis, steps) in PROFILE_CASES.items():
+        L = [1.3 * ni for ni in n]
+        c, v = bprofile_table(L[axis])
+        _nd_run(name, dims, n, L, (0.0, 0.0, 0.0), steps, profile=(axis, c, v))
+
+
 def nd_fixture(name):
     dims, n, B, steps = ND_CASES[name]
     L = [1.3 * ni for ni in n]
-    R = po.RefND(dims, n, L, 0.1, 0, B, ND_SPECIES, seed=9)
+    _nd_run(name, dims, n, L, B, steps)
+
+
+def _nd_run(name, dims, n, L, B, steps, profile=None):
+    R = po.RefND(dims, n, L, 0.1, 0, B, ND_SPECIES, seed=9, profile=profile)
     R.initialize()
     out = {"steps": steps}
     for k in range(len(ND_SPECIES)):
@@ -147,6 +174,8 @@ def nd_fixture(name):
             out[f"final_s{k}_{key}"] = arr
     rho, phi, E = R.fields()
     out.update(rho=rho, phi=phi, E=E, time=R.time())
+    if profile is not None:
+        out.update(prof_axis=profile[0], prof_c=profile[1], prof_v=profile[2])
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
 
 
@@ -240,6 +269,7 @@ def main(names=None):
         print("golden vectors written to", HERE)
         return
     mixed_fixture()
+    bprofile_fixture()
     swarm_ensemble_fixture()
     swarm_fixture()
     collide_hg_fixture()

@@ -178,3 +178,80 @@ def test_push_items_and_autotuner_leave_results_unchanged():
     out = autotune.tune_plasma(plan, apic.FP32, sort_intervals=(4, 8), push_items=(1, 4), steps=8)
     assert out["sort_interval"] in (4, 8) and out["push_items"] in (1, 4)
     assert len(out["table"]) == 4 and all(r["ms_per_step"] > 0 for r in out["table"])
+
+
+def _with_profile(cfg, axis, coords, values):
+    """Switch a device config to a tabulated B (uniform B cleared)."""
+    import ctypes as C
+    pc = np.ascontiguousarray(coords, dtype=np.float64)
+    pv = np.ascontiguousarray(values, dtype=np.float64).ravel()
+    cfg._profile_keep = (pc, pv)
+    cfg.magnetic_field[:] = [0.0, 0.0, 0.0]
+    cfg.profile_axis, cfg.profile_rows = axis, pc.size
+    cfg.profile_coordinates = pc.ctypes.data_as(C.POINTER(C.c_double))
+    cfg.profile_values = pv.ctypes.data_as(C.POINTER(C.c_double))
+    return cfg
+
+
+def _profile_for(wl, axis, rows=11):
+    Lax = wl.length[axis] if axis < wl.dims else 0.0
+    c = np.linspace(0.0, Lax if Lax > 0 else 1.0, rows) ** 1.0
+    if axis >= wl.dims:
+        c = np.linspace(-1.0, 1.0, rows)
+    B0 = np.linalg.norm(wl.B) or 0.01
+    u = c / (np.max(np.abs(c)) or 1.0)
+    v = np.stack([0.3 * B0 * np.sin(2.0 * u), 0.1 * B0 + 0.0 * u, B0 * (1.0 + 0.5 * np.cos(3.0 * u))], axis=1)
+    return c, v
+
+
+@pytest.mark.parametrize("dims,axis", [(2, 0), (2, 1), (2, 2), (3, 2), (3, 0)])
+def test_tabulated_magnetic_field_parity(dims, axis):
+    """magnetic_field_profile: B piecewise linear along one axis, evaluated at
+    each particle in every Boris kick.  FP64 form against the oracle (bit-exact
+    with the reference on the golden runs) within 1e-12; FP32 form within the
+    FP32 bounds of the uniform-B case."""
+    wl = W.plasma_2d(cells=(32, 16), ppc=8, seed=3) if dims == 2 else W.plasma_3d(cells=(16, 8, 8), ppc=4, seed=5)
+    c, v = _profile_for(wl, axis)
+    eps = 8.8541878128e-12
+    for prec in (apic.FP64, apic.FP32):
+        cfg = _with_profile(W.to_device_config_nd(wl, precision=prec, sort_interval=4), axis, c, v)
+        dev = apic.SimulationND(cfg)
+        ora = po.SimND(wl.dims, wl.n, wl.length, wl.dt, eps, (0.0, 0.0, 0.0),
+                       [(q, m, w) for (q, m, w, pos, vv) in wl.species])
+        ora.set_profile(axis, c, v)
+        for k, (q, m, w, pos, vv) in enumerate(wl.species):
+            dev.load(k, pos, vv)
+            ora.load(k, pos, vv, vv)
+        dev.initialize()
+        ora.initialize()
+        dev.step(10)
+        ora.step(10)
+        for k in range(2):
+            a, b = dev.particles(k), ora.particles(k)
+            if prec == apic.FP64:
+                for name, x, y in zip(("pos", "v", "vh"), a, b):
+                    x, y = (x[: wl.dims], y[: wl.dims]) if name == "pos" else (x, y)
+                    assert rel_max(x, y) < TOL, (dims, axis, k, name, rel_max(x, y))
+            else:
+                cell = wl.length[0] / wl.n[0]
+                dpos = np.abs(a[0][: wl.dims] - b[0][: wl.dims])
+                dpos = np.minimum(dpos, np.array(wl.length)[: wl.dims, None] - dpos)
+                assert dpos.max() < 1e-5 * cell, (dims, axis, k, dpos.max() / cell)
+                assert np.max(np.abs(a[2] - b[2])) < 1e-5 * np.max(np.abs(b[2]))
+        if prec == apic.FP64:
+            for name, x, y in zip(("rho", "phi", "E"), dev.fields(), ora.fields()):
+                assert rel_max(x, y) < TOL, (name, rel_max(x, y))
+        dev.close()
+
+
+def test_tabulated_magnetic_field_rejections():
+    wl = W.plasma_2d(cells=(16, 16), ppc=2, seed=3)
+    c, v = _profile_for(wl, 0)
+    cfg = W.to_device_config_nd(wl)
+    cfg = _with_profile(cfg, 0, c, v)
+    cfg.magnetic_field[:] = [0.0, 0.0, 0.01]
+    with pytest.raises(apic.ApicError, match="mutually exclusive"):
+        apic.SimulationND(cfg)
+    short = _with_profile(W.to_device_config_nd(wl), 0, c[:-2], v[:-2])  # stops before length_x
+    with pytest.raises(apic.ApicError, match="cover"):
+        apic.SimulationND(short)

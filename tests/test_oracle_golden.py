@@ -180,3 +180,23 @@ def test_mixed_spectral_tridiagonal_solve_bit_exact(name):
     phi, E = po.solve_mixed_2d(f["rho"], tuple(int(v) for v in f["n"]), f["L"], int(f["axis"]), float(f["eps"]),
                                float(f["lower"]), float(f["upper"]))
     assert np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
+
+
+@pytest.mark.parametrize("name,dims,n", [("sim2d_bprofile", 2, (16, 8)), ("sim3d_bprofile", 3, (8, 4, 8))])
+def test_tabulated_magnetic_field_run_bit_exact(name, dims, n):
+    """Simulation2D / Simulation3D with magnetic_field_profile (B tabulated along
+    one axis, evaluated at each particle's position in every Boris kick):
+    25 steps, bit-exact."""
+    f = load(f"{name}.npz")
+    L = [1.3 * ni for ni in n]
+    sim = po.SimND(dims, n, L, 0.1, 1.0, (0.0, 0.0, 0.0), ND_SPECIES)
+    sim.set_profile(int(f["prof_axis"]), f["prof_c"], f["prof_v"])
+    for k in range(2):
+        sim.load(k, f[f"init_s{k}_pos"], f[f"init_s{k}_v"], f[f"init_s{k}_vh"])
+    sim.initialize_fields()
+    sim.step(int(f["steps"]))
+    for k in range(2):
+        for key, arr in zip(("pos", "v", "vh"), sim.particles(k)):
+            assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
+    rho, phi, E = sim.fields()
+    assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
