@@ -587,6 +587,62 @@ def field_solve_mixed_2d(n, length, periodic_axis, permittivity, lower_potential
     return phi, E.reshape(2, N)
 
 
+class ParticleState:
+    """An AuroraPIC particle-state file (.aps version 1, the reference's
+    external initial state), parsed by the library: `species` maps each name
+    (sorted) to (pos[3][n], vel[3][n]) arrays ready for the loaders."""
+
+    def __init__(self, path, max_particles=1 << 40):
+        L = lib()
+        L.apic_aps_read.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_void_p)]
+        L.apic_aps_info.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_size_t),
+                                    C.POINTER(C.c_size_t), C.POINTER(C.c_uint64)]
+        L.apic_aps_species.argtypes = [C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        L.apic_aps_records.argtypes = [C.c_void_p, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.apic_aps_free.argtypes = [C.c_void_p]
+        L.apic_aps_last_error.restype = C.c_char_p
+        h = C.c_void_p()
+        rc = L.apic_aps_read(os.fsencode(path), max_particles, C.byref(h))
+        if rc:
+            raise ApicError(rc, L.apic_aps_last_error().decode())
+        try:
+            d, u, n, ns, sig = C.c_int(), C.c_int(), C.c_size_t(), C.c_size_t(), C.c_uint64()
+            L.apic_aps_info(h, C.byref(d), C.byref(u), C.byref(n), C.byref(ns), C.byref(sig))
+            self.dimension, self.units, self.particle_count, self.signature = d.value, u.value, n.value, sig.value
+            self.species = {}
+            for k in range(ns.value):
+                name = C.create_string_buffer(4096)
+                cnt = C.c_size_t()
+                L.apic_aps_species(h, k, name, 4096, C.byref(cnt))
+                pos, vel = np.zeros((3, cnt.value)), np.zeros((3, cnt.value))
+                L.apic_aps_records(h, k, dptr(pos), dptr(vel))
+                self.species[name.value.decode()] = (pos, vel)
+        finally:
+            L.apic_aps_free(h)
+
+    @staticmethod
+    def write(path, dimension, units, species, overwrite=False):
+        """species: {name: (pos[3][n], vel[3][n])}; returns the signature."""
+        L = lib()
+        L.apic_aps_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_char_p),
+                                     C.POINTER(C.c_size_t), C.POINTER(C.POINTER(C.c_double)),
+                                     C.POINTER(C.POINTER(C.c_double)), C.c_int, C.POINTER(C.c_uint64)]
+        L.apic_aps_last_error.restype = C.c_char_p
+        names = list(species)
+        keep = [(np.ascontiguousarray(species[k][0], dtype=np.float64), np.ascontiguousarray(species[k][1], dtype=np.float64))
+                for k in names]
+        nm = (C.c_char_p * len(names))(*[k.encode() for k in names])
+        counts = (C.c_size_t * len(names))(*[p.shape[1] for p, _ in keep])
+        pp = (C.POINTER(C.c_double) * len(names))(*[dptr(p) for p, _ in keep])
+        vv = (C.POINTER(C.c_double) * len(names))(*[dptr(v) for _, v in keep])
+        sig = C.c_uint64()
+        rc = L.apic_aps_write(os.fsencode(path), dimension, units, len(names), nm, counts, pp, vv, int(overwrite),
+                              C.byref(sig))
+        if rc:
+            raise ApicError(rc, L.apic_aps_last_error().decode())
+        return sig.value
+
+
 def _simnd_load_maxwellian(self, species, n, seed, thermal_speed, drift_x=0.0, perturb_axis=0, perturb_amplitude=0.0):
     L = _bind_nd()
     L.apic_simnd_load_maxwellian.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_uint64, C.c_double, C.c_double,

@@ -534,6 +534,36 @@ APIC_EXPORT int apic_swarm_server_set_kernel_timing(apic_swarm_server* srv, int 
 APIC_EXPORT int apic_swarm_server_kernel_times(apic_swarm_server* srv, double* push_ms, double* collide_ms,
                                                uint64_t* push_launches, double* push_bytes);
 
+/* ---- particle-state interchange (.aps version 1) ------------------------------
+ * The reference's external initial-state files (load_external_particle_state,
+ * write_external_particle_state, external_particle_state_signature,
+ * src/ParticleState.cpp:112-262, :541-624): parsed on the host into per-species
+ * component arrays for apic_sim1d_load_particles / apic_simnd_load_particles.
+ * Species are ordered by name; records of a species keep file order. */
+typedef struct apic_aps apic_aps;
+APIC_EXPORT const char* apic_aps_last_error(void);
+/* Reads and validates a file (the reference's checks and messages); at most
+ * max_particles records. */
+APIC_EXPORT int apic_aps_read(const char* path, size_t max_particles, apic_aps** out);
+APIC_EXPORT void apic_aps_free(apic_aps* state);
+/* dimension 1-3, units apic_units, total records, species, and the canonical
+ * 64-bit FNV-1a signature (the reference's initial_state_signature). */
+APIC_EXPORT int apic_aps_info(const apic_aps* state, int* dimension, int* units, size_t* particle_count,
+                              size_t* nspecies, uint64_t* signature);
+/* Species k: its name (NUL-terminated, name_capacity bytes available) and
+ * record count. */
+APIC_EXPORT int apic_aps_species(const apic_aps* state, size_t k, char* name, size_t name_capacity, size_t* count);
+/* Species k's records as component-major arrays: pos [3][count], vel [3][count]
+ * (either may be NULL). */
+APIC_EXPORT int apic_aps_records(const apic_aps* state, size_t k, double* pos, double* vel);
+/* Writes species k's count records (pos[k], vel[k]: [3][counts[k]]) in the
+ * reference's deterministic form (17 significant digits, species by name);
+ * overwrite = 0 refuses an existing file.  *signature (if non-NULL) receives
+ * the state's signature. */
+APIC_EXPORT int apic_aps_write(const char* path, int dimension, int units, size_t nspecies,
+                               const char* const* names, const size_t* counts, const double* const* pos,
+                               const double* const* vel, int overwrite, uint64_t* signature);
+
 #ifdef __cplusplus
 }
 #endif

@@ -497,6 +497,43 @@ def ref_solve_mixed_2d(rho, n, L, periodic_axis, eps, lower, upper):
     return phi, E.reshape(2, N)
 
 
+def ref_aps_write(path, dimension, si, species):
+    """The reference's write_external_particle_state; species {name: (pos[3][n],
+    vel[3][n])}; returns its signature."""
+    Lb = ref()
+    Lb.ref_aps_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_char_p), _SZP,
+                                 C.POINTER(_DP), C.POINTER(_DP), C.POINTER(C.c_uint64)]
+    names = list(species)
+    keep = [(np.ascontiguousarray(species[k][0], dtype=np.float64), np.ascontiguousarray(species[k][1], dtype=np.float64))
+            for k in names]
+    nm = (C.c_char_p * len(names))(*[k.encode() for k in names])
+    counts = (C.c_size_t * len(names))(*[p.shape[1] for p, _ in keep])
+    pp = (_DP * len(names))(*[dptr(p) for p, _ in keep])
+    vv = (_DP * len(names))(*[dptr(v) for _, v in keep])
+    sig = C.c_uint64()
+    if Lb.ref_aps_write(os.fsencode(path), dimension, si, len(names), nm, counts, pp, vv, C.byref(sig)):
+        raise RuntimeError(Lb.ref_last_error().decode())
+    return sig.value
+
+
+def ref_aps_read(path, max_particles=1 << 30, capacity=1 << 20):
+    """The reference's load_external_particle_state: (signature, [(pos, vel)] by name)."""
+    Lb = ref()
+    Lb.ref_aps_read.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(C.c_uint64), _SZP, _SZP, _DP, _DP, C.c_size_t]
+    sig, ns = C.c_uint64(), C.c_size_t()
+    counts = (C.c_size_t * 64)()
+    pos, vel = np.zeros(capacity), np.zeros(capacity)
+    if Lb.ref_aps_read(os.fsencode(path), max_particles, C.byref(sig), C.byref(ns), counts, dptr(pos), dptr(vel),
+                       capacity):
+        raise RuntimeError(Lb.ref_last_error().decode())
+    out, off = [], 0
+    for k in range(ns.value):
+        n = counts[k]
+        out.append((pos[off: off + 3 * n].reshape(3, n).copy(), vel[off: off + 3 * n].reshape(3, n).copy()))
+        off += 3 * n
+    return sig.value, out
+
+
 def sizes3(n):
     n = list(n) + [1] * (3 - len(n))
     return (C.c_size_t * 3)(*n)

@@ -11,6 +11,7 @@
 #include "pic/Grid.hpp"
 #include "pic/Mesh2D.hpp"
 #include "pic/Mesh3D.hpp"
+#include "pic/ParticleState.hpp"
 #include "pic/Pusher.hpp"
 #include "pic/Simulation.hpp"
 #include "pic/Simulation2D.hpp"
@@ -531,6 +532,59 @@ int ref_solve_mixed_2d(const size_t* n, const double* L, int periodic_axis, doub
         std::memcpy(phi, mesh.phi().data(), N * 8);
         std::memcpy(E, mesh.electric_x().data(), N * 8);
         std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+/* write_external_particle_state with species k's records pos[k], vel[k]
+ * ([3][counts[k]]); *signature = external_particle_state_signature. */
+int ref_aps_write(const char* path, int dimension, int si, size_t nspecies, const char* const* names,
+                  const size_t* counts, const double* const* pos, const double* const* vel, uint64_t* signature) {
+    try {
+        pic::ExternalParticleState st;
+        st.spatial_dimension = (size_t)dimension;
+        st.unit_system = si ? pic::UnitSystem::SI : pic::UnitSystem::Normalized;
+        for (size_t k = 0; k < nspecies; ++k) {
+            auto& recs = st.species[names[k]];
+            const size_t n = counts[k];
+            for (size_t i = 0; i < n; ++i) {
+                pic::ExternalParticleRecord r;
+                r.position = {pos[k][i], pos[k][n + i], pos[k][2 * n + i]};
+                r.velocity = {vel[k][i], vel[k][n + i], vel[k][2 * n + i]};
+                recs.push_back(r);
+            }
+            st.particle_count += n;
+        }
+        st.signature = pic::external_particle_state_signature(st);
+        pic::write_external_particle_state(path, st, true);
+        *signature = st.signature;
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+/* load_external_particle_state: signature and, per species in name order,
+ * the record count (counts[k]) and records appended to pos/vel as
+ * [species][3][count] blocks (capacity values each). */
+int ref_aps_read(const char* path, size_t max_particles, uint64_t* signature, size_t* nspecies, size_t* counts,
+                 double* pos, double* vel, size_t capacity) {
+    try {
+        const auto st = pic::load_external_particle_state(path, max_particles);
+        *signature = st.signature;
+        *nspecies = st.species.size();
+        size_t k = 0, off = 0;
+        for (const auto& [name, recs] : st.species) {
+            (void)name;
+            const size_t n = recs.size();
+            counts[k++] = n;
+            if (off + 3 * n > capacity) throw std::runtime_error("capacity");
+            for (size_t i = 0; i < n; ++i) {
+                pos[off + i] = recs[i].position.x; pos[off + n + i] = recs[i].position.y;
+                pos[off + 2 * n + i] = recs[i].position.z;
+                vel[off + i] = recs[i].velocity.x; vel[off + n + i] = recs[i].velocity.y;
+                vel[off + 2 * n + i] = recs[i].velocity.z;
+            }
+            off += 3 * n;
+        }
         return 0;
     } catch (const std::exception& e) { return fail(e); }
 }

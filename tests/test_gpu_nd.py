@@ -255,3 +255,37 @@ def test_tabulated_magnetic_field_rejections():
     short = _with_profile(W.to_device_config_nd(wl), 0, c[:-2], v[:-2])  # stops before length_x
     with pytest.raises(apic.ApicError, match="cover"):
         apic.SimulationND(short)
+
+
+def test_particle_state_file_drives_a_device_run(tmp_path):
+    """An .aps initial state (written, then parsed by the library) loaded into a
+    2D3V device run gives the oracle's run on the same records (1e-12)."""
+    wl = W.plasma_2d(cells=(32, 16), ppc=4, seed=9)
+    names = ["electrons", "ions"]
+    sp = {names[k]: (np.asarray(pos, dtype=np.float64), np.asarray(v, dtype=np.float64))
+          for k, (q, m, w, pos, v) in enumerate(wl.species)}
+    for k in sp:
+        p3 = np.zeros((3, sp[k][0].shape[1]))
+        p3[:2] = sp[k][0][:2]
+        sp[k] = (p3, sp[k][1])
+    path = str(tmp_path / "init.aps")
+    apic.ParticleState.write(path, 2, apic.SI, sp)
+    st = apic.ParticleState(path)
+    assert st.dimension == 2 and sorted(st.species) == names
+    cfg = W.to_device_config_nd(wl, sort_interval=4)
+    dev = apic.SimulationND(cfg)
+    ora = po.SimND(wl.dims, wl.n, wl.length, wl.dt, 8.8541878128e-12, wl.B,
+                   [(q, m, w) for (q, m, w, pos, v) in wl.species])
+    for k, name in enumerate(names):
+        pos, vel = st.species[name]
+        dev.load(k, pos, vel)
+        ora.load(k, pos, vel, vel)
+    dev.initialize()
+    ora.initialize()
+    dev.step(5)
+    ora.step(5)
+    for k in range(2):
+        a, b = dev.particles(k), ora.particles(k)
+        for name, x, y in zip(("pos", "v", "vh"), a, b):
+            x, y = (x[:2], y[:2]) if name == "pos" else (x, y)
+            assert rel_max(x, y) < TOL, (k, name)
