@@ -568,6 +568,27 @@ def field_solve_periodic_nd(dims, n, length, permittivity, rho):
     return phi, E.reshape(dims, N)
 
 
+def field_solve_dirichlet_nd(n, length, permittivity, rho, side_potentials=None):
+    """FieldSolver::solve(Mesh2D&/Mesh3D&) with walls on every side (2D side
+    potentials left, right, bottom, top; 3D grounded); returns (phi, E[dims])."""
+    L = _bind_nd()
+    L.apic_field_solve_dirichlet_nd.argtypes = [C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.c_double,
+                                                C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double)]
+    dims = len(n)
+    N = int(np.prod(n))
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    if rho.size != N:
+        raise ValueError("rho must hold prod(n) values")
+    phi, E = np.zeros(N), np.zeros(dims * N)
+    ns = (C.c_size_t * 3)(*(list(n) + [1] * (3 - dims)))
+    Lv = np.ascontiguousarray(list(length) + [1.0] * (3 - dims), dtype=np.float64)
+    pot = None if side_potentials is None else np.ascontiguousarray(side_potentials, dtype=np.float64)
+    _check_nd(L.apic_field_solve_dirichlet_nd(dims, ns, dptr(Lv), permittivity, dptr(pot) if pot is not None else None,
+                                              dptr(rho), dptr(phi), dptr(E)))
+    return phi, E.reshape(dims, N)
+
+
 def field_solve_mixed_2d(n, length, periodic_axis, permittivity, lower_potential, upper_potential, rho):
     """FieldSolver::solve(Mesh2D&) with one periodic axis (0: x, 1: y) and wall
     potentials on the other; returns (phi, E[2]) on the nx * ny mesh."""

@@ -2061,6 +2061,206 @@ static void solve_mixed_2d(const size_t* n, const double* length, int periodic_a
     APIC_CUDA(e);
 }
 
+// ---- fully Dirichlet 2D / 3D solve --------------------------------------------------
+//
+// FieldSolver::solve(Mesh2D&/Mesh3D&) on meshes with walls on every side.  The
+// reference iterates SOR to a 1e-11 update (solve_dirichlet_iterative,
+// src/FieldSolver.cpp:761-907); here the same discrete system is solved directly:
+// the discrete sine transform (DST-I) diagonalises the Dirichlet second
+// difference of each axis (eigenvalues 4 sin^2(pi m / (2 (M + 1))) / h^2 over the
+// M interior nodes), so the interior potential is three DST passes, a division
+// and three more DST passes, each DST-I an odd-extended complex FFT of length
+// 2 (M + 1).  Wall potentials (2D sides, corners the mean of their two sides;
+// 3D grounded) enter the right-hand side of the nodes next to the walls.
+
+// interior right-hand side, compact [Mz][My][Mx]
+__global__ void k_dir_rhs(const double* __restrict__ rho, double* __restrict__ u, int nx, int ny, int nz3, double eps,
+                          double idx2, double idy2, double left, double right, double bottom, double top) {
+    const int Mx = nx - 2, My = ny - 2, Mz = nz3 > 1 ? nz3 - 2 : 1;
+    const size_t M = (size_t)Mx * My * Mz;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < M; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % Mx), j = (int)((q / Mx) % My), k = (int)(q / ((size_t)Mx * My));
+        const size_t node = ((size_t)(nz3 > 1 ? k + 1 : 0) * ny + (j + 1)) * nx + (i + 1);
+        double b = rho[node] / eps;
+        if (nz3 == 1) {  // 2D walls at their potentials; 3D walls are grounded
+            if (i == 0) b += left * idx2;
+            if (i == Mx - 1) b += right * idx2;
+            if (j == 0) b += bottom * idy2;
+            if (j == My - 1) b += top * idy2;
+        }
+        u[q] = b;
+    }
+}
+
+// DST-I of lines of M values (u[base + k * stride]) in place: one CTA per line,
+// X_m = sum_k x_k sin(pi k m / (M + 1)) = -Im(FFT(odd extension))_m / 2.
+__global__ void __launch_bounds__(kFftThreads) k_dst_lines(double* __restrict__ u, int M, long long stride, int lines_a,
+                                                           long long stride_a, long long stride_b, const Cplx* tw) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    const int N = 2 * (M + 1);
+    Cplx* a = reinterpret_cast<Cplx*>(dsm);
+    Cplx* b = a + N;
+    Cplx* tws = b + N;
+    const long long l = blockIdx.x;
+    const long long base = (l % lines_a) * stride_a + (l / lines_a) * stride_b;
+    for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        tws[k] = tw[k];
+        double v = 0.0;
+        if (k >= 1 && k <= M) v = u[base + (long long)(k - 1) * stride];
+        else if (k >= M + 2) v = -u[base + (long long)(N - k - 1) * stride];
+        a[k] = {v, 0.0};
+    }
+    __syncthreads();
+    const Cplx* r = fft_lines(a, b, 1, N, tws, false);
+    for (int m = threadIdx.x + 1; m <= M; m += blockDim.x) u[base + (long long)(m - 1) * stride] = -0.5 * r[m].im;
+}
+
+// divide by the eigenvalues of minus the discrete Laplacian; scale folds in the
+// inverse-DST normalisation 2 / (M + 1) of every axis
+__global__ void k_dir_divide(double* __restrict__ u, int Mx, int My, int Mz, double idx2, double idy2, double idz2,
+                             double scale) {
+    const size_t M = (size_t)Mx * My * Mz;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < M; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % Mx), j = (int)((q / Mx) % My), k = (int)(q / ((size_t)Mx * My));
+        const double sx = sin(3.141592653589793 * (i + 1) / (2.0 * (Mx + 1)));
+        const double sy = sin(3.141592653589793 * (j + 1) / (2.0 * (My + 1)));
+        double lam = 4.0 * sx * sx * idx2 + 4.0 * sy * sy * idy2;
+        if (Mz > 1 || idz2 > 0.0) {
+            const double sz = sin(3.141592653589793 * (k + 1) / (2.0 * (Mz + 1)));
+            lam += 4.0 * sz * sz * idz2;
+        }
+        u[q] *= scale / lam;
+    }
+}
+
+// the full mesh: wall nodes (apply_dirichlet_boundary_potentials,
+// src/FieldSolver.cpp:267-296, or grounded in 3D) and the interior solution
+__global__ void k_dir_assemble(const double* __restrict__ u, double* __restrict__ phi, int nx, int ny, int nz3,
+                               double left, double right, double bottom, double top) {
+    const size_t N = (size_t)nx * ny * nz3;
+    const int Mx = nx - 2, My = ny - 2;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / ((size_t)nx * ny));
+        const bool wi = i == 0 || i == nx - 1, wj = j == 0 || j == ny - 1, wk = nz3 > 1 && (k == 0 || k == nz3 - 1);
+        double v;
+        if (!wi && !wj && !wk) {
+            v = u[((size_t)(nz3 > 1 ? k - 1 : 0) * My + (j - 1)) * Mx + (i - 1)];
+        } else if (nz3 > 1) {
+            v = 0.0;
+        } else if (wi && wj) {
+            v = 0.5 * ((i == 0 ? left : right) + (j == 0 ? bottom : top));
+        } else if (wj) {
+            v = j == 0 ? bottom : top;
+        } else {
+            v = i == 0 ? left : right;
+        }
+        phi[q] = v;
+    }
+}
+
+// 3D E by differences, one-sided at the walls (src/FieldSolver.cpp:872-904)
+__global__ void k_dir_efield3(const double* __restrict__ phi, double* __restrict__ E, int nx, int ny, int nz, double dx,
+                              double dy, double dz) {
+    const size_t N = (size_t)nx * ny * nz, sy = nx, sz = (size_t)nx * ny;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < N; q += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(q % nx), j = (int)((q / nx) % ny), k = (int)(q / sz);
+        double ex, ey, ez;
+        if (i == 0) ex = -(phi[q + 1] - phi[q]) / dx;
+        else if (i + 1 == nx) ex = -(phi[q] - phi[q - 1]) / dx;
+        else ex = -(phi[q + 1] - phi[q - 1]) / (2.0 * dx);
+        if (j == 0) ey = -(phi[q + sy] - phi[q]) / dy;
+        else if (j + 1 == ny) ey = -(phi[q] - phi[q - sy]) / dy;
+        else ey = -(phi[q + sy] - phi[q - sy]) / (2.0 * dy);
+        if (k == 0) ez = -(phi[q + sz] - phi[q]) / dz;
+        else if (k + 1 == nz) ez = -(phi[q] - phi[q - sz]) / dz;
+        else ez = -(phi[q + sz] - phi[q - sz]) / (2.0 * dz);
+        E[q] = ex;
+        E[N + q] = ey;
+        E[2 * N + q] = ez;
+    }
+}
+
+static void solve_dirichlet_nd(int dims, const size_t* n, const double* length, double permittivity,
+                               const double* pot, const double* rho, double* phi, double* electric) {
+    require(dims == 2 || dims == 3, "dims must be 2 or 3");
+    require(n && length && rho && phi && electric, "null argument");
+    require(std::isfinite(permittivity) && permittivity > 0, "field-solver permittivity must be positive and finite");
+    double side[4] = {0.0, 0.0, 0.0, 0.0};
+    if (pot) {
+        for (int a = 0; a < 4; ++a) {
+            require(std::isfinite(pot[a]), "wall potentials must be finite");
+            side[a] = pot[a];
+        }
+        require(dims == 2 || (side[0] == 0.0 && side[1] == 0.0 && side[2] == 0.0 && side[3] == 0.0),
+                "3D Dirichlet walls are grounded");
+    }
+    size_t N = 1, Mtot = 1;
+    for (int a = 0; a < dims; ++a) {
+        require(n[a] >= 3 && pow2(n[a] - 1) && 2 * (n[a] - 1) <= (size_t)kMaxLine,
+                "each extent must be 2^k + 1 nodes, 3 to 513", APIC_ERR_UNSUPPORTED);
+        require(std::isfinite(length[a]) && length[a] > 0, "domain lengths must be positive and finite");
+        N *= n[a];
+        Mtot *= n[a] - 2;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
+    const int nx = (int)n[0], ny = (int)n[1], nz3 = dims == 3 ? (int)n[2] : 1;
+    const int Mx = nx - 2, My = ny - 2, Mz = dims == 3 ? nz3 - 2 : 1;
+    // Mesh2D / Mesh3D Dirichlet spacing L / (n - 1)
+    const double dx = length[0] / (double)(nx - 1), dy = length[1] / (double)(ny - 1);
+    const double dz = dims == 3 ? length[2] / (double)(nz3 - 1) : 1.0;
+    const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy), idz2 = dims == 3 ? 1.0 / (dz * dz) : 0.0;
+    MixedScratch S;
+    APIC_CUDA(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
+    double* d_rho = S.get<double>(N);
+    double* d_phi = S.get<double>(N);
+    double* d_E = S.get<double>((size_t)dims * N);
+    double* d_u = S.get<double>(Mtot);
+    const int M[3] = {Mx, My, Mz};
+    Cplx* d_tw[3] = {nullptr, nullptr, nullptr};
+    for (int a = 0; a < dims; ++a) {
+        const int L2 = 2 * (M[a] + 1);
+        std::vector<Cplx> tw(L2);
+        const double twopi = 2.0 * 3.141592653589793;
+        for (int k = 0; k < L2; ++k) tw[k] = {std::cos(twopi * k / L2), -std::sin(twopi * k / L2)};
+        d_tw[a] = S.get<Cplx>(L2);
+        APIC_CUDA(cudaMemcpyAsync(d_tw[a], tw.data(), L2 * sizeof(Cplx), cudaMemcpyHostToDevice, S.s));
+    }
+    APIC_CUDA(cudaMemcpyAsync(d_rho, rho, N * sizeof(double), cudaMemcpyHostToDevice, S.s));
+    const unsigned g = (unsigned)std::min<size_t>((N + 255) / 256, 4096);
+    k_dir_rhs<<<g, 256, 0, S.s>>>(d_rho, d_u, nx, ny, nz3, permittivity, idx2, idy2, side[0], side[1], side[2],
+                                  side[3]);
+    APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(3 * kMaxLine * sizeof(Cplx))));
+    // axis a: element stride, then the two line axes (stride_a over lines_a, stride_b over the rest)
+    auto dst_axis = [&](int a) {
+        const long long sx = 1, sy = Mx, sz = (long long)Mx * My;
+        long long stride, stride_a, stride_b;
+        int lines_a;
+        size_t lines;
+        if (a == 0) { stride = sx; lines_a = My; stride_a = sy; stride_b = sz; lines = (size_t)My * Mz; }
+        else if (a == 1) { stride = sy; lines_a = Mx; stride_a = sx; stride_b = sz; lines = (size_t)Mx * Mz; }
+        else { stride = sz; lines_a = Mx; stride_a = sx; stride_b = sy; lines = (size_t)Mx * My; }
+        const size_t smem = 3 * (size_t)(2 * (M[a] + 1)) * sizeof(Cplx);
+        k_dst_lines<<<(unsigned)lines, kFftThreads, smem, S.s>>>(d_u, M[a], stride, lines_a, stride_a, stride_b, d_tw[a]);
+    };
+    for (int a = 0; a < dims; ++a) dst_axis(a);
+    double scale = 1.0;
+    for (int a = 0; a < dims; ++a) scale *= 2.0 / (double)(M[a] + 1);
+    k_dir_divide<<<g, 256, 0, S.s>>>(d_u, Mx, My, Mz, idx2, idy2, idz2, scale);
+    for (int a = 0; a < dims; ++a) dst_axis(a);
+    k_dir_assemble<<<g, 256, 0, S.s>>>(d_u, d_phi, nx, ny, nz3, side[0], side[1], side[2], side[3]);
+    if (dims == 2) k_mixed_efield<<<g, 256, 0, S.s>>>(d_phi, d_E, nx, ny, dx, dy, 0, 0);
+    else k_dir_efield3<<<g, 256, 0, S.s>>>(d_phi, d_E, nx, ny, nz3, dx, dy, dz);
+    APIC_CUDA(cudaGetLastError());
+    APIC_CUDA(cudaMemcpyAsync(phi, d_phi, N * sizeof(double), cudaMemcpyDeviceToHost, S.s));
+    APIC_CUDA(cudaMemcpyAsync(electric, d_E, (size_t)dims * N * sizeof(double), cudaMemcpyDeviceToHost, S.s));
+    const cudaError_t e = bounded_wait(S.s, 600.0);
+    if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
+    APIC_CUDA(e);
+}
+
 }  // namespace nd
 }  // namespace apic
 
@@ -2223,6 +2423,13 @@ int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length
         S.solver.F.rho_in = d_rho;
         S.solver.solve();
         S.read_fields(nullptr, phi, electric);
+    });
+}
+
+int apic_field_solve_dirichlet_nd(int dims, const size_t* n, const double* length, double permittivity,
+                                  const double* side_potentials, const double* rho, double* phi, double* electric) {
+    return guarded_nd(nullptr, [&] {
+        apic::nd::solve_dirichlet_nd(dims, n, length, permittivity, side_potentials, rho, phi, electric);
     });
 }
 

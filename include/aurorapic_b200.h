@@ -376,6 +376,20 @@ APIC_EXPORT int apic_simnd_launch_count(apic_sim_nd* sim, uint64_t* launches);
 APIC_EXPORT int apic_field_solve_periodic_nd(int dims, const size_t* n, const double* length, double permittivity,
                                              const double* rho, double* phi, double* electric);
 
+/* FieldSolver::solve(Mesh2D&/Mesh3D&) for a mesh with walls on every side
+ * (solve_dirichlet_iterative, src/FieldSolver.cpp:761-907, with
+ * apply_dirichlet_boundary_potentials, :267-296): 2D walls at
+ * side_potentials = {left, right, bottom, top} (NULL: grounded; corner nodes the
+ * mean of their two sides), 3D walls grounded (side_potentials NULL or zero).
+ * The reference iterates SOR until the largest update is below 1e-11; this
+ * solves the same discrete system directly (discrete sine transforms), so the
+ * results agree to the reference's convergence.  Mesh spacing L / (n - 1); every
+ * extent 2^k + 1 nodes from 3 to 513 (APIC_ERR_UNSUPPORTED otherwise).  rho,
+ * phi: N = prod(n) values (index (k * ny + j) * nx + i); electric: [dims][N]. */
+APIC_EXPORT int apic_field_solve_dirichlet_nd(int dims, const size_t* n, const double* length, double permittivity,
+                                              const double* side_potentials, const double* rho, double* phi,
+                                              double* electric);
+
 /* FieldSolver::solve(Mesh2D&) for a mesh with exactly one periodic axis
  * (solve_mixed_spectral_tridiagonal, src/FieldSolver.cpp:501-657, and
  * compute_electric_field, :298-346): Fourier transform along the periodic axis,

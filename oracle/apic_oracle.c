@@ -1083,6 +1083,78 @@ int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* 
     return 0;
 }
 
+/* solve_dirichlet_iterative(Mesh2D&) / (Mesh3D&), src/FieldSolver.cpp:761-907:
+ * fixed wall potentials (2D: left, right, bottom, top, corners the mean of their
+ * two sides, apply_dirichlet_boundary_potentials :267-296; 3D: grounded), then
+ * lexicographic SOR (omega 1.7 in 2D, 1.65 in 3D) until the largest update is
+ * below 1e-11, then E by differences (one-sided at the walls).  Mesh spacing
+ * L / (n - 1).  E holds [dims][N].  Returns nonzero when SOR does not converge. */
+int ora_solve_dirichlet_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                           double eps, const double* pot) {
+    const size_t nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
+    const double dx = L[0] / (double)(nx - 1), dy = L[1] / (double)(ny - 1);
+    const double dz = dims == 3 ? L[2] / (double)(nz - 1) : 1.0;
+    const size_t N = nx * ny * nz;
+    for (size_t i = 0; i < N; ++i) phi[i] = 0.0;
+    if (dims == 2) {
+        const double left = pot ? pot[0] : 0.0, right = pot ? pot[1] : 0.0;
+        const double bottom = pot ? pot[2] : 0.0, top = pot ? pot[3] : 0.0;
+        for (size_t j = 0; j < ny; ++j) { phi[j * nx] = left; phi[j * nx + nx - 1] = right; }
+        for (size_t i = 0; i < nx; ++i) { phi[i] = bottom; phi[(ny - 1) * nx + i] = top; }
+        phi[0] = 0.5 * (left + bottom);
+        phi[nx - 1] = 0.5 * (right + bottom);
+        phi[(ny - 1) * nx] = 0.5 * (left + top);
+        phi[(ny - 1) * nx + nx - 1] = 0.5 * (right + top);
+    }
+    const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy), idz2 = dims == 3 ? 1.0 / (dz * dz) : 0.0;
+    const double diag = dims == 3 ? 2.0 * (idx2 + idy2 + idz2) : 2.0 * (idx2 + idy2);
+    const double omega = dims == 3 ? 1.65 : 1.7;
+    const size_t maxit = dims == 3 ? (50000 > 150 * N ? 50000 : 150 * N) : (20000 > 100 * N ? 20000 : 100 * N);
+    int converged = 0;
+    for (size_t it = 0; it < maxit && !converged; ++it) {
+        double md = 0.0;
+        for (size_t k = (dims == 3 ? 1 : 0); k + (dims == 3 ? 1 : 0) < nz; ++k)
+            for (size_t j = 1; j + 1 < ny; ++j)
+                for (size_t i = 1; i + 1 < nx; ++i) {
+                    const size_t id = (k * ny + j) * nx + i;
+                    const double rhs = rho[id] / eps;
+                    double up;
+                    if (dims == 2)
+                        up = ((phi[id - 1] + phi[id + 1]) * idx2 + (phi[id - nx] + phi[id + nx]) * idy2 + rhs) / diag;
+                    else
+                        up = ((phi[id - 1] + phi[id + 1]) * idx2 + (phi[id - nx] + phi[id + nx]) * idy2 +
+                              (phi[id - nx * ny] + phi[id + nx * ny]) * idz2 + rhs) / diag;
+                    const double d = omega * (up - phi[id]);
+                    phi[id] += d;
+                    if (fabs(d) > md) md = fabs(d);
+                }
+        if (md < 1.0e-11) converged = 1;
+    }
+    if (!converged) return seterr(1, "Dirichlet Poisson solve did not converge");
+    for (size_t k = 0; k < nz; ++k)
+        for (size_t j = 0; j < ny; ++j)
+            for (size_t i = 0; i < nx; ++i) {
+                const size_t id = (k * ny + j) * nx + i;
+                double ex, ey;
+                if (i == 0) ex = -(phi[id + 1] - phi[id]) / dx;
+                else if (i + 1 == nx) ex = -(phi[id] - phi[id - 1]) / dx;
+                else ex = -(phi[id + 1] - phi[id - 1]) / (2.0 * dx);
+                if (j == 0) ey = -(phi[id + nx] - phi[id]) / dy;
+                else if (j + 1 == ny) ey = -(phi[id] - phi[id - nx]) / dy;
+                else ey = -(phi[id + nx] - phi[id - nx]) / (2.0 * dy);
+                E[id] = ex;
+                E[N + id] = ey;
+                if (dims == 3) {
+                    double ez;
+                    if (k == 0) ez = -(phi[id + nx * ny] - phi[id]) / dz;
+                    else if (k + 1 == nz) ez = -(phi[id] - phi[id - nx * ny]) / dz;
+                    else ez = -(phi[id + nx * ny] - phi[id - nx * ny]) / (2.0 * dz);
+                    E[2 * N + id] = ez;
+                }
+            }
+    return 0;
+}
+
 /* Periodic CIC stencil of one axis, src/Mesh2D.cpp:96-129, src/FieldSolver.cpp:936-960 */
 static void cic_axis(double x, double L, double d, size_t n, size_t* i0, size_t* i1, double* f) {
     const double xp = wrap(x, L);

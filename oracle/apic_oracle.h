@@ -95,6 +95,10 @@ const char* ora_last_error(void);
 /* ---- structured 2D3V / 3D3V periodic -------------------------------------- */
 void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
                   double eps);
+/* FieldSolver::solve(Mesh2D&/Mesh3D&) on fully Dirichlet meshes (the reference's
+ * SOR); pot: 2D left, right, bottom, top (NULL = grounded); 3D grounded. */
+int ora_solve_dirichlet_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                           double eps, const double* pot);
 /* FieldSolver::solve(Mesh2D&) with exactly one periodic axis (power of two). */
 int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* n, const double* L,
                        int periodic_axis, double eps, double lower, double upper);

@@ -482,6 +482,36 @@ def solve_mixed_2d(rho, n, L, periodic_axis, eps, lower, upper):
     return phi, E.reshape(2, N)
 
 
+def solve_dirichlet_nd(rho, n, L, eps, potentials=None):
+    """Oracle SOR solve on a fully Dirichlet mesh: (phi, E[dims])."""
+    Lb = oracle()
+    Lb.ora_solve_dirichlet_nd.argtypes = [_DP, _DP, _DP, C.c_int, _SZP, _DP, C.c_double, _DP]
+    dims = len(n)
+    N = int(np.prod(n))
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    phi, E = np.zeros(N), np.zeros(dims * N)
+    pot = None if potentials is None else np.ascontiguousarray(potentials, dtype=np.float64)
+    rc = Lb.ora_solve_dirichlet_nd(dptr(rho), dptr(phi), dptr(E), dims, sizes3(n), dptr(arr3(L)), eps,
+                                   dptr(pot) if pot is not None else None)
+    if rc:
+        raise RuntimeError(Lb.ora_last_error().decode())
+    return phi, E.reshape(dims, N)
+
+
+def ref_solve_dirichlet_nd(rho, n, L, eps, potentials=(0.0, 0.0, 0.0, 0.0)):
+    """The reference's FieldSolver on a fully Dirichlet Mesh2D / Mesh3D."""
+    Lb = ref()
+    Lb.ref_solve_dirichlet_nd.argtypes = [C.c_int, _SZP, _DP, C.c_double, _DP, _DP, _DP, _DP]
+    dims = len(n)
+    N = int(np.prod(n))
+    rho = np.ascontiguousarray(rho, dtype=np.float64).ravel()
+    phi, E = np.zeros(N), np.zeros(dims * N)
+    pot = np.ascontiguousarray(potentials, dtype=np.float64)
+    if Lb.ref_solve_dirichlet_nd(dims, sizes3(n), dptr(arr3(L)), eps, dptr(pot), dptr(rho), dptr(phi), dptr(E)):
+        raise RuntimeError(Lb.ref_last_error().decode())
+    return phi, E.reshape(dims, N)
+
+
 def ref_solve_mixed_2d(rho, n, L, periodic_axis, eps, lower, upper):
     """The reference's own FieldSolver on a mixed Mesh2D, through the harness."""
     Lb = ref()

@@ -589,6 +589,37 @@ int ref_aps_read(const char* path, size_t max_particles, uint64_t* signature, si
     } catch (const std::exception& e) { return fail(e); }
 }
 
+/* FieldSolver::solve on a fully Dirichlet Mesh2D (side potentials pot: left,
+ * right, bottom, top) or Mesh3D (grounded). */
+int ref_solve_dirichlet_nd(int dims, const size_t* n, const double* L, double eps, const double* pot,
+                           const double* rho, double* phi, double* E) {
+    try {
+        pic::FieldSolver solver(eps);
+        if (dims == 2) {
+            pic::BoundaryConfig2D bc;
+            bc.left.potential = pot[0]; bc.right.potential = pot[1];
+            bc.bottom.potential = pot[2]; bc.top.potential = pot[3];
+            pic::Mesh2D mesh(n[0], n[1], L[0], L[1], pic::Boundary::Dirichlet, pic::Boundary::Dirichlet, bc);
+            const size_t N = n[0] * n[1];
+            std::memcpy(mesh.rho().data(), rho, N * 8);
+            solver.solve(mesh);
+            std::memcpy(phi, mesh.phi().data(), N * 8);
+            std::memcpy(E, mesh.electric_x().data(), N * 8);
+            std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+        } else {
+            pic::Mesh3D mesh(n[0], n[1], n[2], L[0], L[1], L[2], pic::Boundary::Dirichlet);
+            const size_t N = n[0] * n[1] * n[2];
+            std::memcpy(mesh.rho().data(), rho, N * 8);
+            solver.solve(mesh);
+            std::memcpy(phi, mesh.phi().data(), N * 8);
+            std::memcpy(E, mesh.electric_x().data(), N * 8);
+            std::memcpy(E + N, mesh.electric_y().data(), N * 8);
+            std::memcpy(E + 2 * N, mesh.electric_z().data(), N * 8);
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
 int ref_solve_nd(int dims, const size_t* n, const double* L, double eps, const double* rho, double* phi, double* E) {
     try {
         pic::FieldSolver solver(eps);

@@ -262,6 +262,24 @@ def mixed_fixture():
                             lower=lo, upper=hi, rho=rho.ravel(), phi=phi, E=E)
 
 
+DIRICHLET_CASES = {
+    # name: (n, L, side potentials left, right, bottom, top)
+    "dirichlet2d": ((17, 9), (0.02, 0.01), (0.0, 50.0, -10.0, 5.0)),
+    "dirichlet3d": ((9, 5, 9), (0.01, 0.005, 0.01), (0.0, 0.0, 0.0, 0.0)),
+}
+
+
+def dirichlet_fixture():
+    """FieldSolver::solve on fully Dirichlet meshes (the reference's SOR)."""
+    eps = 8.8541878128e-12
+    for k, (name, (n, L, pot)) in enumerate(DIRICHLET_CASES.items()):
+        rng = np.random.default_rng(70 + k)
+        rho = 1e-6 * (1.0 + 0.3 * rng.standard_normal(int(np.prod(n))))
+        phi, E = po.ref_solve_dirichlet_nd(rho, n, L, eps, pot)
+        np.savez_compressed(os.path.join(HERE, f"{name}.npz"), n=np.array(n), L=np.array(L), eps=eps,
+                            pot=np.array(pot), rho=rho, phi=phi, E=E)
+
+
 def main(names=None):
     if names:
         for n in names:
@@ -269,6 +287,7 @@ def main(names=None):
         print("golden vectors written to", HERE)
         return
     mixed_fixture()
+    dirichlet_fixture()
     bprofile_fixture()
     swarm_ensemble_fixture()
     swarm_fixture()

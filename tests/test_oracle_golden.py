@@ -200,3 +200,14 @@ def test_tabulated_magnetic_field_run_bit_exact(name, dims, n):
             assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
     rho, phi, E = sim.fields()
     assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
+
+
+@pytest.mark.parametrize("name", ["dirichlet2d", "dirichlet3d"])
+def test_dirichlet_sor_solve_bit_exact(name):
+    """FieldSolver::solve on fully Dirichlet meshes (2D side potentials with the
+    corner rule, 3D grounded): the restated SOR is bit-exact with the reference."""
+    f = load(f"{name}.npz")
+    n = tuple(int(v) for v in f["n"])
+    pot = f["pot"] if len(n) == 2 else None
+    phi, E = po.solve_dirichlet_nd(f["rho"], n, f["L"], float(f["eps"]), pot)
+    assert np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
