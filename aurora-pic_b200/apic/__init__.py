@@ -109,6 +109,54 @@ class CollideStats(C.Structure):
     ]
 
 
+MAX_EEDF_REGIONS = 8
+SA_DENSITY, SA_VELOCITY_X, SA_VELOCITY_Y, SA_VELOCITY_Z, SA_KINETIC_ENERGY = range(5)
+SA_POTENTIAL, SA_ELECTRIC, SA_ELECTRIC_SQUARED, SA_COLLISION_ENERGY = range(5, 9)
+
+
+class SpatialAverage1D(C.Structure):
+    """apic_spatial_average1d: SpatialAverage1DConfig + PhaseEedf1DConfig."""
+    _fields_ = [
+        ("interval", C.c_size_t), ("start_step", C.c_size_t), ("end_step", C.c_size_t),
+        ("rf_frequency", C.c_double), ("rf_cycles", C.c_size_t), ("phase_bins", C.c_size_t),
+        ("eedf_species", C.c_int), ("eedf_bins", C.c_size_t), ("eedf_energy_max", C.c_double),
+        ("eedf_regions", C.c_int), ("eedf_x_min", C.c_double * MAX_EEDF_REGIONS),
+        ("eedf_x_max", C.c_double * MAX_EEDF_REGIONS),
+    ]
+
+
+class PhaseEedf1D(C.Structure):
+    _fields_ = [
+        ("macro_observations", C.c_uint64), ("overflow_macro_observations", C.c_uint64),
+        ("represented_observations", C.c_double), ("overflow_represented_observations", C.c_double),
+        ("weighted_energy_sum", C.c_double), ("weighted_energy_squared_sum", C.c_double),
+        ("weighted_velocity_x_sum", C.c_double), ("weighted_velocity_y_sum", C.c_double),
+        ("weighted_velocity_z_sum", C.c_double),
+    ]
+
+
+def spatial_average1d(interval=1, start_step=1, end_step=1, rf_frequency=0.0, rf_cycles=0, phase_bins=0,
+                      eedf_species=-1, eedf_bins=0, eedf_energy_max=0.0, eedf_regions=()) -> SpatialAverage1D:
+    """Spatial-average settings of a 1D run (the reference's spatial_average_*
+    and phase_eedf_* keys; eedf_regions as (x_min, x_max) pairs)."""
+    a = SpatialAverage1D()
+    a.interval, a.start_step, a.end_step = interval, start_step, end_step
+    a.rf_frequency, a.rf_cycles, a.phase_bins = rf_frequency, rf_cycles, phase_bins
+    a.eedf_species, a.eedf_bins, a.eedf_energy_max = eedf_species, eedf_bins, eedf_energy_max
+    a.eedf_regions = len(eedf_regions)
+    for i, (lo, hi) in enumerate(eedf_regions):
+        a.eedf_x_min[i], a.eedf_x_max[i] = lo, hi
+    return a
+
+
+def validate_spatial_average(cfg: "Config1D", sa: SpatialAverage1D):
+    """Raises ApicError with the reference's message for an invalid setting
+    (host only: no device needed)."""
+    rc = lib().apic_spatial_average1d_validate(C.byref(cfg), C.byref(sa))
+    if rc != 0:
+        raise ApicError(rc, lib().apic_sim1d_last_error(None).decode())
+
+
 _DP = C.POINTER(C.c_double)
 _U8P = C.POINTER(C.c_uint8)
 _U64P = C.POINTER(C.c_uint64)
@@ -152,6 +200,11 @@ def lib() -> C.CDLL:
     L.apic_sim1d_cuda_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.apic_sim1d_set_kernel_timing.argtypes = [C.c_void_p, C.c_int]
     L.apic_sim1d_kernel_times.argtypes = [C.c_void_p, _DP, _DP, _U64P]
+    L.apic_spatial_average1d_validate.argtypes = [C.POINTER(Config1D), C.POINTER(SpatialAverage1D)]
+    L.apic_sim1d_enable_spatial_average.argtypes = [C.c_void_p, C.POINTER(SpatialAverage1D)]
+    L.apic_sim1d_spatial_average_counts.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, _U64P]
+    L.apic_sim1d_spatial_sums.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _DP]
+    L.apic_sim1d_phase_eedf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(PhaseEedf1D), _DP]
     L.apic_deposit_solve_gather_1d.argtypes = [
         C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _DP, _DP,
         C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
@@ -247,7 +300,8 @@ class Simulation1D:
 
     def close(self):
         if getattr(self, "h", None):
-            lib().apic_sim1d_destroy(self.h)
+            if _lib is not None:  # the library outlives every handle, except at interpreter exit
+                _lib.apic_sim1d_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -320,6 +374,37 @@ class Simulation1D:
         n = C.c_uint64()
         _check(lib().apic_sim1d_kernel_times(self.h, C.byref(a), C.byref(b), C.byref(n)), self.h)
         return a.value, b.value, n.value
+
+    # -- CCP campaign diagnostics --
+    def enable_spatial_average(self, sa: SpatialAverage1D):
+        self._sa = sa
+        _check(lib().apic_sim1d_enable_spatial_average(self.h, C.byref(sa)), self.h)
+
+    def spatial_counts(self):
+        """(samples, collision steps, per-bin samples, per-bin collision steps)"""
+        P = int(self._sa.phase_bins)
+        a, b = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        pa, pb = np.zeros(max(P, 1), np.uint64), np.zeros(max(P, 1), np.uint64)
+        _check(lib().apic_sim1d_spatial_average_counts(self.h, a.ctypes.data_as(_U64P), b.ctypes.data_as(_U64P),
+                                                       pa.ctypes.data_as(_U64P), pb.ctypes.data_as(_U64P)), self.h)
+        return int(a[0]), int(b[0]), pa[:P], pb[:P]
+
+    def spatial_sums(self, quantity, index=0, phase=-1):
+        out = np.zeros(self.cfg.nx)
+        _check(lib().apic_sim1d_spatial_sums(self.h, quantity, index, phase, dptr(out)), self.h)
+        return out
+
+    def phase_eedf(self, phase, region):
+        """(counts [macro, overflow macro], sums [represented, overflow
+        represented, weighted energy, energy^2, v_x, v_y, v_z], histogram)"""
+        e = PhaseEedf1D()
+        hist = np.zeros(max(int(self._sa.eedf_bins), 1))
+        _check(lib().apic_sim1d_phase_eedf(self.h, phase, region, C.byref(e), dptr(hist)), self.h)
+        cnt = np.array([e.macro_observations, e.overflow_macro_observations], np.uint64)
+        sums = np.array([e.represented_observations, e.overflow_represented_observations, e.weighted_energy_sum,
+                         e.weighted_energy_squared_sum, e.weighted_velocity_x_sum, e.weighted_velocity_y_sum,
+                         e.weighted_velocity_z_sum])
+        return cnt, sums, hist[:int(self._sa.eedf_bins)]
 
     @property
     def time(self) -> float:

@@ -33,7 +33,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <memory>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -89,7 +91,7 @@ struct BirthRec {
     unsigned long long key;  // (parent species, parent slot, product index) ordering key
     double x, v[3];
     int species;
-    int pad;
+    int pad;  // secondary record: the parent's ionization channel
 };
 
 struct SpeciesDev {
@@ -141,6 +143,12 @@ struct Params1D {
     BirthRec* births;
     unsigned births_cap;
     DevState* st;
+    // campaign diagnostics: spatial collision-energy density of the collision
+    // part this pass applies ([channel][nx]; null outside the window) and the
+    // slice of its RF phase bin (null without phase bins)
+    double* coll_acc;
+    double* coll_phase_acc;
+    int coll_off[kMaxModels];  // first channel of each model in the channel numbering
 };
 
 // ---- field gather / deposit (reference arithmetic) ----------------------
@@ -245,6 +253,32 @@ __device__ __forceinline__ unsigned physical_slot_from(const unsigned* lstart, c
     return __ldg(start + r) + (idx - __ldg(lstart + r));
 }
 
+// ---- campaign diagnostics stencil ---------------------------------------------
+
+// Node volume of the diagnostics deposits: Grid::node_volume, src/Grid.cpp:26-30
+template <bool DIRICHLET>
+__device__ __forceinline__ double node_volume(const Params1D& p, int i) {
+    return (DIRICHLET && (i == 0 || i + 1 == p.nx)) ? 0.5 * p.dx : p.dx;
+}
+
+// deposit_spatial_collision_energy, src/Simulation.cpp:1171-1212: the energy
+// change as a density on the particle's two nodes (FP64 atomics: the sum's
+// rounding depends on the order of the collisions).
+template <bool DIRICHLET>
+__device__ __forceinline__ void collision_energy_deposit(const Params1D& p, double x, int channel, double e) {
+    const Cic d = cic<DIRICHLET>(x, p);
+    const double a0 = e * d.w0 / node_volume<DIRICHLET>(p, d.i0);
+    const double a1 = e * d.w1 / node_volume<DIRICHLET>(p, d.i1);
+    double* row = p.coll_acc + (size_t)channel * p.nx;
+    atomicAdd(row + d.i0, a0);
+    atomicAdd(row + d.i1, a1);
+    if (p.coll_phase_acc) {
+        row = p.coll_phase_acc + (size_t)channel * p.nx;
+        atomicAdd(row + d.i0, a0);
+        atomicAdd(row + d.i1, a1);
+    }
+}
+
 // ---- the fused particle pass -----------------------------------------------
 
 // A particle whose first exponential waiting time falls inside the step is a
@@ -273,7 +307,10 @@ __device__ __forceinline__ void st_comp(double* d, float* f, unsigned long long 
     else d[i] = v;
 }
 
-template <int VDIM, bool DIRICHLET, bool F32>
+// DIAG: the instantiation that also deposits the spatial collision energy (run
+// only inside a campaign-diagnostics window, so the plain pass keeps its
+// register allocation).
+template <int VDIM, bool DIRICHLET, bool F32, bool DIAG>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* sE = reinterpret_cast<double*>(smem_raw);
@@ -401,7 +438,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                                  const unsigned long long key =
                                      ((unsigned long long)s << 56) | ((unsigned long long)slot << 16) | (nion << 1);
                                  BirthRec a, b;
-                                 a.key = key; a.species = C.secondary; a.pad = 0;
+                                 a.key = key; a.species = C.secondary; a.pad = DIAG ? ch : 0;
                                  b.key = key | 1ull; b.species = C.ion; b.pad = 0;
                                  a.x = b.x = px;
                                  for (int d = 0; d < 3; ++d) { a.v[d] = vs[d]; b.v[d] = vi[d]; }
@@ -426,6 +463,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                     if (r.channel[ch]) {
                         atomicAdd(&st->chan[S.model][ch], (unsigned long long)r.channel[ch]);
                         atomicAdd(&st->chan_energy[S.model][ch], r.energy_change[ch] * S.weight);
+                    }
+                }
+                if (DIAG && p.coll_acc) {
+                    // tracked_energy_change, src/Simulation.cpp:862-923: the weighted
+                    // projectile change per channel, deposited at the particle (the
+                    // product pairs' energies follow from the births list in the
+                    // post kernel)
+                    for (int ch = 0; ch < M.nch; ++ch) {
+                        const double t = r.energy_change[ch] * S.weight;
+                        if (t != 0.0) collision_energy_deposit<DIRICHLET>(p, px, p.coll_off[S.model] + ch, t);
                     }
                 }
                 ce.v[0] = vel[0]; ce.v[1] = vel[1]; ce.v[2] = vel[2];
@@ -629,6 +676,20 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
     if (nb > (unsigned)kMaxBirths) {
         if (tid == 0) atomicOr(&st->error, kErrBirths);
         nb = kMaxBirths;
+    }
+    if (p.coll_acc) {
+        // collision-energy diagnostics: each product pair's energy in its
+        // channel at the parent's position (records come in pairs: secondary, ion)
+        for (unsigned j = tid; 2 * j + 1 < nb; j += kPostThreads) {
+            const BirthRec a = p.births[2 * j], b = p.births[2 * j + 1];
+            const SpeciesDev& A = p.sp[a.species];
+            const SpeciesDev& B = p.sp[b.species];
+            const double added =
+                0.5 * A.mass * A.weight * (a.v[0] * a.v[0] + a.v[1] * a.v[1] + a.v[2] * a.v[2]) +
+                0.5 * B.mass * B.weight * (b.v[0] * b.v[0] + b.v[1] * b.v[1] + b.v[2] * b.v[2]);
+            const int parent = (int)(a.key >> 56);
+            collision_energy_deposit<DIRICHLET>(p, a.x, p.coll_off[p.sp[parent].model] + a.pad, added);
+        }
     }
     if (nb > 0) {
         int idx[kPostItems];
@@ -894,6 +955,160 @@ __global__ void k_widen1d(const float* __restrict__ in, double* __restrict__ out
     for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = (double)in[i];
 }
 
+// ---- campaign diagnostics: moments of a sample ------------------------------
+
+constexpr int kMomThreads = 512;
+constexpr int kMaxEedfRegions = APIC_MAX_EEDF_REGIONS;
+constexpr size_t kMomentSmemMax = 200 * 1024;  // moment rows (5 nx doubles) + a staged EEDF histogram
+
+struct MomentArgs {
+    double* scratch;               // [5][nspecies][nx] moments of this sample (zero on entry)
+    int eedf_species;              // -1: no phase EEDF this sample
+    int regions;
+    double xmin[kMaxEedfRegions], xmax[kMaxEedfRegions];
+    unsigned bins;
+    double emax, escale;
+    unsigned long long* eedf_cnt;  // [regions][2] of the sample's phase bin
+    double* eedf_sum;              // [regions][7]
+    double* eedf_hist;             // [regions][bins]
+    int hist_shared;               // histogram staged in shared memory
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Species::deposit_velocity_moments (src/Species.cpp:285-336) of every species
+// and accumulate_phase_eedf (src/Simulation.cpp:1238-1285) of the EEDF species,
+// on the state right after a step's collision part (time-centred v in S.v, the
+// layout dense).  Per CTA the five moment rows live in shared memory (FP64
+// atomics), then are added to the sample's scratch rows; the EEDF sums are
+// warp-reduced per region.  One CTA per SM.
+template <int VDIM, bool DIRICHLET, bool F32>
+__global__ void __launch_bounds__(kMomThreads) k_moments1d(Params1D p, MomentArgs a) {
+    extern __shared__ __align__(16) unsigned char mom_raw[];
+    double* sm = reinterpret_cast<double*>(mom_raw);  // [5][nx]
+    double* sh = sm + 5 * p.nx;                       // [regions][bins] when staged
+    __shared__ double s_es[kMaxEedfRegions][7];
+    __shared__ unsigned long long s_ec[kMaxEedfRegions][2];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int nx = p.nx;
+    for (int s = 0; s < p.nspecies; ++s) {
+        const SpeciesDev& S = p.sp[s];
+        const unsigned n = p.st->n[s];
+        const bool eedf = s == a.eedf_species;
+        const unsigned hist_n = eedf && a.hist_shared ? (unsigned)a.regions * a.bins : 0u;
+        for (int i = tid; i < 5 * nx; i += kMomThreads) sm[i] = 0.0;
+        for (unsigned i = tid; i < hist_n; i += kMomThreads) sh[i] = 0.0;
+        if (tid < kMaxEedfRegions * 7) (&s_es[0][0])[tid] = 0.0;
+        if (tid < kMaxEedfRegions * 2) (&s_ec[0][0])[tid] = 0ull;
+        __syncthreads();
+        const double w = S.weight;
+        const double hmw = 0.5 * S.mass * S.weight;
+        double* hist = a.hist_shared ? sh : a.eedf_hist;
+        for (unsigned base = blockIdx.x * kMomThreads; base < n; base += gridDim.x * kMomThreads) {
+            const unsigned i = base + tid;
+            const bool live = i < n;
+            double x = 0.0, v = 0.0, vy = 0.0, vz = 0.0;
+            if (live) {
+                x = S.x[0][i];
+                v = S.v[i];
+                if (VDIM == 3) {
+                    vy = ld_comp<F32>(S.vy[0], S.vy32[0], i);
+                    vz = ld_comp<F32>(S.vz[0], S.vz32[0], i);
+                }
+                const Cic d = cic<DIRICHLET>(x, p);
+                const double pe = hmw * (v * v + vy * vy + vz * vz);
+                const double vol0 = node_volume<DIRICHLET>(p, d.i0), vol1 = node_volume<DIRICHLET>(p, d.i1);
+                const double r0 = w * d.w0 / vol0, r1 = w * d.w1 / vol1;
+                atomicAdd(sm + d.i0, r0);
+                atomicAdd(sm + nx + d.i0, r0 * v);
+                atomicAdd(sm + 2 * nx + d.i0, r0 * vy);
+                atomicAdd(sm + 3 * nx + d.i0, r0 * vz);
+                atomicAdd(sm + 4 * nx + d.i0, pe * d.w0 / vol0);
+                atomicAdd(sm + d.i1, r1);
+                atomicAdd(sm + nx + d.i1, r1 * v);
+                atomicAdd(sm + 2 * nx + d.i1, r1 * vy);
+                atomicAdd(sm + 3 * nx + d.i1, r1 * vz);
+                atomicAdd(sm + 4 * nx + d.i1, pe * d.w1 / vol1);
+            }
+            if (eedf) {
+                const double vsq = v * v + (VDIM == 3 ? vy * vy + vz * vz : 0.0);
+                const double energy = 0.5 * S.mass * vsq / a.escale;
+                for (int r = 0; r < a.regions; ++r) {
+                    const bool in = live && !(x < a.xmin[r] || x > a.xmax[r]);
+                    const bool over = in && energy >= a.emax;
+                    const unsigned c0 = __popc(__ballot_sync(0xffffffffu, in));
+                    if (c0 == 0) continue;  // warp-uniform
+                    const unsigned c1 = __popc(__ballot_sync(0xffffffffu, over));
+                    double q[7] = {in ? w : 0.0, over ? w : 0.0, in ? w * energy : 0.0,
+                                   in ? w * energy * energy : 0.0, in ? w * v : 0.0, in ? w * vy : 0.0,
+                                   in ? w * vz : 0.0};
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) q[k] = warp_sum(q[k]);
+                    if (lane == 0) {
+                        atomicAdd(&s_ec[r][0], (unsigned long long)c0);
+                        if (c1) atomicAdd(&s_ec[r][1], (unsigned long long)c1);
+#pragma unroll
+                        for (int k = 0; k < 7; ++k)
+                            if (q[k] != 0.0) atomicAdd(&s_es[r][k], q[k]);
+                    }
+                    if (in && !over) {
+                        unsigned long long b = (unsigned long long)(energy / a.emax * (double)a.bins);
+                        if (b > a.bins - 1) b = a.bins - 1;
+                        atomicAdd(hist + (size_t)r * a.bins + b, w);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        for (int i = tid; i < 5 * nx; i += kMomThreads) {
+            const double val = sm[i];
+            if (val != 0.0) {
+                const int q = i / nx, j = i - q * nx;
+                atomicAdd(a.scratch + ((size_t)q * p.nspecies + s) * nx + j, val);
+            }
+        }
+        if (eedf) {
+            for (unsigned i = tid; i < hist_n; i += kMomThreads)
+                if (sh[i] != 0.0) atomicAdd(a.eedf_hist + i, sh[i]);
+            if (tid < a.regions * 7) {
+                const double val = s_es[tid / 7][tid % 7];
+                if (val != 0.0) atomicAdd(a.eedf_sum + tid, val);
+            }
+            if (tid < a.regions * 2) {
+                const unsigned long long c = s_ec[tid / 2][tid % 2];
+                if (c) atomicAdd(a.eedf_cnt + tid, c);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// The sample's moments and the fields (phi, E, E^2) added to the window sums
+// and to the sample's phase bin (null: none); the scratch rows are cleared for
+// the next sample (src/Simulation.cpp:1335-1361).
+__global__ void k_sa_fold1d(Params1D p, double* scratch, double* tot, double* bin) {
+    const int nx = p.nx;
+    const int moments = 5 * p.nspecies * nx;
+    const int total = moments + 3 * nx;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        double v;
+        if (i < moments) {
+            v = scratch[i];
+            scratch[i] = 0.0;
+        } else {
+            const int f = (i - moments) / nx, j = i - moments - f * nx;
+            const double e = p.E[j];
+            v = f == 0 ? p.phi[j] : (f == 1 ? e : e * e);
+        }
+        tot[i] += v;
+        if (bin) bin[i] += v;
+    }
+}
+
 // Simulation::sample reductions (src/Simulation.cpp:1140-1161,
 // src/Species.cpp:338-351): per-block partial sums, then the last block adds
 // the partials in block order, so the result does not depend on scheduling.
@@ -1043,6 +1258,56 @@ std::string describe_device_error(unsigned w) {
     return s;
 }
 
+// validate_spatial_average_1d, src/Config.cpp:1377-1524, for an enabled
+// spatial average (the EEDF species by index, its regions by bounds).
+void validate_spatial_average(const apic_config1d& c, const apic_spatial_average1d& a) {
+    if (a.eedf_species < 0) {
+        require(a.eedf_bins == 0 && a.eedf_energy_max == 0.0 && a.eedf_regions == 0,
+                "disabled phase_eedf cannot configure species, bins, energy maximum, or regions");
+    } else {
+        require(a.phase_bins != 0, "phase_eedf requires spatial averaging with phase bins");
+        require(a.eedf_bins != 0 && a.eedf_bins <= 1000000 && std::isfinite(a.eedf_energy_max) &&
+                    a.eedf_energy_max > 0.0 && a.eedf_regions > 0,
+                "phase_eedf requires a species, 1..1000000 bins, a positive energy maximum, and at least one region");
+        require(a.eedf_species < c.nspecies, "phase_eedf species does not exist: " + std::to_string(a.eedf_species));
+        require(a.eedf_regions <= kMaxEedfRegions, "phase_eedf supports at most 8 regions on the device",
+                APIC_ERR_UNSUPPORTED);
+        for (int r = 0; r < a.eedf_regions; ++r)
+            require(std::isfinite(a.eedf_x_min[r]) && std::isfinite(a.eedf_x_max[r]) && a.eedf_x_min[r] >= 0.0 &&
+                        a.eedf_x_max[r] <= c.length && a.eedf_x_max[r] > a.eedf_x_min[r],
+                    "phase_eedf regions require unique safe names and 0 <= x_min < x_max <= length");
+    }
+    require(std::isfinite(a.rf_frequency) && a.rf_frequency >= 0.0,
+            "spatial_average_rf_frequency must be non-negative and finite");
+    require(a.interval != 0, "spatial_average_interval must be positive");
+    require(a.start_step != 0 && a.end_step >= a.start_step, "spatial_average requires 1 <= start_step <= end_step");
+    if (a.rf_frequency == 0.0) {
+        require(a.rf_cycles == 0 && a.phase_bins == 0,
+                "spatial_average_rf_cycles requires positive spatial_average_rf_frequency");
+        return;
+    }
+    require(a.rf_cycles != 0, "positive spatial_average_rf_frequency requires positive spatial_average_rf_cycles");
+    const double spc_value = 1.0 / (a.rf_frequency * c.dt);
+    require(std::isfinite(spc_value) && spc_value <= (double)std::numeric_limits<long long>::max(),
+            "spatial-average RF steps per cycle are invalid");
+    const size_t spc = (size_t)std::llround(spc_value);
+    require(spc != 0 && !(std::fabs(spc_value - (double)spc) > 1e-10 * std::max(1.0, spc_value)),
+            "spatial-average RF period must contain an integer number of timesteps");
+    require(a.rf_cycles <= std::numeric_limits<size_t>::max() / spc, "spatial-average RF window step count overflows");
+    require(a.end_step - a.start_step + 1 == a.rf_cycles * spc,
+            "spatial-average step window does not span the configured whole RF cycles");
+    require(a.end_step % spc == 0, "spatial-average RF window must end at the time-zero drive phase");
+    require(spc % a.interval == 0, "spatial_average_interval must divide RF steps per cycle");
+    const size_t per_cycle = spc / a.interval;
+    require(!(a.phase_bins > per_cycle || (a.phase_bins != 0 && per_cycle % a.phase_bins != 0)),
+            "spatial_average_phase_bins must divide the sampled RF cycle");
+    for (const apic_voltage_drive& d : {c.drive_left, c.drive_right}) {
+        if (d.amplitude == 0.0) continue;
+        require(!(std::fabs(d.frequency - a.rf_frequency) > 1e-12 * std::max(d.frequency, a.rf_frequency)),
+                "spatial-average RF frequency does not match the electrode drive");
+    }
+}
+
 struct Sim1D {
     apic_config1d cfg{};
     std::string last_error;
@@ -1067,6 +1332,141 @@ struct Sim1D {
         allocations.push_back(ptr);
         APIC_CUDA(cudaMemsetAsync(ptr, 0, std::max<size_t>(count, 1) * sizeof(T), stream));
         return static_cast<T*>(ptr);
+    }
+
+    // ---- campaign diagnostics (spatial average, phase bins, collision energy, phase EEDF) ----
+    struct SpatialAvg {
+        bool on = false;
+        apic_spatial_average1d cfg{};
+        size_t spc = 0, P = 0;  // RF steps per cycle, phase bins
+        int nch = 0;
+        double* tot = nullptr;         // [5][nspecies][nx] moments + [3][nx] fields
+        double* phase = nullptr;       // [P][same block]
+        double* scratch = nullptr;     // [5][nspecies][nx] of one sample
+        double* coll = nullptr;        // [nch][nx]
+        double* coll_phase = nullptr;  // [P][nch][nx]
+        unsigned long long* eedf_cnt = nullptr;  // [P][regions][2]
+        double* eedf_sum = nullptr;              // [P][regions][7]
+        double* eedf_hist = nullptr;             // [P][regions][bins]
+        bool hist_shared = false;
+        uint64_t samples = 0, coll_steps = 0;
+        std::vector<uint64_t> psamples, pcoll;
+    } sa;
+
+    size_t sa_block() const { return (5 * (size_t)cfg.nspecies + 3) * cfg.nx; }
+
+    void enable_spatial_average(const apic_spatial_average1d& a) {
+        require(!initialized, "spatial averaging must be enabled before initialize() or resume()", APIC_ERR_STATE);
+        require(!sa.on, "spatial averaging is already enabled", APIC_ERR_STATE);
+        validate_spatial_average(cfg, a);
+        sa.cfg = a;
+        sa.spc = a.rf_frequency > 0.0 ? (size_t)std::llround(1.0 / (a.rf_frequency * cfg.dt)) : 0;
+        sa.P = a.phase_bins;
+        sa.nch = 0;
+        for (int m = 0; m < cfg.nmodels; ++m) {
+            p.coll_off[m] = sa.nch;
+            sa.nch += cfg.models[m].nch;
+        }
+        const size_t nx = cfg.nx;
+        sa.tot = dalloc<double>(sa_block());
+        sa.phase = dalloc<double>(sa.P * sa_block());
+        sa.scratch = dalloc<double>(5 * (size_t)cfg.nspecies * nx);
+        sa.coll = dalloc<double>((size_t)sa.nch * nx);
+        sa.coll_phase = dalloc<double>(sa.P * (size_t)sa.nch * nx);
+        if (a.eedf_species >= 0) {
+            const size_t R = (size_t)a.eedf_regions;
+            sa.eedf_cnt = dalloc<unsigned long long>(sa.P * R * 2);
+            sa.eedf_sum = dalloc<double>(sa.P * R * 7);
+            sa.eedf_hist = dalloc<double>(sa.P * R * a.eedf_bins);
+            sa.hist_shared = (5 * nx + R * a.eedf_bins) * sizeof(double) <= kMomentSmemMax;
+        }
+        sa.psamples.assign(sa.P, 0);
+        sa.pcoll.assign(sa.P, 0);
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        sa.on = true;
+        drop_graphs();
+    }
+
+    // begin_spatial_collision_step, src/Simulation.cpp:1214-1236: arms the
+    // collision-energy deposit of the pass that applies collision step `cs`.
+    void arm_collision_step(uint64_t cs) {
+        p.coll_acc = nullptr;
+        p.coll_phase_acc = nullptr;
+        const auto& a = sa.cfg;
+        if (!sa.on || sa.nch == 0 || cs < a.start_step || cs > a.end_step) return;
+        p.coll_acc = sa.coll;
+        ++sa.coll_steps;
+        if (sa.P) {
+            const size_t bin = (size_t)((cs - a.start_step) % sa.spc) * sa.P / sa.spc;
+            p.coll_phase_acc = sa.coll_phase + bin * (size_t)sa.nch * cfg.nx;
+            ++sa.pcoll[bin];
+        }
+    }
+    void disarm() {
+        p.coll_acc = nullptr;
+        p.coll_phase_acc = nullptr;
+    }
+
+    bool sample_step(uint64_t k) const {
+        const auto& a = sa.cfg;
+        return sa.on && k >= a.start_step && k <= a.end_step && (k - a.start_step) % a.interval == 0;
+    }
+
+    // accumulate_spatial_average (src/Simulation.cpp:1287-1370) after step k:
+    // the pending collision part is applied first (one pass that writes the
+    // time-centred v), then the moments, the fields and the phase EEDF.
+    void take_sample(uint64_t k) {
+        if (pending) {
+            arm_collision_step(step);
+            launch_pass(kModeSyncMcc | kModeWriteV, 0);
+            disarm();
+            pending = false;
+        }
+        const auto& a = sa.cfg;
+        size_t bin = sa.P;
+        if (sa.P) {
+            const size_t per_cycle = sa.spc / a.interval;
+            bin = (size_t)((k - a.start_step) / a.interval) % per_cycle * sa.P / per_cycle;
+        }
+        MomentArgs m{};
+        m.scratch = sa.scratch;
+        m.eedf_species = (bin < sa.P && a.eedf_species >= 0) ? a.eedf_species : -1;
+        size_t smem = 5 * cfg.nx * sizeof(double);
+        if (m.eedf_species >= 0) {
+            const size_t R = (size_t)a.eedf_regions;
+            m.regions = a.eedf_regions;
+            for (int r = 0; r < a.eedf_regions; ++r) { m.xmin[r] = a.eedf_x_min[r]; m.xmax[r] = a.eedf_x_max[r]; }
+            m.bins = (unsigned)a.eedf_bins;
+            m.emax = a.eedf_energy_max;
+            m.escale = cfg.units == APIC_SI ? 1.602176634e-19 : 1.0;  // include/pic/Types.hpp:9
+            m.eedf_cnt = sa.eedf_cnt + bin * R * 2;
+            m.eedf_sum = sa.eedf_sum + bin * R * 7;
+            m.eedf_hist = sa.eedf_hist + bin * R * a.eedf_bins;
+            m.hist_shared = sa.hist_shared ? 1 : 0;
+            if (sa.hist_shared) smem += R * a.eedf_bins * sizeof(double);
+        }
+        const Params1D q = pass_params(0);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const bool dir = cfg.boundary == APIC_DIRICHLET;
+        const int form = (cfg.velocity_dimensions == 3 ? 4 : 0) | (dir ? 2 : 0) | (fp32 ? 1 : 0);
+        switch (form) {
+            case 0: k_moments1d<1, false, false><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 1: k_moments1d<1, false, true><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 2: k_moments1d<1, true, false><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 3: k_moments1d<1, true, true><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 4: k_moments1d<3, false, false><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 5: k_moments1d<3, false, true><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            case 6: k_moments1d<3, true, false><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+            default: k_moments1d<3, true, true><<<sms, kMomThreads, smem, stream>>>(q, m); break;
+        }
+        APIC_CUDA(cudaGetLastError());
+        double* bin_blk = bin < sa.P ? sa.phase + bin * sa_block() : nullptr;
+        const unsigned fold_blocks = (unsigned)std::min<size_t>((sa_block() + 255) / 256, 1024);
+        k_sa_fold1d<<<fold_blocks, 256, 0, stream>>>(q, sa.scratch, sa.tot, bin_blk);
+        APIC_CUDA(cudaGetLastError());
+        if (bin_blk) ++sa.psamples[bin];
+        ++sa.samples;
     }
 
     // graphs of two steady steps (collision part pending), one per buffer parity
@@ -1314,9 +1714,14 @@ struct Sim1D {
     template <int VDIM, bool DIR, bool F32>
     static void set_attributes() {
         const int smem = kMaxNx1D * 16;
-        APIC_CUDA(cudaFuncSetAttribute(k_pass1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        APIC_CUDA(cudaFuncSetAttribute(k_pass1d<VDIM, DIR, F32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem));
+        APIC_CUDA(cudaFuncSetAttribute(k_pass1d<VDIM, DIR, F32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem));
         const int psm = (int)post_smem_bytes(DIR ? kMaxNx1D : kMaxNx1DPeriodic, DIR);
         APIC_CUDA(cudaFuncSetAttribute(k_post1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
+        APIC_CUDA(cudaFuncSetAttribute(k_moments1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kMomentSmemMax));
     }
 
     // The post kernel takes a whole SM's registers (one 512-thread CTA), so
@@ -1327,7 +1732,10 @@ struct Sim1D {
 
     template <int VDIM, bool DIR, bool F32>
     void launch_kernels(const Params1D& q, int blocks, size_t smem, size_t post_smem, unsigned post, EvPair& ev) {
-        k_pass1d<VDIM, DIR, F32><<<blocks, kThreads, smem, stream>>>(q);
+        if (q.coll_acc)
+            k_pass1d<VDIM, DIR, F32, true><<<blocks, kThreads, smem, stream>>>(q);
+        else
+            k_pass1d<VDIM, DIR, F32, false><<<blocks, kThreads, smem, stream>>>(q);
         if (timing) cudaEventRecord(ev.b, stream);
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(1);
@@ -1513,10 +1921,13 @@ struct Sim1D {
         require(initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
         for (size_t i = 0; i < nsteps; ++i) {
             const unsigned mode = (pending ? kModeSyncMcc : 0u) | kModeKickDrift | kModeDeposit;
+            if (pending) arm_collision_step(step);
             launch_pass(mode, kPostSolve | kPostAdvance | kPostPushBirths);
+            disarm();
             pending = true;
             time += cfg.dt;
             ++step;
+            if (sample_step(step)) take_sample(step);
         }
     }
 
@@ -1525,7 +1936,9 @@ struct Sim1D {
     void finish() {
         if (!initialized) return;
         if (pending) {
+            arm_collision_step(step);
             launch_pass(kModeSyncMcc | kModeWriteV, 0);
+            disarm();
             pending = false;
         }
     }
@@ -1731,7 +2144,7 @@ int apic_sim1d_step_group(apic_sim1d* const* sims, size_t n, size_t nsteps) {
             const int rc = guarded(sims[i], [&] {
                 apic::Sim1D& S = sims[i]->impl;
                 apic::require(S.initialized, "initialize() or resume() must precede step()", APIC_ERR_STATE);
-                if (S.timing) S.do_steps(2); else S.steady_pair();
+                if (S.timing || S.sa.on) S.do_steps(2); else S.steady_pair();
             });
             if (rc != APIC_OK) return rc;
             left[i] -= 2;
@@ -1852,6 +2265,90 @@ int apic_sim1d_kernel_times(apic_sim1d* sim, double* pass_ms, double* post_ms, u
 
 double apic_sim1d_time(const apic_sim1d* sim) { return sim ? sim->impl.time : 0.0; }
 uint64_t apic_sim1d_step_count(const apic_sim1d* sim) { return sim ? sim->impl.step : 0; }
+
+int apic_spatial_average1d_validate(const apic_config1d* cfg, const apic_spatial_average1d* sa) {
+    if (!cfg || !sa) return APIC_ERR_INVALID;
+    return guarded(nullptr, [&] { apic::validate_spatial_average(*cfg, *sa); });
+}
+int apic_sim1d_enable_spatial_average(apic_sim1d* sim, const apic_spatial_average1d* sa) {
+    if (!sim || !sa) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.enable_spatial_average(*sa); });
+}
+int apic_sim1d_spatial_average_counts(apic_sim1d* sim, uint64_t* samples, uint64_t* collision_steps,
+                                      uint64_t* phase_samples, uint64_t* collision_phase_steps) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        auto& S = sim->impl;
+        apic::require(S.sa.on, "spatial averaging is not enabled", APIC_ERR_STATE);
+        S.finish();
+        S.sync_status();
+        if (samples) *samples = S.sa.samples;
+        if (collision_steps) *collision_steps = S.sa.coll_steps;
+        for (size_t b = 0; b < S.sa.P; ++b) {
+            if (phase_samples) phase_samples[b] = S.sa.psamples[b];
+            if (collision_phase_steps) collision_phase_steps[b] = S.sa.pcoll[b];
+        }
+    });
+}
+int apic_sim1d_spatial_sums(apic_sim1d* sim, int quantity, int index, int phase, double* out) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        auto& S = sim->impl;
+        apic::require(S.sa.on, "spatial averaging is not enabled", APIC_ERR_STATE);
+        apic::require(phase >= -1 && (phase < 0 || (size_t)phase < S.sa.P), "phase bin out of range");
+        const size_t nx = S.cfg.nx, ns = (size_t)S.cfg.nspecies;
+        const double* src = nullptr;
+        if (quantity == APIC_SA_COLLISION_ENERGY) {
+            apic::require(index >= 0 && index < S.sa.nch, "collision channel out of range");
+            src = phase < 0 ? S.sa.coll + (size_t)index * nx
+                            : S.sa.coll_phase + ((size_t)phase * (size_t)S.sa.nch + (size_t)index) * nx;
+        } else {
+            const double* blk = phase < 0 ? S.sa.tot : S.sa.phase + (size_t)phase * S.sa_block();
+            if (quantity >= APIC_SA_DENSITY && quantity <= APIC_SA_KINETIC_ENERGY) {
+                apic::require(index >= 0 && (size_t)index < ns, "species index out of range");
+                src = blk + ((size_t)quantity * ns + (size_t)index) * nx;
+            } else if (quantity >= APIC_SA_POTENTIAL && quantity <= APIC_SA_ELECTRIC_SQUARED) {
+                src = blk + 5 * ns * nx + (size_t)(quantity - APIC_SA_POTENTIAL) * nx;
+            } else {
+                throw Error(APIC_ERR_INVALID, "unknown spatial-average quantity");
+            }
+        }
+        S.finish();
+        S.sync_status();
+        APIC_CUDA(cudaMemcpyAsync(out, src, nx * sizeof(double), cudaMemcpyDeviceToHost, S.stream));
+        APIC_CUDA(cudaStreamSynchronize(S.stream));
+    });
+}
+int apic_sim1d_phase_eedf(apic_sim1d* sim, int phase, int region, apic_phase_eedf1d* out, double* histogram) {
+    if (!sim || !out) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        auto& S = sim->impl;
+        const auto& a = S.sa.cfg;
+        apic::require(S.sa.on && a.eedf_species >= 0, "phase EEDF is not enabled", APIC_ERR_STATE);
+        apic::require(phase >= 0 && (size_t)phase < S.sa.P && region >= 0 && region < a.eedf_regions,
+                      "phase bin or region out of range");
+        S.finish();
+        S.sync_status();
+        const size_t at = (size_t)phase * (size_t)a.eedf_regions + (size_t)region;
+        unsigned long long cnt[2];
+        double sums[7];
+        APIC_CUDA(cudaMemcpyAsync(cnt, S.sa.eedf_cnt + at * 2, sizeof cnt, cudaMemcpyDeviceToHost, S.stream));
+        APIC_CUDA(cudaMemcpyAsync(sums, S.sa.eedf_sum + at * 7, sizeof sums, cudaMemcpyDeviceToHost, S.stream));
+        if (histogram)
+            APIC_CUDA(cudaMemcpyAsync(histogram, S.sa.eedf_hist + at * a.eedf_bins, a.eedf_bins * sizeof(double),
+                                      cudaMemcpyDeviceToHost, S.stream));
+        APIC_CUDA(cudaStreamSynchronize(S.stream));
+        out->macro_observations = cnt[0];
+        out->overflow_macro_observations = cnt[1];
+        out->represented_observations = sums[0];
+        out->overflow_represented_observations = sums[1];
+        out->weighted_energy_sum = sums[2];
+        out->weighted_energy_squared_sum = sums[3];
+        out->weighted_velocity_x_sum = sums[4];
+        out->weighted_velocity_y_sum = sums[5];
+        out->weighted_velocity_z_sum = sums[6];
+    });
+}
 
 int apic_deposit_solve_gather_1d(int boundary, size_t nx, double length, double permittivity, double phi_left,
                                  double phi_right, int nspecies, const double* charge, const double* weight,

@@ -253,6 +253,66 @@ APIC_EXPORT int apic_sim1d_model_safe_speed(const apic_sim1d* sim, int model, do
 APIC_EXPORT int apic_sim1d_kernel_times(apic_sim1d* sim, double* pass_ms, double* post_ms, uint64_t* passes);
 APIC_EXPORT uint64_t apic_sim1d_step_count(const apic_sim1d* sim);
 
+/* ---- 1D CCP campaign diagnostics ------------------------------------------ */
+
+#define APIC_MAX_EEDF_REGIONS 8
+
+/* SpatialAverage1DConfig + PhaseEedf1DConfig (include/pic/Config.hpp:145-168)
+ * of an enabled spatial average: the EEDF species by index (-1: no phase
+ * EEDF) and its regions by their bounds. */
+typedef struct {
+    size_t interval, start_step, end_step;
+    double rf_frequency;
+    size_t rf_cycles, phase_bins;
+    int eedf_species;
+    size_t eedf_bins;
+    double eedf_energy_max;
+    int eedf_regions;
+    double eedf_x_min[APIC_MAX_EEDF_REGIONS], eedf_x_max[APIC_MAX_EEDF_REGIONS];
+} apic_spatial_average1d;
+
+/* PhaseEedfAccumulator1D without its histogram, include/pic/Simulation.hpp:43-54 */
+typedef struct {
+    uint64_t macro_observations, overflow_macro_observations;
+    double represented_observations, overflow_represented_observations;
+    double weighted_energy_sum, weighted_energy_squared_sum;
+    double weighted_velocity_x_sum, weighted_velocity_y_sum, weighted_velocity_z_sum;
+} apic_phase_eedf1d;
+
+/* Quantities of apic_sim1d_spatial_sums: per-node sums over the samples of the
+ * represented density, the velocity-weighted densities, the kinetic-energy
+ * density (index = species), the potential, the field and its square (index
+ * unused), and the spatial collision-energy density (index = channel, numbered
+ * across the models in model order). */
+enum {
+    APIC_SA_DENSITY = 0, APIC_SA_VELOCITY_X = 1, APIC_SA_VELOCITY_Y = 2, APIC_SA_VELOCITY_Z = 3,
+    APIC_SA_KINETIC_ENERGY = 4, APIC_SA_POTENTIAL = 5, APIC_SA_ELECTRIC = 6, APIC_SA_ELECTRIC_SQUARED = 7,
+    APIC_SA_COLLISION_ENERGY = 8
+};
+
+/* validate_spatial_average_1d (src/Config.cpp:1377-1524) against a 1D
+ * configuration, with the reference's messages.  Host only: needs no device. */
+APIC_EXPORT int apic_spatial_average1d_validate(const apic_config1d* cfg, const apic_spatial_average1d* sa);
+/* Enables the spatial average, phase bins, spatial collision energy and phase
+ * EEDF of Simulation (accumulate_spatial_average, begin_spatial_collision_step,
+ * deposit_spatial_collision_energy, accumulate_phase_eedf,
+ * src/Simulation.cpp:1163-1370).  Before initialize()/resume(); sums start at
+ * zero.  Sample steps cost one extra particle pass (the collision part of the
+ * step is applied before the moments are taken). */
+APIC_EXPORT int apic_sim1d_enable_spatial_average(apic_sim1d* sim, const apic_spatial_average1d* sa);
+/* spatial_average_samples, spatial_collision_steps and, per phase bin (arrays
+ * of phase_bins entries, may be NULL), the bin samples and collision steps
+ * (include/pic/Simulation.hpp:31-41, :94-100) */
+APIC_EXPORT int apic_sim1d_spatial_average_counts(apic_sim1d* sim, uint64_t* samples, uint64_t* collision_steps,
+                                                  uint64_t* phase_samples, uint64_t* collision_phase_steps);
+/* nx sums of one quantity; phase -1: the whole window, else that phase bin
+ * (include/pic/Simulation.hpp:86-93, the spatial sums of src/Simulation.cpp:543-580) */
+APIC_EXPORT int apic_sim1d_spatial_sums(apic_sim1d* sim, int quantity, int index, int phase, double* out);
+/* phase_eedf_accumulators()[phase][region], include/pic/Simulation.hpp:101-104;
+ * histogram: eedf_bins entries (may be NULL) */
+APIC_EXPORT int apic_sim1d_phase_eedf(apic_sim1d* sim, int phase, int region, apic_phase_eedf1d* out,
+                                      double* histogram);
+
 /* ---- stateless kernels (host buffers in, host buffers out) --------------- */
 
 /* Species::deposit_charge(Grid&) summed over species + FieldSolver::solve(Grid&,

@@ -545,6 +545,24 @@ struct ora_sim1d {
     uint64_t candidates, nulls, per_channel[ORA_MAX_MODELS][ORA_MAX_CHANNELS];
     ora_product* staged;
     size_t nstaged, staged_cap;
+    struct {
+        int on;
+        ora_spatial_average1d cfg;
+        size_t spc;              /* RF steps per cycle (0: no RF contract) */
+        size_t P;                /* phase bins */
+        int nch, off[ORA_MAX_MODELS];
+        double* tot;             /* [5 moments][species][nx] + [3 fields][nx] */
+        double* phase;           /* [P][same block] */
+        double* scratch;         /* [5][nx], one species of one sample */
+        double* coll;            /* [nch][nx] */
+        double* coll_phase;      /* [P][nch][nx] */
+        uint64_t samples, coll_steps, *psamples, *pcoll;
+        int coll_active;
+        size_t coll_phase_id;
+        uint64_t* eedf_cnt;      /* [P][R][2] */
+        double* eedf_sum;        /* [P][R][7] */
+        double* eedf_hist;       /* [P][R][bins] */
+    } diag;
 };
 
 static void store_reserve(ora_store* s, size_t cap) {
@@ -596,6 +614,9 @@ void ora_sim1d_destroy(ora_sim1d* s) {
         free(s->sp[i].vy); free(s->sp[i].vz); free(s->sp[i].alive);
     }
     free(s->rho); free(s->phi); free(s->E); free(s->staged);
+    free(s->diag.tot); free(s->diag.phase); free(s->diag.scratch); free(s->diag.coll);
+    free(s->diag.coll_phase); free(s->diag.psamples); free(s->diag.pcoll);
+    free(s->diag.eedf_cnt); free(s->diag.eedf_sum); free(s->diag.eedf_hist);
     free(s);
 }
 
@@ -680,6 +701,244 @@ static int stage_product(ora_sim1d* s, int species, double x, const double v[3])
     return 0;
 }
 
+/* ---- CCP campaign diagnostics, src/Simulation.cpp:1163-1370 ------------- */
+
+static size_t diag_block(const ora_sim1d* s) { return (5 * (size_t)s->cfg.nspecies + 3) * s->cfg.nx; }
+
+int ora_sim1d_enable_spatial_average(ora_sim1d* s, const ora_spatial_average1d* cfg) {
+    const size_t nx = s->cfg.nx;
+    s->diag.on = 1;
+    s->diag.cfg = *cfg;
+    s->diag.spc = cfg->rf_frequency > 0.0 ? (size_t)llround(1.0 / (cfg->rf_frequency * s->cfg.dt)) : 0;
+    s->diag.P = cfg->phase_bins;
+    s->diag.nch = 0;
+    for (int m = 0; m < s->cfg.nmodels; ++m) {
+        s->diag.off[m] = s->diag.nch;
+        s->diag.nch += s->cfg.models[m].nch;
+    }
+    const size_t P = s->diag.P, nch = (size_t)s->diag.nch;
+    s->diag.tot = calloc(diag_block(s), sizeof(double));
+    s->diag.phase = calloc(P * diag_block(s) + 1, sizeof(double));
+    s->diag.scratch = calloc(5 * nx, sizeof(double));
+    s->diag.coll = calloc(nch * nx + 1, sizeof(double));
+    s->diag.coll_phase = calloc(P * nch * nx + 1, sizeof(double));
+    s->diag.psamples = calloc(P + 1, sizeof(uint64_t));
+    s->diag.pcoll = calloc(P + 1, sizeof(uint64_t));
+    if (cfg->eedf_species >= 0) {
+        const size_t R = (size_t)cfg->eedf_regions;
+        s->diag.eedf_cnt = calloc(P * R * 2 + 1, sizeof(uint64_t));
+        s->diag.eedf_sum = calloc(P * R * 7 + 1, sizeof(double));
+        s->diag.eedf_hist = calloc(P * R * cfg->eedf_bins + 1, sizeof(double));
+    }
+    return 0;
+}
+
+/* begin_spatial_collision_step, src/Simulation.cpp:1214-1236 */
+static void diag_begin_collision_step(ora_sim1d* s) {
+    const ora_spatial_average1d* a = &s->diag.cfg;
+    const uint64_t cs = s->step + 1;
+    s->diag.coll_active = 0;
+    s->diag.coll_phase_id = s->diag.P;
+    if (!s->diag.on || s->diag.nch == 0 || cs < a->start_step || cs > a->end_step) return;
+    s->diag.coll_active = 1;
+    ++s->diag.coll_steps;
+    if (s->diag.P) {
+        const size_t in_cycle = (size_t)(cs - a->start_step) % s->diag.spc;
+        s->diag.coll_phase_id = in_cycle * s->diag.P / s->diag.spc;
+        ++s->diag.pcoll[s->diag.coll_phase_id];
+    }
+}
+
+/* The two-node CIC stencil of the diagnostics deposits (periodic wrap, or the
+ * clamped Dirichlet form with the half-cell wall volumes),
+ * src/Simulation.cpp:1193-1211, src/Species.cpp:314-334 */
+static void diag_stencil(const ora_sim1d* s, double x, size_t node[2], double shape[2], double vol[2]) {
+    const ora_config1d* c = &s->cfg;
+    const double dx = s->dx;
+    if (!c->dirichlet) {
+        const double coordinate = wrap(x, c->length) / dx;
+        const size_t cell = (size_t)floor(coordinate);
+        const double f = coordinate - (double)cell;
+        node[0] = cell % c->nx; node[1] = (cell + 1) % c->nx;
+        shape[0] = 1.0 - f; shape[1] = f;
+        vol[0] = vol[1] = dx;
+    } else {
+        const double bounded = x < 0.0 ? 0.0 : (c->length < x ? c->length : x);
+        const double coordinate = bounded / dx;
+        double fl = floor(coordinate);
+        if ((double)(c->nx - 2) < fl) fl = (double)(c->nx - 2);
+        const size_t cell = (size_t)fl;
+        const double f = coordinate - (double)cell;
+        node[0] = cell; node[1] = cell + 1;
+        shape[0] = 1.0 - f; shape[1] = f;
+        vol[0] = node_volume(cell, c->nx, dx, 1);
+        vol[1] = node_volume(cell + 1, c->nx, dx, 1);
+    }
+}
+
+/* deposit_spatial_collision_energy, src/Simulation.cpp:1171-1212 */
+static void diag_collision_energy(ora_sim1d* s, double x, int channel, double e) {
+    if (!s->diag.coll_active) return;
+    size_t node[2];
+    double shape[2], vol[2];
+    diag_stencil(s, x, node, shape, vol);
+    const size_t nx = s->cfg.nx;
+    for (int k = 0; k < 2; ++k) {
+        const double density = e * shape[k] / vol[k];
+        s->diag.coll[(size_t)channel * nx + node[k]] += density;
+        if (s->diag.coll_phase_id < s->diag.P)
+            s->diag.coll_phase[(s->diag.coll_phase_id * (size_t)s->diag.nch + (size_t)channel) * nx + node[k]] +=
+                density;
+    }
+}
+
+/* The stored transverse velocity as the device's moment pass reads it (mode 2:
+ * rounded to float, as stored after the collision part). */
+static double diag_comp(const ora_sim1d* s, double v) { return s->mode == 2 ? f32_round(v) : v; }
+
+/* accumulate_phase_eedf, src/Simulation.cpp:1238-1285 */
+static void diag_eedf(ora_sim1d* s, size_t phase) {
+    const ora_spatial_average1d* a = &s->diag.cfg;
+    const int sid = a->eedf_species;
+    const ora_store* st = &s->sp[sid];
+    const double scale = s->cfg.si ? 1.602176634e-19 : 1.0; /* include/pic/Types.hpp:9 */
+    const double weight = s->cfg.species[sid].weight, mass = s->cfg.species[sid].mass;
+    const size_t R = (size_t)a->eedf_regions;
+    for (size_t i = 0; i < st->n; ++i) {
+        if (!st->alive[i]) continue;
+        const double vy = diag_comp(s, st->vy[i]), vz = diag_comp(s, st->vz[i]);
+        const double vsq = st->v[i] * st->v[i] + (s->cfg.vdim == 3 ? vy * vy + vz * vz : 0.0);
+        const double energy = 0.5 * mass * vsq / scale;
+        for (size_t r = 0; r < R; ++r) {
+            if (st->x[i] < a->eedf_x_min[r] || st->x[i] > a->eedf_x_max[r]) continue;
+            uint64_t* cnt = s->diag.eedf_cnt + (phase * R + r) * 2;
+            double* sum = s->diag.eedf_sum + (phase * R + r) * 7;
+            ++cnt[0];
+            sum[0] += weight;
+            sum[2] += weight * energy;
+            sum[3] += weight * energy * energy;
+            sum[4] += weight * st->v[i];
+            sum[5] += weight * (s->cfg.vdim == 3 ? vy : st->vy[i]);
+            sum[6] += weight * (s->cfg.vdim == 3 ? vz : st->vz[i]);
+            if (energy >= a->eedf_energy_max) {
+                ++cnt[1];
+                sum[1] += weight;
+            } else {
+                size_t bin = (size_t)(energy / a->eedf_energy_max * (double)a->eedf_bins);
+                if (bin > a->eedf_bins - 1) bin = a->eedf_bins - 1;
+                s->diag.eedf_hist[(phase * R + r) * a->eedf_bins + bin] += weight;
+            }
+        }
+    }
+}
+
+/* accumulate_spatial_average, src/Simulation.cpp:1287-1370, with
+ * Species::deposit_velocity_moments, src/Species.cpp:285-336 */
+static void diag_accumulate(ora_sim1d* s) {
+    const ora_spatial_average1d* a = &s->diag.cfg;
+    const uint64_t k = s->step;
+    if (!s->diag.on || k < a->start_step || k > a->end_step || (k - a->start_step) % a->interval != 0) return;
+    const size_t nx = s->cfg.nx, ns = (size_t)s->cfg.nspecies, P = s->diag.P;
+    size_t phase = P;
+    if (P) {
+        const size_t per_cycle = s->diag.spc / a->interval;
+        const size_t in_cycle = (size_t)((k - a->start_step) / a->interval) % per_cycle;
+        phase = in_cycle * P / per_cycle;
+    }
+    if (s->mode == 2) ora_sim1d_round_fp32(s); /* the device stores its state here */
+    double* bin = phase < P ? s->diag.phase + phase * diag_block(s) : NULL;
+    for (size_t sid = 0; sid < ns; ++sid) {
+        const ora_store* st = &s->sp[sid];
+        const double weight = s->cfg.species[sid].weight, mass = s->cfg.species[sid].mass;
+        double* sc = s->diag.scratch;
+        memset(sc, 0, 5 * nx * sizeof(double));
+        for (size_t i = 0; i < st->n; ++i) {
+            if (!st->alive[i]) continue;
+            const double v = st->v[i];
+            const double vy = s->cfg.vdim == 3 ? diag_comp(s, st->vy[i]) : 0.0;
+            const double vz = s->cfg.vdim == 3 ? diag_comp(s, st->vz[i]) : 0.0;
+            const double pe = 0.5 * mass * weight * (v * v + vy * vy + vz * vz);
+            size_t node[2];
+            double shape[2], vol[2];
+            diag_stencil(s, st->x[i], node, shape, vol);
+            for (int q = 0; q < 2; ++q) {
+                const double rd = weight * shape[q] / vol[q];
+                sc[0 * nx + node[q]] += rd;
+                sc[1 * nx + node[q]] += rd * v;
+                sc[2 * nx + node[q]] += rd * vy;
+                sc[3 * nx + node[q]] += rd * vz;
+                sc[4 * nx + node[q]] += pe * shape[q] / vol[q];
+            }
+        }
+        for (size_t m = 0; m < 5; ++m)
+            for (size_t i = 0; i < nx; ++i) {
+                s->diag.tot[(m * ns + sid) * nx + i] += sc[m * nx + i];
+                if (bin) bin[(m * ns + sid) * nx + i] += sc[m * nx + i];
+            }
+    }
+    double* f = s->diag.tot + 5 * ns * nx;
+    for (size_t i = 0; i < nx; ++i) {
+        f[i] += s->phi[i];
+        f[nx + i] += s->E[i];
+        f[2 * nx + i] += s->E[i] * s->E[i];
+        if (bin) {
+            double* g = bin + 5 * ns * nx;
+            g[i] += s->phi[i];
+            g[nx + i] += s->E[i];
+            g[2 * nx + i] += s->E[i] * s->E[i];
+        }
+    }
+    if (bin) ++s->diag.psamples[phase];
+    if (phase < P && a->eedf_species >= 0) diag_eedf(s, phase);
+    ++s->diag.samples;
+}
+
+void ora_sim1d_spatial_counts(const ora_sim1d* s, uint64_t* samples, uint64_t* collision_steps,
+                              uint64_t* phase_samples, uint64_t* collision_phase_steps) {
+    if (samples) *samples = s->diag.samples;
+    if (collision_steps) *collision_steps = s->diag.coll_steps;
+    for (size_t p = 0; p < s->diag.P; ++p) {
+        if (phase_samples) phase_samples[p] = s->diag.psamples[p];
+        if (collision_phase_steps) collision_phase_steps[p] = s->diag.pcoll[p];
+    }
+}
+
+int ora_sim1d_spatial_sums(const ora_sim1d* s, int quantity, int index, int phase, double* out) {
+    const size_t nx = s->cfg.nx, ns = (size_t)s->cfg.nspecies;
+    if (!s->diag.on || phase < -1 || (phase >= 0 && (size_t)phase >= s->diag.P)) return seterr(1, "bad phase");
+    const double* src;
+    if (quantity == 8) {
+        if (index < 0 || index >= s->diag.nch) return seterr(1, "bad channel");
+        src = phase < 0 ? s->diag.coll + (size_t)index * nx
+                        : s->diag.coll_phase + ((size_t)phase * (size_t)s->diag.nch + (size_t)index) * nx;
+    } else {
+        const double* blk = phase < 0 ? s->diag.tot : s->diag.phase + (size_t)phase * diag_block(s);
+        if (quantity >= 0 && quantity < 5) {
+            if (index < 0 || (size_t)index >= ns) return seterr(1, "bad species");
+            src = blk + ((size_t)quantity * ns + (size_t)index) * nx;
+        } else if (quantity >= 5 && quantity < 8) {
+            src = blk + 5 * ns * nx + (size_t)(quantity - 5) * nx;
+        } else {
+            return seterr(1, "bad quantity");
+        }
+    }
+    memcpy(out, src, nx * sizeof(double));
+    return 0;
+}
+
+int ora_sim1d_phase_eedf(const ora_sim1d* s, int phase, int region, uint64_t* counts, double* sums,
+                         double* histogram) {
+    const ora_spatial_average1d* a = &s->diag.cfg;
+    if (!s->diag.on || a->eedf_species < 0 || phase < 0 || (size_t)phase >= s->diag.P || region < 0 ||
+        region >= a->eedf_regions)
+        return seterr(1, "bad phase or region");
+    const size_t at = (size_t)phase * (size_t)a->eedf_regions + (size_t)region;
+    if (counts) memcpy(counts, s->diag.eedf_cnt + at * 2, 2 * sizeof(uint64_t));
+    if (sums) memcpy(sums, s->diag.eedf_sum + at * 7, 7 * sizeof(double));
+    if (histogram) memcpy(histogram, s->diag.eedf_hist + at * a->eedf_bins, a->eedf_bins * sizeof(double));
+    return 0;
+}
+
 /* initialize_leapfrog_half_step, src/Pusher.cpp:66-68 */
 static double init_half(double v, double E, double qm, double dt) { return v - 0.5 * qm * E * dt; }
 
@@ -721,6 +980,25 @@ static int apply_collisions(ora_sim1d* s) {
                 stage_product(s, ch->ion_species, st->x[i], cs.secondary_ion_velocity[k]);
             }
             if (cs.removed) return seterr(8, "1D MCC produced an unsupported primary removal event");
+            if (s->diag.coll_active) {
+                /* tracked_energy_change: the weighted projectile change, plus each
+                 * product pair's energy in its channel, src/Simulation.cpp:862-923 */
+                double tracked[ORA_MAX_CHANNELS];
+                const double w = c->species[sid].weight;
+                for (int ch = 0; ch < c->models[m].nch; ++ch) tracked[ch] = cs.energy_change[ch] * w;
+                for (int k = 0; k < cs.nsecondaries && k < 16; ++k) {
+                    const ora_channel* chp = &c->models[m].ch[cs.secondary_channel[k]];
+                    const ora_species* A = &c->species[chp->secondary_species];
+                    const ora_species* B = &c->species[chp->ion_species];
+                    const double* vs = cs.secondary_velocity[k];
+                    const double* vi = cs.secondary_ion_velocity[k];
+                    tracked[cs.secondary_channel[k]] +=
+                        0.5 * A->mass * A->weight * (vs[0] * vs[0] + vs[1] * vs[1] + vs[2] * vs[2]) +
+                        0.5 * B->mass * B->weight * (vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]);
+                }
+                for (int ch = 0; ch < c->models[m].nch; ++ch)
+                    if (tracked[ch] != 0.0) diag_collision_energy(s, st->x[i], s->diag.off[m] + ch, tracked[ch]);
+            }
             st->vh[i] = init_half(st->v[i], gather(s, st->x[i]), qm, c->dt);
         }
     }
@@ -801,10 +1079,12 @@ static int step_once(ora_sim1d* s) {
             st->v[i] = st->vh[i] + 0.5 * qm * gather(s, st->x[i]) * c->dt;
         }
     }
+    diag_begin_collision_step(s);
     const int rc = apply_collisions(s);
     if (rc) return rc;
     ++s->step;
     s->time += c->dt;
+    diag_accumulate(s);
     return 0;
 }
 

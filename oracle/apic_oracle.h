@@ -90,6 +90,21 @@ void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t*
                       double* eleft, double* eright);
 double ora_sim1d_kinetic(const ora_sim1d* s, int species);
 double ora_sim1d_field_energy(const ora_sim1d* s);
+/* CCP campaign diagnostics (src/Simulation.cpp:1163-1370): spatial averages,
+ * phase bins, spatial collision energy and the phase EEDF.  Enable before
+ * initialize; the configuration is assumed valid (the device validates it).
+ * quantity: 0 density, 1-3 velocity x/y/z density, 4 kinetic-energy density
+ * (index = species), 5 potential, 6 electric, 7 electric squared (index
+ * ignored), 8 collision-energy density (index = global channel); phase -1 =
+ * the whole window. */
+int ora_sim1d_enable_spatial_average(ora_sim1d* s, const ora_spatial_average1d* cfg);
+void ora_sim1d_spatial_counts(const ora_sim1d* s, uint64_t* samples, uint64_t* collision_steps,
+                              uint64_t* phase_samples, uint64_t* collision_phase_steps);
+int ora_sim1d_spatial_sums(const ora_sim1d* s, int quantity, int index, int phase, double* out);
+/* counts: macro, overflow macro; sums: represented, overflow represented,
+ * weighted energy, weighted energy^2, weighted v_x, v_y, v_z */
+int ora_sim1d_phase_eedf(const ora_sim1d* s, int phase, int region, uint64_t* counts, double* sums,
+                         double* histogram);
 const char* ora_last_error(void);
 
 /* ---- structured 2D3V / 3D3V periodic -------------------------------------- */

@@ -70,6 +70,20 @@ typedef struct {
     ora_mcc_model models[ORA_MAX_MODELS];
 } ora_config1d;
 
+/* SpatialAverage1DConfig + PhaseEedf1DConfig, include/pic/Config.hpp:145-168
+ * (the EEDF species by index; regions by bounds) */
+#define ORA_MAX_EEDF_REGIONS 8
+typedef struct {
+    size_t interval, start_step, end_step;
+    double rf_frequency;
+    size_t rf_cycles, phase_bins;
+    int eedf_species;            /* -1: no phase EEDF */
+    size_t eedf_bins;
+    double eedf_energy_max;
+    int eedf_regions;
+    double eedf_x_min[ORA_MAX_EEDF_REGIONS], eedf_x_max[ORA_MAX_EEDF_REGIONS];
+} ora_spatial_average1d;
+
 /* Per-call collision statistics (one particle, one timestep). */
 typedef struct {
     uint64_t candidates, null_collisions;

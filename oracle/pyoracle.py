@@ -94,6 +94,32 @@ class Rng(C.Structure):
     ]
 
 
+class SpatialAverage1D(C.Structure):
+    """ora_spatial_average1d (SpatialAverage1DConfig + PhaseEedf1DConfig)."""
+    _fields_ = [
+        ("interval", C.c_size_t), ("start_step", C.c_size_t), ("end_step", C.c_size_t),
+        ("rf_frequency", C.c_double), ("rf_cycles", C.c_size_t), ("phase_bins", C.c_size_t),
+        ("eedf_species", C.c_int), ("eedf_bins", C.c_size_t), ("eedf_energy_max", C.c_double),
+        ("eedf_regions", C.c_int), ("eedf_x_min", C.c_double * 8), ("eedf_x_max", C.c_double * 8),
+    ]
+
+
+def spatial_average1d(interval=1, start_step=1, end_step=1, rf_frequency=0.0, rf_cycles=0, phase_bins=0,
+                      eedf_species=-1, eedf_bins=0, eedf_energy_max=0.0, eedf_regions=()):
+    a = SpatialAverage1D()
+    a.interval, a.start_step, a.end_step = interval, start_step, end_step
+    a.rf_frequency, a.rf_cycles, a.phase_bins = rf_frequency, rf_cycles, phase_bins
+    a.eedf_species, a.eedf_bins, a.eedf_energy_max = eedf_species, eedf_bins, eedf_energy_max
+    a.eedf_regions = len(eedf_regions)
+    for i, (lo, hi) in enumerate(eedf_regions):
+        a.eedf_x_min[i], a.eedf_x_max[i] = lo, hi
+    return a
+
+
+# quantities of the spatial sums
+SA_DENSITY, SA_VX, SA_VY, SA_VZ, SA_KINETIC, SA_POTENTIAL, SA_ELECTRIC, SA_ELECTRIC2, SA_COLLISION = range(9)
+
+
 def ensure_built() -> None:
     """Build the C restatement (and the reference harness when the reference
     tree is present) with oracle/Makefile."""
@@ -166,6 +192,10 @@ def oracle() -> C.CDLL:
         L.ora_sim1d_field_energy.restype = C.c_double
         L.ora_sim1d_field_energy.argtypes = [C.c_void_p]
         L.ora_last_error.restype = C.c_char_p
+        L.ora_sim1d_enable_spatial_average.argtypes = [C.c_void_p, C.POINTER(SpatialAverage1D)]
+        L.ora_sim1d_spatial_counts.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, _U64P]
+        L.ora_sim1d_spatial_sums.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _DP]
+        L.ora_sim1d_phase_eedf.argtypes = [C.c_void_p, C.c_int, C.c_int, _U64P, _DP, _DP]
         L.ora_collider_init.argtypes = [C.c_void_p, C.POINTER(MccModel), C.c_double]
         L.ora_collide3.argtypes = [C.c_void_p, _DP, C.c_double, C.POINTER(Rng), C.POINTER(CollideStats)]
         _oracle = L
@@ -201,6 +231,13 @@ def ref() -> C.CDLL:
             _DP, _DP, C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
         L.ref_collide3.argtypes = [C.POINTER(MccModel), C.c_double, C.c_char_p, C.c_size_t, _DP, _U64P,
                                    C.c_double, C.POINTER(CollideStats), _U64P, C.c_size_t]
+        L.ref1d_create_diag.argtypes = [C.POINTER(Config1D), C.POINTER(SpatialAverage1D), C.c_char_p,
+                                        C.POINTER(C.c_void_p)]
+        L.ref1d_run_diag.argtypes = [C.POINTER(Config1D), C.POINTER(SpatialAverage1D), C.c_size_t, C.c_char_p]
+        L.ref1d_validate_diag.argtypes = [C.POINTER(Config1D), C.POINTER(SpatialAverage1D), C.c_char_p]
+        L.ref1d_collision_energy.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.ref1d_collision_steps.argtypes = [C.c_void_p, _U64P, _U64P]
+        L.ref1d_phase_eedf.argtypes = [C.c_void_p, C.c_int, C.c_int, _U64P, _DP, _DP]
         L.ref_mt64.argtypes = [C.c_uint64, C.c_size_t, _U64P]
         L.ref_dist.argtypes = [C.c_int, C.c_uint64, C.c_size_t, _DP]
         _ref = L
@@ -344,16 +381,47 @@ class Sim1D:
     def time(self):
         return oracle().ora_sim1d_time(self.h)
 
+    # -- CCP campaign diagnostics --
+    def enable_spatial_average(self, sa: "SpatialAverage1D"):
+        self.sa = sa
+        oracle().ora_sim1d_enable_spatial_average(self.h, C.byref(sa))
+
+    def spatial_counts(self):
+        P = max(int(self.sa.phase_bins), 1)
+        a, b = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
+        pa, pb = np.zeros(P, np.uint64), np.zeros(P, np.uint64)
+        oracle().ora_sim1d_spatial_counts(self.h, u64ptr(a), u64ptr(b), u64ptr(pa), u64ptr(pb))
+        P = int(self.sa.phase_bins)
+        return int(a[0]), int(b[0]), pa[:P], pb[:P]
+
+    def spatial_sums(self, quantity, index=0, phase=-1):
+        out = np.zeros(self.cfg.nx)
+        if oracle().ora_sim1d_spatial_sums(self.h, quantity, index, phase, dptr(out)):
+            raise RuntimeError(oracle().ora_last_error().decode())
+        return out
+
+    def phase_eedf(self, phase, region):
+        cnt, sums = np.zeros(2, np.uint64), np.zeros(7)
+        hist = np.zeros(max(int(self.sa.eedf_bins), 1))
+        if oracle().ora_sim1d_phase_eedf(self.h, phase, region, u64ptr(cnt), dptr(sums), dptr(hist)):
+            raise RuntimeError(oracle().ora_last_error().decode())
+        return cnt, sums, hist[:int(self.sa.eedf_bins)]
+
 
 class Ref1D:
     """The reference's own Simulation, driven through the harness."""
 
-    def __init__(self, cfg: Config1D, workdir: str):
+    def __init__(self, cfg: Config1D, workdir: str, spatial_average=None):
         L = ref()
         self.cfg = cfg
         self.workdir = workdir
+        self.sa = spatial_average
         h = C.c_void_p()
-        if L.ref1d_create(C.byref(cfg), workdir.encode(), C.byref(h)):
+        if spatial_average is None:
+            rc = L.ref1d_create(C.byref(cfg), workdir.encode(), C.byref(h))
+        else:
+            rc = L.ref1d_create_diag(C.byref(cfg), C.byref(spatial_average), workdir.encode(), C.byref(h))
+        if rc:
             raise RuntimeError(L.ref_last_error().decode())
         self.h = h
 
@@ -416,6 +484,41 @@ class Ref1D:
 
     def time(self):
         return ref().ref1d_time(self.h)
+
+    def collision_energy(self, channel, phase=-1):
+        out = np.zeros(self.cfg.nx)
+        ref().ref1d_collision_energy(self.h, channel, phase, dptr(out))
+        return out
+
+    def collision_steps(self):
+        a = np.zeros(1, np.uint64)
+        P = max(int(self.sa.phase_bins), 1)
+        pb = np.zeros(P, np.uint64)
+        ref().ref1d_collision_steps(self.h, u64ptr(a), u64ptr(pb))
+        return int(a[0]), pb[:int(self.sa.phase_bins)]
+
+    def phase_eedf(self, phase, region):
+        cnt, sums = np.zeros(2, np.uint64), np.zeros(7)
+        hist = np.zeros(max(int(self.sa.eedf_bins), 1))
+        self._chk(ref().ref1d_phase_eedf(self.h, phase, region, u64ptr(cnt), dptr(sums), dptr(hist)))
+        return cnt, sums, hist[:int(self.sa.eedf_bins)]
+
+
+def ref_run_spatial_average(cfg: Config1D, sa: SpatialAverage1D, steps: int, workdir: str) -> str:
+    """Simulation::run of the reference over `steps` steps; returns the folder
+    holding its spatial-average CSV files."""
+    L = ref()
+    if L.ref1d_run_diag(C.byref(cfg), C.byref(sa), steps, workdir.encode()):
+        raise RuntimeError(L.ref_last_error().decode())
+    return os.path.join(workdir, "out")
+
+
+def ref_validate_spatial_average(cfg: Config1D, sa: SpatialAverage1D, workdir: str):
+    """The reference's configuration error for `sa`, or None."""
+    L = ref()
+    if L.ref1d_validate_diag(C.byref(cfg), C.byref(sa), workdir.encode()):
+        return L.ref_last_error().decode()
+    return None
 
 
 def config_from_workload(wl, tables: TableSet, seed=12345, threads=0, particles=None, own_loading=False):

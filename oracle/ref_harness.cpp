@@ -256,6 +256,94 @@ int ref1d_rng_state(void* h, const char* path, uint64_t* out313) {
     } catch (const std::exception& e) { return fail(e); }
 }
 
+// --- CCP campaign diagnostics (src/Simulation.cpp:1163-1560) ---------------
+
+namespace {
+void apply_spatial_average(pic::Config& c, const ora_spatial_average1d& a) {
+    c.spatial_average.enabled = true;
+    c.spatial_average.interval = a.interval;
+    c.spatial_average.start_step = a.start_step;
+    c.spatial_average.end_step = a.end_step;
+    c.spatial_average.rf_frequency = a.rf_frequency;
+    c.spatial_average.rf_cycles = a.rf_cycles;
+    c.spatial_average.phase_bins = a.phase_bins;
+    c.phase_eedf.enabled = a.eedf_species >= 0;
+    if (a.eedf_species >= 0) c.phase_eedf.species = species_name(a.eedf_species);
+    c.phase_eedf.energy_bins = a.eedf_bins;
+    c.phase_eedf.energy_max = a.eedf_energy_max;
+    for (int r = 0; r < a.eedf_regions; ++r)
+        c.phase_eedf.regions.push_back({"r" + std::to_string(r), a.eedf_x_min[r], a.eedf_x_max[r]});
+}
+}  // namespace
+
+int ref1d_create_diag(const ora_config1d* cfg, const ora_spatial_average1d* sa, const char* workdir,
+                      void** out) {
+    try {
+        auto r = std::make_unique<Ref1D>();
+        pic::Config c = make_config_1d(*cfg, workdir);
+        apply_spatial_average(c, *sa);
+        r->sim = std::make_unique<pic::Simulation>(c);
+        *out = r.release();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// Simulation::run over `steps` steps; the spatial-average CSV files land in workdir/out.
+int ref1d_run_diag(const ora_config1d* cfg, const ora_spatial_average1d* sa, size_t steps,
+                   const char* workdir) {
+    try {
+        pic::Config c = make_config_1d(*cfg, workdir);
+        apply_spatial_average(c, *sa);
+        c.steps = steps;
+        c.output_interval = steps;
+        pic::Simulation sim(c);
+        sim.run();
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// spatial_collision_energy_sums (phase -1) or the phase slice; returns the channel count
+int ref1d_collision_energy(void* h, int channel, int phase, double* out) {
+    const auto& sim = *static_cast<Ref1D*>(h)->sim;
+    const auto& src = phase < 0 ? sim.spatial_collision_energy_sums()
+                                : sim.spatial_collision_phase_energy_sums().at(phase);
+    const auto& row = src.at(channel);
+    std::memcpy(out, row.data(), row.size() * sizeof(double));
+    return static_cast<int>(src.size());
+}
+
+void ref1d_collision_steps(void* h, uint64_t* steps, uint64_t* phase_steps) {
+    const auto& sim = *static_cast<Ref1D*>(h)->sim;
+    *steps = sim.spatial_collision_steps();
+    const auto& ps = sim.spatial_collision_phase_steps();
+    for (size_t i = 0; i < ps.size(); ++i) phase_steps[i] = ps[i];
+}
+
+int ref1d_phase_eedf(void* h, int phase, int region, uint64_t* counts, double* sums, double* hist) {
+    try {
+        const auto& a = static_cast<Ref1D*>(h)->sim->phase_eedf_accumulators().at(phase).at(region);
+        counts[0] = a.macro_observations;
+        counts[1] = a.overflow_macro_observations;
+        const double v[7] = {a.represented_observations, a.overflow_represented_observations,
+                             a.weighted_energy_sum, a.weighted_energy_squared_sum,
+                             a.weighted_velocity_x_sum, a.weighted_velocity_y_sum, a.weighted_velocity_z_sum};
+        std::memcpy(sums, v, sizeof v);
+        std::memcpy(hist, a.histogram.data(), a.histogram.size() * sizeof(double));
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+// Config validation of the spatial average alone (validate_spatial_average_1d,
+// src/Config.cpp:1377-1524), through the Simulation constructor.
+int ref1d_validate_diag(const ora_config1d* cfg, const ora_spatial_average1d* sa, const char* workdir) {
+    try {
+        pic::Config c = make_config_1d(*cfg, workdir);
+        apply_spatial_average(c, *sa);
+        pic::Simulation sim(c);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
 // --- kernel-level entry points --------------------------------------------
 
 // Species::deposit_charge + FieldSolver::solve + interpolate_electric on one grid.

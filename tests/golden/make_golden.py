@@ -280,12 +280,81 @@ def dirichlet_fixture():
                             pot=np.array(pot), rho=rho, phi=phi, E=E)
 
 
+CCP_DIAG_CASES = {
+    # name: steps, spatial-average settings
+    "rf": (400, dict(interval=4, start_step=1, end_step=400, rf_frequency=13.56e6, rf_cycles=1, phase_bins=4,
+                     eedf_species=0, eedf_bins=32, eedf_energy_max=50.0,
+                     eedf_regions=((0.0, 0.02), (0.02, 0.067)))),
+    "window": (40, dict(interval=5, start_step=3, end_step=37)),
+}
+
+
+def ccp_diag_deck():
+    return W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0)
+
+
+def _read_csv(path):
+    import csv
+    with open(path) as f:
+        rows = list(csv.reader(f))
+    return rows[0], rows[1:]
+
+
+def ccp_diag_fixture():
+    """Campaign diagnostics of a small RF discharge: the collision-energy and
+    phase-EEDF accumulators read through the reference's accessors after
+    initialize + step, and the spatial-average CSV files of Simulation::run
+    over the same steps (values printed with 17 significant digits)."""
+    wl = ccp_diag_deck()
+    for name, (steps, kw) in CCP_DIAG_CASES.items():
+        T = po.TableSet()
+        cfg = po.config_from_workload(wl, T, seed=2024, own_loading=True)
+        sa = po.spatial_average1d(**kw)
+        R = po.Ref1D(cfg, tempfile.mkdtemp(), spatial_average=sa)
+        R.initialize()
+        out = {"steps": steps}
+        for s in range(cfg.nspecies):
+            for k, v in R.particles(s).items():
+                out[f"init_s{s}_{k}"] = v
+        out["rng_state"] = R.rng_state()
+        R.step(steps)
+        nch = sum(cfg.models[m].nch for m in range(cfg.nmodels))
+        P = int(sa.phase_bins)
+        out["collision_energy"] = np.array([R.collision_energy(c) for c in range(nch)])
+        if P:
+            out["collision_energy_phase"] = np.array([[R.collision_energy(c, p) for c in range(nch)]
+                                                      for p in range(P)])
+        cs, ps = R.collision_steps()
+        out["collision_steps"] = cs
+        out["collision_phase_steps"] = ps
+        if sa.eedf_species >= 0:
+            cnt, sums, hist = [], [], []
+            for p in range(P):
+                for r in range(sa.eedf_regions):
+                    c, sm, h = R.phase_eedf(p, r)
+                    cnt.append(c); sums.append(sm); hist.append(h)
+            out["eedf_counts"] = np.array(cnt)
+            out["eedf_sums"] = np.array(sums)
+            out["eedf_hist"] = np.array(hist)
+        folder = po.ref_run_spatial_average(cfg, sa, steps, tempfile.mkdtemp())
+        files = ["spatial_average", "spatial_kinetic_energy", "spatial_field_average"]
+        if P:
+            files += ["spatial_phase_moments", "spatial_phase_fields"]
+        for f in files:
+            header, rows = _read_csv(os.path.join(folder, f + ".csv"))
+            numeric = [i for i, h in enumerate(header) if h != "species"]
+            out[f"csv_{f}"] = np.array([[float(r[i]) for i in numeric] for r in rows])
+            out[f"csv_{f}_header"] = np.array([header[i] for i in numeric])
+        np.savez_compressed(os.path.join(HERE, f"ccp_diag_{name}.npz"), **out)
+
+
 def main(names=None):
     if names:
         for n in names:
             globals()[f"{n}_fixture"]()
         print("golden vectors written to", HERE)
         return
+    ccp_diag_fixture()
     mixed_fixture()
     dirichlet_fixture()
     bprofile_fixture()

@@ -211,3 +211,102 @@ def test_dirichlet_sor_solve_bit_exact(name):
     pot = f["pot"] if len(n) == 2 else None
     phi, E = po.solve_dirichlet_nd(f["rho"], n, f["L"], float(f["eps"]), pot)
     assert np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
+
+
+# ---- CCP campaign diagnostics (src/Simulation.cpp:1163-1560) ----------------
+
+E_CHARGE = 1.602176634e-19
+
+
+def _ccp_diag_setup(name):
+    from golden.make_golden import CCP_DIAG_CASES, ccp_diag_deck
+    steps, kw = CCP_DIAG_CASES[name]
+    f = load(f"ccp_diag_{name}.npz")
+    wl = ccp_diag_deck()
+    T = po.TableSet()
+    cfg = po.config_from_workload(wl, T, seed=2024)
+    sim = po.Sim1D(cfg, 0)
+    sa = po.spatial_average1d(**kw)
+    sim.enable_spatial_average(sa)
+    for s in range(cfg.nspecies):
+        sim.load(s, *[f[f"init_s{s}_{k}"] for k in ("x", "v", "vh", "vy", "vz", "alive")])
+    sim.initialize_fields(0.0, 0)
+    sim.set_mt(f["rng_state"])
+    sim.step(steps)
+    return sim, sa, cfg, wl, f, T
+
+
+def _csv_tables(sim, sa, cfg, wl):
+    """write_spatial_average's derived columns (src/Simulation.cpp:1372-1560)
+    from the oracle's sums, without the node coordinate column."""
+    nx, ns = cfg.nx, cfg.nspecies
+    samples, _, psamples, _ = sim.spatial_counts()
+    dims = float(cfg.vdim)
+    dens = [sim.spatial_sums(po.SA_DENSITY, s) for s in range(ns)]
+    ke = [sim.spatial_sums(po.SA_KINETIC, s) for s in range(ns)]
+    t = {"spatial_average": [], "spatial_kinetic_energy": [], "spatial_field_average": []}
+    for s in range(ns):
+        for i in range(nx):
+            t["spatial_average"].append([s, i, dens[s][i] / float(samples)])
+            me = ke[s][i] / dens[s][i] / E_CHARGE if dens[s][i] > 0.0 else 0.0
+            t["spatial_kinetic_energy"].append([s, i, me, 2.0 * me / dims])
+    phi, E, E2 = (sim.spatial_sums(q) for q in (po.SA_POTENTIAL, po.SA_ELECTRIC, po.SA_ELECTRIC2))
+    for i in range(nx):
+        t["spatial_field_average"].append([i, phi[i] / float(samples), E[i] / float(samples),
+                                           np.sqrt(E2[i] / float(samples))])
+    P = int(sa.phase_bins)
+    if P:
+        t["spatial_phase_moments"], t["spatial_phase_fields"] = [], []
+        for p in range(P):
+            n = float(psamples[p])
+            frac = (float(p) + 0.5) / float(P)
+            for s in range(ns):
+                m = [sim.spatial_sums(q, s, p) for q in range(5)]
+                mass = wl.species[s].mass
+                for i in range(nx):
+                    d = m[0][i]
+                    ux = m[1][i] / d if d > 0.0 else 0.0
+                    uy = m[2][i] / d if d > 0.0 else 0.0
+                    uz = m[3][i] / d if d > 0.0 else 0.0
+                    me = m[4][i] / d / E_CHARGE if d > 0.0 else 0.0
+                    drift = 0.5 * mass * (ux * ux + uy * uy + uz * uz) / E_CHARGE
+                    temp = 2.0 / dims * max(0.0, me - drift)
+                    t["spatial_phase_moments"].append([p, frac, n, s, i, d / n if n > 0 else 0.0, ux, uy, uz, me,
+                                                       temp])
+            fphi, fE, fE2 = (sim.spatial_sums(q, 0, p) for q in (po.SA_POTENTIAL, po.SA_ELECTRIC, po.SA_ELECTRIC2))
+            for i in range(nx):
+                t["spatial_phase_fields"].append([p, frac, n, i, fphi[i] / n, fE[i] / n, np.sqrt(fE2[i] / n)])
+    return {k: np.array(v) for k, v in t.items()}
+
+
+@pytest.mark.parametrize("name", ["rf", "window"])
+def test_ccp_campaign_diagnostics_bit_exact(name):
+    """Oracle mode 0 against the reference's own run: the collision-energy
+    and phase-EEDF accumulators bit for bit, and every derived column of the
+    spatial-average CSV files (17 significant digits round-trip a double)."""
+    sim, sa, cfg, wl, f, _keep = _ccp_diag_setup(name)
+    P = int(sa.phase_bins)
+    samples, csteps, psamples, pcoll = sim.spatial_counts()
+    assert csteps == int(f["collision_steps"])
+    assert np.array_equal(pcoll, f["collision_phase_steps"])
+    nch = f["collision_energy"].shape[0]
+    for c in range(nch):
+        assert np.array_equal(sim.spatial_sums(po.SA_COLLISION, c), f["collision_energy"][c]), c
+        for p in range(P):
+            assert np.array_equal(sim.spatial_sums(po.SA_COLLISION, c, p), f["collision_energy_phase"][p][c])
+    assert np.any(f["collision_energy"] != 0.0)
+    if sa.eedf_species >= 0:
+        k = 0
+        for p in range(P):
+            for r in range(sa.eedf_regions):
+                cnt, sums, hist = sim.phase_eedf(p, r)
+                assert np.array_equal(cnt, f["eedf_counts"][k]), (p, r)
+                assert np.array_equal(sums, f["eedf_sums"][k]), (p, r)
+                assert np.array_equal(hist, f["eedf_hist"][k]), (p, r)
+                k += 1
+    tables = _csv_tables(sim, sa, cfg, wl)
+    for key, mine in tables.items():
+        ref = f[f"csv_{key}"]
+        header = list(f[f"csv_{key}_header"])
+        cols = [i for i, h in enumerate(header) if not h.startswith("x_")]
+        assert np.array_equal(ref[:, cols], mine), key
