@@ -200,6 +200,8 @@ def lib() -> C.CDLL:
     L.apic_sim1d_cuda_stream.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
     L.apic_sim1d_set_kernel_timing.argtypes = [C.c_void_p, C.c_int]
     L.apic_sim1d_kernel_times.argtypes = [C.c_void_p, _DP, _DP, _U64P]
+    L.apic_sim1d_enable_power_transfer.argtypes = [C.c_void_p]
+    L.apic_sim1d_power_transfer.argtypes = [C.c_void_p, C.c_int, _DP]
     L.apic_spatial_average1d_validate.argtypes = [C.POINTER(Config1D), C.POINTER(SpatialAverage1D)]
     L.apic_sim1d_enable_spatial_average.argtypes = [C.c_void_p, C.POINTER(SpatialAverage1D)]
     L.apic_sim1d_spatial_average_counts.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, _U64P]
@@ -376,6 +378,14 @@ class Simulation1D:
         return a.value, b.value, n.value
 
     # -- CCP campaign diagnostics --
+    def enable_power_transfer(self):
+        _check(lib().apic_sim1d_enable_power_transfer(self.h), self.h)
+
+    def electric_work(self, species) -> float:
+        w = C.c_double()
+        _check(lib().apic_sim1d_power_transfer(self.h, species, C.byref(w)), self.h)
+        return w.value
+
     def enable_spatial_average(self, sa: SpatialAverage1D):
         self._sa = sa
         _check(lib().apic_sim1d_enable_spatial_average(self.h, C.byref(sa)), self.h)

@@ -85,6 +85,7 @@ struct DevState {
     double chan_energy[kMaxModels][kMaxChannels];
     unsigned long long lost[kMaxSpecies][2];
     double lost_energy[kMaxSpecies][2];
+    double work[kMaxSpecies];  // electric-work ledger (species_power_transfer), when enabled
 };
 
 struct BirthRec {
@@ -121,6 +122,9 @@ struct SpeciesDev {
     float* vy32[2];
     float* vz32[2];
     double* stage;  // FP32 form: FP64 staging for host copies (capacity)
+    // electric-work ledger: the time-centred v each particle had at the end of
+    // its last step (double-buffered like the state); null unless enabled
+    double* vold[2];
 };
 
 struct Params1D {
@@ -149,6 +153,7 @@ struct Params1D {
     double* coll_acc;
     double* coll_phase_acc;
     int coll_off[kMaxModels];  // first channel of each model in the channel numbering
+    int ledger;                // electric-work ledger enabled (SpeciesDev::vold allocated)
 };
 
 // ---- field gather / deposit (reference arithmetic) ----------------------
@@ -255,6 +260,12 @@ __device__ __forceinline__ unsigned physical_slot_from(const unsigned* lstart, c
 
 // ---- campaign diagnostics stencil ---------------------------------------------
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Node volume of the diagnostics deposits: Grid::node_volume, src/Grid.cpp:26-30
 template <bool DIRICHLET>
 __device__ __forceinline__ double node_volume(const Params1D& p, int i) {
@@ -352,6 +363,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
         r0 = __shfl_sync(0xffffffffu, r0, 0);
 
         double x[kItems], vh[kItems], vy[kItems], vz[kItems], vc[kItems], Ek[kItems];
+        double vo[kItems];  // DIAG with the ledger: v at the end of the particle's last step
+        double wsum = 0.0;  // DIAG with the ledger: this thread's electric work
         bool keep[kItems];
         int queued[kItems];
 #pragma unroll
@@ -367,6 +380,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
             vz[k] = (VDIM == 3 && live) ? ld_comp<F32>(S.vz[0], S.vz32[0], ph) : 0.0;
             vc[k] = 0.0;
             if ((mode & kModeInitHalf) && live) vc[k] = S.v[ph];
+            vo[k] = 0.0;
+            if (DIAG && p.ledger && live)
+                vo[k] = (mode & (kModeKickDrift | kModeSyncMcc)) ? S.vold[0][ph] : S.v[ph];
         }
         // -- phase A: gather, synchronize, first collision draw --
 #pragma unroll
@@ -383,6 +399,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
             if (mode & kModeSyncMcc) {
                 // synchronize_leapfrog, src/Pusher.cpp:78-80
                 vc[k] = vh[k] + S.hqm * E * p.dt;
+                // electric-work ledger, src/Simulation.cpp:1109-1114
+                if (DIAG && p.ledger) wsum += 0.5 * S.mass * S.weight * (vc[k] * vc[k] - vo[k] * vo[k]);
                 if (mcc) {
                     const MccModelDev& M = p.model[S.model];
                     // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
@@ -500,6 +518,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                     x[k] = wrap_periodic(x[k], p.L);
                 } else if (x[k] < 0.0 || x[k] > p.L) {
                     // absorbing walls and loss ledger, src/Simulation.cpp:1047-1077
+                    if (DIAG && p.ledger) {
+                        const double vp = (mode & (kModeSyncMcc | kModeInitHalf)) ? vc[k] : vo[k];
+                        const double hmw = 0.5 * S.mass * S.weight;
+                        wsum += hmw * vh[k] * vh[k] - hmw * vp * vp;
+                    }
                     const double sp2 = vh[k] * vh[k] + vy[k] * vy[k] + vz[k] * vz[k];
                     const double e = 0.5 * S.mass * S.weight * sp2;
                     const int side = x[k] < 0.0 ? 0 : 1;
@@ -516,6 +539,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 atomicAdd(&sRho[d.i0], (unsigned long long)a0);
                 atomicAdd(&sRho[d.i1], (unsigned long long)a1);
             }
+        }
+        if (DIAG && p.ledger) {
+            const double w = warp_sum(wsum);
+            if (lane == 0 && w != 0.0) atomicAdd(&st->work[s], w);
         }
         // ---- order-preserving compaction of the survivors ----
         unsigned ballots[kItems];
@@ -557,6 +584,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 st_comp<F32>(S.vz[1], S.vz32[1], o, vz[k]);
             }
             if (mode & (kModeWriteV | kModeInitHalf)) S.v[o] = vc[k];
+            if (DIAG && p.ledger) S.vold[1][o] = (mode & (kModeSyncMcc | kModeInitHalf)) ? vc[k] : vo[k];
         }
         __syncthreads();
     }
@@ -750,6 +778,10 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                 if (!DIRICHLET) {
                     bx[k] = wrap_periodic(bx[k], p.L);
                 } else if (bx[k] < 0.0 || bx[k] > p.L) {
+                    if (p.ledger) {  // electric work of a wall crossing, src/Simulation.cpp:1047-1056
+                        const double hmw = 0.5 * S.mass * S.weight;
+                        atomicAdd(&st->work[r.species], hmw * bvh[k] * bvh[k] - hmw * bv[k][0] * bv[k][0]);
+                    }
                     const double sp2 = bvh[k] * bvh[k] + bv[k][1] * bv[k][1] + bv[k][2] * bv[k][2];
                     const int side = bx[k] < 0.0 ? 0 : 1;
                     atomicAdd(&st->lost[r.species][side], 1ull);
@@ -785,6 +817,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                     st_comp<F32>(S.vz[1], S.vz32[1], o, bv[k][2]);
                 }
                 S.v[o] = bv[k][0];
+                if (p.ledger) S.vold[1][o] = bv[k][0];
             }
             if (tid == 0) s_kept[s] = total;
         }
@@ -973,12 +1006,6 @@ struct MomentArgs {
     double* eedf_hist;             // [regions][bins]
     int hist_shared;               // histogram staged in shared memory
 };
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // Species::deposit_velocity_moments (src/Species.cpp:285-336) of every species
 // and accumulate_phase_eedf (src/Simulation.cpp:1238-1285) of the EEDF species,
@@ -1407,6 +1434,22 @@ struct Sim1D {
         p.coll_phase_acc = nullptr;
     }
 
+    // species_power_transfer, src/Simulation.cpp:1094-1132: keeps each
+    // particle's end-of-step v (one more FP64 array per buffer, 16 bytes of
+    // traffic per particle-step) and runs the diagnostics pass instantiation.
+    void enable_power_transfer() {
+        require(!initialized, "the electric-work ledger must be enabled before initialize() or resume()",
+                APIC_ERR_STATE);
+        if (p.ledger) return;
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            p.sp[s].vold[0] = dalloc<double>(cfg.species[s].capacity);
+            p.sp[s].vold[1] = dalloc<double>(cfg.species[s].capacity);
+        }
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        p.ledger = 1;
+        drop_graphs();
+    }
+
     bool sample_step(uint64_t k) const {
         const auto& a = sa.cfg;
         return sa.on && k >= a.start_step && k <= a.end_step && (k - a.start_step) % a.interval == 0;
@@ -1676,6 +1719,7 @@ struct Sim1D {
             S.rstart[0] = B.rstart[in]; S.rstart[1] = B.rstart[out];
             S.rcount[0] = B.rcount[in]; S.rcount[1] = B.rcount[out];
             S.rlstart[0] = B.rlstart[in]; S.rlstart[1] = B.rlstart[out];
+            S.vold[0] = B.vold[in]; S.vold[1] = B.vold[out];
         }
         return q;
     }
@@ -1732,7 +1776,7 @@ struct Sim1D {
 
     template <int VDIM, bool DIR, bool F32>
     void launch_kernels(const Params1D& q, int blocks, size_t smem, size_t post_smem, unsigned post, EvPair& ev) {
-        if (q.coll_acc)
+        if (q.coll_acc || q.ledger)
             k_pass1d<VDIM, DIR, F32, true><<<blocks, kThreads, smem, stream>>>(q);
         else
             k_pass1d<VDIM, DIR, F32, false><<<blocks, kThreads, smem, stream>>>(q);
@@ -1881,6 +1925,7 @@ struct Sim1D {
     // Simulation::initialize, src/Simulation.cpp:698-769
     void initialize() {
         set_time(0.0, 0);
+        APIC_CUDA(cudaMemsetAsync(&st->work[0], 0, sizeof(double) * kMaxSpecies, stream));  // src/Simulation.cpp:706-710
         launch_pass(kModeDeposit, kPostSolve);
         launch_pass(kModeInitHalf, 0);
         pending = false;
@@ -2273,6 +2318,20 @@ int apic_spatial_average1d_validate(const apic_config1d* cfg, const apic_spatial
 int apic_sim1d_enable_spatial_average(apic_sim1d* sim, const apic_spatial_average1d* sa) {
     if (!sim || !sa) return APIC_ERR_INVALID;
     return guarded(sim, [&] { sim->impl.enable_spatial_average(*sa); });
+}
+int apic_sim1d_enable_power_transfer(apic_sim1d* sim) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.enable_power_transfer(); });
+}
+int apic_sim1d_power_transfer(apic_sim1d* sim, int species, double* electric_work) {
+    if (!sim || !electric_work) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        auto& S = sim->impl;
+        apic::require(species >= 0 && species < S.cfg.nspecies, "species index out of range");
+        apic::require(S.p.ledger != 0, "the electric-work ledger is not enabled", APIC_ERR_STATE);
+        S.finish();
+        *electric_work = S.read_state().work[species];
+    });
 }
 int apic_sim1d_spatial_average_counts(apic_sim1d* sim, uint64_t* samples, uint64_t* collision_steps,
                                       uint64_t* phase_samples, uint64_t* collision_phase_steps) {

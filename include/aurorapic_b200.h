@@ -255,6 +255,14 @@ APIC_EXPORT uint64_t apic_sim1d_step_count(const apic_sim1d* sim);
 
 /* ---- 1D CCP campaign diagnostics ------------------------------------------ */
 
+/* Enables the per-species electric-work ledger of Simulation::step (the work
+ * term of every synchronisation and wall crossing, src/Simulation.cpp:1047-1056,
+ * :1094-1132).  Before initialize()/resume(); initialize() resets it.  Costs one
+ * more FP64 array per particle buffer (16 bytes of traffic per particle-step). */
+APIC_EXPORT int apic_sim1d_enable_power_transfer(apic_sim1d* sim);
+/* species_power_transfer()[species].electric_work, include/pic/Simulation.hpp:77-81 */
+APIC_EXPORT int apic_sim1d_power_transfer(apic_sim1d* sim, int species, double* electric_work);
+
 #define APIC_MAX_EEDF_REGIONS 8
 
 /* SpatialAverage1DConfig + PhaseEedf1DConfig (include/pic/Config.hpp:145-168)

@@ -545,6 +545,7 @@ struct ora_sim1d {
     uint64_t candidates, nulls, per_channel[ORA_MAX_MODELS][ORA_MAX_CHANNELS];
     ora_product* staged;
     size_t nstaged, staged_cap;
+    double electric_work[ORA_MAX_SPECIES]; /* species_power_transfer_, src/Simulation.cpp:1094-1132 */
     struct {
         int on;
         ora_spatial_average1d cfg;
@@ -666,6 +667,7 @@ static void deposit_and_solve(ora_sim1d* s, double field_time) {
 int ora_sim1d_initialize(ora_sim1d* s) {
     s->time = 0.0;
     s->step = 0;
+    memset(s->electric_work, 0, sizeof s->electric_work);
     deposit_and_solve(s, 0.0);
     for (int sid = 0; sid < s->cfg.nspecies; ++sid) {
         ora_store* st = &s->sp[sid];
@@ -1035,6 +1037,7 @@ static int apply_collisions(ora_sim1d* s) {
 /* Simulation::step, src/Simulation.cpp:1008-1138 */
 static int step_once(ora_sim1d* s) {
     const ora_config1d* c = &s->cfg;
+    double work[ORA_MAX_SPECIES] = {0.0, 0.0, 0.0, 0.0}; /* one chunk per species: the serial runtime */
     for (int sid = 0; sid < c->nspecies; ++sid) {
         ora_store* st = &s->sp[sid];
         const double qm = c->species[sid].charge / c->species[sid].mass;
@@ -1048,6 +1051,9 @@ static int step_once(ora_sim1d* s) {
             if (!c->dirichlet) {
                 st->x[i] = wrap(st->x[i], c->length);
             } else if (st->x[i] < 0.0 || st->x[i] > c->length) {
+                /* electric work of a wall crossing, src/Simulation.cpp:1047-1056 */
+                const double hmw = 0.5 * c->species[sid].mass * c->species[sid].weight;
+                work[sid] += hmw * st->vh[i] * st->vh[i] - hmw * st->v[i] * st->v[i];
                 const double sp2 = st->vh[i] * st->vh[i] + st->vy[i] * st->vy[i] + st->vz[i] * st->vz[i];
                 const double e = 0.5 * c->species[sid].mass * c->species[sid].weight * sp2;
                 if (st->x[i] < 0.0) { st->lost_left++; st->e_left += e; }
@@ -1075,9 +1081,14 @@ static int step_once(ora_sim1d* s) {
         const double qm = c->species[sid].charge / c->species[sid].mass;
         for (size_t i = 0; i < st->n; ++i) {
             if (!st->alive[i]) continue;
+            const double old_velocity = st->v[i];
             /* synchronize_leapfrog, src/Pusher.cpp:78-80 */
             st->v[i] = st->vh[i] + 0.5 * qm * gather(s, st->x[i]) * c->dt;
+            /* the electric-work ledger, src/Simulation.cpp:1109-1114 */
+            work[sid] += 0.5 * c->species[sid].mass * c->species[sid].weight *
+                         (st->v[i] * st->v[i] - old_velocity * old_velocity);
         }
+        s->electric_work[sid] += work[sid];
     }
     diag_begin_collision_step(s);
     const int rc = apply_collisions(s);
@@ -1137,6 +1148,8 @@ void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t*
     const ora_store* st = &s->sp[species];
     *left = st->lost_left; *right = st->lost_right; *eleft = st->e_left; *eright = st->e_right;
 }
+
+double ora_sim1d_electric_work(const ora_sim1d* s, int species) { return s->electric_work[species]; }
 
 /* Species::kinetic_energy, src/Species.cpp:338-351 */
 double ora_sim1d_kinetic(const ora_sim1d* s, int species) {

@@ -90,6 +90,9 @@ void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t*
                       double* eleft, double* eright);
 double ora_sim1d_kinetic(const ora_sim1d* s, int species);
 double ora_sim1d_field_energy(const ora_sim1d* s);
+/* species_power_transfer()[species].electric_work since initialize,
+ * src/Simulation.cpp:1094-1132 */
+double ora_sim1d_electric_work(const ora_sim1d* s, int species);
 /* CCP campaign diagnostics (src/Simulation.cpp:1163-1370): spatial averages,
  * phase bins, spatial collision energy and the phase EEDF.  Enable before
  * initialize; the configuration is assumed valid (the device validates it).

@@ -189,6 +189,8 @@ def oracle() -> C.CDLL:
         L.ora_sim1d_losses.argtypes = [C.c_void_p, C.c_int, _U64P, _U64P, _DP, _DP]
         L.ora_sim1d_kinetic.restype = C.c_double
         L.ora_sim1d_kinetic.argtypes = [C.c_void_p, C.c_int]
+        L.ora_sim1d_electric_work.restype = C.c_double
+        L.ora_sim1d_electric_work.argtypes = [C.c_void_p, C.c_int]
         L.ora_sim1d_field_energy.restype = C.c_double
         L.ora_sim1d_field_energy.argtypes = [C.c_void_p]
         L.ora_last_error.restype = C.c_char_p
@@ -226,6 +228,8 @@ def ref() -> C.CDLL:
         L.ref1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, C.c_size_t]
         L.ref1d_losses.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _DP, _DP]
         L.ref1d_rng_state.argtypes = [C.c_void_p, C.c_char_p, _U64P]
+        L.ref1d_electric_work.restype = C.c_double
+        L.ref1d_electric_work.argtypes = [C.c_void_p, C.c_int]
         L.ref_deposit_solve_gather_1d.argtypes = [
             C.c_int, C.c_size_t, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int,
             _DP, _DP, C.POINTER(C.c_size_t), C.POINTER(_DP), _DP, _DP, _DP, C.c_size_t, _DP, _DP]
@@ -378,6 +382,9 @@ class Sim1D:
     def field_energy(self):
         return oracle().ora_sim1d_field_energy(self.h)
 
+    def electric_work(self, s):
+        return oracle().ora_sim1d_electric_work(self.h, s)
+
     def time(self):
         return oracle().ora_sim1d_time(self.h)
 
@@ -484,6 +491,9 @@ class Ref1D:
 
     def time(self):
         return ref().ref1d_time(self.h)
+
+    def electric_work(self, s):
+        return ref().ref1d_electric_work(self.h, s)
 
     def collision_energy(self, channel, phase=-1):
         out = np.zeros(self.cfg.nx)

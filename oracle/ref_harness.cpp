@@ -230,6 +230,10 @@ int ref1d_collisions(void* h, uint64_t* candidates, uint64_t* nulls, uint64_t* p
     return static_cast<int>(d.channel_collisions.size());
 }
 
+double ref1d_electric_work(void* h, int species) {
+    return static_cast<Ref1D*>(h)->sim->species_power_transfer().at(species).electric_work;
+}
+
 int ref1d_losses(void* h, int species, size_t* left, size_t* right, double* eleft,
                  double* eright) {
     const auto& l = static_cast<Ref1D*>(h)->sim->species_boundary_losses().at(species);

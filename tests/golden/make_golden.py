@@ -116,6 +116,7 @@ def sim_fixture(name, wl, steps, with_rng=False):
         for k, v in p.items():
             out[f"final_s{s}_{k}"] = v
         out[f"losses_s{s}"] = np.array(R.losses(s)[:2], np.uint64)
+        out[f"electric_work_s{s}"] = R.electric_work(s)
     rho, phi, E = R.fields()
     out.update(rho=rho, phi=phi, E=E, time=R.time())
     c, nl, per = R.collisions()

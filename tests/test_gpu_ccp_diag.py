@@ -1,5 +1,6 @@
 """CCP campaign diagnostics on the device (spatial average, RF phase bins,
-spatial collision energy, phase EEDF; src/Simulation.cpp:1163-1370) against
+spatial collision energy, phase EEDF; src/Simulation.cpp:1163-1370) and the
+electric-work ledger (src/Simulation.cpp:1047-1056, :1094-1132) against
 the oracle, whose restatement is pinned bit for bit to the reference's own
 accumulators and CSV output (tests/test_oracle_golden.py).
 
@@ -39,12 +40,14 @@ def _deck(frequency=F):
     return wl
 
 
-def _device(wl, kw, precision=apic.FP64, seed=0x5EED):
+def _device(wl, kw, precision=apic.FP64, seed=0x5EED, ledger=False):
     cfg, tabs = W.to_device_config(wl, precision=precision, seed=seed)
     dev = apic.Simulation1D(cfg, tabs)
     load_device(dev, wl)
     if kw is not None:
         dev.enable_spatial_average(apic.spatial_average1d(**kw))
+    if ledger:
+        dev.enable_power_transfer()
     dev.initialize()
     return dev, tabs
 
@@ -53,9 +56,17 @@ def _oracle(wl, kw, mode, seed=0x5EED):
     T = po.TableSet()
     ora = po.Sim1D(oracle_config(wl, T), mode, seed)
     load_oracle(ora, wl)
-    ora.enable_spatial_average(po.spatial_average1d(**kw))
+    if kw is not None:
+        ora.enable_spatial_average(po.spatial_average1d(**kw))
     ora.initialize()
     return ora, T
+
+
+def _check_work(dev, ora, nspecies, tol):
+    for s in range(nspecies):
+        w, wo = dev.electric_work(s), ora.electric_work(s)
+        assert abs(w - wo) <= tol * (abs(wo) + ora.kinetic(s)), (s, w, wo)
+        assert wo != 0.0
 
 
 def _compare(dev, ora, kw, nspecies, nch, tol, count_tol=0.0):
@@ -148,8 +159,61 @@ def test_fp32_form_matches_oracle_mode2():
     _compare(dev, ora, SHORT, 2, nch, 1e-5, count_tol=0.01)
 
 
+def test_electric_work_ledger_with_walls_and_products_fp64():
+    """The work of every synchronisation and wall crossing (products pushed
+    in the post kernel included), read part way through and at the end; the
+    ledger leaves the FP64 trajectory bit for bit as a run without it."""
+    wl = _deck(10 * F)
+    dev, _t1 = _device(wl, None, ledger=True)
+    ora, _t2 = _oracle(wl, None, 1)
+    dev.step(17)
+    ora.step(17)
+    _check_work(dev, ora, 2, TOL)
+    dev.step(23)
+    ora.step(23)
+    _check_work(dev, ora, 2, TOL)
+    assert dev.boundary_losses(0).absorbed_left + dev.boundary_losses(0).absorbed_right > 0
+    plain, _t3 = _device(wl, None)
+    plain.step(40)
+    for s in range(2):
+        a, b = dev.particles(s), plain.particles(s)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (s, k)
+
+
+def test_electric_work_ledger_two_stream_graphs_and_fp32():
+    """Periodic two-stream deck stepped through step_group (the graph path),
+    FP64 against oracle mode 1; the FP32 form against oracle mode 2."""
+    wl = W.two_stream(particles_per_beam=512, nx=64, seed=3, steps=50)
+    dev, _t1 = _device(wl, None, ledger=True)
+    ora, _t2 = _oracle(wl, None, 1)
+    apic.step_group([dev], 50)
+    ora.step(50)
+    _check_work(dev, ora, 2, TOL)
+    dev32, _t3 = _device(wl, None, precision=apic.FP32, ledger=True)
+    ora2, _t4 = _oracle(wl, None, 2)
+    dev32.step(50)
+    ora2.step(50)
+    _check_work(dev32, ora2, 2, 1e-5)
+
+
+def test_ledger_and_spatial_average_together():
+    wl = _deck(10 * F)
+    dev, _t1 = _device(wl, SHORT, ledger=True)
+    ora, _t2 = _oracle(wl, SHORT, 1)
+    dev.step(40)
+    ora.step(40)
+    _check_work(dev, ora, 2, TOL)
+    nch = sum(len(m.channels) for m in wl.models)
+    _compare(dev, ora, SHORT, 2, nch, TOL)
+
+
 def test_enable_after_initialize_is_refused():
     wl = _deck()
     dev, _t = _device(wl, None)
     with pytest.raises(apic.ApicError, match="before initialize"):
         dev.enable_spatial_average(apic.spatial_average1d(**WINDOW))
+    with pytest.raises(apic.ApicError, match="before initialize"):
+        dev.enable_power_transfer()
+    with pytest.raises(apic.ApicError, match="not enabled"):
+        dev.electric_work(0)

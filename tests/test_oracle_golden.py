@@ -117,6 +117,7 @@ def _run_sim(name, wl):
         for k in ("x", "v", "vh", "vy", "vz", "alive"):
             assert np.array_equal(p[k], f[f"final_s{s}_{k}"]), (name, s, k)
         assert sim.losses(s)[:2] == tuple(int(v) for v in f[f"losses_s{s}"])
+        assert sim.electric_work(s) == float(f[f"electric_work_s{s}"]), (name, s)
     rho, phi, E = sim.fields()
     assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"]) and np.array_equal(E, f["E"])
     assert sim.time() == float(f["time"])
