@@ -829,6 +829,28 @@ class SwarmRequest(C.Structure):
     ]
 
 
+class SpatialTownsendConfig(C.Structure):
+    """apic_spatial_townsend_config: the spatial_* controls of SwarmBenchmarkConfig."""
+    _fields_ = [
+        ("histories", C.c_size_t), ("length_m", C.c_double), ("bins", C.c_size_t),
+        ("fit_begin_bin", C.c_size_t), ("fit_end_bin", C.c_size_t), ("max_steps", C.c_size_t),
+        ("work_item_limit", C.c_uint64), ("min_r_squared", C.c_double),
+    ]
+
+
+class SpatialFluxPoint(C.Structure):
+    _fields_ = [("distance_m", C.c_double), ("net_crossings_per_injected_electron", C.c_double),
+                ("standard_error", C.c_double)]
+
+
+class SpatialTownsendResult(C.Structure):
+    _fields_ = [
+        ("townsend_1_m", C.c_double), ("townsend_standard_error_1_m", C.c_double), ("fit_r_squared", C.c_double),
+        ("histories_completed", C.c_uint64), ("maximum_active_particles", C.c_uint64),
+        ("particle_updates", C.c_uint64),
+    ]
+
+
 def _bind_swarm():
     L = lib()
     if getattr(L, "_swarm_bound", False):
@@ -851,6 +873,9 @@ def _bind_swarm():
     L.apic_swarm_server_set_kernel_timing.argtypes = [P, C.c_int]
     L.apic_swarm_server_kernel_times.argtypes = [P, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                                  C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    L.apic_swarm_spatial_townsend.argtypes = [
+        C.POINTER(SwarmConfig), C.POINTER(SpatialTownsendConfig), C.POINTER(MccModel), C.c_double, C.c_uint64,
+        C.POINTER(C.c_uint64), C.POINTER(SpatialTownsendResult), C.POINTER(SpatialFluxPoint), C.POINTER(C.c_double)]
     L._swarm_bound = True
     return L
 
@@ -867,6 +892,24 @@ def swarm_run(cfg: SwarmConfig, gas: MccModel, fields_td):
     out = (SwarmResult * len(f))()
     _check_swarm(L.apic_swarm_run(C.byref(cfg), C.byref(gas), f.ctypes.data_as(C.POINTER(C.c_double)), len(f), out))
     return list(out)
+
+
+def swarm_spatial_townsend(cfg: SwarmConfig, sp: SpatialTownsendConfig, gas: MccModel, reduced_field_td, seed,
+                           scan_particle_updates=0, history_crossings=False):
+    """run_spatial_townsend on the device for one reduced field.  Returns
+    (SpatialTownsendResult, profile[bins, 3] as (distance, mean net crossings,
+    standard error), crossings[histories, bins] or None, scan updates after)."""
+    L = _bind_swarm()
+    out = SpatialTownsendResult()
+    prof = (SpatialFluxPoint * max(int(sp.bins), 1))()
+    cross = np.zeros((int(sp.histories), int(sp.bins))) if history_crossings else None
+    scan = C.c_uint64(scan_particle_updates)
+    _check_swarm(L.apic_swarm_spatial_townsend(
+        C.byref(cfg), C.byref(sp), C.byref(gas), reduced_field_td, seed, C.byref(scan), C.byref(out), prof,
+        None if cross is None else cross.ctypes.data_as(C.POINTER(C.c_double))))
+    p = np.array([[q.distance_m, q.net_crossings_per_injected_electron, q.standard_error]
+                  for q in prof[:int(sp.bins)]])
+    return out, p, cross, scan.value
 
 
 class SwarmServer:

@@ -1436,6 +1436,479 @@ struct Server {
     }
 };
 
+// ---- spatial Townsend pass (run_spatial_townsend, src/Swarm.cpp:645-938) ----------
+//
+// Each history starts from one electron injected toward the planes and follows
+// its cascade until every electron has left [0, L).  One warp owns one history
+// at a time and takes the next from a global counter when it is done, so the
+// uneven cascades balance across the GPU without host round trips.  The
+// history's population lives in three per-warp global buffers (current, next,
+// births), structure of arrays (v_x, v_y, v_z, x); per step the lanes walk the
+// population 32 at a time: half kick, energy check, drift, plane crossings
+// (counted as integers per plane, then added as weight x count once per step,
+// so the tally does not depend on the order of the lanes), exit test, MCC,
+// half kick.  Survivors keep their order, the secondaries follow in parent
+// order, and a population above the target is systematically resampled by
+// index (every electron of a history carries one weight).
+constexpr int kTownsendWarps = 8;
+constexpr unsigned kErrNoTermination = 1u << 12;
+constexpr unsigned kErrSecondaries = 1u << 13;
+constexpr unsigned kErrWorkLimit = 1u << 14;
+
+struct TownsendParams {
+    const MccModelDev* model;
+    uint64_t seed;
+    double half_kick, dt, sd, max_energy_ev, length;
+    const double* planes;  // bins
+    unsigned H, bins, N, limit, max_steps;
+    double* crossings;     // H x bins
+    int* counts;           // warps x bins
+    double* pop;           // warps x 3 buffers x 4 components x limit
+    double* stage;         // warps x 32 lanes x kMaxBirthsPerElectron x 3
+    unsigned long long* updates;  // H
+    unsigned* max_active;         // H
+    unsigned* next;
+    unsigned* error;
+    unsigned long long* work_used;  // particle updates of this pass so far
+    unsigned long long work_left;   // spatial_work_item_limit minus the scan's earlier updates
+};
+
+// std::upper_bound over the plane positions
+__device__ __forceinline__ unsigned upper_plane(const double* planes, unsigned n, double value) {
+    unsigned lo = 0, hi = n;
+    while (lo < hi) {
+        const unsigned mid = (lo + hi) >> 1;
+        if (value < __ldg(planes + mid)) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kTownsendWarps * 32) k_townsend(TownsendParams P) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned warp_slot = blockIdx.x * kTownsendWarps + (threadIdx.x >> 5);
+    const MccModelDev& M = *P.model;
+    const size_t L = P.limit;
+    int* cnt = P.counts + (size_t)warp_slot * P.bins;
+    double* base = P.pop + (size_t)warp_slot * 12 * L;
+    double* stage = P.stage + ((size_t)warp_slot * 32 + lane) * kMaxBirthsPerElectron * 3;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;) {
+        unsigned h = 0;
+        if (lane == 0) h = atomicAdd(P.next, 1u);
+        h = __shfl_sync(full, h, 0);
+        if (h >= P.H || *(volatile unsigned*)P.error) break;
+        const uint32_t hs = 0x80000000u | h;
+        double* cur = base;
+        double* nxt = base + 4 * L;
+        double* brn = base + 8 * L;
+        double* row = P.crossings + (size_t)h * P.bins;
+        if (lane == 0) {
+            // the injected electron, src/Swarm.cpp:689-696
+            PhiloxStream rng(P.seed, 0xFFFFFFFEu, 0u, hs);
+            double unit = canonical(rng);
+            if (unit < 2.2250738585072014e-308) unit = 2.2250738585072014e-308;
+            const double inward = P.sd * sqrt(-2.0 * log(unit));
+            NormalState ns;
+            cur[0] = -inward;
+            cur[L] = normal(ns, rng, 0.0, P.sd);
+            cur[2 * L] = normal(ns, rng, 0.0, P.sd);
+            cur[3 * L] = 0.0;
+        }
+        for (unsigned b = lane; b < P.bins; b += 32) {
+            cnt[b] = 0;
+            row[b] = 0.0;
+        }
+        __syncwarp();
+        unsigned pop = 1, maxa = 0, err = 0;
+        unsigned long long upd = 0;
+        double w = 1.0;
+        bool terminated = false;
+        for (unsigned step = 0; step < P.max_steps; ++step) {
+            if (pop == 0) {
+                terminated = true;
+                break;
+            }
+            const unsigned active = pop;
+            maxa = max(maxa, active);
+            upd += active;
+            // the scan's work-item limit, src/Swarm.cpp:703-711
+            unsigned over = 0;
+            if (lane == 0) over = atomicAdd(P.work_used, (unsigned long long)active) + active > P.work_left;
+            if (__shfl_sync(full, over, 0)) {
+                err |= kErrWorkLimit;
+                break;
+            }
+            unsigned ns = 0, nb = 0;
+            for (unsigned b0 = 0; b0 < active; b0 += 32) {
+                const unsigned i = b0 + lane;
+                bool keep = false;
+                unsigned births = 0;
+                double v[3] = {0.0, 0.0, 0.0}, x = 0.0;
+                if (i < active) {
+                    v[0] = cur[i];
+                    v[1] = cur[L + i];
+                    v[2] = cur[2 * L + i];
+                    x = cur[3 * L + i];
+                    v[0] += P.half_kick;
+                    if (ke_ev(v[0], v[1], v[2]) > P.max_energy_ev) {
+                        err |= kErrMaxEnergyPre;
+                    } else {
+                        const double old_d = -x;
+                        x += v[0] * P.dt;
+                        const double new_d = -x;
+                        if (new_d > old_d) {
+                            const unsigned a = upper_plane(P.planes, P.bins, old_d);
+                            const unsigned e = upper_plane(P.planes, P.bins, new_d);
+                            for (unsigned k = a; k < e; ++k) atomicAdd(cnt + k, 1);
+                        } else if (new_d < old_d) {
+                            const unsigned a = upper_plane(P.planes, P.bins, new_d);
+                            const unsigned e = upper_plane(P.planes, P.bins, old_d);
+                            for (unsigned k = a; k < e; ++k) atomicAdd(cnt + k, -1);
+                        }
+                        if (!(new_d < 0.0 || new_d >= P.length)) {
+                            PhiloxStream rng(P.seed, i, step, hs);
+                            CollideResult r;
+                            collide3(M, v, P.dt, rng, r,
+                                     [&](int, const double* vs, const double*) {
+                                         if (births < (unsigned)kMaxBirthsPerElectron) {
+                                             stage[3 * births] = vs[0];
+                                             stage[3 * births + 1] = vs[1];
+                                             stage[3 * births + 2] = vs[2];
+                                         }
+                                         ++births;
+                                     },
+                                     false, 0.0);
+                            err |= r.error;
+                            v[0] += P.half_kick;
+                            if (ke_ev(v[0], v[1], v[2]) > P.max_energy_ev) err |= kErrMaxEnergy;
+                            if (births > (unsigned)kMaxBirthsPerElectron) err |= kErrSecondaries;
+                            keep = !r.removed;
+                        }
+                    }
+                }
+                const unsigned ball = __ballot_sync(full, keep);
+                if (keep) {
+                    const unsigned o = ns + __popc(ball & lt);
+                    nxt[o] = v[0];
+                    nxt[L + o] = v[1];
+                    nxt[2 * L + o] = v[2];
+                    nxt[3 * L + o] = x;
+                }
+                ns += __popc(ball);
+                unsigned incl = births;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const unsigned t = __shfl_up_sync(full, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const unsigned total = __shfl_sync(full, incl, 31);
+                // particles.size() >= population_limit before a push, src/Swarm.cpp:797-802
+                if ((unsigned long long)active + nb + total > L) err |= kErrPopulation;
+                if (!err && births) {
+                    const unsigned at = nb + incl - births;
+                    for (unsigned k = 0; k < births; ++k) {
+                        brn[at + k] = stage[3 * k];
+                        brn[L + at + k] = stage[3 * k + 1];
+                        brn[2 * L + at + k] = stage[3 * k + 2];
+                        brn[3 * L + at + k] = x;
+                    }
+                }
+                nb += total;
+                err = __reduce_or_sync(full, err);
+                if (err) break;
+            }
+            if (err) break;
+            __syncwarp();
+            for (unsigned b = lane; b < P.bins; b += 32) {
+                const int c = cnt[b];
+                if (c) {
+                    row[b] += w * (double)c;
+                    cnt[b] = 0;
+                }
+            }
+            for (unsigned k = lane; k < nb; k += 32) {
+                nxt[ns + k] = brn[k];
+                nxt[L + ns + k] = brn[L + k];
+                nxt[2 * L + ns + k] = brn[2 * L + k];
+                nxt[3 * L + ns + k] = brn[3 * L + k];
+            }
+            maxa = max(maxa, active + nb);
+            pop = ns + nb;
+            __syncwarp();
+            if (pop > P.N) {
+                // systematic_resample by index, src/Swarm.cpp:616-643
+                double u = 0.0;
+                if (lane == 0) {
+                    PhiloxStream rng(P.seed, 0xFFFFFFFFu, step, hs);
+                    u = uniform01(rng);
+                }
+                u = __shfl_sync(full, u, 0);
+                for (unsigned q = lane; q < P.N; q += 32) {
+                    const double t = (u + (double)q) * (double)pop / (double)P.N;
+                    const double c = ceil(t) - 1.0;
+                    unsigned j = c < 0.0 ? 0u : (unsigned)c;
+                    if (j > pop - 1) j = pop - 1;
+                    cur[q] = nxt[j];
+                    cur[L + q] = nxt[L + j];
+                    cur[2 * L + q] = nxt[2 * L + j];
+                    cur[3 * L + q] = nxt[3 * L + j];
+                }
+                w = (double)pop * w / (double)P.N;
+                pop = P.N;
+                __syncwarp();
+            } else {
+                double* t = cur;
+                cur = nxt;
+                nxt = t;
+            }
+        }
+        if (!err && !terminated && pop == 0) terminated = true;
+        if (!err && !terminated) err |= kErrNoTermination;
+        if (lane == 0) {
+            P.updates[h] = upd;
+            P.max_active[h] = maxa;
+            if (err) atomicOr(P.error, err);
+        }
+        if (err) break;
+    }
+}
+
+// validate_config's spatial section, src/Swarm.cpp:380-440
+static void validate_spatial(const apic_swarm_config& c, const apic_spatial_townsend_config& sp) {
+    if (sp.histories == 0) {
+        require(sp.length_m == 0.0 && sp.bins == 0 && sp.fit_begin_bin == 0 && sp.fit_end_bin == 0 &&
+                    sp.max_steps == 0 && sp.min_r_squared == 0.0,
+                "spatial Townsend controls require positive spatial_histories");
+        return;
+    }
+    require(c.population_model == APIC_SWARM_BRANCHING,
+            "spatial Townsend estimation requires population_model = branching_resampled");
+    require(std::isfinite(sp.length_m) && sp.length_m > 0.0, "spatial_length_m must be positive and finite");
+    require(sp.bins >= 4, "spatial_bins must be at least 4");
+    const size_t fit_end = sp.fit_end_bin == 0 ? sp.bins : sp.fit_end_bin;
+    require(!(sp.fit_begin_bin >= fit_end || fit_end > sp.bins || fit_end - sp.fit_begin_bin < 3),
+            "spatial Townsend fit range must contain at least three valid bins");
+    require(sp.max_steps != 0, "spatial_max_steps and spatial_work_item_limit must be positive");
+    require(!(sp.histories < c.uncertainty_blocks || c.uncertainty_blocks == 0 ||
+              sp.histories % c.uncertainty_blocks != 0),
+            "spatial_histories must be divisible by uncertainty_blocks");
+    require(sp.histories <= 1000000 / sp.bins, "spatial history-profile allocation exceeds the safety limit");
+    require(std::isfinite(sp.min_r_squared) && sp.min_r_squared >= 0.0 && sp.min_r_squared <= 1.0,
+            "spatial_min_r_squared must be between 0 and 1");
+}
+
+// linear_slope, src/Swarm.cpp:136-163
+static double linear_slope(const std::vector<double>& v, size_t begin, size_t end, double step) {
+    const size_t count = end - begin;
+    const double mean_index = 0.5 * (double)(count - 1);
+    double cov = 0.0, iv = 0.0, mv = 0.0;
+    for (size_t i = begin; i < end; ++i) mv += v[i];
+    mv /= (double)count;
+    for (size_t l = 0; l < count; ++l) {
+        const double ci = (double)l - mean_index;
+        cov += ci * (v[begin + l] - mv);
+        iv += ci * ci;
+    }
+    return cov / (iv * step);
+}
+
+// slope_r_squared, src/Swarm.cpp:202-231
+static double slope_r_squared(const std::vector<double>& v, size_t begin, size_t end) {
+    const size_t count = end - begin;
+    double mean = 0.0;
+    for (size_t i = begin; i < end; ++i) mean += v[i];
+    mean /= (double)count;
+    const double mean_index = 0.5 * (double)(count - 1);
+    double cov = 0.0, iv = 0.0, vv = 0.0;
+    for (size_t l = 0; l < count; ++l) {
+        const double ci = (double)l - mean_index, cv = v[begin + l] - mean;
+        cov += ci * cv;
+        iv += ci * ci;
+        vv += cv * cv;
+    }
+    if (vv == 0.0) return 1.0;
+    return std::clamp(cov * cov / (iv * vv), 0.0, 1.0);
+}
+
+// One field's spatial Townsend pass on the device; the flux statistics and
+// the fit (src/Swarm.cpp:835-938) on the host from the per-history crossings.
+static void spatial_townsend(const apic_swarm_config& c, const apic_spatial_townsend_config& sp,
+                             const apic_mcc_model& gas, double td, uint64_t seed, uint64_t* scan,
+                             apic_spatial_townsend_result* out, apic_spatial_flux_point* profile,
+                             double* history_crossings) {
+    validate_spatial(c, sp);
+    std::memset(out, 0, sizeof *out);
+    if (sp.histories == 0) return;
+    require(c.particles > 0 && c.timestep > 0 && std::isfinite(c.timestep), "swarm particles and timestep must be positive");
+    require(std::isfinite(c.max_energy_ev) && c.max_energy_ev > 0, "swarm max_energy_ev must be positive and finite");
+    require(gas.nch >= 1, "swarm gas dataset has no collision channels");
+    bool has_elastic = false;
+    for (int i = 0; i < gas.nch && i < kMaxChannels; ++i) {
+        require(gas.ch[i].process != APIC_CHARGE_EXCHANGE,
+                "electron swarm benchmark does not support charge-exchange channels");
+        require(gas.ch[i].energy_frame == APIC_FRAME_PROJECTILE,
+                "electron swarm benchmark requires projectile-frame cross-section energy");
+        has_elastic = has_elastic || gas.ch[i].process == APIC_ELASTIC;
+    }
+    require(has_elastic, "electron swarm benchmark requires an elastic channel");
+    const size_t H = sp.histories, bins = sp.bins, N = c.particles;
+    const size_t limit = population_limit(N, c.population_limit);
+    require(limit < (1u << 30) && N <= limit, "swarm population limit out of range", APIC_ERR_UNSUPPORTED);
+
+    std::vector<void*> allocations;
+    cudaStream_t stream = nullptr;
+    APIC_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    struct Release {
+        std::vector<void*>& a;
+        cudaStream_t s;
+        ~Release() {
+            cudaStreamSynchronize(s);
+            for (void* p : a) cudaFree(p);
+            cudaStreamDestroy(s);
+        }
+    } release{allocations, stream};
+    DeviceArena arena{allocations, stream};
+    apic_mcc_model m = gas;  // collision_config, src/Swarm.cpp:520-557
+    m.species = 0;
+    m.gas_units_si = 1;
+    m.neutral_density = c.neutral_density;
+    m.neutral_temperature = c.neutral_temperature;
+    m.max_frequency = c.max_frequency;
+    if (m.max_candidates == 0) m.max_candidates = 64;
+    MccModelDev model{};
+    build_model(m, kElectronMass, arena, model);
+
+    const double spacing = sp.length_m / (double)(bins + 1);
+    std::vector<double> planes(bins);
+    for (size_t b = 0; b < bins; ++b) planes[b] = (double)(b + 1) * spacing;
+    int device = 0, sms = 148;
+    APIC_CUDA(cudaGetDevice(&device));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    size_t free_b = 0, total_b = 0;
+    APIC_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_warp = 12 * limit * sizeof(double) + bins * sizeof(int) +
+                            32 * kMaxBirthsPerElectron * 3 * sizeof(double);
+    const size_t budget = std::min<size_t>(free_b / 4, (size_t)8 << 30);
+    size_t warps = std::min<size_t>(H, (size_t)sms * 4 * kTownsendWarps);
+    warps = std::min(warps, std::max<size_t>(budget / per_warp, 1));
+    const size_t blocks = (warps + kTownsendWarps - 1) / kTownsendWarps;
+    warps = blocks * kTownsendWarps;
+    require(warps * per_warp <= free_b, "spatial Townsend population buffers do not fit in device memory",
+            APIC_ERR_CAPACITY);
+
+    TownsendParams P{};
+    P.model = arena.upload(&model, 1);
+    P.seed = seed;
+    const double E = td * kTownsend * c.neutral_density;  // src/Swarm.cpp:662-667
+    P.half_kick = 0.5 * (-kEvToJ * E / kElectronMass) * c.timestep;
+    P.dt = c.timestep;
+    P.sd = std::sqrt(2.0 * c.initial_mean_energy_ev * kEvToJ / (3.0 * kElectronMass));
+    P.max_energy_ev = c.max_energy_ev;
+    P.length = sp.length_m;
+    P.planes = arena.upload(planes.data(), bins);
+    P.H = (unsigned)H;
+    P.bins = (unsigned)bins;
+    P.N = (unsigned)N;
+    P.limit = (unsigned)limit;
+    P.max_steps = (unsigned)std::min<size_t>(sp.max_steps, 0xFFFFFFFFu);
+    P.crossings = arena.alloc<double>(H * bins);
+    P.counts = arena.alloc<int>(warps * bins);
+    P.pop = arena.alloc<double>(warps * 12 * limit);
+    P.stage = arena.alloc<double>(warps * 32 * kMaxBirthsPerElectron * 3);
+    P.updates = arena.alloc<unsigned long long>(H);
+    P.max_active = arena.alloc<unsigned>(H);
+    P.next = arena.alloc<unsigned>(1);
+    P.error = arena.alloc<unsigned>(1);
+    const uint64_t work_limit = sp.work_item_limit ? sp.work_item_limit : 100000000ull;
+    require(*scan <= work_limit, "spatial Townsend scan exceeded spatial_work_item_limit");
+    P.work_used = arena.alloc<unsigned long long>(1);
+    P.work_left = work_limit - *scan;
+    k_townsend<<<(unsigned)blocks, kTownsendWarps * 32, 0, stream>>>(P);
+    APIC_CUDA(cudaGetLastError());
+    std::vector<double> cross(H * bins);
+    std::vector<unsigned long long> upd(H);
+    std::vector<unsigned> maxa(H);
+    unsigned err = 0;
+    APIC_CUDA(cudaMemcpyAsync(cross.data(), P.crossings, H * bins * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    APIC_CUDA(cudaMemcpyAsync(upd.data(), P.updates, H * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+    APIC_CUDA(cudaMemcpyAsync(maxa.data(), P.max_active, H * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    APIC_CUDA(cudaMemcpyAsync(&err, P.error, sizeof err, cudaMemcpyDeviceToHost, stream));
+    const cudaError_t we = bounded_wait(stream, 3600.0);
+    if (we == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "spatial Townsend pass did not complete in time");
+    APIC_CUDA(we);
+    if (err) {
+        const int status = (err & kErrMajorant) ? APIC_ERR_MAJORANT
+                           : (err & kErrCandidates) ? APIC_ERR_CANDIDATES
+                           : (err & (kErrPopulation | kErrSecondaries)) ? APIC_ERR_CAPACITY
+                           : (err & kErrNonFinite) ? APIC_ERR_NONFINITE
+                                                   : APIC_ERR_INVALID;
+        std::string msg;
+        if (err & kErrMaxEnergyPre) msg += "spatial Townsend particle energy exceeded max_energy_ev before collision lookup; ";
+        if (err & kErrMaxEnergy) msg += "spatial Townsend particle energy exceeded max_energy_ev; ";
+        if (err & kErrPopulation) msg += "spatial Townsend branching exceeded population_limit before resampling; ";
+        if (err & kErrNoTermination) msg += "spatial Townsend history did not terminate within spatial_max_steps; ";
+        if (err & kErrWorkLimit) msg += "spatial Townsend scan exceeded spatial_work_item_limit; ";
+        if (err & kErrSecondaries) msg += "more than 8 secondaries of one electron in one step; ";
+        if (err & kErrMajorant) msg += "MCC total collision frequency exceeds configured max_frequency; ";
+        if (err & kErrCandidates) msg += "MCC candidate limit exceeded; ";
+        if (err & kErrNonFinite) msg += "electron velocity became non-finite; ";
+        throw Error(status, msg);
+    }
+    uint64_t total = 0, max_active = 0;
+    for (size_t h = 0; h < H; ++h) {
+        total += upd[h];
+        max_active = std::max<uint64_t>(max_active, maxa[h]);
+    }
+    *scan += total;
+    if (history_crossings) std::memcpy(history_crossings, cross.data(), H * bins * sizeof(double));
+
+    std::vector<double> log_flux(bins, 0.0);
+    for (size_t b = 0; b < bins; ++b) {
+        double sum = 0.0, sq = 0.0;
+        for (size_t h = 0; h < H; ++h) {
+            const double value = cross[h * bins + b];
+            sum += value;
+            sq += value * value;
+        }
+        const double hist = (double)H;
+        const double mean = sum / hist;
+        double se = 0.0;
+        if (H > 1) se = std::sqrt(std::max(0.0, sq - sum * sum / hist) / (hist * (hist - 1.0)));
+        profile[b].distance_m = planes[b];
+        profile[b].net_crossings_per_injected_electron = mean;
+        profile[b].standard_error = se;
+        if (mean > 0.0) log_flux[b] = std::log(mean);
+    }
+    const size_t fb = sp.fit_begin_bin, fe = sp.fit_end_bin == 0 ? bins : sp.fit_end_bin;
+    for (size_t b = fb; b < fe; ++b)
+        require(profile[b].net_crossings_per_injected_electron > 0.0,
+                "spatial Townsend fit requires positive net flux at every fit plane; increase spatial_histories or "
+                "adjust the fit range");
+    const size_t nblocks = c.uncertainty_blocks, hpb = H / nblocks;
+    std::vector<double> slopes, block_log(bins, 0.0);
+    for (size_t blk = 0; blk < nblocks; ++blk) {
+        for (size_t b = 0; b < bins; ++b) {
+            double sum = 0.0;
+            for (size_t l = 0; l < hpb; ++l) sum += cross[(blk * hpb + l) * bins + b];
+            const double flux = sum / (double)hpb;
+            require(!(b >= fb && b < fe && !(flux > 0.0)),
+                    "spatial Townsend uncertainty block has non-positive fit flux; increase spatial_histories");
+            if (flux > 0.0) block_log[b] = std::log(flux);
+        }
+        slopes.push_back(linear_slope(block_log, fb, fe, spacing));
+    }
+    double mean_slope = 0.0, se_slope = 0.0;
+    block_mean_and_error(slopes.data(), slopes.size(), slopes.size(), mean_slope, se_slope);
+    out->townsend_1_m = linear_slope(log_flux, fb, fe, spacing);
+    out->townsend_standard_error_1_m = se_slope;
+    out->fit_r_squared = slope_r_squared(log_flux, fb, fe);
+    out->histories_completed = H;
+    out->maximum_active_particles = max_active;
+    out->particle_updates = total;
+    require(!(out->fit_r_squared < sp.min_r_squared), "spatial Townsend log-flux fit did not meet spatial_min_r_squared");
+}
+
 }  // namespace swarm
 }  // namespace apic
 
@@ -1638,6 +2111,22 @@ int apic_swarm_run(const apic_swarm_config* cfg, const apic_mcc_model* gas, cons
         }
         for (size_t f = 0; f < nfields; ++f)
             if (results[f].status != APIC_OK) throw apic::Error(results[f].status, results[f].message);
+    });
+}
+
+int apic_swarm_spatial_townsend(const apic_swarm_config* cfg, const apic_spatial_townsend_config* sp,
+                                const apic_mcc_model* gas, double reduced_field_td, uint64_t seed,
+                                uint64_t* scan_particle_updates, apic_spatial_townsend_result* out,
+                                apic_spatial_flux_point* profile, double* history_crossings) {
+    if (!cfg || !sp || !gas || !out || (sp->histories && !profile)) {
+        g_swarm_error = "null argument";
+        return APIC_ERR_INVALID;
+    }
+    return guarded_swarm(nullptr, [&] {
+        uint64_t scan = scan_particle_updates ? *scan_particle_updates : 0;
+        apic::swarm::spatial_townsend(*cfg, *sp, *gas, reduced_field_td, seed, &scan, out, profile,
+                                      history_crossings);
+        if (scan_particle_updates) *scan_particle_updates = scan;
     });
 }
 

@@ -549,6 +549,42 @@ typedef struct {
 APIC_EXPORT int apic_swarm_run(const apic_swarm_config* cfg, const apic_mcc_model* gas, const double* fields_td,
                                size_t nfields, apic_swarm_result* results);
 
+/* The spatial-Townsend controls of SwarmBenchmarkConfig, include/pic/Swarm.hpp:46-55
+ * (work_item_limit 0: 100000000; fit_end_bin 0: bins). */
+typedef struct {
+    size_t histories;
+    double length_m;
+    size_t bins, fit_begin_bin, fit_end_bin;
+    size_t max_steps;
+    uint64_t work_item_limit;
+    double min_r_squared;
+} apic_spatial_townsend_config;
+
+/* SwarmSpatialFluxPoint, include/pic/Swarm.hpp:66-70 */
+typedef struct {
+    double distance_m, net_crossings_per_injected_electron, standard_error;
+} apic_spatial_flux_point;
+
+/* The spatial-Townsend fields of SwarmBenchmarkResult, include/pic/Swarm.hpp:85-92 */
+typedef struct {
+    double townsend_1_m, townsend_standard_error_1_m, fit_r_squared;
+    uint64_t histories_completed, maximum_active_particles, particle_updates;
+} apic_spatial_townsend_result;
+
+/* run_spatial_townsend (src/Swarm.cpp:645-938) for one reduced field: every
+ * history's cascade on the device (one warp per history, histories balanced
+ * through a global counter; Philox streams per history), the flux profile,
+ * log-linear fit and block errors on the host.  FP64.  The reference runs it
+ * after run_field with the same seed (cfg->seed + field index).
+ * scan_particle_updates: in/out particle updates of the whole scan so far (may
+ * be NULL); profile: sp->bins points; history_crossings (may be NULL):
+ * histories x bins net crossings.  Same validation and messages as the
+ * reference. */
+APIC_EXPORT int apic_swarm_spatial_townsend(const apic_swarm_config* cfg, const apic_spatial_townsend_config* sp,
+                                            const apic_mcc_model* gas, double reduced_field_td, uint64_t seed,
+                                            uint64_t* scan_particle_updates, apic_spatial_townsend_result* out,
+                                            apic_spatial_flux_point* profile, double* history_crossings);
+
 /* Serving: a persistent batch of swarm runs on one GPU.  No reference
  * counterpart (the reference runs fields one after another): requests are
  * admitted while run slots and the device memory budget allow, every active

@@ -2124,3 +2124,280 @@ int ora_swarm_run_field(const ora_swarm_config* cfg, const ora_mcc_model* gas, d
     free(P); free(R); free(vs); free(es); free(ls);
     return rc;
 }
+
+/* ---- spatial Townsend pass, src/Swarm.cpp:645-938 ------------------------- */
+
+/* slope_r_squared, src/Swarm.cpp:202-231 */
+static double swarm_slope_r_squared(const double* v, size_t begin, size_t end) {
+    const size_t count = end - begin;
+    double mean = 0.0;
+    for (size_t i = begin; i < end; ++i) mean += v[i];
+    mean /= (double)count;
+    const double mean_index = 0.5 * (double)(count - 1);
+    double covariance = 0.0, index_variance = 0.0, value_variance = 0.0;
+    for (size_t l = 0; l < count; ++l) {
+        const double ci = (double)l - mean_index;
+        const double cv = v[begin + l] - mean;
+        covariance += ci * cv;
+        index_variance += ci * ci;
+        value_variance += cv * cv;
+    }
+    if (value_variance == 0.0) return 1.0;
+    double r = covariance * covariance / (index_variance * value_variance);
+    return r < 0.0 ? 0.0 : (r > 1.0 ? 1.0 : r);
+}
+
+/* std::upper_bound over the plane positions */
+static size_t swarm_upper_bound(const double* planes, size_t n, double value) {
+    size_t lo = 0, hi = n;
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (value < planes[mid]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+typedef struct {
+    double v[3], pos[3], w;
+    int alive;
+} townsend_particle;
+
+int ora_swarm_spatial_townsend(const ora_swarm_config* cfg, const ora_spatial_config* sp, const ora_mcc_model* gas,
+                               double td, uint64_t seed, int mode, uint64_t* scan_updates, ora_spatial_result* out,
+                               double* profile, double* history_crossings) {
+    memset(out, 0, sizeof *out);
+    if (sp->histories == 0) return 0;
+    ora_mcc_model model = *gas; /* collision_config, src/Swarm.cpp:520-557 */
+    model.neutral_density = cfg->neutral_density;
+    model.max_frequency = cfg->max_frequency;
+    model.neutral_temperature = cfg->neutral_temperature;
+    model.si = 1;
+    if (model.max_candidates == 0) model.max_candidates = 64;
+    ora_collider col;
+    if (ora_collider_init(&col, &model, kSwarmElectronMass)) return 4;
+
+    ora_mt64 mt;
+    ora_mt64_seed(&mt, seed ^ 0x9e3779b97f4a7c15ULL);
+    ora_rng shared;
+    memset(&shared, 0, sizeof shared);
+    shared.kind = ORA_SRC_MT64;
+    shared.mt = &mt;
+    const double sd = sqrt(2.0 * cfg->initial_mean_energy_ev * kSwarmEvToJ / (3.0 * kSwarmElectronMass));
+    ora_normal nst = {0, 0.0};
+    const double E = td * kSwarmTownsend * cfg->neutral_density;
+    const double acceleration = -kSwarmEvToJ * E / kSwarmElectronMass;
+    const double half_kick = 0.5 * acceleration * cfg->timestep;
+    const size_t bins = sp->bins, H = sp->histories, N = cfg->particles;
+    const double spacing = sp->length_m / (double)(bins + 1);
+    double* planes = (double*)malloc(bins * sizeof(double));
+    for (size_t b = 0; b < bins; ++b) planes[b] = (double)(b + 1) * spacing;
+    const size_t limit = ora_swarm_population_limit(cfg);
+    const uint64_t work_limit = sp->work_item_limit ? sp->work_item_limit : 100000000ull;
+
+    double* crossings = (double*)calloc(H * bins, sizeof(double));
+    long long* net = (long long*)calloc(bins, sizeof(long long));
+    townsend_particle* P = (townsend_particle*)calloc(limit + 1, sizeof *P);
+    townsend_particle* R = (townsend_particle*)calloc(N + 1, sizeof *R);
+    uint64_t updates = 0;
+    size_t max_active = 0;
+    int rc = 0;
+    for (size_t h = 0; h < H && !rc; ++h) {
+        double* row = crossings + h * bins;
+        const uint32_t hs = 0x80000000u | (uint32_t)h;
+        size_t M = 1;
+        double w = 1.0; /* mode 1: the one weight of the history */
+        memset(&P[0], 0, sizeof P[0]);
+        P[0].w = 1.0;
+        P[0].alive = 1;
+        {
+            ora_rng src;
+            ora_rng* r = &shared;
+            ora_normal pn = {0, 0.0};
+            ora_normal* ns = &nst;
+            if (mode != 0) {
+                swarm_philox(&src, seed, 0xFFFFFFFEu, 0u, hs);
+                r = &src;
+                ns = &pn;
+            }
+            double unit = ora_canonical(r);
+            if (unit < 2.2250738585072014e-308) unit = 2.2250738585072014e-308; /* max(u, DBL_MIN) */
+            const double inward = sd * sqrt(-2.0 * log(unit));
+            P[0].v[0] = -inward;
+            P[0].v[1] = ora_normal_draw(ns, r, 0.0, sd);
+            P[0].v[2] = ora_normal_draw(ns, r, 0.0, sd);
+        }
+        int terminated = 0;
+        for (size_t step = 0; step < sp->max_steps; ++step) {
+            if (M == 0) { terminated = 1; break; }
+            const size_t active = M;
+            if (active > max_active) max_active = active;
+            if ((uint64_t)active > work_limit - *scan_updates) {
+                rc = seterr(9, "spatial Townsend scan exceeded spatial_work_item_limit");
+                break;
+            }
+            *scan_updates += active;
+            updates += active;
+            if (mode != 0) memset(net, 0, bins * sizeof(long long));
+            for (size_t i = 0; i < active && !rc; ++i) {
+                townsend_particle* p = &P[i];
+                p->v[0] += half_kick;
+                if (swarm_ke_ev(p->v) > cfg->max_energy_ev) {
+                    rc = seterr(9, "spatial Townsend particle energy exceeded max_energy_ev before collision lookup");
+                    break;
+                }
+                const double old_distance = -p->pos[0];
+                p->pos[0] += p->v[0] * cfg->timestep;
+                p->pos[1] += p->v[1] * cfg->timestep;
+                p->pos[2] += p->v[2] * cfg->timestep;
+                const double new_distance = -p->pos[0];
+                if (new_distance > old_distance) {
+                    const size_t a = swarm_upper_bound(planes, bins, old_distance);
+                    const size_t b = swarm_upper_bound(planes, bins, new_distance);
+                    for (size_t k = a; k < b; ++k) {
+                        if (mode == 0) row[k] += p->w; else ++net[k];
+                    }
+                } else if (new_distance < old_distance) {
+                    const size_t a = swarm_upper_bound(planes, bins, new_distance);
+                    const size_t b = swarm_upper_bound(planes, bins, old_distance);
+                    for (size_t k = a; k < b; ++k) {
+                        if (mode == 0) row[k] -= p->w; else --net[k];
+                    }
+                }
+                if (new_distance < 0.0 || new_distance >= sp->length_m) {
+                    p->alive = 0;
+                    continue;
+                }
+                ora_rng cr;
+                ora_rng* r = &shared;
+                if (mode != 0) {
+                    swarm_philox(&cr, seed, (uint32_t)i, (uint32_t)step, hs);
+                    r = &cr;
+                }
+                ora_collide_stats st;
+                const int crc = ora_collide3(&col, p->v, cfg->timestep, r, &st);
+                if (crc) { rc = crc; break; }
+                p->v[0] += half_kick;
+                if (swarm_ke_ev(p->v) > cfg->max_energy_ev) {
+                    rc = seterr(9, "spatial Townsend particle energy exceeded max_energy_ev");
+                    break;
+                }
+                for (int k = 0; k < st.nsecondaries && k < 16; ++k) {
+                    if (M >= limit) {
+                        rc = seterr(9, "spatial Townsend branching exceeded population_limit before resampling");
+                        break;
+                    }
+                    townsend_particle* q = &P[M++];
+                    p = &P[i];
+                    memcpy(q->v, st.secondary_velocity[k], sizeof q->v);
+                    memcpy(q->pos, p->pos, sizeof q->pos);
+                    q->w = p->w;
+                    q->alive = 1;
+                }
+                if (st.removed) P[i].alive = 0;
+            }
+            if (rc) break;
+            if (mode != 0)
+                for (size_t k = 0; k < bins; ++k)
+                    if (net[k]) row[k] += w * (double)net[k];
+            if (M > max_active) max_active = M;
+            size_t kept = 0; /* erase_if, stable */
+            for (size_t i = 0; i < M; ++i) if (P[i].alive) P[kept++] = P[i];
+            M = kept;
+            if (M > N) {
+                /* systematic_resample, src/Swarm.cpp:616-643 */
+                if (mode == 0) {
+                    double ws = 0.0;
+                    for (size_t i = 0; i < M; ++i) ws += P[i].w;
+                    const double ow = ws / (double)N;
+                    const double offset = ora_uniform01(&shared) * ow;
+                    size_t src = 0;
+                    double cumulative = P[0].w;
+                    for (size_t s = 0; s < N; ++s) {
+                        const double threshold = offset + (double)s * ow;
+                        while (src + 1 < M && cumulative < threshold) {
+                            ++src;
+                            cumulative += P[src].w;
+                        }
+                        R[s] = P[src];
+                        R[s].w = ow;
+                    }
+                } else {
+                    ora_rng r;
+                    swarm_philox(&r, seed, 0xFFFFFFFFu, (uint32_t)step, hs);
+                    const double u = ora_uniform01(&r);
+                    for (size_t s = 0; s < N; ++s) {
+                        const double t = (u + (double)s) * (double)M / (double)N;
+                        const double c = ceil(t) - 1.0;
+                        size_t j = c < 0.0 ? 0 : (size_t)c;
+                        if (j > M - 1) j = M - 1;
+                        R[s] = P[j];
+                    }
+                    w = (double)M * w / (double)N;
+                }
+                memcpy(P, R, N * sizeof *P);
+                M = N;
+            }
+        }
+        if (rc) break;
+        if (!terminated && M == 0) terminated = 1;
+        if (!terminated) rc = seterr(9, "spatial Townsend history did not terminate within spatial_max_steps");
+    }
+    if (!rc) {
+        double* logf = (double*)calloc(bins, sizeof(double));
+        for (size_t b = 0; b < bins; ++b) {
+            double sum = 0.0, sq = 0.0;
+            for (size_t h = 0; h < H; ++h) {
+                const double value = crossings[h * bins + b];
+                sum += value;
+                sq += value * value;
+            }
+            const double hist = (double)H;
+            const double mean = sum / hist;
+            double se = 0.0;
+            if (H > 1) {
+                const double centered = sq - sum * sum / hist;
+                se = sqrt((centered > 0.0 ? centered : 0.0) / (hist * (hist - 1.0)));
+            }
+            profile[3 * b] = planes[b];
+            profile[3 * b + 1] = mean;
+            profile[3 * b + 2] = se;
+            if (mean > 0.0) logf[b] = log(mean);
+        }
+        const size_t fb = sp->fit_begin_bin, fe = sp->fit_end_bin == 0 ? bins : sp->fit_end_bin;
+        for (size_t b = fb; b < fe && !rc; ++b)
+            if (!(profile[3 * b + 1] > 0.0))
+                rc = seterr(9, "spatial Townsend fit requires positive net flux at every fit plane; increase "
+                               "spatial_histories or adjust the fit range");
+        const size_t blocks = cfg->uncertainty_blocks, hpb = H / blocks;
+        double* slopes = (double*)calloc(blocks, sizeof(double));
+        double* blog = (double*)calloc(bins, sizeof(double));
+        for (size_t blk = 0; blk < blocks && !rc; ++blk) {
+            for (size_t b = 0; b < bins && !rc; ++b) {
+                double sum = 0.0;
+                for (size_t l = 0; l < hpb; ++l) sum += crossings[(blk * hpb + l) * bins + b];
+                const double flux = sum / (double)hpb;
+                if (b >= fb && b < fe && !(flux > 0.0))
+                    rc = seterr(9, "spatial Townsend uncertainty block has non-positive fit flux; increase "
+                                   "spatial_histories");
+                if (flux > 0.0) blog[b] = log(flux);
+            }
+            slopes[blk] = swarm_linear_slope(blog, fb, fe, spacing);
+        }
+        if (!rc) {
+            double m = 0.0, se = 0.0;
+            ora_block_mean_and_error(slopes, blocks, blocks, &m, &se);
+            out->townsend_1_m = swarm_linear_slope(logf, fb, fe, spacing);
+            out->townsend_se_1_m = se;
+            out->fit_r_squared = swarm_slope_r_squared(logf, fb, fe);
+            out->histories_completed = H;
+            out->maximum_active_particles = max_active;
+            out->particle_updates = updates;
+            if (out->fit_r_squared < sp->min_r_squared)
+                rc = seterr(9, "spatial Townsend log-flux fit did not meet spatial_min_r_squared");
+        }
+        free(slopes); free(blog); free(logf);
+    }
+    if (history_crossings) memcpy(history_crossings, crossings, H * bins * sizeof(double));
+    free(planes); free(crossings); free(net); free(P); free(R);
+    return rc;
+}

@@ -158,6 +158,20 @@ size_t ora_swarm_population_limit(const ora_swarm_config* cfg);
  * samples (optional): 3 x (steps - burn_in) doubles: velocity, energy, log weight. */
 int ora_swarm_run_field(const ora_swarm_config* cfg, const ora_mcc_model* gas, double td, uint64_t seed, int mode,
                         ora_swarm_result* out, double* samples);
+/* run_spatial_townsend, src/Swarm.cpp:645-938, for one reduced field.
+ * mode 0: one mt19937_64 stream seeded with seed ^ 0x9e3779b97f4a7c15 shared by
+ *         every history (bit-exact with run_swarm_benchmark);
+ * mode 1: the device form: each history h draws from Philox streams keyed on
+ *         seed with stream word 0x80000000 | h (slot 0xFFFFFFFE: injection;
+ *         slot = electron index, counter step: collisions; slot 0xFFFFFFFF:
+ *         resampling offset); plane crossings counted per step and added as
+ *         weight x net count; one weight per history, resampling by index.
+ * scan_updates: in/out particle updates of the scan so far (all fields).
+ * profile: bins x (plane position, mean net crossings, standard error);
+ * history_crossings (optional): histories x bins. */
+int ora_swarm_spatial_townsend(const ora_swarm_config* cfg, const ora_spatial_config* sp, const ora_mcc_model* gas,
+                               double td, uint64_t seed, int mode, uint64_t* scan_updates, ora_spatial_result* out,
+                               double* profile, double* history_crossings);
 
 #ifdef __cplusplus
 }

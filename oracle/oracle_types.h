@@ -108,6 +108,22 @@ typedef struct {
     uint64_t seed;
 } ora_swarm_config;
 
+/* Spatial-Townsend controls of SwarmBenchmarkConfig, include/pic/Swarm.hpp:46-55 */
+typedef struct {
+    size_t histories;
+    double length_m;
+    size_t bins, fit_begin_bin, fit_end_bin; /* fit_end_bin 0: bins */
+    size_t max_steps;
+    uint64_t work_item_limit;
+    double min_r_squared;
+} ora_spatial_config;
+
+/* Spatial-Townsend fields of SwarmBenchmarkResult, include/pic/Swarm.hpp:85-92 */
+typedef struct {
+    double townsend_1_m, townsend_se_1_m, fit_r_squared;
+    uint64_t histories_completed, maximum_active_particles, particle_updates;
+} ora_spatial_result;
+
 /* SwarmBenchmarkResult subset, include/pic/Swarm.hpp:73-115 */
 typedef struct {
     double reduced_field_td, electric_field_v_m;

@@ -940,3 +940,64 @@ def swarm_from_spec(spec, tables: TableSet):
                        initial_mean_energy_ev=spec.initial_mean_energy_ev, max_energy_ev=spec.max_energy_ev,
                        seed=spec.seed)
     return cfg, gas
+
+
+# Spatial Townsend pass (run_spatial_townsend, src/Swarm.cpp:645-938)
+
+class SpatialConfig(C.Structure):
+    _fields_ = [
+        ("histories", C.c_size_t), ("length_m", C.c_double), ("bins", C.c_size_t),
+        ("fit_begin_bin", C.c_size_t), ("fit_end_bin", C.c_size_t), ("max_steps", C.c_size_t),
+        ("work_item_limit", C.c_uint64), ("min_r_squared", C.c_double),
+    ]
+
+
+class SpatialResult(C.Structure):
+    _fields_ = [
+        ("townsend_1_m", C.c_double), ("townsend_se_1_m", C.c_double), ("fit_r_squared", C.c_double),
+        ("histories_completed", C.c_uint64), ("maximum_active_particles", C.c_uint64),
+        ("particle_updates", C.c_uint64),
+    ]
+
+
+def spatial_config(*, histories, length_m, bins, fit_begin_bin=0, fit_end_bin=0, max_steps, work_item_limit=0,
+                   min_r_squared=0.0) -> SpatialConfig:
+    return SpatialConfig(histories, length_m, bins, fit_begin_bin, fit_end_bin, max_steps, work_item_limit,
+                         min_r_squared)
+
+
+def swarm_spatial_townsend(cfg: SwarmConfig, sp: SpatialConfig, gas: MccModel, td: float, seed: int, mode: int,
+                           scan_updates: int = 0):
+    """run_spatial_townsend on the oracle (mode 0 reference form, 1 device
+    form).  Returns (SpatialResult, profile[bins, 3], crossings[histories, bins],
+    scan updates after the pass)."""
+    L = oracle()
+    L.ora_swarm_spatial_townsend.argtypes = [C.POINTER(SwarmConfig), C.POINTER(SpatialConfig), C.POINTER(MccModel),
+                                             C.c_double, C.c_uint64, C.c_int, _U64P, C.POINTER(SpatialResult), _DP,
+                                             _DP]
+    out = SpatialResult()
+    prof = np.zeros((sp.bins, 3))
+    cross = np.zeros((sp.histories, sp.bins))
+    scan = np.array([scan_updates], np.uint64)
+    rc = L.ora_swarm_spatial_townsend(C.byref(cfg), C.byref(sp), C.byref(gas), td, seed, mode, u64ptr(scan),
+                                      C.byref(out), dptr(prof), dptr(cross))
+    if rc:
+        raise RuntimeError(L.ora_last_error().decode())
+    return out, prof, cross, int(scan[0])
+
+
+def ref_swarm_run_spatial(cfg: SwarmConfig, sp: SpatialConfig, gas: MccModel, fields, workdir):
+    """pic::run_swarm_benchmark with the spatial Townsend controls: per field
+    (SwarmResult, SpatialResult, profile[bins, 3])."""
+    L = ref()
+    L.ref_swarm_run_spatial.argtypes = [C.POINTER(SwarmConfig), C.POINTER(SpatialConfig), C.POINTER(MccModel), _DP,
+                                        C.c_size_t, C.c_char_p, C.POINTER(SwarmResult), C.POINTER(SpatialResult),
+                                        _DP]
+    f = np.ascontiguousarray(fields, dtype=np.float64)
+    out = (SwarmResult * len(f))()
+    sout = (SpatialResult * len(f))()
+    prof = np.zeros((len(f), sp.bins, 3))
+    if L.ref_swarm_run_spatial(C.byref(cfg), C.byref(sp), C.byref(gas), dptr(f), len(f), workdir.encode(), out, sout,
+                               dptr(prof)):
+        raise RuntimeError(L.ref_last_error().decode())
+    return [(out[k], sout[k], prof[k]) for k in range(len(f))]

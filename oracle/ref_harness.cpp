@@ -779,8 +779,11 @@ std::string write_gas_dataset(const ora_mcc_model& gas, const std::string& dir) 
 
 extern "C" {
 
-int ref_swarm_run(const ora_swarm_config* cfg, const ora_mcc_model* gas, const double* fields, size_t nfields,
-                  const char* workdir, ora_swarm_result* out) {
+// run_swarm_benchmark; with sp, the spatial Townsend pass of every field too
+// (sp_out[f], profiles: f x bins x (plane, mean, standard error)).
+static int swarm_run_impl(const ora_swarm_config* cfg, const ora_spatial_config* sp, const ora_mcc_model* gas,
+                          const double* fields, size_t nfields, const char* workdir, ora_swarm_result* out,
+                          ora_spatial_result* sp_out, double* profiles) {
     try {
         pic::SwarmBenchmarkConfig c;
         c.gas_data_file = write_gas_dataset(*gas, workdir);
@@ -801,9 +804,34 @@ int ref_swarm_run(const ora_swarm_config* cfg, const ora_mcc_model* gas, const d
         c.max_energy_ev = cfg->max_energy_ev;
         c.seed = cfg->seed;
         c.output_file = std::string(workdir) + "/swarm.csv";
+        if (sp) {
+            c.spatial_histories = sp->histories;
+            c.spatial_length_m = sp->length_m;
+            c.spatial_bins = sp->bins;
+            c.spatial_fit_begin_bin = sp->fit_begin_bin;
+            c.spatial_fit_end_bin = sp->fit_end_bin;
+            c.spatial_max_steps = sp->max_steps;
+            if (sp->work_item_limit) c.spatial_work_item_limit = sp->work_item_limit;
+            c.spatial_min_r_squared = sp->min_r_squared;
+        }
         const auto results = pic::run_swarm_benchmark(c);
         for (size_t f = 0; f < results.size(); ++f) {
             const auto& r = results[f];
+            if (sp) {
+                ora_spatial_result& q = sp_out[f];
+                q.townsend_1_m = r.spatial_flux_townsend_1_m;
+                q.townsend_se_1_m = r.spatial_flux_townsend_standard_error_1_m;
+                q.fit_r_squared = r.spatial_flux_fit_r_squared;
+                q.histories_completed = r.spatial_histories_completed;
+                q.maximum_active_particles = r.spatial_maximum_active_particles;
+                q.particle_updates = r.spatial_particle_updates;
+                for (size_t b = 0; b < r.spatial_flux_profile.size(); ++b) {
+                    double* row = profiles + (f * sp->bins + b) * 3;
+                    row[0] = r.spatial_flux_profile[b].distance_m;
+                    row[1] = r.spatial_flux_profile[b].net_crossings_per_injected_electron;
+                    row[2] = r.spatial_flux_profile[b].standard_error;
+                }
+            }
             ora_swarm_result& o = out[f];
             std::memset(&o, 0, sizeof o);
             o.reduced_field_td = r.reduced_field_td;
@@ -847,6 +875,17 @@ int ref_swarm_run(const ora_swarm_config* cfg, const ora_mcc_model* gas, const d
     } catch (const std::exception& e) {
         return fail(e);
     }
+}
+
+int ref_swarm_run(const ora_swarm_config* cfg, const ora_mcc_model* gas, const double* fields, size_t nfields,
+                  const char* workdir, ora_swarm_result* out) {
+    return swarm_run_impl(cfg, nullptr, gas, fields, nfields, workdir, out, nullptr, nullptr);
+}
+
+int ref_swarm_run_spatial(const ora_swarm_config* cfg, const ora_spatial_config* sp, const ora_mcc_model* gas,
+                          const double* fields, size_t nfields, const char* workdir, ora_swarm_result* out,
+                          ora_spatial_result* sp_out, double* profiles) {
+    return swarm_run_impl(cfg, sp, gas, fields, nfields, workdir, out, sp_out, profiles);
 }
 
 }  // extern "C"

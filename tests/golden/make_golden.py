@@ -349,6 +349,35 @@ def ccp_diag_fixture():
         np.savez_compressed(os.path.join(HERE, f"ccp_diag_{name}.npz"), **out)
 
 
+def townsend_deck():
+    """A swarm deck whose spatial Townsend pass is short: the 4-process gas at
+    1e23 m^-3, two fields, ten electrons per history population (so the
+    cascades are resampled), 50 histories over 2 mm and 8 planes."""
+    ch, mn = W.swarm_gas_4process(table_rows=512, e_max_ev=400.0)
+    ng, T = 1e23, 300.0
+    nu = W.swarm_max_frequency(ch, ng, mn, T, 200.0)
+    spec = W.SwarmSpec("townsend", ch, mn, ng, T, nu, 0.1 / nu, 100, 50, 10, [450.0, 600.0], branching=True,
+                       uncertainty_blocks=5, initial_mean_energy_ev=1.0, max_energy_ev=200.0, seed=77)
+    sp = po.spatial_config(histories=50, length_m=2e-3, bins=8, fit_begin_bin=1, max_steps=200000)
+    return spec, sp
+
+
+def townsend_fixture():
+    """run_swarm_benchmark with the spatial Townsend controls: per field the
+    spatial result fields and the flux profile."""
+    spec, sp = townsend_deck()
+    T = po.TableSet()
+    cfg, gas = po.swarm_from_spec(spec, T)
+    rows = po.ref_swarm_run_spatial(cfg, sp, gas, spec.fields_td, tempfile.mkdtemp())
+    out = {}
+    for f, (_, r, prof) in enumerate(rows):
+        out[f"f{f}_scalars"] = np.array([r.townsend_1_m, r.townsend_se_1_m, r.fit_r_squared])
+        out[f"f{f}_counts"] = np.array([r.histories_completed, r.maximum_active_particles, r.particle_updates],
+                                       np.uint64)
+        out[f"f{f}_profile"] = prof
+    np.savez_compressed(os.path.join(HERE, "swarm_townsend.npz"), **out)
+
+
 def main(names=None):
     if names:
         for n in names:
@@ -356,6 +385,7 @@ def main(names=None):
         print("golden vectors written to", HERE)
         return
     ccp_diag_fixture()
+    townsend_fixture()
     mixed_fixture()
     dirichlet_fixture()
     bprofile_fixture()

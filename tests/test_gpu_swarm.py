@@ -256,3 +256,44 @@ def test_launch_complete_overlapping_1d_decks_keeps_results():
         x, y = decks[0][0].particles(k), ref.particles(k)
         for key in x:
             assert np.array_equal(x[key], y[key])
+
+
+def test_spatial_townsend_matches_oracle_device_form():
+    """run_spatial_townsend on the device against oracle mode 1 (the same
+    per-history Philox streams): per-history net crossings, the flux profile
+    and the fitted coefficient, over two fields sharing one work-item scan."""
+    from golden.make_golden import townsend_deck
+    spec, osp = townsend_deck()
+    T = po.TableSet()
+    ocfg, ogas = po.swarm_from_spec(spec, T)
+    cfg, gas, _tabs = W.to_device_swarm(spec)
+    sp = apic.SpatialTownsendConfig(osp.histories, osp.length_m, osp.bins, osp.fit_begin_bin, osp.fit_end_bin,
+                                    osp.max_steps, osp.work_item_limit, osp.min_r_squared)
+    scan_d = scan_o = 0
+    for k, td in enumerate(spec.fields_td):
+        d, dprof, dcross, scan_d = apic.swarm_spatial_townsend(cfg, sp, gas, td, spec.seed + k, scan_d, True)
+        o, oprof, ocross, scan_o = po.swarm_spatial_townsend(ocfg, osp, ogas, td, spec.seed + k, 1, scan_o)
+        assert (d.histories_completed, d.maximum_active_particles, d.particle_updates) == \
+            (o.histories_completed, o.maximum_active_particles, o.particle_updates)
+        assert np.max(np.abs(dcross - ocross)) <= 1e-12 * np.max(np.abs(ocross))
+        assert np.max(np.abs(dprof - oprof)) <= 1e-12 * np.max(np.abs(oprof))
+        assert abs(d.townsend_1_m - o.townsend_1_m) <= 1e-10 * abs(o.townsend_1_m)
+        assert abs(d.townsend_standard_error_1_m - o.townsend_se_1_m) <= 1e-8 * o.townsend_se_1_m
+    assert scan_d == scan_o
+
+
+def test_spatial_townsend_errors_match_reference_messages():
+    from golden.make_golden import townsend_deck
+    spec, osp = townsend_deck()
+    cfg, gas, _tabs = W.to_device_swarm(spec)
+    sp = apic.SpatialTownsendConfig(osp.histories, osp.length_m, osp.bins, osp.fit_begin_bin, osp.fit_end_bin,
+                                    osp.max_steps, osp.work_item_limit, osp.min_r_squared)
+    bad = apic.SpatialTownsendConfig(sp.histories, sp.length_m, 3, 0, 0, sp.max_steps, 0, 0.0)
+    with pytest.raises(apic.ApicError, match="spatial_bins must be at least 4"):
+        apic.swarm_spatial_townsend(cfg, bad, gas, 600.0, 1)
+    short = apic.SpatialTownsendConfig(sp.histories, sp.length_m, sp.bins, 1, 0, 20, 0, 0.0)
+    with pytest.raises(apic.ApicError, match="did not terminate within spatial_max_steps"):
+        apic.swarm_spatial_townsend(cfg, short, gas, 600.0, 1)
+    tiny = apic.SpatialTownsendConfig(sp.histories, sp.length_m, sp.bins, 1, 0, sp.max_steps, 1000, 0.0)
+    with pytest.raises(apic.ApicError, match="exceeded spatial_work_item_limit"):
+        apic.swarm_spatial_townsend(cfg, tiny, gas, 600.0, 1)

@@ -117,3 +117,36 @@ def test_fp32_storage_tracks_fp64_form():
     b, sb = po.swarm_run_field(cfg, gas, 300.0, 7, 2, samples=True)
     assert abs(a.mean_energy_ev - b.mean_energy_ev) < 1e-4 * a.mean_energy_ev
     assert abs(a.mean_velocity_x - b.mean_velocity_x) < 1e-3 * abs(a.mean_velocity_x)
+
+
+def test_spatial_townsend_bit_exact_against_reference():
+    """run_spatial_townsend (src/Swarm.cpp:645-938): oracle mode 0 against the
+    reference's own run_swarm_benchmark over two fields (seed + f, one
+    particle-update scan across the fields): result fields and the flux
+    profile bit for bit (tests/golden/swarm_townsend.npz)."""
+    import os
+    from golden.make_golden import townsend_deck
+    f = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "swarm_townsend.npz"))
+    spec, sp = townsend_deck()
+    T = po.TableSet()
+    cfg, gas = po.swarm_from_spec(spec, T)
+    scan = 0
+    for k, td in enumerate(spec.fields_td):
+        r, prof, _, scan = po.swarm_spatial_townsend(cfg, sp, gas, td, spec.seed + k, 0, scan)
+        assert np.array_equal(np.array([r.townsend_1_m, r.townsend_se_1_m, r.fit_r_squared]), f[f"f{k}_scalars"])
+        assert [r.histories_completed, r.maximum_active_particles, r.particle_updates] == list(f[f"f{k}_counts"])
+        assert np.array_equal(prof, f[f"f{k}_profile"])
+    assert scan == int(f["f0_counts"][2] + f["f1_counts"][2])
+
+
+def test_spatial_townsend_device_form_is_consistent():
+    """Mode 1 (the device form, per-history Philox streams) estimates the same
+    Townsend coefficient within the combined standard errors."""
+    from golden.make_golden import townsend_deck
+    spec, sp = townsend_deck()
+    T = po.TableSet()
+    cfg, gas = po.swarm_from_spec(spec, T)
+    for k, td in enumerate(spec.fields_td):
+        a = po.swarm_spatial_townsend(cfg, sp, gas, td, spec.seed + k, 0)[0]
+        b = po.swarm_spatial_townsend(cfg, sp, gas, td, spec.seed + k, 1)[0]
+        assert abs(a.townsend_1_m - b.townsend_1_m) < 3.0 * np.hypot(a.townsend_se_1_m, b.townsend_se_1_m)
