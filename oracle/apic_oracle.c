@@ -1382,13 +1382,30 @@ int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* 
  * lexicographic SOR (omega 1.7 in 2D, 1.65 in 3D) until the largest update is
  * below 1e-11, then E by differences (one-sided at the walls).  Mesh spacing
  * L / (n - 1).  E holds [dims][N].  Returns nonzero when SOR does not converge. */
+static int solve_dirichlet_sor(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                               double eps, const double* pot, int warm);
+
 int ora_solve_dirichlet_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
                            double eps, const double* pot) {
+    return solve_dirichlet_sor(rho, phi, E, dims, n, L, eps, pot, 0);
+}
+
+/* The same solve started from the potential already in phi: inside a run the
+ * mesh keeps its potential between steps, so the reference's SOR starts from
+ * the previous step's solution. */
+int ora_solve_dirichlet_nd_warm(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                                double eps, const double* pot) {
+    return solve_dirichlet_sor(rho, phi, E, dims, n, L, eps, pot, 1);
+}
+
+static int solve_dirichlet_sor(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                               double eps, const double* pot, int warm) {
     const size_t nx = n[0], ny = n[1], nz = dims == 3 ? n[2] : 1;
     const double dx = L[0] / (double)(nx - 1), dy = L[1] / (double)(ny - 1);
     const double dz = dims == 3 ? L[2] / (double)(nz - 1) : 1.0;
     const size_t N = nx * ny * nz;
-    for (size_t i = 0; i < N; ++i) phi[i] = 0.0;
+    if (!warm)
+        for (size_t i = 0; i < N; ++i) phi[i] = 0.0;
     if (dims == 2) {
         const double left = pot ? pot[0] : 0.0, right = pot ? pot[1] : 0.0;
         const double bottom = pot ? pot[2] : 0.0, top = pot ? pot[3] : 0.0;
@@ -1549,6 +1566,12 @@ struct ora_simnd {
     double *pos[ORA_MAX_SPECIES], *v[ORA_MAX_SPECIES], *vh[ORA_MAX_SPECIES]; /* [3][np] each */
     double *rho, *phi, *E;
     double time;
+    /* 2D walls: Dirichlet field axes, side potentials and particle boundaries
+     * (left, right, bottom, top: 0 periodic, 1 absorbing, 2 reflecting) */
+    int walls, dir[2], pbc[4];
+    double pot[4];
+    uint8_t* alive[ORA_MAX_SPECIES];
+    uint64_t losses[ORA_MAX_SPECIES][4];
 };
 
 ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double dt, double eps, const double* B,
@@ -1577,7 +1600,7 @@ ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double d
 void ora_simnd_destroy(ora_simnd* s) {
     if (!s) return;
     free(s->prof_c); free(s->prof_v);
-    for (int k = 0; k < ORA_MAX_SPECIES; ++k) { free(s->pos[k]); free(s->v[k]); free(s->vh[k]); }
+    for (int k = 0; k < ORA_MAX_SPECIES; ++k) { free(s->pos[k]); free(s->v[k]); free(s->vh[k]); free(s->alive[k]); }
     free(s->rho); free(s->phi); free(s->E); free(s);
 }
 
@@ -1591,11 +1614,87 @@ void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const dou
     memcpy(s->pos[k], pos, 3 * np * sizeof(double));
     memcpy(s->v[k], v, 3 * np * sizeof(double));
     memcpy(s->vh[k], vh, 3 * np * sizeof(double));
+    free(s->alive[k]);
+    s->alive[k] = malloc(np + 1);
+    memset(s->alive[k], 1, np + 1);
+}
+
+/* Mesh2D with a boundary per axis (src/Mesh2D.cpp:51-88) and the 2D particle
+ * boundaries (src/Simulation2D.cpp:38-97, :1309-1335). */
+int ora_simnd_set_walls(ora_simnd* s, const int* dirichlet, const double* potentials, const int* particle) {
+    if (s->dims != 2) return seterr(1, "walls are 2D only");
+    s->walls = dirichlet[0] || dirichlet[1];
+    for (int a = 0; a < 2; ++a) {
+        s->dir[a] = dirichlet[a];
+        s->d[a] = s->L[a] / (double)(dirichlet[a] ? s->n[a] - 1 : s->n[a]);
+    }
+    for (int k = 0; k < 4; ++k) { s->pot[k] = potentials[k]; s->pbc[k] = particle[k]; }
+    return 0;
+}
+
+void ora_simnd_alive_losses(const ora_simnd* s, int k, uint8_t* alive, uint64_t* losses) {
+    if (alive) for (size_t i = 0; i < s->np[k]; ++i) alive[i] = s->alive[k] ? s->alive[k][i] : 1;
+    if (losses) for (int q = 0; q < 4; ++q) losses[q] = s->losses[k][q];
+}
+
+/* One axis of the 2D CIC stencil with a wall or a wrap, src/Mesh2D.cpp:96-129,
+ * src/FieldSolver.cpp:926-960 */
+static void wall_axis(const ora_simnd* s, int a, double x, size_t* i0, size_t* i1, double* f) {
+    const size_t n = s->n[a];
+    const double L = s->L[a];
+    if (!s->dir[a]) {
+        cic_axis(x, L, s->d[a], n, i0, i1, f);
+        return;
+    }
+    const double c = x < 0.0 ? 0.0 : (L < x ? L : x);
+    const double g = c / s->d[a];
+    size_t i = (size_t)floor(g);
+    if (i > n - 2) i = n - 2;
+    double fr = g - (double)i;
+    *f = fr < 0.0 ? 0.0 : (fr > 1.0 ? 1.0 : fr);
+    *i0 = i;
+    *i1 = i + 1;
+}
+
+/* Mesh2D::node_area, src/Mesh2D.cpp:77-88 */
+static double wall_node_area(const ora_simnd* s, size_t i, size_t j) {
+    const double wx = !s->dir[0] ? s->d[0] : ((i == 0 || i + 1 == s->n[0]) ? 0.5 * s->d[0] : s->d[0]);
+    const double wy = !s->dir[1] ? s->d[1] : ((j == 0 || j + 1 == s->n[1]) ? 0.5 * s->d[1] : s->d[1]);
+    return wx * wy;
 }
 
 static void simnd_deposit_solve(ora_simnd* s) {
     const size_t N = s->n[0] * s->n[1] * s->n[2];
     memset(s->rho, 0, N * sizeof(double));
+    if (s->walls) {
+        /* deposit_charge_cic(Mesh2D&), src/Mesh2D.cpp:90-144 */
+        const size_t nx = s->n[0];
+        for (int k = 0; k < s->nspecies; ++k) {
+            const double q = s->q[k] * s->w[k];
+            const size_t np = s->np[k];
+            for (size_t p = 0; p < np; ++p) {
+                if (!s->alive[k][p]) continue;
+                size_t i0, i1, j0, j1;
+                double fx, fy;
+                wall_axis(s, 0, s->pos[k][p], &i0, &i1, &fx);
+                wall_axis(s, 1, s->pos[k][np + p], &j0, &j1, &fy);
+                s->rho[j0 * nx + i0] += q * (1.0 - fx) * (1.0 - fy) / wall_node_area(s, i0, j0);
+                s->rho[j0 * nx + i1] += q * fx * (1.0 - fy) / wall_node_area(s, i1, j0);
+                s->rho[j1 * nx + i0] += q * (1.0 - fx) * fy / wall_node_area(s, i0, j1);
+                s->rho[j1 * nx + i1] += q * fx * fy / wall_node_area(s, i1, j1);
+            }
+        }
+        /* FieldSolver::solve(Mesh2D&), src/FieldSolver.cpp:389-397 */
+        if (s->dir[0] && s->dir[1]) {
+            ora_solve_dirichlet_nd_warm(s->rho, s->phi, s->E, 2, s->n, s->L, s->eps, s->pot);
+        } else {
+            const int periodic_axis = s->dir[0] ? 1 : 0;
+            const double lo = periodic_axis == 1 ? s->pot[0] : s->pot[2];
+            const double hi = periodic_axis == 1 ? s->pot[1] : s->pot[3];
+            ora_solve_mixed_2d(s->rho, s->phi, s->E, s->n, s->L, periodic_axis, s->eps, lo, hi);
+        }
+        return;
+    }
     for (int k = 0; k < s->nspecies; ++k)
         ora_deposit_nd(s->rho, s->dims, s->n, s->L, s->q[k] * s->w[k], s->np[k], s->pos[k]);
     ora_solve_nd(s->rho, s->phi, s->E, s->dims, s->n, s->L, s->eps);
@@ -1604,6 +1703,20 @@ static void simnd_deposit_solve(ora_simnd* s) {
 static void simnd_gather(const ora_simnd* s, const double* pos, size_t np, size_t i, double e[3]) {
     double p[3] = {pos[i], pos[np + i], s->dims == 3 ? pos[2 * np + i] : 0.0};
     e[2] = 0.0;
+    if (s->walls) {
+        /* interpolate_electric(Mesh2D&), src/FieldSolver.cpp:926-975 */
+        const size_t nx = s->n[0], N = s->n[0] * s->n[1];
+        size_t i0, i1, j0, j1;
+        double fx, fy;
+        wall_axis(s, 0, p[0], &i0, &i1, &fx);
+        wall_axis(s, 1, p[1], &j0, &j1, &fy);
+        const double w00 = (1.0 - fx) * (1.0 - fy), w10 = fx * (1.0 - fy), w01 = (1.0 - fx) * fy, w11 = fx * fy;
+        for (int c = 0; c < 2; ++c) {
+            const double* E = s->E + c * N;
+            e[c] = E[j0 * nx + i0] * w00 + E[j0 * nx + i1] * w10 + E[j1 * nx + i0] * w01 + E[j1 * nx + i1] * w11;
+        }
+        return;
+    }
     ora_gather_nd(s->E, s->dims, s->n, s->L, p, e);
 }
 
@@ -1649,6 +1762,7 @@ void ora_simnd_initialize(ora_simnd* s) {
         const double qm = s->q[k] / s->m[k];
         const size_t np = s->np[k];
         for (size_t i = 0; i < np; ++i) {
+            if (s->alive[k] && !s->alive[k][i]) continue;
             double e[3];
             simnd_gather(s, s->pos[k], np, i, e);
             double v[3] = {s->v[k][i], s->v[k][np + i], s->v[k][2 * np + i]};
@@ -1667,12 +1781,37 @@ void ora_simnd_initialize(ora_simnd* s) {
 /* apply_lower/upper_boundary with periodic particle boundaries, src/Simulation2D.cpp:57-97 */
 static double wrap_if_outside(double c, double L) { return (c >= 0.0 && c <= L) ? c : wrap(c, L); }
 
+/* reflect_coordinate, src/Simulation2D.cpp:43-54 */
+static void reflect_coordinate(double* c, double* v, double L) {
+    while (*c < 0.0 || *c > L) {
+        if (*c < 0.0) { *c = -*c; *v = -*v; }
+        else { *c = 2.0 * L - *c; *v = -*v; }
+    }
+}
+
+/* Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335:
+ * returns 0 when the particle is absorbed */
+static int apply_walls(ora_simnd* s, int k, double* x, double* y, double* vx, double* vy) {
+    double* c[4] = {x, x, y, y};
+    double* v[4] = {vx, vx, vy, vy};
+    const double L[4] = {s->L[0], s->L[0], s->L[1], s->L[1]};
+    for (int side = 0; side < 4; ++side) {
+        const int lower = (side & 1) == 0;
+        if (lower ? *c[side] >= 0.0 : *c[side] <= L[side]) continue;
+        if (s->pbc[side] == 1) { s->losses[k][side]++; return 0; }
+        if (s->pbc[side] == 2) reflect_coordinate(c[side], v[side], L[side]);
+        else *c[side] = wrap(*c[side], L[side]);
+    }
+    return 1;
+}
+
 void ora_simnd_step(ora_simnd* s, size_t steps) {
     for (size_t it = 0; it < steps; ++it) {
         for (int k = 0; k < s->nspecies; ++k) {
             const double qm = s->q[k] / s->m[k];
             const size_t np = s->np[k];
             for (size_t i = 0; i < np; ++i) {
+                if (s->alive[k] && !s->alive[k][i]) continue;
                 double e[3];
                 simnd_gather(s, s->pos[k], np, i, e);
                 double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};
@@ -1680,6 +1819,14 @@ void ora_simnd_step(ora_simnd* s, size_t steps) {
                 if (s->boris) simnd_b(s, s->pos[k], np, i, B);
                 if (s->boris) ora_boris(v, e, B, qm, s->dt);
                 else for (int a = 0; a < s->dims; ++a) v[a] += qm * e[a] * s->dt;
+                if (s->walls) {
+                    double x = s->pos[k][i] + v[0] * s->dt, y = s->pos[k][np + i] + v[1] * s->dt;
+                    if (!apply_walls(s, k, &x, &y, &v[0], &v[1])) s->alive[k][i] = 0;
+                    s->pos[k][i] = x;
+                    s->pos[k][np + i] = y;
+                    for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
+                    continue;
+                }
                 for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
                 for (int a = 0; a < s->dims; ++a) {
                     double c = s->pos[k][a * np + i] + v[a] * s->dt;
@@ -1692,6 +1839,7 @@ void ora_simnd_step(ora_simnd* s, size_t steps) {
             const double qm = s->q[k] / s->m[k];
             const size_t np = s->np[k];
             for (size_t i = 0; i < np; ++i) {
+                if (s->alive[k] && !s->alive[k][i]) continue;
                 double e[3];
                 simnd_gather(s, s->pos[k], np, i, e);
                 double v[3] = {s->vh[k][i], s->vh[k][np + i], s->vh[k][2 * np + i]};

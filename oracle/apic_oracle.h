@@ -117,6 +117,8 @@ void ora_solve_nd(const double* rho, double* phi, double* E, int dims, const siz
  * SOR); pot: 2D left, right, bottom, top (NULL = grounded); 3D grounded. */
 int ora_solve_dirichlet_nd(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
                            double eps, const double* pot);
+int ora_solve_dirichlet_nd_warm(const double* rho, double* phi, double* E, int dims, const size_t* n, const double* L,
+                                double eps, const double* pot);
 /* FieldSolver::solve(Mesh2D&) with exactly one periodic axis (power of two). */
 int ora_solve_mixed_2d(const double* rho, double* phi, double* E, const size_t* n, const double* L,
                        int periodic_axis, double eps, double lower, double upper);
@@ -129,6 +131,11 @@ typedef struct ora_simnd ora_simnd;
 ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double dt, double eps, const double* B,
                             int nspecies, const double* q, const double* m, const double* w_eff);
 void ora_simnd_destroy(ora_simnd* s);
+/* 2D walls (before load): Dirichlet field axes [x, y], side potentials and
+ * particle boundaries [left, right, bottom, top] (0 periodic, 1 absorbing,
+ * 2 reflecting); absorbed particles stay in place with alive = 0 */
+int ora_simnd_set_walls(ora_simnd* s, const int* dirichlet, const double* potentials, const int* particle);
+void ora_simnd_alive_losses(const ora_simnd* s, int k, uint8_t* alive, uint64_t* losses);
 void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const double* v, const double* vh);
 /* magnetic_field_profile: B piecewise linear along `axis` (values rows x 3) */
 int ora_simnd_set_profile(ora_simnd* s, int axis, size_t rows, const double* coords, const double* values);

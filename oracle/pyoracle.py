@@ -712,6 +712,26 @@ class SimND:
         if Lb.ora_simnd_set_profile(self.h, axis, len(self._prof[0]), dptr(self._prof[0]), dptr(self._prof[1])):
             raise RuntimeError(Lb.ora_last_error().decode())
 
+    def set_walls(self, dirichlet, potentials, particle):
+        """2D walls (before load): Dirichlet field axes (x, y), side potentials
+        and particle boundaries (left, right, bottom, top: 0 periodic,
+        1 absorbing, 2 reflecting)."""
+        Lb = _nd_bind()
+        Lb.ora_simnd_set_walls.argtypes = [C.c_void_p, C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]
+        d = (C.c_int * 2)(*dirichlet)
+        pot = np.ascontiguousarray(potentials, dtype=np.float64)
+        pb = (C.c_int * 4)(*particle)
+        if Lb.ora_simnd_set_walls(self.h, d, dptr(pot), pb):
+            raise RuntimeError(Lb.ora_last_error().decode())
+
+    def alive_losses(self, k):
+        Lb = _nd_bind()
+        Lb.ora_simnd_alive_losses.argtypes = [C.c_void_p, C.c_int, _U8P, _U64P]
+        al = np.zeros(self.np[k], np.uint8)
+        lo = np.zeros(4, np.uint64)
+        Lb.ora_simnd_alive_losses(self.h, k, u8ptr(al), u64ptr(lo))
+        return al, lo
+
     def __del__(self):
         if getattr(self, "h", None):
             _nd_bind().ora_simnd_destroy(self.h)
@@ -768,10 +788,15 @@ def _refnd_bind():
 class RefND:
     """The reference's Simulation2D / Simulation3D (periodic) through the harness."""
 
-    def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0, profile=None):
+    def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0, profile=None, walls=None):
         """species: list of (q, m, w, count, drift_x, thermal); profile: optional
-        (axis, coordinates, values[rows][3]) magnetic_field_profile."""
+        (axis, coordinates, values[rows][3]) magnetic_field_profile; walls:
+        optional 2D (dirichlet[2], potentials[4], particle boundaries[4])."""
         Lb = _refnd_bind()
+        if walls is not None:
+            Lb.refnd_set_walls.argtypes = [C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]
+            self._pot = np.ascontiguousarray(walls[1], dtype=np.float64)
+            Lb.refnd_set_walls((C.c_int * 2)(*walls[0]), dptr(self._pot), (C.c_int * 4)(*walls[2]))
         self.dims, self.n, self.N = dims, list(n), int(np.prod(n))
         cols = [np.array([s[i] for s in species], dtype=np.float64) for i in (0, 1, 2, 4, 5)]
         counts = (C.c_size_t * len(species))(*[s[3] for s in species])
@@ -817,6 +842,15 @@ class RefND:
         pos, v, vh = np.zeros((3, n)), np.zeros((3, n)), np.zeros((3, n))
         _refnd_bind().refnd_get(self.h, k, dptr(pos), dptr(v), dptr(vh))
         return pos, v, vh
+
+    def alive_losses(self, k):
+        Lb = _refnd_bind()
+        Lb.refnd_alive_losses.argtypes = [C.c_void_p, C.c_int, _U8P, _U64P]
+        n = Lb.refnd_count(self.h, k)
+        al = np.zeros(n, np.uint8)
+        lo = np.zeros(4, np.uint64)
+        Lb.refnd_alive_losses(self.h, k, u8ptr(al), u64ptr(lo))
+        return al, lo
 
     def fields(self):
         rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(self.dims * self.N)

@@ -467,6 +467,22 @@ struct RefND {
 extern "C" {
 
 // species: q, m, w, count, drift_x, thermal (isotropic) per species
+// 2D walls for the next refnd_create*: mesh boundary per axis (Dirichlet
+// when set), side potentials (left, right, bottom, top) and particle
+// boundaries per side (0 periodic, 1 absorbing, 2 reflecting).
+static struct {
+    bool set = false;
+    int dirichlet[2];
+    double pot[4];
+    int pbc[4];
+} g_walls;
+
+void refnd_set_walls(const int* dirichlet, const double* pot, const int* pbc) {
+    g_walls.set = true;
+    for (int a = 0; a < 2; ++a) g_walls.dirichlet[a] = dirichlet[a];
+    for (int k = 0; k < 4; ++k) { g_walls.pot[k] = pot[k]; g_walls.pbc[k] = pbc[k]; }
+}
+
 int refnd_create_profile(int dims, const size_t* n, const double* L, double dt, int si, const double* B,
                          int nspecies, const double* q, const double* m, const double* w, const size_t* count,
                          const double* drift, const double* thermal, unsigned seed, int threads, int prof_axis,
@@ -494,6 +510,24 @@ int refnd_create_profile(int dims, const size_t* n, const double* L, double dt, 
             c.magnetic_field_profile = profile;
             c.seed = seed; c.runtime = rt;
             c.output_dir = std::filesystem::temp_directory_path() / "apic_ref2d";
+            if (g_walls.set) {
+                auto bnd = [](int d) { return d ? pic::Boundary::Dirichlet : pic::Boundary::Periodic; };
+                auto pb = [](int k) {
+                    return k == 1 ? pic::ParticleBoundary::Absorbing
+                           : k == 2 ? pic::ParticleBoundary::Reflecting : pic::ParticleBoundary::Periodic;
+                };
+                c.boundary_x = bnd(g_walls.dirichlet[0]);
+                c.boundary_y = bnd(g_walls.dirichlet[1]);
+                c.boundary_config.left.potential = g_walls.pot[0];
+                c.boundary_config.right.potential = g_walls.pot[1];
+                c.boundary_config.bottom.potential = g_walls.pot[2];
+                c.boundary_config.top.potential = g_walls.pot[3];
+                c.particle_boundary_config.left = pb(g_walls.pbc[0]);
+                c.particle_boundary_config.right = pb(g_walls.pbc[1]);
+                c.particle_boundary_config.bottom = pb(g_walls.pbc[2]);
+                c.particle_boundary_config.top = pb(g_walls.pbc[3]);
+                g_walls.set = false;
+            }
             size_t mx = 0;
             for (int s = 0; s < nspecies; ++s) {
                 pic::Species2DConfig sc;
@@ -578,6 +612,18 @@ int refnd_get(void* h, int s, double* pos, double* v, double* vh) {
             vh[i] = ps[i].velocity_half.x; vh[n + i] = ps[i].velocity_half.y; vh[2 * n + i] = ps[i].velocity_half.z;
         }
     }
+    return 0;
+}
+
+// 2D: alive flags and species_boundary_losses (left, right, bottom, top)
+int refnd_alive_losses(void* h, int s, uint8_t* alive, uint64_t* losses) {
+    auto* r = static_cast<RefND*>(h);
+    if (r->dims != 2) return 1;
+    const auto& ps = r->s2->species().at(s).particles();
+    for (size_t i = 0; i < ps.size(); ++i) alive[i] = ps[i].alive ? 1 : 0;
+    const auto& l = r->s2->species_boundary_losses().at(s);
+    losses[0] = l.absorbed_left; losses[1] = l.absorbed_right;
+    losses[2] = l.absorbed_bottom; losses[3] = l.absorbed_top;
     return 0;
 }
 

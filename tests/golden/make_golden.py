@@ -162,8 +162,8 @@ def nd_fixture(name):
     _nd_run(name, dims, n, L, B, steps)
 
 
-def _nd_run(name, dims, n, L, B, steps, profile=None):
-    R = po.RefND(dims, n, L, 0.1, 0, B, ND_SPECIES, seed=9, profile=profile)
+def _nd_run(name, dims, n, L, B, steps, profile=None, walls=None):
+    R = po.RefND(dims, n, L, 0.1, 0, B, ND_SPECIES, seed=9, profile=profile, walls=walls)
     R.initialize()
     out = {"steps": steps}
     for k in range(len(ND_SPECIES)):
@@ -173,11 +173,33 @@ def _nd_run(name, dims, n, L, B, steps, profile=None):
     for k in range(len(ND_SPECIES)):
         for key, arr in zip(("pos", "v", "vh"), R.particles(k)):
             out[f"final_s{k}_{key}"] = arr
+        if walls is not None:
+            al, lo = R.alive_losses(k)
+            out[f"final_s{k}_alive"] = al
+            out[f"losses_s{k}"] = lo
     rho, phi, E = R.fields()
     out.update(rho=rho, phi=phi, E=E, time=R.time())
+    if walls is not None:
+        out.update(walls_dirichlet=np.array(walls[0]), walls_potentials=np.array(walls[1]),
+                   walls_particle=np.array(walls[2]))
     if profile is not None:
         out.update(prof_axis=profile[0], prof_c=profile[1], prof_v=profile[2])
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+
+
+# 2D runs with walls: name -> cells, B, Dirichlet axes, side potentials, particle
+# boundaries (left, right, bottom, top: 0 periodic, 1 absorbing, 2 reflecting)
+WALL_CASES = {
+    "sim2d_walls_mixed": ((17, 8), (0.0, 0.0, 0.7), (1, 0), (0.0, 0.4, 0.0, 0.0), (1, 2, 0, 0)),
+    "sim2d_walls_dirichlet": ((17, 9), (0.0, 0.0, 0.0), (1, 1), (1.0, -0.5, 0.25, 0.0), (1, 1, 2, 1)),
+}
+
+
+def walls_fixture():
+    """Simulation2D with a wall axis (mixed solve) and with walls on every side
+    (the reference's SOR): absorbing and reflecting particle boundaries, 25 steps."""
+    for name, (n, B, d, pot, pb) in WALL_CASES.items():
+        _nd_run(name, 2, n, (4.0, 2.0), B, 25, walls=(d, pot, pb))
 
 
 def collide_hg_fixture():
@@ -386,6 +408,7 @@ def main(names=None):
         return
     ccp_diag_fixture()
     townsend_fixture()
+    walls_fixture()
     mixed_fixture()
     dirichlet_fixture()
     bprofile_fixture()

@@ -311,3 +311,30 @@ def test_ccp_campaign_diagnostics_bit_exact(name):
         header = list(f[f"csv_{key}_header"])
         cols = [i for i, h in enumerate(header) if not h.startswith("x_")]
         assert np.array_equal(ref[:, cols], mine), key
+
+
+@pytest.mark.parametrize("name", ["sim2d_walls_mixed", "sim2d_walls_dirichlet"])
+def test_2d_run_with_walls_bit_exact(name):
+    """Simulation2D with walls: clamped CIC deposit over half-cell wall areas,
+    clamped gather, absorbing and reflecting particle boundaries with the
+    per-side loss ledger, and the mixed spectral-tridiagonal or the SOR
+    Dirichlet solve (src/Simulation2D.cpp:38-97, :1309-1364, src/Mesh2D.cpp:77-144,
+    src/FieldSolver.cpp:389-397): 25 steps, bit-exact."""
+    from golden.make_golden import WALL_CASES
+    n, B, d, pot, pb = WALL_CASES[name]
+    f = load(f"{name}.npz")
+    sim = po.SimND(2, n, (4.0, 2.0), 0.1, 1.0, B, ND_SPECIES)
+    sim.set_walls(d, pot, pb)
+    for k in range(2):
+        sim.load(k, f[f"init_s{k}_pos"], f[f"init_s{k}_v"], f[f"init_s{k}_vh"])
+    sim.initialize_fields()
+    sim.step(int(f["steps"]))
+    for k in range(2):
+        al, lo = sim.alive_losses(k)
+        assert np.array_equal(al, f[f"final_s{k}_alive"]), (name, k)
+        assert np.array_equal(lo, f[f"losses_s{k}"]), (name, k)
+        for key, arr in zip(("pos", "v", "vh"), sim.particles(k)):
+            assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
+    rho, phi, E = sim.fields()
+    assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"])
+    assert np.array_equal(E[:2].ravel(), f["E"].ravel()[: 2 * len(rho)])
