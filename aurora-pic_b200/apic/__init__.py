@@ -482,6 +482,7 @@ class ConfigND(C.Structure):
         ("species_sort_interval", C.c_size_t * MAX_SPECIES),
         ("profile_axis", C.c_int), ("profile_rows", C.c_size_t),
         ("profile_coordinates", C.POINTER(C.c_double)), ("profile_values", C.POINTER(C.c_double)),
+        ("wall_axis", C.c_int * 2), ("wall_potential", C.c_double * 4), ("particle_boundary", C.c_int * 4),
     ]
 
 
@@ -531,7 +532,7 @@ def _check_nd(rc, handle=None):
 
 def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), units=NORMALIZED,
               relative_permittivity=1.0, out_of_plane_depth=1.0, precision=FP64, sort_interval=16,
-              push_items=0, species_sort_interval=None, magnetic_field_profile=None) -> ConfigND:
+              push_items=0, species_sort_interval=None, magnetic_field_profile=None, walls=None) -> ConfigND:
     """magnetic_field_profile: optional (axis, coordinates, values[rows][3]), B
     tabulated along one axis (the arrays are kept on the returned config until
     the simulation is created, which copies them)."""
@@ -558,6 +559,15 @@ def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), u
         c.profile_axis, c.profile_rows = int(ax), int(pc.size)
         c.profile_coordinates = pc.ctypes.data_as(C.POINTER(C.c_double))
         c.profile_values = pv.ctypes.data_as(C.POINTER(C.c_double))
+    if walls is not None:
+        # (wall axes [x, y], potentials [left, right, bottom, top], particle boundaries
+        #  [left, right, bottom, top]: 0 auto, 1 absorbing, 2 reflecting, 3 periodic)
+        axes, pots, pbs = walls
+        for a in range(2):
+            c.wall_axis[a] = int(axes[a])
+        for k in range(4):
+            c.wall_potential[k] = float(pots[k])
+            c.particle_boundary[k] = int(pbs[k])
     return c
 
 
@@ -616,6 +626,22 @@ class SimulationND:
         _check_nd(_bind_nd().apic_simnd_read_particles(self.h, species, n, dptr(pos), dptr(v), dptr(vh), C.byref(got)),
                   self.h)
         return pos, v, vh
+
+    def alive(self, species):
+        n = self.count(species) if hasattr(self, "count") else None
+        n = n if n is not None else len(self.particles(species)[0][0])
+        out = np.zeros(n, np.uint8)
+        L = lib()
+        L.apic_simnd_read_alive.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _U8P]
+        _check_nd(L.apic_simnd_read_alive(self.h, species, n, out.ctypes.data_as(_U8P)), self.h)
+        return out
+
+    def boundary_losses(self, species):
+        out = np.zeros(4, np.uint64)
+        L = lib()
+        L.apic_simnd_boundary_losses.argtypes = [C.c_void_p, C.c_int, _U64P]
+        _check_nd(L.apic_simnd_boundary_losses(self.h, species, out.ctypes.data_as(_U64P)), self.h)
+        return out
 
     def fields(self):
         rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(self.dims * self.N)

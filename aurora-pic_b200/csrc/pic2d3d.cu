@@ -58,6 +58,8 @@ struct SpeciesND {
     float tb[3], sb[3];  // Boris t = hqmdt B and s = 2 t / (1 + t^2)
     float drift[3];    // dt / d_a: cell units per unit velocity
     float dep_fixed;   // dep * rho_scale
+    uint8_t* alive;    // 2D walls with an absorbing side: Particle::alive (null: all alive)
+    int index;         // species index (loss ledger row)
 };
 
 struct ParamsND {
@@ -74,6 +76,11 @@ struct ParamsND {
     int prof_axis, prof_rows;
     const double* prof_c;  // coordinates
     const double* prof_v;  // rows x 3
+    // 2D walls: Dirichlet axes, particle boundaries (left, right, bottom, top:
+    // 0 periodic, 1 absorbing, 2 reflecting) and the absorbed counts [species][4]
+    int wall[2];
+    int pbc[4];
+    unsigned long long* losses;
 };
 
 // TabulatedVectorField1D::evaluate, src/PrescribedField.cpp:89-113, at coordinate
@@ -144,10 +151,39 @@ __device__ __forceinline__ Axis axis(double x, double L, double d, int n) {
     return a;
 }
 
-template <int DIM>
+// One axis of the CIC stencil on a wall axis: clamp into [0, L], cell
+// min(floor, n - 2), fraction clamped to [0, 1], src/Mesh2D.cpp:96-129,
+// src/FieldSolver.cpp:926-960
+__device__ __forceinline__ Axis axis_wall(double x, double L, double d, int n) {
+    const double c = x < 0.0 ? 0.0 : (L < x ? L : x);
+    const double g = c / d;
+    unsigned long long i = (unsigned long long)floor(g);
+    if (i > (unsigned long long)(n - 2)) i = (unsigned long long)(n - 2);
+    double f = g - (double)i;
+    f = f < 0.0 ? 0.0 : (f > 1.0 ? 1.0 : f);
+    Axis a;
+    a.i0 = (int)i;
+    a.i1 = (int)i + 1;
+    a.f = f;
+    return a;
+}
+
+template <bool WALLS>
+__device__ __forceinline__ Axis axis2(const ParamsND& p, int a, double x) {
+    return (WALLS && p.wall[a]) ? axis_wall(x, p.L[a], p.d[a], p.n[a]) : axis(x, p.L[a], p.d[a], p.n[a]);
+}
+
+// 1 / node_area relative to an interior node: 2 on each wall-axis wall node
+// (Mesh2D::node_area halves the cell there, src/Mesh2D.cpp:77-88)
+template <bool WALLS>
+__device__ __forceinline__ double area_factor(const ParamsND& p, int a, int i) {
+    return (WALLS && p.wall[a] && (i == 0 || i == p.n[a] - 1)) ? 2.0 : 1.0;
+}
+
+template <int DIM, bool WALLS = false>
 __device__ __forceinline__ void gather(const ParamsND& p, const double pos[3], double e[3]) {
-    const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
-    const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+    const Axis ax = DIM == 2 ? axis2<WALLS>(p, 0, pos[0]) : axis(pos[0], p.L[0], p.d[0], p.n[0]);
+    const Axis ay = DIM == 2 ? axis2<WALLS>(p, 1, pos[1]) : axis(pos[1], p.L[1], p.d[1], p.n[1]);
     const int nx = p.n[0];
     if (DIM == 2) {
         const double fx = ax.f, fy = ay.f;
@@ -237,7 +273,7 @@ __device__ __forceinline__ void deposit(const ParamsND& p, const SpeciesND& S, c
 // over its run with a segmented shuffle scan (integer, so the total does not
 // depend on the order), and the run's last lane commits them.  All 32 lanes
 // must call this; `valid` marks lanes that carry a particle.
-template <int DIM>
+template <int DIM, bool WALLS = false>
 __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND& S, const double pos[3], bool valid) {
     constexpr int K = DIM == 2 ? 4 : 8;
     const int lane = threadIdx.x & 31;
@@ -245,10 +281,24 @@ __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND&
     size_t node[K];
     unsigned cell = 0xFFFFFFFFu;
     if (valid) {
-        const Axis ax = axis(pos[0], p.L[0], p.d[0], p.n[0]);
-        const Axis ay = axis(pos[1], p.L[1], p.d[1], p.n[1]);
+        const Axis ax = DIM == 2 ? axis2<WALLS>(p, 0, pos[0]) : axis(pos[0], p.L[0], p.d[0], p.n[0]);
+        const Axis ay = DIM == 2 ? axis2<WALLS>(p, 1, pos[1]) : axis(pos[1], p.L[1], p.d[1], p.n[1]);
         const int nx = p.n[0];
-        if (DIM == 2) {
+        if (DIM == 2 && WALLS) {
+            // q shape / node_area over the wall nodes' half cells, src/Mesh2D.cpp:131-142
+            const double fx = ax.f, fy = ay.f;
+            const double x0 = area_factor<WALLS>(p, 0, ax.i0), x1 = area_factor<WALLS>(p, 0, ax.i1);
+            const double y0 = area_factor<WALLS>(p, 1, ay.i0), y1 = area_factor<WALLS>(p, 1, ay.i1);
+            a[0] = to_fixed(S.dep * (1.0 - fx) * (1.0 - fy) * (x0 * y0), p.rho_scale);
+            a[1] = to_fixed(S.dep * fx * (1.0 - fy) * (x1 * y0), p.rho_scale);
+            a[2] = to_fixed(S.dep * (1.0 - fx) * fy * (x0 * y1), p.rho_scale);
+            a[3] = to_fixed(S.dep * fx * fy * (x1 * y1), p.rho_scale);
+            node[0] = (size_t)ay.i0 * nx + ax.i0;
+            node[1] = (size_t)ay.i0 * nx + ax.i1;
+            node[2] = (size_t)ay.i1 * nx + ax.i0;
+            node[3] = (size_t)ay.i1 * nx + ax.i1;
+            cell = (unsigned)node[0];
+        } else if (DIM == 2) {
             const double fx = ax.f, fy = ay.f;
             a[0] = to_fixed(S.dep * (1.0 - fx) * (1.0 - fy), p.rho_scale);
             a[1] = to_fixed(S.dep * fx * (1.0 - fy), p.rho_scale);
@@ -301,10 +351,36 @@ enum : int { kPushStep = 0, kPushDepositOnly = 1, kPushInitHalf = 2, kPushSync =
 // One particle per thread.  Modes: a full step (kick, drift, wrap, deposit),
 // deposit only (initialize/resume), half-step initialisation from v
 // (initialize_{boris,leapfrog}_half_step) and synchronisation into v.
-template <int DIM, bool BORIS, int MODE>
+// reflect_coordinate, src/Simulation2D.cpp:43-54 (a particle crosses at most a
+// few domain lengths per step; the bound only guards against runaway input)
+__device__ __forceinline__ void reflect_coordinate(double& c, double& v, double L) {
+    for (int guard = 0; guard < (1 << 20) && (c < 0.0 || c > L); ++guard) {
+        if (c < 0.0) { c = -c; v = -v; }
+        else { c = 2.0 * L - c; v = -v; }
+    }
+}
+
+// Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335, with
+// apply_lower/upper_boundary (:57-97): returns the absorbing side, or -1.
+__device__ __forceinline__ int apply_walls(const ParamsND& p, double& x, double& y, double& vx, double& vy) {
+#pragma unroll
+    for (int side = 0; side < 4; ++side) {
+        double& c = side < 2 ? x : y;
+        double& v = side < 2 ? vx : vy;
+        const double L = p.L[side >> 1];
+        if ((side & 1) == 0 ? c >= 0.0 : c <= L) continue;
+        const int kind = p.pbc[side];
+        if (kind == 1) return side;
+        if (kind == 2) reflect_coordinate(c, v, L);
+        else c = wrap_periodic(c, L);
+    }
+    return -1;
+}
+
+template <int DIM, bool BORIS, int MODE, bool WALLS = false>
 __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int buf) {
     const unsigned i = blockIdx.x * kThreads + threadIdx.x;
-    const bool valid = i < S.n;
+    const bool valid = i < S.n && (!WALLS || !S.alive || S.alive[i]);
     if (MODE == kPushInitHalf || MODE == kPushSync) {
         if (!valid) return;
     } else if (blockIdx.x * kThreads + (threadIdx.x & ~31u) >= S.n) {
@@ -313,11 +389,11 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     const unsigned j = valid ? i : 0u;
     double pos[3] = {S.pos[buf][0][j], S.pos[buf][1][j], DIM == 3 ? S.pos[buf][2][j] : 0.0};
     if (MODE == kPushDepositOnly) {
-        deposit_warp<DIM>(p, S, pos, valid);
+        deposit_warp<DIM, WALLS>(p, S, pos, valid);
         return;
     }
     double e[3];
-    gather<DIM>(p, pos, e);
+    gather<DIM, WALLS>(p, pos, e);
     if (MODE == kPushInitHalf) {
         double v[3] = {S.v[0][i], S.v[1][i], S.v[2][i]};
         if (BORIS) {
@@ -352,16 +428,47 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     } else {
         for (int a = 0; a < DIM; ++a) vh[a] += S.qm * e[a] * p.dt;
     }
-    for (int a = 0; a < DIM; ++a) {
-        const double c = pos[a] + vh[a] * p.dt;
-        // periodic particle boundary: wrap only outside [0, L], src/Simulation2D.cpp:57-97
-        pos[a] = (c >= 0.0 && c <= p.L[a]) ? c : wrap_periodic(c, p.L[a]);
+    bool absorbed = false;
+    if (WALLS) {
+        double x = pos[0] + vh[0] * p.dt, y = pos[1] + vh[1] * p.dt;
+        const int side = valid ? apply_walls(p, x, y, vh[0], vh[1]) : -1;
+        pos[0] = x;
+        pos[1] = y;
+        if (side >= 0) {
+            absorbed = true;
+            S.alive[i] = 0;
+            atomicAdd(p.losses + 4 * S.index + side, 1ull);
+        }
+    } else {
+        for (int a = 0; a < DIM; ++a) {
+            const double c = pos[a] + vh[a] * p.dt;
+            // periodic particle boundary: wrap only outside [0, L], src/Simulation2D.cpp:57-97
+            pos[a] = (c >= 0.0 && c <= p.L[a]) ? c : wrap_periodic(c, p.L[a]);
+        }
     }
     if (valid) {
         for (int a = 0; a < DIM; ++a) S.pos[buf][a][i] = pos[a];
         for (int a = 0; a < 3; ++a) S.vh[buf][a][i] = vh[a];
     }
-    deposit_warp<DIM>(p, S, pos, valid);
+    deposit_warp<DIM, WALLS>(p, S, pos, valid && !absorbed);
+}
+
+// 2D walls: fixed-point density to FP64 (the accumulator is cleared for the
+// next deposit)
+__global__ void k_walls_rho(unsigned long long* __restrict__ acc, double* __restrict__ rho, size_t N,
+                            double inv_scale) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        rho[i] = (double)(long long)acc[i] * inv_scale;
+        acc[i] = 0ull;
+    }
+}
+
+// 2D walls: the field planes (Ex | Ey) into the interleaved layout of the push
+__global__ void k_walls_interleave(const double* __restrict__ planes, double* __restrict__ E, size_t N) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x) {
+        E[2 * i] = planes[i];
+        E[2 * i + 1] = planes[N + i];
+    }
 }
 
 // ---- FP32 particle form ---------------------------------------------------------
@@ -1154,13 +1261,14 @@ constexpr int kSampleBlocks = 148;
 __global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double* partial, unsigned* done,
                                                    double* out, const double* E, const double* rho,
                                                    long long N, double half_eps_vol, double vol, int species,
-                                                   int last_species) {
+                                                   int last_species, int wall_x, int wall_y, int nx, int ny) {
     __shared__ double red[8], red2[8], red3[8];
     __shared__ bool last;
     const int tid = threadIdx.x;
     double ke = 0.0, fe = 0.0, l1 = 0.0;
     for (unsigned i = blockIdx.x * 256 + tid; i < S.n; i += gridDim.x * 256)
-        ke += S.hmw * (S.v[0][i] * S.v[0][i] + S.v[1][i] * S.v[1][i] + S.v[2][i] * S.v[2][i]);
+        if (!S.alive || S.alive[i])
+            ke += S.hmw * (S.v[0][i] * S.v[0][i] + S.v[1][i] * S.v[1][i] + S.v[2][i] * S.v[2][i]);
     if (last_species) {
         for (long long g = blockIdx.x * 256 + tid; g < N; g += gridDim.x * 256) {
             double e2;
@@ -1171,8 +1279,12 @@ __global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double
                 const double4 e = reinterpret_cast<const double4*>(E)[g];
                 e2 = e.x * e.x + e.y * e.y + e.z * e.z;
             }
-            fe += half_eps_vol * e2;
-            l1 += fabs(rho[g]) * vol;
+            // Mesh2D::node_area: half cells on the wall nodes, src/Mesh2D.cpp:77-88
+            const int gi = (int)(g % nx), gj = (int)(g / nx);
+            const double f = ((wall_x && (gi == 0 || gi == nx - 1)) ? 0.5 : 1.0) *
+                             ((wall_y && (gj == 0 || gj == ny - 1)) ? 0.5 : 1.0);
+            fe += half_eps_vol * e2 * f;
+            l1 += fabs(rho[g]) * vol * f;
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -1331,6 +1443,24 @@ struct Solver {
     }
 };
 
+// field solves with walls (defined with their stand-alone entry points below)
+__global__ void __launch_bounds__(kFftThreads) k_mixed_forward(const double* __restrict__ rho, Cplx* __restrict__ hat,
+                                                               int nx, int np, int periodic_y, const Cplx* tw);
+__global__ void k_mixed_tridiag(Cplx* __restrict__ hat, double* __restrict__ mu, int nd, int np, double inv_dsq,
+                                double inv_psq, double eps, double lower, double upper);
+__global__ void __launch_bounds__(kFftThreads) k_mixed_inverse(const Cplx* __restrict__ hat, double* __restrict__ phi,
+                                                               int nx, int np, int periodic_y, const Cplx* tw);
+__global__ void k_mixed_efield(const double* __restrict__ phi, double* __restrict__ E, int nx, int ny, double dx,
+                               double dy, int periodic_x, int periodic_y);
+__global__ void k_dir_rhs(const double* __restrict__ rho, double* __restrict__ u, int nx, int ny, int nz3, double eps,
+                          double idx2, double idy2, double left, double right, double bottom, double top);
+__global__ void __launch_bounds__(kFftThreads) k_dst_lines(double* __restrict__ u, int M, long long stride, int lines_a,
+                                                           long long stride_a, long long stride_b, const Cplx* tw);
+__global__ void k_dir_divide(double* __restrict__ u, int Mx, int My, int Mz, double idx2, double idy2, double idz2,
+                             double scale);
+__global__ void k_dir_assemble(const double* __restrict__ u, double* __restrict__ phi, int nx, int ny, int nz3,
+                               double left, double right, double bottom, double top);
+
 struct SimND {
     apic_config_nd cfg{};
     std::string last_error;
@@ -1385,10 +1515,26 @@ struct SimND {
         require(c.dims == 2 || c.dims == 3, "dims must be 2 or 3");
         require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
         fp32 = c.precision == APIC_FP32;
+        walls = c.wall_axis[0] != 0 || c.wall_axis[1] != 0;
+        if (walls) {
+            require(c.dims == 2, "walls are supported on 2D meshes", APIC_ERR_UNSUPPORTED);
+            require(!fp32, "2D runs with walls use the FP64 particle form", APIC_ERR_UNSUPPORTED);
+            for (int k = 0; k < 4; ++k) {
+                require(c.particle_boundary[k] >= 0 && c.particle_boundary[k] <= 3, "unknown particle boundary");
+                require(std::isfinite(c.wall_potential[k]), "wall potentials must be finite");
+            }
+        }
         for (int a = 0; a < c.dims; ++a) {
             require(c.n[a] >= 3, "mesh extents must be at least 3");
-            require(pow2(c.n[a]) && c.n[a] <= (size_t)kMaxLine,
-                    "periodic device meshes need power-of-two extents up to 1024", APIC_ERR_UNSUPPORTED);
+            const bool wall = walls && c.wall_axis[a];
+            if (!wall)
+                require(pow2(c.n[a]) && c.n[a] <= (size_t)kMaxLine,
+                        "periodic device meshes need power-of-two extents up to 1024", APIC_ERR_UNSUPPORTED);
+            else if (c.wall_axis[0] && c.wall_axis[1])
+                require(pow2(c.n[a] - 1) && 2 * (c.n[a] - 1) <= (size_t)kMaxLine,
+                        "walls on every side need extents of 2^k + 1 nodes up to 513", APIC_ERR_UNSUPPORTED);
+            else
+                require(c.n[a] <= 65536, "the wall axis allows up to 65536 nodes", APIC_ERR_UNSUPPORTED);
             require(std::isfinite(c.length[a]) && c.length[a] > 0, "domain lengths must be positive and finite");
         }
         require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
@@ -1414,7 +1560,8 @@ struct SimND {
         for (int a = 0; a < 3; ++a) {
             p.n[a] = a < c.dims ? (int)c.n[a] : 1;
             p.L[a] = a < c.dims ? c.length[a] : 1.0;
-            p.d[a] = p.L[a] / (double)p.n[a];  // Mesh2D/Mesh3D periodic dx, src/Mesh2D.cpp:59-62
+            // Mesh2D/Mesh3D dx: L / n periodic, L / (n - 1) on a wall axis, src/Mesh2D.cpp:57-62
+            p.d[a] = p.L[a] / (double)(walls && a < 2 && c.wall_axis[a] ? p.n[a] - 1 : p.n[a]);
             p.B[a] = c.magnetic_field[a];
             N *= (size_t)p.n[a];
             if (a < c.dims) cellvol *= p.d[a];
@@ -1449,7 +1596,7 @@ struct SimND {
             require(std::isfinite(S.mass) && S.mass > 0, "species mass must be positive and finite");
             require(S.capacity > 0 && S.capacity < (1ull << 31), "species capacity out of range");
             const double w = c.dims == 2 ? S.weight / depth : S.weight;  // Species2D::deposit_charge
-            bound += (double)S.capacity * std::fabs(S.charge * w) / cellvol;
+            bound += (double)S.capacity * std::fabs(S.charge * w) / cellvol * (walls ? 4.0 : 1.0);
         }
         const int bits = bound > 0 ? (int)std::floor(61.0 - std::log2(bound)) : 0;
         p.rho_scale = std::ldexp(1.0, bits);
@@ -1483,10 +1630,15 @@ struct SimND {
             for (int a = 0; a < 3; ++a) D.sb[a] = (float)(2.0 * hq * c.magnetic_field[a] / (1.0 + t2));
             for (int a = 0; a < 3; ++a) D.drift[a] = a < c.dims ? (float)(c.dt / p.d[a]) : 0.0f;
             D.dep_fixed = (float)(D.dep * p.rho_scale);
+            D.index = s;
         }
         solver.allocs = &allocations;
         solver.stream = stream;
-        solver.setup(c.dims, c.n, c.length, p.eps, p.inv_rho_scale);
+        if (walls) {
+            setup_walls(c);
+        } else {
+            solver.setup(c.dims, c.n, c.length, p.eps, p.inv_rho_scale);
+        }
         p.E = solver.F.E;
         p.rho_acc = solver.F.rho_acc;
         if (c.profile_rows) {  // copied: the caller's arrays may go away after create
@@ -1574,7 +1726,10 @@ struct SimND {
             APIC_CUDA(cudaGetLastError());
             return;
         }
-        if (cfg.dims == 2) {
+        if (cfg.dims == 2 && walls) {
+            if (boris) k_push<2, true, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
+            else k_push<2, false, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
+        } else if (cfg.dims == 2) {
             if (boris) k_push<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
             else k_push<2, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
         } else {
@@ -1632,6 +1787,7 @@ struct SimND {
         require(n <= cfg.species[s].capacity, "initial particle count exceeds max_particles_per_species",
                 APIC_ERR_CAPACITY);
         SpeciesND& S = sp[s];
+        if (S.alive && n) APIC_CUDA(cudaMemsetAsync(S.alive, 1, n, stream));
         const int b = buf[s];
         const size_t bytes = n * sizeof(double);
         for (int a = 0; a < cfg.dims; ++a)
@@ -1666,9 +1822,123 @@ struct SimND {
         initialized = false;
     }
 
+    // ---- 2D walls: persistent solve scratch on the run's stream ----
+    bool walls = false;
+    int wall_mode = 0;  // 1: one wall axis (mixed solve), 2: walls on every side
+    int periodic_axis = 0;
+    double* w_planes = nullptr;  // Ex | Ey
+    double* w_mu = nullptr;
+    Cplx* w_hat = nullptr;
+    Cplx* w_tw = nullptr;
+    double* w_u = nullptr;
+    Cplx* w_dtw[2] = {nullptr, nullptr};
+
+    void setup_walls(const apic_config_nd& c) {
+        const size_t N = c.n[0] * c.n[1];
+        for (int k = 0; k < 4; ++k) {
+            const int kind = c.particle_boundary[k];
+            const bool wall = c.wall_axis[k >> 1] != 0;
+            // resolve_particle_boundary, src/Simulation2D.cpp:38-41 (Auto follows the field boundary)
+            p.pbc[k] = kind == 0 ? (wall ? 1 : 0) : (kind == 1 ? 1 : (kind == 2 ? 2 : 0));
+        }
+        p.wall[0] = c.wall_axis[0] != 0;
+        p.wall[1] = c.wall_axis[1] != 0;
+        p.losses = dalloc<unsigned long long>(4 * APIC_MAX_SPECIES);
+        const bool absorbing = p.pbc[0] == 1 || p.pbc[1] == 1 || p.pbc[2] == 1 || p.pbc[3] == 1;
+        for (int s = 0; s < c.nspecies; ++s)
+            sp[s].alive = absorbing ? dalloc<uint8_t>(c.species[s].capacity) : nullptr;
+        solver.F.dims = 2;
+        solver.F.rho_acc = dalloc<unsigned long long>(N);
+        solver.F.rho = dalloc<double>(N);
+        solver.F.phi = dalloc<double>(N);
+        solver.F.E = dalloc<double>(2 * N);
+        w_planes = dalloc<double>(2 * N);
+        const double twopi = 2.0 * 3.141592653589793;
+        if (p.wall[0] && p.wall[1]) {
+            wall_mode = 2;
+            const int M[2] = {(int)c.n[0] - 2, (int)c.n[1] - 2};
+            w_u = dalloc<double>((size_t)M[0] * M[1]);
+            for (int a = 0; a < 2; ++a) {
+                const int L2 = 2 * (M[a] + 1);
+                std::vector<Cplx> tw(L2);
+                for (int k = 0; k < L2; ++k) tw[k] = {std::cos(twopi * k / L2), -std::sin(twopi * k / L2)};
+                w_dtw[a] = dalloc<Cplx>(L2);
+                APIC_CUDA(cudaMemcpyAsync(w_dtw[a], tw.data(), L2 * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
+            }
+            APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)(3 * kMaxLine * sizeof(Cplx))));
+        } else {
+            wall_mode = 1;
+            periodic_axis = p.wall[0] ? 1 : 0;
+            const size_t np = c.n[periodic_axis];
+            w_mu = dalloc<double>(N);
+            w_hat = dalloc<Cplx>(N);
+            std::vector<Cplx> tw(np);
+            for (size_t k = 0; k < np; ++k) tw[k] = {std::cos(twopi * k / np), -std::sin(twopi * k / np)};
+            w_tw = dalloc<Cplx>(np);
+            APIC_CUDA(cudaMemcpyAsync(w_tw, tw.data(), np * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
+            const size_t smem = 3 * np * sizeof(Cplx);
+            APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        }
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // FieldSolver::solve(Mesh2D&) with walls, src/FieldSolver.cpp:389-397: the
+    // mixed spectral-tridiagonal solve, or the direct sine-transform solve of
+    // the system the reference's SOR iterates on; E by differences.
+    void solve_walls() {
+        const int nx = p.n[0], ny = p.n[1];
+        const size_t N = (size_t)nx * ny;
+        const unsigned g = (unsigned)std::min<size_t>((N + 255) / 256, 4096);
+        const double* pot = cfg.wall_potential;
+        k_walls_rho<<<g, 256, 0, stream>>>(solver.F.rho_acc, solver.F.rho, N, p.inv_rho_scale);
+        const double dx = p.d[0], dy = p.d[1];
+        if (wall_mode == 1) {
+            const int py = periodic_axis == 1;
+            const int nd = py ? nx : ny, np = py ? ny : nx;
+            const double hd = py ? dx : dy, hp = py ? dy : dx;
+            const double lo = py ? pot[0] : pot[2], hi = py ? pot[1] : pot[3];
+            const size_t smem = 3 * (size_t)np * sizeof(Cplx);
+            k_mixed_forward<<<(unsigned)nd, kFftThreads, smem, stream>>>(solver.F.rho, w_hat, nx, np, py, w_tw);
+            k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, stream>>>(w_hat, w_mu, nd, np, 1.0 / (hd * hd),
+                                                                              1.0 / (hp * hp), p.eps, lo, hi);
+            k_mixed_inverse<<<(unsigned)nd, kFftThreads, smem, stream>>>(w_hat, solver.F.phi, nx, np, py, w_tw);
+            k_mixed_efield<<<g, 256, 0, stream>>>(solver.F.phi, w_planes, nx, ny, dx, dy, py ? 0 : 1, py);
+        } else {
+            const int Mx = nx - 2, My = ny - 2;
+            const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy);
+            k_dir_rhs<<<g, 256, 0, stream>>>(solver.F.rho, w_u, nx, ny, 1, p.eps, idx2, idy2, pot[0], pot[1], pot[2],
+                                             pot[3]);
+            const int M[2] = {Mx, My};
+            auto dst_axis = [&](int a) {
+                const long long stride = a == 0 ? 1 : Mx, stride_a = a == 0 ? Mx : 1, stride_b = (long long)Mx * My;
+                const int lines_a = a == 0 ? My : Mx;
+                const size_t smem = 3 * (size_t)(2 * (M[a] + 1)) * sizeof(Cplx);
+                k_dst_lines<<<(unsigned)lines_a, kFftThreads, smem, stream>>>(w_u, M[a], stride, lines_a, stride_a,
+                                                                               stride_b, w_dtw[a]);
+            };
+            dst_axis(0);
+            dst_axis(1);
+            const double scale = (2.0 / (double)(Mx + 1)) * (2.0 / (double)(My + 1));
+            k_dir_divide<<<g, 256, 0, stream>>>(w_u, Mx, My, 1, idx2, idy2, 0.0, scale);
+            dst_axis(0);
+            dst_axis(1);
+            k_dir_assemble<<<g, 256, 0, stream>>>(w_u, solver.F.phi, nx, ny, 1, pot[0], pot[1], pot[2], pot[3]);
+            k_mixed_efield<<<g, 256, 0, stream>>>(solver.F.phi, w_planes, nx, ny, dx, dy, 0, 0);
+        }
+        k_walls_interleave<<<g, 256, 0, stream>>>(w_planes, solver.F.E, N);
+        APIC_CUDA(cudaGetLastError());
+    }
+
+    void solve_fields() {
+        if (walls) solve_walls();
+        else solver.solve();
+    }
+
     void deposit_and_solve() {
         for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushDepositOnly>(s);
-        solver.solve();
+        solve_fields();
     }
 
     void initialize() {
@@ -1708,7 +1978,7 @@ struct SimND {
         for (int s = 0; s < cfg.nspecies; ++s)
             if (sort_mask >> s & 1u) sort_species(s);
         for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
-        solver.solve();
+        solve_fields();
     }
 
     void launch_step_graph(unsigned sort_mask) {
@@ -1741,7 +2011,7 @@ struct SimND {
         for (size_t it = 0; it < nsteps; ++it) {
             unsigned sort_mask = 0;
             for (int s = 0; s < cfg.nspecies; ++s)
-                if (since_sort[s] >= species_interval[s] && sp[s].n) sort_mask |= 1u << s;
+                if (!walls && since_sort[s] >= species_interval[s] && sp[s].n) sort_mask |= 1u << s;
             for (int s = 0; s < cfg.nspecies; ++s) {
                 if (since_sort[s] < species_interval[s]) continue;
                 since_sort[s] = 0;
@@ -1764,7 +2034,7 @@ struct SimND {
                 APIC_CUDA(cudaEventRecord(ev.b, stream));
                 for (int s = 0; s < cfg.nspecies; ++s) launch_push<kPushStep>(s);
                 APIC_CUDA(cudaEventRecord(ev.c, stream));
-                solver.solve();
+                solve_fields();
                 APIC_CUDA(cudaEventRecord(ev.d, stream));
                 ev.sorted = sort_mask != 0;
                 events.push_back(ev);
@@ -1827,6 +2097,25 @@ struct SimND {
         return n;
     }
 
+    void read_alive(int s, size_t cap, uint8_t* alive) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        const size_t n = sp[s].n;
+        require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
+        sync();
+        if (sp[s].alive) APIC_CUDA(cudaMemcpyAsync(alive, sp[s].alive, n, cudaMemcpyDeviceToHost, stream));
+        else std::memset(alive, 1, n);
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    void read_losses(int s, uint64_t* out) {
+        require(s >= 0 && s < cfg.nspecies, "species index out of range");
+        sync();
+        unsigned long long h[4] = {0, 0, 0, 0};
+        if (p.losses) APIC_CUDA(cudaMemcpyAsync(h, p.losses + 4 * s, sizeof h, cudaMemcpyDeviceToHost, stream));
+        APIC_CUDA(cudaStreamSynchronize(stream));
+        for (int k = 0; k < 4; ++k) out[k] = h[k];
+    }
+
     void read_fields(double* rho, double* phi, double* E) {
         sync();
         const size_t N = ncells;
@@ -1852,7 +2141,8 @@ struct SimND {
             if (initialized) launch_push<kPushSync>(s);
             k_sample_nd<<<kSampleBlocks, 256, 0, stream>>>(sp[s], cfg.dims, sample_partial, sample_done, sample_out,
                                                            solver.F.E, solver.F.rho, (long long)ncells,
-                                                           0.5 * p.eps * vol, vol, s, s == cfg.nspecies - 1);
+                                                           0.5 * p.eps * vol, vol, s, s == cfg.nspecies - 1,
+                                                           p.wall[0], p.wall[1], p.n[0], p.n[1]);
             APIC_CUDA(cudaGetLastError());
         }
         double h[8];
@@ -2359,6 +2649,14 @@ int apic_simnd_read_particles(apic_sim_nd* sim, int species, size_t capacity, do
 int apic_simnd_read_fields(apic_sim_nd* sim, double* rho, double* phi, double* electric) {
     if (!sim) return APIC_ERR_INVALID;
     return guarded_nd(sim, [&] { sim->impl.read_fields(rho, phi, electric); });
+}
+int apic_simnd_read_alive(apic_sim_nd* sim, int species, size_t capacity, uint8_t* alive) {
+    if (!sim || !alive) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.read_alive(species, capacity, alive); });
+}
+int apic_simnd_boundary_losses(apic_sim_nd* sim, int species, uint64_t* absorbed) {
+    if (!sim || !absorbed) return APIC_ERR_INVALID;
+    return guarded_nd(sim, [&] { sim->impl.read_losses(species, absorbed); });
 }
 
 int apic_simnd_sample(apic_sim_nd* sim, apic_sample_nd* out) {

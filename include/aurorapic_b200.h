@@ -376,6 +376,16 @@ typedef struct {
     size_t profile_rows;
     const double* profile_coordinates;  /* profile_rows values */
     const double* profile_values;       /* profile_rows x (Bx, By, Bz) */
+    /* 2D walls (Simulation2DConfig boundary_x / boundary_y, boundary_config, particle_boundary_config,
+       include/pic/Simulation2D.hpp:118-135): wall_axis[a] = 1 makes axis a a Dirichlet axis whose n[a]
+       counts nodes (spacing length / (n - 1)); one wall axis solves by FFT along the periodic axis and
+       a tridiagonal sweep per mode, two by a direct sine-transform solve (extents 2^k + 1).  Sides are
+       left, right, bottom, top.  particle_boundary: 0 auto (periodic on a periodic axis, absorbing on
+       a wall axis), 1 absorbing, 2 reflecting, 3 periodic.  FP64 form; particles are not re-sorted;
+       absorbed particles stay in place, flagged dead (apic_simnd_read_alive). */
+    int wall_axis[2];
+    double wall_potential[4];
+    int particle_boundary[4];
 } apic_config_nd;
 
 /* DiagnosticSample2D / DiagnosticSample3D, src/Diagnostics.cpp:111-137, :205-232 */
@@ -427,6 +437,12 @@ APIC_EXPORT int apic_simnd_read_particles(apic_sim_nd* sim, int species, size_t 
                                           double* v, double* v_half, size_t* n);
 /* Mesh2D/Mesh3D rho(), phi(), electric_{x,y,z}() (E is [dims][N]). */
 APIC_EXPORT int apic_simnd_read_fields(apic_sim_nd* sim, double* rho, double* phi, double* electric);
+/* Particle::alive of a 2D run with walls (1 for every particle without absorbing sides), in the
+ * order of apic_simnd_read_particles. */
+APIC_EXPORT int apic_simnd_read_alive(apic_sim_nd* sim, int species, size_t capacity, uint8_t* alive);
+/* species_boundary_losses()[species] (BoundaryLoss2D, include/pic/Diagnostics.hpp:27-32):
+ * absorbed left, right, bottom, top. */
+APIC_EXPORT int apic_simnd_boundary_losses(apic_sim_nd* sim, int species, uint64_t* absorbed);
 APIC_EXPORT int apic_simnd_sample(apic_sim_nd* sim, apic_sample_nd* out);
 APIC_EXPORT int apic_simnd_cuda_stream(apic_sim_nd* sim, void** stream);
 APIC_EXPORT int apic_simnd_set_kernel_timing(apic_sim_nd* sim, int enable);

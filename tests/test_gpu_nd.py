@@ -1,6 +1,8 @@
 """Parity of the device 2D3V / 3D3V periodic step against the CPU oracle
 (itself bit-exact with Simulation2D / Simulation3D), through the C ABI.
 FP64 form: particle state and fields within 1e-12 relative (max-norm)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -351,3 +353,50 @@ def test_dirichlet_solve_against_exact_and_reference_sor(n, L, pot):
 def test_dirichlet_solve_rejects_other_extents():
     with pytest.raises(apic.ApicError, match="2\\^k \\+ 1"):
         apic.field_solve_dirichlet_nd((16, 9), (1.0, 1.0), 1.0, np.zeros(16 * 9))
+
+
+# ---- 2D runs with walls ---------------------------------------------------------
+
+WALL_SPECIES = [(-1.0, 1.0, 0.05, 400), (1.0, 50.0, 0.05, 400)]
+
+
+def _walls_pair(name):
+    from golden.make_golden import WALL_CASES
+    n, B, d, pot, pb = WALL_CASES[name]
+    f = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"{name}.npz"))
+    # the device's particle-boundary codes: 0 auto, 1 absorbing, 2 reflecting, 3 periodic
+    dev_pb = [3 if k == 0 else k for k in pb]
+    cfg = apic.config_nd(dims=2, n=n, length=(4.0, 2.0), dt=0.1, magnetic_field=B,
+                         species=[(q, m, w, cap) for q, m, w, cap in WALL_SPECIES], walls=(d, pot, dev_pb))
+    dev = apic.SimulationND(cfg)
+    ora = po.SimND(2, n, (4.0, 2.0), 0.1, 1.0, B, [(q, m, w) for q, m, w, _ in WALL_SPECIES])
+    ora.set_walls(d, pot, pb)
+    for k in range(2):
+        pos, v, vh = f[f"init_s{k}_pos"], f[f"init_s{k}_v"], f[f"init_s{k}_vh"]
+        dev.load(k, pos[:2], v, vh)
+        ora.load(k, pos, v, vh)
+    dev.resume(0.0, 0)
+    ora.initialize_fields()
+    return dev, ora, f
+
+
+@pytest.mark.parametrize("name,tol", [("sim2d_walls_mixed", 1e-12), ("sim2d_walls_dirichlet", 1e-6)])
+def test_2d_walls_against_oracle(name, tol):
+    """2D runs with walls on the device against the oracle (bit-exact with the
+    reference): one wall axis (mixed solve) within 1e-12; walls on every side
+    within 1e-6, since the device solves the discrete system directly while the
+    reference's SOR stops at a 1e-11 update (about 1e-8 in the potential).
+    Absorbed particles and the per-side loss counts exact."""
+    dev, ora, f = _walls_pair(name)
+    dev.step(25)
+    ora.step(25)
+    for k in range(2):
+        al, lo = ora.alive_losses(k)
+        assert np.array_equal(dev.alive(k), al), (name, k)
+        assert np.array_equal(dev.boundary_losses(k), lo), (name, k)
+        dpos, _, dvh = dev.particles(k)
+        opos, _, ovh = ora.particles(k)
+        keep = al == 1
+        assert rel_max(dpos[:2][:, keep], opos[:2][:, keep]) < tol, (name, k)
+        assert rel_max(dvh[:, keep], ovh[:, keep]) < tol, (name, k)
+    assert f["losses_s0"].sum() > 0
