@@ -76,10 +76,11 @@ public:
     explicit Simulation(const Config& cfg) {
         if (int rc = apic_sim1d_create(&cfg, &h_); rc != APIC_OK) raise(rc, apic_sim1d_last_error(nullptr));
         nspecies_ = cfg.nspecies;
+        nx_ = cfg.nx;
     }
     Simulation(const Simulation&) = delete;
     Simulation& operator=(const Simulation&) = delete;
-    Simulation(Simulation&& o) noexcept : h_(std::exchange(o.h_, nullptr)), nspecies_(o.nspecies_) {}
+    Simulation(Simulation&& o) noexcept : h_(std::exchange(o.h_, nullptr)), nspecies_(o.nspecies_), nx_(o.nx_) {}
     ~Simulation() { apic_sim1d_destroy(h_); }
 
     /* Species::particles() as loaded before initialize(). */
@@ -117,12 +118,44 @@ public:
     std::size_t step_count() const { return (std::size_t)apic_sim1d_step_count(h_); }
     apic_sim1d* handle() const { return h_; }
 
+    /* Config::spatial_average / phase_eedf, and the per-species electric-work
+     * ledger: both before initialize(). */
+    void enable_spatial_average(const apic_spatial_average1d& sa) {
+        check(apic_sim1d_enable_spatial_average(h_, &sa));
+    }
+    void enable_power_transfer() { check(apic_sim1d_enable_power_transfer(h_)); }
+    /* species_power_transfer()[s].electric_work, include/pic/Simulation.hpp:77-81 */
+    double electric_work(int species) const {
+        double w = 0.0;
+        check(apic_sim1d_power_transfer(h_, species, &w));
+        return w;
+    }
+    /* spatial_collision_energy_sums()[channel] (phase -1) or its phase slice,
+     * include/pic/Simulation.hpp:86-93 */
+    std::vector<double> spatial_collision_energy(int channel, int phase = -1) const {
+        return spatial_sums(APIC_SA_COLLISION_ENERGY, channel, phase);
+    }
+    /* the per-node sums behind the spatial-average output (apic_sim1d_spatial_sums) */
+    std::vector<double> spatial_sums(int quantity, int index, int phase = -1) const {
+        std::vector<double> out(nx_hint());
+        check(apic_sim1d_spatial_sums(h_, quantity, index, phase, out.data()));
+        return out;
+    }
+    /* phase_eedf_accumulators()[phase][region] without its histogram */
+    apic_phase_eedf1d phase_eedf(int phase, int region, std::vector<double>* histogram = nullptr) const {
+        apic_phase_eedf1d e{};
+        check(apic_sim1d_phase_eedf(h_, phase, region, &e, histogram ? histogram->data() : nullptr));
+        return e;
+    }
+
 private:
     void check(int rc) const {
         if (rc != APIC_OK) raise(rc, apic_sim1d_last_error(h_));
     }
+    std::size_t nx_hint() const { return nx_; }
     apic_sim1d* h_ = nullptr;
     int nspecies_ = 0;
+    std::size_t nx_ = 0;
 };
 
 /* ---- pic::Simulation2D / Simulation3D (periodic) ------------------------------- */
