@@ -186,6 +186,7 @@ def lib() -> C.CDLL:
     L.apic_sim1d_resume.argtypes = [C.c_void_p, C.c_double, C.c_uint64]
     L.apic_sim1d_step.argtypes = [C.c_void_p, C.c_size_t]
     L.apic_sim1d_synchronize.argtypes = [C.c_void_p]
+    L.apic_sim1d_set_wait_limit.argtypes = [C.c_void_p, C.c_double]
     L.apic_sim1d_count.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t)]
     L.apic_sim1d_read_particles.argtypes = [C.c_void_p, C.c_int, C.c_size_t, _DP, _DP, _DP, _DP, _DP,
                                             C.POINTER(C.c_size_t)]
@@ -328,6 +329,9 @@ class Simulation1D:
 
     def synchronize(self):
         _check(lib().apic_sim1d_synchronize(self.h), self.h)
+
+    def set_wait_limit(self, seconds):
+        _check(lib().apic_sim1d_set_wait_limit(self.h, seconds), self.h)
 
     def count(self, species) -> int:
         n = C.c_size_t()

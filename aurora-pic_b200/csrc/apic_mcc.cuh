@@ -76,7 +76,8 @@ __device__ inline int upper_bound_indexed(const MccChannelDev& c, double energy)
     int lo = 0, hi = c.rows;
     if (ix.nbins > 0) {
         const double t = (log2(energy) - ix.lmin) * ix.inv_width;
-        const int b = t < -1.0 ? -1 : (t > (double)ix.nbins ? ix.nbins : (int)floor(t));
+        // (a NaN energy takes the whole table: the search stays inside it)
+        const int b = !(t >= -1.0) ? -1 : (t > (double)ix.nbins ? ix.nbins : (int)floor(t));
         lo = b >= 1 ? (int)__ldg(ix.first_gt + (b - 1)) : 0;
         hi = b + 2 <= ix.nbins ? (int)__ldg(ix.first_gt + (b + 2)) : c.rows;
     }

@@ -194,7 +194,9 @@ __device__ __forceinline__ Cic cic_periodic(double x, double L, double dx, int n
 }
 
 __device__ __forceinline__ Cic cic_dirichlet(double x, double L, double dx, int nx) {
-    const double xp = x < 0.0 ? 0.0 : (L < x ? L : x);  // std::clamp
+    // std::clamp (a NaN position, already flagged as non-finite, lands on the
+    // left wall so that every index stays inside the grid)
+    const double xp = !(x >= 0.0) ? 0.0 : (L < x ? L : x);
     const double g = xp / dx;
     double fl = floor(g);
     const double lim = (double)(nx - 2);
@@ -405,6 +407,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                     const MccModelDev& M = p.model[S.model];
                     // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
                     const double s2 = vc[k] * vc[k] + vy[k] * vy[k] + vz[k] * vz[k];
+                    if (!isfinite(s2)) {  // NullCollisionModel rejects non-finite velocities, src/Collision.cpp:910-916
+                        atomicOr(&st->error, kErrNonFinite);
+                        continue;
+                    }
                     if (!(s2 <= M.v_safe2) && !frequency_bound_ok(M, sqrt(s2))) atomicOr(&st->error, kErrMajorant);
                     PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
                     const uint64_t d0 = rng.next();
@@ -530,7 +536,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                     atomicAdd(&st->lost_energy[s][side], e);
                     keep[k] = false;
                 }
-                if (!isfinite(x[k]) || !isfinite(vh[k])) atomicOr(&st->error, kErrNonFinite);
+                if (!isfinite(x[k]) || !isfinite(vh[k])) {
+                    // flagged and dropped: a non-finite particle deposits nothing
+                    atomicOr(&st->error, kErrNonFinite);
+                    keep[k] = false;
+                }
             }
             if ((mode & kModeDeposit) && keep[k]) {
                 const Cic d = cic<DIRICHLET>(x[k], p);
@@ -1351,6 +1361,7 @@ struct Sim1D {
     double time = 0.0;
     uint64_t step = 0;
     double neutral_stddev[kMaxModels] = {0, 0, 0, 0};
+    double wait_limit_s = 600.0;  // longest host wait for the handle's stream
 
     template <class T>
     T* dalloc(size_t count) {
@@ -1989,7 +2000,7 @@ struct Sim1D {
     }
 
     int sync_status() {
-        const cudaError_t e = bounded_wait(stream, 600.0);
+        const cudaError_t e = bounded_wait(stream, wait_limit_s);
         if (e == cudaErrorNotReady) throw Error(APIC_ERR_TIMEOUT, "device work did not complete in time");
         APIC_CUDA(e);
         unsigned word = 0;
@@ -2207,6 +2218,14 @@ int apic_sim1d_step_group(apic_sim1d* const* sims, size_t n, size_t nsteps) {
 int apic_sim1d_synchronize(apic_sim1d* sim) {
     if (!sim) return APIC_ERR_INVALID;
     return guarded(sim, [&] { sim->impl.sync_status(); });
+}
+
+int apic_sim1d_set_wait_limit(apic_sim1d* sim, double seconds) {
+    if (!sim) return APIC_ERR_INVALID;
+    return guarded(sim, [&] {
+        apic::require(std::isfinite(seconds) && seconds > 0.0, "wait limit must be positive and finite");
+        sim->impl.wait_limit_s = seconds;
+    });
 }
 
 int apic_sim1d_count(apic_sim1d* sim, int species, size_t* n) {

@@ -941,6 +941,10 @@ __global__ void k_unpermute(const unsigned* id, const double* src, double* dst, 
 enum : int { kFwdFromRho = 0, kFwdInPlace = 1, kFwdMulInv = 2, kInvInPlace = 3, kInvToFields = 4 };
 constexpr int kFftThreads = 256;             // threads per FFT tile
 constexpr size_t kFftTileBytes = 100 * 1024;  // shared-memory budget of one tile (lines per tile follow)
+// Largest dynamic shared memory of an FFT tile: four line buffers plus the
+// twiddles fit the tile budget whenever a tile holds more than one line, and a
+// single 1024-point line takes 4 x 16 KB + 16 KB.
+constexpr size_t kFftSmemMax = kFftTileBytes > 5 * 1024 * 16 ? kFftTileBytes : 5 * 1024 * 16;
 
 struct FftPass {
     int n, log2n;
@@ -1322,6 +1326,13 @@ __global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double
 static bool pow2(size_t v) { return v >= 2 && (v & (v - 1)) == 0; }
 static int ilog2(size_t v) { int k = 0; while ((size_t(1) << k) < v) ++k; return k; }
 
+// Raises the dynamic shared-memory limit of every FFT / wall-solve kernel, once
+// per device, to a fixed bound that covers every tile any mesh here uses.  The
+// limit is a property of the kernel function shared by every simulation and
+// solve in the process, so it is never lowered to one mesh's need (a later
+// small mesh would otherwise make an earlier large mesh's launches fail).
+void ensure_solver_attributes();
+
 struct Solver {
     FieldsND F{};
     FftPass px{}, py{}, pz{};    // paired passes (four line buffers)
@@ -1413,11 +1424,8 @@ struct Solver {
         if (dims == 3) pz.tw = F.nz == F.nx ? px.tw : (F.nz == F.ny ? py.tw : twiddles(F.nz));
         smem_pair = std::max(smem_of(px, kFwdMulInv), smem_of(py, kFwdMulInv));
         if (dims == 3) smem_pair = std::max(smem_pair, smem_of(pz, kFwdMulInv));
-        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdFromRho>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
-        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
-        APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
-        APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
-        APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pair));
+        require(smem_pair <= kFftSmemMax, "FFT tile exceeds the shared-memory bound", APIC_ERR_UNSUPPORTED);
+        ensure_solver_attributes();
     }
 
     size_t smem_of(const FftPass& f, int mode) const {
@@ -1460,6 +1468,30 @@ __global__ void k_dir_divide(double* __restrict__ u, int Mx, int My, int Mz, dou
                              double scale);
 __global__ void k_dir_assemble(const double* __restrict__ u, double* __restrict__ phi, int nx, int ny, int nz3,
                                double left, double right, double bottom, double top);
+
+namespace {
+std::mutex g_attr_mu;
+bool g_attr_done[64] = {};
+}  // namespace
+
+void ensure_solver_attributes() {
+    int dev = 0;
+    APIC_CUDA(cudaGetDevice(&dev));
+    require(dev >= 0 && dev < 64, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_attr_mu);
+    if (g_attr_done[dev]) return;
+    const int fft = (int)kFftSmemMax;
+    APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdFromRho>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    const int lines = (int)(3 * kMaxLine * sizeof(Cplx));  // three line buffers of the longest extent
+    APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
+    APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
+    APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
+    g_attr_done[dev] = true;
+}
 
 struct SimND {
     apic_config_nd cfg{};
@@ -1865,8 +1897,7 @@ struct SimND {
                 w_dtw[a] = dalloc<Cplx>(L2);
                 APIC_CUDA(cudaMemcpyAsync(w_dtw[a], tw.data(), L2 * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
             }
-            APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(3 * kMaxLine * sizeof(Cplx))));
+            ensure_solver_attributes();
         } else {
             wall_mode = 1;
             periodic_axis = p.wall[0] ? 1 : 0;
@@ -1877,9 +1908,7 @@ struct SimND {
             for (size_t k = 0; k < np; ++k) tw[k] = {std::cos(twopi * k / np), -std::sin(twopi * k / np)};
             w_tw = dalloc<Cplx>(np);
             APIC_CUDA(cudaMemcpyAsync(w_tw, tw.data(), np * sizeof(Cplx), cudaMemcpyHostToDevice, stream));
-            const size_t smem = 3 * np * sizeof(Cplx);
-            APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            ensure_solver_attributes();
         }
         APIC_CUDA(cudaStreamSynchronize(stream));
     }
@@ -2335,8 +2364,7 @@ static void solve_mixed_2d(const size_t* n, const double* length, int periodic_a
     APIC_CUDA(cudaMemcpyAsync(d_tw, tw.data(), np * sizeof(Cplx), cudaMemcpyHostToDevice, S.s));
     APIC_CUDA(cudaMemcpyAsync(d_rho, rho, N * sizeof(double), cudaMemcpyHostToDevice, S.s));
     const size_t smem = 3 * np * sizeof(Cplx);
-    APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ensure_solver_attributes();
     k_mixed_forward<<<(unsigned)nd, kFftThreads, smem, S.s>>>(d_rho, d_hat, (int)nx, (int)np, periodic_y, d_tw);
     k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, S.s>>>(d_hat, d_mu, (int)nd, (int)np, 1.0 / (hd * hd),
                                                                      1.0 / (hp * hp), permittivity, lower, upper);
@@ -2521,8 +2549,7 @@ static void solve_dirichlet_nd(int dims, const size_t* n, const double* length, 
     const unsigned g = (unsigned)std::min<size_t>((N + 255) / 256, 4096);
     k_dir_rhs<<<g, 256, 0, S.s>>>(d_rho, d_u, nx, ny, nz3, permittivity, idx2, idy2, side[0], side[1], side[2],
                                   side[3]);
-    APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)(3 * kMaxLine * sizeof(Cplx))));
+    ensure_solver_attributes();
     // axis a: element stride, then the two line axes (stride_a over lines_a, stride_b over the rest)
     auto dst_axis = [&](int a) {
         const long long sx = 1, sy = Mx, sz = (long long)Mx * My;
@@ -2783,8 +2810,23 @@ __global__ void k_noalloc_deinterleave(const double* E, int dims, long long N, d
 }  // namespace apic
 
 namespace {
-std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[64] = {};
+// A caller buffer of the allocation-free solve must be device (or managed)
+// memory of the current device: a host pointer would make the kernels fault.
+void require_device_buffer(const void* ptr, const char* name) {
+    cudaPointerAttributes a{};
+    const cudaError_t e = cudaPointerGetAttributes(&a, ptr);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw apic::Error(APIC_ERR_INVALID, std::string(name) + " is not a device pointer");
+    }
+    apic::require(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged,
+                  std::string(name) + " must be device or managed memory (got a host pointer)");
+    if (a.type == cudaMemoryTypeDevice) {
+        int dev = 0;
+        APIC_CUDA(cudaGetDevice(&dev));
+        apic::require(a.device == dev, std::string(name) + " belongs to another device than the current one");
+    }
+}
 }  // namespace
 
 extern "C" int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, const double* length,
@@ -2807,28 +2849,15 @@ extern "C" int apic_field_solve_periodic_nd_noalloc(int dims, const size_t* n, c
                       "allocation-free solve: mesh has " + std::to_string(N) + " points, the scratch array holds " +
                           std::to_string(kNoAllocMaxPoints),
                       APIC_ERR_CAPACITY);
-        int dev = 0;
-        APIC_CUDA(cudaGetDevice(&dev));
-        apic::require(dev >= 0 && dev < 64, "device index out of range");
+        require_device_buffer(d_rho, "d_rho");
+        require_device_buffer(d_phi, "d_phi");
+        require_device_buffer(d_electric, "d_electric");
+        // the scratch array's address in the current device's context, looked
+        // up on every call (cheap), so it stays valid after a device reset; and
+        // the FFT kernels' fixed shared-memory limit (set once per device)
         void* base = nullptr;
-        {
-            // once per device, with that device current: the scratch array's
-            // device address, and the shared-memory limit of the FFT kernels
-            std::lock_guard<std::mutex> lock(g_noalloc_mu);
-            if (!g_noalloc_ptr[dev]) {
-                void* p = nullptr;
-                APIC_CUDA(cudaGetSymbolAddress(&p, g_solve_scratch));
-                g_noalloc_ptr[dev] = p;
-            }
-            base = g_noalloc_ptr[dev];
-            // the FFT tiles below stay under 118 KB of shared memory
-            const int smem = 118 * 1024;
-            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdFromRho>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-            APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        }
+        APIC_CUDA(cudaGetSymbolAddress(&base, g_solve_scratch));
+        ensure_solver_attributes();
         unsigned char* bytes = static_cast<unsigned char*>(base);
         Cplx* W = reinterpret_cast<Cplx*>(bytes);
         Cplx* A = W + kNoAllocMaxPoints;

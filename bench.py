@@ -67,6 +67,10 @@ def parse():
     ap.add_argument("--ppc", type=int, default=None)
     ap.add_argument("--cells", type=int, default=None, help="cells per axis")
     ap.add_argument("--sort-interval", type=int, default=0, help="plasma: 0 = chosen by the autotuner")
+    ap.add_argument("--push-items", type=int, default=0, help="plasma FP32: particles per thread (0 = autotuned)")
+    ap.add_argument("--steps-per-launch", type=int, default=0, help="swarm: graph length (0 = autotuned)")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="ccp1d at N=1: skip the nested 2D3V / 3D3V / swarm-serving records")
     ap.add_argument("--no-autotune", action="store_true", help="skip the autotuner (fixed defaults)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -562,7 +566,7 @@ def bench_plasma(args, rank, dist):
     plan = W.plasma_plan(dims, cells=cells, ppc=args.ppc, seed=11 + 2 * rank)
     prec = apic.FP32 if args.precision == "fp32" else apic.FP64
     tuned = None
-    sort_interval, push_items = args.sort_interval or 16, 0
+    sort_interval, push_items = args.sort_interval or 16, args.push_items
     if not args.no_autotune and not args.sort_interval:
         from apic import autotune
         tuned = autotune.tune_plasma(plan, prec, steps=32)
@@ -790,8 +794,8 @@ def bench_swarm(args, rank, dist):
     free, _ = torch.cuda.mem_get_info()
     budget = int(min(64 << 30, 0.6 * free))
     rng = np.random.default_rng(5 + rank)
-    spl, tuned = 200, None
-    if not args.no_autotune:
+    spl, tuned = args.steps_per_launch or 200, None
+    if not args.no_autotune and not args.steps_per_launch:
         from apic import autotune
         sample = [_swarm_draw(rng, spec, W, k, 5_000_000) for k in range(12)]
         tuned = autotune.tune_swarm_server(gas, sample, prec, min(budget, 16 << 30))
@@ -906,6 +910,55 @@ def bench_swarm(args, rank, dist):
     }
 
 
+# The nested records of the default run: the other benchmark shapes with the
+# settings the autotuner picked for them on the B200 (sort interval and
+# particles per thread of the plasma decks, graph length of the swarm server),
+# a few timed steps each and a shorter CPU sample, so the whole default run
+# stays within a few minutes.
+OTHER_CONFIGS = {
+    "plasma2d": {"sort_interval": 8, "push_items": 4, "e2e_steps": 2},
+    "plasma3d": {"sort_interval": 8, "push_items": 1, "e2e_steps": 1},
+    "swarm": {"steps_per_launch": 100, "requests": 48, "mixed_requests": 16},
+}
+
+
+def bench_other_configs(args, rank, dist, world):
+    """The 2D3V (512^2 x 64 ppc), 3D3V (256^3 x 8 ppc) and swarm-serving
+    shapes measured the way their own --workload runs measure them, each with
+    its roofline, end-to-end figure, clocks and CPU baseline."""
+    out = {}
+    for wk, over in OTHER_CONFIGS.items():
+        a = argparse.Namespace(**vars(args))
+        a.workload, a.precision, a.no_autotune = wk, "fp32", True
+        a.steps = max(args.steps, 20)
+        a.warmup = max(args.warmup, 3)
+        for k, v in over.items():
+            setattr(a, k, v)
+        t0 = time.perf_counter()
+        try:
+            part = bench_swarm(a, rank, dist) if wk == "swarm" else bench_plasma(a, rank, dist)
+        except Exception as e:  # reported in the record, never fatal to the headline
+            out[wk] = {"error": f"{type(e).__name__}: {e}"}
+            continue
+        rec = {k: part[k] for k in ("value", "ms_per_step", "dtype", "config", "e2e", "roofline", "gpu_launches",
+                                    "clocks") if k in part}
+        rec["unit"] = "particle-steps/s"
+        rec["steps"], rec["warmup"] = a.steps, a.warmup
+        if "swarm" in part:
+            rec["swarm"] = part["swarm"]
+        rec["cpu_baseline"] = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                from apic import workloads as W
+                wl = None if wk == "swarm" else W.plasma_plan(2 if wk == "plasma2d" else 3)
+                rec["cpu_baseline"] = cpu_reference_sample(a, wl, min(args.cpu_seconds, 10.0), os.cpu_count() or 1)
+            except Exception as e:
+                rec["cpu_baseline"] = {"value": None, "error": str(e)}
+        rec["wall_s"] = time.perf_counter() - t0
+        out[wk] = rec
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -923,8 +976,11 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    others = None
     if args.workload == "ccp1d":
         part = bench_ccp1d(args, rank, dist)
+        if world == 1 and not args.no_other_configs:
+            others = bench_other_configs(args, rank, dist, world)
     elif args.workload == "swarm":
         part = bench_swarm(args, rank, dist)
     else:
@@ -958,6 +1014,8 @@ def main():
             b = dict(part["batched"])
             b["vs_single_run"] = b["value"] / part["value"]
             line["batched"] = b
+        if others:
+            line["configs"] = others
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

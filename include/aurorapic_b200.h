@@ -224,6 +224,11 @@ APIC_EXPORT int apic_sim1d_step_group(apic_sim1d* const* sims, size_t n, size_t 
 
 /* Waits (bounded) for the handle's stream and returns the device error word. */
 APIC_EXPORT int apic_sim1d_synchronize(apic_sim1d* sim);
+/* Longest time (seconds, default 600) a synchronising call waits for the
+ * handle's device work before it gives up with APIC_ERR_TIMEOUT; the work
+ * itself is not cancelled, and a later synchronising call waits again.  No
+ * reference counterpart (the reference's step() runs to completion). */
+APIC_EXPORT int apic_sim1d_set_wait_limit(apic_sim1d* sim, double seconds);
 
 /* Species::particles() read access.  Brings the state to the reference's
  * post-step() form (time-centred v) before copying. */
@@ -497,8 +502,11 @@ APIC_EXPORT int apic_field_solve_mixed_2d(const size_t* n, const double* length,
  * FFT work arrays live in a static device array inside the library (about
  * 5.8 MB, kept by every GPU that loads the library until the process exits),
  * so N = nx*ny*nz may not exceed 65536 (APIC_ERR_CAPACITY beyond) and each
- * extent must be a power of two up to 1024.  The first call on a device looks
- * up that array's device address; make it before any stream capture.  Work is
+ * extent must be a power of two up to 1024.  Buffers that are not device (or
+ * managed) memory of the current device are refused with APIC_ERR_INVALID.
+ * Every call looks up that array's address in the current device's context;
+ * the first call on a device also sets the FFT kernels' shared-memory limit
+ * there, so make it before any stream capture.  Work is
  * enqueued on `stream` (a cudaStream_t, NULL for the default stream) and the
  * call returns without waiting.  Every call shares the one array, so calls
  * whose work overlaps on the GPU (different streams, or different host

@@ -67,7 +67,7 @@ struct DiagnosticSample {  // include/pic/Diagnostics.hpp
 
 /* ---- pic::Simulation (1D) ----------------------------------------------------- */
 
-/* Config is the C struct itself: the adapter of INTEGRATION.md fills it from
+/* Config is the C struct itself: a reference-side adapter fills it from
  * pic::Config field by field. */
 using Config = apic_config1d;
 

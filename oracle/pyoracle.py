@@ -120,11 +120,21 @@ def spatial_average1d(interval=1, start_step=1, end_step=1, rf_frequency=0.0, rf
 SA_DENSITY, SA_VX, SA_VY, SA_VZ, SA_KINETIC, SA_POTENTIAL, SA_ELECTRIC, SA_ELECTRIC2, SA_COLLISION = range(9)
 
 
+def reference_tree_present() -> bool:
+    """Whether the reference's source tree is present on this host (the
+    Makefile knows where: APIC_REFERENCE or its default)."""
+    try:
+        out = subprocess.run(["make", "-s", "-C", HERE, "has-ref"], check=True, capture_output=True, text=True)
+    except (OSError, subprocess.CalledProcessError):
+        return False
+    return out.stdout.strip() == "yes"
+
+
 def ensure_built() -> None:
     """Build the C restatement (and the reference harness when the reference
     tree is present) with oracle/Makefile."""
     targets = ["oracle"]
-    if os.path.isdir(os.environ.get("APIC_REFERENCE", "/root/reference")):
+    if reference_tree_present():
         targets.append("ref")
     if not os.path.exists(ORACLE_SO) or ("ref" in targets and not os.path.exists(REF_SO)):
         subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)

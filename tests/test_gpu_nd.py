@@ -400,3 +400,19 @@ def test_2d_walls_against_oracle(name, tol):
         assert rel_max(dpos[:2][:, keep], opos[:2][:, keep]) < tol, (name, k)
         assert rel_max(dvh[:, keep], ovh[:, keep]) < tol, (name, k)
     assert f["losses_s0"].sum() > 0
+
+
+def test_small_solve_does_not_break_a_large_simulation():
+    """The FFT kernels' shared-memory limit belongs to the kernel functions and
+    is shared by every simulation in the process: a small stand-alone solve made
+    after a 512^2 simulation was created must leave that simulation steppable."""
+    plan = W.plasma_plan(2, cells=(512, 512), ppc=1, seed=4)
+    sim = apic.SimulationND(plan.config(precision=apic.FP64, sort_interval=16))
+    plan.load(sim)
+    sim.initialize()
+    rng = np.random.default_rng(9)
+    apic.field_solve_periodic_nd(2, (64, 64), (1.0, 1.0), 1.0, rng.standard_normal(64 * 64))
+    sim.step(2)
+    sim.synchronize()
+    assert sim.sample().step == 2
+    sim.close()

@@ -65,3 +65,24 @@ def test_noalloc_rejects_meshes_beyond_the_array():
     rc = fn(2, ns, Ls, 1.0, buf.data_ptr(), buf.data_ptr(), buf.data_ptr(), None)
     assert rc == 3  # APIC_ERR_CAPACITY
     assert b"scratch array holds 65536" in lib.apic_simnd_last_error(None)
+
+
+def test_noalloc_rejects_host_buffers():
+    """A host buffer (the older allocating API took host arrays) is refused
+    before any kernel could touch it."""
+    torch = pytest.importorskip("torch")
+    lib = apic.lib()
+    fn = lib.apic_field_solve_periodic_nd_noalloc
+    fn.argtypes = [C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.c_double, C.c_void_p, C.c_void_p,
+                   C.c_void_p, C.c_void_p]
+    host = np.zeros(2 * 64 * 64)
+    dev = torch.zeros(2 * 64 * 64, dtype=torch.float64, device="cuda")
+    ns = (C.c_size_t * 3)(64, 64, 1)
+    Ls = (C.c_double * 3)(1.0, 1.0, 1.0)
+    for args in ((host.ctypes.data, dev.data_ptr(), dev.data_ptr()),
+                 (dev.data_ptr(), host.ctypes.data, dev.data_ptr()),
+                 (dev.data_ptr(), dev.data_ptr(), host.ctypes.data)):
+        rc = fn(2, ns, Ls, 1.0, *args, None)
+        assert rc == 1, rc  # APIC_ERR_INVALID
+        assert b"device or managed memory" in lib.apic_simnd_last_error(None) or \
+            b"not a device pointer" in lib.apic_simnd_last_error(None)
