@@ -22,7 +22,7 @@ MAX_CHANNELS = 8
 
 PERIODIC, DIRICHLET = 0, 1
 NORMALIZED, SI = 0, 1
-FP64, FP32 = 0, 1
+FP64, FP32, FP32_STORAGE = 0, 1, 2
 ELASTIC, EXCITATION, IONIZATION, ATTACHMENT, CHARGE_EXCHANGE = range(5)
 ISOTROPIC, BACKWARD, HENYEY_GREENSTEIN = 0, 1, 2
 

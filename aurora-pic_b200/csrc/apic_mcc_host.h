@@ -11,6 +11,7 @@
 #include "aurorapic_b200.h"
 #include "apic_common.cuh"
 #include "apic_mcc.cuh"
+#include "apic_mcc32.cuh"
 
 namespace apic {
 
@@ -343,6 +344,57 @@ inline void build_model(const apic_mcc_model& m, double mass, DeviceArena& arena
     D.v_safe2 = D.v_safe < 0.0 ? -1.0 : std::nextafter(D.v_safe * D.v_safe, 0.0);
     build_safe_bins(m, mass, sd, arena, D);
     APIC_CUDA(cudaStreamSynchronize(arena.stream));  // host tables may be freed after this
+}
+
+// The single-precision copy of a model built by build_model (FP32 particle
+// form): tables rounded to float, the same bracket index, float constants.
+inline void build_model32(const apic_mcc_model& m, DeviceArena& arena, const MccModelDev& D, MccModel32& F) {
+    F = MccModel32{};
+    F.nch = D.nch;
+    F.shared_grid = D.shared_grid;
+    F.particle_mass = (float)D.particle_mass;
+    F.neutral_mass = (float)D.neutral_mass;
+    F.neutral_density = (float)D.neutral_density;
+    F.max_frequency = (float)D.max_frequency;
+    F.inv_max_frequency = (float)(1.0 / D.max_frequency);
+    F.neutral_stddev = (float)D.neutral_stddev;
+    F.com_mass = (float)D.com_mass;
+    // |v|^2 below which the FP64 safe speed holds, rounded down in float
+    F.v_safe2 = D.v_safe < 0.0 ? -1.0f : std::nextafter((float)std::min(D.v_safe * D.v_safe, 1e37), 0.0f);
+    const double total = D.particle_mass + D.neutral_mass;
+    F.m_frac = (float)(D.particle_mass / total);
+    F.n_frac = (float)(D.neutral_mass / total);
+    F.max_candidates = D.max_candidates;
+    auto narrow = [&](const double* x, size_t n) {
+        std::vector<float> f(n);
+        for (size_t i = 0; i < n; ++i) f[i] = (float)x[i];
+        const float* d = arena.upload(f.data(), n);
+        APIC_CUDA(cudaStreamSynchronize(arena.stream));  // the host vector dies here
+        return d;
+    };
+    for (int ci = 0; ci < m.nch; ++ci) {
+        const apic_mcc_channel& ch = m.ch[ci];
+        const MccChannelDev& C = D.ch[ci];
+        MccChannel32& G = F.ch[ci];
+        G.process = C.process;
+        G.angular = C.angular;
+        G.frame = C.frame;
+        G.threshold = (float)C.threshold;
+        G.secondary = C.secondary;
+        G.ion = C.ion;
+        G.rows = C.rows;
+        G.energy = narrow(ch.energy, ch.rows);
+        G.sigma = narrow(ch.sigma, ch.rows);
+        G.first_gt = C.index.first_gt;
+        G.nbins = C.index.nbins;
+        G.lmin = (float)C.index.lmin;
+        G.inv_width = (float)C.index.inv_width;
+        if (C.mu_rows) {
+            G.mu_rows = C.mu_rows;
+            G.mu_energy = narrow(ch.mean_cosine_energy, ch.mean_cosine_rows);
+            G.mu = narrow(ch.mean_cosine, ch.mean_cosine_rows);
+        }
+    }
 }
 
 }  // namespace apic

@@ -41,6 +41,7 @@
 
 #include "apic_common.cuh"
 #include "apic_mcc.cuh"
+#include "apic_mcc32.cuh"
 #include "apic_mcc_host.h"
 #include "apic_rng.cuh"
 
@@ -121,7 +122,15 @@ struct SpeciesDev {
     float* vh32[2];
     float* vy32[2];
     float* vz32[2];
-    double* stage;  // FP32 form: FP64 staging for host copies (capacity)
+    double* stage;  // FP32 forms: FP64 staging for host copies (capacity)
+    // FP32 cell form: the position as the index of the cell holding the
+    // particle (its left node) and the float offset in [0, 1] inside it; null
+    // in the other forms (which keep x in FP64)
+    int* cell[2];
+    float* off[2];
+    // FP32 cell form constants: q/m dt, q/(2m) dt, dt/dx, and the fixed-point
+    // charge of a whole particle on one node (q w / dx times the density scale)
+    float qmdt32, hqmdt32, dtdx32, dep32;
     // electric-work ledger: the time-centred v each particle had at the end of
     // its last step (double-buffered like the state); null unless enabled
     double* vold[2];
@@ -129,7 +138,8 @@ struct SpeciesDev {
 
 struct Params1D {
     int nspecies, vdim, dirichlet, nx;
-    int f32;  // FP32 particle form
+    int f32;  // FP32 velocities (both FP32 forms)
+    int c32;  // FP32 cell form: int32 cell + float offset positions, FP32 arithmetic
     double L, dx, inv_dx, dt, eps, rho_scale, inv_rho_scale;
     unsigned mode;
     uint64_t seed;
@@ -154,6 +164,10 @@ struct Params1D {
     double* coll_phase_acc;
     int coll_off[kMaxModels];  // first channel of each model in the channel numbering
     int ledger;                // electric-work ledger enabled (SpeciesDev::vold allocated)
+    // FP32 cell form: the collision models in single precision, and the FP64
+    // models in device memory for the (rare) exact frequency-bound check
+    MccModel32 model32[kMaxModels];
+    const MccModelDev* gmodel;
 };
 
 // ---- field gather / deposit (reference arithmetic) ----------------------
@@ -606,6 +620,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
     }
 }
 
+#include "pic1d_c32.cuh"
+
 // ---- post kernel: products, density, field solve -----------------------------
 
 struct Affine {
@@ -630,7 +646,7 @@ __host__ __device__ inline size_t post_smem_bytes(int nx, bool dirichlet) {
            (dirichlet ? (size_t)2 * nx * 8 : (size_t)2 * nx * 8 /* twiddles */ + (size_t)4 * nx * 8 /* spectra */);
 }
 
-template <int VDIM, bool DIRICHLET, bool F32>
+template <int VDIM, bool DIRICHLET, bool F32, bool C32 = false>
 __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned post) {
     using Sort = cub::BlockRadixSort<unsigned long long, kPostThreads, kPostItems, int>;
     using ScanU = cub::BlockScan<unsigned, kPostThreads>;
@@ -820,7 +836,15 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                 if (!flags[k]) continue;
                 const unsigned long long o = (unsigned long long)s_bstart[s] + ranks[k];
                 if (o >= S.capacity) { atomicOr(&st->error, kErrCapacity); continue; }
-                S.x[1][o] = bx[k];
+                if (C32) {
+                    int c;
+                    float f;
+                    position_to_cell<DIRICHLET>(bx[k], p, c, f);
+                    S.cell[1][o] = c;
+                    S.off[1][o] = f;
+                } else {
+                    S.x[1][o] = bx[k];
+                }
                 st_comp<F32>(S.vh[1], S.vh32[1], o, bvh[k]);
                 if (VDIM == 3) {
                     st_comp<F32>(S.vy[1], S.vy32[1], o, bv[k][1]);
@@ -1354,7 +1378,8 @@ struct Sim1D {
     DevState* st = nullptr;
     std::vector<void*> allocations;
     std::vector<std::vector<double>> tables;  // host copies (kept for safe_speed)
-    bool fp32 = false;      // FP32 particle form (APIC_FP32)
+    bool fp32 = false;      // FP32 velocities (APIC_FP32 and APIC_FP32_STORAGE)
+    bool c32 = false;       // FP32 cell form (APIC_FP32): cell + offset positions, FP32 arithmetic
     bool pending = false;   // collision part of the last step not yet applied
     bool initialized = false;
     int parity = 0;         // which of the two buffers holds the current state
@@ -1395,6 +1420,7 @@ struct Sim1D {
 
     void enable_spatial_average(const apic_spatial_average1d& a) {
         require(!initialized, "spatial averaging must be enabled before initialize() or resume()", APIC_ERR_STATE);
+        require(!c32, "spatial averaging runs in the FP64 and FP32_STORAGE forms", APIC_ERR_UNSUPPORTED);
         require(!sa.on, "spatial averaging is already enabled", APIC_ERR_STATE);
         validate_spatial_average(cfg, a);
         sa.cfg = a;
@@ -1449,6 +1475,7 @@ struct Sim1D {
     // particle's end-of-step v (one more FP64 array per buffer, 16 bytes of
     // traffic per particle-step) and runs the diagnostics pass instantiation.
     void enable_power_transfer() {
+        require(!c32, "the electric-work ledger runs in the FP64 and FP32_STORAGE forms", APIC_ERR_UNSUPPORTED);
         require(!initialized, "the electric-work ledger must be enabled before initialize() or resume()",
                 APIC_ERR_STATE);
         if (p.ledger) return;
@@ -1551,8 +1578,10 @@ struct Sim1D {
         require(std::isfinite(c.dt) && c.dt > 0, "simulation dt must be positive and finite");
         require(c.nspecies >= 1 && c.nspecies <= kMaxSpecies, "species count out of range");
         require(c.nmodels >= 0 && c.nmodels <= kMaxModels, "model count out of range");
-        require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
-        fp32 = c.precision == APIC_FP32;
+        require(c.precision == APIC_FP64 || c.precision == APIC_FP32 || c.precision == APIC_FP32_STORAGE,
+                "unknown precision");
+        fp32 = c.precision != APIC_FP64;
+        c32 = c.precision == APIC_FP32;
         const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
         require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
         int ndev = 0;
@@ -1567,6 +1596,7 @@ struct Sim1D {
         const bool dir = c.boundary == APIC_DIRICHLET;
         p.nspecies = c.nspecies;
         p.f32 = fp32 ? 1 : 0;
+        p.c32 = c32 ? 1 : 0;
         p.vdim = c.velocity_dimensions;
         p.dirichlet = dir;
         p.nx = (int)c.nx;
@@ -1603,6 +1633,10 @@ struct Sim1D {
             S.hqm = 0.5 * S.qm;
             S.qw = sp.charge * sp.weight;
             S.qwdx = sp.charge * sp.weight / p.dx;
+            S.qmdt32 = (float)(S.qm * c.dt);
+            S.hqmdt32 = (float)(S.hqm * c.dt);
+            S.dtdx32 = (float)(c.dt / p.dx);
+            S.dep32 = (float)(S.qwdx * p.rho_scale);
             S.mass = sp.mass;
             S.weight = sp.weight;
             S.model = -1;
@@ -1617,7 +1651,12 @@ struct Sim1D {
             S.chunk_surv = dalloc<unsigned>(maxr);
             const bool v3 = c.velocity_dimensions == 3;
             for (int b = 0; b < 2; ++b) {
-                S.x[b] = dalloc<double>(cap);
+                if (c32) {
+                    S.cell[b] = dalloc<int>(cap);
+                    S.off[b] = dalloc<float>(cap);
+                } else {
+                    S.x[b] = dalloc<double>(cap);
+                }
                 if (fp32) {
                     S.vh32[b] = dalloc<float>(cap);
                     S.vy32[b] = v3 ? dalloc<float>(cap) : nullptr;
@@ -1657,7 +1696,14 @@ struct Sim1D {
             neutral_stddev[mi] = p.model[mi].neutral_stddev;
             p.sp[m.species].model = mi;
             draw_threshold(m.max_frequency, c.dt, p.sp[m.species].cand_draw_min, p.sp[m.species].no_candidates);
+            if (c32) build_model32(m, arena, p.model[mi], p.model32[mi]);
             APIC_CUDA(cudaStreamSynchronize(stream));  // host tables may be freed after create
+        }
+        if (c32 && c.nmodels > 0) {
+            MccModelDev* g = dalloc<MccModelDev>(c.nmodels);
+            APIC_CUDA(cudaMemcpyAsync(g, p.model, c.nmodels * sizeof(MccModelDev), cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            p.gmodel = g;
         }
         p.E = dalloc<double>(c.nx);
         p.rho = dalloc<double>(c.nx);
@@ -1708,6 +1754,8 @@ struct Sim1D {
             set_attributes<3, false, false>(); set_attributes<3, true, false>();
             set_attributes<1, false, true>(); set_attributes<1, true, true>();
             set_attributes<3, false, true>(); set_attributes<3, true, true>();
+            set_attributes_c32<1, false>(); set_attributes_c32<1, true>();
+            set_attributes_c32<3, false>(); set_attributes_c32<3, true>();
             attr_done = true;
         }
     }
@@ -1721,6 +1769,8 @@ struct Sim1D {
             const SpeciesDev& B = p.sp[s];
             const int in = parity, out = parity ^ 1;
             S.x[0] = B.x[in]; S.x[1] = B.x[out];
+            S.cell[0] = B.cell[in]; S.cell[1] = B.cell[out];
+            S.off[0] = B.off[in]; S.off[1] = B.off[out];
             S.vh[0] = B.vh[in]; S.vh[1] = B.vh[out];
             S.vy[0] = B.vy[in]; S.vy[1] = B.vy[out];
             S.vz[0] = B.vz[in]; S.vz[1] = B.vz[out];
@@ -1741,8 +1791,8 @@ struct Sim1D {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         size_t tiles = 0;
         for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
-        // one resident wave of k_pass1d: kMinBlocks CTAs per SM
-        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * kMinBlocks));
+        // one resident wave of the pass kernel: kMinBlocks (kMinBlocks32) CTAs per SM
+        blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * (c32 ? kMinBlocks32 : kMinBlocks)));
         return blocks_cache;
     }
 
@@ -1777,6 +1827,32 @@ struct Sim1D {
         APIC_CUDA(cudaFuncSetAttribute(k_post1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, psm));
         APIC_CUDA(cudaFuncSetAttribute(k_moments1d<VDIM, DIR, F32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)kMomentSmemMax));
+    }
+
+    template <int VDIM, bool DIR>
+    static void set_attributes_c32() {
+        APIC_CUDA(cudaFuncSetAttribute(k_pass1d_c32<VDIM, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kMaxNx1D * 12));
+        const int psm = (int)post_smem_bytes(DIR ? kMaxNx1D : kMaxNx1DPeriodic, DIR);
+        APIC_CUDA(cudaFuncSetAttribute(k_post1d<VDIM, DIR, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       psm));
+    }
+
+    template <int VDIM, bool DIR>
+    void launch_kernels_c32(const Params1D& q, int blocks, size_t post_smem, unsigned post, EvPair& ev) {
+        k_pass1d_c32<VDIM, DIR><<<blocks, kThreads, (size_t)cfg.nx * 12, stream>>>(q);
+        if (timing) cudaEventRecord(ev.b, stream);
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3(1);
+        lc.blockDim = dim3(kPostThreads);
+        lc.dynamicSmemBytes = post_smem;
+        lc.stream = stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributePriority;
+        attr[0].val.priority = post_priority;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        APIC_CUDA(cudaLaunchKernelEx(&lc, k_post1d<VDIM, DIR, true, true>, q, post));
     }
 
     // The post kernel takes a whole SM's registers (one 512-thread CTA), so
@@ -1819,7 +1895,14 @@ struct Sim1D {
             APIC_CUDA(cudaEventRecord(ev.a, stream));
         }
         const int form = (cfg.velocity_dimensions == 3 ? 4 : 0) | (dir ? 2 : 0) | (fp32 ? 1 : 0);
-        switch (form) {
+        if (c32) {
+            switch (form & 6) {
+                case 0: launch_kernels_c32<1, false>(q, blocks, post_smem, post, ev); break;
+                case 2: launch_kernels_c32<1, true>(q, blocks, post_smem, post, ev); break;
+                case 4: launch_kernels_c32<3, false>(q, blocks, post_smem, post, ev); break;
+                default: launch_kernels_c32<3, true>(q, blocks, post_smem, post, ev); break;
+            }
+        } else switch (form) {
             case 0: launch_kernels<1, false, false>(q, blocks, smem, post_smem, post, ev); break;
             case 1: launch_kernels<1, false, true>(q, blocks, smem, post_smem, post, ev); break;
             case 2: launch_kernels<1, true, false>(q, blocks, smem, post_smem, post, ev); break;
@@ -1862,6 +1945,36 @@ struct Sim1D {
         APIC_CUDA(cudaMemcpyAsync(host, stage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     }
 
+    // Positions of species s from host doubles into the current buffer (FP32
+    // cell form: through the staging array into cell + offset).
+    void put_x(int s, const double* host, size_t n) {
+        if (n == 0) return;
+        SpeciesDev& B = p.sp[s];
+        if (!c32) {
+            APIC_CUDA(cudaMemcpyAsync(B.x[parity], host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+            return;
+        }
+        APIC_CUDA(cudaMemcpyAsync(B.stage, host, n * sizeof(double), cudaMemcpyHostToDevice, stream));
+        const unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 4096);
+        if (cfg.boundary == APIC_DIRICHLET)
+            k_x_to_cell<true><<<g, 256, 0, stream>>>(B.stage, B.cell[parity], B.off[parity], (unsigned)n, p);
+        else
+            k_x_to_cell<false><<<g, 256, 0, stream>>>(B.stage, B.cell[parity], B.off[parity], (unsigned)n, p);
+        APIC_CUDA(cudaGetLastError());
+    }
+    void get_x(int s, double* host, size_t n) {
+        if (n == 0) return;
+        const SpeciesDev& B = p.sp[s];
+        if (!c32) {
+            APIC_CUDA(cudaMemcpyAsync(host, B.x[parity], n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            return;
+        }
+        const unsigned g = (unsigned)std::min<size_t>((n + 255) / 256, 4096);
+        k_cell_to_x<<<g, 256, 0, stream>>>(B.cell[parity], B.off[parity], B.stage, (unsigned)n, p.dx);
+        APIC_CUDA(cudaGetLastError());
+        APIC_CUDA(cudaMemcpyAsync(host, B.stage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+
     void load(int s, size_t n, const double* x, const double* v, const double* vh, const double* vy,
               const double* vz, const uint8_t* alive) {
         require(s >= 0 && s < cfg.nspecies, "species index out of range");
@@ -1872,7 +1985,7 @@ struct Sim1D {
                     APIC_ERR_CAPACITY);
             SpeciesDev& B = p.sp[s];
             const size_t bytes = n * sizeof(double);
-            APIC_CUDA(cudaMemcpyAsync(B.x[parity], x, bytes, cudaMemcpyHostToDevice, stream));
+            put_x(s, x, n);
             put_comp(s, B.vh[parity], B.vh32[parity], vh, n);
             APIC_CUDA(cudaMemcpyAsync(B.v, v, bytes, cudaMemcpyHostToDevice, stream));
             if (cfg.velocity_dimensions == 3) {
@@ -1900,7 +2013,7 @@ struct Sim1D {
         APIC_CUDA(cudaStreamSynchronize(stream));
         SpeciesDev& B = p.sp[s];
         const size_t bytes = m * sizeof(double);
-        APIC_CUDA(cudaMemcpyAsync(B.x[parity], hx.data(), bytes, cudaMemcpyHostToDevice, stream));
+        put_x(s, hx.data(), m);
         put_comp(s, B.vh[parity], B.vh32[parity], hvh.data(), m);
         APIC_CUDA(cudaMemcpyAsync(B.v, hv.data(), bytes, cudaMemcpyHostToDevice, stream));
         if (cfg.velocity_dimensions == 3) {
@@ -2036,7 +2149,7 @@ struct Sim1D {
         require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
         const SpeciesDev& B = p.sp[s];
         const size_t bytes = n * sizeof(double);
-        if (x) APIC_CUDA(cudaMemcpyAsync(x, B.x[parity], bytes, cudaMemcpyDeviceToHost, stream));
+        if (x) get_x(s, x, n);
         if (v) APIC_CUDA(cudaMemcpyAsync(v, B.v, bytes, cudaMemcpyDeviceToHost, stream));
         if (vh) get_comp(s, B.vh[parity], B.vh32[parity], vh, n);
         if (cfg.velocity_dimensions == 3) {

@@ -56,9 +56,12 @@ typedef enum { APIC_PERIODIC = 0, APIC_DIRICHLET = 1 } apic_boundary;
 typedef enum { APIC_NORMALIZED = 0, APIC_SI = 1 } apic_units;
 /* Particle storage form.  FP64: x and velocities in double, bit-faithful to
  * the reference arithmetic.  FP32: integer cell index + float in-cell offset
- * and float velocities; charge accumulation, field solve and diagnostics
- * stay FP64. */
-typedef enum { APIC_FP64 = 0, APIC_FP32 = 1 } apic_precision;
+ * and float velocities, with the particle arithmetic (gather, push, walls,
+ * null-collision loop) in FP32; charge accumulation (64-bit fixed point),
+ * field solve and energy ledgers stay FP64.  FP32_STORAGE (1D only): float
+ * velocities with an FP64 position and FP64 arithmetic, for runs that want
+ * the campaign diagnostics with FP32 velocity storage. */
+typedef enum { APIC_FP64 = 0, APIC_FP32 = 1, APIC_FP32_STORAGE = 2 } apic_precision;
 
 /* CollisionProcessKind, include/pic/Config.hpp:42-48 */
 typedef enum {

@@ -1,5 +1,5 @@
-"""The 1D FP32 particle form (v_half, v_y, v_z stored as float; position,
-fields and all arithmetic FP64) through the C ABI.
+"""The 1D FP32 storage form (APIC_FP32_STORAGE: v_half, v_y, v_z stored as
+float; position, fields and all arithmetic FP64) through the C ABI.
 
 Parity: against oracle mode 2, which stores the same components as float at
 the same points, the state agrees bit for bit except where the two FP64
@@ -29,7 +29,7 @@ FP32_VS_FP64 = {"x": 1e-6, "vh": 1e-5, "v": 1e-5, "vy": 1e-6, "vz": 1e-6, "field
 
 
 def _pair(wl, seed=0x5EED):
-    cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=seed)
+    cfg, tabs = W.to_device_config(wl, precision=apic.FP32_STORAGE, seed=seed)
     dev = apic.Simulation1D(cfg, tabs)
     load_device(dev, wl)
     dev.initialize()
@@ -118,7 +118,7 @@ def test_fp32_step_group_and_readback_idempotent():
              W.two_stream(particles_per_beam=2048, nx=64, seed=4)]
 
     def make(wl, k):
-        cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=77 + k)
+        cfg, tabs = W.to_device_config(wl, precision=apic.FP32_STORAGE, seed=77 + k)
         sim = apic.Simulation1D(cfg, tabs)
         load_device(sim, wl)
         sim.initialize()

@@ -7,7 +7,7 @@ accumulators and CSV output (tests/test_oracle_golden.py).
 FP64 form: sample counts and EEDF observation counts exact; every per-node sum
 within 1e-12 of the oracle relative to the largest magnitude of its row (the
 device adds with FP64 atomics, so only the order of the additions differs).
-FP32 particle form: against oracle mode 2 within the FP32 form's bounds."""
+FP32 storage form: against oracle mode 2 within the FP32 form's bounds."""
 import numpy as np
 import pytest
 
@@ -148,10 +148,10 @@ def test_window_without_rf_contract_through_step_group():
 
 
 def test_fp32_form_matches_oracle_mode2():
-    """The FP32 particle form: every sample stores the state as the read-back
+    """The FP32 storage form: every sample stores the state as the read-back
     does; against oracle mode 2 the sums agree within the FP32 form's bounds."""
     wl = _deck(10 * F)
-    dev, _t1 = _device(wl, SHORT, precision=apic.FP32)
+    dev, _t1 = _device(wl, SHORT, precision=apic.FP32_STORAGE)
     ora, _t2 = _oracle(wl, SHORT, 2)
     dev.step(40)
     ora.step(40)
@@ -183,14 +183,14 @@ def test_electric_work_ledger_with_walls_and_products_fp64():
 
 def test_electric_work_ledger_two_stream_graphs_and_fp32():
     """Periodic two-stream deck stepped through step_group (the graph path),
-    FP64 against oracle mode 1; the FP32 form against oracle mode 2."""
+    FP64 against oracle mode 1; the FP32 storage form against oracle mode 2."""
     wl = W.two_stream(particles_per_beam=512, nx=64, seed=3, steps=50)
     dev, _t1 = _device(wl, None, ledger=True)
     ora, _t2 = _oracle(wl, None, 1)
     apic.step_group([dev], 50)
     ora.step(50)
     _check_work(dev, ora, 2, TOL)
-    dev32, _t3 = _device(wl, None, precision=apic.FP32, ledger=True)
+    dev32, _t3 = _device(wl, None, precision=apic.FP32_STORAGE, ledger=True)
     ora2, _t4 = _oracle(wl, None, 2)
     dev32.step(50)
     ora2.step(50)
