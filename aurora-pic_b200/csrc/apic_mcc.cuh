@@ -28,6 +28,7 @@ enum : unsigned {
     kErrTimeout = 1u << 4,
     kErrReplay = 1u << 5,
     kErrBirths = 1u << 6,
+    kErrCandBuffer = 1u << 7,  // collision candidates of one pass beyond the candidate buffer
 };
 
 // Bracket index of a table: bin b of a uniform grid in log2(energy) stores the

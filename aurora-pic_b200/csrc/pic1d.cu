@@ -79,6 +79,7 @@ struct DevState {
     unsigned nranges[kMaxSpecies];  // ranges of the current input layout
     unsigned nbirths;
     unsigned error;
+    unsigned holes[kMaxSpecies];    // FP32 cell form: dead slots among [0, n)
     unsigned long long step;
     double time;
     unsigned long long candidates, nulls;
@@ -99,7 +100,9 @@ struct BirthRec {
 struct SpeciesDev {
     double qm, hqm, qw, qwdx, mass, weight;
     int model;
-    unsigned capacity;
+    unsigned capacity;  // slots of a particle buffer
+    unsigned nscratch;  // entries of chunk_surv
+    unsigned live_cap;  // max_particles_per_species (the FP32 cell form's buffers add room for holes)
     // MCC first waiting time inside the step exactly when the first 64-bit
     // draw is >= cand_draw_min (see draw_threshold); no_candidates: never
     uint64_t cand_draw_min;
@@ -131,10 +134,15 @@ struct SpeciesDev {
     // FP32 cell form constants: q/m dt, q/(2m) dt, dt/dx, and the fixed-point
     // charge of a whole particle on one node (q w / dx times the density scale)
     float qmdt32, hqmdt32, dtdx32, dep32;
+    // FP32 cell form candidates: P = 1 - exp(-nu dt) of the first waiting time
+    // falling inside the step, and 1 / (nu dt) for the geometric gaps
+    float cand_p32, inv_nudt32;
     // electric-work ledger: the time-centred v each particle had at the end of
     // its last step (double-buffered like the state); null unless enabled
     double* vold[2];
 };
+
+struct CandRec32;
 
 struct Params1D {
     int nspecies, vdim, dirichlet, nx;
@@ -168,6 +176,12 @@ struct Params1D {
     // models in device memory for the (rare) exact frequency-bound check
     MccModel32 model32[kMaxModels];
     const MccModelDev* gmodel;
+    // this step's collision candidates (FP32 cell form): region b of
+    // cand_per_region records belongs to CTA b of the pass, which stores its
+    // count in cand_count[b]
+    CandRec32* cands;
+    unsigned* cand_count;
+    unsigned cand_regions, cand_per_region;
 };
 
 // ---- field gather / deposit (reference arithmetic) ----------------------
@@ -686,10 +700,22 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
     }
 
     // -- output range table: chunk c of the pass kept its survivors at slots
-    //    [c * kTile, c * kTile + surv_c); logical starts are their prefix sums --
-    for (int s = 0; s < p.nspecies; ++s) {
+    //    [c * kTile, c * kTile + surv_c); logical starts are their prefix sums
+    //    (the FP32 cell form updates its slots in place: products go after n) --
+    constexpr unsigned CHUNK = (unsigned)kTile;
+    constexpr int OUT = C32 ? 0 : 1;  // buffer receiving the products
+    if (C32) {
+        if (tid < p.nspecies) {
+            s_surv[tid] = st->n[tid];
+            s_bstart[tid] = st->n[tid];
+            s_nch[tid] = 0;
+            s_kept[tid] = 0;
+        }
+        __syncthreads();
+    }
+    for (int s = 0; s < (C32 ? 0 : p.nspecies); ++s) {
         const SpeciesDev& S = p.sp[s];
-        const unsigned nch = (st->n[s] + kTile - 1) / kTile;
+        const unsigned nch = (st->n[s] + CHUNK - 1) / CHUNK;
         if (tid == 0) s_carry = 0;
         __syncthreads();
         for (unsigned b0 = 0; b0 < nch; b0 += kPostThreads * kPostItems) {
@@ -706,7 +732,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
             for (int k = 0; k < kPostItems; ++k) {
                 const unsigned c = b0 + tid * kPostItems + k;
                 if (c < nch) {
-                    S.rstart[1][c] = c * kTile;
+                    S.rstart[1][c] = c * CHUNK;
                     S.rcount[1][c] = cnt[k];
                     S.rlstart[1][c] = carry + pre[k];
                 }
@@ -718,7 +744,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         if (tid == 0) {
             s_surv[s] = s_carry;
             s_nch[s] = nch;
-            s_bstart[s] = nch ? (nch - 1) * kTile + S.chunk_surv[nch - 1] : 0u;
+            s_bstart[s] = nch ? (nch - 1) * CHUNK + S.chunk_surv[nch - 1] : 0u;
             s_kept[s] = 0;
         }
         __syncthreads();
@@ -840,18 +866,18 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
                     int c;
                     float f;
                     position_to_cell<DIRICHLET>(bx[k], p, c, f);
-                    S.cell[1][o] = c;
-                    S.off[1][o] = f;
+                    S.cell[OUT][o] = c;
+                    S.off[OUT][o] = f;
                 } else {
-                    S.x[1][o] = bx[k];
+                    S.x[OUT][o] = bx[k];
                 }
-                st_comp<F32>(S.vh[1], S.vh32[1], o, bvh[k]);
+                st_comp<F32>(S.vh[OUT], S.vh32[OUT], o, bvh[k]);
                 if (VDIM == 3) {
-                    st_comp<F32>(S.vy[1], S.vy32[1], o, bv[k][1]);
-                    st_comp<F32>(S.vz[1], S.vz32[1], o, bv[k][2]);
+                    st_comp<F32>(S.vy[OUT], S.vy32[OUT], o, bv[k][1]);
+                    st_comp<F32>(S.vz[OUT], S.vz32[OUT], o, bv[k][2]);
                 }
                 S.v[o] = bv[k][0];
-                if (p.ledger) S.vold[1][o] = bv[k][0];
+                if (p.ledger) S.vold[OUT][o] = bv[k][0];
             }
             if (tid == 0) s_kept[s] = total;
         }
@@ -864,8 +890,12 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
             atomicOr(&st->error, kErrCapacity);
             kept = S.capacity > s_bstart[tid] ? S.capacity - s_bstart[tid] : 0u;
         }
+        // the FP32 cell form's slots include holes: the configured capacity
+        // bounds the live particles (max_particles_per_species)
+        if (C32 && (unsigned long long)(s_surv[tid] - st->holes[tid]) + kept > S.live_cap)
+            atomicOr(&st->error, kErrCapacity);
         unsigned nr = s_nch[tid];
-        if (kept) {  // this pass's products form one more range after the last chunk
+        if (kept && !C32) {  // this pass's products form one more range after the last chunk
             S.rstart[1][nr] = s_bstart[tid];
             S.rcount[1][nr] = kept;
             S.rlstart[1][nr] = s_surv[tid];
@@ -1184,6 +1214,7 @@ __global__ void __launch_bounds__(256) k_sample1d(Params1D p, double* partial, u
         const double hmw = 0.5 * S.mass * S.weight;
         double acc = 0.0;
         for (unsigned i = blockIdx.x * 256 + tid; i < n; i += gridDim.x * 256) {
+            if (p.c32 && S.cell[0][i] == kDeadCell) continue;  // a hole of the FP32 cell form
             const double v = S.v[i];
             double sq = v * v;
             if (p.vdim == 3) {
@@ -1301,7 +1332,7 @@ int status_from_device(unsigned w) {
     if (w & kErrMajorant) return APIC_ERR_MAJORANT;
     if (w & kErrCandidates) return APIC_ERR_CANDIDATES;
     if (w & kErrNonFinite) return APIC_ERR_NONFINITE;
-    if (w & (kErrCapacity | kErrBirths)) return APIC_ERR_CAPACITY;
+    if (w & (kErrCapacity | kErrBirths | kErrCandBuffer)) return APIC_ERR_CAPACITY;
     if (w & kErrTimeout) return APIC_ERR_TIMEOUT;
     if (w & kErrReplay) return APIC_ERR_INVALID;
     return APIC_OK;
@@ -1314,6 +1345,7 @@ std::string describe_device_error(unsigned w) {
     if (w & kErrNonFinite) s += "particle state became non-finite; ";
     if (w & kErrCapacity) s += "reactive collisions exceeded max_particles_per_species; ";
     if (w & kErrBirths) s += "ionization products in one step exceeded the per-step product buffer; ";
+    if (w & kErrCandBuffer) s += "collision candidates of one step exceeded the candidate buffer; ";
     if (w & kErrTimeout) s += "device look-back wait timed out; ";
     if (w & kErrReplay) s += "recorded draw array exhausted; ";
     return s;
@@ -1621,6 +1653,15 @@ struct Sim1D {
             bound += (double)sp.capacity * std::fabs(sp.charge * sp.weight) / (dir ? 0.5 * p.dx : p.dx);
         }
         int bits = bound > 0 ? (int)std::floor(61.0 - std::log2(bound)) : 0;
+        if (c32) {
+            // the FP32 cell form converts one particle's share of a node to a
+            // 32-bit integer: a whole particle's charge on an end node (twice
+            // q w / dx) stays below 2^30
+            double per = 0.0;
+            for (int s = 0; s < c.nspecies; ++s)
+                per = std::max(per, 2.0 * std::fabs(c.species[s].charge * c.species[s].weight) / p.dx);
+            if (per > 0) bits = std::min(bits, (int)std::floor(30.0 - std::log2(per)));
+        }
         p.rho_scale = std::ldexp(1.0, bits);
         p.inv_rho_scale = std::ldexp(1.0, -bits);
 
@@ -1640,9 +1681,15 @@ struct Sim1D {
             S.mass = sp.mass;
             S.weight = sp.weight;
             S.model = -1;
-            S.capacity = (unsigned)sp.capacity;
-            const size_t cap = sp.capacity;
-            const size_t maxr = (cap + kTile - 1) / kTile + 2;
+            // the FP32 cell form's buffers also hold the holes left between compactions
+            const size_t cap = c32 ? sp.capacity + sp.capacity / 16 + 4096 : sp.capacity;
+            require(cap < (1ull << 31), "species capacity out of range");
+            S.capacity = (unsigned)cap;
+            S.live_cap = (unsigned)sp.capacity;
+            // range tables of the pass chunks (FP32 cell form: chunk counts of the compaction)
+            const size_t chunk = c32 ? (size_t)kChunk32 : (size_t)kTile;
+            const size_t maxr = (cap + chunk - 1) / chunk + 3;
+            S.nscratch = (unsigned)maxr;
             for (int b = 0; b < 2; ++b) {
                 S.rstart[b] = dalloc<unsigned>(maxr);
                 S.rcount[b] = dalloc<unsigned>(maxr);
@@ -1696,10 +1743,31 @@ struct Sim1D {
             neutral_stddev[mi] = p.model[mi].neutral_stddev;
             p.sp[m.species].model = mi;
             draw_threshold(m.max_frequency, c.dt, p.sp[m.species].cand_draw_min, p.sp[m.species].no_candidates);
-            if (c32) build_model32(m, arena, p.model[mi], p.model32[mi]);
+            if (c32) {
+                build_model32(m, arena, p.model[mi], p.model32[mi]);
+                const double nudt = m.max_frequency * c.dt;
+                p.sp[m.species].cand_p32 = (float)(-std::expm1(-nudt));
+                p.sp[m.species].inv_nudt32 = (float)(1.0 / nudt);
+            }
             APIC_CUDA(cudaStreamSynchronize(stream));  // host tables may be freed after create
         }
         if (c32 && c.nmodels > 0) {
+            // candidate buffer: twice the expected candidates of a step plus
+            // room for fluctuations (overflow sets an error, never a fault)
+            size_t phys = 0;
+            double pmax = 0.0;
+            for (int s = 0; s < c.nspecies; ++s) {
+                phys += p.sp[s].capacity;
+                if (p.sp[s].model >= 0) pmax = std::max(pmax, (double)p.sp[s].cand_p32);
+            }
+            // one region per CTA of the pass: twice its expected candidates plus slack
+            const int regions = grid_blocks();
+            const double per_cta = (double)phys / regions;
+            const size_t per = (size_t)std::min(std::ceil(per_cta) + 32.0, std::ceil(2.0 * pmax * per_cta) + 256.0);
+            p.cands = dalloc<CandRec32>(per * regions);
+            p.cand_count = dalloc<unsigned>(regions);
+            p.cand_regions = (unsigned)regions;
+            p.cand_per_region = (unsigned)per;
             MccModelDev* g = dalloc<MccModelDev>(c.nmodels);
             APIC_CUDA(cudaMemcpyAsync(g, p.model, c.nmodels * sizeof(MccModelDev), cudaMemcpyHostToDevice, stream));
             APIC_CUDA(cudaStreamSynchronize(stream));
@@ -1790,9 +1858,12 @@ struct Sim1D {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         size_t tiles = 0;
-        for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;
+        for (int s = 0; s < cfg.nspecies; ++s) tiles += (cfg.species[s].capacity + kTile - 1) / kTile;  // 8 warp chunks of c32 per tile
         // one resident wave of the pass kernel: kMinBlocks (kMinBlocks32) CTAs per SM
         blocks_cache = (int)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)sms * (c32 ? kMinBlocks32 : kMinBlocks)));
+#ifdef APIC_C32_GRID_DIV
+        if (c32) blocks_cache = std::max(1, blocks_cache / APIC_C32_GRID_DIV);
+#endif
         return blocks_cache;
     }
 
@@ -1841,6 +1912,8 @@ struct Sim1D {
     template <int VDIM, bool DIR>
     void launch_kernels_c32(const Params1D& q, int blocks, size_t post_smem, unsigned post, EvPair& ev) {
         k_pass1d_c32<VDIM, DIR><<<blocks, kThreads, (size_t)cfg.nx * 12, stream>>>(q);
+        if (VDIM == 3 && cfg.nmodels > 0 && (q.mode & kModeSyncMcc))
+            k_collide1d_c32<VDIM, DIR><<<148 * 8, kCollideThreads, 0, stream>>>(q);
         if (timing) cudaEventRecord(ev.b, stream);
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(1);
@@ -1917,7 +1990,39 @@ struct Sim1D {
             events.push_back(ev);
         }
         APIC_CUDA(cudaGetLastError());
+        if (!c32) parity ^= 1;  // the FP32 cell form updates its buffer in place
+    }
+
+    // FP32 cell form: squeezes the holes out of every species' slots, order
+    // preserved (into the other buffer, which becomes the current one).
+    void compact32() {
+        const int sms = 148;
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            SpeciesDev& B = p.sp[s];
+            const int in = parity, out = parity ^ 1;
+            unsigned* counts = B.chunk_surv;
+            unsigned* n_old = B.chunk_surv + B.nscratch - 1;
+            k_c32_count<<<sms * 4, 256, 0, stream>>>(B.cell[in], &st->n[s], counts);
+            k_c32_scan<<<1, kScanThreads, 0, stream>>>(counts, &st->n[s], &st->holes[s], n_old);
+            C32Arrays a{B.cell[in], B.off[in], B.vh32[in], B.vy32[in], B.vz32[in], B.v};
+            // S.v is not carried: it is rewritten by every read-back
+            k_c32_scatter<<<sms * 4, 256, 0, stream>>>(a, B.cell[out], B.off[out], B.vh32[out], B.vy32[out],
+                                                       B.vz32[out], nullptr, n_old, counts);
+        }
+        APIC_CUDA(cudaGetLastError());
         parity ^= 1;
+    }
+    bool compaction_due(uint64_t k) const { return c32 && k % kCompactSteps == 0; }
+
+    // FP32 cell form read-back: one component of the live particles, in slot
+    // order, to host doubles (the device layout is left as it is).
+    void gather32(int s, int component, double* host, size_t n) {
+        SpeciesDev& B = p.sp[s];
+        const int in = parity;
+        C32Arrays a{B.cell[in], B.off[in], B.vh32[in], B.vy32[in], B.vz32[in], B.v};
+        k_c32_gather<<<148 * 4, 256, 0, stream>>>(a, component, p.dx, &st->n[s], B.chunk_surv, B.stage);
+        APIC_CUDA(cudaGetLastError());
+        APIC_CUDA(cudaMemcpyAsync(host, B.stage, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     }
 
     // One velocity component of species s between host doubles and the
@@ -2037,6 +2142,7 @@ struct Sim1D {
         APIC_CUDA(cudaMemcpyAsync(B.rlstart[parity], &h[2], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaMemcpyAsync(&st->n[s], &h[1], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
         APIC_CUDA(cudaMemcpyAsync(&st->nranges[s], &h[3], sizeof(unsigned), cudaMemcpyHostToDevice, stream));
+        APIC_CUDA(cudaMemsetAsync(&st->holes[s], 0, sizeof(unsigned), stream));
     }
 
     void set_time(double t, uint64_t k) {
@@ -2066,6 +2172,10 @@ struct Sim1D {
     // Two steps with the collision part of the previous step pending, as one
     // CUDA graph launch (kernel parameters depend only on the buffer parity).
     void steady_pair() {
+        if (compaction_due(step + 1) || compaction_due(step + 2)) {
+            do_steps(2);
+            return;
+        }
         const int par = parity;
         if (!pair_exec[par]) {
             const bool t = timing;
@@ -2097,6 +2207,7 @@ struct Sim1D {
             time += cfg.dt;
             ++step;
             if (sample_step(step)) take_sample(step);
+            if (compaction_due(step)) compact32();
         }
     }
 
@@ -2139,16 +2250,37 @@ struct Sim1D {
     size_t count(int s) {
         require(s >= 0 && s < cfg.nspecies, "species index out of range");
         finish();
-        return read_state().n[s];
+        const DevState h = read_state();
+        return h.n[s] - h.holes[s];
     }
 
     size_t read_particles(int s, size_t cap, double* x, double* v, double* vh, double* vy, double* vz) {
         require(s >= 0 && s < cfg.nspecies, "species index out of range");
         finish();
-        const size_t n = read_state().n[s];
+        const DevState h = read_state();
+        const size_t n = h.n[s] - h.holes[s];
         require(cap >= n, "output capacity below the particle count", APIC_ERR_CAPACITY);
         const SpeciesDev& B = p.sp[s];
         const size_t bytes = n * sizeof(double);
+        if (c32) {
+            // the live particles in slot order, through the staging array
+            unsigned* counts = B.chunk_surv;
+            k_c32_count<<<148 * 4, 256, 0, stream>>>(B.cell[parity], &st->n[s], counts);
+            k_c32_scan<<<1, kScanThreads, 0, stream>>>(counts, &st->n[s], nullptr, counts + B.nscratch - 1);
+            APIC_CUDA(cudaGetLastError());
+            if (x) gather32(s, 0, x, n);
+            if (v) gather32(s, 1, v, n);
+            if (vh) gather32(s, 2, vh, n);
+            if (cfg.velocity_dimensions == 3) {
+                if (vy) gather32(s, 3, vy, n);
+                if (vz) gather32(s, 4, vz, n);
+            } else {
+                if (vy) std::memset(vy, 0, bytes);
+                if (vz) std::memset(vz, 0, bytes);
+            }
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            return n;
+        }
         if (x) get_x(s, x, n);
         if (v) APIC_CUDA(cudaMemcpyAsync(v, B.v, bytes, cudaMemcpyDeviceToHost, stream));
         if (vh) get_comp(s, B.vh[parity], B.vh32[parity], vh, n);
@@ -2396,9 +2528,9 @@ int apic_sim1d_sample(apic_sim1d* sim, apic_sample1d* out) {
         std::memset(out, 0, sizeof *out);
         const apic::DevState h = S.sample_device(out);
         for (int s = 0; s < S.cfg.nspecies; ++s) {
-            out->live_by_species[s] = h.n[s];
+            out->live_by_species[s] = h.n[s] - h.holes[s];
             out->kinetic_energy += out->kinetic_by_species[s];
-            out->live_particles += h.n[s];
+            out->live_particles += h.n[s] - h.holes[s];
         }
         out->total_energy = out->kinetic_energy + out->field_energy;
         out->step = S.step;
