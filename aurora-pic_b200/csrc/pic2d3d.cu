@@ -121,10 +121,11 @@ __device__ __forceinline__ void field_b(const ParamsND& p, const double pos[3], 
     profile_b(p, a < p.dims ? (a == 0 ? pos[0] : (a == 1 ? pos[1] : pos[2])) : 0.0, B);
 }
 
-// FP32 form: each CIC weight is rounded to a multiple of 2^-25 and summed per
-// species in 64-bit integers (runs of lanes in one cell first add theirs with a
-// single warp reduction), so the density does not depend on particle order.
-constexpr float kWeightScale = 33554432.0f;  // 2^25
+// FP32 form: each CIC weight is rounded to a multiple of 2^-23 and summed per
+// species in 64-bit integers (runs of particles in one cell first add theirs in
+// 32-bit registers and warp reductions: 8 particles per lane x 32 lanes x 2^23
+// stays below 2^32), so the density does not depend on particle order.
+constexpr float kWeightScale = 8388608.0f;  // 2^23
 
 // wrap_periodic, src/FieldSolver.cpp:15-17, with the exact fast branch for |x| < 2L
 __device__ __forceinline__ double wrap_periodic(double x, double L) {
@@ -727,6 +728,216 @@ __global__ void __launch_bounds__(kThreads) k_push32_step(ParamsND p, SpeciesND 
         }
         deposit32_warp<DIM>(p, acc, valid, ix, iy, iz, f);
     }
+}
+
+// The step push of the FP32 form with ITEMS consecutive particles per thread
+// (loaded and stored as vectors).  Particles are sorted by cell, so a thread's
+// particles mostly share a cell: the field at the cell's nodes is fetched once
+// per run of equal cells, and the CIC weights of a run are summed in registers
+// (the deposit of src/Mesh2D.cpp:90-144 / src/Mesh3D.cpp:62-126 at the pushed
+// positions).  A run that ends inside the thread is committed with one 64-bit
+// atomic per node; each lane's last run joins a warp-segmented sum over the
+// lanes holding the same cell, whose last lane commits it.
+template <int DIM, bool BORIS, int ITEMS, bool PROF>
+__global__ void __launch_bounds__(kThreads) k_push32_run(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
+    constexpr int NN = DIM == 2 ? 4 : 8;  // nodes of a cell
+    const unsigned first = (blockIdx.x * kThreads + threadIdx.x) * ITEMS;
+    const int lane = threadIdx.x & 31;
+    if ((blockIdx.x * kThreads + (threadIdx.x & ~31u)) * ITEMS >= S.n) return;  // whole warp past the end
+    const int nx = p.n[0], ny = p.n[1], nz = DIM == 3 ? p.n[2] : 1;
+    unsigned cl[ITEMS];
+    float fo[ITEMS][3], vv[ITEMS][3];
+    const bool full = first + ITEMS <= S.n;
+    if (full) {
+        if (ITEMS == 4) {
+            const uint4 c = __ldcs(reinterpret_cast<const uint4*>(S.cell[buf] + first));
+            cl[0] = c.x; cl[1] = c.y; cl[2 % ITEMS] = c.z; cl[3 % ITEMS] = c.w;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a < DIM) {
+                    const float4 f = __ldcs(reinterpret_cast<const float4*>(S.off[buf][a] + first));
+                    fo[0][a] = f.x; fo[1][a] = f.y; fo[2 % ITEMS][a] = f.z; fo[3 % ITEMS][a] = f.w;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < ITEMS; ++k) fo[k][a] = 0.0f;
+                }
+                const float4 v = __ldcs(reinterpret_cast<const float4*>(S.vel[buf][a] + first));
+                vv[0][a] = v.x; vv[1][a] = v.y; vv[2 % ITEMS][a] = v.z; vv[3 % ITEMS][a] = v.w;
+            }
+        } else {
+            const uint2 c = __ldcs(reinterpret_cast<const uint2*>(S.cell[buf] + first));
+            cl[0] = c.x; cl[1 % ITEMS] = c.y;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a < DIM) {
+                    const float2 f = __ldcs(reinterpret_cast<const float2*>(S.off[buf][a] + first));
+                    fo[0][a] = f.x; fo[1 % ITEMS][a] = f.y;
+                } else {
+                    fo[0][a] = 0.0f; fo[1 % ITEMS][a] = 0.0f;
+                }
+                const float2 v = __ldcs(reinterpret_cast<const float2*>(S.vel[buf][a] + first));
+                vv[0][a] = v.x; vv[1 % ITEMS][a] = v.y;
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const unsigned i = first + k;
+            const bool ok = i < S.n;
+            cl[k] = ok ? S.cell[buf][i] : 0u;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                fo[k][a] = (ok && a < DIM) ? S.off[buf][a][i] : 0.0f;
+                vv[k][a] = ok ? S.vel[buf][a][i] : 0.0f;
+            }
+        }
+    }
+    const unsigned kNoCell = 0xFFFFFFFFu;
+    unsigned gcell = kNoCell;   // cell whose node fields are cached
+    float en[NN][3];            // the field at its nodes
+    unsigned rcell = kNoCell;   // cell of the current deposit run
+    unsigned racc[NN];          // its summed quantised weights
+#pragma unroll
+    for (int j = 0; j < NN; ++j) racc[j] = 0u;
+    auto commit = [&](unsigned c, const unsigned* w) {
+        int ix, iy, iz;
+        unpack_cell(c, ix, iy, iz);
+        const int ix1 = (ix + 1) & (nx - 1), iy1 = (iy + 1) & (ny - 1);
+        const int iz1 = DIM == 3 ? (iz + 1) & (nz - 1) : 0;
+#pragma unroll
+        for (int j = 0; j < NN; ++j) {
+            if (!w[j]) continue;
+            const int xx = (j & 1) ? ix1 : ix, yy = (j & 2) ? iy1 : iy, zz = (j & 4) ? iz1 : iz;
+            atomicAdd(acc + ((size_t)zz * ny + yy) * nx + xx, (unsigned long long)w[j]);
+        }
+    };
+#pragma unroll
+    for (int k = 0; k < ITEMS; ++k) {
+        if (first + k >= S.n) continue;
+        int ix, iy, iz;
+        unpack_cell(cl[k], ix, iy, iz);
+        float* f = fo[k];
+        float* v = vv[k];
+        if (cl[k] != gcell) {  // the field at the new cell's nodes
+            gcell = cl[k];
+            const int ix1 = (ix + 1) & (nx - 1), iy1 = (iy + 1) & (ny - 1);
+            if (DIM == 2) {
+                const float2* E = reinterpret_cast<const float2*>(p.E32);
+                const float2 a = __ldg(E + iy * nx + ix), b = __ldg(E + iy * nx + ix1),
+                             c = __ldg(E + iy1 * nx + ix), d = __ldg(E + iy1 * nx + ix1);
+                en[0][0] = a.x; en[0][1] = a.y; en[1][0] = b.x; en[1][1] = b.y;
+                en[2][0] = c.x; en[2][1] = c.y; en[3][0] = d.x; en[3][1] = d.y;
+#pragma unroll
+                for (int j = 0; j < NN; ++j) en[j][2] = 0.0f;
+            } else {
+                const int iz1 = (iz + 1) & (nz - 1);
+                const float4* E = reinterpret_cast<const float4*>(p.E32);
+#pragma unroll
+                for (int j = 0; j < NN; ++j) {
+                    const int xx = (j & 1) ? ix1 : ix, yy = (j & 2) ? iy1 : iy, zz = (j & 4) ? iz1 : iz;
+                    const float4 q = __ldg(E + ((size_t)zz * ny + yy) * nx + xx);
+                    en[j][0] = q.x; en[j][1] = q.y; en[j][2] = q.z;
+                }
+            }
+        }
+        // bilinear / trilinear gather, src/FieldSolver.cpp:925-1038 (the
+        // arithmetic of gather32, so every particles-per-thread choice gives
+        // the same bits)
+        const float wx[2] = {1.0f - f[0], f[0]}, wy[2] = {1.0f - f[1], f[1]};
+        float e[3] = {0.0f, 0.0f, 0.0f};
+        if (DIM == 2) {
+            const float w00 = wx[0] * wy[0], w10 = wx[1] * wy[0], w01 = wx[0] * wy[1], w11 = wx[1] * wy[1];
+            e[0] = fmaf(en[0][0], w00, fmaf(en[1][0], w10, fmaf(en[2][0], w01, en[3][0] * w11)));
+            e[1] = fmaf(en[0][1], w00, fmaf(en[1][1], w10, fmaf(en[2][1], w01, en[3][1] * w11)));
+        } else {
+            const float wz[2] = {1.0f - f[2], f[2]};
+#pragma unroll
+            for (int j = 0; j < NN; ++j) {
+                const float w = wx[j & 1] * (wy[(j >> 1) & 1] * wz[(j >> 2) & 1]);
+                e[0] = fmaf(en[j][0], w, e[0]);
+                e[1] = fmaf(en[j][1], w, e[1]);
+                e[2] = fmaf(en[j][2], w, e[2]);
+            }
+        }
+        // kick + drift, src/Pusher.cpp:109-128, :162-174
+        if (BORIS && PROF) {
+            float tp[3], sp[3];
+            boris_ts32(p, S, ix, iy, iz, f, tp, sp);
+            boris32(v, e, S.hqmdt, tp, sp);
+        } else if (BORIS) {
+            boris32(v, e, S.hqmdt, S.tb, S.sb);
+        } else {
+            for (int a = 0; a < DIM; ++a) v[a] = fmaf(S.qmdt, e[a], v[a]);
+        }
+        advance(f[0], ix, v[0] * S.drift[0], nx);
+        advance(f[1], iy, v[1] * S.drift[1], ny);
+        if (DIM == 3) advance(f[2], iz, v[2] * S.drift[2], nz);
+        cl[k] = pack_cell(ix, iy, iz);
+        // deposit at the pushed position into the run of its cell
+        if (cl[k] != rcell) {
+            if (rcell != kNoCell) commit(rcell, racc);
+            rcell = cl[k];
+#pragma unroll
+            for (int j = 0; j < NN; ++j) racc[j] = 0u;
+        }
+        const float ux[2] = {1.0f - f[0], f[0]}, uy[2] = {1.0f - f[1], f[1]};
+        const float uz[2] = {DIM == 3 ? 1.0f - f[2] : 1.0f, DIM == 3 ? f[2] : 0.0f};
+#pragma unroll
+        for (int j = 0; j < NN; ++j)
+            racc[j] += (unsigned)__float2int_rn(ux[j & 1] * uy[(j >> 1) & 1] * uz[(j >> 2) & 1] * kWeightScale);
+    }
+    // the state back, in place
+    if (full) {
+        if (ITEMS == 4) {
+            __stcs(reinterpret_cast<uint4*>(S.cell[buf] + first), make_uint4(cl[0], cl[1], cl[2 % ITEMS], cl[3 % ITEMS]));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a < DIM)
+                    __stcs(reinterpret_cast<float4*>(S.off[buf][a] + first),
+                           make_float4(fo[0][a], fo[1][a], fo[2 % ITEMS][a], fo[3 % ITEMS][a]));
+                __stcs(reinterpret_cast<float4*>(S.vel[buf][a] + first),
+                       make_float4(vv[0][a], vv[1][a], vv[2 % ITEMS][a], vv[3 % ITEMS][a]));
+            }
+        } else {
+            __stcs(reinterpret_cast<uint2*>(S.cell[buf] + first), make_uint2(cl[0], cl[1 % ITEMS]));
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a < DIM)
+                    __stcs(reinterpret_cast<float2*>(S.off[buf][a] + first), make_float2(fo[0][a], fo[1 % ITEMS][a]));
+                __stcs(reinterpret_cast<float2*>(S.vel[buf][a] + first), make_float2(vv[0][a], vv[1 % ITEMS][a]));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const unsigned i = first + k;
+            if (i >= S.n) continue;
+            S.cell[buf][i] = cl[k];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (a < DIM) S.off[buf][a][i] = fo[k][a];
+                S.vel[buf][a][i] = vv[k][a];
+            }
+        }
+    }
+    // each lane's last run: summed over the lanes that end in the same cell
+    const unsigned key = rcell;
+    const unsigned prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+#pragma unroll
+    for (int j = 0; j < NN; ++j) {
+        unsigned q = racc[j];
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, q, d);
+            if (lane - d >= start) q += t;
+        }
+        racc[j] = q;
+    }
+    if (tail && key != kNoCell) commit(key, racc);
 }
 
 // FP64 staging <-> FP32 state.  The cell/offset split follows the periodic CIC
@@ -1722,8 +1933,8 @@ struct SimND {
         }
         switch (items) {
             case 1: k_push32_step<DIM, BORIS, 1, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
-            case 2: k_push32_step<DIM, BORIS, 2, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
-            case 4: k_push32_step<DIM, BORIS, 4, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 2: k_push32_run<DIM, BORIS, 2, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
+            case 4: k_push32_run<DIM, BORIS, 4, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
             default: k_push32_step<DIM, BORIS, 8, false><<<g, kThreads, 0, stream>>>(p, S, b, acc); break;
         }
     }
