@@ -1762,6 +1762,7 @@ struct Sim1D {
             }
             // one region per CTA of the pass: twice its expected candidates plus slack
             const int regions = grid_blocks();
+            require(regions <= kMaxRegions, "pass grid above the collision kernel's region limit", APIC_ERR_UNSUPPORTED);
             const double per_cta = (double)phys / regions;
             const size_t per = (size_t)std::min(std::ceil(per_cta) + 32.0, std::ceil(2.0 * pmax * per_cta) + 256.0);
             p.cands = dalloc<CandRec32>(per * regions);
@@ -1913,7 +1914,7 @@ struct Sim1D {
     void launch_kernels_c32(const Params1D& q, int blocks, size_t post_smem, unsigned post, EvPair& ev) {
         k_pass1d_c32<VDIM, DIR><<<blocks, kThreads, (size_t)cfg.nx * 12, stream>>>(q);
         if (VDIM == 3 && cfg.nmodels > 0 && (q.mode & kModeSyncMcc))
-            k_collide1d_c32<VDIM, DIR><<<148 * 8, kCollideThreads, 0, stream>>>(q);
+            k_collide1d_c32<VDIM, DIR><<<148 * 4, kCollideThreads, 0, stream>>>(q);
         if (timing) cudaEventRecord(ev.b, stream);
         cudaLaunchConfig_t lc = {};
         lc.gridDim = dim3(1);

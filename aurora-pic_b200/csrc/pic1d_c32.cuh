@@ -33,7 +33,7 @@ constexpr unsigned kCompactSteps = 32;      // steps between compactions (at ste
 
 // resident CTAs of k_pass1d_c32 per SM (register budget of the launch bounds)
 #ifndef APIC_C32_MIN_BLOCKS
-#define APIC_C32_MIN_BLOCKS 3
+#define APIC_C32_MIN_BLOCKS 4
 #endif
 constexpr int kMinBlocks32 = APIC_C32_MIN_BLOCKS;
 
@@ -347,14 +347,36 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks32) k_pass1d_c32(Params1D 
 
 // The collision candidates of the pass, one per thread in full warps: the
 // null-collision loop (collide3f), then the rest of the particle's step as in
-// the pass (re-initialise, kick, drift, walls, deposit, write back).
+// the pass (re-initialise, kick, drift, walls, deposit, write back).  The
+// pass's regions hold few records each, so every CTA first takes the prefix
+// sums of the region counts and numbers the candidates densely.
 constexpr int kCollideThreads = 128;
+constexpr int kMaxRegions = 2048;  // regions (CTAs of the pass) the dense numbering covers
 template <int VDIM, bool DIRICHLET>
 __global__ void __launch_bounds__(kCollideThreads) k_collide1d_c32(Params1D p) {
     __shared__ unsigned long long s_cand, s_null, s_chan[kMaxModels][kMaxChannels], s_lost[kMaxSpecies][2];
     __shared__ double s_energy[kMaxModels][kMaxChannels], s_lost_energy[kMaxSpecies][2];
     __shared__ unsigned s_dead[kMaxSpecies];
+    __shared__ unsigned s_start[kMaxRegions + 1];  // first dense index of each region
     const int tid = threadIdx.x;
+    const unsigned regions = min(p.cand_regions, (unsigned)kMaxRegions);
+    {
+        // exclusive prefix sums of the region counts, 16 per thread
+        using Scan = cub::BlockScan<unsigned, kCollideThreads>;
+        __shared__ typename Scan::TempStorage tmp;
+        constexpr int PER = kMaxRegions / kCollideThreads;
+        unsigned c[PER], o[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const unsigned r = tid * PER + k;
+            c[k] = r < regions ? __ldg(p.cand_count + r) : 0u;
+        }
+        unsigned total;
+        Scan(tmp).ExclusiveSum(c, o, total);
+#pragma unroll
+        for (int k = 0; k < PER; ++k) s_start[tid * PER + k] = o[k];
+        if (tid == 0) s_start[kMaxRegions] = total;
+    }
     if (tid < kMaxModels * kMaxChannels) {
         (&s_chan[0][0])[tid] = 0ull;
         (&s_energy[0][0])[tid] = 0.0;
@@ -368,16 +390,20 @@ __global__ void __launch_bounds__(kCollideThreads) k_collide1d_c32(Params1D p) {
     __syncthreads();
     DevState* st = p.st;
     const unsigned mode = p.mode;
-    // candidate q lives in region q / cand_per_region (one per CTA of the pass)
-    const unsigned span = p.cand_regions * p.cand_per_region;
+    const unsigned ntotal = s_start[kMaxRegions];
     const uint32_t mcc_step = (uint32_t)(st->step - 1ull);
     const float dt = (float)p.dt;
     const float dt_in = dt * (1.0f - kFltEpsilon);  // largest first wait kept inside the step
     const int nx = p.nx;
     const int ncell = DIRICHLET ? nx - 1 : nx;
-    for (unsigned q = blockIdx.x * kCollideThreads + tid; q < span; q += gridDim.x * kCollideThreads) {
-        if (q % p.cand_per_region >= __ldg(p.cand_count + q / p.cand_per_region)) continue;
-        const CandRec32 rec = p.cands[q];
+    for (unsigned d = blockIdx.x * kCollideThreads + tid; d < ntotal; d += gridDim.x * kCollideThreads) {
+        // region holding dense index d: the last region whose start is <= d
+        unsigned lo = 0, hi = regions;
+        while (hi - lo > 1) {
+            const unsigned mid = (lo + hi) >> 1;
+            if (s_start[mid] <= d) lo = mid; else hi = mid;
+        }
+        const CandRec32 rec = p.cands[(size_t)lo * p.cand_per_region + (d - s_start[lo])];
         const int s = (int)rec.species;
         const SpeciesDev& S = p.sp[s];
         const MccModel32& M = p.model32[S.model];
