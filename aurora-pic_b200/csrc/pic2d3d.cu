@@ -18,10 +18,6 @@
 // re-sorted by cell every `sort_interval` steps so gathers and atomics stay
 // local.  Compiled with --fmad=false: particle arithmetic follows the
 // reference operation by operation.
-#include <cub/block/block_radix_sort.cuh>
-#include <cub/block/block_reduce.cuh>
-#include <cub/block/block_scan.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -990,103 +986,24 @@ __global__ void k_cell_hist32(ParamsND p, SpeciesND S, int buf, unsigned* count)
     if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + key, (unsigned)__popc(peers));
 }
 
-// The scatter of the FP32 counting sort with coalesced writes: each CTA sorts
-// a chunk of kSortChunk particles by cell in shared memory (radix sort over the
-// bits the chunk's cell range needs), reserves each cell run of the chunk with
-// one atomic on that cell's cursor, and writes the particles in sorted order,
-// so every lane writes a run of consecutive slots instead of single particles
-// spread over the array.  The order inside a cell depends on the CTAs' timing;
-// nothing downstream depends on it (the deposit sums integers, read-backs
-// follow the particle ids).
-constexpr int kSortItems = 8;
-constexpr int kSortChunk = kThreads * kSortItems;
 template <int DIM>
-__global__ void __launch_bounds__(kThreads) k_cell_scatter_sorted(ParamsND p, SpeciesND S, int from,
-                                                                  unsigned* cursor) {
-    using Sort = cub::BlockRadixSort<unsigned, kThreads, kSortItems, unsigned short>;
-    using ReduceU = cub::BlockReduce<unsigned, kThreads>;
-    using ScanI = cub::BlockScan<int, kThreads>;
-    __shared__ union {
-        typename Sort::TempStorage sort;
-        typename ReduceU::TempStorage reduce;
-        typename ScanI::TempStorage scan;
-    } tmp;
-    __shared__ unsigned s_key[kSortChunk];   // sorted keys, then a staged payload array
-    __shared__ unsigned s_base[kSortChunk];  // destination of each run, at the run's head
-    __shared__ unsigned s_kmin, s_kmax;
+__global__ void k_cell_scatter32(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
+    const unsigned i = blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = i < S.n;
     const int to = from ^ 1;
-    const unsigned base = blockIdx.x * kSortChunk;
-    const int tid = threadIdx.x;
-    const unsigned n = S.n;
-    const unsigned nvalid = n > base ? min(n - base, (unsigned)kSortChunk) : 0u;
-    // keys (linear cell index) in a blocked arrangement, coalesced through shared memory
-    for (int k = tid; k < kSortChunk; k += kThreads)
-        s_key[k] = (unsigned)k < nvalid ? linear_cell(p, S.cell[from][base + k]) : 0xFFFFFFFFu;
-    __syncthreads();
-    unsigned key[kSortItems];
-    unsigned short rank[kSortItems];
-    unsigned lo = 0xFFFFFFFFu, hi = 0u;
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const int pos = tid * kSortItems + k;
-        key[k] = s_key[pos];
-        rank[k] = (unsigned short)pos;
-        if ((unsigned)pos < nvalid) { lo = min(lo, key[k]); hi = max(hi, key[k]); }
-    }
-    const unsigned kmin = ReduceU(tmp.reduce).Reduce(lo, cub::Min());
-    __syncthreads();
-    const unsigned kmax = ReduceU(tmp.reduce).Reduce(hi, cub::Max());
-    if (tid == 0) { s_kmin = kmin; s_kmax = kmax; }
-    __syncthreads();
-    // keys relative to the chunk's smallest; the padding sorts last
-    const unsigned range = s_kmax >= s_kmin ? s_kmax - s_kmin + 1u : 0u;
-    const int bits = range ? 32 - __clz(range) : 1;
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k)
-        key[k] = (unsigned)(tid * kSortItems + k) < nvalid ? key[k] - s_kmin : range;
-    Sort(tmp.sort).Sort(key, rank, 0, bits);
-    __syncthreads();
-    // run heads and tails in the sorted chunk
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) s_key[tid * kSortItems + k] = key[k];
-    __syncthreads();
-    int head[kSortItems];
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const int pos = tid * kSortItems + k;
-        head[k] = (pos == 0 || s_key[pos - 1] != key[k]) ? pos : 0;
-    }
-    ScanI(tmp.scan).InclusiveScan(head, head, cub::Max());
-    // each run's tail reserves the run's slots with one atomic
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const int pos = tid * kSortItems + k;
-        if ((unsigned)pos >= nvalid) continue;
-        const bool tail = pos + 1 == (int)nvalid || s_key[pos + 1] != key[k];
-        if (tail) s_base[head[k]] = atomicAdd(cursor + key[k] + s_kmin, (unsigned)(pos - head[k] + 1));
-    }
-    __syncthreads();
-    unsigned dst[kSortItems];
-#pragma unroll
-    for (int k = 0; k < kSortItems; ++k) {
-        const int pos = tid * kSortItems + k;
-        dst[k] = s_base[head[k]] + (unsigned)(pos - head[k]);
-    }
-    // the payload, one array at a time staged through shared memory
-    auto move = [&](const unsigned* src, unsigned* out) {
-        __syncthreads();
-        for (int k = tid; k < kSortChunk; k += kThreads) s_key[k] = (unsigned)k < nvalid ? src[base + k] : 0u;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < kSortItems; ++k)
-            if ((unsigned)(tid * kSortItems + k) < nvalid) out[dst[k]] = s_key[rank[k]];
-    };
-    move(S.cell[from], S.cell[to]);
-    for (int a = 0; a < DIM; ++a)
-        move(reinterpret_cast<const unsigned*>(S.off[from][a]), reinterpret_cast<unsigned*>(S.off[to][a]));
-    for (int a = 0; a < 3; ++a)
-        move(reinterpret_cast<const unsigned*>(S.vel[from][a]), reinterpret_cast<unsigned*>(S.vel[to][a]));
-    move(S.id[from], S.id[to]);
+    const unsigned c = valid ? S.cell[from][i] : 0u;
+    const unsigned key = valid ? linear_cell(p, c) : 0xFFFFFFFFu;
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (valid && lane == leader) base = atomicAdd(cursor + key, (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!valid) return;
+    const unsigned o = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
+    S.cell[to][o] = c;
+    for (int a = 0; a < DIM; ++a) S.off[to][a][o] = S.off[from][a][i];
+    for (int a = 0; a < 3; ++a) S.vel[to][a][o] = S.vel[from][a][i];
+    S.id[to][o] = S.id[from][i];
 }
 
 // ---- particle sort by cell -------------------------------------------------------
@@ -2078,9 +1995,8 @@ struct SimND {
         k_scan_blocks<<<1, kThreads, 0, stream>>>(block_sums, nb);
         k_scan_add<<<nb, kThreads, 0, stream>>>(cell_offset, block_sums, (unsigned)ncells);
         if (fp32) {
-            const unsigned chunks = (S.n + kSortChunk - 1) / kSortChunk;
-            if (cfg.dims == 2) k_cell_scatter_sorted<2><<<chunks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
-            else k_cell_scatter_sorted<3><<<chunks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+            if (cfg.dims == 2) k_cell_scatter32<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+            else k_cell_scatter32<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
         } else if (cfg.dims == 2) {
             k_cell_scatter<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
         } else {
