@@ -656,12 +656,15 @@ def bench_plasma(args, rank, dist):
     # case of the same deck, scaled by the particles per launch (the state is
     # streamed once per launch, so traffic grows in proportion)
     traffic, traffic_note = None, None
+    items = push_items or (4 if dims == 2 else 2)
+    run_kernel = prec == apic.FP32 and items in (2, 4)  # consecutive particles per thread (k_push32_run)
     if prec == apic.FP32:
         captured = {2: 4194304, 3: 16777216}[dims]
-        t = _profiled_traffic(f"k_push32_plasma{dims}d_fp32.md")
+        name = f"k_push32_run_plasma{dims}d_fp32.md" if run_kernel and dims == 2 else f"k_push32_plasma{dims}d_fp32.md"
+        t = _profiled_traffic(name)
         if t:
             traffic = t * (P / 2) / captured
-            traffic_note = f"ncu capture of {captured} particles per launch scaled to {P // 2}"
+            traffic_note = f"ncu capture ({name}) of {captured} particles per launch scaled to {P // 2}"
     form = ("FP32 particles: packed int32 cell + FP32 offsets + FP32 velocities; FP64 fixed-point deposit, "
             "FP64 spectral solve; error against the FP64 oracle after 10 steps (tests/test_gpu_nd.py): positions "
             "< 1e-5 cell, velocities < 1e-5 thermal, fields < 1e-4") if prec == apic.FP32 else \
@@ -677,7 +680,8 @@ def bench_plasma(args, rank, dist):
                 "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": traffic, "traffic_note": traffic_note, "peak_kind": peak_kind,
-                     "kernel": ("k_push32" if prec == apic.FP32 else "k_push") + f"<{dims}, boris>",
+                     "kernel": (("k_push32_run" if run_kernel else "k_push32_step") if prec == apic.FP32 else "k_push")
+                     + f"<{dims}, boris, items={items}>",
                      "bytes_per_particle_step": bpp, "push_ms": per_step_push,
                      "solve_ms": solve_ms / max(nsteps, 1), "sort_ms_per_step": sort_ms / max(nsteps, 1)},
         "gpu_launches": launches,
