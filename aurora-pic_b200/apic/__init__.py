@@ -733,6 +733,103 @@ def field_solve_mixed_2d(n, length, periodic_axis, permittivity, lower_potential
     return phi, E.reshape(2, N)
 
 
+class ApcInfo(C.Structure):
+    _fields_ = [
+        ("units", C.c_int), ("relative_permittivity", C.c_double), ("permittivity", C.c_double),
+        ("velocity_dimensions", C.c_int), ("collisions_enabled", C.c_int), ("collision_signature", C.c_uint64),
+        ("candidates", C.c_uint64), ("null_collisions", C.c_uint64), ("nchannels", C.c_size_t),
+        ("boundary_loss_origin_step", C.c_uint64), ("power_transfer_origin_step", C.c_uint64),
+        ("spatial_average_enabled", C.c_int), ("step", C.c_uint64), ("time", C.c_double), ("nspecies", C.c_size_t),
+    ]
+
+
+def _bind_apc():
+    L = lib()
+    if getattr(L, "_apc_bound", False):
+        return L
+    L.apic_apc_last_error.restype = C.c_char_p
+    L.apic_apc_read.argtypes = [C.c_char_p, C.POINTER(C.c_void_p)]
+    L.apic_apc_free.argtypes = [C.c_void_p]
+    L.apic_apc_write.argtypes = [C.c_void_p, C.c_char_p]
+    L.apic_apc_get_info.argtypes = [C.c_void_p, C.POINTER(ApcInfo)]
+    L.apic_apc_channel.argtypes = [C.c_void_p, C.c_size_t, _U64P, _DP]
+    L.apic_apc_species.argtypes = [C.c_void_p, C.c_size_t, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t),
+                                   C.POINTER(BoundaryLoss), _DP]
+    L.apic_apc_particles.argtypes = [C.c_void_p, C.c_size_t, _DP, _DP, _DP, _DP, _DP, _U8P]
+    L.apic_sim1d_load_checkpoint.argtypes = [C.c_void_p, C.c_void_p]
+    L.apic_sim1d_save_checkpoint.argtypes = [C.c_void_p, C.c_void_p, C.c_char_p]
+    L._apc_bound = True
+    return L
+
+
+class Checkpoint:
+    """A 1D3V checkpoint (.apc version 12) read on the host (apic_apc_*)."""
+
+    def __init__(self, path):
+        L = _bind_apc()
+        h = C.c_void_p()
+        rc = L.apic_apc_read(path.encode(), C.byref(h))
+        if rc:
+            raise ApicError(rc, L.apic_apc_last_error().decode())
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _bind_apc().apic_apc_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def write(self, path):
+        L = _bind_apc()
+        rc = L.apic_apc_write(self.h, path.encode())
+        if rc:
+            raise ApicError(rc, L.apic_apc_last_error().decode())
+
+    def info(self) -> ApcInfo:
+        out = ApcInfo()
+        _bind_apc().apic_apc_get_info(self.h, C.byref(out))
+        return out
+
+    def channel(self, k):
+        c, e = C.c_uint64(), C.c_double()
+        _bind_apc().apic_apc_channel(self.h, k, C.byref(c), C.byref(e))
+        return c.value, e.value
+
+    def species(self, k):
+        name = C.create_string_buffer(256)
+        n = C.c_size_t()
+        loss = BoundaryLoss()
+        w = C.c_double()
+        _bind_apc().apic_apc_species(self.h, k, name, 256, C.byref(n), C.byref(loss), C.byref(w))
+        return name.value.decode(), n.value, loss, w.value
+
+    def particles(self, k):
+        n = self.species(k)[1]
+        out = {key: np.zeros(n) for key in ("x", "v", "vy", "vz", "vh")}
+        alive = np.zeros(n, np.uint8)
+        _bind_apc().apic_apc_particles(self.h, k, *[dptr(out[key]) for key in ("x", "v", "vy", "vz", "vh")],
+                                       alive.ctypes.data_as(_U8P))
+        out["alive"] = alive
+        return out
+
+
+def _sim1d_load_checkpoint(self, checkpoint: Checkpoint):
+    _check(_bind_apc().apic_sim1d_load_checkpoint(self.h, checkpoint.h), self.h)
+
+
+def _sim1d_save_checkpoint(self, meta: Checkpoint, path):
+    _check(_bind_apc().apic_sim1d_save_checkpoint(self.h, meta.h, path.encode()), self.h)
+
+
+Simulation1D.load_checkpoint = _sim1d_load_checkpoint
+Simulation1D.save_checkpoint = _sim1d_save_checkpoint
+
+
 class ParticleState:
     """An AuroraPIC particle-state file (.aps version 1, the reference's
     external initial state), parsed by the library: `species` maps each name

@@ -39,6 +39,7 @@
 #include <thread>
 #include <vector>
 
+#include "apc_internal.h"
 #include "apic_common.cuh"
 #include "apic_mcc.cuh"
 #include "apic_mcc32.cuh"
@@ -2323,6 +2324,107 @@ struct Sim1D {
         return st_h;
     }
 
+    // Simulation::load_checkpoint, src/Simulation.cpp:2018-2899, for the parts
+    // the device holds (see apic_sim1d_load_checkpoint).
+    void load_checkpoint(const Apc& c) {
+        const double rel = cfg.relative_permittivity == 0.0 ? 1.0 : cfg.relative_permittivity;
+        require(c.units == cfg.units && c.relative_permittivity == rel && c.permittivity == p.eps,
+                "checkpoint unit system does not match 1D config");
+        require(c.velocity_dimensions == cfg.velocity_dimensions,
+                "checkpoint velocity dimensions do not match 1D config");
+        size_t nch = 0;
+        for (int m = 0; m < cfg.nmodels; ++m) nch += (size_t)cfg.models[m].nch;
+        require(c.channel_counts.size() == nch, "checkpoint collision diagnostics do not match 1D config");
+        require(c.losses.size() == (size_t)cfg.nspecies,
+                "checkpoint boundary-loss species count does not match 1D config");
+        require(c.electric_work.size() == (size_t)cfg.nspecies,
+                "checkpoint power-transfer species count does not match 1D config");
+        require(!c.spatial_average_enabled && !sa.on, "checkpoint spatial-average contract does not match 1D config");
+        require(c.species.size() == (size_t)cfg.nspecies, "checkpoint species count does not match config");
+        for (int s = 0; s < cfg.nspecies; ++s)
+            require(c.species[s].x.size() <= cfg.species[s].capacity,
+                    "checkpoint particle count exceeds max_particles_per_species", APIC_ERR_CAPACITY);
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            const Apc::Species& sp = c.species[s];
+            load(s, sp.x.size(), sp.x.data(), sp.v.data(), sp.vh.data(), sp.vy.data(), sp.vz.data(), sp.alive.data());
+        }
+        // the ledgers continue from the file's totals
+        DevState h = read_state();
+        h.candidates = c.candidates;
+        h.nulls = c.null_collisions;
+        size_t k = 0;
+        for (int m = 0; m < cfg.nmodels; ++m)
+            for (int ch = 0; ch < cfg.models[m].nch; ++ch, ++k) {
+                h.chan[m][ch] = c.channel_counts[k];
+                h.chan_energy[m][ch] = c.channel_energy[k];
+            }
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            h.lost[s][0] = c.losses[s].left;
+            h.lost[s][1] = c.losses[s].right;
+            h.lost_energy[s][0] = c.losses[s].energy_left;
+            h.lost_energy[s][1] = c.losses[s].energy_right;
+        }
+        APIC_CUDA(cudaMemcpyAsync(st, &h, sizeof h, cudaMemcpyHostToDevice, stream));
+        resume(c.time, c.step);
+        if (p.ledger) {  // resume() keeps the ledger; the file's work replaces it
+            double w[kMaxSpecies] = {0, 0, 0, 0};
+            for (int s = 0; s < cfg.nspecies; ++s) w[s] = c.electric_work[s].second;
+            APIC_CUDA(cudaMemcpyAsync(&st->work[0], w, sizeof w, cudaMemcpyHostToDevice, stream));
+        }
+        APIC_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // Simulation::save_checkpoint, src/Simulation.cpp:1812-2015, of the device
+    // run with meta's identity lines (see apic_sim1d_save_checkpoint).
+    void save_checkpoint(const Apc& meta, const std::string& path) {
+        require(!sa.on, "checkpoints of runs with spatial averaging are written by the FP64 host path only",
+                APIC_ERR_UNSUPPORTED);
+        require(!meta.spatial_average_enabled && meta.spatial_average_nx == cfg.nx &&
+                    meta.species.size() == (size_t)cfg.nspecies,
+                "checkpoint metadata does not match 1D config");
+        size_t nch = 0;
+        for (int m = 0; m < cfg.nmodels; ++m) nch += (size_t)cfg.models[m].nch;
+        require(meta.channel_counts.size() == nch, "checkpoint collision diagnostics do not match 1D config");
+        Apc c = meta;
+        const double rel = cfg.relative_permittivity == 0.0 ? 1.0 : cfg.relative_permittivity;
+        c.units = cfg.units;
+        c.relative_permittivity = rel;
+        c.permittivity = p.eps;
+        c.velocity_dimensions = cfg.velocity_dimensions;
+        finish();
+        const DevState h = read_state();
+        c.candidates = h.candidates;
+        c.null_collisions = h.nulls;
+        size_t k = 0;
+        for (int m = 0; m < cfg.nmodels; ++m)
+            for (int ch = 0; ch < cfg.models[m].nch; ++ch, ++k) {
+                c.channel_counts[k] = h.chan[m][ch];
+                c.channel_energy[k] = h.chan_energy[m][ch];
+            }
+        c.losses.resize(cfg.nspecies);
+        c.electric_work.resize(cfg.nspecies);
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            c.losses[s].name = meta.species[s].name;
+            c.losses[s].left = h.lost[s][0];
+            c.losses[s].right = h.lost[s][1];
+            c.losses[s].energy_left = h.lost_energy[s][0];
+            c.losses[s].energy_right = h.lost_energy[s][1];
+            c.electric_work[s] = {meta.species[s].name, p.ledger ? h.work[s] : 0.0};
+        }
+        if (!p.ledger) c.power_transfer_origin = step;  // counted from here
+        c.step = step;
+        c.time = time;
+        for (int s = 0; s < cfg.nspecies; ++s) {
+            Apc::Species& sp = c.species[s];
+            sp.name = meta.species[s].name;
+            const size_t n = h.n[s] - h.holes[s];
+            sp.x.resize(n); sp.v.resize(n); sp.vy.resize(n); sp.vz.resize(n); sp.vh.resize(n);
+            sp.alive.assign(n, 1);
+            read_particles(s, n, sp.x.data(), sp.v.data(), sp.vh.data(), sp.vy.data(), sp.vz.data());
+        }
+        apc_write(path, c);
+    }
+
     void read_fields(double* rho, double* phi, double* E) {
         sync_status();
         const size_t bytes = cfg.nx * sizeof(double);
@@ -2472,6 +2574,16 @@ int apic_sim1d_set_wait_limit(apic_sim1d* sim, double seconds) {
         apic::require(std::isfinite(seconds) && seconds > 0.0, "wait limit must be positive and finite");
         sim->impl.wait_limit_s = seconds;
     });
+}
+
+int apic_sim1d_load_checkpoint(apic_sim1d* sim, const apic_apc* checkpoint) {
+    if (!sim || !checkpoint) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.load_checkpoint(checkpoint->c); });
+}
+
+int apic_sim1d_save_checkpoint(apic_sim1d* sim, const apic_apc* meta, const char* path) {
+    if (!sim || !meta || !path) return APIC_ERR_INVALID;
+    return guarded(sim, [&] { sim->impl.save_checkpoint(meta->c, path); });
 }
 
 int apic_sim1d_count(apic_sim1d* sim, int species, size_t* n) {

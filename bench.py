@@ -424,7 +424,7 @@ def bench_ccp1d(args, rank, dist):
     bytes_per_pstep = 64 if prec == apic.FP64 else 40
     per_pass_ms = pass_ms / max(passes, 1)
     achieved = bytes_per_pstep * mean_n / (per_pass_ms * 1e-3) / 1e9
-    traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md" if prec == apic.FP64 else "k_pass1d_ccp1d_fp32.md")
+    traffic = _profiled_traffic("k_pass1d_ccp1d_fp64.md" if prec == apic.FP64 else "k_pass1d_c32_ccp1d_fp32.md")
     sim.close()
     # the other storage form of the same discharge, device-timed the same way
     other = apic.FP32 if prec == apic.FP64 else apic.FP64

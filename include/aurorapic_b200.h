@@ -709,6 +709,59 @@ APIC_EXPORT int apic_aps_write(const char* path, int dimension, int units, size_
                                const char* const* names, const size_t* counts, const double* const* pos,
                                const double* const* vel, int overwrite, uint64_t* signature);
 
+/* ---- 1D3V checkpoints (.apc version 12) --------------------------------------
+ * The restart files of Simulation::save_checkpoint / load_checkpoint
+ * (src/Simulation.cpp:1812-2015, :2018-2899), the reference's route for 1D3V
+ * state (its .aps files refuse 1D3V, src/Simulation.cpp:358-363).  Read on the
+ * host into their parts; written back line for line in the reference's form
+ * (numbers at 17 significant digits), so a file read and written again is
+ * byte-identical.  Version 12 only (older files: APIC_ERR_UNSUPPORTED). */
+typedef struct apic_apc apic_apc;
+typedef struct {
+    int units;                      /* apic_units */
+    double relative_permittivity, permittivity;
+    int velocity_dimensions;
+    int collisions_enabled;
+    uint64_t collision_signature;
+    uint64_t candidates, null_collisions;
+    size_t nchannels;               /* every model's channels, in model order */
+    uint64_t boundary_loss_origin_step, power_transfer_origin_step;
+    int spatial_average_enabled;
+    uint64_t step;
+    double time;
+    size_t nspecies;
+} apic_apc_info;
+APIC_EXPORT const char* apic_apc_last_error(void);
+/* load_checkpoint's structural checks and messages (the ones that need no configuration) */
+APIC_EXPORT int apic_apc_read(const char* path, apic_apc** out);
+APIC_EXPORT void apic_apc_free(apic_apc* checkpoint);
+APIC_EXPORT int apic_apc_write(const apic_apc* checkpoint, const char* path);
+APIC_EXPORT int apic_apc_get_info(const apic_apc* checkpoint, apic_apc_info* out);
+/* collision_totals / collision_energy_totals entry k */
+APIC_EXPORT int apic_apc_channel(const apic_apc* checkpoint, size_t k, uint64_t* count, double* energy);
+/* species k: name, particle count (dead entries included), boundary losses, electric work */
+APIC_EXPORT int apic_apc_species(const apic_apc* checkpoint, size_t k, char* name, size_t name_capacity,
+                                 size_t* count, apic_boundary_loss* loss, double* electric_work);
+/* species k's particles as arrays of its particle count */
+APIC_EXPORT int apic_apc_particles(const apic_apc* checkpoint, size_t k, double* x, double* v, double* vy,
+                                   double* vz, double* v_half, uint8_t* alive);
+/* Simulation::load_checkpoint on the device: the configuration checks and
+ * messages of the reference that apply (units, velocity dimensions, species
+ * and channel counts, capacity, a spatial-average contract), then the
+ * particles (dead entries dropped), collision totals, boundary losses,
+ * electric work (when the ledger is enabled), step and time, and the field of
+ * the restored state (deposit_and_solve).  The collision-model signature and
+ * the engine state are not checked: the device draws from its own
+ * counter-based streams. */
+APIC_EXPORT int apic_sim1d_load_checkpoint(apic_sim1d* sim, const apic_apc* checkpoint);
+/* Simulation::save_checkpoint of the device run: its particles (time-centred v,
+ * as after step()), collision totals, boundary losses, electric work (without
+ * the ledger: zero, counted from this step), step and time, with the
+ * collision-model line, species names, engine state and disabled
+ * campaign-diagnostics block taken from `meta` (a checkpoint of the same
+ * configuration, e.g. the one the run was restarted from). */
+APIC_EXPORT int apic_sim1d_save_checkpoint(apic_sim1d* sim, const apic_apc* meta, const char* path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -238,6 +238,8 @@ def ref() -> C.CDLL:
         L.ref1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, C.c_size_t]
         L.ref1d_losses.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _DP, _DP]
         L.ref1d_rng_state.argtypes = [C.c_void_p, C.c_char_p, _U64P]
+        L.ref1d_save_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
+        L.ref1d_load_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
         L.ref1d_electric_work.restype = C.c_double
         L.ref1d_electric_work.argtypes = [C.c_void_p, C.c_int]
         L.ref_deposit_solve_gather_1d.argtypes = [
@@ -472,6 +474,12 @@ class Ref1D:
         rho, phi, E = np.zeros(n), np.zeros(n), np.zeros(n)
         ref().ref1d_get_fields(self.h, dptr(rho), dptr(phi), dptr(E))
         return rho, phi, E
+
+    def save_checkpoint(self, path):
+        self._chk(ref().ref1d_save_checkpoint(self.h, path.encode()))
+
+    def load_checkpoint(self, path):
+        self._chk(ref().ref1d_load_checkpoint(self.h, path.encode()))
 
     def rng_state(self):
         st = np.zeros(313, np.uint64)

@@ -242,6 +242,21 @@ int ref1d_losses(void* h, int species, size_t* left, size_t* right, double* elef
     return 0;
 }
 
+// Simulation::save_checkpoint / load_checkpoint of the reference itself.
+int ref1d_save_checkpoint(void* h, const char* path) {
+    try {
+        static_cast<Ref1D*>(h)->sim->save_checkpoint(path);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
+int ref1d_load_checkpoint(void* h, const char* path) {
+    try {
+        static_cast<Ref1D*>(h)->sim->load_checkpoint(path);
+        return 0;
+    } catch (const std::exception& e) { return fail(e); }
+}
+
 // The engine state of Simulation's private rng_, read back through the
 // reference's own checkpoint writer (the "rng" line, src/Simulation.cpp:2004).
 int ref1d_rng_state(void* h, const char* path, uint64_t* out313) {
