@@ -8,7 +8,7 @@
 // cumulative rates (:596-625), the channel kinematics of apply_channel
 // (:762-829: elastic recoil, threshold losses, ionization halving the
 // remaining energy, backward and Henyey-Greenstein scattering, resonant charge
-// exchange) and ionization secondaries.  Cross sections are the same tables,
+// exchange, attachment) and ionization secondaries.  Cross sections are the same tables,
 // rounded to float, interpolated linearly in energy between the bracketing
 // rows (CrossSectionTable::evaluate, :221-237) found through the FP64 form's
 // log-energy bracket index.
@@ -234,6 +234,7 @@ __device__ inline void normal_pair32(R& r, float stddev, float& a, float& b) {
 struct CollideResult32 {
     unsigned candidates = 0, nulls = 0;
     unsigned error = 0;
+    bool removed = false;  // attachment
 };
 
 __device__ __forceinline__ double energy64(double mass, const float v[3]) {
@@ -288,6 +289,12 @@ __device__ inline void collide3f(const MccModel32& m, float v[3], float dt, floa
         } else {
             const MccChannel32& c = m.ch[ci];
             const double before = energy64(m.particle_mass, v);
+            if (c.process == kAttachment) {  // the projectile is removed, src/Collision.cpp:770-773
+                v[0] = v[1] = v[2] = 0.0f;
+                on_collision(ci, energy64(m.particle_mass, v) - before);
+                res.removed = true;
+                return;
+            }
             if (c.process == kChargeExchange) {
                 v[0] = vn[0]; v[1] = vn[1]; v[2] = vn[2];
             } else {

@@ -132,6 +132,7 @@ struct Batch {
     unsigned qcap;
     int max_runs;
     const MccModelDev* model;  // in device memory: the kernels take references into it
+    const MccModel32* model32; // the same model in single precision (FP32 form)
 };
 
 template <class T>
@@ -254,6 +255,56 @@ __device__ __forceinline__ void finish_candidate(const MccModelDev& M, const Run
     if (!r.removed) atomicAdd(t.surv, 1u);
     atomicAdd(t.vsum, to_fixed((double)vs[0], R.vscale));
     atomicAdd(t.esum, to_fixed(sq3((double)vs[0], (double)vs[1], (double)vs[2]), R.escale));
+    if (err) atomicOr(t.err, err);
+}
+
+// The FP32 form of finish_candidate: the collision loop in FP32 (collide3f) on
+// the float velocity, the first waiting time from the same first 64-bit draw
+// that made the electron a candidate (rounded to a 23-bit uniform, kept inside
+// the step), the later uniforms from the rest of the electron's Philox stream.
+__device__ __forceinline__ void finish_candidate32(const MccModelDev& M, const MccModel32& M32, const RunCfg& R,
+                                                   uint32_t step, uint32_t first, const Candidate& e,
+                                                   const Tally& t) {
+    float v[3];
+    for (int a = 0; a < 3; ++a) v[a] = arr<float>(R.v[a])[e.particle];
+    const float hk = (float)R.half_kick;
+    v[0] += hk;  // the push kernel's first half kick, repeated
+    Philox32 rng(R.seed, e.particle, step, 0u);
+    const uint32_t w0 = rng.next(), w1 = rng.next();
+    const uint64_t d0 = (uint64_t)w1 << 32 | w0;
+    const float dt = (float)R.dt;
+    const float u0 = ((float)(d0 >> 41) + 0.5f) * 1.1920928955078125e-7f;
+    const float first_wait = fminf(-__logf(u0) * M32.inv_max_frequency, dt * (1.0f - kFltEpsilon));
+    CollideResult32 r;
+    unsigned nsec = 0;
+    const uint32_t li = e.particle - first;
+    const uint32_t local_chunk = first / kChunk;
+    unsigned err = 0;
+    collide3f(
+        M32, v, dt, first_wait, rng, r, [&](float speed) { return frequency_bound_ok_far(M, (double)speed); },
+        [&](int ch, double) { atomicAdd(&t.counts[ch], 1u); },
+        [&](int, const float* vs, const float*) {
+            if (!R.branching) return;  // fixed population: secondaries are not followed
+            if (nsec >= (unsigned)kMaxBirthsPerElectron) { err |= kErrBirths; return; }
+            const unsigned bi = atomicAdd(t.births, 1u);
+            if (bi >= (unsigned)kChunk) { err |= kErrBirths; return; }
+            const size_t at = (size_t)local_chunk * kChunk + bi;
+            for (int a = 0; a < 3; ++a) arr<float>(R.sv[a])[at] = vs[a];
+            R.skey[at] = li * kMaxBirthsPerElectron + nsec;
+            ++nsec;
+        });
+    err |= r.error;
+    v[0] += hk;
+    const double s2 = sq3((double)v[0], (double)v[1], (double)v[2]);
+    if (s2 > R.s2_max) err |= kErrMaxEnergy;
+    for (int a = 0; a < 3; ++a) arr<float>(R.v[a])[e.particle] = v[a];
+    if (R.branching) R.alive[e.particle] = r.removed ? 0 : 1;
+    atomicMax(t.emax, (unsigned long long)__double_as_longlong(s2));
+    atomicAdd(t.cand, (unsigned long long)r.candidates);
+    if (r.nulls) atomicAdd(t.nulls, (unsigned long long)r.nulls);
+    if (!r.removed) atomicAdd(t.surv, 1u);
+    atomicAdd(t.vsum, to_fixed((double)v[0], R.vscale));
+    atomicAdd(t.esum, to_fixed(s2, R.escale));
     if (err) atomicOr(t.err, err);
 }
 
@@ -406,7 +457,10 @@ __global__ void __launch_bounds__(kThreads, 4) k_swarm_collide(Batch b) {
         ChunkPartial& P = b.part[e.chunk];
         const uint32_t first = b.chunk_first[e.chunk];
         const Tally tl{&P.vsum, &P.esum, &P.emax_bits, &P.cand, &P.nulls, P.counts, &P.surv, &P.births, &S.error};
-        finish_candidate<T>(*b.model, R, S.step, first, e, tl);
+        if constexpr (sizeof(T) == 4)
+            finish_candidate32(*b.model, *b.model32, R, S.step, first, e, tl);
+        else
+            finish_candidate<T>(*b.model, R, S.step, first, e, tl);
     }
 }
 
@@ -842,6 +896,7 @@ struct Server {
     ChunkPartial* d_part = nullptr;
     Candidate* d_queue = nullptr;
     MccModelDev* d_model = nullptr;
+    MccModel32* d_model32 = nullptr;
     unsigned* d_qlen = nullptr;
     size_t qcap = 0;
     // host mirrors
@@ -887,6 +942,7 @@ struct Server {
         b.qcap = (unsigned)qcap;
         b.max_runs = conf.max_runs;
         b.model = d_model;
+        b.model32 = d_model32;
         return b;
     }
 
@@ -925,6 +981,10 @@ struct Server {
         neutral_density = m.neutral_density;
         max_frequency = m.max_frequency;
         d_model = arena.upload(&model, 1);
+        MccModel32 model32;
+        build_model32(m, arena, model, model32);
+        d_model32 = arena.upload(&model32, 1);
+        APIC_CUDA(cudaStreamSynchronize(stream));
         // the collision-candidate queue has one entry per electron the pool can
         // hold (every electron of a step may be a candidate)
         const size_t per_electron = 6 * (fp32 ? 4 : 8);

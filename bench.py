@@ -891,8 +891,8 @@ def bench_swarm(args, rank, dist):
     steps_done = np.array([r.steps_done for r in results])
     return {
         "value": value, "ms_per_step": 1e3 * t_sat / max(1, (g1 - g0) * spl), "dtype": "f32" if prec == apic.FP32 else "f64",
-        "config": {"workload": WORKLOAD_SWARM, "form": ("FP32 electron velocity + displacement, FP64 collision "
-                                                        "arithmetic and tallies") if prec == apic.FP32 else
+        "config": {"workload": WORKLOAD_SWARM, "form": ("FP32 electron velocity + displacement and FP32 collision "
+                                                        "loops; FP64 tallies") if prec == apic.FP32 else
                    "FP64 electrons", "saturation_requests": len(batch), "steps_per_launch": spl,
                    "autotuned": tuned["table"] if tuned else None,
                    "l2": "electron state of the batch larger than L2"},

@@ -59,21 +59,29 @@ def test_fp64_form_matches_oracle(name):
 
 
 @pytest.mark.parametrize("name", ["swarm_fixed", "swarm_branching"])
-def test_fp32_form_matches_oracle_fp32_storage(name):
-    """FP32 electron storage against oracle mode 2 (the same values rounded to
-    FP32 at the same points): collision counts within 0.1 %, ensemble means
-    within 1e-6 relative."""
+def test_fp32_form_statistically_matches_fp64_form(name):
+    """The FP32 form (float electron state, FP32 collision loops on their own
+    uniforms) against the FP64 form over 12 seeds per field: ensemble means of
+    drift velocity, mean energy and the ionization rate coefficient within 3
+    combined standard errors, candidates within 3 standard errors."""
     spec = swarm_cases()[name]
-    dev = _device(spec, apic.FP32)
-    T = po.TableSet()
-    cfg, gas = po.swarm_from_spec(spec, T)
-    for k, td in enumerate(spec.fields_td):
-        ora, _ = po.swarm_run_field(cfg, gas, td, spec.seed + k, 2)
-        d = dev[k]
-        assert d.status == 0, d.message
-        assert abs(int(d.candidates) - int(ora.candidates)) <= 1e-3 * ora.candidates
-        for key in ("mean_velocity_x", "mean_energy_ev"):
-            assert rel(getattr(d, key), getattr(ora, key)) < 1e-6, (name, td, key)
+    res = {}
+    for prec in (apic.FP64, apic.FP32):
+        cfg, gas, tabs = W.to_device_swarm(spec, prec)
+        runs = []
+        for k in range(12):
+            cfg.seed = spec.seed + 1000 * k
+            runs.append(apic.swarm_run(cfg, gas, spec.fields_td))
+        res[prec] = runs
+    for j, td in enumerate(spec.fields_td):
+        for key in ("drift_velocity", "mean_energy_ev", "ionization_rate", "candidates"):
+            a = np.array([float(getattr(r[j], key)) for r in res[apic.FP64]])
+            b = np.array([float(getattr(r[j], key)) for r in res[apic.FP32]])
+            assert all(r[j].status == 0 for r in res[apic.FP32])
+            if np.all(a == 0) and np.all(b == 0):
+                continue
+            se = np.hypot(a.std(ddof=1), b.std(ddof=1)) / np.sqrt(len(a))
+            assert abs(a.mean() - b.mean()) <= 3 * max(se, 1e-12 * abs(a.mean())), (name, td, key, a.mean(), b.mean(), se)
 
 
 @pytest.mark.parametrize("name", ["ens_fixed", "ens_branching"])
