@@ -487,6 +487,7 @@ class ConfigND(C.Structure):
         ("profile_axis", C.c_int), ("profile_rows", C.c_size_t),
         ("profile_coordinates", C.POINTER(C.c_double)), ("profile_values", C.POINTER(C.c_double)),
         ("wall_axis", C.c_int * 2), ("wall_potential", C.c_double * 4), ("particle_boundary", C.c_int * 4),
+        ("wall_axis_z", C.c_int), ("particle_boundary_z", C.c_int * 2),
     ]
 
 
@@ -564,14 +565,19 @@ def config_nd(*, dims, n, length, dt, species, magnetic_field=(0.0, 0.0, 0.0), u
         c.profile_coordinates = pc.ctypes.data_as(C.POINTER(C.c_double))
         c.profile_values = pv.ctypes.data_as(C.POINTER(C.c_double))
     if walls is not None:
-        # (wall axes [x, y], potentials [left, right, bottom, top], particle boundaries
-        #  [left, right, bottom, top]: 0 auto, 1 absorbing, 2 reflecting, 3 periodic)
+        # (wall axes [x, y(, z)], potentials [left, right, bottom, top] (3D: None,
+        #  grounded), particle boundaries [left, right, bottom, top(, back, front)]:
+        #  0 auto, 1 absorbing, 2 reflecting, 3 periodic)
         axes, pots, pbs = walls
         for a in range(2):
             c.wall_axis[a] = int(axes[a])
+        if len(axes) > 2:
+            c.wall_axis_z = int(axes[2])
         for k in range(4):
-            c.wall_potential[k] = float(pots[k])
+            c.wall_potential[k] = float(pots[k]) if pots is not None else 0.0
             c.particle_boundary[k] = int(pbs[k])
+        for k in range(4, len(pbs)):
+            c.particle_boundary_z[k - 4] = int(pbs[k])
     return c
 
 
@@ -641,7 +647,9 @@ class SimulationND:
         return out
 
     def boundary_losses(self, species):
-        out = np.zeros(4, np.uint64)
+        """absorbed counts of one species per side: left, right, bottom, top
+        (, back, front in 3D)"""
+        out = np.zeros(2 * self.dims, np.uint64)
         L = lib()
         L.apic_simnd_boundary_losses.argtypes = [C.c_void_p, C.c_int, _U64P]
         _check_nd(L.apic_simnd_boundary_losses(self.h, species, out.ctypes.data_as(_U64P)), self.h)

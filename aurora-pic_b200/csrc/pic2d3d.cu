@@ -58,7 +58,7 @@ struct SpeciesND {
     float tb[3], sb[3];  // Boris t = hqmdt B and s = 2 t / (1 + t^2)
     float drift[3];    // dt / d_a: cell units per unit velocity
     float dep_fixed;   // dep * rho_scale
-    uint8_t* alive;    // 2D walls with an absorbing side: Particle::alive (null: all alive)
+    uint8_t* alive;    // runs with walls and an absorbing side: Particle::alive (null: all alive)
     int index;         // species index (loss ledger row)
 };
 
@@ -76,10 +76,11 @@ struct ParamsND {
     int prof_axis, prof_rows;
     const double* prof_c;  // coordinates
     const double* prof_v;  // rows x 3
-    // 2D walls: Dirichlet axes, particle boundaries (left, right, bottom, top:
-    // 0 periodic, 1 absorbing, 2 reflecting) and the absorbed counts [species][4]
-    int wall[2];
-    int pbc[4];
+    // walls: Dirichlet axes, particle boundaries (left, right, bottom, top,
+    // back, front: 0 periodic, 1 absorbing, 2 reflecting) and the absorbed
+    // counts [species][6]
+    int wall[3];
+    int pbc[6];
     unsigned long long* losses;
 };
 
@@ -174,8 +175,9 @@ __device__ __forceinline__ Axis axis2(const ParamsND& p, int a, double x) {
     return (WALLS && p.wall[a]) ? axis_wall(x, p.L[a], p.d[a], p.n[a]) : axis(x, p.L[a], p.d[a], p.n[a]);
 }
 
-// 1 / node_area relative to an interior node: 2 on each wall-axis wall node
-// (Mesh2D::node_area halves the cell there, src/Mesh2D.cpp:77-88)
+// 1 / node_area (node_volume) relative to an interior node: 2 on each
+// wall-axis wall node (Mesh2D::node_area and Mesh3D::node_volume halve the
+// cell there, src/Mesh2D.cpp:77-88, src/Mesh3D.cpp:52-60)
 template <bool WALLS>
 __device__ __forceinline__ double area_factor(const ParamsND& p, int a, int i) {
     return (WALLS && p.wall[a] && (i == 0 || i == p.n[a] - 1)) ? 2.0 : 1.0;
@@ -183,8 +185,8 @@ __device__ __forceinline__ double area_factor(const ParamsND& p, int a, int i) {
 
 template <int DIM, bool WALLS = false>
 __device__ __forceinline__ void gather(const ParamsND& p, const double pos[3], double e[3]) {
-    const Axis ax = DIM == 2 ? axis2<WALLS>(p, 0, pos[0]) : axis(pos[0], p.L[0], p.d[0], p.n[0]);
-    const Axis ay = DIM == 2 ? axis2<WALLS>(p, 1, pos[1]) : axis(pos[1], p.L[1], p.d[1], p.n[1]);
+    const Axis ax = axis2<WALLS>(p, 0, pos[0]);
+    const Axis ay = axis2<WALLS>(p, 1, pos[1]);
     const int nx = p.n[0];
     if (DIM == 2) {
         const double fx = ax.f, fy = ay.f;
@@ -197,7 +199,8 @@ __device__ __forceinline__ void gather(const ParamsND& p, const double pos[3], d
         e[1] = e00.y * w00 + e10.y * w10 + e01.y * w01 + e11.y * w11;
         e[2] = 0.0;
     } else {
-        const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+        // interpolate_electric(Mesh3D&), src/FieldSolver.cpp:978-1038: loops z, y, x
+        const Axis az = axis2<WALLS>(p, 2, pos[2]);
         const double wx[2] = {1.0 - ax.f, ax.f}, wy[2] = {1.0 - ay.f, ay.f}, wz[2] = {1.0 - az.f, az.f};
         const int ii[2] = {ax.i0, ax.i1}, jj[2] = {ay.i0, ay.i1}, kk[2] = {az.i0, az.i1};
         const double4* E4 = reinterpret_cast<const double4*>(p.E);
@@ -282,8 +285,8 @@ __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND&
     size_t node[K];
     unsigned cell = 0xFFFFFFFFu;
     if (valid) {
-        const Axis ax = DIM == 2 ? axis2<WALLS>(p, 0, pos[0]) : axis(pos[0], p.L[0], p.d[0], p.n[0]);
-        const Axis ay = DIM == 2 ? axis2<WALLS>(p, 1, pos[1]) : axis(pos[1], p.L[1], p.d[1], p.n[1]);
+        const Axis ax = axis2<WALLS>(p, 0, pos[0]);
+        const Axis ay = axis2<WALLS>(p, 1, pos[1]);
         const int nx = p.n[0];
         if (DIM == 2 && WALLS) {
             // q shape / node_area over the wall nodes' half cells, src/Mesh2D.cpp:131-142
@@ -311,7 +314,7 @@ __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND&
             node[3] = (size_t)ay.i1 * nx + ax.i1;
             cell = (unsigned)node[0];
         } else {
-            const Axis az = axis(pos[2], p.L[2], p.d[2], p.n[2]);
+            const Axis az = axis2<WALLS>(p, 2, pos[2]);
             const double wx[2] = {1.0 - ax.f, ax.f}, wy[2] = {1.0 - ay.f, ay.f}, wz[2] = {1.0 - az.f, az.f};
             const int ii[2] = {ax.i0, ax.i1}, jj[2] = {ay.i0, ay.i1}, kk[2] = {az.i0, az.i1};
 #pragma unroll
@@ -321,7 +324,14 @@ __device__ __forceinline__ void deposit_warp(const ParamsND& p, const SpeciesND&
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int k = (c * 2 + b) * 2 + q;
-                        a[k] = to_fixed(S.dep * (wx[q] * wy[b] * wz[c]), p.rho_scale);
+                        if (WALLS) {
+                            // q shape / node_volume over the wall nodes' half cells, src/Mesh3D.cpp:110-122
+                            const double f = area_factor<WALLS>(p, 0, ii[q]) * area_factor<WALLS>(p, 1, jj[b]) *
+                                             area_factor<WALLS>(p, 2, kk[c]);
+                            a[k] = to_fixed(S.dep * (wx[q] * wy[b] * wz[c]) * f, p.rho_scale);
+                        } else {
+                            a[k] = to_fixed(S.dep * (wx[q] * wy[b] * wz[c]), p.rho_scale);
+                        }
                         node[k] = ((size_t)kk[c] * p.n[1] + jj[b]) * nx + ii[q];
                     }
             cell = (unsigned)node[0];
@@ -361,18 +371,21 @@ __device__ __forceinline__ void reflect_coordinate(double& c, double& v, double 
     }
 }
 
-// Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335, with
-// apply_lower/upper_boundary (:57-97): returns the absorbing side, or -1.
-__device__ __forceinline__ int apply_walls(const ParamsND& p, double& x, double& y, double& vx, double& vy) {
+// Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335, and
+// Simulation3D::apply_particle_boundaries, src/Simulation3D.cpp:309-340, with
+// apply_lower/upper_boundary (src/Simulation2D.cpp:57-97, src/Simulation3D.cpp:42-83):
+// sides left, right, bottom, top (, back, front); returns the absorbing side, or -1.
+template <int DIM>
+__device__ __forceinline__ int apply_walls(const ParamsND& p, double x[3], double v[3]) {
 #pragma unroll
-    for (int side = 0; side < 4; ++side) {
-        double& c = side < 2 ? x : y;
-        double& v = side < 2 ? vx : vy;
-        const double L = p.L[side >> 1];
+    for (int side = 0; side < 2 * DIM; ++side) {
+        const int a = side >> 1;
+        double& c = x[a];
+        const double L = p.L[a];
         if ((side & 1) == 0 ? c >= 0.0 : c <= L) continue;
         const int kind = p.pbc[side];
         if (kind == 1) return side;
-        if (kind == 2) reflect_coordinate(c, v, L);
+        if (kind == 2) reflect_coordinate(c, v[a], L);
         else c = wrap_periodic(c, L);
     }
     return -1;
@@ -431,14 +444,12 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     }
     bool absorbed = false;
     if (WALLS) {
-        double x = pos[0] + vh[0] * p.dt, y = pos[1] + vh[1] * p.dt;
-        const int side = valid ? apply_walls(p, x, y, vh[0], vh[1]) : -1;
-        pos[0] = x;
-        pos[1] = y;
+        for (int a = 0; a < DIM; ++a) pos[a] = pos[a] + vh[a] * p.dt;
+        const int side = valid ? apply_walls<DIM>(p, pos, vh) : -1;
         if (side >= 0) {
             absorbed = true;
             S.alive[i] = 0;
-            atomicAdd(p.losses + 4 * S.index + side, 1ull);
+            atomicAdd(p.losses + 6 * S.index + side, 1ull);
         }
     } else {
         for (int a = 0; a < DIM; ++a) {
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_push(ParamsND p, SpeciesND S, int 
     deposit_warp<DIM, WALLS>(p, S, pos, valid && !absorbed);
 }
 
-// 2D walls: fixed-point density to FP64 (the accumulator is cleared for the
+// walls: fixed-point density to FP64 (the accumulator is cleared for the
 // next deposit)
 __global__ void k_walls_rho(unsigned long long* __restrict__ acc, double* __restrict__ rho, size_t N,
                             double inv_scale) {
@@ -462,6 +473,12 @@ __global__ void k_walls_rho(unsigned long long* __restrict__ acc, double* __rest
         rho[i] = (double)(long long)acc[i] * inv_scale;
         acc[i] = 0ull;
     }
+}
+
+// 3D walls: the field planes (Ex | Ey | Ez) into the interleaved layout of the push
+__global__ void k_walls_interleave3(const double* __restrict__ planes, double4* __restrict__ E, size_t N) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N; i += (size_t)gridDim.x * blockDim.x)
+        E[i] = make_double4(planes[i], planes[N + i], planes[2 * N + i], 0.0);
 }
 
 // 2D walls: the field planes (Ex | Ey) into the interleaved layout of the push
@@ -1476,7 +1493,8 @@ constexpr int kSampleBlocks = 148;
 __global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double* partial, unsigned* done,
                                                    double* out, const double* E, const double* rho,
                                                    long long N, double half_eps_vol, double vol, int species,
-                                                   int last_species, int wall_x, int wall_y, int nx, int ny) {
+                                                   int last_species, int wall_x, int wall_y, int wall_z, int nx,
+                                                   int ny, int nz) {
     __shared__ double red[8], red2[8], red3[8];
     __shared__ bool last;
     const int tid = threadIdx.x;
@@ -1494,10 +1512,12 @@ __global__ void __launch_bounds__(256) k_sample_nd(SpeciesND S, int dims, double
                 const double4 e = reinterpret_cast<const double4*>(E)[g];
                 e2 = e.x * e.x + e.y * e.y + e.z * e.z;
             }
-            // Mesh2D::node_area: half cells on the wall nodes, src/Mesh2D.cpp:77-88
-            const int gi = (int)(g % nx), gj = (int)(g / nx);
+            // Mesh2D::node_area / Mesh3D::node_volume: half cells on the wall
+            // nodes, src/Mesh2D.cpp:77-88, src/Mesh3D.cpp:52-60
+            const int gi = (int)(g % nx), gj = (int)((g / nx) % ny), gk = (int)(g / ((long long)nx * ny));
             const double f = ((wall_x && (gi == 0 || gi == nx - 1)) ? 0.5 : 1.0) *
-                             ((wall_y && (gj == 0 || gj == ny - 1)) ? 0.5 : 1.0);
+                             ((wall_y && (gj == 0 || gj == ny - 1)) ? 0.5 : 1.0) *
+                             ((wall_z && (gk == 0 || gk == nz - 1)) ? 0.5 : 1.0);
             fe += half_eps_vol * e2 * f;
             l1 += fabs(rho[g]) * vol * f;
         }
@@ -1679,6 +1699,8 @@ __global__ void k_dir_divide(double* __restrict__ u, int Mx, int My, int Mz, dou
                              double scale);
 __global__ void k_dir_assemble(const double* __restrict__ u, double* __restrict__ phi, int nx, int ny, int nz3,
                                double left, double right, double bottom, double top);
+__global__ void k_dir_efield3(const double* __restrict__ phi, double* __restrict__ E, int nx, int ny, int nz, double dx,
+                              double dy, double dz);
 
 namespace {
 std::mutex g_attr_mu;
@@ -1758,18 +1780,28 @@ struct SimND {
         require(c.dims == 2 || c.dims == 3, "dims must be 2 or 3");
         require(c.precision == APIC_FP64 || c.precision == APIC_FP32, "unknown precision");
         fp32 = c.precision == APIC_FP32;
-        walls = c.wall_axis[0] != 0 || c.wall_axis[1] != 0;
+        walls = c.wall_axis[0] != 0 || c.wall_axis[1] != 0 || (c.dims == 3 && c.wall_axis_z != 0);
         if (walls) {
-            require(c.dims == 2, "walls are supported on 2D meshes", APIC_ERR_UNSUPPORTED);
-            require(!fp32, "2D runs with walls use the FP64 particle form", APIC_ERR_UNSUPPORTED);
+            require(!fp32, "runs with walls use the FP64 particle form", APIC_ERR_UNSUPPORTED);
             for (int k = 0; k < 4; ++k) {
                 require(c.particle_boundary[k] >= 0 && c.particle_boundary[k] <= 3, "unknown particle boundary");
                 require(std::isfinite(c.wall_potential[k]), "wall potentials must be finite");
             }
+            if (c.dims == 3) {
+                // Simulation3DConfig has one field boundary for the mesh (src/Mesh3D.cpp:37-48)
+                require(c.wall_axis[0] && c.wall_axis[1] && c.wall_axis_z,
+                        "3D meshes are periodic or Dirichlet on every axis", APIC_ERR_UNSUPPORTED);
+                require(c.wall_potential[0] == 0.0 && c.wall_potential[1] == 0.0 && c.wall_potential[2] == 0.0 &&
+                            c.wall_potential[3] == 0.0,
+                        "3D Dirichlet walls are grounded");
+                for (int k = 0; k < 2; ++k)
+                    require(c.particle_boundary_z[k] >= 0 && c.particle_boundary_z[k] <= 3,
+                            "unknown particle boundary");
+            }
         }
         for (int a = 0; a < c.dims; ++a) {
             require(c.n[a] >= 3, "mesh extents must be at least 3");
-            const bool wall = walls && c.wall_axis[a];
+            const bool wall = walls && (a < 2 ? c.wall_axis[a] != 0 : c.wall_axis_z != 0);
             if (!wall)
                 require(pow2(c.n[a]) && c.n[a] <= (size_t)kMaxLine,
                         "periodic device meshes need power-of-two extents up to 1024", APIC_ERR_UNSUPPORTED);
@@ -1803,8 +1835,10 @@ struct SimND {
         for (int a = 0; a < 3; ++a) {
             p.n[a] = a < c.dims ? (int)c.n[a] : 1;
             p.L[a] = a < c.dims ? c.length[a] : 1.0;
-            // Mesh2D/Mesh3D dx: L / n periodic, L / (n - 1) on a wall axis, src/Mesh2D.cpp:57-62
-            p.d[a] = p.L[a] / (double)(walls && a < 2 && c.wall_axis[a] ? p.n[a] - 1 : p.n[a]);
+            // Mesh2D/Mesh3D dx: L / n periodic, L / (n - 1) on a wall axis,
+            // src/Mesh2D.cpp:57-62, src/Mesh3D.cpp:43-45
+            const bool wall_a = walls && a < c.dims && (a < 2 ? c.wall_axis[a] != 0 : c.wall_axis_z != 0);
+            p.d[a] = p.L[a] / (double)(wall_a ? p.n[a] - 1 : p.n[a]);
             p.B[a] = c.magnetic_field[a];
             N *= (size_t)p.n[a];
             if (a < c.dims) cellvol *= p.d[a];
@@ -1839,7 +1873,8 @@ struct SimND {
             require(std::isfinite(S.mass) && S.mass > 0, "species mass must be positive and finite");
             require(S.capacity > 0 && S.capacity < (1ull << 31), "species capacity out of range");
             const double w = c.dims == 2 ? S.weight / depth : S.weight;  // Species2D::deposit_charge
-            bound += (double)S.capacity * std::fabs(S.charge * w) / cellvol * (walls ? 4.0 : 1.0);
+            // a wall node's half cells (a corner's eighth) raise its density by up to 2^dims
+            bound += (double)S.capacity * std::fabs(S.charge * w) / cellvol * (walls ? (double)(1 << c.dims) : 1.0);
         }
         const int bits = bound > 0 ? (int)std::floor(61.0 - std::log2(bound)) : 0;
         p.rho_scale = std::ldexp(1.0, bits);
@@ -1972,6 +2007,9 @@ struct SimND {
         if (cfg.dims == 2 && walls) {
             if (boris) k_push<2, true, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
             else k_push<2, false, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
+        } else if (walls) {
+            if (boris) k_push<3, true, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
+            else k_push<3, false, MODE, true><<<blocks, kThreads, 0, stream>>>(p, S, b);
         } else if (cfg.dims == 2) {
             if (boris) k_push<2, true, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
             else k_push<2, false, MODE><<<blocks, kThreads, 0, stream>>>(p, S, b);
@@ -2065,43 +2103,47 @@ struct SimND {
         initialized = false;
     }
 
-    // ---- 2D walls: persistent solve scratch on the run's stream ----
+    // ---- walls: persistent solve scratch on the run's stream ----
     bool walls = false;
     int wall_mode = 0;  // 1: one wall axis (mixed solve), 2: walls on every side
     int periodic_axis = 0;
-    double* w_planes = nullptr;  // Ex | Ey
+    double* w_planes = nullptr;  // Ex | Ey (| Ez)
     double* w_mu = nullptr;
     Cplx* w_hat = nullptr;
     Cplx* w_tw = nullptr;
     double* w_u = nullptr;
-    Cplx* w_dtw[2] = {nullptr, nullptr};
+    Cplx* w_dtw[3] = {nullptr, nullptr, nullptr};
 
     void setup_walls(const apic_config_nd& c) {
-        const size_t N = c.n[0] * c.n[1];
-        for (int k = 0; k < 4; ++k) {
-            const int kind = c.particle_boundary[k];
-            const bool wall = c.wall_axis[k >> 1] != 0;
-            // resolve_particle_boundary, src/Simulation2D.cpp:38-41 (Auto follows the field boundary)
+        const int dims = c.dims;
+        const size_t N = c.n[0] * c.n[1] * (dims == 3 ? c.n[2] : 1);
+        for (int k = 0; k < 2 * dims; ++k) {
+            const int kind = k < 4 ? c.particle_boundary[k] : c.particle_boundary_z[k - 4];
+            const bool wall = k < 4 ? c.wall_axis[k >> 1] != 0 : c.wall_axis_z != 0;
+            // resolve_particle_boundary, src/Simulation2D.cpp:38-41, src/Simulation3D.cpp:25-28
+            // (Auto follows the field boundary)
             p.pbc[k] = kind == 0 ? (wall ? 1 : 0) : (kind == 1 ? 1 : (kind == 2 ? 2 : 0));
         }
         p.wall[0] = c.wall_axis[0] != 0;
         p.wall[1] = c.wall_axis[1] != 0;
-        p.losses = dalloc<unsigned long long>(4 * APIC_MAX_SPECIES);
-        const bool absorbing = p.pbc[0] == 1 || p.pbc[1] == 1 || p.pbc[2] == 1 || p.pbc[3] == 1;
+        p.wall[2] = dims == 3 && c.wall_axis_z != 0;
+        p.losses = dalloc<unsigned long long>(6 * APIC_MAX_SPECIES);
+        bool absorbing = false;
+        for (int k = 0; k < 2 * dims; ++k) absorbing = absorbing || p.pbc[k] == 1;
         for (int s = 0; s < c.nspecies; ++s)
             sp[s].alive = absorbing ? dalloc<uint8_t>(c.species[s].capacity) : nullptr;
-        solver.F.dims = 2;
+        solver.F.dims = dims;
         solver.F.rho_acc = dalloc<unsigned long long>(N);
         solver.F.rho = dalloc<double>(N);
         solver.F.phi = dalloc<double>(N);
-        solver.F.E = dalloc<double>(2 * N);
-        w_planes = dalloc<double>(2 * N);
+        solver.F.E = dalloc<double>((dims == 3 ? 4 : 2) * N);
+        w_planes = dalloc<double>((size_t)dims * N);
         const double twopi = 2.0 * 3.141592653589793;
         if (p.wall[0] && p.wall[1]) {
             wall_mode = 2;
-            const int M[2] = {(int)c.n[0] - 2, (int)c.n[1] - 2};
-            w_u = dalloc<double>((size_t)M[0] * M[1]);
-            for (int a = 0; a < 2; ++a) {
+            const int M[3] = {(int)c.n[0] - 2, (int)c.n[1] - 2, dims == 3 ? (int)c.n[2] - 2 : 1};
+            w_u = dalloc<double>((size_t)M[0] * M[1] * M[2]);
+            for (int a = 0; a < dims; ++a) {
                 const int L2 = 2 * (M[a] + 1);
                 std::vector<Cplx> tw(L2);
                 for (int k = 0; k < L2; ++k) tw[k] = {std::cos(twopi * k / L2), -std::sin(twopi * k / L2)};
@@ -2124,10 +2166,48 @@ struct SimND {
         APIC_CUDA(cudaStreamSynchronize(stream));
     }
 
+    // FieldSolver::solve(Mesh3D&) on a Dirichlet mesh, src/FieldSolver.cpp:399-405:
+    // the direct sine-transform solve (grounded walls) of the system the
+    // reference's SOR iterates on; E by differences, one-sided at the walls.
+    void solve_walls3() {
+        const int nx = p.n[0], ny = p.n[1], nz = p.n[2];
+        const size_t N = (size_t)nx * ny * nz;
+        const unsigned g = (unsigned)std::min<size_t>((N + 255) / 256, 4096);
+        k_walls_rho<<<g, 256, 0, stream>>>(solver.F.rho_acc, solver.F.rho, N, p.inv_rho_scale);
+        const int M[3] = {nx - 2, ny - 2, nz - 2};
+        const double idx2 = 1.0 / (p.d[0] * p.d[0]), idy2 = 1.0 / (p.d[1] * p.d[1]), idz2 = 1.0 / (p.d[2] * p.d[2]);
+        k_dir_rhs<<<g, 256, 0, stream>>>(solver.F.rho, w_u, nx, ny, nz, p.eps, idx2, idy2, 0.0, 0.0, 0.0, 0.0);
+        auto dst_axis = [&](int a) {
+            const long long sx = 1, sy = M[0], sz = (long long)M[0] * M[1];
+            long long stride, stride_a, stride_b;
+            int lines_a;
+            size_t lines;
+            if (a == 0) { stride = sx; lines_a = M[1]; stride_a = sy; stride_b = sz; lines = (size_t)M[1] * M[2]; }
+            else if (a == 1) { stride = sy; lines_a = M[0]; stride_a = sx; stride_b = sz; lines = (size_t)M[0] * M[2]; }
+            else { stride = sz; lines_a = M[0]; stride_a = sx; stride_b = sy; lines = (size_t)M[0] * M[1]; }
+            const size_t smem = 3 * (size_t)(2 * (M[a] + 1)) * sizeof(Cplx);
+            k_dst_lines<<<(unsigned)lines, kFftThreads, smem, stream>>>(w_u, M[a], stride, lines_a, stride_a, stride_b,
+                                                                         w_dtw[a]);
+        };
+        for (int a = 0; a < 3; ++a) dst_axis(a);
+        double scale = 1.0;
+        for (int a = 0; a < 3; ++a) scale *= 2.0 / (double)(M[a] + 1);
+        k_dir_divide<<<g, 256, 0, stream>>>(w_u, M[0], M[1], M[2], idx2, idy2, idz2, scale);
+        for (int a = 0; a < 3; ++a) dst_axis(a);
+        k_dir_assemble<<<g, 256, 0, stream>>>(w_u, solver.F.phi, nx, ny, nz, 0.0, 0.0, 0.0, 0.0);
+        k_dir_efield3<<<g, 256, 0, stream>>>(solver.F.phi, w_planes, nx, ny, nz, p.d[0], p.d[1], p.d[2]);
+        k_walls_interleave3<<<g, 256, 0, stream>>>(w_planes, reinterpret_cast<double4*>(solver.F.E), N);
+        APIC_CUDA(cudaGetLastError());
+    }
+
     // FieldSolver::solve(Mesh2D&) with walls, src/FieldSolver.cpp:389-397: the
     // mixed spectral-tridiagonal solve, or the direct sine-transform solve of
     // the system the reference's SOR iterates on; E by differences.
     void solve_walls() {
+        if (cfg.dims == 3) {
+            solve_walls3();
+            return;
+        }
         const int nx = p.n[0], ny = p.n[1];
         const size_t N = (size_t)nx * ny;
         const unsigned g = (unsigned)std::min<size_t>((N + 255) / 256, 4096);
@@ -2347,13 +2427,14 @@ struct SimND {
         APIC_CUDA(cudaStreamSynchronize(stream));
     }
 
+    // absorbed counts of species s per side: 4 in 2D, 6 in 3D
     void read_losses(int s, uint64_t* out) {
         require(s >= 0 && s < cfg.nspecies, "species index out of range");
         sync();
-        unsigned long long h[4] = {0, 0, 0, 0};
-        if (p.losses) APIC_CUDA(cudaMemcpyAsync(h, p.losses + 4 * s, sizeof h, cudaMemcpyDeviceToHost, stream));
+        unsigned long long h[6] = {0, 0, 0, 0, 0, 0};
+        if (p.losses) APIC_CUDA(cudaMemcpyAsync(h, p.losses + 6 * s, sizeof h, cudaMemcpyDeviceToHost, stream));
         APIC_CUDA(cudaStreamSynchronize(stream));
-        for (int k = 0; k < 4; ++k) out[k] = h[k];
+        for (int k = 0; k < 2 * cfg.dims; ++k) out[k] = h[k];
     }
 
     void read_fields(double* rho, double* phi, double* E) {
@@ -2382,16 +2463,21 @@ struct SimND {
             k_sample_nd<<<kSampleBlocks, 256, 0, stream>>>(sp[s], cfg.dims, sample_partial, sample_done, sample_out,
                                                            solver.F.E, solver.F.rho, (long long)ncells,
                                                            0.5 * p.eps * vol, vol, s, s == cfg.nspecies - 1,
-                                                           p.wall[0], p.wall[1], p.n[0], p.n[1]);
+                                                           p.wall[0], p.wall[1], p.wall[2], p.n[0], p.n[1], p.n[2]);
             APIC_CUDA(cudaGetLastError());
         }
         double h[8];
+        unsigned long long lost[6 * APIC_MAX_SPECIES] = {};
         APIC_CUDA(cudaMemcpyAsync(h, sample_out, sizeof h, cudaMemcpyDeviceToHost, stream));
+        if (p.losses) APIC_CUDA(cudaMemcpyAsync(lost, p.losses, sizeof lost, cudaMemcpyDeviceToHost, stream));
         sync();
         for (int s = 0; s < cfg.nspecies; ++s) {
             out->kinetic_by_species[s] = h[s];
             out->kinetic_energy += h[s];
-            out->live_particles += sp[s].n;
+            // live_count: absorbed particles stay in place, flagged dead, each counted once in the ledger
+            uint64_t dead = 0;
+            for (int k = 0; k < 6; ++k) dead += lost[6 * s + k];
+            out->live_particles += sp[s].n - dead;
         }
         out->field_energy = h[4];
         out->charge_l1 = h[5];

@@ -394,6 +394,13 @@ typedef struct {
     int wall_axis[2];
     double wall_potential[4];
     int particle_boundary[4];
+    /* 3D walls (Simulation3DConfig boundary = Dirichlet, particle_boundary_config,
+       include/pic/Simulation3D.hpp:30-66): the 3D mesh is periodic or Dirichlet on every axis, so
+       wall_axis_z = 1 needs wall_axis[0] = wall_axis[1] = 1 and zero wall_potential (grounded walls);
+       extents 2^k + 1 nodes up to 513, solved directly by sine transforms.  particle_boundary then
+       holds left, right, bottom, top and particle_boundary_z back, front (same codes).  FP64 form. */
+    int wall_axis_z;
+    int particle_boundary_z[2];
 } apic_config_nd;
 
 /* DiagnosticSample2D / DiagnosticSample3D, src/Diagnostics.cpp:111-137, :205-232 */
@@ -445,11 +452,13 @@ APIC_EXPORT int apic_simnd_read_particles(apic_sim_nd* sim, int species, size_t 
                                           double* v, double* v_half, size_t* n);
 /* Mesh2D/Mesh3D rho(), phi(), electric_{x,y,z}() (E is [dims][N]). */
 APIC_EXPORT int apic_simnd_read_fields(apic_sim_nd* sim, double* rho, double* phi, double* electric);
-/* Particle::alive of a 2D run with walls (1 for every particle without absorbing sides), in the
+/* Particle::alive of a run with walls (1 for every particle without absorbing sides), in the
  * order of apic_simnd_read_particles. */
 APIC_EXPORT int apic_simnd_read_alive(apic_sim_nd* sim, int species, size_t capacity, uint8_t* alive);
 /* species_boundary_losses()[species] (BoundaryLoss2D, include/pic/Diagnostics.hpp:27-32):
- * absorbed left, right, bottom, top. */
+ * absorbed left, right, bottom, top; 3D runs write six counts (BoundaryLoss3D,
+ * include/pic/Diagnostics.hpp:34-41: ... back, front), per species here, their sum over the
+ * species being the reference's boundary_losses() of the run. */
 APIC_EXPORT int apic_simnd_boundary_losses(apic_sim_nd* sim, int species, uint64_t* absorbed);
 APIC_EXPORT int apic_simnd_sample(apic_sim_nd* sim, apic_sample_nd* out);
 APIC_EXPORT int apic_simnd_cuda_stream(apic_sim_nd* sim, void** stream);

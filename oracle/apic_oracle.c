@@ -1566,12 +1566,12 @@ struct ora_simnd {
     double *pos[ORA_MAX_SPECIES], *v[ORA_MAX_SPECIES], *vh[ORA_MAX_SPECIES]; /* [3][np] each */
     double *rho, *phi, *E;
     double time;
-    /* 2D walls: Dirichlet field axes, side potentials and particle boundaries
-     * (left, right, bottom, top: 0 periodic, 1 absorbing, 2 reflecting) */
-    int walls, dir[2], pbc[4];
+    /* walls: Dirichlet field axes, side potentials (2D) and particle boundaries
+     * (left, right, bottom, top, back, front: 0 periodic, 1 absorbing, 2 reflecting) */
+    int walls, dir[3], pbc[6];
     double pot[4];
     uint8_t* alive[ORA_MAX_SPECIES];
-    uint64_t losses[ORA_MAX_SPECIES][4];
+    uint64_t losses[ORA_MAX_SPECIES][6];
 };
 
 ora_simnd* ora_simnd_create(int dims, const size_t* n, const double* L, double dt, double eps, const double* B,
@@ -1632,9 +1632,25 @@ int ora_simnd_set_walls(ora_simnd* s, const int* dirichlet, const double* potent
     return 0;
 }
 
+/* Mesh3D with Boundary::Dirichlet (grounded walls on every side, spacing
+ * L / (n - 1), src/Mesh3D.cpp:37-60) and the 3D particle boundaries per side
+ * (left, right, bottom, top, back, front; src/Simulation3D.cpp:25-97, :309-340). */
+int ora_simnd_set_walls3d(ora_simnd* s, const int* particle) {
+    if (s->dims != 3) return seterr(1, "3D walls need a 3D run");
+    s->walls = 1;
+    for (int a = 0; a < 3; ++a) {
+        s->dir[a] = 1;
+        s->d[a] = s->L[a] / (double)(s->n[a] - 1);
+    }
+    for (int k = 0; k < 4; ++k) s->pot[k] = 0.0;
+    for (int k = 0; k < 6; ++k) s->pbc[k] = particle[k];
+    return 0;
+}
+
+/* alive flags and the absorbed counts per side (2D: 4 sides, 3D: 6) of species k */
 void ora_simnd_alive_losses(const ora_simnd* s, int k, uint8_t* alive, uint64_t* losses) {
     if (alive) for (size_t i = 0; i < s->np[k]; ++i) alive[i] = s->alive[k] ? s->alive[k][i] : 1;
-    if (losses) for (int q = 0; q < 4; ++q) losses[q] = s->losses[k][q];
+    if (losses) for (int q = 0; q < 2 * s->dims; ++q) losses[q] = s->losses[k][q];
 }
 
 /* One axis of the 2D CIC stencil with a wall or a wrap, src/Mesh2D.cpp:96-129,
@@ -1663,9 +1679,46 @@ static double wall_node_area(const ora_simnd* s, size_t i, size_t j) {
     return wx * wy;
 }
 
+/* Mesh3D::node_volume of a Dirichlet mesh, src/Mesh3D.cpp:52-60 */
+static double wall_node_volume(const ora_simnd* s, size_t i, size_t j, size_t k) {
+    const double wx = (i == 0 || i + 1 == s->n[0]) ? 0.5 * s->d[0] : s->d[0];
+    const double wy = (j == 0 || j + 1 == s->n[1]) ? 0.5 * s->d[1] : s->d[1];
+    const double wz = (k == 0 || k + 1 == s->n[2]) ? 0.5 * s->d[2] : s->d[2];
+    return wx * wy * wz;
+}
+
 static void simnd_deposit_solve(ora_simnd* s) {
     const size_t N = s->n[0] * s->n[1] * s->n[2];
     memset(s->rho, 0, N * sizeof(double));
+    if (s->walls && s->dims == 3) {
+        /* deposit_charge_cic(Mesh3D&) on a Dirichlet mesh, src/Mesh3D.cpp:62-126:
+         * clamped stencil, q shape / node_volume, loops z, y, x */
+        const size_t nx = s->n[0], ny = s->n[1];
+        for (int k = 0; k < s->nspecies; ++k) {
+            const double q = s->q[k] * s->w[k];
+            const size_t np = s->np[k];
+            for (size_t p = 0; p < np; ++p) {
+                if (!s->alive[k][p]) continue;
+                size_t ii[2], jj[2], kk[2];
+                double fx, fy, fz;
+                wall_axis(s, 0, s->pos[k][p], &ii[0], &ii[1], &fx);
+                wall_axis(s, 1, s->pos[k][np + p], &jj[0], &jj[1], &fy);
+                wall_axis(s, 2, s->pos[k][2 * np + p], &kk[0], &kk[1], &fz);
+                const double wx[2] = {1.0 - fx, fx}, wy[2] = {1.0 - fy, fy}, wz[2] = {1.0 - fz, fz};
+                for (int c = 0; c < 2; ++c)
+                    for (int b = 0; b < 2; ++b)
+                        for (int a = 0; a < 2; ++a) {
+                            const double shape = wx[a] * wy[b] * wz[c];
+                            s->rho[(kk[c] * ny + jj[b]) * nx + ii[a]] +=
+                                q * shape / wall_node_volume(s, ii[a], jj[b], kk[c]);
+                        }
+            }
+        }
+        /* FieldSolver::solve(Mesh3D&) -> solve_dirichlet_iterative, src/FieldSolver.cpp:399-405,
+         * started from the previous step's potential */
+        ora_solve_dirichlet_nd_warm(s->rho, s->phi, s->E, 3, s->n, s->L, s->eps, NULL);
+        return;
+    }
     if (s->walls) {
         /* deposit_charge_cic(Mesh2D&), src/Mesh2D.cpp:90-144 */
         const size_t nx = s->n[0];
@@ -1703,6 +1756,27 @@ static void simnd_deposit_solve(ora_simnd* s) {
 static void simnd_gather(const ora_simnd* s, const double* pos, size_t np, size_t i, double e[3]) {
     double p[3] = {pos[i], pos[np + i], s->dims == 3 ? pos[2 * np + i] : 0.0};
     e[2] = 0.0;
+    if (s->walls && s->dims == 3) {
+        /* interpolate_electric(Mesh3D&) on a Dirichlet mesh, src/FieldSolver.cpp:978-1038 */
+        const size_t nx = s->n[0], ny = s->n[1], N = s->n[0] * s->n[1] * s->n[2];
+        size_t ii[2], jj[2], kk[2];
+        double fx, fy, fz;
+        wall_axis(s, 0, p[0], &ii[0], &ii[1], &fx);
+        wall_axis(s, 1, p[1], &jj[0], &jj[1], &fy);
+        wall_axis(s, 2, p[2], &kk[0], &kk[1], &fz);
+        const double wx[2] = {1.0 - fx, fx}, wy[2] = {1.0 - fy, fy}, wz[2] = {1.0 - fz, fz};
+        e[0] = e[1] = e[2] = 0.0;
+        for (int c = 0; c < 2; ++c)
+            for (int b = 0; b < 2; ++b)
+                for (int a = 0; a < 2; ++a) {
+                    const double shape = wx[a] * wy[b] * wz[c];
+                    const size_t id = (kk[c] * ny + jj[b]) * nx + ii[a];
+                    e[0] += s->E[id] * shape;
+                    e[1] += s->E[N + id] * shape;
+                    e[2] += s->E[2 * N + id] * shape;
+                }
+        return;
+    }
     if (s->walls) {
         /* interpolate_electric(Mesh2D&), src/FieldSolver.cpp:926-975 */
         const size_t nx = s->n[0], N = s->n[0] * s->n[1];
@@ -1789,18 +1863,18 @@ static void reflect_coordinate(double* c, double* v, double L) {
     }
 }
 
-/* Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335:
- * returns 0 when the particle is absorbed */
-static int apply_walls(ora_simnd* s, int k, double* x, double* y, double* vx, double* vy) {
-    double* c[4] = {x, x, y, y};
-    double* v[4] = {vx, vx, vy, vy};
-    const double L[4] = {s->L[0], s->L[0], s->L[1], s->L[1]};
-    for (int side = 0; side < 4; ++side) {
-        const int lower = (side & 1) == 0;
-        if (lower ? *c[side] >= 0.0 : *c[side] <= L[side]) continue;
+/* Simulation2D::apply_particle_boundaries, src/Simulation2D.cpp:1309-1335, and
+ * Simulation3D::apply_particle_boundaries, src/Simulation3D.cpp:309-340: sides
+ * in the order left, right, bottom, top (, back, front); returns 0 when the
+ * particle is absorbed */
+static int apply_walls(ora_simnd* s, int k, double* x, double* v) {
+    for (int side = 0; side < 2 * s->dims; ++side) {
+        const int a = side >> 1, lower = (side & 1) == 0;
+        const double L = s->L[a];
+        if (lower ? x[a] >= 0.0 : x[a] <= L) continue;
         if (s->pbc[side] == 1) { s->losses[k][side]++; return 0; }
-        if (s->pbc[side] == 2) reflect_coordinate(c[side], v[side], L[side]);
-        else *c[side] = wrap(*c[side], L[side]);
+        if (s->pbc[side] == 2) reflect_coordinate(&x[a], &v[a], L);
+        else x[a] = wrap(x[a], L);
     }
     return 1;
 }
@@ -1820,10 +1894,10 @@ void ora_simnd_step(ora_simnd* s, size_t steps) {
                 if (s->boris) ora_boris(v, e, B, qm, s->dt);
                 else for (int a = 0; a < s->dims; ++a) v[a] += qm * e[a] * s->dt;
                 if (s->walls) {
-                    double x = s->pos[k][i] + v[0] * s->dt, y = s->pos[k][np + i] + v[1] * s->dt;
-                    if (!apply_walls(s, k, &x, &y, &v[0], &v[1])) s->alive[k][i] = 0;
-                    s->pos[k][i] = x;
-                    s->pos[k][np + i] = y;
+                    double x[3];
+                    for (int a = 0; a < s->dims; ++a) x[a] = s->pos[k][a * np + i] + v[a] * s->dt;
+                    if (!apply_walls(s, k, x, v)) s->alive[k][i] = 0;
+                    for (int a = 0; a < s->dims; ++a) s->pos[k][a * np + i] = x[a];
                     for (int a = 0; a < 3; ++a) s->vh[k][a * np + i] = v[a];
                     continue;
                 }

@@ -135,6 +135,9 @@ void ora_simnd_destroy(ora_simnd* s);
  * particle boundaries [left, right, bottom, top] (0 periodic, 1 absorbing,
  * 2 reflecting); absorbed particles stay in place with alive = 0 */
 int ora_simnd_set_walls(ora_simnd* s, const int* dirichlet, const double* potentials, const int* particle);
+/* 3D walls (before load): a Dirichlet mesh with grounded walls on every side
+ * and particle boundaries [left, right, bottom, top, back, front] */
+int ora_simnd_set_walls3d(ora_simnd* s, const int* particle);
 void ora_simnd_alive_losses(const ora_simnd* s, int k, uint8_t* alive, uint64_t* losses);
 void ora_simnd_load(ora_simnd* s, int k, size_t np, const double* pos, const double* v, const double* vh);
 /* magnetic_field_profile: B piecewise linear along `axis` (values rows x 3) */

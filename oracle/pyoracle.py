@@ -742,13 +742,23 @@ class SimND:
         if Lb.ora_simnd_set_walls(self.h, d, dptr(pot), pb):
             raise RuntimeError(Lb.ora_last_error().decode())
 
+    def set_walls3d(self, particle):
+        """3D walls (before load): a Dirichlet mesh with grounded walls on
+        every side and particle boundaries (left, right, bottom, top, back,
+        front: 0 periodic, 1 absorbing, 2 reflecting)."""
+        Lb = _nd_bind()
+        Lb.ora_simnd_set_walls3d.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        if Lb.ora_simnd_set_walls3d(self.h, (C.c_int * 6)(*particle)):
+            raise RuntimeError(Lb.ora_last_error().decode())
+
     def alive_losses(self, k):
+        """alive flags and the absorbed counts per side of species k (4 in 2D, 6 in 3D)"""
         Lb = _nd_bind()
         Lb.ora_simnd_alive_losses.argtypes = [C.c_void_p, C.c_int, _U8P, _U64P]
         al = np.zeros(self.np[k], np.uint8)
-        lo = np.zeros(4, np.uint64)
+        lo = np.zeros(6, np.uint64)
         Lb.ora_simnd_alive_losses(self.h, k, u8ptr(al), u64ptr(lo))
-        return al, lo
+        return al, lo[:2 * self.dims]
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -809,9 +819,13 @@ class RefND:
     def __init__(self, dims, n, L, dt, si, B, species, seed=12345, threads=0, profile=None, walls=None):
         """species: list of (q, m, w, count, drift_x, thermal); profile: optional
         (axis, coordinates, values[rows][3]) magnetic_field_profile; walls:
-        optional 2D (dirichlet[2], potentials[4], particle boundaries[4])."""
+        optional 2D (dirichlet[2], potentials[4], particle boundaries[4]) or
+        3D particle boundaries[6] (a grounded Dirichlet mesh)."""
         Lb = _refnd_bind()
-        if walls is not None:
+        if walls is not None and dims == 3:
+            Lb.refnd_set_walls3d.argtypes = [C.POINTER(C.c_int)]
+            Lb.refnd_set_walls3d((C.c_int * 6)(*walls))
+        elif walls is not None:
             Lb.refnd_set_walls.argtypes = [C.POINTER(C.c_int), _DP, C.POINTER(C.c_int)]
             self._pot = np.ascontiguousarray(walls[1], dtype=np.float64)
             Lb.refnd_set_walls((C.c_int * 2)(*walls[0]), dptr(self._pot), (C.c_int * 4)(*walls[2]))
@@ -866,9 +880,9 @@ class RefND:
         Lb.refnd_alive_losses.argtypes = [C.c_void_p, C.c_int, _U8P, _U64P]
         n = Lb.refnd_count(self.h, k)
         al = np.zeros(n, np.uint8)
-        lo = np.zeros(4, np.uint64)
+        lo = np.zeros(6, np.uint64)
         Lb.refnd_alive_losses(self.h, k, u8ptr(al), u64ptr(lo))
-        return al, lo
+        return al, lo[:2 * self.dims]
 
     def fields(self):
         rho, phi, E = np.zeros(self.N), np.zeros(self.N), np.zeros(self.dims * self.N)

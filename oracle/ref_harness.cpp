@@ -498,6 +498,18 @@ void refnd_set_walls(const int* dirichlet, const double* pot, const int* pbc) {
     for (int k = 0; k < 4; ++k) { g_walls.pot[k] = pot[k]; g_walls.pbc[k] = pbc[k]; }
 }
 
+// 3D walls for the next refnd_create*: Boundary::Dirichlet (grounded) and the
+// particle boundaries left, right, bottom, top, back, front.
+static struct {
+    bool set = false;
+    int pbc[6];
+} g_walls3;
+
+void refnd_set_walls3d(const int* pbc) {
+    g_walls3.set = true;
+    for (int k = 0; k < 6; ++k) g_walls3.pbc[k] = pbc[k];
+}
+
 int refnd_create_profile(int dims, const size_t* n, const double* L, double dt, int si, const double* B,
                          int nspecies, const double* q, const double* m, const double* w, const size_t* count,
                          const double* drift, const double* thermal, unsigned seed, int threads, int prof_axis,
@@ -564,6 +576,20 @@ int refnd_create_profile(int dims, const size_t* n, const double* L, double dt, 
             c.magnetic_field_profile = profile;
             c.seed = seed; c.runtime = rt;
             c.output_dir = std::filesystem::temp_directory_path() / "apic_ref3d";
+            if (g_walls3.set) {
+                auto pb = [](int k) {
+                    return k == 1 ? pic::ParticleBoundary::Absorbing
+                           : k == 2 ? pic::ParticleBoundary::Reflecting : pic::ParticleBoundary::Periodic;
+                };
+                c.boundary = pic::Boundary::Dirichlet;
+                c.particle_boundary_config.left = pb(g_walls3.pbc[0]);
+                c.particle_boundary_config.right = pb(g_walls3.pbc[1]);
+                c.particle_boundary_config.bottom = pb(g_walls3.pbc[2]);
+                c.particle_boundary_config.top = pb(g_walls3.pbc[3]);
+                c.particle_boundary_config.back = pb(g_walls3.pbc[4]);
+                c.particle_boundary_config.front = pb(g_walls3.pbc[5]);
+                g_walls3.set = false;
+            }
             for (int s = 0; s < nspecies; ++s) {
                 pic::Species3DConfig sc;
                 sc.name = "s" + std::to_string(s);
@@ -630,10 +656,20 @@ int refnd_get(void* h, int s, double* pos, double* v, double* vh) {
     return 0;
 }
 
-// 2D: alive flags and species_boundary_losses (left, right, bottom, top)
+// alive flags and the absorbed counts: 2D species_boundary_losses()[s] (left,
+// right, bottom, top); 3D boundary_losses() of the whole run (left, right,
+// bottom, top, back, front; the reference keeps no per-species ledger in 3D)
 int refnd_alive_losses(void* h, int s, uint8_t* alive, uint64_t* losses) {
     auto* r = static_cast<RefND*>(h);
-    if (r->dims != 2) return 1;
+    if (r->dims == 3) {
+        const auto& ps = r->s3->species().at(s).particles();
+        for (size_t i = 0; i < ps.size(); ++i) alive[i] = ps[i].alive ? 1 : 0;
+        const auto& l = r->s3->boundary_losses();
+        losses[0] = l.absorbed_left; losses[1] = l.absorbed_right;
+        losses[2] = l.absorbed_bottom; losses[3] = l.absorbed_top;
+        losses[4] = l.absorbed_back; losses[5] = l.absorbed_front;
+        return 0;
+    }
     const auto& ps = r->s2->species().at(s).particles();
     for (size_t i = 0; i < ps.size(); ++i) alive[i] = ps[i].alive ? 1 : 0;
     const auto& l = r->s2->species_boundary_losses().at(s);

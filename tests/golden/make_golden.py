@@ -179,7 +179,9 @@ def _nd_run(name, dims, n, L, B, steps, profile=None, walls=None):
             out[f"losses_s{k}"] = lo
     rho, phi, E = R.fields()
     out.update(rho=rho, phi=phi, E=E, time=R.time())
-    if walls is not None:
+    if walls is not None and dims == 3:
+        out.update(walls_particle=np.array(walls))
+    elif walls is not None:
         out.update(walls_dirichlet=np.array(walls[0]), walls_potentials=np.array(walls[1]),
                    walls_particle=np.array(walls[2]))
     if profile is not None:
@@ -200,6 +202,24 @@ def walls_fixture():
     (the reference's SOR): absorbing and reflecting particle boundaries, 25 steps."""
     for name, (n, B, d, pot, pb) in WALL_CASES.items():
         _nd_run(name, 2, n, (4.0, 2.0), B, 25, walls=(d, pot, pb))
+
+
+# 3D runs with walls (a grounded Dirichlet mesh): name -> nodes, B, particle
+# boundaries (left, right, bottom, top, back, front: 0 periodic, 1 absorbing,
+# 2 reflecting)
+WALL3_CASES = {
+    "sim3d_walls_boris": ((17, 9, 9), (0.3, 0.0, 0.5), (1, 2, 1, 2, 1, 1)),
+    "sim3d_walls_leapfrog": ((9, 9, 17), (0.0, 0.0, 0.0), (2, 1, 0, 0, 1, 2)),
+}
+WALL3_LENGTH = (4.0, 2.0, 3.0)
+
+
+def walls3d_fixture():
+    """Simulation3D on a Dirichlet mesh: clamped trilinear CIC over the
+    half-cell wall volumes, the warm-started SOR, absorbing, reflecting and
+    periodic particle boundaries with the run's loss ledger, 25 steps."""
+    for name, (n, B, pb) in WALL3_CASES.items():
+        _nd_run(name, 3, n, WALL3_LENGTH, B, 25, walls=pb)
 
 
 def collide_hg_fixture():
@@ -409,6 +429,7 @@ def main(names=None):
     ccp_diag_fixture()
     townsend_fixture()
     walls_fixture()
+    walls3d_fixture()
     mixed_fixture()
     dirichlet_fixture()
     bprofile_fixture()

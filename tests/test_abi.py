@@ -108,3 +108,20 @@ def test_cpp20_facade_compiles_and_maps_errors(tmp_path):
     out = subprocess.run([str(build_facade_check(tmp_path))], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "invalid_argument: simulation dt must be positive and finite" in out.stdout
+
+
+@pytest.mark.parametrize("walls,msg", [
+    (((1, 1, 0), None, (0,) * 6), "3D meshes are periodic or Dirichlet on every axis"),
+    (((1, 1, 1), (0.0, 1.0, 0.0, 0.0), (0,) * 6), "3D Dirichlet walls are grounded"),
+    (((1, 1, 1), None, (0, 0, 0, 0, 0, 7)), "unknown particle boundary"),
+])
+def test_3d_wall_configuration_checks(walls, msg):
+    """A 3D mesh is periodic or Dirichlet as a whole, with grounded walls
+    (Simulation3DConfig's single field boundary, src/Mesh3D.cpp:37-48,
+    src/FieldSolver.cpp:351-372); create rejects anything else before it looks
+    for a device."""
+    cfg = apic.config_nd(dims=3, n=(9, 9, 9), length=(1.0, 1.0, 1.0), dt=0.1,
+                         species=[(-1.0, 1.0, 1.0, 16)], walls=walls)
+    with pytest.raises(apic.ApicError) as e:
+        apic.SimulationND(cfg)
+    assert msg in str(e.value)

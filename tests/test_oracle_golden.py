@@ -338,3 +338,34 @@ def test_2d_run_with_walls_bit_exact(name):
     rho, phi, E = sim.fields()
     assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"])
     assert np.array_equal(E[:2].ravel(), f["E"].ravel()[: 2 * len(rho)])
+
+
+@pytest.mark.parametrize("name", ["sim3d_walls_boris", "sim3d_walls_leapfrog"])
+def test_3d_run_with_walls_bit_exact(name):
+    """Simulation3D on a Dirichlet mesh: clamped trilinear CIC over the half-cell
+    wall volumes, clamped gather, the warm-started SOR with grounded walls,
+    absorbing, reflecting and periodic particle boundaries in the order left,
+    right, bottom, top, back, front (src/Simulation3D.cpp:25-97, :309-365,
+    src/Mesh3D.cpp:52-126, src/FieldSolver.cpp:830-907, :978-1038): 25 steps,
+    bit-exact.  The reference keeps one loss ledger for the run; the oracle's
+    per-species counts add up to it."""
+    from golden.make_golden import WALL3_CASES, WALL3_LENGTH
+    n, B, pb = WALL3_CASES[name]
+    f = load(f"{name}.npz")
+    sim = po.SimND(3, n, WALL3_LENGTH, 0.1, 1.0, B, ND_SPECIES)
+    sim.set_walls3d(pb)
+    for k in range(2):
+        sim.load(k, f[f"init_s{k}_pos"], f[f"init_s{k}_v"], f[f"init_s{k}_vh"])
+    sim.initialize_fields()
+    sim.step(int(f["steps"]))
+    total = np.zeros(6, np.uint64)
+    for k in range(2):
+        al, lo = sim.alive_losses(k)
+        total += lo
+        assert np.array_equal(al, f[f"final_s{k}_alive"]), (name, k)
+        for key, arr in zip(("pos", "v", "vh"), sim.particles(k)):
+            assert np.array_equal(arr, f[f"final_s{k}_{key}"]), (name, k, key)
+    assert np.array_equal(total, f["losses_s0"]) and total.sum() > 0
+    rho, phi, E = sim.fields()
+    assert np.array_equal(rho, f["rho"]) and np.array_equal(phi, f["phi"])
+    assert np.array_equal(E.ravel()[: 3 * len(rho)], f["E"].ravel())
