@@ -1198,6 +1198,7 @@ struct FieldsND {
     double* phi;
     double* E;
     float* E32;  // FP32 form: interleaved float copy of E (2 or 4 floats per node)
+    const double* kvec[3];  // wavenumbers 2 pi m / L per axis and index (m the signed mode), or null
     int nacc;    // FP32 form: per-species weight accumulators
     unsigned long long* acc[APIC_MAX_SPECIES];
     double acc_scale[APIC_MAX_SPECIES];  // charge density per accumulator unit
@@ -1349,6 +1350,110 @@ __device__ __forceinline__ void tile_elem(const FftPass& f, int b, int& l, int& 
     else { e = b >> f.log2T; l = b & (f.T - 1); }
 }
 
+// Forward input at node g: the species' fixed-point densities summed (or the
+// FP64 rho of a stand-alone solve); the accumulators are cleared and rho kept.
+__device__ __forceinline__ double density_at(const FieldsND& F, long long g) {
+    double r;
+    if (F.rho_in) {
+        r = F.rho_in[g];
+    } else if (F.nacc) {
+        unsigned long long q[APIC_MAX_SPECIES] = {0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < APIC_MAX_SPECIES; ++k)
+            if (k < F.nacc) q[k] = F.acc[k][g];
+        r = 0.0;
+#pragma unroll
+        for (int k = 0; k < APIC_MAX_SPECIES; ++k)
+            if (k < F.nacc) {
+                r += (double)(long long)q[k] * F.acc_scale[k];
+                F.acc[k][g] = 0ull;
+            }
+    } else {
+        r = (double)(long long)F.rho_acc[g] * F.inv_scale;
+        F.rho_acc[g] = 0ull;
+    }
+    F.rho[g] = r;
+    return r;
+}
+
+// k-space multiply at node g (src/FieldSolver.cpp:470-488, :687-712) into two
+// packed spectra A = phi_k + i Ex_k / pack, B = Ey_k / pack + i Ez_k / pack,
+// each E component restricted to its Hermitian part (zero on its own Nyquist
+// plane) so that both inverse transforms are real pairs
+__device__ __forceinline__ void kspace_at(const FieldsND& F, long long g, Cplx r, Cplx& a, Cplx& bb) {
+    const double twopi = 2.0 * 3.141592653589793;
+    const double ip = 1.0 / F.pack;
+    const int ix = (int)(g & (F.nx - 1));
+    const int iy = (int)((g >> F.lnx) & (F.ny - 1));
+    const int iz = F.dims == 3 ? (int)(g >> (F.lnx + F.lny)) : 0;
+    a = {0.0, 0.0};
+    bb = {0.0, 0.0};
+    if (ix != 0 || iy != 0 || iz != 0) {
+        const double mx = ix <= F.nx / 2 ? (double)ix : -(double)(F.nx - ix);
+        const double my = iy <= F.ny / 2 ? (double)iy : -(double)(F.ny - iy);
+        const double kx = twopi * mx / F.L[0];
+        const double ky = twopi * my / F.L[1];
+        double kz = 0.0, k2;
+        if (F.dims == 3) {
+            const double mz = iz <= F.nz / 2 ? (double)iz : -(double)(F.nz - iz);
+            kz = twopi * mz / F.L[2];
+            k2 = kx * kx + ky * ky + kz * kz;
+        } else {
+            k2 = kx * kx + ky * ky;
+        }
+        const double den = F.eps * k2;
+        const double pr = r.re / den, pi = r.im / den;
+        // -(0,1) k phik = (k pi, -(k pr))
+        const bool nyx = (F.nx % 2 == 0) && ix == F.nx / 2;
+        const bool nyy = (F.ny % 2 == 0) && iy == F.ny / 2;
+        const bool nyz = F.dims == 3 && (F.nz % 2 == 0) && iz == F.nz / 2;
+        const double exr = nyx ? 0.0 : kx * pi, exi = nyx ? 0.0 : -(kx * pr);
+        const double eyr = nyy ? 0.0 : ky * pi, eyi = nyy ? 0.0 : -(ky * pr);
+        const double ezr = nyz ? 0.0 : kz * pi, ezi = nyz ? 0.0 : -(kz * pr);
+        a = {pr - exi * ip, pi + exr * ip};
+        bb = {eyr * ip - ezi * ip, eyi * ip + ezr * ip};
+    }
+}
+
+// kspace_at with the wavenumbers read from the per-axis tables (the same
+// values, computed on the host) and one correctly rounded reciprocal of
+// eps k^2 in place of two divisions
+__device__ __forceinline__ void kspace_tab(const FieldsND& F, long long g, Cplx r, Cplx& a, Cplx& bb) {
+    const double ip = 1.0 / F.pack;
+    const int ix = (int)(g & (F.nx - 1));
+    const int iy = (int)((g >> F.lnx) & (F.ny - 1));
+    const int iz = F.dims == 3 ? (int)(g >> (F.lnx + F.lny)) : 0;
+    a = {0.0, 0.0};
+    bb = {0.0, 0.0};
+    if (ix != 0 || iy != 0 || iz != 0) {
+        const double kx = __ldg(F.kvec[0] + ix), ky = __ldg(F.kvec[1] + iy);
+        const double kz = F.dims == 3 ? __ldg(F.kvec[2] + iz) : 0.0;
+        const double k2 = F.dims == 3 ? kx * kx + ky * ky + kz * kz : kx * kx + ky * ky;
+        const double inv = __drcp_rn(F.eps * k2);
+        const double pr = r.re * inv, pi = r.im * inv;
+        const bool nyx = ix == F.nx / 2, nyy = iy == F.ny / 2, nyz = F.dims == 3 && iz == F.nz / 2;
+        const double exr = nyx ? 0.0 : kx * pi, exi = nyx ? 0.0 : -(kx * pr);
+        const double eyr = nyy ? 0.0 : ky * pi, eyi = nyy ? 0.0 : -(ky * pr);
+        const double ezr = nyz ? 0.0 : kz * pi, ezi = nyz ? 0.0 : -(kz * pr);
+        a = {pr - exi * ip, pi + exr * ip};
+        bb = {eyr * ip - ezi * ip, eyi * ip + ezr * ip};
+    }
+}
+
+// phi and E at node g from the inverse transforms of the packed spectra
+__device__ __forceinline__ void store_fields(const FieldsND& F, long long g, Cplx a, Cplx bb) {
+    F.phi[g] = a.re;
+    if (F.dims == 2) {
+        reinterpret_cast<double2*>(F.E)[g] = make_double2(a.im * F.pack, bb.re * F.pack);
+        if (F.E32) reinterpret_cast<float2*>(F.E32)[g] = make_float2((float)(a.im * F.pack), (float)(bb.re * F.pack));
+    } else {
+        reinterpret_cast<double4*>(F.E)[g] = make_double4(a.im * F.pack, bb.re * F.pack, bb.im * F.pack, 0.0);
+        if (F.E32)
+            reinterpret_cast<float4*>(F.E32)[g] =
+                make_float4((float)(a.im * F.pack), (float)(bb.re * F.pack), (float)(bb.im * F.pack), 0.0f);
+    }
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(kFftThreads) k_fft(FieldsND F, FftPass f) {
     extern __shared__ __align__(16) unsigned char fsm[];
@@ -1371,27 +1476,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(FieldsND F, FftPass f) {
         const long long g = base + l * f.ls + e * f.es;
         const int s = l * ld + e;
         if (MODE == kFwdFromRho) {
-            double r;
-            if (F.rho_in) {
-                r = F.rho_in[g];
-            } else if (F.nacc) {
-                unsigned long long q[APIC_MAX_SPECIES] = {0, 0, 0, 0};
-#pragma unroll
-                for (int k = 0; k < APIC_MAX_SPECIES; ++k)
-                    if (k < F.nacc) q[k] = F.acc[k][g];
-                r = 0.0;
-#pragma unroll
-                for (int k = 0; k < APIC_MAX_SPECIES; ++k)
-                    if (k < F.nacc) {
-                        r += (double)(long long)q[k] * F.acc_scale[k];
-                        F.acc[k][g] = 0ull;
-                    }
-            } else {
-                r = (double)(long long)F.rho_acc[g] * F.inv_scale;
-                F.rho_acc[g] = 0ull;
-            }
-            F.rho[g] = r;
-            X[s] = {r, 0.0};
+            X[s] = {density_at(F, g), 0.0};
         } else if (MODE == kFwdInPlace || MODE == kFwdMulInv) {
             X[s] = F.W[g];
         } else {
@@ -1407,46 +1492,12 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(FieldsND F, FftPass f) {
     X = res;
     Y = res + f.T * ld;
     if (MODE == kFwdMulInv) {
-        // k-space multiply (src/FieldSolver.cpp:470-488, :687-712) into two packed
-        // spectra A = phi_k + i Ex_k / pack, B = Ey_k / pack + i Ez_k / pack,
-        // each E component restricted to its Hermitian part (zero on its own
-        // Nyquist plane) so that both inverse transforms are real pairs
-        const double twopi = 2.0 * 3.141592653589793;
-        const double ip = 1.0 / F.pack;
         for (int b = threadIdx.x; b < total; b += blockDim.x) {
             int l, e;
             tile_elem(f, b, l, e);
             const long long g = base + l * f.ls + e * f.es;
-            const int ix = (int)(g & (F.nx - 1));
-            const int iy = (int)((g >> F.lnx) & (F.ny - 1));
-            const int iz = F.dims == 3 ? (int)(g >> (F.lnx + F.lny)) : 0;
-            const Cplx r = X[l * ld + e];
-            Cplx a = {0.0, 0.0}, bb = {0.0, 0.0};
-            if (ix != 0 || iy != 0 || iz != 0) {
-                const double mx = ix <= F.nx / 2 ? (double)ix : -(double)(F.nx - ix);
-                const double my = iy <= F.ny / 2 ? (double)iy : -(double)(F.ny - iy);
-                const double kx = twopi * mx / F.L[0];
-                const double ky = twopi * my / F.L[1];
-                double kz = 0.0, k2;
-                if (F.dims == 3) {
-                    const double mz = iz <= F.nz / 2 ? (double)iz : -(double)(F.nz - iz);
-                    kz = twopi * mz / F.L[2];
-                    k2 = kx * kx + ky * ky + kz * kz;
-                } else {
-                    k2 = kx * kx + ky * ky;
-                }
-                const double den = F.eps * k2;
-                const double pr = r.re / den, pi = r.im / den;
-                // -(0,1) k phik = (k pi, -(k pr))
-                const bool nyx = (F.nx % 2 == 0) && ix == F.nx / 2;
-                const bool nyy = (F.ny % 2 == 0) && iy == F.ny / 2;
-                const bool nyz = F.dims == 3 && (F.nz % 2 == 0) && iz == F.nz / 2;
-                const double exr = nyx ? 0.0 : kx * pi, exi = nyx ? 0.0 : -(kx * pr);
-                const double eyr = nyy ? 0.0 : ky * pi, eyi = nyy ? 0.0 : -(ky * pr);
-                const double ezr = nyz ? 0.0 : kz * pi, ezi = nyz ? 0.0 : -(kz * pr);
-                a = {pr - exi * ip, pi + exr * ip};
-                bb = {eyr * ip - ezi * ip, eyi * ip + ezr * ip};
-            }
+            Cplx a, bb;
+            kspace_at(F, g, X[l * ld + e], a, bb);
             const int s = l * ld + e;
             R1[s] = a;
             R1[f.T * ld + s] = bb;
@@ -1471,19 +1522,170 @@ __global__ void __launch_bounds__(kFftThreads) k_fft(FieldsND F, FftPass f) {
             F.A[g] = X[s];
             F.B[g] = Y[s];
         } else {
-            const Cplx a = X[s], bb = Y[s];
-            F.phi[g] = a.re;
-            if (F.dims == 2) {
-                reinterpret_cast<double2*>(F.E)[g] = make_double2(a.im * F.pack, bb.re * F.pack);
-                if (F.E32) reinterpret_cast<float2*>(F.E32)[g] = make_float2((float)(a.im * F.pack), (float)(bb.re * F.pack));
-            } else {
-                reinterpret_cast<double4*>(F.E)[g] = make_double4(a.im * F.pack, bb.re * F.pack, bb.im * F.pack, 0.0);
-                if (F.E32)
-                    reinterpret_cast<float4*>(F.E32)[g] =
-                        make_float4((float)(a.im * F.pack), (float)(bb.re * F.pack), (float)(bb.im * F.pack), 0.0f);
+            store_fields(F, g, X[s], Y[s]);
+        }
+    }
+}
+
+// ---- 256-point lines: a four-step FFT in registers ---------------------------------
+//
+// Lines of 256 = 16 x 16 points, eight lines per CTA and 16 threads per line.
+// Thread slot s of a line holds the points s + 16 j (j < 16) in registers:
+// a 16-point DFT over j, the twiddles W256^(s k1), one exchange through shared
+// memory (thread s then holds column k1 = s), a second 16-point DFT, and the
+// thread holds the transform at s + 16 k2, the same positions it loaded, so a
+// pass reads and writes each element once and in place.  Lanes run along the
+// line on the x pass (16 consecutive points per half warp) and across the
+// tile's lines on the strided y / z passes (8 consecutive lines, 128 B), so
+// every global access moves whole 128-256 B segments; the registers hold the
+// loads in flight (16 or 32 per thread) instead of a shared-memory tile.
+constexpr int kF256Lines = 8;
+constexpr int kF256Threads = kF256Lines * 16;
+
+template <bool XP>
+__device__ __forceinline__ void f256_map(int tid, int& l, int& s) {
+    if (XP) { s = tid & 15; l = tid >> 4; }
+    else { l = tid & (kF256Lines - 1); s = tid >> 3; }
+}
+
+// exchange slot of (line l, row r, column c): written by slot c as row r,
+// read by slot r as column c; conflict-free for both lane layouts
+template <bool XP>
+__device__ __forceinline__ int f256_xi(int l, int r, int c) {
+    return XP ? (l * 16 + r) * 17 + c : (r * 16 + c) * kF256Lines + l;
+}
+template <bool XP>
+constexpr int f256_xsize() { return XP ? kF256Lines * 16 * 17 : kF256Lines * 256; }
+
+// forward (inv = false) or inverse transforms of NA lines held as a[k][16]
+template <bool XP, int NA>
+__device__ __forceinline__ void fft256(Cplx (&a)[NA][16], Cplx* xb, const Cplx* tws, int l, int s, bool inv) {
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+        dft_small<16>(a[k], inv);
+#pragma unroll
+        for (int k1 = 1; k1 < 16; ++k1) {
+            Cplx w = tws[(s * k1) & 255];
+            if (inv) w.im = -w.im;
+            const Cplx x = a[k][k1];
+            a[k][k1] = {x.re * w.re - x.im * w.im, x.re * w.im + x.im * w.re};
+        }
+    }
+    __syncthreads();  // earlier readers of the exchange buffers are done
+#pragma unroll
+    for (int k = 0; k < NA; ++k)
+#pragma unroll
+        for (int k1 = 0; k1 < 16; ++k1) xb[k * f256_xsize<XP>() + f256_xi<XP>(l, k1, s)] = a[k][k1];
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+#pragma unroll
+        for (int t = 0; t < 16; ++t) a[k][t] = xb[k * f256_xsize<XP>() + f256_xi<XP>(l, s, t)];
+        dft_small<16>(a[k], inv);
+        if (inv) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                a[k][j].re *= 1.0 / 256.0;
+                a[k][j].im *= 1.0 / 256.0;
             }
         }
     }
+}
+
+template <int MODE, bool XP>
+__global__ void __launch_bounds__(kF256Threads, 3) k_fft256(FieldsND F, FftPass f) {
+    extern __shared__ __align__(16) unsigned char f256_sm[];
+    Cplx* tws = reinterpret_cast<Cplx*>(f256_sm);
+    Cplx* xb = tws + 256;
+    for (int k = threadIdx.x; k < 256; k += blockDim.x) tws[k] = f.tw[k];
+    int l, s;
+    f256_map<XP>(threadIdx.x, l, s);
+    const long long base = tile_base(f, blockIdx.x) + l * f.ls + s * f.es;
+    const long long step = 16 * f.es;  // between a thread's points
+    constexpr bool PAIR = MODE == kInvInPlace || MODE == kInvToFields;
+    Cplx a[PAIR ? 2 : 1][16];
+    // ---- load ----
+    if constexpr (MODE == kFwdFromRho) {
+        // density_at with every load issued before the stores (the arrays may
+        // alias as far as the compiler knows); the same sums in species order
+        double r[16];
+        if (F.rho_in) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) r[j] = F.rho_in[base + j * step];
+        } else if (F.nacc) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) r[j] = 0.0;
+            for (int k = 0; k < F.nacc; ++k) {
+                unsigned long long q[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) q[j] = F.acc[k][base + j * step];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) r[j] += (double)(long long)q[j] * F.acc_scale[k];
+            }
+            for (int k = 0; k < F.nacc; ++k)
+#pragma unroll
+                for (int j = 0; j < 16; ++j) F.acc[k][base + j * step] = 0ull;
+        } else {
+            unsigned long long q[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) q[j] = F.rho_acc[base + j * step];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                r[j] = (double)(long long)q[j] * F.inv_scale;
+                F.rho_acc[base + j * step] = 0ull;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            F.rho[base + j * step] = r[j];
+            a[0][j] = {r[j], 0.0};
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const long long g = base + j * step;
+            if (MODE == kFwdInPlace || MODE == kFwdMulInv) a[0][j] = F.W[g];
+            else {
+                a[0][j] = F.A[g];
+                a[PAIR ? 1 : 0][j] = F.B[g];
+            }
+        }
+    }
+    __syncthreads();  // the twiddles are staged
+    if constexpr (MODE == kFwdMulInv) {
+        fft256<XP, 1>(a, xb, tws, l, s, false);
+        Cplx ab[2][16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) kspace_tab(F, base + j * step, a[0][j], ab[0][j], ab[1][j]);
+        fft256<XP, 2>(ab, xb, tws, l, s, true);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const long long g = base + j * step;
+            F.A[g] = ab[0][j];
+            F.B[g] = ab[1][j];
+        }
+    } else {
+        fft256<XP, PAIR ? 2 : 1>(a, xb, tws, l, s, PAIR);
+    // ---- store ----
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const long long g = base + j * step;
+        if (MODE == kFwdFromRho || MODE == kFwdInPlace) F.W[g] = a[0][j];
+        else if (MODE == kInvInPlace) {
+            F.A[g] = a[0][j];
+            F.B[g] = a[PAIR ? 1 : 0][j];
+        } else {
+            store_fields(F, g, a[0][j], a[PAIR ? 1 : 0][j]);
+        }
+    }
+    }
+}
+
+// shared memory of a 256-point pass: the twiddles and one exchange buffer per line set
+template <bool XP>
+constexpr size_t f256_smem(int mode) {
+    return (256 + (size_t)((mode == kFwdMulInv || mode == kInvInPlace || mode == kInvToFields) ? 2 : 1) *
+                      f256_xsize<XP>()) * sizeof(Cplx);
 }
 
 // Simulation2D/3D sample reductions (src/Diagnostics.cpp:111-137, :205-232):
@@ -1568,6 +1770,8 @@ struct Solver {
     FieldsND F{};
     FftPass px{}, py{}, pz{};    // paired passes (four line buffers)
     FftPass pxs{}, pys{};        // single-array forward passes (two line buffers)
+    bool use256[3] = {false, false, false};  // axis a runs the 256-point register kernels
+    FftPass q256[3]{};
     size_t smem_fwd = 0, smem_pair = 0;
     std::vector<void*>* allocs = nullptr;
     cudaStream_t stream = nullptr;
@@ -1653,6 +1857,27 @@ struct Solver {
         px.tw = pxs.tw = twiddles(F.nx);
         py.tw = pys.tw = F.ny == F.nx ? px.tw : twiddles(F.ny);
         if (dims == 3) pz.tw = F.nz == F.nx ? px.tw : (F.nz == F.ny ? py.tw : twiddles(F.nz));
+        for (int a = 0; a < dims; ++a) {  // kspace_at's wavenumbers, src/FieldSolver.cpp:687-712
+            const int na = a == 0 ? F.nx : (a == 1 ? F.ny : F.nz);
+            std::vector<double> kv(na);
+            const double twopi = 2.0 * 3.141592653589793;
+            for (int i = 0; i < na; ++i) {
+                const double m = i <= na / 2 ? (double)i : -(double)(na - i);
+                kv[i] = twopi * m / F.L[a];
+            }
+            double* d = alloc<double>(na);
+            APIC_CUDA(cudaMemcpyAsync(d, kv.data(), na * sizeof(double), cudaMemcpyHostToDevice, stream));
+            APIC_CUDA(cudaStreamSynchronize(stream));
+            F.kvec[a] = d;
+        }
+        for (int a = 0; a < dims; ++a) {
+            const long long lines = a == 0 ? (long long)F.ny * F.nz : F.nx;
+            use256[a] = n[a] == 256 && lines % kF256Lines == 0;
+            if (use256[a]) {
+                q256[a] = pass(a, kF256Lines);
+                q256[a].tw = a == 0 ? px.tw : (a == 1 ? py.tw : pz.tw);
+            }
+        }
         smem_pair = std::max(smem_of(px, kFwdMulInv), smem_of(py, kFwdMulInv));
         if (dims == 3) smem_pair = std::max(smem_pair, smem_of(pz, kFwdMulInv));
         require(smem_pair <= kFftSmemMax, "FFT tile exceeds the shared-memory bound", APIC_ERR_UNSUPPORTED);
@@ -1665,18 +1890,33 @@ struct Solver {
         return (mode == kFwdFromRho || mode == kFwdInPlace) ? 2 * line + tw : 4 * line + tw;
     }
 
+    // one pass along `axis`: the 256-point register kernel where the extent
+    // allows it, else the shared-memory tile kernel with pass `tile`
+    template <int MODE>
+    void fft_pass(int axis, const FftPass& tile) {
+        if (use256[axis]) {
+            const FftPass& q = q256[axis];
+            if (axis == 0)
+                k_fft256<MODE, true><<<(unsigned)tiles(q), kF256Threads, f256_smem<true>(MODE), stream>>>(F, q);
+            else
+                k_fft256<MODE, false><<<(unsigned)tiles(q), kF256Threads, f256_smem<false>(MODE), stream>>>(F, q);
+        } else {
+            k_fft<MODE><<<(unsigned)tiles(tile), kFftThreads, smem_of(tile, MODE), stream>>>(F, tile);
+        }
+    }
+
     // rho_acc -> rho, phi, E (the fixed-point accumulator is cleared)
     void solve() {
         if (F.dims == 2) {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kFftThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
-            k_fft<kFwdMulInv><<<(unsigned)tiles(py), kFftThreads, smem_of(py, kFwdMulInv), stream>>>(F, py);
-            k_fft<kInvToFields><<<(unsigned)tiles(px), kFftThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+            fft_pass<kFwdFromRho>(0, pxs);
+            fft_pass<kFwdMulInv>(1, py);
+            fft_pass<kInvToFields>(0, px);
         } else {
-            k_fft<kFwdFromRho><<<(unsigned)tiles(pxs), kFftThreads, smem_of(pxs, kFwdFromRho), stream>>>(F, pxs);
-            k_fft<kFwdInPlace><<<(unsigned)tiles(pys), kFftThreads, smem_of(pys, kFwdInPlace), stream>>>(F, pys);
-            k_fft<kFwdMulInv><<<(unsigned)tiles(pz), kFftThreads, smem_of(pz, kFwdMulInv), stream>>>(F, pz);
-            k_fft<kInvInPlace><<<(unsigned)tiles(py), kFftThreads, smem_of(py, kInvInPlace), stream>>>(F, py);
-            k_fft<kInvToFields><<<(unsigned)tiles(px), kFftThreads, smem_of(px, kInvToFields), stream>>>(F, px);
+            fft_pass<kFwdFromRho>(0, pxs);
+            fft_pass<kFwdInPlace>(1, pys);
+            fft_pass<kFwdMulInv>(2, pz);
+            fft_pass<kInvInPlace>(1, py);
+            fft_pass<kInvToFields>(0, px);
         }
         APIC_CUDA(cudaGetLastError());
     }
@@ -1719,6 +1959,17 @@ void ensure_solver_attributes() {
     APIC_CUDA(cudaFuncSetAttribute(k_fft<kFwdMulInv>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
     APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvInPlace>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
     APIC_CUDA(cudaFuncSetAttribute(k_fft<kInvToFields>, cudaFuncAttributeMaxDynamicSharedMemorySize, fft));
+    const int f256x = (int)f256_smem<true>(kInvToFields), f256s = (int)f256_smem<false>(kInvToFields);
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdFromRho, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256x));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdInPlace, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256x));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdMulInv, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256x));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kInvInPlace, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256x));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kInvToFields, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256x));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdFromRho, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256s));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdInPlace, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256s));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kFwdMulInv, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256s));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kInvInPlace, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256s));
+    APIC_CUDA(cudaFuncSetAttribute(k_fft256<kInvToFields, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, f256s));
     const int lines = (int)(3 * kMaxLine * sizeof(Cplx));  // three line buffers of the longest extent
     APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
     APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));

@@ -52,8 +52,12 @@ def test_structured_step_parity(case, steps):
     assert s.step == steps and s.live_particles == wl.particles
 
 
-@pytest.mark.parametrize("dims,n", [(2, (64, 32)), (3, (32, 16, 8)), (3, (8, 8, 8))])
+@pytest.mark.parametrize("dims,n", [(2, (64, 32)), (3, (32, 16, 8)), (3, (8, 8, 8)),
+                                    (2, (256, 64)), (2, (32, 256)), (3, (256, 16, 8)), (3, (16, 256, 8)),
+                                    (3, (8, 16, 256)), (3, (256, 256, 64))])
 def test_periodic_solve_against_oracle(dims, n):
+    """Every pass kernel: the shared-memory tile FFTs and, along 256-node axes,
+    the register four-step FFTs (x pass and strided y / z passes)."""
     rng = np.random.default_rng(2)
     N = int(np.prod(n))
     L = [0.7 * (a + 1) for a in range(dims)]
@@ -157,18 +161,21 @@ def test_fp32_energy_conservation_2d():
     assert drift32 < max(2 * drift64, 1e-4), (drift32, drift64)
 
 
-def test_push_items_and_autotuner_leave_results_unchanged():
+@pytest.mark.parametrize("dims,cells,ppc,sort_interval,steps", [
+    (2, (64, 64), 16, 4, 9), (3, (16, 16, 16), 8, 4, 9), (3, (32, 32, 32), 8, 1000, 30)])
+def test_push_items_leave_results_unchanged(dims, cells, ppc, sort_interval, steps):
     """The FP32 push's particles-per-thread knob changes only speed: every
-    setting gives the same particles and fields; the autotuner returns one of
-    the candidates with its timing table."""
-    from apic import autotune
-    plan = W.plasma_plan(2, cells=(64, 64), ppc=16, seed=4)
+    setting (one particle per thread, the shared-memory box pushes at 2 and 4,
+    8 per thread) gives the same particles and fields, also when the particles
+    have drifted far from their sorted order (sorted once, 30 steps: many
+    gather and deposit outside their CTA's box)."""
+    plan = W.plasma_plan(dims, cells=cells, ppc=ppc, seed=4)
     ref = None
     for items in (1, 2, 4, 8):
-        sim = apic.SimulationND(plan.config(precision=apic.FP32, sort_interval=4, push_items=items))
+        sim = apic.SimulationND(plan.config(precision=apic.FP32, sort_interval=sort_interval, push_items=items))
         plan.load(sim)
         sim.initialize()
-        sim.step(9)
+        sim.step(steps)
         got = [sim.particles(k) for k in range(2)] + [sim.fields()]
         sim.close()
         if ref is None:
@@ -177,6 +184,12 @@ def test_push_items_and_autotuner_leave_results_unchanged():
             for a, b in zip(got, ref):
                 for x, y in zip(a, b):
                     assert np.array_equal(x, y), items
+
+
+def test_autotuner_returns_a_candidate():
+    """The autotuner returns one of the candidates with its timing table."""
+    from apic import autotune
+    plan = W.plasma_plan(2, cells=(64, 64), ppc=16, seed=4)
     out = autotune.tune_plasma(plan, apic.FP32, sort_intervals=(4, 8), push_items=(1, 4), steps=8)
     assert out["sort_interval"] in (4, 8) and out["push_items"] in (1, 4)
     assert len(out["table"]) == 4 and all(r["ms_per_step"] > 0 for r in out["table"])
