@@ -1003,24 +1003,46 @@ __global__ void k_cell_hist32(ParamsND p, SpeciesND S, int buf, unsigned* count)
     if (valid && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(count + key, (unsigned)__popc(peers));
 }
 
-template <int DIM>
-__global__ void k_cell_scatter32(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
+// Counting-sort placement of the FP32 form in two passes.  k_cell_rank32 gives
+// each particle its slot (lanes of a warp that share a cell take one atomic per
+// cell: the group's leader adds the group's size and the lanes take
+// consecutive slots in lane order) and records the particle's index there, in
+// the id array of the target buffer; k_cell_gather32 then fills every slot
+// from that index.  The stores of the second pass are coalesced, and the
+// scattered accesses are reads, served mostly from L2 (a particle moves a few
+// cells between sorts); a direct scatter instead writes a partial sector per
+// field for every particle that changed its row or plane.
+__global__ void k_cell_rank32(ParamsND p, SpeciesND S, int from, unsigned* cursor) {
     const unsigned i = blockIdx.x * kThreads + threadIdx.x;
     const bool valid = i < S.n;
-    const int to = from ^ 1;
-    const unsigned c = valid ? S.cell[from][i] : 0u;
-    const unsigned key = valid ? linear_cell(p, c) : 0xFFFFFFFFu;
+    const unsigned key = valid ? linear_cell(p, __ldcs(S.cell[from] + i)) : 0xFFFFFFFFu;
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
     unsigned base = 0;
     if (valid && lane == leader) base = atomicAdd(cursor + key, (unsigned)__popc(peers));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (!valid) return;
-    const unsigned o = base + (unsigned)__popc(peers & ((1u << lane) - 1u));
-    S.cell[to][o] = c;
-    for (int a = 0; a < DIM; ++a) S.off[to][a][o] = S.off[from][a][i];
-    for (int a = 0; a < 3; ++a) S.vel[to][a][o] = S.vel[from][a][i];
-    S.id[to][o] = S.id[from][i];
+    S.id[from ^ 1][base + (unsigned)__popc(peers & ((1u << lane) - 1u))] = i;
+}
+
+template <int DIM>
+__global__ void k_cell_gather32(SpeciesND S, int from) {
+    const unsigned d = blockIdx.x * kThreads + threadIdx.x;
+    if (d >= S.n) return;
+    const int to = from ^ 1;
+    const unsigned i = S.id[to][d];
+    const unsigned c = S.cell[from][i], id = S.id[from][i];
+    float off[3], vel[3];
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) off[a] = S.off[from][a][i];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vel[a] = S.vel[from][a][i];
+    __stcs(S.cell[to] + d, c);
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) __stcs(S.off[to][a] + d, off[a]);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) __stcs(S.vel[to][a] + d, vel[a]);
+    __stcs(S.id[to] + d, id);
 }
 
 // ---- particle sort by cell -------------------------------------------------------
@@ -1111,11 +1133,15 @@ __global__ void k_cell_scatter(ParamsND p, SpeciesND S, int from, unsigned* curs
     const unsigned i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= S.n) return;
     const int to = from ^ 1;
+    // loads first, stores after: the buffers may alias as far as the compiler
+    // knows, so loads placed after stores would each wait for the previous store
     const double pos[3] = {S.pos[from][0][i], S.pos[from][1][i], DIM == 3 ? S.pos[from][2][i] : 0.0};
+    const double vh[3] = {S.vh[from][0][i], S.vh[from][1][i], S.vh[from][2][i]};
+    const unsigned id = S.id[from][i];
     const unsigned o = atomicAdd(cursor + cell_of<DIM>(p, pos), 1u);
     for (int a = 0; a < DIM; ++a) S.pos[to][a][o] = pos[a];
-    for (int a = 0; a < 3; ++a) S.vh[to][a][o] = S.vh[from][a][i];
-    S.id[to][o] = S.id[from][i];
+    for (int a = 0; a < 3; ++a) S.vh[to][a][o] = vh[a];
+    S.id[to][o] = id;
 }
 
 // Device-side loading for large runs: uniform positions displaced by
@@ -2284,8 +2310,9 @@ struct SimND {
         k_scan_blocks<<<1, kThreads, 0, stream>>>(block_sums, nb);
         k_scan_add<<<nb, kThreads, 0, stream>>>(cell_offset, block_sums, (unsigned)ncells);
         if (fp32) {
-            if (cfg.dims == 2) k_cell_scatter32<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
-            else k_cell_scatter32<3><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+            k_cell_rank32<<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
+            if (cfg.dims == 2) k_cell_gather32<2><<<blocks, kThreads, 0, stream>>>(S, buf[s]);
+            else k_cell_gather32<3><<<blocks, kThreads, 0, stream>>>(S, buf[s]);
         } else if (cfg.dims == 2) {
             k_cell_scatter<2><<<blocks, kThreads, 0, stream>>>(p, S, buf[s], cell_offset);
         } else {
@@ -2586,7 +2613,7 @@ struct SimND {
             for (int s = 0; s < cfg.nspecies; ++s) {
                 if (since_sort[s] < species_interval[s]) continue;
                 since_sort[s] = 0;
-                if (sp[s].n) launches += 5;  // histogram, three scan passes, scatter
+                if (sp[s].n) launches += fp32 ? 6 : 5;  // histogram, three scan passes, scatter (FP32: rank + gather)
             }
             if (sort_mask) steps_since_sort = 0;
             for (int s = 0; s < cfg.nspecies; ++s)
