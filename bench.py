@@ -660,7 +660,7 @@ def bench_plasma(args, rank, dist):
     run_kernel = prec == apic.FP32 and items in (2, 4)  # consecutive particles per thread (k_push32_run)
     if prec == apic.FP32:
         captured = {2: 4194304, 3: 16777216}[dims]
-        name = f"k_push32_run_plasma{dims}d_fp32.md" if run_kernel and dims == 2 else f"k_push32_plasma{dims}d_fp32.md"
+        name = f"k_push32_run_plasma{dims}d_fp32.md" if run_kernel else f"k_push32_plasma{dims}d_fp32.md"
         t = _profiled_traffic(name)
         if t:
             traffic = t * (P / 2) / captured
@@ -924,8 +924,8 @@ def bench_swarm(args, rank, dist):
 # a few timed steps each and a shorter CPU sample, so the whole default run
 # stays within a few minutes.
 OTHER_CONFIGS = {
-    "plasma2d": {"sort_interval": 8, "push_items": 4, "e2e_steps": 2},
-    "plasma3d": {"sort_interval": 8, "push_items": 1, "e2e_steps": 1},
+    "plasma2d": {"sort_interval": 4, "push_items": 4, "e2e_steps": 2},
+    "plasma3d": {"sort_interval": 3, "push_items": 2, "e2e_steps": 1},
     "swarm": {"steps_per_launch": 100, "requests": 48, "mixed_requests": 16},
 }
 
