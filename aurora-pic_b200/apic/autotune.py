@@ -48,7 +48,7 @@ def _cache_put(path, key, value):
         json.dump(data, f, indent=1, sort_keys=True)
 
 
-def tune_plasma(plan, precision, sort_intervals=(3, 4, 6, 8, 16), push_items=(1, 2, 4, 8), steps=None, cache=None):
+def tune_plasma(plan, precision, sort_intervals=(2, 3, 4, 6, 8, 16), push_items=(1, 2, 4, 8), steps=None, cache=None):
     """Fastest (sort_interval, push_items) for a workloads.PlasmaPlan deck:
     each candidate runs one full sort period (at least `steps` steps) after a
     warm-up and is timed per step, sort included."""
