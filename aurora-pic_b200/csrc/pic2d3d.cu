@@ -1953,6 +1953,12 @@ __global__ void __launch_bounds__(kFftThreads) k_mixed_forward(const double* __r
                                                                int nx, int np, int periodic_y, const Cplx* tw);
 __global__ void k_mixed_tridiag(Cplx* __restrict__ hat, double* __restrict__ mu, int nd, int np, double inv_dsq,
                                 double inv_psq, double eps, double lower, double upper);
+__global__ void k_mixed_coeffs(double* __restrict__ mu, double* __restrict__ inv, int nd, int np, double inv_dsq,
+                               double inv_psq);
+constexpr int kMixedSweepMaxRows = 4000;  // k_mixed_sweep's shared memory bound: 48 B per interior row
+__global__ void __launch_bounds__(32) k_mixed_sweep(Cplx* __restrict__ hat, const double* __restrict__ mu,
+                                                    const double* __restrict__ inv, int nd, int np, double inv_dsq,
+                                                    double eps, double lower, double upper);
 __global__ void __launch_bounds__(kFftThreads) k_mixed_inverse(const Cplx* __restrict__ hat, double* __restrict__ phi,
                                                                int nx, int np, int periodic_y, const Cplx* tw);
 __global__ void k_mixed_efield(const double* __restrict__ phi, double* __restrict__ E, int nx, int ny, double dx,
@@ -2000,6 +2006,7 @@ void ensure_solver_attributes() {
     APIC_CUDA(cudaFuncSetAttribute(k_mixed_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
     APIC_CUDA(cudaFuncSetAttribute(k_mixed_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
     APIC_CUDA(cudaFuncSetAttribute(k_dst_lines, cudaFuncAttributeMaxDynamicSharedMemorySize, lines));
+    APIC_CUDA(cudaFuncSetAttribute(k_mixed_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, kMixedSweepMaxRows * 48));
     g_attr_done[dev] = true;
 }
 
@@ -2387,6 +2394,7 @@ struct SimND {
     int periodic_axis = 0;
     double* w_planes = nullptr;  // Ex | Ey (| Ez)
     double* w_mu = nullptr;
+    double* w_inv = nullptr;  // per-mode pivots' reciprocals (k_mixed_sweep)
     Cplx* w_hat = nullptr;
     Cplx* w_tw = nullptr;
     double* w_u = nullptr;
@@ -2435,6 +2443,16 @@ struct SimND {
             const size_t np = c.n[periodic_axis];
             w_mu = dalloc<double>(N);
             w_hat = dalloc<Cplx>(N);
+            {
+                const int nd = (int)c.n[periodic_axis ? 0 : 1];
+                const double hd = p.d[periodic_axis ? 0 : 1], hp = p.d[periodic_axis];
+                if (nd - 2 <= kMixedSweepMaxRows) {
+                    w_inv = dalloc<double>(N);
+                    k_mixed_coeffs<<<(unsigned)((np + 127) / 128), 128, 0, stream>>>(
+                        w_mu, w_inv, nd, (int)np, 1.0 / (hd * hd), 1.0 / (hp * hp));
+                    APIC_CUDA(cudaGetLastError());
+                }
+            }
             std::vector<Cplx> tw(np);
             for (size_t k = 0; k < np; ++k) tw[k] = {std::cos(twopi * k / np), -std::sin(twopi * k / np)};
             w_tw = dalloc<Cplx>(np);
@@ -2499,8 +2517,12 @@ struct SimND {
             const double lo = py ? pot[0] : pot[2], hi = py ? pot[1] : pot[3];
             const size_t smem = 3 * (size_t)np * sizeof(Cplx);
             k_mixed_forward<<<(unsigned)nd, kFftThreads, smem, stream>>>(solver.F.rho, w_hat, nx, np, py, w_tw);
-            k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, stream>>>(w_hat, w_mu, nd, np, 1.0 / (hd * hd),
-                                                                              1.0 / (hp * hp), p.eps, lo, hi);
+            if (w_inv)
+                k_mixed_sweep<<<(unsigned)np, 32, (size_t)(nd - 2) * 48, stream>>>(w_hat, w_mu, w_inv, nd, np,
+                                                                                    1.0 / (hd * hd), p.eps, lo, hi);
+            else
+                k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, stream>>>(w_hat, w_mu, nd, np, 1.0 / (hd * hd),
+                                                                                  1.0 / (hp * hp), p.eps, lo, hi);
             k_mixed_inverse<<<(unsigned)nd, kFftThreads, smem, stream>>>(w_hat, solver.F.phi, nx, np, py, w_tw);
             k_mixed_efield<<<g, 256, 0, stream>>>(solver.F.phi, w_planes, nx, ny, dx, dy, py ? 0 : 1, py);
         } else {
@@ -2848,6 +2870,81 @@ __global__ void k_mixed_tridiag(Cplx* __restrict__ hat, double* __restrict__ mu,
     }
 }
 
+// The elimination coefficients of every mode's system depend on the mode
+// only: modified_upper mu[m * ni + k] and the reciprocal of the pivot
+// inv[m * ni + k], computed once per mesh with the arithmetic of the sweep above.
+__global__ void k_mixed_coeffs(double* __restrict__ mu, double* __restrict__ inv, int nd, int np, double inv_dsq,
+                               double inv_psq) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= np) return;
+    const int ni = nd - 2;
+    const double angle = 3.141592653589793 * (double)m / (double)np;
+    const double eig = 4.0 * sin(angle) * sin(angle) * inv_psq;
+    const double diag = 2.0 * inv_dsq + eig;
+    const double off = -inv_dsq;
+    double pu = 0.0;
+    for (int k = 0; k < ni; ++k) {
+        const double den = k == 0 ? diag : diag - off * pu;
+        const double u = k == 0 ? off / diag : (k + 1 == ni ? 0.0 : off / den);
+        mu[(size_t)m * ni + k] = u;
+        inv[(size_t)m * ni + k] = 1.0 / den;
+        pu = u;
+    }
+}
+
+// One mode's forward elimination and back substitution per CTA, on its column
+// staged in shared memory: with the coefficients precomputed, each row is two
+// multiply-adds on the chain, and the column's rows are loaded all at once
+// instead of one dependent global round trip per row.
+__global__ void __launch_bounds__(32) k_mixed_sweep(Cplx* __restrict__ hat, const double* __restrict__ mu,
+                                                    const double* __restrict__ inv, int nd, int np, double inv_dsq,
+                                                    double eps, double lower, double upper) {
+    extern __shared__ __align__(16) unsigned char ssm[];
+    const int m = blockIdx.x, ni = nd - 2, tid = threadIdx.x;
+    Cplx* R = reinterpret_cast<Cplx*>(ssm);
+    Cplx* X = R + ni;
+    double* U = reinterpret_cast<double*>(X + ni);
+    double* V = U + ni;
+    for (int k = tid; k < ni; k += 32) {
+        R[k] = hat[(size_t)(k + 1) * np + m];
+        U[k] = mu[(size_t)m * ni + k];
+        V[k] = inv[(size_t)m * ni + k];
+    }
+    __syncthreads();
+    const double off = -inv_dsq, ieps = 1.0 / eps;
+    const double scale = (double)np;
+    const double lb = m == 0 ? lower * scale : 0.0, ub = m == 0 ? upper * scale : 0.0;
+    if (tid == 0) {
+        double pr = 0.0, pi = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < ni; ++k) {
+            const Cplx rh = R[k];
+            double rr = rh.re * ieps, ri = rh.im * ieps;
+            if (k == 0) rr += inv_dsq * lb;
+            if (k + 1 == ni) rr += inv_dsq * ub;
+            const double xr = (k == 0 ? rr : rr - off * pr) * V[k];
+            const double xi = (k == 0 ? ri : ri - off * pi) * V[k];
+            X[k] = {xr, xi};
+            pr = xr;
+            pi = xi;
+        }
+        Cplx xn = X[ni - 1];
+#pragma unroll 4
+        for (int k = ni - 2; k >= 0; --k) {
+            const Cplx c = X[k];
+            const double u = U[k];
+            xn = {c.re - u * xn.re, c.im - u * xn.im};
+            X[k] = xn;
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < ni; k += 32) hat[(size_t)(k + 1) * np + m] = X[k];
+    if (tid == 0) {
+        hat[m] = {lb, 0.0};
+        hat[(size_t)(nd - 1) * np + m] = {ub, 0.0};
+    }
+}
+
 __global__ void __launch_bounds__(kFftThreads) k_mixed_inverse(const Cplx* __restrict__ hat, double* __restrict__ phi,
                                                                int nx, int np, int periodic_y, const Cplx* tw) {
     extern __shared__ __align__(16) unsigned char msm[];
@@ -2941,8 +3038,16 @@ static void solve_mixed_2d(const size_t* n, const double* length, int periodic_a
     const size_t smem = 3 * np * sizeof(Cplx);
     ensure_solver_attributes();
     k_mixed_forward<<<(unsigned)nd, kFftThreads, smem, S.s>>>(d_rho, d_hat, (int)nx, (int)np, periodic_y, d_tw);
-    k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, S.s>>>(d_hat, d_mu, (int)nd, (int)np, 1.0 / (hd * hd),
-                                                                     1.0 / (hp * hp), permittivity, lower, upper);
+    if (nd - 2 <= (size_t)kMixedSweepMaxRows) {
+        double* d_inv = S.get<double>(N);
+        k_mixed_coeffs<<<(unsigned)((np + 127) / 128), 128, 0, S.s>>>(d_mu, d_inv, (int)nd, (int)np, 1.0 / (hd * hd),
+                                                                        1.0 / (hp * hp));
+        k_mixed_sweep<<<(unsigned)np, 32, (nd - 2) * 48, S.s>>>(d_hat, d_mu, d_inv, (int)nd, (int)np, 1.0 / (hd * hd),
+                                                                 permittivity, lower, upper);
+    } else {
+        k_mixed_tridiag<<<(unsigned)((np + 127) / 128), 128, 0, S.s>>>(d_hat, d_mu, (int)nd, (int)np, 1.0 / (hd * hd),
+                                                                         1.0 / (hp * hp), permittivity, lower, upper);
+    }
     k_mixed_inverse<<<(unsigned)nd, kFftThreads, smem, S.s>>>(d_hat, d_phi, (int)nx, (int)np, periodic_y, d_tw);
     k_mixed_efield<<<(unsigned)std::min<size_t>((N + 255) / 256, 4096), 256, 0, S.s>>>(
         d_phi, d_E, (int)nx, (int)ny, dx, dy, periodic_y ? 0 : 1, periodic_y);
