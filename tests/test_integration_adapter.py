@@ -1,4 +1,5 @@
-"""The reference-side adapter shown in INTEGRATION.md compiles against the
+"""The reference-side adapter of the integration guide (its C++ code block)
+compiles against the
 reference's own public headers and this library's C ABI, so a drift of either
 side's field names breaks this test rather than a maintainer's build.  The
 reference tree's location comes from oracle/Makefile (APIC_REFERENCE or its
