@@ -774,7 +774,14 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
     }
     if (nb > 0) {
         int idx[kPostItems];
-        if (nb <= (unsigned)kPostThreads) {
+        // up to one product per thread: rank tid in item 0 (the blocked scans
+        // below then still visit the products in rank order); more: the radix
+        // sort's blocked layout, ranks tid * kPostItems + k
+        const bool one_each = nb <= (unsigned)kPostThreads;
+        auto rank_of = [&](int k) -> unsigned {
+            return one_each ? (k == 0 ? (unsigned)tid : nb) : (unsigned)(tid * kPostItems + k);
+        };
+        if (one_each) {
             // a few products (the usual case): each finds its rank by counting
             // the smaller keys, one key per thread
             __shared__ unsigned long long s_keys[kPostThreads];
@@ -793,7 +800,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
             __syncthreads();
 #pragma unroll
             for (int k = 0; k < kPostItems; ++k) {
-                const unsigned rank = tid * kPostItems + k;
+                const unsigned rank = rank_of(k);
                 idx[k] = rank < nb ? s_order[rank] : 0;
             }
         } else {
@@ -814,7 +821,7 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         for (int k = 0; k < kPostItems; ++k) {
             keep[k] = false;
             bs[k] = -1;
-            const unsigned rank = tid * kPostItems + k;
+            const unsigned rank = rank_of(k);
             if (rank >= nb) continue;
             const BirthRec r = p.births[idx[k]];
             const SpeciesDev& S = p.sp[r.species];
