@@ -648,6 +648,46 @@ struct AffineCompose {
     }
 };
 
+// Inclusive scan of the affine maps map(i), i < count, over a block of
+// kPostThreads threads: out(i, F_i(0)) with F_i = f_i o ... o f_0.  Rounds of
+// one map per thread; each round is a warp shuffle scan, one warp scanning the
+// warps' totals (with the earlier rounds' composition in front) and two
+// barriers.  s_wt holds kPostThreads / 32 + 1 maps.
+template <class MapF, class OutF>
+__device__ __forceinline__ void block_affine_scan(int count, MapF map, OutF out, Affine* s_wt) {
+    constexpr int NW = kPostThreads / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const AffineCompose compose;
+    Affine carry{1.0, 0.0};
+    for (int base = 0; base < count; base += kPostThreads) {
+        const int i = base + tid;
+        Affine x = i < count ? map(i) : Affine{1.0, 0.0};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Affine y{__shfl_up_sync(0xffffffffu, x.a, o), __shfl_up_sync(0xffffffffu, x.b, o)};
+            if (lane >= o) x = compose(y, x);
+        }
+        if (lane == 31) s_wt[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            Affine w = lane < NW ? s_wt[lane] : Affine{1.0, 0.0};
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const Affine y{__shfl_up_sync(0xffffffffu, w.a, o), __shfl_up_sync(0xffffffffu, w.b, o)};
+                if (lane >= o) w = compose(y, w);
+            }
+            Affine ex{__shfl_up_sync(0xffffffffu, w.a, 1), __shfl_up_sync(0xffffffffu, w.b, 1)};
+            if (lane == 0) ex = Affine{1.0, 0.0};
+            if (lane < NW) s_wt[lane] = compose(carry, ex);
+            if (lane == NW - 1) s_wt[NW] = compose(carry, w);
+        }
+        __syncthreads();
+        if (i < count) out(i, compose(s_wt[warp], x).b);
+        carry = s_wt[NW];
+        __syncthreads();
+    }
+}
+
 __device__ __forceinline__ double electrode(double offset, const apic_voltage_drive& d, double t) {
     // electrode_potential, src/Simulation.cpp:678-685
     return offset + d.amplitude * sin(2.0 * 3.141592653589793 * d.frequency * t + d.phase);
@@ -665,11 +705,9 @@ template <int VDIM, bool DIRICHLET, bool F32, bool C32 = false>
 __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned post) {
     using Sort = cub::BlockRadixSort<unsigned long long, kPostThreads, kPostItems, int>;
     using ScanU = cub::BlockScan<unsigned, kPostThreads>;
-    using ScanA = cub::BlockScan<Affine, kPostThreads>;
     __shared__ union {
         typename Sort::TempStorage sort;
         typename ScanU::TempStorage scan;
-        typename ScanA::TempStorage scana;
     } tmp;
     __shared__ unsigned s_surv[kMaxSpecies], s_kept[kMaxSpecies], s_bstart[kMaxSpecies], s_nch[kMaxSpecies];
     __shared__ double s_red[kPostThreads / 32];
@@ -989,49 +1027,24 @@ __global__ void __launch_bounds__(kPostThreads) k_post1d(Params1D p, unsigned po
         const double phir = electrode(p.phi_right, p.drive_right, field_time);
         const int m = nx - 2;
         const double dx2 = p.dx * p.dx;
-        constexpr int IPT = kMaxNx1D / kPostThreads;
-        Affine f[IPT];
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int i = tid * IPT + k;
-            if (i < m) {
+        __shared__ Affine s_wt[kPostThreads / 32 + 1];
+        double* s_dp = reinterpret_cast<double*>(s_rhoi);  // the fixed-point density is converted already
+        // forward sweep: dp_i = r_i (d_i + dp_{i-1})
+        block_affine_scan(
+            m,
+            [&](int i) {
                 double d = s_rho[i + 1] * dx2 / p.eps;
                 if (i == 0) d += phil;
                 if (i == m - 1) d += phir;
                 const double r = s_c0[i];
-                f[k] = Affine{r, r * d};
-            } else {
-                f[k] = Affine{1.0, 0.0};
-            }
-        }
-        ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
-        __syncthreads();
-        double* s_dp = s_rho;  // dp replaces rho (rho already written out)
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int i = tid * IPT + k;
-            if (i < m) s_dp[i] = f[k].b;
-        }
-        __syncthreads();
+                return Affine{r, r * d};
+            },
+            [&](int i, double v) { s_dp[i] = v; }, s_wt);
         // back substitution in reverse: z_t = a[m-1-t] z_{t-1} + dp[m-1-t]
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int t = tid * IPT + k;
-            if (t < m) {
-                const int ii = m - 1 - t;
-                f[k] = Affine{s_c1[ii], s_dp[ii]};
-            } else {
-                f[k] = Affine{1.0, 0.0};
-            }
-        }
-        ScanA(tmp.scana).InclusiveScan(f, f, AffineCompose());
-        __syncthreads();
         double* s_phi = s_c0;  // coefficients no longer needed
-#pragma unroll
-        for (int k = 0; k < IPT; ++k) {
-            const int t = tid * IPT + k;
-            if (t < m) s_phi[m - t] = f[k].b;
-        }
+        block_affine_scan(
+            m, [&](int t) { return Affine{s_c1[m - 1 - t], s_dp[m - 1 - t]}; },
+            [&](int t, double v) { s_phi[m - t] = v; }, s_wt);
         if (tid == 0) {
             s_phi[0] = phil;
             s_phi[nx - 1] = phir;
