@@ -755,8 +755,29 @@ __global__ void __launch_bounds__(kThreads) k_push32_step(ParamsND p, SpeciesND 
 // positions).  A run that ends inside the thread is committed with one 64-bit
 // atomic per node; each lane's last run joins a warp-segmented sum over the
 // lanes holding the same cell, whose last lane commits it.
+// 2D: the CTA's deposit into a box of nodes in shared memory (kDBoxX cells
+// along x from x0 and the cell rows y0 .. y0 + 2 around the CTA's middle
+// particle), flushed with one 64-bit global atomic per touched node: a
+// particle that left its sorted neighbours then adds into shared memory
+// instead of committing its own global atomics (which, on the few nodes a CTA
+// touches, serialise in L2).  Each node's weight sum is kept as two 32-bit
+// halves (native shared atomics; the low half adds at most 2^16 per commit and
+// the high half 2^14, so neither overflows for the CTA's particles) and
+// reassembled exactly.  Commits outside the box go to global memory as before.
+// (In 3D the box around a CTA's 64 cells needs 1552 nodes; zeroing and
+// flushing them and the kernel's extra registers cost more than the atomics
+// saved, so 3D commits straight to global memory.)
+constexpr int kDBoxX = 48;
+constexpr int kDBoxNodes = (kDBoxX + 1) * 4;
+struct DepositBox {
+    unsigned* lo;
+    unsigned* hi;
+    int x0, y0;
+};
+
 template <int DIM, bool BORIS, int ITEMS, bool PROF>
-__global__ void __launch_bounds__(kThreads) k_push32_run(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
+__device__ __forceinline__ void push_run(const ParamsND& p, const SpeciesND& S, int buf, unsigned long long* acc,
+                                         const DepositBox& box) {
     constexpr int NN = DIM == 2 ? 4 : 8;  // nodes of a cell
     const unsigned first = (blockIdx.x * kThreads + threadIdx.x) * ITEMS;
     const int lane = threadIdx.x & 31;
@@ -839,6 +860,20 @@ __global__ void __launch_bounds__(kThreads) k_push32_run(ParamsND p, SpeciesND S
     auto commit = [&](unsigned c, const unsigned* w) {
         int ix, iy, iz;
         unpack_cell(c, ix, iy, iz);
+        if (DIM == 2) {
+            const int bx = (ix - box.x0) & (nx - 1), by = (iy - box.y0) & (ny - 1);
+            if (bx < kDBoxX && by < 3) {
+                const int b = by * (kDBoxX + 1) + bx;
+#pragma unroll
+                for (int j = 0; j < NN; ++j) {
+                    if (!w[j]) continue;
+                    const int q = b + (j & 1) + ((j >> 1) & 1) * (kDBoxX + 1);
+                    atomicAdd(box.lo + q, w[j] & 0xFFFFu);
+                    atomicAdd(box.hi + q, w[j] >> 16);
+                }
+                return;
+            }
+        }
         const int ix1 = (ix + 1) & (nx - 1), iy1 = (iy + 1) & (ny - 1);
         const int iz1 = DIM == 3 ? (iz + 1) & (nz - 1) : 0;
 #pragma unroll
@@ -975,6 +1010,35 @@ __global__ void __launch_bounds__(kThreads) k_push32_run(ParamsND p, SpeciesND S
         racc[j] = q;
     }
     if (tail && key != kNoCell) commit(key, racc);
+}
+
+template <int DIM, bool BORIS, int ITEMS, bool PROF>
+__global__ void __launch_bounds__(kThreads) k_push32_run(ParamsND p, SpeciesND S, int buf, unsigned long long* acc) {
+    if constexpr (DIM == 2) {
+        __shared__ unsigned s_lo[kDBoxNodes], s_hi[kDBoxNodes];
+        __shared__ int s_anchor[2];
+        const int nx = p.n[0], ny = p.n[1];
+        if (threadIdx.x == 0) {  // the box around the CTA's middle particle, before the push
+            const unsigned mid = min(blockIdx.x * kThreads * ITEMS + (unsigned)(kThreads * ITEMS / 2), S.n - 1u);
+            int ix, iy, iz;
+            unpack_cell(S.cell[buf][mid], ix, iy, iz);
+            s_anchor[0] = (ix - kDBoxX / 2) & (nx - 1);
+            s_anchor[1] = (iy - 1) & (ny - 1);
+        }
+        for (int q = threadIdx.x; q < kDBoxNodes; q += kThreads) { s_lo[q] = 0u; s_hi[q] = 0u; }
+        __syncthreads();
+        const DepositBox box{s_lo, s_hi, s_anchor[0], s_anchor[1]};
+        push_run<DIM, BORIS, ITEMS, PROF>(p, S, buf, acc, box);
+        __syncthreads();
+        for (int q = threadIdx.x; q < kDBoxNodes; q += kThreads) {
+            const unsigned long long v = ((unsigned long long)s_hi[q] << 16) + s_lo[q];
+            if (!v) continue;
+            const int qx = q % (kDBoxX + 1), qy = q / (kDBoxX + 1);
+            atomicAdd(acc + (size_t)((box.y0 + qy) & (ny - 1)) * nx + ((box.x0 + qx) & (nx - 1)), v);
+        }
+    } else {
+        push_run<DIM, BORIS, ITEMS, PROF>(p, S, buf, acc, DepositBox{nullptr, nullptr, 0, 0});
+    }
 }
 
 // FP64 staging <-> FP32 state.  The cell/offset split follows the periodic CIC

@@ -924,7 +924,7 @@ def bench_swarm(args, rank, dist):
 # a few timed steps each and a shorter CPU sample, so the whole default run
 # stays within a few minutes.
 OTHER_CONFIGS = {
-    "plasma2d": {"sort_interval": 4, "push_items": 4, "e2e_steps": 2},
+    "plasma2d": {"sort_interval": 8, "push_items": 4, "e2e_steps": 2},
     "plasma3d": {"sort_interval": 3, "push_items": 2, "e2e_steps": 1},
     "swarm": {"steps_per_launch": 100, "requests": 48, "mixed_requests": 16},
 }
