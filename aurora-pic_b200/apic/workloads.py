@@ -141,13 +141,17 @@ def _rate_bound(mass, channels, e_max_ev, neutral_density, neutral_mass, tempera
     return float(np.max(neutral_density * tot * (v + spread)))
 
 
-def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096, te_ev=1.0) -> Workload1D:
+def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096, te_ev=1.0,
+               vdim=3) -> Workload1D:
     """1D3V capacitive RF discharge with null-collision MCC: Dirichlet gap
     0.067 m, `cells` cells, grounded left electrode, right electrode driven at
     450 V / 13.56 MHz, dt = 1 / (400 f); electrons and He+ (4 amu) at
     particles_per_cell per cell each, Maxwellian Te = 1 eV, Ti = 0.026 eV;
     neutral helium 9.64e20 m^-3 at 300 K (thermal neutrals).  max_frequency is
-    1.25 x the thermal-neutral rate bound over each table's energy range."""
+    1.25 x the thermal-neutral rate bound over each table's energy range.
+    vdim = 1 gives the 1D1V form of the same discharge: one velocity component
+    and the 1V collision interface, which has no ionization channel (the
+    electrons keep elastic scattering and excitation)."""
     f_rf = 13.56e6
     L = 0.067
     nx = cells + 1
@@ -163,7 +167,7 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
         ChannelSpec(ELASTIC, Ee * E_CHARGE, 6e-20 / np.sqrt(1 + Ee / 10.0)),
         ChannelSpec(EXCITATION, Ee * E_CHARGE, hump(Ee, 19.8, 60.0, 1.5e-21), 19.8 * E_CHARGE),
         ChannelSpec(IONIZATION, Ee * E_CHARGE, hump(Ee, 24.6, 120.0, 3.5e-21), 24.6 * E_CHARGE, 0, 1),
-    ]
+    ][: 3 if vdim == 3 else 2]
     i_ch = [
         ChannelSpec(ELASTIC, Ei * E_CHARGE, np.full_like(Ei, 2e-19)),
         ChannelSpec(CHARGE_EXCHANGE, Ei * E_CHARGE, np.full_like(Ei, 5e-19)),
@@ -178,13 +182,16 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
     for q, m, vt in ((-E_CHARGE, M_E, ve), (E_CHARGE, m_he, vi)):
         x = rng.uniform(0.0, L, n)
         v3 = vt * rng.standard_normal((3, n))
-        sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), v3[1].copy(), v3[2].copy(), thermal=vt))
+        if vdim == 3:
+            sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), v3[1].copy(), v3[2].copy(), thermal=vt))
+        else:
+            sp.append(SpeciesSpec(q, m, w, cap, x, v3[0].copy(), thermal=vt))
     models = [
         ModelSpec(0, e_ch, ng, nu_e, m_he, T),
         ModelSpec(1, i_ch, ng, nu_i, m_he, T),
     ]
-    return Workload1D("ccp_helium_1d3v", True, 3, True, nx, L, 1.0 / (400 * f_rf), sp, models,
-                      drive_right=(450.0, f_rf, 0.0), steps=steps)
+    return Workload1D("ccp_helium_1d3v" if vdim == 3 else "ccp_helium_1d1v", True, vdim, True, nx, L,
+                      1.0 / (400 * f_rf), sp, models, drive_right=(450.0, f_rf, 0.0), steps=steps)
 
 
 def to_device_config(wl: Workload1D, precision=0, seed=1):

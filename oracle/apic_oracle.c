@@ -391,6 +391,88 @@ int ora_collide3(const ora_collider* c, double v[3], double dt, ora_rng* r, ora_
     return 0;
 }
 
+/* sample_neutral_velocity (scalar), src/Collision.cpp:687-700 (a fresh normal
+ * distribution object per call, bounded at 8 sigma) */
+static int neutral_1v(const ora_collider* c, ora_rng* r, double* out) {
+    *out = 0.0;
+    if (c->neutral_stddev == 0.0) return 0;
+    ora_normal nd = {0, 0.0};
+    const double limit = kThermalSigma * c->neutral_stddev;
+    for (int attempt = 0; attempt < 1024; ++attempt) {
+        const double value = ora_normal_draw(&nd, r, 0.0, c->neutral_stddev);
+        if (fabs(value) <= limit) { *out = value; return 0; }
+    }
+    return seterr(6, "thermal-neutral scalar sampler exceeded its rejection limit");
+}
+
+/* apply_channel (1V), src/Collision.cpp:717-760: the scattered speed along a
+ * random sign (uniform_int_distribution<int>(0, 1)) */
+static void apply_channel1(const ora_collider* c, int idx, double* v, double vn, ora_rng* r) {
+    const ora_channel* ch = &c->m.ch[idx];
+    if (ch->process == ORA_ATTACHMENT) { *v = 0.0; return; }
+    if (ch->process == ORA_CHARGE_EXCHANGE) { *v = vn; return; }
+    const double rel = *v - vn;
+    double energy = 0.5 * c->particle_mass * rel * rel;
+    if (ch->process == ORA_EXCITATION || ch->process == ORA_IONIZATION) {
+        const double e2 = energy - ch->threshold_energy;
+        energy = 0.0 < e2 ? e2 : 0.0; /* std::max(0.0, e2) */
+    }
+    if (ch->process == ORA_IONIZATION) energy *= 0.5;
+    const double speed = sqrt(2.0 * energy / c->particle_mass);
+    const double scattered = ora_bit(r) == 0 ? -speed : speed;
+    if (ch->process == ORA_ELASTIC && c->m.neutral_mass > 0.0) {
+        const double total = c->particle_mass + c->m.neutral_mass;
+        *v = (c->particle_mass * *v + c->m.neutral_mass * vn) / total + (c->m.neutral_mass / total) * scattered;
+    } else {
+        *v = vn + scattered;
+    }
+}
+
+/* NullCollisionModel::collide(double&), src/Collision.cpp:831-905 */
+int ora_collide1(const ora_collider* c, double* v, double dt, ora_rng* r, ora_collide_stats* st) {
+    memset(st, 0, sizeof *st);
+    const uint64_t start = r->index;
+    for (int ch = 0; ch < c->m.nch; ++ch)
+        if (c->m.ch[ch].process == ORA_IONIZATION || c->m.ch[ch].angular != ORA_ISOTROPIC)
+            return seterr(10, "ionization and anisotropic MCC require the 3V collision interface");
+    if (!isfinite(dt) || !(dt > 0.0)) return seterr(11, "MCC timestep must be positive and finite");
+    double elapsed = 0.0;
+    int rc;
+    for (;;) {
+        if ((rc = validate_bound(c, fabs(*v)))) return rc;
+        const double waiting = -log(open_unit(r)) / c->m.max_frequency;
+        if (!isfinite(waiting) || waiting >= dt - elapsed) break;
+        elapsed += waiting;
+        ++st->candidates;
+        if (st->candidates > c->m.max_candidates)
+            return seterr(2, "MCC candidate limit exceeded");
+        double vn;
+        if ((rc = neutral_1v(c, r, &vn))) return rc;
+        double rates[ORA_MAX_CHANNELS];
+        if ((rc = rates_for_speed(c, fabs(*v - vn), rates))) return rc;
+        const double selection = ora_canonical(r) * c->m.max_frequency;
+        double cumulative = 0.0;
+        int accepted = 0;
+        for (int ch = 0; ch < c->m.nch; ++ch) {
+            cumulative += rates[ch];
+            if (selection < cumulative) {
+                const double before = 0.5 * c->particle_mass * *v * *v;
+                apply_channel1(c, ch, v, vn, r);
+                st->energy_change[ch] += 0.5 * c->particle_mass * *v * *v - before;
+                ++st->channel_collisions[ch];
+                if (c->m.ch[ch].process == ORA_ATTACHMENT) st->removed = 1;
+                accepted = 1;
+                break;
+            }
+        }
+        if (!accepted) ++st->null_collisions;
+        if (st->removed) break;
+    }
+    st->draws = r->index - start;
+    if (r->overrun) return seterr(5, "recorded draw array overrun");
+    return 0;
+}
+
 /* ======================================================================= */
 /* 1D grid kernels. */
 
@@ -970,7 +1052,7 @@ static int apply_collisions(ora_sim1d* s) {
                 rc = ora_collide3(&s->col[m], v, c->dt, &r, &cs);
                 st->v[i] = v[0]; st->vy[i] = v[1]; st->vz[i] = v[2];
             } else {
-                return seterr(7, "1V MCC is not part of this restatement");
+                rc = ora_collide1(&s->col[m], &st->v[i], c->dt, &r, &cs);
             }
             if (rc) return rc;
             s->candidates += cs.candidates;

@@ -51,6 +51,9 @@ typedef struct {
  * 3 thermal bound above max_frequency, 4 invalid input, 5 draw array overrun */
 int ora_collider_init(ora_collider* c, const ora_mcc_model* m, double particle_mass);
 int ora_collide3(const ora_collider* c, double v[3], double dt, ora_rng* r, ora_collide_stats* st);
+/* NullCollisionModel::collide(double&) (1V): elastic, excitation, charge
+ * exchange and attachment with isotropic (random-sign) scattering */
+int ora_collide1(const ora_collider* c, double* v, double dt, ora_rng* r, ora_collide_stats* st);
 
 /* ---- 1D grid kernels ---------------------------------------------------- */
 double ora_gather1d(const double* E, size_t nx, double length, double dx, int dirichlet, double x);

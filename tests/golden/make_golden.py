@@ -420,6 +420,13 @@ def townsend_fixture():
     np.savez_compressed(os.path.join(HERE, "swarm_townsend.npz"), **out)
 
 
+def mcc1v_fixture():
+    """The 1D1V discharge with the 1V collision interface (elastic and
+    excitation electrons, elastic and charge-exchange ions), shared engine."""
+    hot = W.ccp_helium(particles_per_cell=32, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0, vdim=1)
+    sim_fixture("mcc1v", hot, 400, with_rng=True)
+
+
 def main(names=None):
     if names:
         for n in names:
@@ -448,6 +455,7 @@ def main(names=None):
     sim_fixture("rf", rf, 30)
     hot = W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0)
     sim_fixture("mcc", hot, 30, with_rng=True)
+    mcc1v_fixture()
     print("golden vectors written to", HERE)
 
 

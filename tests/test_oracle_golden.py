@@ -145,6 +145,20 @@ def test_mcc_run_bit_exact():
     assert ref_per[2] > 0  # ionization happened
 
 
+def test_mcc_1v_run_bit_exact():
+    """The 1D1V discharge through NullCollisionModel::collide(double&)
+    (src/Collision.cpp:831-905): scalar thermal neutrals, random-sign
+    scattering, elastic recoil, excitation and charge exchange; shared
+    mt19937_64 stream, 400 steps, bit-exact."""
+    hot = W.ccp_helium(particles_per_cell=32, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0, vdim=1)
+    sim, f = _run_sim("mcc1v", hot)
+    c, nl, per = sim.collisions()
+    assert c == int(f["candidates"]) and nl == int(f["nulls"])
+    ref_per = f["per_channel"]
+    assert list(per[0][:2]) + list(per[1][:2]) == [int(v) for v in ref_per]
+    assert min(int(v) for v in ref_per) > 0  # every channel fired
+
+
 ND_CASES = {
     "sim2d_boris": (2, (16, 8), (0.0, 0.0, 0.7)),
     "sim2d_leapfrog": (2, (8, 8), (0.0, 0.0, 0.0)),
