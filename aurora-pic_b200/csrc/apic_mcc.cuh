@@ -392,4 +392,88 @@ __device__ inline void collide3(const MccModelDev& m, double v[3], double dt, S&
     if (s.overrun()) r.error |= kErrReplay;
 }
 
+// NullCollisionModel::collide(double&) (1V), src/Collision.cpp:831-905, with
+// the scalar sample_neutral_velocity (:687-700) and the 1V apply_channel
+// (:717-760): the scattered speed takes a random sign, the top bit of one
+// draw (uniform_int_distribution<int>(0, 1) on a 64-bit engine).  The model
+// has no ionization and only isotropic channels (checked at create).  Same
+// first-iteration convention as collide3.
+template <class S>
+__device__ inline void collide1(const MccModelDev& m, double& v, double dt, S& s, CollideResult& r,
+                                bool have_first = false, double first_wait = 0.0) {
+    if (!isfinite(v)) { r.error |= kErrNonFinite; return; }
+    double elapsed = 0.0;
+    for (;;) {
+        double waiting;
+        if (have_first) {
+            waiting = first_wait;
+            have_first = false;
+        } else {
+            if (!frequency_bound_ok(m, fabs(v))) { r.error |= kErrMajorant; return; }
+            double u = uniform01(s);
+            for (int guard = 0; !(u > 0.0) && guard < 64 && !s.overrun(); ++guard) u = uniform01(s);
+            if (s.overrun()) { r.error |= kErrReplay; return; }
+            waiting = -log(u) / m.max_frequency;
+        }
+        if (!isfinite(waiting) || waiting >= dt - elapsed) break;
+        elapsed += waiting;
+        ++r.candidates;
+        if (r.candidates > m.max_candidates) { r.error |= kErrCandidates; return; }
+        double vn = 0.0;
+        if (m.neutral_stddev != 0.0) {
+            NormalState ns;
+            const double limit = kThermalSigma * m.neutral_stddev;
+            int attempt = 0;
+            for (; attempt < 1024; ++attempt) {
+                vn = normal(ns, s, 0.0, m.neutral_stddev);
+                if (fabs(vn) <= limit) break;
+            }
+            if (attempt == 1024) { r.error |= kErrMajorant; return; }
+        }
+        double rates[kMaxChannels];
+        if (!rates_for_speed(m, fabs(v - vn), rates)) {
+            r.error |= kErrMajorant;
+            return;
+        }
+        const double selection = canonical(s) * m.max_frequency;
+        double cumulative = 0.0;
+        bool accepted = false;
+        for (int ci = 0; ci < m.nch; ++ci) {
+            cumulative += rates[ci];
+            if (selection < cumulative) {
+                const MccChannelDev& c = m.ch[ci];
+                const double before = 0.5 * m.particle_mass * v * v;
+                if (c.process == kAttachment) {
+                    v = 0.0;
+                } else if (c.process == kChargeExchange) {
+                    v = vn;
+                } else {
+                    const double rel = v - vn;
+                    double energy = 0.5 * m.particle_mass * rel * rel;
+                    if (c.process == kExcitation) {
+                        const double e2 = energy - c.threshold;
+                        energy = 0.0 < e2 ? e2 : 0.0;  // std::max(0.0, e2)
+                    }
+                    const double speed = sqrt(2.0 * energy / m.particle_mass);
+                    const double scattered = (s.next() >> 63) == 0ull ? -speed : speed;
+                    if (c.process == kElastic && m.neutral_mass > 0.0) {
+                        const double total = m.particle_mass + m.neutral_mass;
+                        v = (m.particle_mass * v + m.neutral_mass * vn) / total + (m.neutral_mass / total) * scattered;
+                    } else {
+                        v = vn + scattered;
+                    }
+                }
+                r.energy_change[ci] += 0.5 * m.particle_mass * v * v - before;
+                ++r.channel[ci];
+                if (c.process == kAttachment) r.removed = true;
+                accepted = true;
+                break;
+            }
+        }
+        if (!accepted) ++r.nulls;
+        if (r.removed) break;
+    }
+    if (s.overrun()) r.error |= kErrReplay;
+}
+
 }  // namespace apic

@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
         const unsigned n = st->n[s];
         const unsigned nr = st->nranges[s];
         const unsigned base = tile * kTile;
-        const bool mcc = (mode & kModeSyncMcc) && S.model >= 0 && VDIM == 3;
+        const bool mcc = (mode & kModeSyncMcc) && S.model >= 0;
         // one search per warp for the range of its first particle
         const unsigned wfirst = base + (unsigned)(tid & ~31);
         unsigned r0 = 0;
@@ -440,7 +440,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                         atomicOr(&st->error, kErrNonFinite);
                         continue;
                     }
-                    if (!(s2 <= M.v_safe2) && !frequency_bound_ok(M, sqrt(s2))) atomicOr(&st->error, kErrMajorant);
+                    // validate_frequency_bound at |v| (1V: src/Collision.cpp:856) or at speed(v)
+                    if (!(s2 <= M.v_safe2) && !frequency_bound_ok(M, VDIM == 3 ? sqrt(s2) : fabs(vc[k])))
+                        atomicOr(&st->error, kErrMajorant);
                     PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
                     const uint64_t d0 = rng.next();
                     // the raw-draw threshold decides exactly as -log(u)/nu < dt would
@@ -483,7 +485,8 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 const unsigned slot = ce.slot;
                 const double px = ce.x;
                 double vel[3] = {ce.v[0], ce.v[1], ce.v[2]};
-                collide3(M, vel, p.dt, rng, r,
+                if (VDIM == 1) collide1(M, vel[0], p.dt, rng, r, true, ce.first_wait);
+                else collide3(M, vel, p.dt, rng, r,
                          [&](int ch, const double* vs, const double* vi) {
                              const unsigned bslot = atomicAdd(&st->nbirths, 2u);
                              const MccChannelDev& C = M.ch[ch];
@@ -1742,8 +1745,14 @@ struct Sim1D {
             const apic_mcc_model& m = c.models[mi];
             require(m.species >= 0 && m.species < c.nspecies, "MCC species does not exist");
             require(p.sp[m.species].model < 0, "one MCC model per species is supported", APIC_ERR_UNSUPPORTED);
-            require(c.velocity_dimensions == 3, "1D MCC on the device requires velocity_dimensions = 3",
-                    APIC_ERR_UNSUPPORTED);
+            require(c.velocity_dimensions == 3 || !c32,
+                    "the FP32 cell form's collisions need velocity_dimensions = 3", APIC_ERR_UNSUPPORTED);
+            if (c.velocity_dimensions == 1) {
+                // NullCollisionModel::collide(double&), src/Collision.cpp:835-846
+                for (int ci = 0; ci < m.nch && ci < kMaxChannels; ++ci)
+                    require(m.ch[ci].process != APIC_IONIZATION && m.ch[ci].angular == APIC_ISOTROPIC,
+                            "ionization and anisotropic MCC require the 3V collision interface");
+            }
             for (int ci = 0; ci < m.nch && ci < kMaxChannels; ++ci) {
                 const apic_mcc_channel& ch = m.ch[ci];
                 require(ch.process != APIC_ATTACHMENT, "1D MCC does not support attachment");

@@ -194,6 +194,53 @@ def test_ccp_mcc_parity_philox():
         _compare_species(dev, ora, s, tol=1e-11)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_storage"])
+def test_ccp_mcc_1v_parity_philox(precision):
+    """The 1D1V discharge through the 1V collision interface
+    (NullCollisionModel::collide(double&), src/Collision.cpp:831-905): the
+    oracle in device layout with the same Philox streams agrees on every
+    collision decision; the FP32 storage form against oracle mode 2."""
+    wl = W.ccp_helium(particles_per_cell=64, cells=64, seed=5, steps=10, table_rows=256, te_ev=12.0, vdim=1)
+    seed = 0x5EED
+    prec = apic.FP64 if precision == "fp64" else apic.FP32_STORAGE
+    cfg, tabs = W.to_device_config(wl, precision=prec, seed=seed)
+    dev = apic.Simulation1D(cfg, tabs)
+    load_device(dev, wl)
+    dev.initialize()
+    T = po.TableSet()
+    ora = po.Sim1D(oracle_config(wl, T), 1 if prec == apic.FP64 else 2, seed)
+    load_oracle(ora, wl)
+    ora.initialize()
+    dev.step(40)
+    ora.step(40)
+    tot = dev.collision_totals()
+    c, nl, per = ora.collisions()
+    assert tot.candidates == c and tot.null_collisions == nl and c > 100
+    for m in range(2):
+        assert list(tot.channel_collisions[m])[:2] == list(per[m])[:2]
+    assert min(int(per[0][0]), int(per[0][1]), int(per[1][0]) + int(per[1][1])) > 0
+    for s in range(2):
+        _compare_species(dev, ora, s, tol=1e-11 if prec == apic.FP64 else 1e-6)
+    dev.close()
+
+
+def test_1v_mcc_rejections():
+    """The 1V interface takes no ionization or anisotropic channel (the
+    reference's logic_error), and the FP32 cell form's collisions are 3V."""
+    wl = W.ccp_helium(particles_per_cell=4, cells=16, seed=5, steps=10, table_rows=64, te_ev=12.0, vdim=1)
+    wl3 = W.ccp_helium(particles_per_cell=4, cells=16, seed=5, steps=10, table_rows=64, te_ev=12.0)
+    wl.models[0].channels.append(wl3.models[0].channels[2])  # ionization
+    cfg, tabs = W.to_device_config(wl, seed=1)
+    with pytest.raises(apic.ApicError) as e:
+        apic.Simulation1D(cfg, tabs)
+    assert "require the 3V collision interface" in str(e.value)
+    wl.models[0].channels.pop()
+    cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=1)
+    with pytest.raises(apic.ApicError) as e:
+        apic.Simulation1D(cfg, tabs)
+    assert "velocity_dimensions = 3" in str(e.value)
+
+
 def test_step_group_matches_individual_steps():
     """Runs stepped together (overlapping streams, two steps per graph launch)
     end in exactly the state of the same runs stepped one by one."""
