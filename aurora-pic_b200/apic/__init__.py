@@ -74,6 +74,7 @@ class Config1D(C.Structure):
         ("drive_left", VoltageDrive), ("drive_right", VoltageDrive), ("precision", C.c_int),
         ("seed", C.c_uint64), ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
         ("nmodels", C.c_int), ("models", MccModel * MAX_MODELS),
+        ("bgk_enabled", C.c_int), ("bgk_frequency", C.c_double), ("bgk_neutral_velocity", C.c_double),
     ]
 
 
@@ -271,7 +272,9 @@ def mcc_model(species, channels, neutral_density, max_frequency, neutral_mass=0.
 
 def config1d(*, boundary, velocity_dimensions, units, nx, length, dt, species, models=(), phi_left=0.0,
              phi_right=0.0, drive_left=(0.0, 0.0, 0.0), drive_right=(0.0, 0.0, 0.0), precision=FP64, seed=1,
-             relative_permittivity=1.0) -> Config1D:
+             relative_permittivity=1.0, bgk=None) -> Config1D:
+    """bgk = (frequency, neutral_temperature_velocity) enables the legacy BGK
+    collision model (CollisionConfig with model = bgk)."""
     c = Config1D()
     c.boundary, c.velocity_dimensions, c.units = boundary, velocity_dimensions, units
     c.relative_permittivity = relative_permittivity
@@ -286,6 +289,8 @@ def config1d(*, boundary, velocity_dimensions, units, nx, length, dt, species, m
     c.nmodels = len(models)
     for i, mm in enumerate(models):
         c.models[i] = mm
+    if bgk is not None:
+        c.bgk_enabled, c.bgk_frequency, c.bgk_neutral_velocity = 1, bgk[0], bgk[1]
     return c
 
 

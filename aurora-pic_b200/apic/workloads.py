@@ -90,6 +90,7 @@ class Workload1D:
     drive_left: tuple = (0.0, 0.0, 0.0)
     drive_right: tuple = (0.0, 0.0, 0.0)
     steps: int = 100
+    bgk: tuple = None  # (frequency, neutral_temperature_velocity): the legacy BGK model
 
     @property
     def particles(self) -> int:
@@ -142,7 +143,7 @@ def _rate_bound(mass, channels, e_max_ev, neutral_density, neutral_mass, tempera
 
 
 def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows=4096, te_ev=1.0,
-               vdim=3) -> Workload1D:
+               vdim=3, bgk=None) -> Workload1D:
     """1D3V capacitive RF discharge with null-collision MCC: Dirichlet gap
     0.067 m, `cells` cells, grounded left electrode, right electrode driven at
     450 V / 13.56 MHz, dt = 1 / (400 f); electrons and He+ (4 amu) at
@@ -151,7 +152,9 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
     1.25 x the thermal-neutral rate bound over each table's energy range.
     vdim = 1 gives the 1D1V form of the same discharge: one velocity component
     and the 1V collision interface, which has no ionization channel (the
-    electrons keep elastic scattering and excitation)."""
+    electrons keep elastic scattering and excitation).  bgk = (frequency,
+    neutral_temperature_velocity) replaces the MCC models by the legacy BGK
+    model, which relaxes every species to that neutral Maxwellian."""
     f_rf = 13.56e6
     L = 0.067
     nx = cells + 1
@@ -190,8 +193,11 @@ def ccp_helium(particles_per_cell=512, cells=512, seed=7, steps=4000, table_rows
         ModelSpec(0, e_ch, ng, nu_e, m_he, T),
         ModelSpec(1, i_ch, ng, nu_i, m_he, T),
     ]
-    return Workload1D("ccp_helium_1d3v" if vdim == 3 else "ccp_helium_1d1v", True, vdim, True, nx, L,
-                      1.0 / (400 * f_rf), sp, models, drive_right=(450.0, f_rf, 0.0), steps=steps)
+    name = "ccp_helium_1d3v" if vdim == 3 else "ccp_helium_1d1v"
+    if bgk is not None:
+        models, name = [], name + "_bgk"
+    return Workload1D(name, True, vdim, True, nx, L, 1.0 / (400 * f_rf), sp, models,
+                      drive_right=(450.0, f_rf, 0.0), steps=steps, bgk=bgk)
 
 
 def to_device_config(wl: Workload1D, precision=0, seed=1):
@@ -207,7 +213,7 @@ def to_device_config(wl: Workload1D, precision=0, seed=1):
                    units=SI if wl.si else NORMALIZED, nx=wl.nx, length=wl.length, dt=wl.dt,
                    species=[(s.charge, s.mass, s.weight, s.capacity) for s in wl.species], models=models,
                    phi_left=wl.phi_left, phi_right=wl.phi_right, drive_left=wl.drive_left,
-                   drive_right=wl.drive_right, precision=precision, seed=seed)
+                   drive_right=wl.drive_right, precision=precision, seed=seed, bgk=wl.bgk)
     return cfg, tabs
 
 

@@ -156,6 +156,8 @@ struct Params1D {
     apic_voltage_drive drive_left, drive_right;
     SpeciesDev sp[kMaxSpecies];
     MccModelDev model[kMaxModels];
+    int bgk;                   // legacy BGK model active
+    double bgk_prob, bgk_vt;   // 1 - exp(-frequency dt), neutral_temperature_velocity
     double* E;
     double* rho;
     double* phi;
@@ -432,6 +434,31 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 vc[k] = vh[k] + S.hqm * E * p.dt;
                 // electric-work ledger, src/Simulation.cpp:1109-1114
                 if (DIAG && p.ledger) wsum += 0.5 * S.mass * S.weight * (vc[k] * vc[k] - vo[k] * vo[k]);
+                if (p.bgk) {
+                    // the legacy BGK branch, src/Simulation.cpp:772-834: relax to a
+                    // neutral Maxwellian with probability 1 - exp(-nu dt), drawn from
+                    // the particle's stream (the one its MCC would use; the two
+                    // models exclude each other)
+                    PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
+                    if (uniform01(rng) < p.bgk_prob) {
+                        const double hmw = 0.5 * S.mass * S.weight;
+                        const double before =
+                            hmw * (vc[k] * vc[k] + (VDIM == 3 ? vy[k] * vy[k] + vz[k] * vz[k] : 0.0));
+                        NormalState ns;
+                        vc[k] = normal(ns, rng, 0.0, p.bgk_vt);
+                        if (VDIM == 3) {
+                            vy[k] = normal(ns, rng, 0.0, p.bgk_vt);
+                            vz[k] = normal(ns, rng, 0.0, p.bgk_vt);
+                        }
+                        const double change =
+                            hmw * (vc[k] * vc[k] + (VDIM == 3 ? vy[k] * vy[k] + vz[k] * vz[k] : 0.0)) - before;
+                        atomicAdd(&st->candidates, 1ull);
+                        atomicAdd(&st->chan[0][0], 1ull);
+                        atomicAdd(&st->chan_energy[0][0], change);
+                        if (DIAG && p.coll_acc) collision_energy_deposit<DIRICHLET>(p, x[k], 0, change);
+                        queued[k] = -2;  // re-initialise the half step in phase C
+                    }
+                }
                 if (mcc) {
                     const MccModelDev& M = p.model[S.model];
                     // first iteration of NullCollisionModel::collide, src/Collision.cpp:926-933
@@ -546,6 +573,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                     vc[k] = ce.v[0]; vy[k] = ce.v[1]; vz[k] = ce.v[2];
                 }
                 // initialize_leapfrog_half_step after the collision, src/Simulation.cpp:924-926
+                vh[k] = vc[k] - S.hqm * E * p.dt;
+            } else if (queued[k] == -2) {
+                // the BGK particle's initialize_leapfrog_half_step, src/Simulation.cpp:829-833
                 vh[k] = vc[k] - S.hqm * E * p.dt;
             }
             if (mode & kModeKickDrift) {
@@ -1487,6 +1517,7 @@ struct Sim1D {
             p.coll_off[m] = sa.nch;
             sa.nch += cfg.models[m].nch;
         }
+        if (cfg.bgk_enabled) sa.nch = 1;  // the "bgk" channel, src/Simulation.cpp:484-485
         const size_t nx = cfg.nx;
         sa.tot = dalloc<double>(sa_block());
         sa.phase = dalloc<double>(sa.P * sa_block());
@@ -1640,6 +1671,15 @@ struct Sim1D {
         c32 = c.precision == APIC_FP32;
         const double rel = c.relative_permittivity == 0.0 ? 1.0 : c.relative_permittivity;
         require(std::isfinite(rel) && rel > 0, "relative_permittivity must be positive and finite");
+        // the collision checks of validate() and the Simulation constructor,
+        // src/Simulation.cpp:95-100, :388-392
+        require(std::isfinite(c.bgk_frequency) && c.bgk_frequency >= 0.0,
+                "collision frequency must be non-negative and finite");
+        require(std::isfinite(c.bgk_neutral_velocity) && c.bgk_neutral_velocity >= 0.0,
+                "neutral_temperature_velocity must be non-negative and finite");
+        require(!c.bgk_enabled || c.nmodels == 0,
+                "named collision models cannot be combined with the legacy collision model");
+        require(!c.bgk_enabled || !c32, "the FP32 cell form does not take the legacy BGK model", APIC_ERR_UNSUPPORTED);
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
             throw Error(APIC_ERR_NO_DEVICE, "no CUDA device is visible");
@@ -1666,6 +1706,11 @@ struct Sim1D {
         p.phi_right = c.phi_right;
         p.drive_left = c.drive_left;
         p.drive_right = c.drive_right;
+        // the legacy BGK branch runs when enabled with a positive frequency,
+        // src/Simulation.cpp:772-776 (the probability on the host, as there)
+        p.bgk = c.bgk_enabled && c.bgk_frequency > 0.0 ? 1 : 0;
+        p.bgk_prob = 1.0 - std::exp(-c.bgk_frequency * c.dt);
+        p.bgk_vt = c.bgk_neutral_velocity;
 
         // fixed-point scale: worst-case |rho| bound below 2^62
         double bound = 0.0;
@@ -2353,6 +2398,17 @@ struct Sim1D {
         return st_h;
     }
 
+    // the diagnostics channels in the reference's numbering, as (model,
+    // channel) slots of the device totals: every model's channels in model
+    // order, or the legacy BGK model's one "bgk" channel
+    std::vector<std::pair<int, int>> channel_slots() const {
+        std::vector<std::pair<int, int>> out;
+        if (cfg.bgk_enabled) out.emplace_back(0, 0);
+        for (int m = 0; m < cfg.nmodels; ++m)
+            for (int ch = 0; ch < cfg.models[m].nch; ++ch) out.emplace_back(m, ch);
+        return out;
+    }
+
     // Simulation::load_checkpoint, src/Simulation.cpp:2018-2899, for the parts
     // the device holds (see apic_sim1d_load_checkpoint).
     void load_checkpoint(const Apc& c) {
@@ -2361,9 +2417,8 @@ struct Sim1D {
                 "checkpoint unit system does not match 1D config");
         require(c.velocity_dimensions == cfg.velocity_dimensions,
                 "checkpoint velocity dimensions do not match 1D config");
-        size_t nch = 0;
-        for (int m = 0; m < cfg.nmodels; ++m) nch += (size_t)cfg.models[m].nch;
-        require(c.channel_counts.size() == nch, "checkpoint collision diagnostics do not match 1D config");
+        const auto slots = channel_slots();
+        require(c.channel_counts.size() == slots.size(), "checkpoint collision diagnostics do not match 1D config");
         require(c.losses.size() == (size_t)cfg.nspecies,
                 "checkpoint boundary-loss species count does not match 1D config");
         require(c.electric_work.size() == (size_t)cfg.nspecies,
@@ -2381,12 +2436,10 @@ struct Sim1D {
         DevState h = read_state();
         h.candidates = c.candidates;
         h.nulls = c.null_collisions;
-        size_t k = 0;
-        for (int m = 0; m < cfg.nmodels; ++m)
-            for (int ch = 0; ch < cfg.models[m].nch; ++ch, ++k) {
-                h.chan[m][ch] = c.channel_counts[k];
-                h.chan_energy[m][ch] = c.channel_energy[k];
-            }
+        for (size_t k = 0; k < slots.size(); ++k) {
+            h.chan[slots[k].first][slots[k].second] = c.channel_counts[k];
+            h.chan_energy[slots[k].first][slots[k].second] = c.channel_energy[k];
+        }
         for (int s = 0; s < cfg.nspecies; ++s) {
             h.lost[s][0] = c.losses[s].left;
             h.lost[s][1] = c.losses[s].right;
@@ -2411,9 +2464,8 @@ struct Sim1D {
         require(!meta.spatial_average_enabled && meta.spatial_average_nx == cfg.nx &&
                     meta.species.size() == (size_t)cfg.nspecies,
                 "checkpoint metadata does not match 1D config");
-        size_t nch = 0;
-        for (int m = 0; m < cfg.nmodels; ++m) nch += (size_t)cfg.models[m].nch;
-        require(meta.channel_counts.size() == nch, "checkpoint collision diagnostics do not match 1D config");
+        const auto slots = channel_slots();
+        require(meta.channel_counts.size() == slots.size(), "checkpoint collision diagnostics do not match 1D config");
         Apc c = meta;
         const double rel = cfg.relative_permittivity == 0.0 ? 1.0 : cfg.relative_permittivity;
         c.units = cfg.units;
@@ -2424,12 +2476,10 @@ struct Sim1D {
         const DevState h = read_state();
         c.candidates = h.candidates;
         c.null_collisions = h.nulls;
-        size_t k = 0;
-        for (int m = 0; m < cfg.nmodels; ++m)
-            for (int ch = 0; ch < cfg.models[m].nch; ++ch, ++k) {
-                c.channel_counts[k] = h.chan[m][ch];
-                c.channel_energy[k] = h.chan_energy[m][ch];
-            }
+        for (size_t k = 0; k < slots.size(); ++k) {
+            c.channel_counts[k] = h.chan[slots[k].first][slots[k].second];
+            c.channel_energy[k] = h.chan_energy[slots[k].first][slots[k].second];
+        }
         c.losses.resize(cfg.nspecies);
         c.electric_work.resize(cfg.nspecies);
         for (int s = 0; s < cfg.nspecies; ++s) {

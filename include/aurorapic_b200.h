@@ -135,6 +135,16 @@ typedef struct {
     apic_species species[APIC_MAX_SPECIES];
     int nmodels;
     apic_mcc_model models[APIC_MAX_MODELS];
+    /* The legacy BGK model (CollisionConfig with model = bgk,
+     * src/Simulation.cpp:481-485, :771-834): each step every live particle of
+     * every species is replaced, with probability 1 - exp(-frequency dt), by a
+     * Maxwellian neutral of standard deviation bgk_neutral_velocity per
+     * component, then its half-step velocity is re-initialised.  Its one
+     * "bgk" channel is totals entry [0][0].  Excludes MCC models (nmodels = 0);
+     * FP64 and FP32 storage forms. */
+    int bgk_enabled;
+    double bgk_frequency;
+    double bgk_neutral_velocity;    /* neutral_temperature_velocity */
 } apic_config1d;
 
 /* DiagnosticSample, include/pic/Diagnostics.hpp (Simulation::sample,

@@ -625,6 +625,7 @@ struct ora_sim1d {
     ora_collider col[ORA_MAX_MODELS];
     ora_mt64 mt;
     uint64_t candidates, nulls, per_channel[ORA_MAX_MODELS][ORA_MAX_CHANNELS];
+    double bgk_energy;           /* channel_energy_change of the "bgk" channel */
     ora_product* staged;
     size_t nstaged, staged_cap;
     double electric_work[ORA_MAX_SPECIES]; /* species_power_transfer_, src/Simulation.cpp:1094-1132 */
@@ -680,6 +681,23 @@ ora_sim1d* ora_sim1d_create(const ora_config1d* cfg, int mode, uint64_t philox_s
     s->phi = calloc(cfg->nx, sizeof(double));
     s->E = calloc(cfg->nx, sizeof(double));
     ora_mt64_seed(&s->mt, cfg->seed);
+    /* the collision checks of validate() and the Simulation constructor,
+     * src/Simulation.cpp:95-100, :388-392 */
+    if (!isfinite(cfg->bgk_frequency) || cfg->bgk_frequency < 0.0) {
+        seterr(4, "collision frequency must be non-negative and finite");
+        ora_sim1d_destroy(s);
+        return NULL;
+    }
+    if (!isfinite(cfg->bgk_neutral_velocity) || cfg->bgk_neutral_velocity < 0.0) {
+        seterr(4, "neutral_temperature_velocity must be non-negative and finite");
+        ora_sim1d_destroy(s);
+        return NULL;
+    }
+    if (cfg->bgk && cfg->nmodels > 0) {
+        seterr(4, "named collision models cannot be combined with the legacy collision model");
+        ora_sim1d_destroy(s);
+        return NULL;
+    }
     for (int m = 0; m < cfg->nmodels; ++m) {
         const ora_mcc_model* mm = &cfg->models[m];
         if (ora_collider_init(&s->col[m], mm, cfg->species[mm->species].mass)) {
@@ -800,6 +818,7 @@ int ora_sim1d_enable_spatial_average(ora_sim1d* s, const ora_spatial_average1d* 
         s->diag.off[m] = s->diag.nch;
         s->diag.nch += s->cfg.models[m].nch;
     }
+    if (s->cfg.bgk) s->diag.nch = 1; /* the "bgk" channel */
     const size_t P = s->diag.P, nch = (size_t)s->diag.nch;
     s->diag.tot = calloc(diag_block(s), sizeof(double));
     s->diag.phase = calloc(P * diag_block(s) + 1, sizeof(double));
@@ -1026,10 +1045,57 @@ int ora_sim1d_phase_eedf(const ora_sim1d* s, int phase, int region, uint64_t* co
 /* initialize_leapfrog_half_step, src/Pusher.cpp:66-68 */
 static double init_half(double v, double E, double qm, double dt) { return v - 0.5 * qm * E * dt; }
 
+/* The legacy BGK branch of apply_collisions, src/Simulation.cpp:772-834:
+ * every live particle of every species relaxes to a fresh neutral Maxwellian
+ * with probability 1 - exp(-frequency dt), then re-initialises its half-step
+ * velocity.  Mode 0 draws from the shared engine with one normal_distribution
+ * (and its saved value) per species; modes 1-2 draw from the particle's
+ * (seed, slot, step, species) Philox stream with its own normal state. */
+static void apply_bgk(ora_sim1d* s) {
+    const ora_config1d* c = &s->cfg;
+    const double probability = 1.0 - exp(-c->bgk_frequency * c->dt);
+    const double vt = c->bgk_neutral_velocity;
+    for (int sid = 0; sid < c->nspecies; ++sid) {
+        ora_store* st = &s->sp[sid];
+        const double qm = c->species[sid].charge / c->species[sid].mass;
+        ora_normal shared_normal = {0, 0.0};
+        for (size_t i = 0; i < st->n; ++i) {
+            if (!st->alive[i]) continue;
+            ora_rng r;
+            ora_normal own = {0, 0.0};
+            ora_normal* ns = &own;
+            memset(&r, 0, sizeof r);
+            if (s->mode == 0) { r.kind = ORA_SRC_MT64; r.mt = &s->mt; ns = &shared_normal; }
+            else {
+                r.kind = ORA_SRC_PHILOX;
+                r.key[0] = (uint32_t)s->philox_seed; r.key[1] = (uint32_t)(s->philox_seed >> 32);
+                r.ctr[0] = (uint32_t)i; r.ctr[1] = (uint32_t)s->step; r.ctr[2] = (uint32_t)sid;
+            }
+            if (ora_uniform01(&r) >= probability) continue;
+            const double before = 0.5 * c->species[sid].mass * c->species[sid].weight *
+                (st->v[i] * st->v[i] + (c->vdim == 3 ? st->vy[i] * st->vy[i] + st->vz[i] * st->vz[i] : 0.0));
+            st->v[i] = ora_normal_draw(ns, &r, 0.0, vt);
+            if (c->vdim == 3) {
+                st->vy[i] = ora_normal_draw(ns, &r, 0.0, vt);
+                st->vz[i] = ora_normal_draw(ns, &r, 0.0, vt);
+            }
+            ++s->candidates;
+            ++s->per_channel[0][0];
+            const double after = 0.5 * c->species[sid].mass * c->species[sid].weight *
+                (st->v[i] * st->v[i] + (c->vdim == 3 ? st->vy[i] * st->vy[i] + st->vz[i] * st->vz[i] : 0.0));
+            const double change = after - before;
+            s->bgk_energy += change;
+            if (s->diag.coll_active) diag_collision_energy(s, st->x[i], 0, change);
+            st->vh[i] = init_half(st->v[i], gather(s, st->x[i]), qm, c->dt);
+        }
+    }
+}
+
 /* apply_collisions (named null-collision models), src/Simulation.cpp:835-1006 */
 static int apply_collisions(ora_sim1d* s) {
     const ora_config1d* c = &s->cfg;
     s->nstaged = 0;
+    if (c->bgk && c->bgk_frequency > 0.0) apply_bgk(s);
     for (int m = 0; m < c->nmodels; ++m) {
         const int sid = c->models[m].species;
         ora_store* st = &s->sp[sid];
@@ -1218,6 +1284,8 @@ void ora_sim1d_set_mt(ora_sim1d* s, const uint64_t* state313) {
     for (int i = 0; i < 312; ++i) s->mt.mt[i] = state313[i];
     s->mt.mti = (int)state313[312];
 }
+
+double ora_sim1d_bgk_energy(const ora_sim1d* s) { return s->bgk_energy; }
 
 void ora_sim1d_collisions(const ora_sim1d* s, uint64_t* candidates, uint64_t* nulls, uint64_t* per_channel) {
     *candidates = s->candidates;

@@ -87,6 +87,8 @@ void ora_sim1d_fields(const ora_sim1d* s, double* rho, double* phi, double* E);
 double ora_sim1d_time(const ora_sim1d* s);
 /* engine state in std::mersenne_twister_engine's text order: 312 words, index */
 void ora_sim1d_set_mt(ora_sim1d* s, const uint64_t* state313);
+/* channel_energy_change of the legacy BGK model's "bgk" channel */
+double ora_sim1d_bgk_energy(const ora_sim1d* s);
 void ora_sim1d_collisions(const ora_sim1d* s, uint64_t* candidates, uint64_t* nulls,
                           uint64_t* per_channel /* [nmodels][ORA_MAX_CHANNELS] */);
 void ora_sim1d_losses(const ora_sim1d* s, int species, uint64_t* left, uint64_t* right,

@@ -68,6 +68,11 @@ typedef struct {
     ora_species species[ORA_MAX_SPECIES];
     int nmodels;
     ora_mcc_model models[ORA_MAX_MODELS];
+    /* the legacy BGK model (CollisionConfig with model = bgk; one "bgk"
+     * channel), src/Simulation.cpp:481-485, :771-834 */
+    int bgk;
+    double bgk_frequency;
+    double bgk_neutral_velocity; /* neutral_temperature_velocity */
 } ora_config1d;
 
 /* SpatialAverage1DConfig + PhaseEedf1DConfig, include/pic/Config.hpp:145-168

@@ -69,6 +69,7 @@ class Config1D(C.Structure):
         ("seed", C.c_uint), ("threads", C.c_int), ("max_particles", C.c_size_t),
         ("nspecies", C.c_int), ("species", SpeciesCfg * MAX_SPECIES),
         ("nmodels", C.c_int), ("models", MccModel * MAX_MODELS),
+        ("bgk", C.c_int), ("bgk_frequency", C.c_double), ("bgk_neutral_velocity", C.c_double),
     ]
 
 
@@ -196,6 +197,8 @@ def oracle() -> C.CDLL:
         L.ora_sim1d_time.argtypes = [C.c_void_p]
         L.ora_sim1d_set_mt.argtypes = [C.c_void_p, _U64P]
         L.ora_sim1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P]
+        L.ora_sim1d_bgk_energy.restype = C.c_double
+        L.ora_sim1d_bgk_energy.argtypes = [C.c_void_p]
         L.ora_sim1d_losses.argtypes = [C.c_void_p, C.c_int, _U64P, _U64P, _DP, _DP]
         L.ora_sim1d_kinetic.restype = C.c_double
         L.ora_sim1d_kinetic.argtypes = [C.c_void_p, C.c_int]
@@ -236,6 +239,7 @@ def ref() -> C.CDLL:
         L.ref1d_get_fields.argtypes = [C.c_void_p, _DP, _DP, _DP]
         L.ref1d_sample.argtypes = [C.c_void_p, _DP, _DP, C.POINTER(C.c_size_t)]
         L.ref1d_collisions.argtypes = [C.c_void_p, _U64P, _U64P, _U64P, C.c_size_t]
+        L.ref1d_channel_energy.argtypes = [C.c_void_p, _DP, C.c_size_t]
         L.ref1d_losses.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), _DP, _DP]
         L.ref1d_rng_state.argtypes = [C.c_void_p, C.c_char_p, _U64P]
         L.ref1d_save_checkpoint.argtypes = [C.c_void_p, C.c_char_p]
@@ -302,7 +306,8 @@ def make_model(species, channels, neutral_density, max_frequency, neutral_mass=0
 
 def config1d(*, dirichlet, vdim, si, nx, length, dt, species, models=(), phi_left=0.0,
              phi_right=0.0, drive_left=(0, 0, 0), drive_right=(0, 0, 0), seed=12345, threads=0,
-             max_particles=0) -> Config1D:
+             max_particles=0, bgk=None) -> Config1D:
+    """bgk: (frequency, neutral_temperature_velocity) enables the legacy BGK model."""
     c = Config1D()
     c.dirichlet, c.vdim, c.si, c.nx, c.length, c.dt = dirichlet, vdim, si, nx, length, dt
     c.phi_left, c.phi_right = phi_left, phi_right
@@ -315,6 +320,8 @@ def config1d(*, dirichlet, vdim, si, nx, length, dt, species, models=(), phi_lef
     c.nmodels = len(models)
     for i, m in enumerate(models):
         c.models[i] = m
+    if bgk is not None:
+        c.bgk, c.bgk_frequency, c.bgk_neutral_velocity = 1, bgk[0], bgk[1]
     return c
 
 
@@ -381,6 +388,9 @@ class Sim1D:
         per = np.zeros(MAX_MODELS * MAX_CHANNELS, np.uint64)
         oracle().ora_sim1d_collisions(self.h, u64ptr(c), u64ptr(nl), u64ptr(per))
         return int(c[0]), int(nl[0]), per.reshape(MAX_MODELS, MAX_CHANNELS)
+
+    def bgk_energy(self):
+        return oracle().ora_sim1d_bgk_energy(self.h)
 
     def losses(self, s):
         a, b = np.zeros(1, np.uint64), np.zeros(1, np.uint64)
@@ -493,6 +503,11 @@ class Ref1D:
         k = ref().ref1d_collisions(self.h, u64ptr(c), u64ptr(nl), u64ptr(per), 64)
         return int(c[0]), int(nl[0]), per[:k]
 
+    def channel_energy(self):
+        out = np.zeros(64)
+        k = ref().ref1d_channel_energy(self.h, dptr(out), 64)
+        return out[:k]
+
     def losses(self, s):
         a, b = C.c_size_t(), C.c_size_t()
         ea, eb = np.zeros(1), np.zeros(1)
@@ -568,7 +583,7 @@ def config_from_workload(wl, tables: TableSet, seed=12345, threads=0, particles=
     return config1d(dirichlet=int(wl.dirichlet), vdim=wl.vdim, si=int(wl.si), nx=wl.nx, length=wl.length,
                     dt=wl.dt, species=species, models=models, phi_left=wl.phi_left, phi_right=wl.phi_right,
                     drive_left=wl.drive_left, drive_right=wl.drive_right, seed=seed, threads=threads,
-                    max_particles=max(s.capacity for s in wl.species))
+                    max_particles=max(s.capacity for s in wl.species), bgk=getattr(wl, "bgk", None))
 
 
 # ---------------------------------------------------------------------------

@@ -141,6 +141,12 @@ pic::Config make_config_1d(const ora_config1d& in, const std::string& dir) {
         }
         c.species.push_back(sc);
     }
+    if (in.bgk) {
+        c.collisions.enabled = true;
+        c.collisions.model = pic::CollisionModelKind::BGK;
+        c.collisions.frequency = in.bgk_frequency;
+        c.collisions.neutral_temperature_velocity = in.bgk_neutral_velocity;
+    }
     for (int m = 0; m < in.nmodels; ++m) {
         pic::NamedCollisionConfig named;
         named.name = "model" + std::to_string(m);
@@ -228,6 +234,13 @@ int ref1d_collisions(void* h, uint64_t* candidates, uint64_t* nulls, uint64_t* p
     for (size_t i = 0; i < d.channel_collisions.size() && i < cap; ++i)
         per_channel[i] = d.channel_collisions[i];
     return static_cast<int>(d.channel_collisions.size());
+}
+
+int ref1d_channel_energy(void* h, double* energy, size_t cap) {
+    const auto& d = static_cast<Ref1D*>(h)->sim->collision_diagnostics();
+    for (size_t i = 0; i < d.channel_energy_change.size() && i < cap; ++i)
+        energy[i] = d.channel_energy_change[i];
+    return static_cast<int>(d.channel_energy_change.size());
 }
 
 double ref1d_electric_work(void* h, int species) {

@@ -97,7 +97,7 @@ def collide_fixture():
     np.savez_compressed(os.path.join(HERE, "collide3.npz"), **out)
 
 
-def sim_fixture(name, wl, steps, with_rng=False):
+def sim_fixture(name, wl, steps, with_rng=False, with_energy=False):
     T = po.TableSet()
     cfg = po.config_from_workload(wl, T, seed=2024, own_loading=True)
     work = tempfile.mkdtemp()
@@ -121,6 +121,8 @@ def sim_fixture(name, wl, steps, with_rng=False):
     out.update(rho=rho, phi=phi, E=E, time=R.time())
     c, nl, per = R.collisions()
     out.update(candidates=c, nulls=nl, per_channel=per)
+    if with_energy:
+        out["channel_energy"] = R.channel_energy()
     np.savez_compressed(os.path.join(HERE, f"sim1d_{name}.npz"), **out)
 
 
@@ -427,6 +429,18 @@ def mcc1v_fixture():
     sim_fixture("mcc1v", hot, 400, with_rng=True)
 
 
+BGK = (2.0e8, 3.0e5)  # frequency (1/s), neutral_temperature_velocity (m/s)
+
+
+def bgk_fixture():
+    """The RF discharge deck with the legacy BGK model instead of MCC, 1D3V and
+    1D1V (electrons and ions relax to one neutral Maxwellian), shared engine."""
+    for vdim in (3, 1):
+        wl = W.ccp_helium(particles_per_cell=32, cells=32, seed=6, steps=10, table_rows=96, te_ev=4.0,
+                          vdim=vdim, bgk=BGK)
+        sim_fixture(f"bgk{vdim}v", wl, 60, with_rng=True, with_energy=True)
+
+
 def main(names=None):
     if names:
         for n in names:
@@ -456,6 +470,7 @@ def main(names=None):
     hot = W.ccp_helium(particles_per_cell=8, cells=32, seed=5, steps=10, table_rows=96, te_ev=12.0)
     sim_fixture("mcc", hot, 30, with_rng=True)
     mcc1v_fixture()
+    bgk_fixture()
     print("golden vectors written to", HERE)
 
 

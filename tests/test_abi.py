@@ -125,3 +125,22 @@ def test_3d_wall_configuration_checks(walls, msg):
     with pytest.raises(apic.ApicError) as e:
         apic.SimulationND(cfg)
     assert msg in str(e.value)
+
+
+@pytest.mark.parametrize("bgk,models,msg", [
+    ((-1.0, 1.0), False, "collision frequency must be non-negative and finite"),
+    ((float("nan"), 1.0), False, "collision frequency must be non-negative and finite"),
+    ((1.0, -2.0), False, "neutral_temperature_velocity must be non-negative and finite"),
+    ((1.0e8, 1.0e5), True, "named collision models cannot be combined with the legacy collision model"),
+])
+def test_bgk_configuration_checks(bgk, models, msg):
+    """The legacy BGK model's checks (src/Simulation.cpp:95-100, :388-392) run
+    in create before it looks for a device."""
+    from apic import workloads as W
+    wl = W.ccp_helium(particles_per_cell=2, cells=8, seed=1, steps=1, table_rows=16, bgk=bgk)
+    if models:
+        wl.models = W.ccp_helium(particles_per_cell=2, cells=8, seed=1, steps=1, table_rows=16).models
+    cfg, tabs = W.to_device_config(wl)
+    with pytest.raises(apic.ApicError) as e:
+        apic.Simulation1D(cfg, tabs)
+    assert msg in str(e.value)

@@ -30,10 +30,12 @@ def _decks():
     rf = W.ccp_helium(particles_per_cell=8, cells=32, seed=12, table_rows=256)
     rf.models = []
     ts = W.two_stream(particles_per_beam=256, nx=32, seed=3)
-    return {"mcc": (mcc, 12), "rf": (rf, 30), "two_stream": (ts, 20)}
+    # the legacy BGK model (one "bgk" channel and its signature line)
+    bgk = W.ccp_helium(particles_per_cell=8, cells=32, seed=13, table_rows=64, te_ev=4.0, bgk=(2.0e8, 3.0e5))
+    return {"mcc": (mcc, 12), "rf": (rf, 30), "two_stream": (ts, 20), "bgk": (bgk, 25)}
 
 
-@pytest.mark.parametrize("case", ["mcc", "rf", "two_stream"])
+@pytest.mark.parametrize("case", ["mcc", "rf", "two_stream", "bgk"])
 def test_reference_checkpoint_round_trip_is_byte_identical(case, tmp_path):
     if not po.reference_available():
         pytest.skip("reference library not built on this host")
@@ -94,7 +96,7 @@ def _oracle_from_checkpoint(wl, c, seed, T):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["rf", "mcc"])
+@pytest.mark.parametrize("case", ["rf", "mcc", "bgk"])
 def test_device_restart_from_a_reference_checkpoint(case, tmp_path):
     """A device run restarted from a file the reference wrote matches the
     oracle restarted from the same file: FP64 state within 1e-11 after 10

@@ -224,6 +224,53 @@ def test_ccp_mcc_1v_parity_philox(precision):
     dev.close()
 
 
+BGK = (2.0e8, 3.0e5)  # frequency (1/s), neutral_temperature_velocity (m/s)
+
+
+@pytest.mark.parametrize("vdim,precision", [(3, "fp64"), (1, "fp64"), (3, "fp32_storage")])
+def test_bgk_parity_philox(vdim, precision):
+    """The legacy BGK branch (src/Simulation.cpp:772-834) on the RF discharge
+    deck: the oracle in device layout with the same Philox streams agrees on
+    every relaxation (counts exact), state within 1e-11 (FP64) or against
+    oracle mode 2 within 1e-6 (FP32 storage form); the channel's energy change
+    within 1e-9 (the device sums it with FP64 atomics in another order)."""
+    wl = W.ccp_helium(particles_per_cell=64, cells=64, seed=6, steps=10, table_rows=64, te_ev=4.0, vdim=vdim,
+                      bgk=BGK)
+    seed = 0xB6C
+    prec = apic.FP64 if precision == "fp64" else apic.FP32_STORAGE
+    cfg, tabs = W.to_device_config(wl, precision=prec, seed=seed)
+    dev = apic.Simulation1D(cfg, tabs)
+    load_device(dev, wl)
+    dev.initialize()
+    T = po.TableSet()
+    ora = po.Sim1D(oracle_config(wl, T), 1 if prec == apic.FP64 else 2, seed)
+    load_oracle(ora, wl)
+    ora.initialize()
+    dev.step(40)
+    ora.step(40)
+    tot = dev.collision_totals()
+    c, nl, per = ora.collisions()
+    assert tot.candidates == c == int(per[0][0]) == tot.channel_collisions[0][0] and c > 1000
+    assert tot.null_collisions == nl == 0
+    e, eo = tot.channel_energy_change[0][0], ora.bgk_energy()
+    assert abs(e - eo) <= 1e-9 * abs(eo) and eo != 0.0, (e, eo)
+    for s in range(2):
+        _compare_species(dev, ora, s, tol=1e-11 if prec == apic.FP64 else 1e-6)
+        b = dev.boundary_losses(s)
+        assert (b.absorbed_left, b.absorbed_right) == ora.losses(s)[:2]
+    dev.close()
+
+
+def test_bgk_rejections():
+    """BGK excludes named MCC models (the reference's message) and the FP32
+    cell form does not take it."""
+    wl = W.ccp_helium(particles_per_cell=4, cells=16, seed=5, steps=10, table_rows=64, bgk=BGK)
+    cfg, tabs = W.to_device_config(wl, precision=apic.FP32, seed=1)
+    with pytest.raises(apic.ApicError) as e:
+        apic.Simulation1D(cfg, tabs)
+    assert "legacy BGK" in str(e.value)
+
+
 def test_1v_mcc_rejections():
     """The 1V interface takes no ionization or anisotropic channel (the
     reference's logic_error), and the FP32 cell form's collisions are 3V."""

@@ -114,6 +114,23 @@ def test_rf_phase_bins_and_eedf_match_oracle_fp64():
     assert np.any(dev.spatial_sums(apic.SA_COLLISION_ENERGY, 2) != 0.0)  # ionization deposits
 
 
+def test_bgk_collision_energy_and_ledger_match_oracle_fp64():
+    """The legacy BGK model (src/Simulation.cpp:772-834) deposits each
+    relaxation's energy change in its one "bgk" channel; with the phase bins,
+    EEDF and the electric-work ledger over one 40-step RF cycle everything
+    agrees with the oracle as for MCC."""
+    wl = W.ccp_helium(particles_per_cell=16, cells=64, seed=11, steps=40, table_rows=64, te_ev=4.0,
+                      bgk=(2.0e8, 3.0e5))
+    wl.drive_right = (450.0, 10 * F, 0.0)
+    dev, _t1 = _device(wl, SHORT, ledger=True)
+    ora, _t2 = _oracle(wl, SHORT, 1)
+    dev.step(40)
+    ora.step(40)
+    _compare(dev, ora, SHORT, 2, 1, TOL)
+    _check_work(dev, ora, 2, TOL)
+    assert np.any(dev.spatial_sums(apic.SA_COLLISION_ENERGY, 0) != 0.0)
+
+
 def test_long_rf_cycle_fp64_and_unperturbed_trajectory():
     """The 13.56 MHz discharge over a whole cycle (400 steps, 100 samples):
     counts exact, sums within the long-run bound; and the diagnostics leave

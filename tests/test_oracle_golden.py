@@ -159,6 +159,41 @@ def test_mcc_1v_run_bit_exact():
     assert min(int(v) for v in ref_per) > 0  # every channel fired
 
 
+BGK = (2.0e8, 3.0e5)  # frequency (1/s), neutral_temperature_velocity (m/s)
+
+
+@pytest.mark.parametrize("vdim", [3, 1])
+def test_bgk_run_bit_exact(vdim):
+    """The legacy BGK branch of apply_collisions (src/Simulation.cpp:772-834)
+    on the RF discharge deck: every species relaxes to one neutral Maxwellian,
+    the engine and each species' normal_distribution (with its saved value)
+    shared, 60 steps; state, counts and the channel's energy change bit-exact."""
+    wl = W.ccp_helium(particles_per_cell=32, cells=32, seed=6, steps=10, table_rows=96, te_ev=4.0,
+                      vdim=vdim, bgk=BGK)
+    sim, f = _run_sim(f"bgk{vdim}v", wl)
+    c, nl, per = sim.collisions()
+    assert c == int(f["candidates"]) and nl == int(f["nulls"]) == 0
+    assert per[0][0] == int(f["per_channel"][0]) == c > 1000
+    assert sim.bgk_energy() == float(f["channel_energy"][0])
+
+
+def test_bgk_validation_messages():
+    """Simulation's collision checks (src/Simulation.cpp:95-100, :388-392)."""
+    wl = W.ccp_helium(particles_per_cell=4, cells=8, seed=6, steps=1, table_rows=16, bgk=BGK)
+    T = po.TableSet()
+    for bgk, msg in (((-1.0, 1.0), "collision frequency must be non-negative and finite"),
+                     ((float("nan"), 1.0), "collision frequency must be non-negative and finite"),
+                     ((1.0, float("inf")), "neutral_temperature_velocity must be non-negative and finite")):
+        wl.bgk = bgk
+        with pytest.raises(RuntimeError, match=msg):
+            po.Sim1D(po.config_from_workload(wl, T), 0)
+    wl.bgk = BGK
+    cfg = po.config_from_workload(W.ccp_helium(particles_per_cell=4, cells=8, seed=6, steps=1, table_rows=16), T)
+    cfg.bgk, cfg.bgk_frequency, cfg.bgk_neutral_velocity = 1, *BGK
+    with pytest.raises(RuntimeError, match="named collision models cannot be combined"):
+        po.Sim1D(cfg, 0)
+
+
 ND_CASES = {
     "sim2d_boris": (2, (16, 8), (0.0, 0.0, 0.7)),
     "sim2d_leapfrog": (2, (8, 8), (0.0, 0.0, 0.0)),
