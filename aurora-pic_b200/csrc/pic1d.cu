@@ -351,9 +351,36 @@ __device__ __forceinline__ void st_comp(double* d, float* f, unsigned long long 
     else d[i] = v;
 }
 
-// DIAG: the instantiation that also deposits the spatial collision energy (run
-// only inside a campaign-diagnostics window, so the plain pass keeps its
-// register allocation).
+// The legacy BGK branch, src/Simulation.cpp:772-834: with probability
+// 1 - exp(-nu dt) the particle relaxes to a neutral Maxwellian of standard
+// deviation vt, drawn from its own stream (the one its MCC would use; the two
+// models exclude each other), and the run's totals count it.  Returns the
+// energy change (hmw = m w / 2) through `change` and whether it relaxed.  Out
+// of line, with plain arguments, so that the pass keeps the register
+// allocation of runs without it.
+template <int VDIM>
+__device__ __noinline__ bool bgk_relax(uint64_t seed, unsigned idx, uint32_t step, uint32_t s, double prob, double vt,
+                                       double hmw, DevState* st, double& v, double& vy, double& vz, double& change) {
+    PhiloxStream rng(seed, idx, step, s);
+    if (!(uniform01(rng) < prob)) return false;
+    const double before = hmw * (v * v + (VDIM == 3 ? vy * vy + vz * vz : 0.0));
+    NormalState ns;
+    v = normal(ns, rng, 0.0, vt);
+    if (VDIM == 3) {
+        vy = normal(ns, rng, 0.0, vt);
+        vz = normal(ns, rng, 0.0, vt);
+    }
+    change = hmw * (v * v + (VDIM == 3 ? vy * vy + vz * vz : 0.0)) - before;
+    atomicAdd(&st->candidates, 1ull);
+    atomicAdd(&st->chan[0][0], 1ull);
+    atomicAdd(&st->chan_energy[0][0], change);
+    return true;
+}
+
+// DIAG: the instantiation that also deposits the spatial collision energy,
+// keeps the electric-work ledger and applies the legacy BGK model (run only
+// inside a campaign-diagnostics window, with the ledger or with BGK, so the
+// plain pass keeps its register allocation).
 template <int VDIM, bool DIRICHLET, bool F32, bool DIAG>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -434,30 +461,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 vc[k] = vh[k] + S.hqm * E * p.dt;
                 // electric-work ledger, src/Simulation.cpp:1109-1114
                 if (DIAG && p.ledger) wsum += 0.5 * S.mass * S.weight * (vc[k] * vc[k] - vo[k] * vo[k]);
-                if (p.bgk) {
-                    // the legacy BGK branch, src/Simulation.cpp:772-834: relax to a
-                    // neutral Maxwellian with probability 1 - exp(-nu dt), drawn from
-                    // the particle's stream (the one its MCC would use; the two
-                    // models exclude each other)
-                    PhiloxStream rng(p.seed, idx, mcc_step, (uint32_t)s);
-                    if (uniform01(rng) < p.bgk_prob) {
-                        const double hmw = 0.5 * S.mass * S.weight;
-                        const double before =
-                            hmw * (vc[k] * vc[k] + (VDIM == 3 ? vy[k] * vy[k] + vz[k] * vz[k] : 0.0));
-                        NormalState ns;
-                        vc[k] = normal(ns, rng, 0.0, p.bgk_vt);
-                        if (VDIM == 3) {
-                            vy[k] = normal(ns, rng, 0.0, p.bgk_vt);
-                            vz[k] = normal(ns, rng, 0.0, p.bgk_vt);
-                        }
-                        const double change =
-                            hmw * (vc[k] * vc[k] + (VDIM == 3 ? vy[k] * vy[k] + vz[k] * vz[k] : 0.0)) - before;
-                        atomicAdd(&st->candidates, 1ull);
-                        atomicAdd(&st->chan[0][0], 1ull);
-                        atomicAdd(&st->chan_energy[0][0], change);
-                        if (DIAG && p.coll_acc) collision_energy_deposit<DIRICHLET>(p, x[k], 0, change);
-                        queued[k] = -2;  // re-initialise the half step in phase C
-                    }
+                double change;
+                if (DIAG && p.bgk && bgk_relax<VDIM>(p.seed, idx, mcc_step, (uint32_t)s, p.bgk_prob, p.bgk_vt,
+                                             0.5 * S.mass * S.weight, st, vc[k], vy[k], vz[k], change)) {
+                    if (DIAG && p.coll_acc) collision_energy_deposit<DIRICHLET>(p, x[k], 0, change);
+                    queued[k] = -2;  // re-initialise the half step in phase C
                 }
                 if (mcc) {
                     const MccModelDev& M = p.model[S.model];
@@ -574,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_pass1d(Params1D p) {
                 }
                 // initialize_leapfrog_half_step after the collision, src/Simulation.cpp:924-926
                 vh[k] = vc[k] - S.hqm * E * p.dt;
-            } else if (queued[k] == -2) {
+            } else if (DIAG && queued[k] == -2) {
                 // the BGK particle's initialize_leapfrog_half_step, src/Simulation.cpp:829-833
                 vh[k] = vc[k] - S.hqm * E * p.dt;
             }
@@ -2012,7 +2020,7 @@ struct Sim1D {
 
     template <int VDIM, bool DIR, bool F32>
     void launch_kernels(const Params1D& q, int blocks, size_t smem, size_t post_smem, unsigned post, EvPair& ev) {
-        if (q.coll_acc || q.ledger)
+        if (q.coll_acc || q.ledger || q.bgk)
             k_pass1d<VDIM, DIR, F32, true><<<blocks, kThreads, smem, stream>>>(q);
         else
             k_pass1d<VDIM, DIR, F32, false><<<blocks, kThreads, smem, stream>>>(q);
