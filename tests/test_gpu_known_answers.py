@@ -1,11 +1,13 @@
 """The reference's own analytic known-answer tests, run on the device through
 the C ABI (tests/test_core.cpp of the reference: the spectral Poisson
-benchmarks :980-1066 and the permittivity contract :267-300, the
-constant-acceleration leapfrog :1068-1107, the Boris cyclotron rotations
-:1220-1358 and the zero-cross-section swarm :6187-6233), with the reference's
+benchmarks :980-1066 and the permittivity contract :267-300, the MCC
+envelopes :336-432, the constant-acceleration leapfrog :1068-1107, the Boris
+cyclotron rotations :1220-1358, the CIC deposit checks :1874-1966 and
+:2133-2146 and the zero-cross-section swarm :6187-6233), with the reference's
 tolerances where the device runs the same operation.  The periodic device
-solve takes power-of-two extents, so the Poisson benchmarks use the
-power-of-two meshes nearest to the reference's with the same Fourier modes."""
+solve takes power-of-two extents, so the Poisson and CIC benchmarks use
+power-of-two meshes near the reference's, with the same Fourier modes and
+particle positions."""
 import math
 
 import numpy as np
@@ -160,3 +162,123 @@ def test_zero_cross_section_swarm_drift_and_energy():
     assert abs(r.mean_energy_ev - mean) <= 1e-13 * mean, (r.mean_energy_ev, mean)
     assert abs(r.diffusion_longitudinal) <= 1e-30
     assert r.channel_collisions[0] == 0
+
+
+def test_cic_1d_dirichlet_boundary_half_volume():
+    """A particle on the left electrode (charge 2, weight 0.5, 5 nodes over
+    1 m) puts its whole charge on node 0 over half a control volume: rho[0] = 8
+    and the charge is conserved (the reference's 1D Dirichlet CIC check, 1e-12)."""
+    rho, _phi, _E, _eq = apic.deposit_solve_gather_1d(apic.DIRICHLET, 5, 1.0, 1.0, 0.0, 0.0, [2.0], [0.5],
+                                                      [np.array([0.0])])
+    vol = np.full(5, 0.25)
+    vol[0] = vol[-1] = 0.125
+    assert abs(rho[0] - 8.0) < 1e-12
+    assert abs(np.sum(rho * vol) - 1.0) < 1e-12
+
+
+def _deposit_nd(n, L, charge, weight, pos):
+    """rho of the periodic FP64 mesh after loading particles at `pos` ([dims][k])."""
+    dims = len(n)
+    cfg = apic.config_nd(dims=dims, n=n, length=L, dt=0.1, species=[(charge, 1.0, weight, 16)])
+    sim = apic.SimulationND(cfg)
+    pos = np.asarray(pos, dtype=np.float64)
+    p3 = np.zeros((3, pos.shape[1]))
+    p3[:dims] = pos
+    sim.load(0, p3, np.zeros((3, pos.shape[1])))
+    sim.initialize()
+    rho = sim.fields()[0]
+    sim.close()
+    return rho
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_cic_wrapped_deposit(dims):
+    """Two live particles of charge 2 x weight 0.5 on a periodic 4^dims mesh,
+    one of them outside the box (wrapped): the weights on the corner, x, y (and
+    z) nodes and the total charge of the reference's CIC check (1e-12)."""
+    n = (4,) * dims
+    if dims == 2:
+        rho = _deposit_nd(n, (1.0, 1.0), 2.0, 0.5, [[0.125, 1.125], [0.125, -0.125]])
+        idx = lambda i, j: j * 4 + i
+        assert abs(rho[idx(0, 0)] - 8.0) < 1e-12 and abs(rho[idx(1, 0)] - 8.0) < 1e-12
+        assert abs(rho[idx(0, 1)] - 4.0) < 1e-12
+        assert abs(rho.sum() * 0.25 * 0.25 - 2.0) < 1e-12
+    else:
+        rho = _deposit_nd(n, (1.0, 1.0, 1.0), 2.0, 0.5, [[0.125, 1.125], [0.125, -0.125], [0.125, 0.875]])
+        idx = lambda i, j, k: (k * 4 + j) * 4 + i
+        assert abs(rho[idx(0, 0, 0)] - 16.0) < 1e-12 and abs(rho[idx(1, 0, 0)] - 16.0) < 1e-12
+        assert abs(rho[idx(0, 1, 0)] - 8.0) < 1e-12 and abs(rho[idx(0, 0, 3)] - 8.0) < 1e-12
+        assert abs(rho.sum() * 0.25 ** 3 - 2.0) < 1e-12
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_cic_exact_shape_function(dims):
+    """One interior particle: the 4 (8) node densities are the bilinear
+    (trilinear) shape-function weights of the reference's M1 CIC benchmark and
+    the charge is conserved (1e-12; power-of-two meshes)."""
+    if dims == 2:
+        n, L, pos, q, w = (8, 8), (1.0, 1.5), (0.31, 0.44), -1.5, 2.0
+    else:
+        n, L, pos, q, w = (8, 8, 4), (1.2, 1.0, 0.8), (0.37, 0.46, 0.51), 1.25, 0.8
+    d = [l / k for l, k in zip(L, n)]
+    rho = _deposit_nd(n, L, q, w, [[p] for p in pos])
+    g = [p / dd for p, dd in zip(pos, d)]
+    i0 = [int(math.floor(x)) for x in g]
+    f = [x - i for x, i in zip(g, i0)]
+    expected = np.zeros(int(np.prod(n)))
+    cellvol = float(np.prod(d))
+    for corner in range(1 << dims):
+        w_c, idx, stride = 1.0, 0, 1
+        for a in range(dims):
+            b = (corner >> a) & 1
+            w_c *= f[a] if b else 1.0 - f[a]
+            idx += ((i0[a] + b) % n[a]) * stride
+            stride *= n[a]
+        expected[idx] += q * w * w_c / cellvol
+    assert np.max(np.abs(rho - expected)) < 1e-12
+    assert abs(rho.sum() * cellvol - q * w) < 1e-12
+
+
+def _elastic_model(angular=False):
+    """The reference's envelope gas: sigma(E) on the table (0, 0), (1, 0.5),
+    (2, 1), neutral density 1, max_frequency 2, infinitely heavy neutrals
+    (neutral_mass 0), unit particle mass; Henyey-Greenstein with a constant
+    mean cosine 0.8 when `angular`."""
+    tabs = apic.Tables()
+    kw = dict(angular=apic.HENYEY_GREENSTEIN, mu_energy=[0.0, 2.0], mu=[0.8, 0.8]) if angular else {}
+    ch = tabs.channel(W.ELASTIC, [0.0, 1.0, 2.0], [0.0, 0.5, 1.0], **kw)
+    return apic.mcc_model(0, [ch], 1.0, 2.0, 0.0, 0.0, 0, 64), tabs
+
+
+def test_mcc_elastic_envelopes():
+    """10000 collide calls at |v| = sqrt(2) over dt = 0.1 (the reference's MCC
+    envelope checks, on the device's Philox streams): candidates within
+    (1800, 2200), accepted elastic collisions within (620, 800), the speed kept
+    to 1e-14 and the scattered directions isotropic."""
+    m, _tabs = _elastic_model()
+    n = 10000
+    v0 = np.zeros((n, 3))
+    v0[:, 0] = math.sqrt(2.0)
+    v, stats = apic.collide3(m, 1.0, v0, 0.1, seed=8128, step=0, stream=0)
+    cand = sum(s.candidates for s in stats)
+    hits = np.array([s.channel_collisions[0] for s in stats])
+    assert 1800 < cand < 2200, cand
+    assert 620 < hits.sum() < 800, hits.sum()
+    assert np.max(np.abs(np.linalg.norm(v, axis=1) - math.sqrt(2.0))) < 1e-14
+    mean_dir = (v[hits > 0] / math.sqrt(2.0)).sum(axis=0)
+    assert np.all(np.abs(mean_dir) < 0.1 * hits.sum()), mean_dir
+
+
+def test_mcc_henyey_greenstein_mean_cosine():
+    """20000 calls with Henyey-Greenstein scattering of mean cosine 0.8: the
+    particles scattered exactly once keep the configured mean cosine within
+    0.04 and their speed to 1e-14 (the reference's anisotropic envelope)."""
+    m, _tabs = _elastic_model(angular=True)
+    n = 20000
+    v0 = np.zeros((n, 3))
+    v0[:, 0] = math.sqrt(2.0)
+    v, stats = apic.collide3(m, 1.0, v0, 0.1, seed=161803, step=0, stream=0)
+    once = np.array([s.channel_collisions[0] == 1 for s in stats])
+    assert np.max(np.abs(np.linalg.norm(v, axis=1) - math.sqrt(2.0))) < 1e-14
+    assert once.sum() > 1200
+    assert abs(np.mean(v[once, 0] / math.sqrt(2.0)) - 0.8) < 0.04
