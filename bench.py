@@ -892,7 +892,11 @@ def bench_swarm(args, rank, dist):
     return {
         "value": value, "ms_per_step": 1e3 * t_sat / max(1, (g1 - g0) * spl), "dtype": "f32" if prec == apic.FP32 else "f64",
         "config": {"workload": WORKLOAD_SWARM, "form": ("FP32 electron velocity + displacement and FP32 collision "
-                                                        "loops; FP64 tallies") if prec == apic.FP32 else
+                                                        "loops; FP64 tallies; error against the FP64 form "
+                                                        "(tests/test_gpu_swarm.py): over 12 seeds per field the "
+                                                        "ensemble means of drift velocity, mean energy and the "
+                                                        "ionization rate coefficient within 3 combined standard "
+                                                        "errors") if prec == apic.FP32 else
                    "FP64 electrons", "saturation_requests": len(batch), "steps_per_launch": spl,
                    "autotuned": tuned["table"] if tuned else None,
                    "l2": "electron state of the batch larger than L2"},
