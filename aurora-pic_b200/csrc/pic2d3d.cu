@@ -993,9 +993,13 @@ __device__ __forceinline__ void push_run(const ParamsND& p, const SpeciesND& S, 
         }
     }
     // each lane's last run: summed over the lanes that end in the same cell
+    // 3D: segments of at most 4 lanes (a cell's run spans about 4 lanes at 8
+    // particles per cell): two shuffle steps instead of five per node, for a
+    // few more commits; measured 5.89 -> 5.69 ms per 256^3 step
+    constexpr int RSEG = DIM == 3 ? 4 : 32;
     const unsigned key = rcell;
     const unsigned prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const bool head = lane == 0 || prev != key;
+    const bool head = (lane & (RSEG - 1)) == 0 || prev != key;
     const unsigned heads = __ballot_sync(0xffffffffu, head);
     const int start = 31 - __clz(heads & (0xFFFFFFFFu >> (31 - lane)));
     const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
@@ -1003,7 +1007,7 @@ __device__ __forceinline__ void push_run(const ParamsND& p, const SpeciesND& S, 
     for (int j = 0; j < NN; ++j) {
         unsigned q = racc[j];
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
+        for (int d = 1; d < RSEG; d <<= 1) {
             const unsigned t = __shfl_up_sync(0xffffffffu, q, d);
             if (lane - d >= start) q += t;
         }
