@@ -993,10 +993,11 @@ __device__ __forceinline__ void push_run(const ParamsND& p, const SpeciesND& S, 
         }
     }
     // each lane's last run: summed over the lanes that end in the same cell
-    // 3D: segments of at most 4 lanes (a cell's run spans about 4 lanes at 8
-    // particles per cell): two shuffle steps instead of five per node, for a
-    // few more commits; measured 5.89 -> 5.69 ms per 256^3 step
-    constexpr int RSEG = DIM == 3 ? 4 : 32;
+    // segments of at most 4 lanes in 3D (a cell's run spans about 4 lanes at 8
+    // particles per cell) and 8 in 2D: two or three shuffle steps instead of
+    // five per node, for a few more commits; measured 5.89 -> 5.69 ms per
+    // 256^3 step and 0.371 -> 0.368 ms per 512^2 step
+    constexpr int RSEG = DIM == 3 ? 4 : 8;
     const unsigned key = rcell;
     const unsigned prev = __shfl_up_sync(0xffffffffu, key, 1);
     const bool head = (lane & (RSEG - 1)) == 0 || prev != key;
