@@ -118,6 +118,15 @@ class Clocks:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
+            # the sampler is running before the timed region starts, so even a
+            # region shorter than the sampling period gets its first sample
+            # (waited for at most 3 s)
+            t0 = time.time()
+            while time.time() - t0 < 3.0 and self.proc.poll() is None:
+                self.f.flush()
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self
